@@ -1,0 +1,390 @@
+"""Benchmark of the vertical-physics hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config eddy_1440x1080x75]
+
+A step is one pass of the path over the whole synthetic domain: Wright EOS ->
+coefficient assembly (PP81 + KPP + Bryan-Lewis gate) -> implicit momentum
+viscosity (u, v) -> implicit tracer diffusion of every tracer with the KPP
+non-local tendency.  The metric is cells/s (nx*ny*nz per step, the
+reference's Mcells/s convention, benchmarks/bench_ocean.F90:149-150) on the
+1440x1080x75 eddy-permitting configuration with T, S and 2 passives, FP64.
+
+One JSON line from rank 0:
+  value        device-resident cells/s (state in HBM before timing)
+  e2e          cells/s through the C ABI with host buffers: every step
+               uploads the state (h, u, v, tracers, forcing) from pinned host
+               memory with vphys_set_field and downloads the results (u, v,
+               tracers, kv, kt, ks, bl_depth) with vphys_get_field
+  roofline     dominant kernel: algorithmic bytes / its CUDA-event time vs the
+               measured HBM copy bandwidth (MEASURED_PEAKS.json)
+  cpu_baseline the CPU restatement (oracle) on the host cores, bounded sample
+
+Multi-GPU (torchrun): every rank owns an independent full-size domain
+(columns shard with no data-path exchange); value = all ranks' cells / the
+slowest rank's time (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "vertical-physics cells/s on 1 B200: learned+FP32 vs plain FP64 at stated error"
+PEAK_FALLBACK_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="eddy_1440x1080x75")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-sample", default="360x270", help="nx x ny of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return PEAK_FALLBACK_GBS, "fallback"
+
+
+def bytes_per_cell(ntr: int, nz: int) -> dict:
+    """Algorithmic FP64 bytes per cell (each input read once, each output written once)."""
+    ifc = (nz + 1) / nz
+    return {
+        "eos": 8 * 4.0,                                   # h, T, S -> rho
+        "assemble": 8 * 4.0 + 24 * ifc,                   # h, rho, u, v -> kv, kt, ks
+        "momentum": 8 * 4.0 + 16.0,                      # h, kv, u, v -> u, v
+        "tracers": 8 * 2.0 + 16.0 * ntr,                  # h, kt, c_t -> c_t
+        # whole path at the interface (h, rho, u, v, c_t in; u, v, c_t, kv, kt, ks out)
+        "path": 8 * (4 + ntr) + 8 * (2 + ntr) + 24 * ifc,
+    }
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def traffic_from_profiles(kernel: str):
+    """dram bytes per launch of `kernel` from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "traffic.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        parts = line.split()
+        if len(parts) >= 2 and parts[0] == kernel:
+            try:
+                return float(parts[1])
+            except ValueError:
+                return None
+    return None
+
+
+# ---------------------------------------------------------------------------
+# CPU arm (the oracle: the C restatement of the reference)
+# ---------------------------------------------------------------------------
+def cpu_run(cfg_name: str, sample: str, steps: int, warmup: int):
+    from oracle import oracle as o
+    from roundabout_b200.config import hot_path_config
+    from roundabout_b200.synthetic import CONFIGS, make_columns
+
+    o.build()
+    spec = dict(CONFIGS[cfg_name])
+    sx, sy = (int(x) for x in sample.lower().split("x"))
+    spec["nx"], spec["ny"] = min(sx, spec["nx"]), min(sy, spec["ny"])
+    ntr = spec.pop("ntracers")
+    cols = make_columns(ntracers=ntr, seed=1234, **spec)
+    cfg = hot_path_config(ntracers=ntr)
+    st = o.OracleState(cols.nx, cols.ny, cols.nz, ntr)
+    st.seed_backgrounds(cfg)
+    st.h[...] = cols.h
+    st.u[...] = cols.u
+    st.v[...] = cols.v
+    for t in range(ntr):
+        st.tracers[t][...] = cols.tracers[t]
+    st.tau_x[...] = cols.tau_x
+    st.tau_y[...] = cols.tau_y
+    st.q_heat[...] = cols.q_heat
+    st.q_salt[...] = cols.q_salt
+    st.wet[...] = cols.wet
+    st.stress_mag_from_tau()
+    threads = os.cpu_count() or 1
+    o.set_threads(threads)
+    for _ in range(warmup):
+        st.call("vpo_step", cfg, 3600.0, 1)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        st.call("vpo_step", cfg, 3600.0, 1)
+    el = time.perf_counter() - t0
+    cells = cols.nx * cols.ny * cols.nz
+    return {"value": cells * steps / el, "unit": "cells/s", "cores": threads, "kind": "port",
+            "sample": f"{cols.nx}x{cols.ny}x{cols.nz} slice of the same generator, {ntr} tracers, {steps} steps "
+                      f"(C restatement of the reference, -O2 -ffp-contract=off, OpenMP)",
+            "ms_per_step": el / steps * 1e3}
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from roundabout_b200.synthetic import CONFIGS
+
+    spec = dict(CONFIGS[args.config])
+    ntr = spec["ntracers"]
+    nx, ny, nz = spec["nx"], spec["ny"], spec["nz"]
+    config_out = {"workload": args.config, "nx": nx, "ny": ny, "nz": nz, "tracers": ntr, "dt_s": 3600.0,
+                  "closures": "PP81+KPP+Bryan-Lewis, Wright EOS, hvel_mom6 z_clear",
+                  "l2": "working set >> 126 MB L2 (no flush needed)", "land_frac": spec["land_frac"]}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        r = cpu_run(args.config, args.cpu_sample, max(1, args.steps), max(0, min(args.warmup, 1)))
+        line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": "cells/s",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config_out,
+                "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "e2e": {"value": r["value"], "unit": "cells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(local)
+
+    from roundabout_b200 import _ffi
+    from roundabout_b200.column import VerticalPhysics
+    from roundabout_b200.config import hot_path_config
+    from roundabout_b200.synthetic import make_columns
+
+    gen_spec = dict(spec)
+    gen_spec.pop("ntracers")
+    cols = make_columns(ntracers=ntr, seed=1234 + rank, **gen_spec)
+    cfg = hot_path_config(ntracers=ntr)
+    vp = VerticalPhysics(nx, ny, nz, ntr, cfg)
+    vp.load_columns(cols)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    dt = 3600.0
+    for _ in range(max(3, args.warmup)):
+        vp.step(dt, 1)
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier()
+        ev0.record()
+        for _ in range(args.steps):
+            vp.step(dt, 1)
+        ev1.record()
+        barrier()
+    ms = ev0.elapsed_time(ev1)
+    ms = max_over_ranks(ms)
+    cells = nx * ny * nz
+    value = cells * args.steps * world / (ms / 1e3)
+
+    # ---- per-kernel device times (same stream, CUDA events) ----
+    reps = 5
+    stage_ms = {}
+    stages = {
+        "eos": lambda: vp.eos(),
+        "assemble": lambda: vp.assemble(),
+        "momentum": lambda: vp.vdiff_momentum(dt),
+        "tracers": lambda: vp.lib.vphys_step and _tracers_fused(vp, dt),
+    }
+    for name, fn in stages.items():
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        stage_ms[name] = a.elapsed_time(b) / reps
+    bpc = bytes_per_cell(ntr, nz)
+    kernel_of = {"eos": "k_eos_wright", "assemble": "k_assemble", "momentum": "k_momentum",
+                 "tracers": "k_tracers"}
+    dom = max(("assemble", "momentum", "tracers", "eos"), key=lambda k: stage_ms[k])
+    peak, peak_kind = peaks()
+    achieved = bpc[dom] * cells / (stage_ms[dom] / 1e3) / 1e9
+    traffic = traffic_from_profiles(kernel_of[dom])
+    roofline = {"bound": "hbm", "kernel": kernel_of[dom], "achieved": round(achieved, 1), "peak": peak,
+                "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+                "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
+                else "fallback 6.65 TB/s",
+                "algorithmic_bytes_per_cell": round(bpc[dom], 2),
+                "stage_ms": {k: round(v, 4) for k, v in stage_ms.items()},
+                "path_bytes_per_cell": round(bpc["path"], 2),
+                "path_achieved_gbs": round(bpc["path"] * cells / (ms / args.steps / 1e3) / 1e9, 1)}
+
+    # ---- end to end through the C ABI with host buffers ----
+    e2e = None
+    if args.e2e_steps > 0:
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a.T)).pin_memory()  # noqa: E731
+        host_in = {"h": pin(cols.h), "u": pin(cols.u), "v": pin(cols.v), "q_heat": pin(cols.q_heat),
+                   "q_salt": pin(cols.q_salt), "tau_x": pin(cols.tau_x), "tau_y": pin(cols.tau_y)}
+        host_tr = [pin(t) for t in cols.tracers]
+        host_out = {n: torch.empty(tuple(reversed(vp.shape(n))), dtype=torch.float64).pin_memory()
+                    for n in ("kv", "kt", "ks", "bl_depth")}
+        lib, hdl = vp.lib, vp.handle
+        import ctypes
+
+        def put(fid, t):
+            _ffi.check(lib.vphys_set_field(hdl, fid, ctypes.c_void_p(t.data_ptr()), t.numel()), "set_field")
+
+        def take(fid, t):
+            _ffi.check(lib.vphys_get_field(hdl, fid, ctypes.c_void_p(t.data_ptr()), t.numel()), "get_field")
+
+        def e2e_step():
+            for n, t in host_in.items():
+                put(_ffi.FIELD_NAMES[n], t)
+            for k, t in enumerate(host_tr):
+                put(_ffi.FIELD_TRACER0 + k, t)
+            _ffi.check(lib.vphys_stress_mag(hdl), "stress_mag")
+            _ffi.check(lib.vphys_step(hdl, dt, 1), "step")
+            take(_ffi.FIELD_U, host_in["u"])
+            take(_ffi.FIELD_V, host_in["v"])
+            for k, t in enumerate(host_tr):
+                take(_ffi.FIELD_TRACER0 + k, t)
+            for n, t in host_out.items():
+                take(_ffi.FIELD_NAMES[n], t)
+
+        h2d = sum(t.numel() * 8 for t in host_in.values()) + sum(t.numel() * 8 for t in host_tr)
+        d2h = (host_in["u"].numel() + host_in["v"].numel()) * 8 + sum(t.numel() * 8 for t in host_tr) + \
+            sum(t.numel() * 8 for t in host_out.values())
+        e2e_step()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        barrier()
+        el = max_over_ranks(time.perf_counter() - t0)
+        e2e = {"value": cells * args.e2e_steps * world / el, "unit": "cells/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "ms_per_step": el / args.e2e_steps * 1e3,
+               "what": "C-ABI vphys_set_field (pinned host -> HBM) of h, u, v, tracers, forcing; vphys_step; "
+                       "vphys_get_field of u, v, tracers, kv, kt, ks, bl_depth"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_run(args.config, args.cpu_sample, 2, 1)
+        cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    clocks = clk.summary()
+    line = {"metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config_out,
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": 4 * args.steps, "clocks": clocks,
+            "mode": "plain FP64, bit-identical to the CPU restatement"}
+    vp.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def _tracers_fused(vp, dt):
+    """The step's tracer launch: diffusion of every tracer with the fused
+    non-local tendency (vphys_vdiff_tracers + vphys_nonlocal in one kernel is
+    what vphys_step runs; timed here through the diffusion entry point)."""
+    vp.vdiff_tracers(dt)
+    return True
+
+
+if __name__ == "__main__":
+    main()

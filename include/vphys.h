@@ -1,0 +1,289 @@
+/* vphys.h -- C ABI of the B200-native vertical-physics library (libvphys.so).
+ *
+ * The library replaces, behind plain C entry points, the vertical-physics
+ * hot path of Roundabout (JorgeG94/roundabout):
+ *
+ *   vmix_compute_pp81 -> vmix_apply_kpp_overlay -> vmix_split_kd_heat_salt
+ *   -> vmix_assemble -> vdiff_apply_momentum -> vdiff_apply_tracers
+ *   -> vmix_apply_nonlocal_tendencies            (+ the Wright EOS precursor)
+ *
+ * i.e. the body of `vmix_build_coefficients` + `vmix_apply_in_stage`
+ * (src/core/ocean/dynamics/split_rk2/rdb_ocean_dyn.F90:1473-1634, 1636-1900).
+ * Every entry point cites the reference routine it replaces.
+ *
+ * Conventions (identical to the reference, include/rdb_ocean.h:1-60):
+ *   - every array is FP64, Fortran order (i fastest, then j, then k);
+ *   - layers are bottom-up: k = 1 (index 0 here) is the BED, k = nz the surface;
+ *   - cell arrays are (nx, ny, nz); interface arrays (kv, kt, ks) are
+ *     (nx, ny, nz+1) with interface k at the bottom of layer k;
+ *   - u-face arrays are (nx+1, ny, nz), v-face arrays (nx, ny+1, nz);
+ *   - 2-D column arrays are (nx, ny); 2-D u/v face arrays (nx+1, ny) / (nx, ny+1);
+ *   - tracers are stored as CONCENTRATION; a layer with h <= 1.5e-4 m
+ *     (H_VANISHED) is an inert filler that keeps its value.
+ *
+ * Memory: the handle owns one device buffer per field (allocated at create,
+ * in HBM); vphys_bind() replaces any of them by a caller-owned device pointer
+ * (zero copy: a Fortran caller passes `c_loc` of an OpenACC/CUDA device
+ * array, a Python caller a torch tensor's data_ptr()).  vphys_set_field() /
+ * vphys_get_field() copy between host memory and the current device buffer.
+ *
+ * Errors: every entry point returns an int status (VPHYS_OK = 0); the
+ * specific reason is pushed onto an error ring read by vphys_last_error()
+ * (same snprintf-style contract as rdb_ocean_last_error,
+ * include/rdb_ocean.h:314).  Nothing traps or aborts.
+ *
+ * Threading: a handle is bound to one CUDA stream (vphys_set_stream); it is
+ * not thread-safe per handle.  Entry points enqueue work on that stream and
+ * return without synchronising, except where stated.
+ */
+#ifndef VPHYS_H
+#define VPHYS_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (values of the reference where one exists:
+ *      include/rdb_ocean.h:79-89) ------------------------------------ */
+#define VPHYS_OK 0
+#define VPHYS_ERR_CONFIG 2          /* RDB_OCEAN_ERR_CONFIG_VALIDATE */
+#define VPHYS_ERR_BAD_HANDLE 10     /* RDB_OCEAN_ERR_BAD_HANDLE */
+#define VPHYS_ERR_NOT_INITIALISED 12
+#define VPHYS_ERR_NOT_FOUND 13      /* unknown field id */
+#define VPHYS_ERR_BAD_SHAPE 14      /* RDB_OCEAN_ERR_BAD_SHAPE */
+#define VPHYS_ERR_CUDA 30           /* a CUDA runtime call failed */
+#define VPHYS_ERR_GUARD 31          /* vmix_guard tripped: negative/NaN K
+                                       (vmix_assemble status=1,
+                                       rdb_ocean_vmix.F90:2264-2277) */
+#define VPHYS_ERR_TOO_DEEP 32       /* nz > VPHYS_NZ_MAX */
+#define VPHYS_ERR_ALLOC 33          /* device allocation failed */
+
+/* Largest nz the column kernels accept; the reference's own per-column
+ * stack bound NZ_STACK_MAX (src/core/rdb_constants.F90:107-124) is 128 and
+ * must cover nz + 1. */
+#define VPHYS_NZ_MAX 127
+
+/* interior_closure tags (rdb_ocean_vmix.F90:146-158) */
+#define VPHYS_INTERIOR_PP81 1
+#define VPHYS_INTERIOR_NONE 4
+
+/* ---- configuration ---------------------------------------------------
+ * Every knob the path reads, with the reference default
+ * (ocean_vmix_t rdb_ocean_vmix.F90:198-483; ocean_vdiff_t
+ * rdb_ocean_vdiff.F90:78-260; namelist defaults src/core/rdb_config.F90:
+ * 1872-1893, 1936-1945).  vphys_config_default() fills them. */
+typedef struct vphys_config {
+    /* closure selection */
+    int use_closure;          /* 1: PP81/none + contributors + assembly */
+    int interior_closure;     /* VPHYS_INTERIOR_PP81 (default) | _NONE */
+    int use_kpp;              /* KPP overlay (default 0 in ocean_vmix_t) */
+    int bkgnd_profile;        /* Bryan-Lewis background (default 0) */
+    int vmix_guard;           /* negative/NaN guard before the clip (0) */
+    int kd_smooth_iterations; /* 1-2-1 smoothing passes (0) */
+    int conv_enable;          /* convective adjustment contributor (0) */
+    int pad0;
+    /* PP81 (rdb_ocean_vmix.F90:233-265) */
+    double pp81_nu0;          /* 1e-2 */
+    double pp81_nu_bg;        /* 1e-4 */
+    double pp81_kappa_bg;     /* 1e-5 */
+    double pp81_alpha;        /* 5 */
+    double rho0;              /* 1035 */
+    double shear2_floor;      /* 1e-10 */
+    /* KPP (rdb_ocean_vmix.F90:306-339) */
+    double ri_crit;           /* 0.3 */
+    double cs_nonlocal;       /* 6.3 */
+    double c_vt2;             /* 1.8 */
+    double alpha_T;           /* dimensional, kg m-3 K-1 (1.7e-4 default) */
+    double beta_S;            /* dimensional, kg m-3 psu-1 (7.6e-4 default) */
+    double cp;                /* 3992 (SEAWATER_CP_DEFAULT) */
+    /* KV_ML_INVZ2 surface band (rdb_ocean_vmix.F90:309-322) */
+    double kv_ml_invz2;       /* 0 = off */
+    double hmix_fixed;        /* 20 */
+    /* convection (rdb_ocean_vmix.F90:532-555) */
+    double conv_kd;           /* 1 */
+    double conv_prandtl;      /* 1 */
+    double conv_n2_thresh;    /* 0 */
+    /* assembly gate (rdb_ocean_vmix.F90:341-371) */
+    double kv_bg;             /* = pp81_nu_bg */
+    double kt_bg;             /* = pp81_kappa_bg */
+    double ks_bg;             /* = pp81_kappa_bg */
+    double kv_max;            /* huge */
+    double kd_max;            /* huge */
+    /* Bryan-Lewis (rdb_ocean_vmix.F90:383-410) */
+    double bkgnd_kd_sfc;      /* 1e-5 */
+    double bkgnd_kd_deep;     /* 1.3e-4 */
+    double bkgnd_z0;          /* 2500 */
+    double bkgnd_delta;       /* 222 */
+    double bkgnd_prandtl;     /* -1 (off) */
+    /* Wright EOS reference pressure (rdb_eos.F90:909-959) */
+    double eos_p_ref;         /* 0 Pa */
+    /* momentum vdiff (ocean_vdiff_t) */
+    int hvel_mom6;            /* 1 (namelist default) */
+    int hvel_harmonic;        /* 0 */
+    int hvel_upwind;          /* 1 */
+    int use_harmonic;         /* 0 */
+    int implicit_stress;      /* 0: wind stress folded into the top row */
+    int implicit_drag;        /* 0: bottom drag folded into the bed row */
+    int zlevel_faces;         /* 0 */
+    int bbl_glue;             /* 0 (latched off without a bottom drag) */
+    double hbbl_visc;         /* 10 */
+    double bbl_piston;        /* 3e-4 */
+    double kv_bbl_bg;         /* 1e-4 */
+    /* tracer registry roles (0-based tracer index, -1 = absent);
+     * rdb_multilayer_state.F90:550-551 puts S first, T second */
+    int idx_temperature;      /* 1 */
+    int idx_salinity;         /* 0 */
+    int idx_pseudo_salt;      /* -1 */
+    /* step options */
+    int eos_in_step;          /* 1: vphys_step runs the Wright EOS first */
+    int remnant;              /* 1: momentum also writes visc_rem_u/v */
+    int budgets;              /* 1: tracers accumulate heat/salt budgets */
+} vphys_config;
+
+/* ---- field ids (vphys_bind / vphys_set_field / vphys_get_field) ----- */
+enum vphys_field {
+    VPHYS_FIELD_H = 0,          /* in      (nx, ny, nz)     layer thickness */
+    VPHYS_FIELD_RHO = 1,        /* in/out  (nx, ny, nz)     potential density */
+    VPHYS_FIELD_U = 2,          /* in/out  (nx+1, ny, nz)   u_face_x_layer */
+    VPHYS_FIELD_V = 3,          /* in/out  (nx, ny+1, nz)   v_face_y_layer */
+    VPHYS_FIELD_KV = 4,         /* out     (nx, ny, nz+1) */
+    VPHYS_FIELD_KT = 5,         /* out     (nx, ny, nz+1) */
+    VPHYS_FIELD_KS = 6,         /* out     (nx, ny, nz+1) */
+    VPHYS_FIELD_BL_DEPTH = 7,   /* in/out  (nx, ny)  lagged KPP h_b (state) */
+    VPHYS_FIELD_B0 = 8,         /* out     (nx, ny)  surface buoyancy flux */
+    VPHYS_FIELD_STRESS_MAG = 9, /* in      (nx, ny)  |tau| at cell centres */
+    VPHYS_FIELD_Q_HEAT = 10,    /* in      (nx, ny)  W m-2 */
+    VPHYS_FIELD_Q_SALT = 11,    /* in      (nx, ny) */
+    VPHYS_FIELD_WET = 12,       /* in      (nx, ny)  1 wet, 0 land */
+    VPHYS_FIELD_TAU_X = 13,     /* in      (nx+1, ny) */
+    VPHYS_FIELD_TAU_Y = 14,     /* in      (nx, ny+1) */
+    VPHYS_FIELD_LAMBDA_BOT_U = 15, /* in   (nx+1, ny)  1/s */
+    VPHYS_FIELD_LAMBDA_BOT_V = 16, /* in   (nx, ny+1) */
+    VPHYS_FIELD_VISC_REM_U = 17,   /* out  (nx+1, ny, nz) */
+    VPHYS_FIELD_VISC_REM_V = 18,   /* out  (nx, ny+1, nz) */
+    VPHYS_FIELD_GAMMA_T = 19,   /* out     (nx, ny, nz+1) KPP non-local T flux */
+    VPHYS_FIELD_GAMMA_S = 20,   /* out     (nx, ny, nz+1) */
+    VPHYS_FIELD_HEAT_BUDGET = 21, /* in/out (nx, ny, nz) */
+    VPHYS_FIELD_SALT_BUDGET = 22, /* in/out (nx, ny, nz) */
+    VPHYS_FIELD_K_TOP_U = 23,   /* in int32 (nx+1, ny), 1-based (default nz) */
+    VPHYS_FIELD_K_TOP_V = 24,   /* in int32 (nx, ny+1) */
+    VPHYS_FIELD_K_BOT_U = 25,   /* in int32 (nx+1, ny), 1-based (default 1) */
+    VPHYS_FIELD_K_BOT_V = 26,   /* in int32 (nx, ny+1) */
+    VPHYS_FIELD_TRACER0 = 64    /* in/out  (nx, ny, nz); tracer t is
+                                   VPHYS_FIELD_TRACER0 + t */
+};
+
+typedef struct vphys_handle_s *vphys_handle;
+
+/* ---- lifecycle ------------------------------------------------------- */
+
+/* Fill *cfg with the reference defaults listed above. */
+int vphys_config_default(vphys_config *cfg);
+
+/* Allocate a handle for an (nx, ny, nz) grid with ntracer tracers and
+ * allocate every field in HBM (zeroed; k_top = nz, k_bot = 1, wet = 1).
+ * Replaces ocean_vmix_init + ocean_vdiff_init + vmix_seed_backgrounds
+ * (rdb_ocean_vmix.F90:798-913, rdb_ocean_vdiff.F90:328-372): kv = kv_bg,
+ * kt = ks = kt_bg on interior interfaces, 0 on the bed and surface ones.
+ * nz must be in [1, VPHYS_NZ_MAX].  On failure *out is NULL. */
+int vphys_create(int nx, int ny, int nz, int ntracer, const vphys_config *cfg,
+                 vphys_handle *out);
+
+/* Idempotent on NULL; frees every handle-owned buffer; *h = NULL. */
+int vphys_destroy(vphys_handle *h);
+
+/* Replace the configuration (validated; VPHYS_ERR_CONFIG on a bad one). */
+int vphys_set_config(vphys_handle h, const vphys_config *cfg);
+int vphys_get_config(vphys_handle h, vphys_config *cfg);
+
+/* Run the handle's work on this CUDA stream (cudaStream_t as void*;
+ * NULL = the legacy default stream). */
+int vphys_set_stream(vphys_handle h, void *stream);
+
+/* Zero-copy: use the caller's device array for `field` from now on.
+ * The pointer must stay valid while the handle uses it; NULL restores the
+ * handle-owned buffer. */
+int vphys_bind(vphys_handle h, int field, void *device_ptr);
+
+/* Synchronous host<->device copies of a whole field (n = element count,
+ * checked against the field's shape: VPHYS_ERR_BAD_SHAPE).  Double fields
+ * take double*, the K_TOP/K_BOT fields int32*. */
+int vphys_set_field(vphys_handle h, int field, const void *host, size_t n);
+int vphys_get_field(vphys_handle h, int field, void *host, size_t n);
+
+/* Current device pointer and shape of a field, like
+ * rdb_ocean_get_kv_ptr(handle, ptr, nx, ny, nz, gen)
+ * (include/rdb_ocean.h:378-385); *gen = number of completed vphys_step
+ * steps.  The pointer is a DEVICE pointer. */
+int vphys_get_ptr(vphys_handle h, int field, void **ptr, int *nx, int *ny,
+                  int *nz, int *gen);
+
+/* ---- the hot path, stage by stage ------------------------------------ */
+
+/* Wright (1997) EOS at eos_p_ref: rho from (T, S, h); vanished layers take
+ * rho0.  Replaces eos_wright_impl (src/equation_of_state/rdb_eos.F90:909-959). */
+int vphys_eos_wright(vphys_handle h);
+
+/* |tau| at cell centres from the face stresses TAU_X/TAU_Y into STRESS_MAG.
+ * Replaces ocean_surfstress_derived_impl
+ * (rdb_ocean_surface_stress.F90:858-875). */
+int vphys_stress_mag(vphys_handle h);
+
+/* The whole coefficient build: interior closure (PP81 or background seed),
+ * KPP overlay (+ bl_depth, b0, gamma_t/gamma_s), KV_ML_INVZ2, convection,
+ * heat/salt split, assembly gate (guard, Bryan-Lewis or scalar floors,
+ * ceilings, optional 1-2-1 smoothing).  Replaces vmix_build_coefficients
+ * (rdb_ocean_dyn.F90:1473-1634) with vmix_compute_pp81
+ * (rdb_ocean_vmix.F90:1007-1074), vmix_apply_kpp_overlay (1076-1516),
+ * vmix_add_kv_ml_invz2 (1716-1766), vmix_apply_convection (1768-1849),
+ * vmix_split_kd_heat_salt (1850-1934), vmix_assemble (2183-2366).
+ * Returns VPHYS_ERR_GUARD (after finishing the clip, like the reference's
+ * status=1 path) when vmix_guard is on and a negative/NaN K was seen; this
+ * return synchronises the stream. */
+int vphys_assemble(vphys_handle h);
+
+/* Backward-Euler vertical viscosity on U and V with kv.  Replaces
+ * vdiff_apply_momentum -> diffuse_velocity_columns_impl
+ * (rdb_ocean_vdiff.F90:455-718, 1416-1926). */
+int vphys_vdiff_momentum(vphys_handle h, double dt);
+
+/* Backward-Euler vertical diffusion: kt on temperature, ks on salinity and
+ * every other tracer.  Replaces vdiff_apply_tracers
+ * (rdb_ocean_vdiff.F90:1107-1414). */
+int vphys_vdiff_tracers(vphys_handle h, double dt);
+
+/* KPP non-local tendencies on T (gamma_t), S and pseudo-salt (gamma_s),
+ * using the gamma of the last vphys_assemble.  Replaces
+ * vmix_apply_nonlocal_tendencies (rdb_ocean_vmix.F90:1605-1714). */
+int vphys_nonlocal(vphys_handle h, double dt);
+
+/* n_steps of the whole chain (the body of vmix_apply_in_stage on a thermo
+ * step, rdb_ocean_dyn.F90:1636-1900): [EOS] -> assemble -> momentum ->
+ * tracers -> non-local, with the tracer solve and the non-local tendency
+ * fused.  Asynchronous; safe to capture in a CUDA graph once the handle's
+ * buffers are allocated.  n_steps <= 0 is a successful no-op. */
+int vphys_step(vphys_handle h, double dt, int n_steps);
+
+/* Block until the handle's stream is idle; VPHYS_ERR_CUDA on a CUDA error. */
+int vphys_synchronize(vphys_handle h);
+
+/* ---- errors ------------------------------------------------------------
+ * Ring of recent messages, index 0 = most recent.  Copies up to cap bytes
+ * (NUL-terminated if room), returns the full message length; 0 when idx is
+ * out of range or cap <= 0 (rdb_ocean_last_error, include/rdb_ocean.h:314). */
+int vphys_last_error(int idx, char *buf, int cap);
+
+/* Library version string (static storage). */
+const char *vphys_version(void);
+
+/* sizeof(vphys_config) as compiled into the library, so a binding in another
+ * language can verify its mirror of the struct before passing one. */
+size_t vphys_config_sizeof(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VPHYS_H */

@@ -1,0 +1,964 @@
+/* vphys_oracle.c -- CPU FP64 restatement of Roundabout's vertical-physics hot
+ * path.  TEST INFRASTRUCTURE ONLY (see vphys_oracle.h).  Each routine cites
+ * the reference lines it restates; loop variables are 1-based like the
+ * Fortran so the index arithmetic can be read against it line by line.
+ *
+ * Build: gcc -O2 -ffp-contract=off -fopenmp -fPIC -shared (oracle/Makefile).
+ */
+#include "vphys_oracle.h"
+
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* ---- constants (src/core/rdb_constants.F90:37, 44, 67, 85, 94) ---- */
+static const double GRAVITY = 9.80665;
+static const double H_VANISHED = 1.5e-4;
+static const double H_DIV_EPS = 1.0e-20;
+static const double PI_ = 3.141592653589793115997963468544185161590576171875; /* 4*atan(1) */
+
+/* Fortran MAX/MIN on finite operands. */
+static inline double fmx(double a, double b) { return a > b ? a : b; }
+static inline double fmn(double a, double b) { return a < b ? a : b; }
+
+/* 1-based Fortran-order accessors. */
+#define C3(a, i, j, k) (a)[((size_t)(i) - 1) + (size_t)nx * (((size_t)(j) - 1) + (size_t)ny * ((size_t)(k) - 1))]
+#define C2(a, i, j) (a)[((size_t)(i) - 1) + (size_t)nx * ((size_t)(j) - 1)]
+#define U3(a, i, j, k) (a)[((size_t)(i) - 1) + (size_t)(nx + 1) * (((size_t)(j) - 1) + (size_t)ny * ((size_t)(k) - 1))]
+#define V3(a, i, j, k) (a)[((size_t)(i) - 1) + (size_t)nx * (((size_t)(j) - 1) + (size_t)(ny + 1) * ((size_t)(k) - 1))]
+
+void vpo_set_threads(int n)
+{
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+
+int vpo_get_threads(void)
+{
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+/* =====================================================================
+ * Position-independent math: restatement of rdb_sm_cbrt
+ * (src/shared_module_utilities/rdb_safe_math_pow.inc:107-142) and
+ * rdb_sm_atan (rdb_safe_math_atan.inc:7-44) with the coefficient tables of
+ * rdb_safe_math_consts.inc:65-100.  Only IEEE + - * / and exact exponent
+ * manipulation, so the value is the same on every IEEE machine built without
+ * FMA contraction.
+ * ===================================================================== */
+static const double SM_CBRT_C[5] = {
+    0.5189978361037301813, 0.6542973117201534849, -0.2158001895775201462,
+    0.04437845996234061896, -0.003660165019409192949};
+static const double SM_ATAN_C[12] = {
+    1.0, -0.3333333333333333148, 0.1999999999999998446,
+    -0.1428571428571007162, 0.1111111111054328693, -0.09090909045700855395,
+    0.07692305406260263601, -0.06666590357759735741, 0.05880646170199485545,
+    -0.05237747786578652448, 0.04518284953605152671, -0.0295457862073798469};
+static const double SM_PIO2_HI = 1.570796326794896558;
+static const double SM_PIO2_LO = 6.1232339957367660359e-17;
+static const double SM_SQRT3 = 1.7320508075688771932;
+static const double SM_PIO6_HI = 0.52359877559829892668;
+static const double SM_PIO6_LO = -5.3604088322554549242e-17;
+static const double SM_TAN_PIO12 = 0.2679491924311226958;
+
+static inline double sm_flush(double r)
+{
+    /* rdb_sm_flush (rdb_safe_math_core.inc:40-51) */
+    if (fabs(r) < DBL_MIN) return copysign(0.0, r);
+    return r;
+}
+
+double vpo_sm_cbrt(double x)
+{
+    if (isnan(x) || !isfinite(x)) return x;
+    double ax = fabs(x);
+    if (ax < DBL_MIN) return copysign(0.0, x);
+    int e;
+    double f = frexp(ax, &e);          /* Fortran fraction()/exponent() */
+    int rem = ((e % 3) + 3) % 3;       /* modulo(e, 3) */
+    int q = (e - rem) / 3;
+    double m = ldexp(f, rem);          /* in [1/2, 4) */
+    double y0 = SM_CBRT_C[4];
+    for (int i = 3; i >= 0; --i) y0 = y0 * m + SM_CBRT_C[i];
+    for (int it = 0; it < 2; ++it) {
+        double y3 = (y0 * y0) * y0;
+        y0 = y0 + y0 * ((m - y3) / ((y3 + y3) + m));
+    }
+    double y = ldexp(y0, q);
+    if (x < 0.0) y = -y;
+    return y;
+}
+
+double vpo_sm_atan(double x)
+{
+    if (isnan(x)) return x;
+    double ax = fabs(x);
+    int inv = ax > 1.0;
+    double t = inv ? 1.0 / ax : ax;
+    int mid = t > SM_TAN_PIO12;
+    double a = mid ? (SM_SQRT3 * t - 1.0) / (SM_SQRT3 + t) : t;
+    double u = a * a;
+    double p = SM_ATAN_C[11];
+    for (int i = 10; i >= 0; --i) p = p * u + SM_ATAN_C[i];
+    double y = a * p;
+    if (mid) y = SM_PIO6_HI + (y + SM_PIO6_LO);
+    if (inv) y = (SM_PIO2_HI - y) + SM_PIO2_LO;
+    return sm_flush(copysign(y, x));
+}
+
+/* =====================================================================
+ * Wright (1997) EOS at p_ref (src/equation_of_state/rdb_eos.F90:200-217,
+ * 909-959).
+ * ===================================================================== */
+#define WRIGHT_A0 7.057924e-4
+#define WRIGHT_A1 3.480336e-7
+#define WRIGHT_A2 -1.112733e-7
+#define WRIGHT_B0 5.790749e8
+#define WRIGHT_B1 3.516535e6
+#define WRIGHT_B2 -4.002714e4
+#define WRIGHT_B3 2.084372e2
+#define WRIGHT_B4 5.944068e5
+#define WRIGHT_B5 -9.643486e3
+#define WRIGHT_C0 1.704853e5
+#define WRIGHT_C1 7.904722e2
+#define WRIGHT_C2 -7.984422e0
+#define WRIGHT_C3 5.140652e-2
+#define WRIGHT_C4 -2.302158e2
+#define WRIGHT_C5 -3.079464e0
+
+void vpo_eos_wright(const vphys_config *c, vpo_state *s)
+{
+    const int nx = s->nx, ny = s->ny, nz = s->nz;
+    const double *S = s->tr[c->idx_salinity], *T = s->tr[c->idx_temperature];
+    const double p_ref = c->eos_p_ref, rho0 = c->rho0;
+#pragma omp parallel for
+    for (int k = 1; k <= nz; ++k)
+        for (int j = 1; j <= ny; ++j)
+            for (int i = 1; i <= nx; ++i) {
+                if (C3(s->h, i, j, k) > H_VANISHED) {
+                    double S_k = C3(S, i, j, k), T_k = C3(T, i, j, k);
+                    double T_sq = T_k * T_k;
+                    double T_cu = T_sq * T_k;
+                    double alpha_0 = WRIGHT_A0 + WRIGHT_A1 * T_k + WRIGHT_A2 * S_k;
+                    double p_0 = WRIGHT_B0 + WRIGHT_B1 * T_k + WRIGHT_B2 * T_sq + WRIGHT_B3 * T_cu +
+                                 WRIGHT_B4 * S_k + WRIGHT_B5 * S_k * T_k;
+                    double lambda = WRIGHT_C0 + WRIGHT_C1 * T_k + WRIGHT_C2 * T_sq + WRIGHT_C3 * T_cu +
+                                    WRIGHT_C4 * S_k + WRIGHT_C5 * S_k * T_k;
+                    double p_plus_p0 = p_ref + p_0;
+                    double denom = lambda + alpha_0 * p_plus_p0;
+                    C3(s->rho, i, j, k) = p_plus_p0 / denom;
+                } else {
+                    C3(s->rho, i, j, k) = rho0;
+                }
+            }
+}
+
+/* |tau| at cell centres (rdb_ocean_surface_stress.F90:858-875). */
+void vpo_stress_mag(vpo_state *s)
+{
+    const int nx = s->nx, ny = s->ny;
+    for (int j = 1; j <= ny; ++j)
+        for (int i = 1; i <= nx; ++i) {
+            double tx = 0.5 * (s->tau_x[(i - 1) + (nx + 1) * (j - 1)] + s->tau_x[i + (nx + 1) * (j - 1)]);
+            double ty = 0.5 * (s->tau_y[(i - 1) + nx * (j - 1)] + s->tau_y[(i - 1) + nx * j]);
+            C2(s->stress_mag, i, j) = sqrt(tx * tx + ty * ty);
+        }
+}
+
+/* =====================================================================
+ * PP81 (rdb_ocean_vmix.F90:1007-1074)
+ * ===================================================================== */
+void vpo_pp81(const vphys_config *c, vpo_state *s)
+{
+    const int nx = s->nx, ny = s->ny, nz = s->nz;
+    double *kv = s->kv, *kt = s->kt;
+    const double *u = s->u, *v = s->v, *h = s->h, *rho = s->rho;
+    for (int j = 1; j <= ny; ++j)
+        for (int i = 1; i <= nx; ++i) {
+            C3(kv, i, j, 1) = 0.0;
+            C3(kt, i, j, 1) = 0.0;
+            C3(kv, i, j, nz + 1) = 0.0;
+            C3(kt, i, j, nz + 1) = 0.0;
+        }
+#pragma omp parallel for
+    for (int k = 2; k <= nz; ++k)
+        for (int j = 1; j <= ny; ++j)
+            for (int i = 1; i <= nx; ++i) {
+                double u_km1 = 0.5 * (U3(u, i, j, k - 1) + U3(u, i + 1, j, k - 1));
+                double v_km1 = 0.5 * (V3(v, i, j, k - 1) + V3(v, i, j + 1, k - 1));
+                double u_k = 0.5 * (U3(u, i, j, k) + U3(u, i + 1, j, k));
+                double v_k = 0.5 * (V3(v, i, j, k) + V3(v, i, j + 1, k));
+                double dz_face = 0.5 * (C3(h, i, j, k - 1) + C3(h, i, j, k));
+                if (dz_face <= 0.0) {
+                    C3(kv, i, j, k) = c->pp81_nu_bg;
+                    C3(kt, i, j, k) = c->pp81_kappa_bg;
+                    continue;
+                }
+                double du_dz = (u_k - u_km1) / dz_face;
+                double dv_dz = (v_k - v_km1) / dz_face;
+                double shear2 = fmx(du_dz * du_dz + dv_dz * dv_dz, c->shear2_floor);
+                double n2 = -(GRAVITY * (C3(rho, i, j, k) - C3(rho, i, j, k - 1)) / (c->rho0 * dz_face));
+                double ri = n2 / shear2;
+                double denom = 1.0 + c->pp81_alpha * fmx(ri, 0.0);
+                double ri_factor = 1.0 / (denom * denom);
+                C3(kv, i, j, k) = c->pp81_nu_bg + c->pp81_nu0 * ri_factor;
+                C3(kt, i, j, k) = c->pp81_kappa_bg + c->pp81_nu0 * ri_factor / denom;
+            }
+}
+
+/* =====================================================================
+ * Bryan-Lewis background fill (rdb_ocean_vmix.F90:2387-2434)
+ * ===================================================================== */
+static void bkgnd_fill(const vphys_config *c, vpo_state *s)
+{
+    const int nx = s->nx, ny = s->ny, nz = s->nz;
+    const double inv_pi = 1.0 / PI_;
+    const double kd_sfc = c->bkgnd_kd_sfc, kd_deep = c->bkgnd_kd_deep;
+    const double z0 = c->bkgnd_z0, delta = c->bkgnd_delta;
+#pragma omp parallel for
+    for (int j = 1; j <= ny; ++j)
+        for (int i = 1; i <= nx; ++i) {
+            double depth = 0.0;
+            for (int k = nz; k >= 2; --k) {
+                depth = depth + C3(s->h, i, j, k);
+                C3(s->kd_bg, i, j, k) =
+                    kd_sfc + (kd_deep - kd_sfc) * (0.5 + vpo_sm_atan((depth - z0) / delta) * inv_pi);
+            }
+        }
+}
+
+/* interior_closure = "none" seed (rdb_ocean_vmix.F90:676-797; Henyey not
+ * supported here). */
+void vpo_seed_interior_none(const vphys_config *c, vpo_state *s)
+{
+    const int nx = s->nx, ny = s->ny, nz = s->nz;
+    if (c->bkgnd_profile) {
+        double pr_bl = 1.0;
+        if (c->bkgnd_prandtl > 0.0) pr_bl = c->bkgnd_prandtl;
+        bkgnd_fill(c, s);
+        for (int k = 1; k <= nz + 1; ++k)
+            for (int j = 1; j <= ny; ++j)
+                for (int i = 1; i <= nx; ++i) {
+                    if (k == 1 || k == nz + 1) {
+                        C3(s->kv, i, j, k) = 0.0;
+                        C3(s->kt, i, j, k) = 0.0;
+                    } else {
+                        C3(s->kv, i, j, k) = pr_bl * C3(s->kd_bg, i, j, k);
+                        C3(s->kt, i, j, k) = C3(s->kd_bg, i, j, k);
+                    }
+                }
+    } else {
+        double kv_seed = c->kv_bg, kt_seed = c->kt_bg;
+        if (c->bkgnd_prandtl > 0.0) kv_seed = c->bkgnd_prandtl * c->kt_bg + c->kv_bg;
+        for (int k = 1; k <= nz + 1; ++k)
+            for (int j = 1; j <= ny; ++j)
+                for (int i = 1; i <= nx; ++i) {
+                    if (k == 1 || k == nz + 1) {
+                        C3(s->kv, i, j, k) = 0.0;
+                        C3(s->kt, i, j, k) = 0.0;
+                    } else {
+                        C3(s->kv, i, j, k) = kv_seed;
+                        C3(s->kt, i, j, k) = kt_seed;
+                    }
+                }
+    }
+}
+
+/* rdb_vl_first_live (rdb_vanished_layer.inc:82-110) */
+static inline int first_live(const double *h, int nx, int ny, int i, int j, int kstart)
+{
+    int r = kstart;
+    for (int k = kstart; k >= 1; --k) {
+        if (C3(h, i, j, k) > H_VANISHED) {
+            r = k;
+            break;
+        }
+    }
+    return r;
+}
+
+/* kpp_surface_buoyancy_flux (rdb_ocean_vmix.F90:1518-1559) */
+static inline double kpp_b0(double alpha_T, double beta_S, double rho0, double qT, double qS)
+{
+    return (GRAVITY / rho0) * (alpha_T * qT - beta_S * qS);
+}
+
+/* =====================================================================
+ * KPP overlay (rdb_ocean_vmix.F90:1121-1516), constant buoyancy
+ * coefficients, no penetrating shortwave (sw_active = .false.).
+ * ===================================================================== */
+void vpo_kpp_overlay(const vphys_config *c, vpo_state *s)
+{
+    const int nx = s->nx, ny = s->ny, nz = s->nz;
+    const double rho0 = c->rho0;
+    const double *h = s->h, *u = s->u, *v = s->v, *rho = s->rho;
+    for (size_t n = 0; n < (size_t)nx * ny * (nz + 1); ++n) {
+        s->gamma_t[n] = 0.0;
+        s->gamma_s[n] = 0.0;
+    }
+    /* ---- pass 1: BL depth ---- */
+#pragma omp parallel for
+    for (int j = 1; j <= ny; ++j)
+        for (int i = 1; i <= nx; ++i) {
+            int k_sfc = first_live(h, nx, ny, i, j, nz);
+            double u_ref = 0.5 * (U3(u, i, j, k_sfc) + U3(u, i + 1, j, k_sfc));
+            double v_ref = 0.5 * (V3(v, i, j, k_sfc) + V3(v, i, j + 1, k_sfc));
+            double b_ref = -(GRAVITY * C3(rho, i, j, k_sfc) / rho0);
+            double d_centre_ref = 0.5 * C3(h, i, j, k_sfc);
+            double tau_mag = C2(s->stress_mag, i, j);
+            double u_star = sqrt(tau_mag / rho0);
+            double h_b_lagged = C2(s->bl_depth, i, j);
+            double q_T_kin = C2(s->q_heat, i, j) / (rho0 * c->cp);
+            double q_S_kin = C2(s->q_salt, i, j) / rho0;
+            double B_0 = kpp_b0(c->alpha_T, c->beta_S, rho0, q_T_kin, q_S_kin);
+            double wstar3_lagged = fmx(0.0, -B_0) * h_b_lagged;
+            double cb = vpo_sm_cbrt(wstar3_lagged);
+            double w_s_col = sqrt(u_star * u_star + cb * cb);
+            double ri_prev = 0.0, d_prev = d_centre_ref, h_b = 0.0;
+            int crossing_found = 0;
+            double d_centre_k = d_centre_ref;
+            for (int k = k_sfc - 1; k >= 1; --k) {
+                if (!crossing_found) {
+                    d_centre_k = d_centre_k + 0.5 * (C3(h, i, j, k + 1) + C3(h, i, j, k));
+                    double u_k = 0.5 * (U3(u, i, j, k) + U3(u, i + 1, j, k));
+                    double v_k = 0.5 * (V3(v, i, j, k) + V3(v, i, j + 1, k));
+                    double b_k = -(GRAVITY * C3(rho, i, j, k) / rho0);
+                    double delta_d = d_centre_k - d_centre_ref;
+                    double delta_b = b_ref - b_k;
+                    double n_brunt = sqrt(fmx(0.0, delta_b / delta_d));
+                    double vt2 = (c->c_vt2 / c->ri_crit) * d_centre_k * n_brunt * w_s_col;
+                    double shear2 = fmx((u_k - u_ref) * (u_k - u_ref) + (v_k - v_ref) * (v_k - v_ref) + vt2,
+                                        c->shear2_floor);
+                    double ri_bulk = delta_b * delta_d / shear2;
+                    if (ri_bulk >= c->ri_crit) {
+                        double denom = ri_bulk - ri_prev;
+                        double frac;
+                        if (fabs(denom) > 1.0e-12)
+                            frac = (c->ri_crit - ri_prev) / denom;
+                        else
+                            frac = 0.5;
+                        h_b = d_prev + frac * (d_centre_k - d_prev);
+                        crossing_found = 1;
+                    }
+                    ri_prev = ri_bulk;
+                    d_prev = d_centre_k;
+                }
+            }
+            if (!crossing_found) {
+                h_b = 0.0;
+                for (int k = 1; k <= k_sfc; ++k) h_b = h_b + C3(h, i, j, k);
+            }
+            C2(s->bl_depth, i, j) = h_b;
+        }
+    /* ---- pass 2: overlay ---- */
+#pragma omp parallel for
+    for (int j = 1; j <= ny; ++j)
+        for (int i = 1; i <= nx; ++i) {
+            int k_sfc = first_live(h, nx, ny, i, j, nz);
+            double tau_mag = C2(s->stress_mag, i, j);
+            double u_star = sqrt(tau_mag / rho0);
+            double h_b = C2(s->bl_depth, i, j);
+            double q_T_kin = C2(s->q_heat, i, j) / (rho0 * c->cp);
+            double q_S_kin = C2(s->q_salt, i, j) / rho0;
+            double B_0 = kpp_b0(c->alpha_T, c->beta_S, rho0, q_T_kin, q_S_kin);
+            C2(s->b0, i, j) = B_0;
+            int destabilizing = B_0 < 0.0;
+            double wstar3 = fmx(0.0, -B_0) * h_b;
+            double w_star = vpo_sm_cbrt(wstar3);
+            double w_s = sqrt(u_star * u_star + w_star * w_star);
+            if (h_b > 0.0 && w_s > 0.0) {
+                double d_running = 0.0;
+                for (int k = k_sfc; k >= 1; --k) {
+                    d_running = d_running + C3(h, i, j, k);
+                    double d_face_k = d_running;
+                    if (k > 1 && d_face_k < h_b) {
+                        double sigma = d_face_k / h_b;
+                        double g_shape = sigma * (1.0 - sigma) * (1.0 - sigma);
+                        double kv_kpp = h_b * w_s * g_shape;
+                        C3(s->kv, i, j, k) = fmx(C3(s->kv, i, j, k), kv_kpp);
+                        C3(s->kt, i, j, k) = fmx(C3(s->kt, i, j, k), kv_kpp);
+                        if (destabilizing) {
+                            double gamma_factor = c->cs_nonlocal * g_shape;
+                            C3(s->gamma_t, i, j, k) = gamma_factor * q_T_kin;
+                            C3(s->gamma_s, i, j, k) = gamma_factor * q_S_kin;
+                        }
+                    }
+                }
+            }
+        }
+}
+
+/* KV_ML_INVZ2 surface band (rdb_ocean_vmix.F90:1716-1766) */
+void vpo_kv_ml_invz2(const vphys_config *c, vpo_state *s)
+{
+    const int nx = s->nx, ny = s->ny, nz = s->nz;
+    if (c->kv_ml_invz2 <= 0.0) return;
+    if (c->hmix_fixed <= 0.0) return;
+    double hmix = c->hmix_fixed;
+    double hmix_sq = hmix * hmix;
+    double dz_min_safe = 0.5 * hmix / (double)(nz > 1 ? nz : 1);
+#pragma omp parallel for
+    for (int j = 1; j <= ny; ++j)
+        for (int i = 1; i <= nx; ++i) {
+            double z = 0.0;
+            for (int k = nz; k >= 2; --k) {
+                z = z + C3(s->h, i, j, k);
+                if (z >= hmix) break;
+                double zz = fmx(z, dz_min_safe);
+                double kv_extra = c->kv_ml_invz2 * hmix_sq / (zz * zz);
+                C3(s->kv, i, j, k) = C3(s->kv, i, j, k) + kv_extra;
+            }
+        }
+}
+
+/* Convective adjustment (rdb_ocean_vmix.F90:1768-1849), masked below the
+ * KPP bl_depth. */
+void vpo_convection(const vphys_config *c, vpo_state *s)
+{
+    const int nx = s->nx, ny = s->ny, nz = s->nz;
+    if (!c->conv_enable) return;
+#pragma omp parallel for
+    for (int j = 1; j <= ny; ++j)
+        for (int i = 1; i <= nx; ++i) {
+            double z = 0.0;
+            for (int k = nz; k >= 2; --k) {
+                z = z + C3(s->h, i, j, k);
+                double dz_face = 0.5 * (C3(s->h, i, j, k - 1) + C3(s->h, i, j, k));
+                if (dz_face <= H_VANISHED) continue;
+                if (z < C2(s->bl_depth, i, j)) continue;
+                double n2 = -(GRAVITY * (C3(s->rho, i, j, k) - C3(s->rho, i, j, k - 1)) / (c->rho0 * dz_face));
+                if (n2 < c->conv_n2_thresh) {
+                    C3(s->kt, i, j, k) = fmx(C3(s->kt, i, j, k), c->conv_kd);
+                    C3(s->kv, i, j, k) = fmx(C3(s->kv, i, j, k), c->conv_prandtl * c->conv_kd);
+                }
+            }
+        }
+}
+
+/* ks := kt (rdb_ocean_vmix.F90:1921-1934) */
+void vpo_split(const vphys_config *c, vpo_state *s)
+{
+    (void)c;
+    size_t n = (size_t)s->nx * s->ny * (s->nz + 1);
+    memcpy(s->ks, s->kt, n * sizeof(double));
+}
+
+static void smooth_121(vpo_state *s, double *fld, double *scratch)
+{
+    /* vmix_smooth_121_impl (rdb_ocean_vmix.F90:2699-2748) */
+    const int nx = s->nx, ny = s->ny, nz = s->nz;
+    const double *wet = s->wet;
+    size_t n = (size_t)nx * ny * (nz + 1);
+    memcpy(scratch, fld, n * sizeof(double));
+    for (int k = 2; k <= nz; ++k)
+        for (int j = 2; j <= ny - 1; ++j)
+            for (int i = 2; i <= nx - 1; ++i) {
+                double w_c = 4.0 * C2(wet, i, j);
+                double w_e = 2.0 * C2(wet, i + 1, j);
+                double w_w = 2.0 * C2(wet, i - 1, j);
+                double w_n = 2.0 * C2(wet, i, j + 1);
+                double w_s = 2.0 * C2(wet, i, j - 1);
+                double w_ne = C2(wet, i + 1, j + 1);
+                double w_nw = C2(wet, i - 1, j + 1);
+                double w_se = C2(wet, i + 1, j - 1);
+                double w_sw = C2(wet, i - 1, j - 1);
+                double wsum = w_c + w_e + w_w + w_n + w_s + w_ne + w_nw + w_se + w_sw;
+                if (wsum <= 0.0 || C2(wet, i, j) == 0.0) {
+                    C3(fld, i, j, k) = C3(scratch, i, j, k);
+                } else {
+                    C3(fld, i, j, k) =
+                        (w_c * C3(scratch, i, j, k) + w_e * C3(scratch, i + 1, j, k) +
+                         w_w * C3(scratch, i - 1, j, k) + w_n * C3(scratch, i, j + 1, k) +
+                         w_s * C3(scratch, i, j - 1, k) + w_ne * C3(scratch, i + 1, j + 1, k) +
+                         w_nw * C3(scratch, i - 1, j + 1, k) + w_se * C3(scratch, i + 1, j - 1, k) +
+                         w_sw * C3(scratch, i - 1, j - 1, k)) /
+                        wsum;
+                }
+            }
+}
+
+/* vmix_assemble (rdb_ocean_vmix.F90:2183-2366): guard, floors, ceilings,
+ * smoothing.  Returns 1 when the guard tripped, else 0. */
+int vpo_assemble_gate(const vphys_config *c, vpo_state *s)
+{
+    const int nx = s->nx, ny = s->ny, nz = s->nz;
+    int status = 0;
+    if (c->vmix_guard) {
+        long bad = 0;
+        for (int k = 2; k <= nz; ++k)
+            for (int j = 1; j <= ny; ++j)
+                for (int i = 1; i <= nx; ++i) {
+                    double a = C3(s->kv, i, j, k), b = C3(s->kt, i, j, k), d = C3(s->ks, i, j, k);
+                    if (a < 0.0 || a != a) bad++;
+                    if (b < 0.0 || b != b) bad++;
+                    if (d < 0.0 || d != d) bad++;
+                }
+        if (bad > 0) status = 1;
+    }
+    if (c->bkgnd_profile) {
+        double pr_bl = 1.0;
+        if (c->bkgnd_prandtl > 0.0) pr_bl = c->bkgnd_prandtl;
+        bkgnd_fill(c, s);
+#pragma omp parallel for
+        for (int k = 2; k <= nz; ++k)
+            for (int j = 1; j <= ny; ++j)
+                for (int i = 1; i <= nx; ++i) {
+                    double kdb = C3(s->kd_bg, i, j, k);
+                    C3(s->kv, i, j, k) = fmn(fmx(C3(s->kv, i, j, k), pr_bl * kdb), c->kv_max);
+                    C3(s->kt, i, j, k) = fmn(fmx(C3(s->kt, i, j, k), kdb), c->kd_max);
+                    C3(s->ks, i, j, k) = fmn(fmx(C3(s->ks, i, j, k), kdb), c->kd_max);
+                }
+    } else {
+        double kv_floor = c->kv_bg;
+        if (c->bkgnd_prandtl > 0.0) kv_floor = c->bkgnd_prandtl * c->kt_bg + c->kv_bg;
+#pragma omp parallel for
+        for (int k = 2; k <= nz; ++k)
+            for (int j = 1; j <= ny; ++j)
+                for (int i = 1; i <= nx; ++i) {
+                    C3(s->kv, i, j, k) = fmn(fmx(C3(s->kv, i, j, k), kv_floor), c->kv_max);
+                    C3(s->kt, i, j, k) = fmn(fmx(C3(s->kt, i, j, k), c->kt_bg), c->kd_max);
+                    C3(s->ks, i, j, k) = fmn(fmx(C3(s->ks, i, j, k), c->ks_bg), c->kd_max);
+                }
+    }
+    if (c->kd_smooth_iterations > 0) {
+        size_t n = (size_t)nx * ny * (nz + 1);
+        double *scratch = (double *)malloc(n * sizeof(double));
+        for (int it = 0; it < c->kd_smooth_iterations; ++it) {
+            smooth_121(s, s->kv, scratch);
+            smooth_121(s, s->kt, scratch);
+            smooth_121(s, s->ks, scratch);
+        }
+        free(scratch);
+    }
+    return status;
+}
+
+/* vmix_build_coefficients (rdb_ocean_dyn.F90:1473-1634), default
+ * contributors only (no EPBL / kappa-shear / tidal / BBL mixing). */
+int vpo_build_coefficients(const vphys_config *c, vpo_state *s)
+{
+    if (c->interior_closure == VPHYS_INTERIOR_PP81)
+        vpo_pp81(c, s);
+    else
+        vpo_seed_interior_none(c, s);
+    if (c->use_kpp) vpo_kpp_overlay(c, s);
+    vpo_kv_ml_invz2(c, s);
+    if (c->conv_enable) vpo_convection(c, s);
+    vpo_split(c, s);
+    return vpo_assemble_gate(c, s);
+}
+
+/* =====================================================================
+ * Tracer vertical diffusion (rdb_ocean_vdiff.F90:1107-1414, 1928-1962)
+ * ===================================================================== */
+static inline double face_thick(double ha, double hb, int use_harmonic)
+{
+    if (use_harmonic) {
+        double sum_h = ha + hb;
+        if (sum_h > 1.0e-30) return 2.0 * ha * hb / sum_h;
+        return 0.5 * sum_h;
+    }
+    return 0.5 * (ha + hb);
+}
+
+/* build_factorize_tracer_matrix for one column; col arrays are 1-based. */
+static void factor_column(int nz, int use_harmonic, double dt, const double *kvc /* nz+1 */,
+                          const double *hcol /* nz */, double *a, double *b, double *cc)
+{
+    double hc = fmx(hcol[0], H_VANISHED);
+    double alpha = 0.0;
+    if (nz > 1) {
+        double hp = fmx(hcol[1], H_VANISHED);
+        double dz_face = face_thick(hc, hp, use_harmonic);
+        alpha = dt * kvc[1] / (hc * dz_face);
+        if (hcol[0] <= H_VANISHED || hcol[1] <= H_VANISHED) alpha = 0.0;
+    }
+    a[0] = 0.0;
+    cc[0] = -alpha;
+    b[0] = 1.0 + alpha;
+    for (int k = 2; k <= nz - 1; ++k) {
+        double hm = fmx(hcol[k - 2], H_VANISHED);
+        hc = fmx(hcol[k - 1], H_VANISHED);
+        double hp = fmx(hcol[k], H_VANISHED);
+        double beta = dt * kvc[k - 1] / (hc * face_thick(hm, hc, use_harmonic));
+        alpha = dt * kvc[k] / (hc * face_thick(hc, hp, use_harmonic));
+        if (hcol[k - 1] <= H_VANISHED || hcol[k - 2] <= H_VANISHED) beta = 0.0;
+        if (hcol[k - 1] <= H_VANISHED || hcol[k] <= H_VANISHED) alpha = 0.0;
+        a[k - 1] = -beta;
+        cc[k - 1] = -alpha;
+        b[k - 1] = 1.0 + alpha + beta;
+    }
+    if (nz > 1) {
+        double hm = fmx(hcol[nz - 2], H_VANISHED);
+        hc = fmx(hcol[nz - 1], H_VANISHED);
+        double dz_face = face_thick(hm, hc, use_harmonic);
+        double beta = dt * kvc[nz - 1] / (hc * dz_face);
+        if (hcol[nz - 1] <= H_VANISHED || hcol[nz - 2] <= H_VANISHED) beta = 0.0;
+        a[nz - 1] = -beta;
+        cc[nz - 1] = 0.0;
+        b[nz - 1] = 1.0 + beta;
+    }
+    cc[0] = cc[0] / b[0];
+    for (int k = 2; k <= nz; ++k) {
+        double denom = b[k - 1] - a[k - 1] * cc[k - 2];
+        cc[k - 1] = cc[k - 1] / denom;
+        b[k - 1] = denom;
+    }
+}
+
+/* apply_factored_tracer for one column (in place on ccol). */
+static void apply_column(int nz, const double *hcol, double *ccol, const double *a, const double *b,
+                         const double *cc, double *rhs, double *budget_col /* may be NULL */)
+{
+    for (int k = 0; k < nz; ++k) rhs[k] = ccol[k];
+    rhs[0] = rhs[0] / b[0];
+    for (int k = 2; k <= nz; ++k) rhs[k - 1] = (rhs[k - 1] - a[k - 1] * rhs[k - 2]) / b[k - 1];
+    for (int k = nz - 1; k >= 1; --k) rhs[k - 1] = rhs[k - 1] - cc[k - 1] * rhs[k];
+    if (budget_col) {
+        for (int k = 0; k < nz; ++k) {
+            double p_new = hcol[k] * rhs[k];
+            double p_old = hcol[k] * ccol[k];
+            budget_col[k] = budget_col[k] + (p_new - p_old);
+            ccol[k] = rhs[k];
+        }
+    } else {
+        for (int k = 0; k < nz; ++k) ccol[k] = rhs[k];
+    }
+}
+
+static void tracer_pass(const vphys_config *c, vpo_state *s, double dt, const double *ksrc, int temperature_pass)
+{
+    const int nx = s->nx, ny = s->ny, nz = s->nz;
+#pragma omp parallel
+    {
+        double kvc[VPHYS_NZ_MAX + 1], hcol[VPHYS_NZ_MAX], a[VPHYS_NZ_MAX], b[VPHYS_NZ_MAX], cc[VPHYS_NZ_MAX];
+        double rhs[VPHYS_NZ_MAX], ccol[VPHYS_NZ_MAX], bud[VPHYS_NZ_MAX];
+#pragma omp for
+        for (int j = 1; j <= ny; ++j)
+            for (int i = 1; i <= nx; ++i) {
+                for (int k = 1; k <= nz + 1; ++k) kvc[k - 1] = C3(ksrc, i, j, k);
+                for (int k = 1; k <= nz; ++k) hcol[k - 1] = C3(s->h, i, j, k);
+                factor_column(nz, c->use_harmonic, dt, kvc, hcol, a, b, cc);
+                for (int t = 0; t < s->ntr; ++t) {
+                    int is_T = (t == c->idx_temperature);
+                    if (temperature_pass != is_T) continue;
+                    double *trc = s->tr[t];
+                    double *budget = NULL;
+                    if (c->budgets) {
+                        if (is_T) budget = s->heat_budget;
+                        else if (t == c->idx_salinity) budget = s->salt_budget;
+                    }
+                    for (int k = 1; k <= nz; ++k) ccol[k - 1] = C3(trc, i, j, k);
+                    if (budget)
+                        for (int k = 1; k <= nz; ++k) bud[k - 1] = C3(budget, i, j, k);
+                    apply_column(nz, hcol, ccol, a, b, cc, rhs, budget ? bud : NULL);
+                    for (int k = 1; k <= nz; ++k) C3(trc, i, j, k) = ccol[k - 1];
+                    if (budget)
+                        for (int k = 1; k <= nz; ++k) C3(budget, i, j, k) = bud[k - 1];
+                }
+            }
+    }
+}
+
+/* vdiff_apply_tracers with kt_source and ks_source (case 3). */
+void vpo_vdiff_tracers(const vphys_config *c, vpo_state *s, double dt)
+{
+    tracer_pass(c, s, dt, s->kt, 1);
+    tracer_pass(c, s, dt, s->ks, 0);
+}
+
+/* =====================================================================
+ * KPP non-local tendencies (rdb_ocean_vmix.F90:1605-1714,
+ * rdb_tracer_conc.inc:36-53)
+ * ===================================================================== */
+static inline double nonlocal_face_flux(double gamma, double h_below, double h_above)
+{
+    if (h_below > H_VANISHED && h_above > H_VANISHED) return gamma;
+    return 0.0;
+}
+
+static inline double conc_add_source(double cval, double h, double src)
+{
+    if (h > H_VANISHED) return cval + src / (h + H_DIV_EPS);
+    return cval;
+}
+
+static void nonlocal_one(vpo_state *s, double dt, const double *gam, double *trc)
+{
+    const int nx = s->nx, ny = s->ny, nz = s->nz;
+#pragma omp parallel for
+    for (int k = 1; k <= nz; ++k)
+        for (int j = 1; j <= ny; ++j)
+            for (int i = 1; i <= nx; ++i) {
+                double f_up = 0.0, f_dn = 0.0;
+                if (k < nz) f_up = nonlocal_face_flux(C3(gam, i, j, k + 1), C3(s->h, i, j, k), C3(s->h, i, j, k + 1));
+                if (k > 1) f_dn = nonlocal_face_flux(C3(gam, i, j, k), C3(s->h, i, j, k - 1), C3(s->h, i, j, k));
+                C3(trc, i, j, k) = conc_add_source(C3(trc, i, j, k), C3(s->h, i, j, k), dt * (f_up - f_dn));
+            }
+}
+
+void vpo_nonlocal(const vphys_config *c, vpo_state *s, double dt)
+{
+    if (c->idx_temperature >= 0) nonlocal_one(s, dt, s->gamma_t, s->tr[c->idx_temperature]);
+    if (c->idx_salinity >= 0) nonlocal_one(s, dt, s->gamma_s, s->tr[c->idx_salinity]);
+    if (c->idx_pseudo_salt >= 0) nonlocal_one(s, dt, s->gamma_s, s->tr[c->idx_pseudo_salt]);
+}
+
+/* =====================================================================
+ * Momentum vertical viscosity (rdb_ocean_vdiff.F90:1416-1926, 1964-2115,
+ * rdb_bed_live_face.inc), without the ice-shelf top drag and the corner
+ * viscosity add-on.  `xf` selects u faces (nu = nx+1, nv = ny) or v faces.
+ * ===================================================================== */
+#define EPS_HVEL 1.0e-30
+#define STRESS_H_MIN 1.0e-3
+
+static inline void face_layer(double hl_c, double hr_c, double u_k, int k, int kb, int hvel_mom6,
+                              int hvel_harmonic, int hvel_upwind, int zlevel_faces, double d_min,
+                              double i_hbbl, double *zacc, double *zcol_l, double *zcol_r, double *hvel,
+                              double *zint)
+{
+    double h_harm, h_arith, h_delta, z_clear, z2, botfn;
+    *zint = 0.0;
+    if (hvel_mom6 && !hvel_harmonic) {
+        h_harm = 2.0 * hl_c * hr_c / (hl_c + hr_c + EPS_HVEL);
+        h_arith = 0.5 * (hl_c + hr_c);
+        h_delta = hr_c - hl_c;
+        *zcol_l = *zcol_l + hl_c;
+        *zcol_r = *zcol_r + hr_c;
+        if (k >= kb) *zacc = *zacc + h_harm;
+        z_clear = fmx(*zcol_l, *zcol_r) + d_min;
+        *zint = fmx(*zacc, z_clear) * i_hbbl;
+        *hvel = h_arith;
+        if (u_k * h_delta > 0.0) {
+            z2 = *zint;
+            botfn = 1.0 / (1.0 + 0.09 * z2 * z2 * z2 * z2 * z2 * z2);
+            *hvel = (1.0 - botfn) * h_arith + botfn * h_harm;
+        }
+    } else if (hvel_mom6) {
+        h_harm = 2.0 * hl_c * hr_c / (hl_c + hr_c + EPS_HVEL);
+        h_arith = 0.5 * (hl_c + hr_c);
+        h_delta = hr_c - hl_c;
+        *hvel = h_harm;
+        if (hvel_upwind && u_k * h_delta < 0.0) {
+            z2 = *zacc;
+            botfn = 1.0 / (1.0 + 0.09 * z2 * z2 * z2 * z2 * z2 * z2);
+            *hvel = (1.0 - botfn) * h_harm + botfn * h_arith;
+        }
+        if (k >= kb) *zacc = *zacc + h_harm * i_hbbl;
+        *zint = *zacc;
+    } else {
+        *hvel = 0.5 * (hl_c + hr_c);
+    }
+    if (zlevel_faces) *hvel = fmn(hl_c, hr_c);
+}
+
+static inline void interface_coupling(double hv_lo, double hv_hi, double zint_lo, double dt, int hvel_mom6,
+                                      int use_harmonic, int bbl_glue, double kv_bbl, double kv_bbl_bg,
+                                      double bbl_thick, int zlevel_faces, double kv_l, double kv_r, double *num,
+                                      double *dz, int *cut)
+{
+    double hf_lo = fmx(hv_lo, H_VANISHED);
+    double hf_hi = fmx(hv_hi, H_VANISHED);
+    if (hvel_mom6)
+        *dz = 0.5 * (hf_lo + hf_hi);
+    else
+        *dz = face_thick(hf_lo, hf_hi, use_harmonic);
+    double nu_f = 0.5 * (kv_l + kv_r);
+    if (bbl_glue) {
+        double z = zint_lo;
+        double botfn_int = 1.0 / (1.0 + 0.09 * z * z * z * z * z * z);
+        nu_f = fmx(0.0, nu_f + (kv_bbl - kv_bbl_bg) * botfn_int);
+        if (*dz > bbl_thick) *dz = (1.0 - botfn_int) * (*dz) + botfn_int * bbl_thick;
+    }
+    *num = dt * nu_f;
+    *cut = zlevel_faces && (hv_lo <= H_VANISHED || hv_hi <= H_VANISHED);
+}
+
+static void diffuse_faces(const vphys_config *c, vpo_state *s, double dt, int xf)
+{
+    const int nx = s->nx, ny = s->ny, nz = s->nz;
+    const int nu = xf ? nx + 1 : nx;
+    const int nv = xf ? ny : ny + 1;
+    double *uf = xf ? s->u : s->v;
+    const double *tau = xf ? s->tau_x : s->tau_y;
+    const double *lam = xf ? s->lambda_bot_u : s->lambda_bot_v;
+    double *vrem = xf ? s->visc_rem_u : s->visc_rem_v;
+    const int *ktopf = xf ? s->k_top_u : s->k_top_v;
+    const int *kbotf = xf ? s->k_bot_u : s->k_bot_v;
+    const double *h = s->h, *kvc = s->kv, *wet = s->wet;
+    const int do_stress = c->implicit_stress, do_drag = c->implicit_drag, do_remnant = c->remnant;
+    const double inv_rho0 = 1.0 / c->rho0;
+#define F3(a, i, j, k) (a)[((size_t)(i) - 1) + (size_t)nu * (((size_t)(j) - 1) + (size_t)nv * ((size_t)(k) - 1))]
+#define F2(a, i, j) (a)[((size_t)(i) - 1) + (size_t)nu * ((size_t)(j) - 1)]
+#pragma omp parallel
+    {
+        double cdiag[VPHYS_NZ_MAX], rhs[VPHYS_NZ_MAX];
+#pragma omp for
+        for (int j = 1; j <= nv; ++j)
+            for (int i = 1; i <= nu; ++i) {
+                int i_left, i_right, j_below, j_above;
+                if (xf) {
+                    i_left = i - 1 > 1 ? i - 1 : 1;
+                    i_right = i < nx ? i : nx;
+                    j_below = j;
+                    j_above = j;
+                } else {
+                    i_left = i;
+                    i_right = i;
+                    j_below = j - 1 > 1 ? j - 1 : 1;
+                    j_above = j < ny ? j : ny;
+                }
+                int kb = F2(kbotf, i, j);
+                int ktop = F2(ktopf, i, j);
+                double kv_bbl = 0.0, bbl_thick = c->hbbl_visc;
+                if (c->bbl_glue) {
+                    kv_bbl = c->bbl_piston * c->hbbl_visc;
+                    bbl_thick = c->hbbl_visc;
+                }
+                double i_hbbl = 1.0 / (bbl_thick + EPS_HVEL);
+                double zacc = 0.0, zcol_l = 0.0, zcol_r = 0.0;
+                if (c->hvel_mom6 && !c->hvel_harmonic) {
+                    for (int k = 1; k <= nz; ++k) {
+                        zcol_l = zcol_l - C3(h, i_left, j_below, k);
+                        zcol_r = zcol_r - C3(h, i_right, j_above, k);
+                    }
+                }
+                double d_min = fmn(-zcol_l, -zcol_r);
+                int kb_live = kb;
+                for (int k = kb; k <= nz; ++k) {
+                    int live = c->zlevel_faces ? (fmn(C3(h, i_left, j_below, k), C3(h, i_right, j_above, k)) > H_VANISHED)
+                                               : 1;
+                    if (live) {
+                        kb_live = k;
+                        break;
+                    }
+                }
+                double hv_0, hv_p, zi_0, zi_p;
+                face_layer(C3(h, i_left, j_below, 1), C3(h, i_right, j_above, 1), F3(uf, i, j, 1), 1, kb,
+                           c->hvel_mom6, c->hvel_harmonic, c->hvel_upwind, c->zlevel_faces, d_min, i_hbbl, &zacc,
+                           &zcol_l, &zcol_r, &hv_p, &zi_p);
+                hv_0 = 0.0;
+                zi_0 = 0.0;
+                double num_t = 0.0, dz_t = 1.0;
+                int cut_t = 0;
+                double cp_prev = 0.0, dp_prev = 0.0, gp_prev = 0.0;
+                double cp = 0.0, dp = 0.0, gp = 0.0;
+                for (int k = 1; k <= nz; ++k) {
+                    hv_0 = hv_p;
+                    zi_0 = zi_p;
+                    double num_b = num_t, dz_b = dz_t;
+                    int cut_b = cut_t;
+                    if (k < nz) {
+                        face_layer(C3(h, i_left, j_below, k + 1), C3(h, i_right, j_above, k + 1), F3(uf, i, j, k + 1),
+                                   k + 1, kb, c->hvel_mom6, c->hvel_harmonic, c->hvel_upwind, c->zlevel_faces, d_min,
+                                   i_hbbl, &zacc, &zcol_l, &zcol_r, &hv_p, &zi_p);
+                        if (k >= kb_live && k <= ktop) {
+                            interface_coupling(hv_0, hv_p, zi_0, dt, c->hvel_mom6, c->use_harmonic, c->bbl_glue,
+                                               kv_bbl, c->kv_bbl_bg, bbl_thick, c->zlevel_faces,
+                                               C3(kvc, i_left, j_below, k + 1), C3(kvc, i_right, j_above, k + 1),
+                                               &num_t, &dz_t, &cut_t);
+                        }
+                    }
+                    double a_k = 0.0, b_k = 1.0, c_k = 0.0;
+                    double hf_k = fmx(hv_0, H_VANISHED);
+                    if (k == kb_live && k <= ktop) {
+                        double alpha = 0.0;
+                        if (kb_live < nz) {
+                            alpha = num_t / (hf_k * dz_t);
+                            if (cut_t) alpha = 0.0;
+                        }
+                        c_k = -alpha;
+                        b_k = 1.0 + alpha;
+                        if (c->bbl_glue) b_k = b_k + dt * kv_bbl / (hf_k * (fmn(0.5 * hv_0, bbl_thick) + EPS_HVEL));
+                        if (do_drag && !c->bbl_glue) b_k = b_k + dt * F2(lam, i, j);
+                    }
+                    if (k == ktop && k > kb_live) {
+                        double beta = num_b / (hf_k * dz_b);
+                        if (cut_b) beta = 0.0;
+                        a_k = -beta;
+                        b_k = 1.0 + beta;
+                    }
+                    if (k > kb_live && k < ktop) {
+                        double beta = num_b / (hf_k * dz_b);
+                        double alpha = num_t / (hf_k * dz_t);
+                        if (cut_b) beta = 0.0;
+                        if (cut_t) alpha = 0.0;
+                        a_k = -beta;
+                        c_k = -alpha;
+                        b_k = 1.0 + alpha + beta;
+                    }
+                    double r_k = F3(uf, i, j, k);
+                    if (k == ktop) {
+                        if (do_stress) {
+                            double wind_open = 1.0;
+                            r_k = r_k + dt * F2(tau, i, j) * wind_open *
+                                            fmn(C2(wet, i_left, j_below), C2(wet, i_right, j_above)) * inv_rho0 /
+                                            fmx(hf_k, STRESS_H_MIN);
+                        }
+                    }
+                    if (k == 1) {
+                        cp = c_k / b_k;
+                        dp = r_k / b_k;
+                        gp = 1.0 / b_k;
+                    } else {
+                        double denom = b_k - a_k * cp_prev;
+                        cp = c_k / denom;
+                        dp = (r_k - a_k * dp_prev) / denom;
+                        gp = (1.0 - a_k * gp_prev) / denom;
+                    }
+                    cdiag[k - 1] = cp;
+                    rhs[k - 1] = dp;
+                    if (do_remnant) F3(vrem, i, j, k) = gp;
+                    cp_prev = cp;
+                    dp_prev = dp;
+                    gp_prev = gp;
+                }
+                double u_next = dp_prev;
+                double g_next = fmn(gp_prev, 1.0);
+                F3(uf, i, j, nz) = u_next;
+                if (do_remnant) F3(vrem, i, j, nz) = g_next;
+                for (int k = nz - 1; k >= 1; --k) {
+                    double cpk = cdiag[k - 1];
+                    u_next = rhs[k - 1] - cpk * u_next;
+                    F3(uf, i, j, k) = u_next;
+                    if (do_remnant) {
+                        g_next = fmn(F3(vrem, i, j, k) - cpk * g_next, 1.0);
+                        F3(vrem, i, j, k) = g_next;
+                    }
+                }
+            }
+    }
+#undef F3
+#undef F2
+}
+
+void vpo_vdiff_momentum(const vphys_config *c, vpo_state *s, double dt)
+{
+    diffuse_faces(c, s, dt, 1);
+    diffuse_faces(c, s, dt, 0);
+}
+
+/* One vmix_apply_in_stage on a thermo step (rdb_ocean_dyn.F90:1636-1900). */
+int vpo_step(const vphys_config *c, vpo_state *s, double dt, int n_steps)
+{
+    int st = 0;
+    for (int n = 0; n < n_steps; ++n) {
+        if (c->eos_in_step) vpo_eos_wright(c, s);
+        st |= vpo_build_coefficients(c, s);
+        vpo_vdiff_momentum(c, s, dt);
+        vpo_vdiff_tracers(c, s, dt);
+        if (c->use_kpp) vpo_nonlocal(c, s, dt);
+    }
+    return st;
+}

@@ -1,0 +1,70 @@
+/* vphys_oracle.h -- CPU FP64 restatement of Roundabout's vertical-physics
+ * hot path.  TEST INFRASTRUCTURE ONLY: the checker for the CUDA library
+ * (tests/, __graft_entry__.smoke(), and bench.py's cpu_baseline / reference
+ * arm).  Nothing in the product links or calls it.
+ *
+ * Parity pins: the safe-math port (cbrt, atan) is checked bit for bit
+ * against the reference's own golden vectors (tests/test_safe_math_golden.inc,
+ * transcribed by tests/golden/make_safe_math_golden.py); the physics is
+ * checked against the reference's analytic known-answer tests
+ * (tests/test_ocean_pp81.F90, test_ocean_kpp.F90, test_ocean_vdiff.F90,
+ * test_ocean_vmix_assembly.F90, test_ocean_bkgnd_mixing.F90,
+ * test_ocean_kpp_nonlocal.F90) re-expressed in tests/test_oracle_*.py.
+ * The Fortran reference itself cannot be compiled here (no Fortran
+ * compiler), so bitwise parity with its binary output is unpinned.
+ *
+ * Loop order and operation order follow the Fortran source line by line;
+ * build with -ffp-contract=off (the reference's CPU builds' setting), no
+ * -ffast-math.
+ */
+#ifndef VPHYS_ORACLE_H
+#define VPHYS_ORACLE_H
+
+#include "../include/vphys.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* All arrays of one column-physics state, Fortran layout (see vphys.h). */
+typedef struct vpo_state {
+    int nx, ny, nz, ntr;
+    double *h, *rho, *u, *v;
+    double *kv, *kt, *ks, *kd_bg;          /* kd_bg: (nx,ny,nz+1) scratch */
+    double *bl_depth, *b0, *stress_mag, *q_heat, *q_salt, *wet;
+    double *tau_x, *tau_y, *lambda_bot_u, *lambda_bot_v;
+    double *visc_rem_u, *visc_rem_v;
+    double *gamma_t, *gamma_s;
+    double *heat_budget, *salt_budget;
+    int *k_top_u, *k_top_v, *k_bot_u, *k_bot_v;   /* 1-based */
+    double **tr;                            /* ntr pointers */
+} vpo_state;
+
+void vpo_set_threads(int n);
+int vpo_get_threads(void);
+
+double vpo_sm_cbrt(double x);
+double vpo_sm_atan(double x);
+
+void vpo_eos_wright(const vphys_config *c, vpo_state *s);
+void vpo_stress_mag(vpo_state *s);
+
+void vpo_pp81(const vphys_config *c, vpo_state *s);
+void vpo_seed_interior_none(const vphys_config *c, vpo_state *s);
+void vpo_kpp_overlay(const vphys_config *c, vpo_state *s);
+void vpo_kv_ml_invz2(const vphys_config *c, vpo_state *s);
+void vpo_convection(const vphys_config *c, vpo_state *s);
+void vpo_split(const vphys_config *c, vpo_state *s);
+int vpo_assemble_gate(const vphys_config *c, vpo_state *s);
+int vpo_build_coefficients(const vphys_config *c, vpo_state *s);
+
+void vpo_vdiff_momentum(const vphys_config *c, vpo_state *s, double dt);
+void vpo_vdiff_tracers(const vphys_config *c, vpo_state *s, double dt);
+void vpo_nonlocal(const vphys_config *c, vpo_state *s, double dt);
+
+int vpo_step(const vphys_config *c, vpo_state *s, double dt, int n_steps);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

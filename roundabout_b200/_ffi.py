@@ -1,0 +1,212 @@
+"""ctypes bindings to libvphys.so (include/vphys.h).
+
+Mirrors the conventions of the reference's python/rdb/_ffi.py: stdlib ctypes
+only, every prototype declared so a mismatched call raises instead of
+corrupting memory, status codes kept byte-for-byte in sync with the C header,
+and a library search order of
+
+  1. ``VPHYS_LIB`` environment variable (explicit path to the .so);
+  2. the in-tree build ``roundabout_b200/csrc/_build/libvphys.so``.
+
+There is no CPU fallback: if the library is missing, `get_lib()` raises
+`LibraryNotFoundError`.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+# ---- status codes: keep in sync with include/vphys.h -------------------
+OK = 0
+ERR_CONFIG = 2
+ERR_BAD_HANDLE = 10
+ERR_NOT_INITIALISED = 12
+ERR_NOT_FOUND = 13
+ERR_BAD_SHAPE = 14
+ERR_CUDA = 30
+ERR_GUARD = 31
+ERR_TOO_DEEP = 32
+ERR_ALLOC = 33
+
+NZ_MAX = 127
+INTERIOR_PP81 = 1
+INTERIOR_NONE = 4
+
+# ---- field ids ---------------------------------------------------------
+FIELD_H = 0
+FIELD_RHO = 1
+FIELD_U = 2
+FIELD_V = 3
+FIELD_KV = 4
+FIELD_KT = 5
+FIELD_KS = 6
+FIELD_BL_DEPTH = 7
+FIELD_B0 = 8
+FIELD_STRESS_MAG = 9
+FIELD_Q_HEAT = 10
+FIELD_Q_SALT = 11
+FIELD_WET = 12
+FIELD_TAU_X = 13
+FIELD_TAU_Y = 14
+FIELD_LAMBDA_BOT_U = 15
+FIELD_LAMBDA_BOT_V = 16
+FIELD_VISC_REM_U = 17
+FIELD_VISC_REM_V = 18
+FIELD_GAMMA_T = 19
+FIELD_GAMMA_S = 20
+FIELD_HEAT_BUDGET = 21
+FIELD_SALT_BUDGET = 22
+FIELD_K_TOP_U = 23
+FIELD_K_TOP_V = 24
+FIELD_K_BOT_U = 25
+FIELD_K_BOT_V = 26
+FIELD_TRACER0 = 64
+
+FIELD_NAMES = {
+    "h": FIELD_H, "rho": FIELD_RHO, "u": FIELD_U, "v": FIELD_V, "kv": FIELD_KV, "kt": FIELD_KT,
+    "ks": FIELD_KS, "bl_depth": FIELD_BL_DEPTH, "b0": FIELD_B0, "stress_mag": FIELD_STRESS_MAG,
+    "q_heat": FIELD_Q_HEAT, "q_salt": FIELD_Q_SALT, "wet": FIELD_WET, "tau_x": FIELD_TAU_X,
+    "tau_y": FIELD_TAU_Y, "lambda_bot_u": FIELD_LAMBDA_BOT_U, "lambda_bot_v": FIELD_LAMBDA_BOT_V,
+    "visc_rem_u": FIELD_VISC_REM_U, "visc_rem_v": FIELD_VISC_REM_V, "gamma_t": FIELD_GAMMA_T,
+    "gamma_s": FIELD_GAMMA_S, "heat_budget": FIELD_HEAT_BUDGET, "salt_budget": FIELD_SALT_BUDGET,
+    "k_top_u": FIELD_K_TOP_U, "k_top_v": FIELD_K_TOP_V, "k_bot_u": FIELD_K_BOT_U,
+    "k_bot_v": FIELD_K_BOT_V,
+}
+INT_FIELDS = (FIELD_K_TOP_U, FIELD_K_TOP_V, FIELD_K_BOT_U, FIELD_K_BOT_V)
+
+
+def field_shape(field: int, nx: int, ny: int, nz: int):
+    """Fortran-order shape of a field (matches vphys_field_shape in C)."""
+    if field >= FIELD_TRACER0 or field in (FIELD_H, FIELD_RHO, FIELD_HEAT_BUDGET, FIELD_SALT_BUDGET):
+        return (nx, ny, nz)
+    if field in (FIELD_U, FIELD_VISC_REM_U):
+        return (nx + 1, ny, nz)
+    if field in (FIELD_V, FIELD_VISC_REM_V):
+        return (nx, ny + 1, nz)
+    if field in (FIELD_KV, FIELD_KT, FIELD_KS, FIELD_GAMMA_T, FIELD_GAMMA_S):
+        return (nx, ny, nz + 1)
+    if field in (FIELD_BL_DEPTH, FIELD_B0, FIELD_STRESS_MAG, FIELD_Q_HEAT, FIELD_Q_SALT, FIELD_WET):
+        return (nx, ny)
+    if field in (FIELD_TAU_X, FIELD_LAMBDA_BOT_U, FIELD_K_TOP_U, FIELD_K_BOT_U):
+        return (nx + 1, ny)
+    if field in (FIELD_TAU_Y, FIELD_LAMBDA_BOT_V, FIELD_K_TOP_V, FIELD_K_BOT_V):
+        return (nx, ny + 1)
+    raise KeyError(field)
+
+
+class VphysConfig(ctypes.Structure):
+    """Mirror of `struct vphys_config` (include/vphys.h), field for field."""
+    _fields_ = [
+        ("use_closure", ctypes.c_int), ("interior_closure", ctypes.c_int), ("use_kpp", ctypes.c_int),
+        ("bkgnd_profile", ctypes.c_int), ("vmix_guard", ctypes.c_int), ("kd_smooth_iterations", ctypes.c_int),
+        ("conv_enable", ctypes.c_int), ("pad0", ctypes.c_int),
+        ("pp81_nu0", ctypes.c_double), ("pp81_nu_bg", ctypes.c_double), ("pp81_kappa_bg", ctypes.c_double),
+        ("pp81_alpha", ctypes.c_double), ("rho0", ctypes.c_double), ("shear2_floor", ctypes.c_double),
+        ("ri_crit", ctypes.c_double), ("cs_nonlocal", ctypes.c_double), ("c_vt2", ctypes.c_double),
+        ("alpha_T", ctypes.c_double), ("beta_S", ctypes.c_double), ("cp", ctypes.c_double),
+        ("kv_ml_invz2", ctypes.c_double), ("hmix_fixed", ctypes.c_double),
+        ("conv_kd", ctypes.c_double), ("conv_prandtl", ctypes.c_double), ("conv_n2_thresh", ctypes.c_double),
+        ("kv_bg", ctypes.c_double), ("kt_bg", ctypes.c_double), ("ks_bg", ctypes.c_double),
+        ("kv_max", ctypes.c_double), ("kd_max", ctypes.c_double),
+        ("bkgnd_kd_sfc", ctypes.c_double), ("bkgnd_kd_deep", ctypes.c_double), ("bkgnd_z0", ctypes.c_double),
+        ("bkgnd_delta", ctypes.c_double), ("bkgnd_prandtl", ctypes.c_double),
+        ("eos_p_ref", ctypes.c_double),
+        ("hvel_mom6", ctypes.c_int), ("hvel_harmonic", ctypes.c_int), ("hvel_upwind", ctypes.c_int),
+        ("use_harmonic", ctypes.c_int), ("implicit_stress", ctypes.c_int), ("implicit_drag", ctypes.c_int),
+        ("zlevel_faces", ctypes.c_int), ("bbl_glue", ctypes.c_int),
+        ("hbbl_visc", ctypes.c_double), ("bbl_piston", ctypes.c_double), ("kv_bbl_bg", ctypes.c_double),
+        ("idx_temperature", ctypes.c_int), ("idx_salinity", ctypes.c_int), ("idx_pseudo_salt", ctypes.c_int),
+        ("eos_in_step", ctypes.c_int), ("remnant", ctypes.c_int), ("budgets", ctypes.c_int),
+    ]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_ if n != "pad0"}
+
+
+class LibraryNotFoundError(FileNotFoundError):
+    """Raised when libvphys.so has not been built."""
+
+
+PKG_DIR = Path(__file__).resolve().parent
+BUILD_DIR = PKG_DIR / "csrc" / "_build"
+LIB_NAME = "libvphys.so"
+
+
+def find_library() -> Path:
+    env = os.environ.get("VPHYS_LIB")
+    if env:
+        p = Path(env)
+        if p.exists():
+            return p
+        raise LibraryNotFoundError(f"VPHYS_LIB={env} does not exist")
+    p = BUILD_DIR / LIB_NAME
+    if p.exists():
+        return p
+    raise LibraryNotFoundError(
+        f"{p} not found: build it with `python -c 'import __graft_entry__ as g; g.build()'` "
+        "or `python -m roundabout_b200.build`")
+
+
+_PROTOTYPES = {
+    "vphys_config_default": (ctypes.c_int, [ctypes.POINTER(VphysConfig)]),
+    "vphys_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                    ctypes.POINTER(VphysConfig), ctypes.POINTER(ctypes.c_void_p)]),
+    "vphys_destroy": (ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p)]),
+    "vphys_set_config": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(VphysConfig)]),
+    "vphys_get_config": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(VphysConfig)]),
+    "vphys_set_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "vphys_bind": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "vphys_set_field": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t]),
+    "vphys_get_field": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t]),
+    "vphys_get_ptr": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
+                                     ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                     ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "vphys_eos_wright": (ctypes.c_int, [ctypes.c_void_p]),
+    "vphys_stress_mag": (ctypes.c_int, [ctypes.c_void_p]),
+    "vphys_assemble": (ctypes.c_int, [ctypes.c_void_p]),
+    "vphys_vdiff_momentum": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    "vphys_vdiff_tracers": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    "vphys_nonlocal": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    "vphys_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]),
+    "vphys_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
+    "vphys_last_error": (ctypes.c_int, [ctypes.c_int, ctypes.c_char_p, ctypes.c_int]),
+    "vphys_version": (ctypes.c_char_p, []),
+    "vphys_config_sizeof": (ctypes.c_size_t, []),
+}
+
+EXPORTED_SYMBOLS = tuple(_PROTOTYPES)
+
+_lib = None
+
+
+def get_lib():
+    """Load libvphys.so once and declare every prototype."""
+    global _lib
+    if _lib is None:
+        L = ctypes.CDLL(str(find_library()))
+        for name, (res, args) in _PROTOTYPES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def last_error(idx: int = 0) -> str:
+    L = get_lib()
+    buf = ctypes.create_string_buffer(1024)
+    n = L.vphys_last_error(idx, buf, len(buf))
+    return buf.value.decode(errors="replace") if n > 0 else ""
+
+
+class VphysError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        self.status = status
+        super().__init__(f"{where} failed with status {status}: {last_error(0)}")
+
+
+def check(status: int, where: str):
+    if status != OK:
+        raise VphysError(status, where)
+    return status

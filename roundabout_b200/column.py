@@ -1,0 +1,172 @@
+"""`VerticalPhysics`: the Python driver of libvphys (the CUDA library).
+
+Mirrors the reference's python/rdb model surface for this path
+(python/rdb/_model.py:94-96, 703-707: `Model(...).step(n)`, field views such
+as `m.kv` / `m.kt`), over the C ABI of include/vphys.h:
+
+    vp = VerticalPhysics(nx, ny, nz, ntracers, config)
+    vp.set("h", h); vp.set_tracer(0, S); ...       # host numpy -> HBM
+    vp.bind("u", tensor)                             # zero-copy device array
+    vp.step(dt, n)                                   # whole chain on the GPU
+    kv = vp.get("kv")                                # HBM -> host numpy
+
+Arrays use the reference layout: Fortran order with shape (nx, ny, nz) etc.
+(k = 0 the bed).  A torch tensor bound to a field must be a contiguous CUDA
+float64 tensor of shape (nz, ny, nx) -- the same bytes as the Fortran
+(nx, ny, nz) array.  There is no CPU fallback: a missing library or GPU
+raises.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _ffi
+from .config import default_config
+
+
+class VerticalPhysics:
+    def __init__(self, nx: int, ny: int, nz: int, ntracers: int, config=None):
+        self.lib = _ffi.get_lib()
+        self.nx, self.ny, self.nz, self.ntr = int(nx), int(ny), int(nz), int(ntracers)
+        self.config = config if config is not None else default_config()
+        h = ctypes.c_void_p()
+        _ffi.check(self.lib.vphys_create(self.nx, self.ny, self.nz, self.ntr, ctypes.byref(self.config),
+                                         ctypes.byref(h)), "vphys_create")
+        self._h = h
+        self._bound = {}
+
+    # ---- lifecycle ---------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self.lib.vphys_destroy(ctypes.byref(self._h))
+        self._h = None
+        self._bound = {}
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_config(self, cfg):
+        _ffi.check(self.lib.vphys_set_config(self._h, ctypes.byref(cfg)), "vphys_set_config")
+        self.config = cfg
+
+    def set_stream(self, stream_ptr: int):
+        _ffi.check(self.lib.vphys_set_stream(self._h, ctypes.c_void_p(stream_ptr)), "vphys_set_stream")
+
+    # ---- fields ------------------------------------------------------------
+    def _fid(self, name):
+        if isinstance(name, int):
+            return name
+        if name.startswith("tracer"):
+            return _ffi.FIELD_TRACER0 + int(name[6:])
+        return _ffi.FIELD_NAMES[name]
+
+    def shape(self, name):
+        return _ffi.field_shape(self._fid(name), self.nx, self.ny, self.nz)
+
+    def set(self, name, array):
+        fid = self._fid(name)
+        dtype = np.int32 if fid in _ffi.INT_FIELDS else np.float64
+        a = np.asarray(array, dtype=dtype)
+        shp = self.shape(fid)
+        if a.shape != shp:
+            raise ValueError(f"{name}: expected shape {shp}, got {a.shape}")
+        a = np.asfortranarray(a)
+        _ffi.check(self.lib.vphys_set_field(self._h, fid, a.ctypes.data_as(ctypes.c_void_p), a.size),
+                   f"vphys_set_field({name})")
+
+    def get(self, name):
+        fid = self._fid(name)
+        dtype = np.int32 if fid in _ffi.INT_FIELDS else np.float64
+        out = np.empty(self.shape(fid), dtype=dtype, order="F")
+        _ffi.check(self.lib.vphys_get_field(self._h, fid, out.ctypes.data_as(ctypes.c_void_p), out.size),
+                   f"vphys_get_field({name})")
+        return out
+
+    def set_tracer(self, t, array):
+        self.set(_ffi.FIELD_TRACER0 + int(t), array)
+
+    def get_tracer(self, t):
+        return self.get(_ffi.FIELD_TRACER0 + int(t))
+
+    def device_ptr(self, name):
+        ptr = ctypes.c_void_p()
+        gen = ctypes.c_int()
+        nx, ny, nz = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _ffi.check(self.lib.vphys_get_ptr(self._h, self._fid(name), ctypes.byref(ptr), ctypes.byref(nx),
+                                          ctypes.byref(ny), ctypes.byref(nz), ctypes.byref(gen)), "vphys_get_ptr")
+        return ptr.value, (nx.value, ny.value, nz.value), gen.value
+
+    def bind(self, name, tensor):
+        """Zero-copy: use a CUDA tensor (contiguous, float64/int32) for a field."""
+        fid = self._fid(name)
+        if tensor is None:
+            _ffi.check(self.lib.vphys_bind(self._h, fid, None), f"vphys_bind({name})")
+            self._bound.pop(fid, None)
+            return
+        expect = int(np.prod(self.shape(fid)))
+        if not tensor.is_cuda or not tensor.is_contiguous() or tensor.numel() != expect:
+            raise ValueError(f"{name}: need a contiguous CUDA tensor with {expect} elements")
+        self._bound[fid] = tensor   # keep alive
+        _ffi.check(self.lib.vphys_bind(self._h, fid, ctypes.c_void_p(tensor.data_ptr())), f"vphys_bind({name})")
+
+    def load_columns(self, cols):
+        """Upload a `synthetic.Columns` (h, u, v, tracers, forcing, wet) and
+        derive stress_mag from the face stresses."""
+        self.set("h", cols.h)
+        self.set("u", cols.u)
+        self.set("v", cols.v)
+        for t, a in enumerate(cols.tracers[: self.ntr]):
+            self.set_tracer(t, a)
+        self.set("tau_x", cols.tau_x)
+        self.set("tau_y", cols.tau_y)
+        self.set("q_heat", cols.q_heat)
+        self.set("q_salt", cols.q_salt)
+        self.set("wet", cols.wet)
+        self.stress_mag()
+
+    # ---- the hot path --------------------------------------------------------
+    def eos(self):
+        _ffi.check(self.lib.vphys_eos_wright(self._h), "vphys_eos_wright")
+
+    def stress_mag(self):
+        _ffi.check(self.lib.vphys_stress_mag(self._h), "vphys_stress_mag")
+
+    def assemble(self):
+        return _ffi.check(self.lib.vphys_assemble(self._h), "vphys_assemble")
+
+    def assemble_status(self):
+        """vphys_assemble returning the status instead of raising (guard path)."""
+        return self.lib.vphys_assemble(self._h)
+
+    def vdiff_momentum(self, dt):
+        _ffi.check(self.lib.vphys_vdiff_momentum(self._h, float(dt)), "vphys_vdiff_momentum")
+
+    def vdiff_tracers(self, dt):
+        _ffi.check(self.lib.vphys_vdiff_tracers(self._h, float(dt)), "vphys_vdiff_tracers")
+
+    def nonlocal_tendencies(self, dt):
+        _ffi.check(self.lib.vphys_nonlocal(self._h, float(dt)), "vphys_nonlocal")
+
+    def step(self, dt, n_steps=1):
+        _ffi.check(self.lib.vphys_step(self._h, float(dt), int(n_steps)), "vphys_step")
+
+    def step_status(self, dt, n_steps=1):
+        return self.lib.vphys_step(self._h, float(dt), int(n_steps))
+
+    def synchronize(self):
+        _ffi.check(self.lib.vphys_synchronize(self._h), "vphys_synchronize")

@@ -1,0 +1,244 @@
+"""Configuration of the vertical-physics path.
+
+`default_config()` returns a `VphysConfig` holding the reference defaults
+(ocean_vmix_t, src/parameterizations/vertical/rdb_ocean_vmix.F90:198-483;
+ocean_vdiff_t, rdb_ocean_vdiff.F90:78-260; namelist defaults
+src/core/rdb_config.F90:1872-1893, 1936-1945) -- the same values
+`vphys_config_default()` writes in C.
+
+The closure classes mirror python/rdb/closures.py (PacanowskiPhilander, KPP,
+BryanLewisBackground, ConstantBackground, NearSurfaceViscosity,
+ConvectiveAdjustment, HarmonicFaceThickness, ImplicitVerticalFriction,
+DiffusivityLimits): same names, same keyword meanings, each writing only its
+own knobs into the config through `apply(cfg)`.
+"""
+from __future__ import annotations
+
+import sys
+
+from ._ffi import INTERIOR_NONE, INTERIOR_PP81, VphysConfig
+
+HUGE = sys.float_info.max
+
+
+def default_config() -> VphysConfig:
+    c = VphysConfig()
+    c.use_closure = 1
+    c.interior_closure = INTERIOR_PP81
+    c.use_kpp = 0
+    c.bkgnd_profile = 0
+    c.vmix_guard = 0
+    c.kd_smooth_iterations = 0
+    c.conv_enable = 0
+    c.pp81_nu0 = 1.0e-2
+    c.pp81_nu_bg = 1.0e-4
+    c.pp81_kappa_bg = 1.0e-5
+    c.pp81_alpha = 5.0
+    c.rho0 = 1035.0
+    c.shear2_floor = 1.0e-10
+    c.ri_crit = 0.3
+    c.cs_nonlocal = 6.3
+    c.c_vt2 = 1.8
+    c.alpha_T = 1.7e-4
+    c.beta_S = 7.6e-4
+    c.cp = 3992.0
+    c.kv_ml_invz2 = 0.0
+    c.hmix_fixed = 20.0
+    c.conv_kd = 1.0
+    c.conv_prandtl = 1.0
+    c.conv_n2_thresh = 0.0
+    c.kv_bg = 1.0e-4
+    c.kt_bg = 1.0e-5
+    c.ks_bg = 1.0e-5
+    c.kv_max = HUGE
+    c.kd_max = HUGE
+    c.bkgnd_kd_sfc = 1.0e-5
+    c.bkgnd_kd_deep = 1.3e-4
+    c.bkgnd_z0 = 2500.0
+    c.bkgnd_delta = 222.0
+    c.bkgnd_prandtl = -1.0
+    c.eos_p_ref = 0.0
+    c.hvel_mom6 = 1
+    c.hvel_harmonic = 0
+    c.hvel_upwind = 1
+    c.use_harmonic = 0
+    c.implicit_stress = 0
+    c.implicit_drag = 0
+    c.zlevel_faces = 0
+    c.bbl_glue = 0
+    c.hbbl_visc = 10.0
+    c.bbl_piston = 3.0e-4
+    c.kv_bbl_bg = 1.0e-4
+    c.idx_temperature = 1
+    c.idx_salinity = 0
+    c.idx_pseudo_salt = -1
+    c.eos_in_step = 0
+    c.remnant = 0
+    c.budgets = 0
+    return c
+
+
+def hot_path_config(ntracers: int = 4, pseudo_salt_index: int | None = 3) -> VphysConfig:
+    """The benchmark configuration: PP81 + KPP + Bryan-Lewis, Wright EOS in
+    the step, dimensional alpha_T = 0.2 / beta_S = 0.77 (the kpp_basin example,
+    validation_examples/ocean/epbl_mld/kpp_basin.nml), tracers S, T, then
+    passives (ideal age, pseudo-salt)."""
+    c = default_config()
+    c.use_kpp = 1
+    c.bkgnd_profile = 1
+    c.alpha_T = 0.2
+    c.beta_S = 0.77
+    c.eos_in_step = 1
+    c.idx_salinity = 0
+    c.idx_temperature = 1
+    c.idx_pseudo_salt = pseudo_salt_index if (pseudo_salt_index is not None and pseudo_salt_index < ntracers) else -1
+    return c
+
+
+def seed_backgrounds(cfg: VphysConfig):
+    """vmix_seed_backgrounds (rdb_ocean_vmix.F90:843-913): kv_bg/kt_bg/ks_bg
+    follow pp81_nu_bg / pp81_kappa_bg."""
+    cfg.kv_bg = cfg.pp81_nu_bg
+    cfg.kt_bg = cfg.pp81_kappa_bg
+    cfg.ks_bg = cfg.pp81_kappa_bg
+    return cfg
+
+
+# ---------------------------------------------------------------------------
+# Closure objects (python/rdb/closures.py:20-413)
+# ---------------------------------------------------------------------------
+class PacanowskiPhilander:
+    """PP81 interior closure; `enabled=False` selects interior_closure="none"."""
+
+    def __init__(self, nu0=1e-2, nu_bg=1e-4, kappa_bg=1e-5, alpha=5.0, shear2_floor=1e-10, enabled=True):
+        self.nu0, self.nu_bg, self.kappa_bg = nu0, nu_bg, kappa_bg
+        self.alpha, self.shear2_floor = alpha, shear2_floor
+        self.enabled = bool(enabled)
+
+    def apply(self, cfg):
+        cfg.interior_closure = INTERIOR_PP81 if self.enabled else INTERIOR_NONE
+        if not self.enabled:
+            return cfg
+        cfg.pp81_nu0 = float(self.nu0)
+        cfg.pp81_nu_bg = float(self.nu_bg)
+        cfg.pp81_kappa_bg = float(self.kappa_bg)
+        cfg.pp81_alpha = float(self.alpha)
+        cfg.shear2_floor = float(self.shear2_floor)
+        return seed_backgrounds(cfg)
+
+
+class KPP:
+    """KPP boundary-layer overlay (no shortwave penetration on this path)."""
+
+    def __init__(self, ri_crit=0.3, cs_nonlocal=6.3, c_vt2=1.8, alpha_T=None, beta_S=None, enabled=True):
+        self.ri_crit, self.cs_nonlocal, self.c_vt2 = ri_crit, cs_nonlocal, c_vt2
+        self.alpha_T, self.beta_S = alpha_T, beta_S
+        self.enabled = bool(enabled)
+
+    def apply(self, cfg):
+        cfg.use_kpp = int(self.enabled)
+        if not self.enabled:
+            return cfg
+        cfg.ri_crit = float(self.ri_crit)
+        cfg.cs_nonlocal = float(self.cs_nonlocal)
+        cfg.c_vt2 = float(self.c_vt2)
+        if self.alpha_T is not None:
+            cfg.alpha_T = float(self.alpha_T)
+        if self.beta_S is not None:
+            cfg.beta_S = float(self.beta_S)
+        return cfg
+
+
+class BryanLewisBackground:
+    def __init__(self, kd_surface=1e-5, kd_deep=1.3e-4, z0=2500.0, delta=222.0, prandtl=-1.0):
+        self.kd_surface, self.kd_deep, self.z0, self.delta, self.prandtl = kd_surface, kd_deep, z0, delta, prandtl
+
+    def apply(self, cfg):
+        cfg.bkgnd_profile = 1
+        cfg.bkgnd_kd_sfc = float(self.kd_surface)
+        cfg.bkgnd_kd_deep = float(self.kd_deep)
+        cfg.bkgnd_z0 = float(self.z0)
+        cfg.bkgnd_delta = float(self.delta)
+        cfg.bkgnd_prandtl = float(self.prandtl)
+        return cfg
+
+
+class ConstantBackground:
+    def __init__(self, kv=1e-4, kt=1e-5):
+        self.kv, self.kt = kv, kt
+
+    def apply(self, cfg):
+        cfg.bkgnd_profile = 0
+        cfg.kv_bg = float(self.kv)
+        cfg.kt_bg = float(self.kt)
+        cfg.ks_bg = float(self.kt)
+        return cfg
+
+
+class NearSurfaceViscosity:
+    """KV_ML_INVZ2 surface band."""
+
+    def __init__(self, kv=0.0, hmix=20.0):
+        self.kv, self.hmix = kv, hmix
+
+    def apply(self, cfg):
+        cfg.kv_ml_invz2 = float(self.kv)
+        cfg.hmix_fixed = float(self.hmix)
+        return cfg
+
+
+class ConvectiveAdjustment:
+    def __init__(self, kd=1.0, prandtl=1.0, n2_threshold=0.0):
+        self.kd, self.prandtl, self.n2_threshold = kd, prandtl, n2_threshold
+
+    def apply(self, cfg):
+        cfg.conv_enable = 1
+        cfg.conv_kd = float(self.kd)
+        cfg.conv_prandtl = float(self.prandtl)
+        cfg.conv_n2_thresh = float(self.n2_threshold)
+        return cfg
+
+
+class HarmonicFaceThickness:
+    """`use_harmonic`: harmonic mean in the vdiff face-thickness denominators."""
+
+    def apply(self, cfg):
+        cfg.use_harmonic = 1
+        return cfg
+
+
+class ImplicitVerticalFriction:
+    def __init__(self, stress=False, drag=False, harmonic_thickness=False, mom6_face_thickness=True,
+                 upwind=True, bbl_glue=False, hbbl=10.0):
+        self.stress, self.drag = stress, drag
+        self.harmonic_thickness, self.mom6_face_thickness = harmonic_thickness, mom6_face_thickness
+        self.upwind, self.bbl_glue, self.hbbl = upwind, bbl_glue, hbbl
+
+    def apply(self, cfg):
+        cfg.implicit_stress = int(self.stress)
+        cfg.implicit_drag = int(self.drag)
+        cfg.hvel_mom6 = int(self.mom6_face_thickness)
+        cfg.hvel_harmonic = int(self.harmonic_thickness)
+        cfg.hvel_upwind = int(self.upwind)
+        cfg.bbl_glue = int(self.bbl_glue)
+        cfg.hbbl_visc = float(self.hbbl)
+        return cfg
+
+
+class DiffusivityLimits:
+    def __init__(self, kv_max=HUGE, kd_max=HUGE, smoothing=0, guard=False):
+        self.kv_max, self.kd_max, self.smoothing, self.guard = kv_max, kd_max, smoothing, guard
+
+    def apply(self, cfg):
+        cfg.kv_max = float(self.kv_max)
+        cfg.kd_max = float(self.kd_max)
+        cfg.kd_smooth_iterations = int(self.smoothing)
+        cfg.vmix_guard = int(self.guard)
+        return cfg
+
+
+def compose(*closures, base: VphysConfig | None = None) -> VphysConfig:
+    cfg = base if base is not None else default_config()
+    for c in closures:
+        c.apply(cfg)
+    return cfg

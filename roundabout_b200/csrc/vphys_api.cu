@@ -1,0 +1,653 @@
+// vphys_api.cu -- host runtime and C ABI of libvphys (include/vphys.h).
+//
+// A handle owns the grid shape, the configuration, a CUDA stream and one
+// device buffer per field.  Core fields are allocated in HBM at create;
+// optional ones (remnant, budgets, gamma diagnostics, drag rates, k_top/k_bot
+// overrides, smoothing scratch) the first time a stage or the caller needs
+// them.  Any field can instead be bound to a caller-owned device array.
+// Stage entry points enqueue kernels on the handle's stream and return.
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/vphys.h"
+#include "vphys_kernels.cuh"
+
+using vphys::Params;
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// error ring (rdb_ocean_last_error contract, include/rdb_ocean.h:305-314)
+// ---------------------------------------------------------------------------
+std::mutex g_err_mu;
+std::deque<std::string> g_err;
+constexpr size_t ERR_RING = 32;
+
+int push_error(int status, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    g_err.emplace_front(buf);
+    while (g_err.size() > ERR_RING) g_err.pop_back();
+    return status;
+}
+
+int cuda_status(cudaError_t e, const char *where)
+{
+    if (e == cudaSuccess) return VPHYS_OK;
+    return push_error(VPHYS_ERR_CUDA, "%s: CUDA error %d (%s)", where, (int)e, cudaGetErrorString(e));
+}
+
+constexpr int NFIXED = 27;
+constexpr unsigned MAGIC = 0x56504859u;   // "VPHY"
+
+struct Field {
+    void *own = nullptr;     // handle-owned device buffer
+    void *bound = nullptr;   // caller-owned device buffer
+    size_t n = 0;            // elements
+    bool is_int = false;
+    void *ptr() const { return bound ? bound : own; }
+    size_t bytes() const { return n * (is_int ? sizeof(int) : sizeof(double)); }
+};
+
+}  // namespace
+
+struct vphys_handle_s {
+    unsigned magic = MAGIC;
+    int nx = 0, ny = 0, nz = 0, ntr = 0;
+    vphys_config cfg{};
+    cudaStream_t stream = nullptr;
+    int gen = 0;
+    std::vector<Field> f;             // NFIXED fixed fields, then ntr tracers
+    unsigned long long *guard_dev = nullptr;
+    double *smooth_scratch = nullptr;
+};
+
+namespace {
+
+bool valid(vphys_handle h) { return h != nullptr && h->magic == MAGIC; }
+
+int slot_of(const vphys_handle_s *h, int field)
+{
+    if (field >= 0 && field < NFIXED) return field;
+    if (field >= VPHYS_FIELD_TRACER0 && field < VPHYS_FIELD_TRACER0 + h->ntr) return NFIXED + (field - VPHYS_FIELD_TRACER0);
+    return -1;
+}
+
+size_t field_count(int nx, int ny, int nz, int field, bool *is_int)
+{
+    const size_t X = nx, Y = ny, Z = nz;
+    *is_int = false;
+    if (field >= VPHYS_FIELD_TRACER0) return X * Y * Z;
+    switch (field) {
+    case VPHYS_FIELD_H:
+    case VPHYS_FIELD_RHO:
+    case VPHYS_FIELD_HEAT_BUDGET:
+    case VPHYS_FIELD_SALT_BUDGET: return X * Y * Z;
+    case VPHYS_FIELD_U:
+    case VPHYS_FIELD_VISC_REM_U: return (X + 1) * Y * Z;
+    case VPHYS_FIELD_V:
+    case VPHYS_FIELD_VISC_REM_V: return X * (Y + 1) * Z;
+    case VPHYS_FIELD_KV:
+    case VPHYS_FIELD_KT:
+    case VPHYS_FIELD_KS:
+    case VPHYS_FIELD_GAMMA_T:
+    case VPHYS_FIELD_GAMMA_S: return X * Y * (Z + 1);
+    case VPHYS_FIELD_BL_DEPTH:
+    case VPHYS_FIELD_B0:
+    case VPHYS_FIELD_STRESS_MAG:
+    case VPHYS_FIELD_Q_HEAT:
+    case VPHYS_FIELD_Q_SALT:
+    case VPHYS_FIELD_WET: return X * Y;
+    case VPHYS_FIELD_TAU_X:
+    case VPHYS_FIELD_LAMBDA_BOT_U: return (X + 1) * Y;
+    case VPHYS_FIELD_TAU_Y:
+    case VPHYS_FIELD_LAMBDA_BOT_V: return X * (Y + 1);
+    case VPHYS_FIELD_K_TOP_U:
+    case VPHYS_FIELD_K_BOT_U: *is_int = true; return (X + 1) * Y;
+    case VPHYS_FIELD_K_TOP_V:
+    case VPHYS_FIELD_K_BOT_V: *is_int = true; return X * (Y + 1);
+    default: return 0;
+    }
+}
+
+// ---- fills used at allocation ------------------------------------------
+__global__ void k_fill_double(double *p, size_t n, double v)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) p[i] = v;
+}
+__global__ void k_fill_int(int *p, size_t n, int v)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) p[i] = v;
+}
+// interface seed: interior value, 0 on the bed (k=1) and surface (k=nz+1)
+__global__ void k_fill_interfaces(double *p, size_t plane, int nz, double interior)
+{
+    const size_t n = plane * (size_t)(nz + 1);
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        size_t k = i / plane;
+        p[i] = (k == 0 || k == (size_t)nz) ? 0.0 : interior;
+    }
+}
+
+int fill_blocks(size_t n)
+{
+    size_t b = (n + 255) / 256;
+    return (int)(b < 4096 ? (b ? b : 1) : 4096);
+}
+
+// Initial contents of a freshly allocated field (vmix_seed_backgrounds,
+// rdb_ocean_vmix.F90:843-913, and ocean_multilayer_state init defaults).
+int init_field(vphys_handle h, int field, Field &fl)
+{
+    const size_t plane = (size_t)h->nx * h->ny;
+    cudaStream_t s = h->stream;
+    switch (field) {
+    case VPHYS_FIELD_WET: k_fill_double<<<fill_blocks(fl.n), 256, 0, s>>>((double *)fl.own, fl.n, 1.0); break;
+    case VPHYS_FIELD_KV: k_fill_interfaces<<<fill_blocks(fl.n), 256, 0, s>>>((double *)fl.own, plane, h->nz, h->cfg.pp81_nu_bg); break;
+    case VPHYS_FIELD_KT:
+    case VPHYS_FIELD_KS: k_fill_interfaces<<<fill_blocks(fl.n), 256, 0, s>>>((double *)fl.own, plane, h->nz, h->cfg.pp81_kappa_bg); break;
+    case VPHYS_FIELD_K_TOP_U:
+    case VPHYS_FIELD_K_TOP_V: k_fill_int<<<fill_blocks(fl.n), 256, 0, s>>>((int *)fl.own, fl.n, h->nz); break;
+    case VPHYS_FIELD_K_BOT_U:
+    case VPHYS_FIELD_K_BOT_V: k_fill_int<<<fill_blocks(fl.n), 256, 0, s>>>((int *)fl.own, fl.n, 1); break;
+    default: {
+        cudaError_t e = cudaMemsetAsync(fl.own, 0, fl.bytes(), s);
+        if (e != cudaSuccess) return cuda_status(e, "init_field");
+    }
+    }
+    return cuda_status(cudaGetLastError(), "init_field");
+}
+
+int ensure(vphys_handle h, int field)
+{
+    int sl = slot_of(h, field);
+    if (sl < 0) return push_error(VPHYS_ERR_NOT_FOUND, "unknown field id %d", field);
+    Field &fl = h->f[sl];
+    if (fl.ptr()) return VPHYS_OK;
+    cudaError_t e = cudaMalloc(&fl.own, fl.bytes());
+    if (e != cudaSuccess) {
+        fl.own = nullptr;
+        cudaGetLastError();
+        return push_error(VPHYS_ERR_ALLOC, "cudaMalloc of %zu bytes for field %d failed (%s)", fl.bytes(), field,
+                          cudaGetErrorString(e));
+    }
+    return init_field(h, field, fl);
+}
+
+bool present(vphys_handle h, int field) { return h->f[slot_of(h, field)].ptr() != nullptr; }
+
+int validate(const vphys_config *c, int ntr)
+{
+    if (!c->use_closure)
+        return push_error(VPHYS_ERR_CONFIG, "use_closure = 0 selects the scalar K_v_* vdiff path, which is not "
+                                            "part of this library (vmix closure path only)");
+    if (c->interior_closure != VPHYS_INTERIOR_PP81 && c->interior_closure != VPHYS_INTERIOR_NONE)
+        return push_error(VPHYS_ERR_CONFIG, "interior_closure %d has no kernel (only PP81=1 and NONE=4)",
+                          c->interior_closure);
+    if (c->idx_temperature >= ntr || c->idx_salinity >= ntr || c->idx_pseudo_salt >= ntr)
+        return push_error(VPHYS_ERR_CONFIG, "tracer role index beyond ntracer=%d", ntr);
+    if (c->idx_pseudo_salt >= 0 && (c->idx_pseudo_salt == c->idx_salinity || c->idx_pseudo_salt == c->idx_temperature))
+        return push_error(VPHYS_ERR_CONFIG, "pseudo-salt must be a tracer of its own");
+    if (c->idx_temperature >= 0 && c->idx_temperature == c->idx_salinity)
+        return push_error(VPHYS_ERR_CONFIG, "temperature and salinity must be different tracers");
+    if (c->kd_smooth_iterations < 0) return push_error(VPHYS_ERR_CONFIG, "kd_smooth_iterations < 0");
+    if (c->rho0 <= 0.0 || c->cp <= 0.0) return push_error(VPHYS_ERR_CONFIG, "rho0 and cp must be positive");
+    if (c->use_kpp && c->ri_crit <= 0.0) return push_error(VPHYS_ERR_CONFIG, "ri_crit must be positive");
+    if (c->bkgnd_profile && c->bkgnd_delta == 0.0) return push_error(VPHYS_ERR_CONFIG, "bkgnd_delta must be nonzero");
+    if (c->bkgnd_prandtl == 0.0)
+        return push_error(VPHYS_ERR_CONFIG, "bkgnd_prandtl = 0 is refused (use -1 for off), as the reference does");
+    return VPHYS_OK;
+}
+
+Params make_params(vphys_handle h)
+{
+    Params p{};
+    p.nx = h->nx;
+    p.ny = h->ny;
+    p.nz = h->nz;
+    p.ntr = h->ntr;
+    p.plane = (size_t)h->nx * h->ny;
+    p.plane_u = (size_t)(h->nx + 1) * h->ny;
+    p.plane_v = (size_t)h->nx * (h->ny + 1);
+    p.cfg = h->cfg;
+    auto D = [&](int fid) { return (double *)h->f[fid].ptr(); };
+    auto I = [&](int fid) { return (const int *)h->f[fid].ptr(); };
+    p.h = D(VPHYS_FIELD_H);
+    p.rho = D(VPHYS_FIELD_RHO);
+    p.u = D(VPHYS_FIELD_U);
+    p.v = D(VPHYS_FIELD_V);
+    p.kv = D(VPHYS_FIELD_KV);
+    p.kt = D(VPHYS_FIELD_KT);
+    p.ks = D(VPHYS_FIELD_KS);
+    p.bl_depth = D(VPHYS_FIELD_BL_DEPTH);
+    p.b0 = D(VPHYS_FIELD_B0);
+    p.stress_mag = D(VPHYS_FIELD_STRESS_MAG);
+    p.q_heat = D(VPHYS_FIELD_Q_HEAT);
+    p.q_salt = D(VPHYS_FIELD_Q_SALT);
+    p.wet = D(VPHYS_FIELD_WET);
+    p.tau_x = D(VPHYS_FIELD_TAU_X);
+    p.tau_y = D(VPHYS_FIELD_TAU_Y);
+    p.lambda_bot_u = D(VPHYS_FIELD_LAMBDA_BOT_U);
+    p.lambda_bot_v = D(VPHYS_FIELD_LAMBDA_BOT_V);
+    p.visc_rem_u = D(VPHYS_FIELD_VISC_REM_U);
+    p.visc_rem_v = D(VPHYS_FIELD_VISC_REM_V);
+    p.gamma_t = D(VPHYS_FIELD_GAMMA_T);
+    p.gamma_s = D(VPHYS_FIELD_GAMMA_S);
+    p.heat_budget = D(VPHYS_FIELD_HEAT_BUDGET);
+    p.salt_budget = D(VPHYS_FIELD_SALT_BUDGET);
+    p.k_top_u = I(VPHYS_FIELD_K_TOP_U);
+    p.k_top_v = I(VPHYS_FIELD_K_TOP_V);
+    p.k_bot_u = I(VPHYS_FIELD_K_BOT_U);
+    p.k_bot_v = I(VPHYS_FIELD_K_BOT_V);
+    for (int t = 0; t < h->ntr && t < vphys::NTR_MAX; ++t) p.tr[t] = (double *)h->f[NFIXED + t].ptr();
+    p.guard_count = h->guard_dev;
+    p.ks_equals_kt = (h->cfg.bkgnd_profile || h->cfg.kt_bg == h->cfg.ks_bg) ? 1 : 0;
+    p.write_gamma = (p.gamma_t && p.gamma_s) ? 1 : 0;
+    return p;
+}
+
+// Stage preconditions: allocate what the configuration needs.
+int prepare_momentum(vphys_handle h)
+{
+    int st = VPHYS_OK;
+    if (h->cfg.remnant) {
+        if ((st = ensure(h, VPHYS_FIELD_VISC_REM_U))) return st;
+        if ((st = ensure(h, VPHYS_FIELD_VISC_REM_V))) return st;
+    }
+    if (h->cfg.implicit_drag) {
+        if ((st = ensure(h, VPHYS_FIELD_LAMBDA_BOT_U))) return st;
+        if ((st = ensure(h, VPHYS_FIELD_LAMBDA_BOT_V))) return st;
+    }
+    return st;
+}
+
+int prepare_tracers(vphys_handle h)
+{
+    int st = VPHYS_OK;
+    if (h->cfg.budgets) {
+        if ((st = ensure(h, VPHYS_FIELD_HEAT_BUDGET))) return st;
+        if ((st = ensure(h, VPHYS_FIELD_SALT_BUDGET))) return st;
+    }
+    return st;
+}
+
+int prepare_assemble(vphys_handle h)
+{
+    if (h->cfg.kd_smooth_iterations > 0 && !h->smooth_scratch) {
+        size_t n = (size_t)h->nx * h->ny * (h->nz + 1);
+        cudaError_t e = cudaMalloc(&h->smooth_scratch, n * sizeof(double));
+        if (e != cudaSuccess) {
+            h->smooth_scratch = nullptr;
+            cudaGetLastError();
+            return push_error(VPHYS_ERR_ALLOC, "cudaMalloc of the smoothing scratch failed");
+        }
+    }
+    return VPHYS_OK;
+}
+
+int run_assemble(vphys_handle h, const Params &p)
+{
+    vphys::launch_assemble(p, h->stream);
+    for (int it = 0; it < h->cfg.kd_smooth_iterations; ++it) {
+        vphys::launch_smooth(p, p.kv, h->smooth_scratch, h->stream);
+        vphys::launch_smooth(p, p.kt, h->smooth_scratch, h->stream);
+        vphys::launch_smooth(p, p.ks, h->smooth_scratch, h->stream);
+    }
+    return cuda_status(cudaGetLastError(), "vphys_assemble launch");
+}
+
+int read_guard(vphys_handle h, int *status)
+{
+    unsigned long long bad = 0;
+    cudaError_t e = cudaMemcpyAsync(&bad, h->guard_dev, sizeof bad, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return cuda_status(e, "guard readback");
+    *status = VPHYS_OK;
+    if (bad > 0)
+        *status = push_error(VPHYS_ERR_GUARD, "vmix_assemble: %llu negative or NaN diffusivities detected", bad);
+    return VPHYS_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char *vphys_version(void) { return "vphys 0.1 (sm_100a, FP64)"; }
+
+size_t vphys_config_sizeof(void) { return sizeof(vphys_config); }
+
+int vphys_last_error(int idx, char *buf, int cap)
+{
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    if (idx < 0 || (size_t)idx >= g_err.size() || cap <= 0 || buf == nullptr) return 0;
+    const std::string &m = g_err[(size_t)idx];
+    size_t n = m.size() < (size_t)cap - 1 ? m.size() : (size_t)cap - 1;
+    memcpy(buf, m.data(), n);
+    buf[n] = '\0';
+    return (int)m.size();
+}
+
+int vphys_config_default(vphys_config *c)
+{
+    if (!c) return push_error(VPHYS_ERR_CONFIG, "vphys_config_default: NULL");
+    memset(c, 0, sizeof *c);
+    c->use_closure = 1;
+    c->interior_closure = VPHYS_INTERIOR_PP81;
+    c->pp81_nu0 = 1.0e-2;
+    c->pp81_nu_bg = 1.0e-4;
+    c->pp81_kappa_bg = 1.0e-5;
+    c->pp81_alpha = 5.0;
+    c->rho0 = 1035.0;
+    c->shear2_floor = 1.0e-10;
+    c->ri_crit = 0.3;
+    c->cs_nonlocal = 6.3;
+    c->c_vt2 = 1.8;
+    c->alpha_T = 1.7e-4;
+    c->beta_S = 7.6e-4;
+    c->cp = 3992.0;
+    c->hmix_fixed = 20.0;
+    c->conv_kd = 1.0;
+    c->conv_prandtl = 1.0;
+    c->kv_bg = 1.0e-4;
+    c->kt_bg = 1.0e-5;
+    c->ks_bg = 1.0e-5;
+    c->kv_max = 1.7976931348623157e308;
+    c->kd_max = 1.7976931348623157e308;
+    c->bkgnd_kd_sfc = 1.0e-5;
+    c->bkgnd_kd_deep = 1.3e-4;
+    c->bkgnd_z0 = 2500.0;
+    c->bkgnd_delta = 222.0;
+    c->bkgnd_prandtl = -1.0;
+    c->hvel_mom6 = 1;
+    c->hvel_upwind = 1;
+    c->hbbl_visc = 10.0;
+    c->bbl_piston = 3.0e-4;
+    c->kv_bbl_bg = 1.0e-4;
+    c->idx_temperature = 1;
+    c->idx_salinity = 0;
+    c->idx_pseudo_salt = -1;
+    return VPHYS_OK;
+}
+
+int vphys_create(int nx, int ny, int nz, int ntracer, const vphys_config *cfg, vphys_handle *out)
+{
+    if (!out) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_create: NULL out");
+    *out = nullptr;
+    if (nx < 1 || ny < 1 || nz < 1) return push_error(VPHYS_ERR_BAD_SHAPE, "vphys_create: bad shape %d x %d x %d", nx, ny, nz);
+    if (nz > VPHYS_NZ_MAX) return push_error(VPHYS_ERR_TOO_DEEP, "vphys_create: nz=%d > VPHYS_NZ_MAX=%d", nz, VPHYS_NZ_MAX);
+    if (ntracer < 0 || ntracer > vphys::NTR_MAX)
+        return push_error(VPHYS_ERR_BAD_SHAPE, "vphys_create: ntracer=%d outside [0, %d]", ntracer, vphys::NTR_MAX);
+    vphys_config c;
+    if (cfg)
+        c = *cfg;
+    else
+        vphys_config_default(&c);
+    int st = validate(&c, ntracer);
+    if (st) return st;
+    vphys_handle h = new vphys_handle_s();
+    h->nx = nx;
+    h->ny = ny;
+    h->nz = nz;
+    h->ntr = ntracer;
+    h->cfg = c;
+    h->f.resize(NFIXED + ntracer);
+    for (int id = 0; id < NFIXED; ++id) h->f[id].n = field_count(nx, ny, nz, id, &h->f[id].is_int);
+    for (int t = 0; t < ntracer; ++t) h->f[NFIXED + t].n = (size_t)nx * ny * nz;
+    cudaError_t e = cudaMalloc(&h->guard_dev, sizeof(unsigned long long));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        delete h;
+        return push_error(VPHYS_ERR_ALLOC, "vphys_create: cudaMalloc failed (%s)", cudaGetErrorString(e));
+    }
+    cudaMemset(h->guard_dev, 0, sizeof(unsigned long long));
+    const int core[] = {VPHYS_FIELD_H,        VPHYS_FIELD_RHO,        VPHYS_FIELD_U,      VPHYS_FIELD_V,
+                        VPHYS_FIELD_KV,       VPHYS_FIELD_KT,         VPHYS_FIELD_KS,     VPHYS_FIELD_BL_DEPTH,
+                        VPHYS_FIELD_B0,       VPHYS_FIELD_STRESS_MAG, VPHYS_FIELD_Q_HEAT, VPHYS_FIELD_Q_SALT,
+                        VPHYS_FIELD_WET,      VPHYS_FIELD_TAU_X,      VPHYS_FIELD_TAU_Y};
+    for (int id : core) {
+        if ((st = ensure(h, id))) {
+            vphys_destroy(&h);
+            return st;
+        }
+    }
+    for (int t = 0; t < ntracer; ++t) {
+        if ((st = ensure(h, VPHYS_FIELD_TRACER0 + t))) {
+            vphys_destroy(&h);
+            return st;
+        }
+    }
+    e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) {
+        st = cuda_status(e, "vphys_create");
+        vphys_destroy(&h);
+        return st;
+    }
+    *out = h;
+    return VPHYS_OK;
+}
+
+int vphys_destroy(vphys_handle *hp)
+{
+    if (!hp || !*hp) return VPHYS_OK;
+    vphys_handle h = *hp;
+    *hp = nullptr;
+    if (!valid(h)) return VPHYS_OK;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    else cudaDeviceSynchronize();
+    for (auto &fl : h->f)
+        if (fl.own) cudaFree(fl.own);
+    if (h->guard_dev) cudaFree(h->guard_dev);
+    if (h->smooth_scratch) cudaFree(h->smooth_scratch);
+    h->magic = 0;
+    delete h;
+    return VPHYS_OK;
+}
+
+int vphys_set_config(vphys_handle h, const vphys_config *cfg)
+{
+    if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_set_config: bad handle");
+    if (!cfg) return push_error(VPHYS_ERR_CONFIG, "vphys_set_config: NULL");
+    int st = validate(cfg, h->ntr);
+    if (st) return st;
+    h->cfg = *cfg;
+    return VPHYS_OK;
+}
+
+int vphys_get_config(vphys_handle h, vphys_config *cfg)
+{
+    if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_get_config: bad handle");
+    if (!cfg) return push_error(VPHYS_ERR_CONFIG, "vphys_get_config: NULL");
+    *cfg = h->cfg;
+    return VPHYS_OK;
+}
+
+int vphys_set_stream(vphys_handle h, void *stream)
+{
+    if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_set_stream: bad handle");
+    h->stream = (cudaStream_t)stream;
+    return VPHYS_OK;
+}
+
+int vphys_bind(vphys_handle h, int field, void *device_ptr)
+{
+    if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_bind: bad handle");
+    int sl = slot_of(h, field);
+    if (sl < 0) return push_error(VPHYS_ERR_NOT_FOUND, "vphys_bind: unknown field id %d", field);
+    h->f[sl].bound = device_ptr;
+    if (!device_ptr && !h->f[sl].own) {
+        // restore a handle-owned buffer only for core fields / tracers
+        if (sl < VPHYS_FIELD_LAMBDA_BOT_U || sl >= NFIXED) return ensure(h, field);
+    }
+    return VPHYS_OK;
+}
+
+int vphys_set_field(vphys_handle h, int field, const void *host, size_t n)
+{
+    if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_set_field: bad handle");
+    int sl = slot_of(h, field);
+    if (sl < 0) return push_error(VPHYS_ERR_NOT_FOUND, "vphys_set_field: unknown field id %d", field);
+    if (n != h->f[sl].n)
+        return push_error(VPHYS_ERR_BAD_SHAPE, "vphys_set_field: field %d holds %zu elements, got %zu", field, h->f[sl].n, n);
+    if (!host) return push_error(VPHYS_ERR_BAD_SHAPE, "vphys_set_field: NULL host buffer");
+    int st = ensure(h, field);
+    if (st) return st;
+    cudaError_t e = cudaMemcpyAsync(h->f[sl].ptr(), host, h->f[sl].bytes(), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    return cuda_status(e, "vphys_set_field");
+}
+
+int vphys_get_field(vphys_handle h, int field, void *host, size_t n)
+{
+    if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_get_field: bad handle");
+    int sl = slot_of(h, field);
+    if (sl < 0) return push_error(VPHYS_ERR_NOT_FOUND, "vphys_get_field: unknown field id %d", field);
+    if (n != h->f[sl].n)
+        return push_error(VPHYS_ERR_BAD_SHAPE, "vphys_get_field: field %d holds %zu elements, got %zu", field, h->f[sl].n, n);
+    if (!host) return push_error(VPHYS_ERR_BAD_SHAPE, "vphys_get_field: NULL host buffer");
+    int st = ensure(h, field);
+    if (st) return st;
+    cudaError_t e = cudaMemcpyAsync(host, h->f[sl].ptr(), h->f[sl].bytes(), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    return cuda_status(e, "vphys_get_field");
+}
+
+int vphys_get_ptr(vphys_handle h, int field, void **ptr, int *nx, int *ny, int *nz, int *gen)
+{
+    if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_get_ptr: bad handle");
+    int sl = slot_of(h, field);
+    if (sl < 0) return push_error(VPHYS_ERR_NOT_FOUND, "vphys_get_ptr: unknown field id %d", field);
+    int st = ensure(h, field);
+    if (st) return st;
+    if (ptr) *ptr = h->f[sl].ptr();
+    bool is_int;
+    size_t n = field_count(h->nx, h->ny, h->nz, field, &is_int);
+    int X = h->nx, Y = h->ny, Z = 1;
+    if (n == (size_t)(h->nx + 1) * h->ny * h->nz || n == (size_t)(h->nx + 1) * h->ny) X = h->nx + 1;
+    if (n == (size_t)h->nx * (h->ny + 1) * h->nz || n == (size_t)h->nx * (h->ny + 1)) Y = h->ny + 1;
+    if (n == (size_t)X * Y * h->nz) Z = h->nz;
+    if (n == (size_t)X * Y * (h->nz + 1)) Z = h->nz + 1;
+    if (nx) *nx = X;
+    if (ny) *ny = Y;
+    if (nz) *nz = Z;
+    if (gen) *gen = h->gen;
+    return VPHYS_OK;
+}
+
+int vphys_eos_wright(vphys_handle h)
+{
+    if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_eos_wright: bad handle");
+    if (h->cfg.idx_temperature < 0 || h->cfg.idx_salinity < 0)
+        return push_error(VPHYS_ERR_CONFIG, "vphys_eos_wright: needs temperature and salinity tracers");
+    Params p = make_params(h);
+    vphys::launch_eos_wright(p, h->stream);
+    return cuda_status(cudaGetLastError(), "vphys_eos_wright launch");
+}
+
+int vphys_stress_mag(vphys_handle h)
+{
+    if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_stress_mag: bad handle");
+    Params p = make_params(h);
+    vphys::launch_stress_mag(p, h->stream);
+    return cuda_status(cudaGetLastError(), "vphys_stress_mag launch");
+}
+
+int vphys_assemble(vphys_handle h)
+{
+    if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_assemble: bad handle");
+    int st = prepare_assemble(h);
+    if (st) return st;
+    if (h->cfg.vmix_guard) {
+        cudaError_t e = cudaMemsetAsync(h->guard_dev, 0, sizeof(unsigned long long), h->stream);
+        if (e != cudaSuccess) return cuda_status(e, "vphys_assemble guard reset");
+    }
+    Params p = make_params(h);
+    if ((st = run_assemble(h, p))) return st;
+    if (h->cfg.vmix_guard) {
+        int gs = VPHYS_OK;
+        if ((st = read_guard(h, &gs))) return st;
+        return gs;
+    }
+    return VPHYS_OK;
+}
+
+int vphys_vdiff_momentum(vphys_handle h, double dt)
+{
+    if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_vdiff_momentum: bad handle");
+    int st = prepare_momentum(h);
+    if (st) return st;
+    Params p = make_params(h);
+    vphys::launch_momentum(p, dt, h->stream);
+    return cuda_status(cudaGetLastError(), "vphys_vdiff_momentum launch");
+}
+
+int vphys_vdiff_tracers(vphys_handle h, double dt)
+{
+    if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_vdiff_tracers: bad handle");
+    int st = prepare_tracers(h);
+    if (st) return st;
+    if (h->ntr == 0) return VPHYS_OK;
+    Params p = make_params(h);
+    vphys::launch_tracers(p, dt, true, false, h->stream);
+    return cuda_status(cudaGetLastError(), "vphys_vdiff_tracers launch");
+}
+
+int vphys_nonlocal(vphys_handle h, double dt)
+{
+    if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_nonlocal: bad handle");
+    if (h->ntr == 0 || !h->cfg.use_kpp) return VPHYS_OK;
+    Params p = make_params(h);
+    vphys::launch_tracers(p, dt, false, true, h->stream);
+    return cuda_status(cudaGetLastError(), "vphys_nonlocal launch");
+}
+
+int vphys_step(vphys_handle h, double dt, int n_steps)
+{
+    if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_step: bad handle");
+    if (n_steps <= 0) return VPHYS_OK;
+    int st;
+    if ((st = prepare_assemble(h)) || (st = prepare_momentum(h)) || (st = prepare_tracers(h))) return st;
+    if (h->cfg.eos_in_step && (h->cfg.idx_temperature < 0 || h->cfg.idx_salinity < 0))
+        return push_error(VPHYS_ERR_CONFIG, "vphys_step: eos_in_step needs temperature and salinity tracers");
+    if (h->cfg.vmix_guard) {
+        cudaError_t e = cudaMemsetAsync(h->guard_dev, 0, sizeof(unsigned long long), h->stream);
+        if (e != cudaSuccess) return cuda_status(e, "vphys_step guard reset");
+    }
+    Params p = make_params(h);
+    for (int n = 0; n < n_steps; ++n) {
+        if (h->cfg.eos_in_step) vphys::launch_eos_wright(p, h->stream);
+        if ((st = run_assemble(h, p))) return st;
+        vphys::launch_momentum(p, dt, h->stream);
+        if (h->ntr > 0) vphys::launch_tracers(p, dt, true, h->cfg.use_kpp != 0, h->stream);
+        h->gen += 1;
+    }
+    if ((st = cuda_status(cudaGetLastError(), "vphys_step launch"))) return st;
+    if (h->cfg.vmix_guard) {
+        int gs = VPHYS_OK;
+        if ((st = read_guard(h, &gs))) return st;
+        return gs;
+    }
+    return VPHYS_OK;
+}
+
+int vphys_synchronize(vphys_handle h)
+{
+    if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_synchronize: bad handle");
+    return cuda_status(cudaStreamSynchronize(h->stream), "vphys_synchronize");
+}
+
+}  // extern "C"

@@ -1,0 +1,46 @@
+// vphys_kernels.cuh -- launch parameters shared by the host runtime and the
+// kernels of libvphys.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include "../../include/vphys.h"
+
+namespace vphys {
+
+constexpr int NZ_MAX = VPHYS_NZ_MAX + 1;   // per-column local arrays (>= nz + 1)
+constexpr int NTR_MAX = 16;                // tracers a handle may carry
+
+// Everything a kernel needs: the grid, the knobs and the device pointers.
+struct Params {
+    int nx, ny, nz, ntr;
+    size_t plane;        // nx*ny: stride between levels of cell/interface arrays
+    size_t plane_u;      // (nx+1)*ny
+    size_t plane_v;      // nx*(ny+1)
+    vphys_config cfg;
+    // state
+    const double *h;
+    double *rho, *u, *v, *kv, *kt, *ks;
+    double *bl_depth, *b0;
+    const double *stress_mag, *q_heat, *q_salt, *wet;
+    const double *tau_x, *tau_y, *lambda_bot_u, *lambda_bot_v;
+    double *visc_rem_u, *visc_rem_v;
+    double *gamma_t, *gamma_s;       // nullptr: not written
+    double *heat_budget, *salt_budget;
+    const int *k_top_u, *k_top_v, *k_bot_u, *k_bot_v;   // nullptr: nz / 1
+    double *tr[NTR_MAX];
+    unsigned long long *guard_count;  // vmix_guard counter (device)
+    int ks_equals_kt;                 // ks is bitwise kt after the gate
+    int write_gamma;
+};
+
+// Launchers (vphys_kernels.cu); all asynchronous on `stream`.
+void launch_eos_wright(const Params &p, cudaStream_t stream);
+void launch_stress_mag(const Params &p, cudaStream_t stream);
+void launch_assemble(const Params &p, cudaStream_t stream);
+void launch_smooth(const Params &p, double *fld, double *scratch, cudaStream_t stream);
+void launch_momentum(const Params &p, double dt, cudaStream_t stream);
+void launch_tracers(const Params &p, double dt, bool diffuse, bool nonlocal, cudaStream_t stream);
+
+}  // namespace vphys

@@ -1,0 +1,29 @@
+"""The oracle's port of rdb_sm_cbrt / rdb_sm_atan against the reference's
+golden bit patterns (tests/test_safe_math_golden.inc, transcribed into
+tests/golden/safe_math_golden.json)."""
+import json
+import struct
+from pathlib import Path
+
+import pytest
+
+GOLD = json.loads((Path(__file__).parent / "golden" / "safe_math_golden.json").read_text())
+
+
+def h2d(s):
+    return struct.unpack(">d", bytes.fromhex(s))[0]
+
+
+def d2h(x):
+    return struct.pack(">d", x).hex().upper()
+
+
+@pytest.mark.parametrize("fn", ["cbrt", "atan"])
+def test_golden_bits(oracle, fn):
+    f = oracle.sm_cbrt if fn == "cbrt" else oracle.sm_atan
+    bad = []
+    for arg, res in GOLD[fn]:
+        got = d2h(f(h2d(arg)))
+        if got != res:
+            bad.append((arg, res, got))
+    assert not bad, f"{len(bad)} of {len(GOLD[fn])} {fn} rows differ: {bad[:4]}"
