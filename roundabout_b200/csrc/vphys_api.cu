@@ -389,6 +389,7 @@ int vphys_create(int nx, int ny, int nz, int ntracer, const vphys_config *cfg, v
     if (!out) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_create: NULL out");
     *out = nullptr;
     if (nx < 1 || ny < 1 || nz < 1) return push_error(VPHYS_ERR_BAD_SHAPE, "vphys_create: bad shape %d x %d x %d", nx, ny, nz);
+    if (ny > 65534) return push_error(VPHYS_ERR_BAD_SHAPE, "vphys_create: ny=%d > 65534 (grid y limit)", ny);
     if (nz > VPHYS_NZ_MAX) return push_error(VPHYS_ERR_TOO_DEEP, "vphys_create: nz=%d > VPHYS_NZ_MAX=%d", nz, VPHYS_NZ_MAX);
     if (ntracer < 0 || ntracer > vphys::NTR_MAX)
         return push_error(VPHYS_ERR_BAD_SHAPE, "vphys_create: ntracer=%d outside [0, %d]", ntracer, vphys::NTR_MAX);

@@ -451,8 +451,10 @@ __device__ __forceinline__ void solve_face(const Params &p, double dt, int i, in
     const double *__restrict__ kvr = p.kv + cr;
     const int *ktp = XF ? p.k_top_u : p.k_top_v;
     const int *kbp = XF ? p.k_bot_u : p.k_bot_v;
-    const int kb = kbp ? kbp[f] : 1;
-    const int ktop = ktp ? ktp[f] : nz;
+    // caller-supplied static indices, clamped into the column so that a bad
+    // value can never index outside it (valid input: a no-op)
+    const int kb = kbp ? min(max(kbp[f], 1), nz) : 1;
+    const int ktop = ktp ? min(max(ktp[f], 1), nz) : nz;
     double kv_bbl = 0.0, bbl_thick = c.hbbl_visc;
     if (c.bbl_glue) {
         kv_bbl = c.bbl_piston * c.hbbl_visc;
