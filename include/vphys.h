@@ -278,6 +278,14 @@ int vphys_last_error(int idx, char *buf, int cap);
 /* Library version string (static storage). */
 const char *vphys_version(void);
 
+/* Device self-test of the exact division used by the kernels (a zero-guarded
+ * quotient and a shared-reciprocal quotient with Markstein's correction):
+ * compares both with the IEEE quotient a/b on n_pairs seeded operand pairs,
+ * exponents in [emin, emin+erange), and writes the number of differing bits
+ * patterns to *mismatches (0 expected).  Synchronous. */
+int vphys_selftest_division(long long n_pairs, unsigned long long seed, int emin, int erange,
+                            unsigned long long *mismatches);
+
 /* sizeof(vphys_config) as compiled into the library, so a binding in another
  * language can verify its mirror of the struct before passing one. */
 size_t vphys_config_sizeof(void);

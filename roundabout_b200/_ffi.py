@@ -173,6 +173,8 @@ _PROTOTYPES = {
     "vphys_last_error": (ctypes.c_int, [ctypes.c_int, ctypes.c_char_p, ctypes.c_int]),
     "vphys_version": (ctypes.c_char_p, []),
     "vphys_config_sizeof": (ctypes.c_size_t, []),
+    "vphys_selftest_division": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_ulonglong, ctypes.c_int, ctypes.c_int,
+                                                ctypes.POINTER(ctypes.c_ulonglong)]),
 }
 
 EXPORTED_SYMBOLS = tuple(_PROTOTYPES)

@@ -72,6 +72,7 @@ struct vphys_handle_s {
     std::vector<Field> f;             // NFIXED fixed fields, then ntr tracers
     unsigned long long *guard_dev = nullptr;
     double *smooth_scratch = nullptr;
+    double *budget_scratch = nullptr;
 };
 
 namespace {
@@ -253,6 +254,7 @@ Params make_params(vphys_handle h)
     p.k_bot_v = I(VPHYS_FIELD_K_BOT_V);
     for (int t = 0; t < h->ntr && t < vphys::NTR_MAX; ++t) p.tr[t] = (double *)h->f[NFIXED + t].ptr();
     p.guard_count = h->guard_dev;
+    p.budget_scratch = h->budget_scratch;
     p.ks_equals_kt = (h->cfg.bkgnd_profile || h->cfg.kt_bg == h->cfg.ks_bg) ? 1 : 0;
     p.write_gamma = (p.gamma_t && p.gamma_s) ? 1 : 0;
     return p;
@@ -279,6 +281,15 @@ int prepare_tracers(vphys_handle h)
     if (h->cfg.budgets) {
         if ((st = ensure(h, VPHYS_FIELD_HEAT_BUDGET))) return st;
         if ((st = ensure(h, VPHYS_FIELD_SALT_BUDGET))) return st;
+        if (!h->budget_scratch) {
+            size_t n = 2 * (size_t)h->nx * h->ny * h->nz;
+            cudaError_t e = cudaMalloc(&h->budget_scratch, n * sizeof(double));
+            if (e != cudaSuccess) {
+                h->budget_scratch = nullptr;
+                cudaGetLastError();
+                return push_error(VPHYS_ERR_ALLOC, "cudaMalloc of the budget scratch failed");
+            }
+        }
     }
     return st;
 }
@@ -330,6 +341,26 @@ extern "C" {
 const char *vphys_version(void) { return "vphys 0.1 (sm_100a, FP64)"; }
 
 size_t vphys_config_sizeof(void) { return sizeof(vphys_config); }
+
+int vphys_selftest_division(long long n_pairs, unsigned long long seed, int emin, int erange,
+                            unsigned long long *mismatches)
+{
+    if (!mismatches || n_pairs < 0 || erange < 1 || emin < -1000 || emin + erange > 1000)
+        return push_error(VPHYS_ERR_CONFIG, "vphys_selftest_division: bad arguments");
+    unsigned long long *bad = nullptr;
+    cudaError_t e = cudaMalloc(&bad, sizeof(unsigned long long));
+    if (e != cudaSuccess) return cuda_status(e, "vphys_selftest_division");
+    const long long threads = 148LL * 4 * 256;
+    const long long per = (n_pairs + threads - 1) / threads;
+    e = cudaMemset(bad, 0, sizeof(unsigned long long));
+    if (e == cudaSuccess) {
+        vphys::launch_selftest_division(seed, per, emin, erange, bad, nullptr);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(mismatches, bad, sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+    cudaFree(bad);
+    return cuda_status(e, "vphys_selftest_division");
+}
 
 int vphys_last_error(int idx, char *buf, int cap)
 {
@@ -454,6 +485,7 @@ int vphys_destroy(vphys_handle *hp)
         if (fl.own) cudaFree(fl.own);
     if (h->guard_dev) cudaFree(h->guard_dev);
     if (h->smooth_scratch) cudaFree(h->smooth_scratch);
+    if (h->budget_scratch) cudaFree(h->budget_scratch);
     h->magic = 0;
     delete h;
     return VPHYS_OK;

@@ -18,6 +18,53 @@ constexpr double EPS_HVEL = 1.0e-30;       // rdb_ocean_vdiff.F90 diffuse_veloci
 constexpr double STRESS_H_MIN = 1.0e-3;
 constexpr double DBL_TINY = 2.2250738585072014e-308;
 
+// ---- exact division helpers ----------------------------------------------
+// xdiv(a, b) == a / b for every input.  A zero numerator is answered directly
+// (the quotient is a zero carrying the XOR of the signs): the general IEEE
+// division takes a slow path of ~90 instructions for a zero operand, and the
+// path divides zeros all the time (a non-local source that is zero below the
+// boundary layer, an ideal-age tracer that starts at zero, the harmonic mean
+// of two vanished layers).
+__device__ __forceinline__ double xdiv(double a, double b)
+{
+    if (a == 0.0 && b != 0.0 && isfinite(b))
+        return ((__double_as_longlong(a) ^ __double_as_longlong(b)) < 0) ? -0.0 : 0.0;
+    return a / b;
+}
+
+// Division of several numerators by one denominator with a single correctly
+// rounded reciprocal y = RN(1/b) and Markstein's correction (P. Markstein,
+// "Computation of elementary functions on the IBM RISC System/6000
+// processor", IBM J. Res. Dev. 34(1), 1990): q0 = RN(a*y), r = a - b*q0
+// (exact with an FMA), q = RN(q0 + r*y) is RN(a/b) when y is within half an
+// ulp of 1/b, q0 within one ulp of a/b and nothing over- or underflows.  The
+// operands are kept inside [2^-500, 2^500] for that; anything else (zeros,
+// extremes, NaN, Inf) takes xdiv.  tests/test_gpu_division.py checks the
+// result against a/b bit for bit.
+struct Rcp {
+    double b, y;
+    bool fast;
+};
+__device__ __forceinline__ Rcp rcp_of(double b)
+{
+    Rcp r;
+    r.b = b;
+    r.y = 1.0 / b;
+    const double ab = fabs(b);
+    r.fast = ab >= 0x1p-500 && ab <= 0x1p500;
+    return r;
+}
+__device__ __forceinline__ double qdiv(double a, const Rcp &r)
+{
+    const double aa = fabs(a);
+    if (r.fast && aa >= 0x1p-500 && aa <= 0x1p500) {
+        const double q0 = __dmul_rn(a, r.y);
+        const double rem = __fma_rn(-r.b, q0, a);
+        return __fma_rn(rem, r.y, q0);
+    }
+    return xdiv(a, r.b);
+}
+
 // Fortran MAX/MIN (finite operands); the same ternary as the CPU restatement.
 __device__ __forceinline__ double fmx(double a, double b) { return a > b ? a : b; }
 __device__ __forceinline__ double fmn(double a, double b) { return a < b ? a : b; }
@@ -43,7 +90,7 @@ __device__ __forceinline__ double sm_cbrt(double x)
 #pragma unroll
     for (int it = 0; it < 2; ++it) {
         double y3 = (y0 * y0) * y0;
-        y0 = y0 + y0 * ((m - y3) / ((y3 + y3) + m));
+        y0 = y0 + y0 * xdiv(m - y3, (y3 + y3) + m);
     }
     double y = ldexp(y0, q);
     return x < 0.0 ? -y : y;
@@ -59,7 +106,7 @@ __device__ __forceinline__ double sm_atan(double x)
     bool inv = ax > 1.0;
     double t = inv ? 1.0 / ax : ax;
     bool mid = t > 0.2679491924311226958;
-    double a = mid ? (1.7320508075688771932 * t - 1.0) / (1.7320508075688771932 + t) : t;
+    double a = mid ? xdiv(1.7320508075688771932 * t - 1.0, 1.7320508075688771932 + t) : t;
     double u = a * a;
     double p = -0.0295457862073798469;
     p = p * u + 0.04518284953605152671;
@@ -86,7 +133,7 @@ __device__ __forceinline__ double face_thick(double ha, double hb, bool use_harm
 {
     if (use_harmonic) {
         double sum_h = ha + hb;
-        if (sum_h > 1.0e-30) return 2.0 * ha * hb / sum_h;
+        if (sum_h > 1.0e-30) return xdiv(2.0 * ha * hb, sum_h);
         return 0.5 * sum_h;
     }
     return 0.5 * (ha + hb);
@@ -95,13 +142,40 @@ __device__ __forceinline__ double face_thick(double ha, double hb, bool use_harm
 // rdb_conc_add_source (rdb_tracer_conc.inc:36-53)
 __device__ __forceinline__ double conc_add_source(double c, double h, double src)
 {
-    return (h > H_VANISHED) ? c + src / (h + H_DIV_EPS) : c;
+    return (h > H_VANISHED) ? c + xdiv(src, h + H_DIV_EPS) : c;
 }
 
 // nonlocal_face_flux (rdb_ocean_vmix.F90:1694-1714)
 __device__ __forceinline__ double nonlocal_face_flux(double gamma, double h_below, double h_above)
 {
     return (h_below > H_VANISHED && h_above > H_VANISHED) ? gamma : 0.0;
+}
+
+// ---- L2 residency hints (PTX createpolicy + cache_hint) ----
+// Intermediates that a thread writes and reads back later in the same kernel
+// (in-place Thomas sweeps) are stored evict_last so the round trip stays in
+// the 126 MB L2; data read once are loaded evict_first.
+__device__ __forceinline__ unsigned long long l2_policy_evict_last()
+{
+    unsigned long long p;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ unsigned long long l2_policy_evict_first()
+{
+    unsigned long long p;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ double ld_hint(const double *ptr, unsigned long long pol)
+{
+    double v;
+    asm volatile("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(ptr), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ void st_hint(double *ptr, double v, unsigned long long pol)
+{
+    asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(ptr), "d"(v), "l"(pol) : "memory");
 }
 
 }  // namespace vphys

@@ -17,11 +17,7 @@
 //   k_smooth_*     optional 1-2-1 horizontal smoothing  rdb_ocean_vmix.F90:2699-2748
 //   k_momentum     u and v face columns: face thickness, coupling, fused
 //                  Thomas sweep, optional remnant      rdb_ocean_vdiff.F90:1416-2115
-//   k_tracers<N>   tracer build + factorisation once per diffusivity, forward
-//                  sweep of all N tracers, back-substitution, budgets, and
-//                  the KPP non-local tendency fused into the store
-//                                                     rdb_ocean_vdiff.F90:1107-1414,
-//                                                     rdb_ocean_vmix.F90:1605-1714
+//   (the tracer kernel lives in vphys_tracers.cu)
 #include <cuda_runtime.h>
 
 #include "vphys_device.cuh"
@@ -114,9 +110,9 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
     if (c.use_kpp) {
         // ---- KPP pass 1 (rdb_ocean_vmix.F90:1288-1426) ----
         const double tau_mag = p.stress_mag[col];
-        const double u_star = sqrt(tau_mag / rho0);
-        q_T_kin = p.q_heat[col] / (rho0 * c.cp);
-        q_S_kin = p.q_salt[col] / rho0;
+        const double u_star = sqrt(xdiv(tau_mag, rho0));
+        q_T_kin = xdiv(p.q_heat[col], rho0 * c.cp);
+        q_S_kin = xdiv(p.q_salt[col], rho0);
         const double B_0 = (GRAVITY / rho0) * (c.alpha_T * q_T_kin - c.beta_S * q_S_kin);
         {
             const double wstar3_lagged = fmx(0.0, -B_0) * h_b;
@@ -140,16 +136,16 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
                 const double b_k = -(GRAVITY * RR(k) / rho0);
                 const double delta_d = d_centre_k - d_centre_ref;
                 const double delta_b = b_ref - b_k;
-                const double n_brunt = sqrt(fmx(0.0, delta_b / delta_d));
+                const double n_brunt = sqrt(fmx(0.0, xdiv(delta_b, delta_d)));
                 const double vt2 = vt2_coef * d_centre_k * n_brunt * w_s_col;
                 const double shear2 =
                     fmx((u_k - u_ref) * (u_k - u_ref) + (v_k - v_ref) * (v_k - v_ref) + vt2, c.shear2_floor);
-                const double ri_bulk = delta_b * delta_d / shear2;
+                const double ri_bulk = xdiv(delta_b * delta_d, shear2);
                 if (ri_bulk >= c.ri_crit) {
                     const double denom = ri_bulk - ri_prev;
                     double frac;
                     if (fabs(denom) > 1.0e-12)
-                        frac = (c.ri_crit - ri_prev) / denom;
+                        frac = xdiv(c.ri_crit - ri_prev, denom);
                     else
                         frac = 0.5;
                     hb_new = d_prev + frac * (d_centre_k - d_prev);
@@ -209,7 +205,7 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
             r_m = RR(q - 1);
             if (c.bkgnd_profile)
                 kdb = c.bkgnd_kd_sfc +
-                      (c.bkgnd_kd_deep - c.bkgnd_kd_sfc) * (0.5 + sm_atan((depth - c.bkgnd_z0) / c.bkgnd_delta) * inv_pi);
+                      (c.bkgnd_kd_deep - c.bkgnd_kd_sfc) * (0.5 + sm_atan(xdiv(depth - c.bkgnd_z0, c.bkgnd_delta)) * inv_pi);
             if (pp81) {
                 // ---- PP81 (rdb_ocean_vmix.F90:1046-1073) ----
                 uc_m = UC(q - 1);
@@ -219,11 +215,12 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
                     kvq = c.pp81_nu_bg;
                     ktq = c.pp81_kappa_bg;
                 } else {
-                    const double du_dz = (uc_c - uc_m) / dz_face;
-                    const double dv_dz = (vc_c - vc_m) / dz_face;
+                    const Rcp rdz = rcp_of(dz_face);
+                    const double du_dz = qdiv(uc_c - uc_m, rdz);
+                    const double dv_dz = qdiv(vc_c - vc_m, rdz);
                     const double shear2 = fmx(du_dz * du_dz + dv_dz * dv_dz, c.shear2_floor);
-                    const double n2 = -(GRAVITY * (r_c - r_m) / (rho0 * dz_face));
-                    const double ri = n2 / shear2;
+                    const double n2 = -xdiv(GRAVITY * (r_c - r_m), rho0 * dz_face);
+                    const double ri = xdiv(n2, shear2);
                     const double denom = 1.0 + c.pp81_alpha * fmx(ri, 0.0);
                     const double ri_factor = 1.0 / (denom * denom);
                     kvq = c.pp81_nu_bg + c.pp81_nu0 * ri_factor;
@@ -241,7 +238,7 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
         // ---- KPP overlay (rdb_ocean_vmix.F90:1496-1514) ----
         double gt = 0.0, gs = 0.0;
         if (kpp_active && q > 1 && q <= k_sfc && d_run < h_b) {
-            const double sigma = d_run / h_b;
+            const double sigma = xdiv(d_run, h_b);
             const double g_shape = sigma * (1.0 - sigma) * (1.0 - sigma);
             const double kv_kpp = h_b * w_s * g_shape;
             kvq = fmx(kvq, kv_kpp);
@@ -266,7 +263,7 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
             if (c.conv_enable) {
                 const double dz_face = 0.5 * (h_m + h_c);
                 if (!(dz_face <= H_VANISHED) && !(depth < h_b)) {
-                    const double n2 = -(GRAVITY * (r_c - r_m) / (rho0 * dz_face));
+                    const double n2 = -xdiv(GRAVITY * (r_c - r_m), rho0 * dz_face);
                     if (n2 < c.conv_n2_thresh) {
                         ktq = fmx(ktq, c.conv_kd);
                         kvq = fmx(kvq, c.conv_prandtl * c.conv_kd);
@@ -365,7 +362,7 @@ __device__ __forceinline__ void face_layer(const vphys_config &c, double hl_c, d
     // vdiff_face_layer (rdb_ocean_vdiff.F90:1964-2056)
     zint = 0.0;
     if (c.hvel_mom6 && !c.hvel_harmonic) {
-        const double h_harm = 2.0 * hl_c * hr_c / (hl_c + hr_c + EPS_HVEL);
+        const double h_harm = xdiv(2.0 * hl_c * hr_c, hl_c + hr_c + EPS_HVEL);
         const double h_arith = 0.5 * (hl_c + hr_c);
         const double h_delta = hr_c - hl_c;
         zcol_l = zcol_l + hl_c;
@@ -380,7 +377,7 @@ __device__ __forceinline__ void face_layer(const vphys_config &c, double hl_c, d
             hvel = (1.0 - botfn) * h_arith + botfn * h_harm;
         }
     } else if (c.hvel_mom6) {
-        const double h_harm = 2.0 * hl_c * hr_c / (hl_c + hr_c + EPS_HVEL);
+        const double h_harm = xdiv(2.0 * hl_c * hr_c, hl_c + hr_c + EPS_HVEL);
         const double h_arith = 0.5 * (hl_c + hr_c);
         const double h_delta = hr_c - hl_c;
         hvel = h_harm;
@@ -419,10 +416,15 @@ __device__ __forceinline__ void interface_coupling(const vphys_config &c, double
     cut = c.zlevel_faces && (hv_lo <= H_VANISHED || hv_hi <= H_VANISHED);
 }
 
+constexpr int MOM_U = 4;   // levels per load block
+
+// diffuse_velocity_columns_impl for one face column (rdb_ocean_vdiff.F90:1611-1925).
+// The Thomas c' of every level sits in shared memory (cpp[(k-1)*bs]); the
+// forward-swept d' is written in place over u with an L2 evict_last hint and
+// read back by the back-substitution.
 template <bool XF>
-__device__ __forceinline__ void solve_face(const Params &p, double dt, int i, int j, double *cdiag, double *rhs)
+__device__ __forceinline__ void solve_face(const Params &p, double dt, int i, int j, double *cpp, int bs)
 {
-    // diffuse_velocity_columns_impl, one face column (rdb_ocean_vdiff.F90:1611-1925)
     const vphys_config &c = p.cfg;
     const int nx = p.nx, ny = p.ny, nz = p.nz;
     const int nu = XF ? nx + 1 : nx;
@@ -431,6 +433,7 @@ __device__ __forceinline__ void solve_face(const Params &p, double dt, int i, in
     const size_t f = (size_t)i + (size_t)nu * j;
     double *__restrict__ uf = (XF ? p.u : p.v) + f;
     double *__restrict__ vrem = c.remnant ? ((XF ? p.visc_rem_u : p.visc_rem_v) + f) : nullptr;
+    const unsigned long long pol_keep = l2_policy_evict_last();
     int il, ir, jb, ja;
     if (XF) {
         il = i - 1 > 0 ? i - 1 : 0;
@@ -478,317 +481,186 @@ __device__ __forceinline__ void solve_face(const Params &p, double dt, int i, in
             }
         }
     }
-    double hv_0, hv_p, zi_0, zi_p;
-    double u_next_in = uf[0];
-    face_layer(c, __ldg(hl), __ldg(hr), u_next_in, 1, kb, d_min, i_hbbl, zacc, zcol_l, zcol_r, hv_p, zi_p);
+    double hv_p, zi_p;
+    double u_k = uf[0];
+    face_layer(c, __ldg(hl), __ldg(hr), u_k, 1, kb, d_min, i_hbbl, zacc, zcol_l, zcol_r, hv_p, zi_p);
     double num_t = 0.0, dz_t = 1.0;
     bool cut_t = false;
     double cp_prev = 0.0, dp_prev = 0.0, gp_prev = 0.0;
     const double lam = (c.implicit_drag && !c.bbl_glue) ? (XF ? p.lambda_bot_u : p.lambda_bot_v)[f] : 0.0;
-    double stress_rhs = 0.0;
     const double inv_rho0 = 1.0 / c.rho0;
-    double u_k = u_next_in;
-    for (int k = 1; k <= nz; ++k) {
-        hv_0 = hv_p;
-        zi_0 = zi_p;
-        const double num_b = num_t, dz_b = dz_t;
-        const bool cut_b = cut_t;
-        double u_kp1 = 0.0;
-        if (k < nz) {
-            u_kp1 = uf[PF * (size_t)k];
-            face_layer(c, __ldg(hl + P * (size_t)k), __ldg(hr + P * (size_t)k), u_kp1, k + 1, kb, d_min, i_hbbl,
-                       zacc, zcol_l, zcol_r, hv_p, zi_p);
-            if (k >= kb_live && k <= ktop) {
-                interface_coupling(c, hv_0, hv_p, zi_0, dt, kv_bbl, bbl_thick, __ldg(kvl + P * (size_t)k),
-                                   __ldg(kvr + P * (size_t)k), num_t, dz_t, cut_t);
+    for (int k0 = 1; k0 <= nz; k0 += MOM_U) {
+        double hln[MOM_U], hrn[MOM_U], un[MOM_U], kvln[MOM_U], kvrn[MOM_U];
+#pragma unroll
+        for (int q = 0; q < MOM_U; ++q) {
+            const int k = k0 + q;
+            if (k < nz) {
+                const size_t o = P * (size_t)k;
+                hln[q] = __ldg(hl + o);
+                hrn[q] = __ldg(hr + o);
+                kvln[q] = __ldg(kvl + o);
+                kvrn[q] = __ldg(kvr + o);
+                un[q] = uf[PF * (size_t)k];
             }
         }
-        double a_k = 0.0, b_k = 1.0, c_k = 0.0;
-        const double hf_k = fmx(hv_0, H_VANISHED);
-        if (k == kb_live && k <= ktop) {
-            double alpha = 0.0;
-            if (kb_live < nz) {
-                alpha = num_t / (hf_k * dz_t);
-                if (cut_t) alpha = 0.0;
+#pragma unroll
+        for (int q = 0; q < MOM_U; ++q) {
+            const int k = k0 + q;
+            if (k <= nz) {
+                const double hv_0 = hv_p, zi_0 = zi_p;
+                const double num_b = num_t, dz_b = dz_t;
+                const bool cut_b = cut_t;
+                double u_kp1 = 0.0;
+                if (k < nz) {
+                    u_kp1 = un[q];
+                    face_layer(c, hln[q], hrn[q], u_kp1, k + 1, kb, d_min, i_hbbl, zacc, zcol_l, zcol_r, hv_p, zi_p);
+                    if (k >= kb_live && k <= ktop)
+                        interface_coupling(c, hv_0, hv_p, zi_0, dt, kv_bbl, bbl_thick, kvln[q], kvrn[q], num_t, dz_t,
+                                           cut_t);
+                }
+                double a_k = 0.0, b_k = 1.0, c_k = 0.0;
+                const double hf_k = fmx(hv_0, H_VANISHED);
+                if (k == kb_live && k <= ktop) {
+                    double alpha = 0.0;
+                    if (kb_live < nz) {
+                        alpha = xdiv(num_t, hf_k * dz_t);
+                        if (cut_t) alpha = 0.0;
+                    }
+                    c_k = -alpha;
+                    b_k = 1.0 + alpha;
+                    if (c.bbl_glue) b_k = b_k + dt * kv_bbl / (hf_k * (fmn(0.5 * hv_0, bbl_thick) + EPS_HVEL));
+                    if (c.implicit_drag && !c.bbl_glue) b_k = b_k + dt * lam;
+                }
+                if (k == ktop && k > kb_live) {
+                    double beta = xdiv(num_b, hf_k * dz_b);
+                    if (cut_b) beta = 0.0;
+                    a_k = -beta;
+                    b_k = 1.0 + beta;
+                }
+                if (k > kb_live && k < ktop) {
+                    double beta = xdiv(num_b, hf_k * dz_b);
+                    double alpha = xdiv(num_t, hf_k * dz_t);
+                    if (cut_b) beta = 0.0;
+                    if (cut_t) alpha = 0.0;
+                    a_k = -beta;
+                    c_k = -alpha;
+                    b_k = 1.0 + alpha + beta;
+                }
+                double r_k = u_k;
+                if (k == ktop && c.implicit_stress) {
+                    const double tau = (XF ? p.tau_x : p.tau_y)[f];
+                    const double wmin = fmn(p.wet[cl], p.wet[cr]);
+                    r_k = r_k + xdiv(dt * tau * 1.0 * wmin * inv_rho0, fmx(hf_k, STRESS_H_MIN));
+                }
+                const Rcp denom = rcp_of((k == 1) ? b_k : b_k - a_k * cp_prev);
+                const double cp = qdiv(c_k, denom);
+                const double dp = qdiv((k == 1) ? r_k : r_k - a_k * dp_prev, denom);
+                double gp = 0.0;
+                if (vrem) gp = qdiv((k == 1) ? 1.0 : 1.0 - a_k * gp_prev, denom);
+                cpp[(size_t)(k - 1) * bs] = cp;
+                if (k < nz) {
+                    st_hint(uf + PF * (size_t)(k - 1), dp, pol_keep);
+                    if (vrem) st_hint(vrem + PF * (size_t)(k - 1), gp, pol_keep);
+                }
+                cp_prev = cp;
+                dp_prev = dp;
+                gp_prev = gp;
+                u_k = u_kp1;
             }
-            c_k = -alpha;
-            b_k = 1.0 + alpha;
-            if (c.bbl_glue) b_k = b_k + dt * kv_bbl / (hf_k * (fmn(0.5 * hv_0, bbl_thick) + EPS_HVEL));
-            if (c.implicit_drag && !c.bbl_glue) b_k = b_k + dt * lam;
         }
-        if (k == ktop && k > kb_live) {
-            double beta = num_b / (hf_k * dz_b);
-            if (cut_b) beta = 0.0;
-            a_k = -beta;
-            b_k = 1.0 + beta;
-        }
-        if (k > kb_live && k < ktop) {
-            double beta = num_b / (hf_k * dz_b);
-            double alpha = num_t / (hf_k * dz_t);
-            if (cut_b) beta = 0.0;
-            if (cut_t) alpha = 0.0;
-            a_k = -beta;
-            c_k = -alpha;
-            b_k = 1.0 + alpha + beta;
-        }
-        double r_k = u_k;
-        if (k == ktop && c.implicit_stress) {
-            const double tau = (XF ? p.tau_x : p.tau_y)[f];
-            const double wmin = fmn(p.wet[cl], p.wet[cr]);
-            stress_rhs = dt * tau * 1.0 * wmin * inv_rho0 / fmx(hf_k, STRESS_H_MIN);
-            r_k = r_k + stress_rhs;
-        }
-        double cp, dp, gp;
-        if (k == 1) {
-            cp = c_k / b_k;
-            dp = r_k / b_k;
-            gp = 1.0 / b_k;
-        } else {
-            const double denom = b_k - a_k * cp_prev;
-            cp = c_k / denom;
-            dp = (r_k - a_k * dp_prev) / denom;
-            gp = (1.0 - a_k * gp_prev) / denom;
-        }
-        cdiag[k - 1] = cp;
-        rhs[k - 1] = dp;
-        if (vrem) vrem[PF * (size_t)(k - 1)] = gp;
-        cp_prev = cp;
-        dp_prev = dp;
-        gp_prev = gp;
-        u_k = u_kp1;
     }
+    // back-substitution (momentum into u, remnant into visc_rem)
     double u_next = dp_prev;
     double g_next = fmn(gp_prev, 1.0);
     uf[PF * (size_t)(nz - 1)] = u_next;
     if (vrem) vrem[PF * (size_t)(nz - 1)] = g_next;
-    for (int k = nz - 1; k >= 1; --k) {
-        const double cpk = cdiag[k - 1];
-        u_next = rhs[k - 1] - cpk * u_next;
-        uf[PF * (size_t)(k - 1)] = u_next;
-        if (vrem) {
-            g_next = fmn(vrem[PF * (size_t)(k - 1)] - cpk * g_next, 1.0);
-            vrem[PF * (size_t)(k - 1)] = g_next;
+    for (int k0 = nz - 1; k0 >= 1; k0 -= MOM_U) {
+        double dps[MOM_U], gps[MOM_U];
+#pragma unroll
+        for (int q = 0; q < MOM_U; ++q) {
+            const int k = k0 - q;
+            if (k >= 1) {
+                dps[q] = ld_hint(uf + PF * (size_t)(k - 1), pol_keep);
+                if (vrem) gps[q] = ld_hint(vrem + PF * (size_t)(k - 1), pol_keep);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < MOM_U; ++q) {
+            const int k = k0 - q;
+            if (k >= 1) {
+                const double cpk = cpp[(size_t)(k - 1) * bs];
+                u_next = dps[q] - cpk * u_next;
+                uf[PF * (size_t)(k - 1)] = u_next;
+                if (vrem) {
+                    g_next = fmn(gps[q] - cpk * g_next, 1.0);
+                    vrem[PF * (size_t)(k - 1)] = g_next;
+                }
+            }
         }
     }
 }
 
+// blockIdx.z = 0: u faces (i <= nx, j < ny); 1: v faces (i < nx, j <= ny)
 __global__ void __launch_bounds__(MOM_THREADS) k_momentum(const Params p, double dt)
 {
+    extern __shared__ double smem[];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
-    if (i > p.nx) return;
-    double cdiag[NZ_MAX], rhs[NZ_MAX];
-    if (j < p.ny) solve_face<true>(p, dt, i, j, cdiag, rhs);
-    if (i < p.nx) solve_face<false>(p, dt, i, j, cdiag, rhs);
-}
-
-// ---------------------------------------------------------------------------
-// Tracers: build + factorise once per diffusivity, forward-sweep every
-// tracer, back-substitute, then store with the budget and the KPP non-local
-// tendency (applied after the diffusion, as vmix_apply_in_stage orders them).
-// ---------------------------------------------------------------------------
-constexpr int TR_THREADS = 128;
-
-// Row k (1-based) of the tracer matrix (build_factorize_tracer_matrix,
-// rdb_ocean_vdiff.F90:1285-1341); hm/hc/hp are the raw thicknesses of layers
-// k-1, k, k+1, kb/kt the diffusivity at interfaces k and k+1.
-__device__ __forceinline__ void tracer_row(int k, int nz, bool use_harmonic, double dt, double hm_raw, double hc_raw,
-                                           double hp_raw, double K_k, double K_kp1, double &a, double &b, double &cc)
-{
-    if (k == 1) {
-        const double hc = fmx(hc_raw, H_VANISHED);
-        double alpha = 0.0;
-        if (nz > 1) {
-            const double hp = fmx(hp_raw, H_VANISHED);
-            const double dz_face = face_thick(hc, hp, use_harmonic);
-            alpha = dt * K_kp1 / (hc * dz_face);
-            if (hc_raw <= H_VANISHED || hp_raw <= H_VANISHED) alpha = 0.0;
-        }
-        a = 0.0;
-        cc = -alpha;
-        b = 1.0 + alpha;
-    } else if (k < nz) {
-        const double hm = fmx(hm_raw, H_VANISHED);
-        const double hc = fmx(hc_raw, H_VANISHED);
-        const double hp = fmx(hp_raw, H_VANISHED);
-        double beta = dt * K_k / (hc * face_thick(hm, hc, use_harmonic));
-        double alpha = dt * K_kp1 / (hc * face_thick(hc, hp, use_harmonic));
-        if (hc_raw <= H_VANISHED || hm_raw <= H_VANISHED) beta = 0.0;
-        if (hc_raw <= H_VANISHED || hp_raw <= H_VANISHED) alpha = 0.0;
-        a = -beta;
-        cc = -alpha;
-        b = 1.0 + alpha + beta;
+    double *cpp = smem + threadIdx.x;
+    if (blockIdx.z == 0) {
+        if (i <= p.nx && j < p.ny) solve_face<true>(p, dt, i, j, cpp, blockDim.x);
     } else {
-        const double hm = fmx(hm_raw, H_VANISHED);
-        const double hc = fmx(hc_raw, H_VANISHED);
-        const double dz_face = face_thick(hm, hc, use_harmonic);
-        double beta = dt * K_k / (hc * dz_face);
-        if (hc_raw <= H_VANISHED || hm_raw <= H_VANISHED) beta = 0.0;
-        a = -beta;
-        cc = 0.0;
-        b = 1.0 + beta;
+        if (i < p.nx && j <= p.ny) solve_face<false>(p, dt, i, j, cpp, blockDim.x);
     }
 }
 
-template <int NTR, bool TWO>
-__global__ void __launch_bounds__(TR_THREADS) k_tracers(const Params p, double dt, int diffuse, int nonlocal)
+// ---------------------------------------------------------------------------
+// Self-test of xdiv / qdiv against the IEEE quotient on seeded operands:
+// random mantissas (plus all-ones and power-of-two ones), exponents in
+// [emin, emin + erange), random signs, zeros one time in 16.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long st_mix(unsigned long long z)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y;
-    if (i >= p.nx) return;
-    const vphys_config &c = p.cfg;
-    const int nx = p.nx, nz = p.nz, ntr = p.ntr;
-    const size_t P = p.plane;
-    const size_t col = (size_t)i + (size_t)nx * j;
-    const double *__restrict__ hp = p.h + col;
-    const int iT = c.idx_temperature, iS = c.idx_salinity, iPS = c.idx_pseudo_salt;
-#define HH(k) __ldg(hp + P * (size_t)((k) - 1))
-    double *trc[NTR];
-#pragma unroll
-    for (int t = 0; t < NTR; ++t) trc[t] = (t < ntr) ? p.tr[t] + col : nullptr;
-
-    double r[NTR][NZ_MAX];
-    double cpA[NZ_MAX];
-    double cpB[TWO ? NZ_MAX : 1];
-
-    if (diffuse) {
-        // ---- upward pass: rows, factorisation, forward sweep of every tracer ----
-        const double *__restrict__ KA = p.kt + col;
-        const double *__restrict__ KB = p.ks + col;
-        double h_m = 0.0, h_c = HH(1), h_p = (nz > 1) ? HH(2) : 0.0;
-        double KA_k = __ldg(KA), KA_kp1 = __ldg(KA + P);
-        double KB_k = TWO ? __ldg(KB) : 0.0, KB_kp1 = TWO ? __ldg(KB + P) : 0.0;
-        double cpA_prev = 0.0, cpB_prev = 0.0;
-        for (int k = 1; k <= nz; ++k) {
-            double aA, bA, cA;
-            tracer_row(k, nz, c.use_harmonic, dt, h_m, h_c, h_p, KA_k, KA_kp1, aA, bA, cA);
-            const double denA = (k == 1) ? bA : bA - aA * cpA_prev;
-            cpA_prev = cA / denA;
-            cpA[k - 1] = cpA_prev;
-            double aB = 0.0, denB = 1.0;
-            if (TWO) {
-                double bB, cB;
-                tracer_row(k, nz, c.use_harmonic, dt, h_m, h_c, h_p, KB_k, KB_kp1, aB, bB, cB);
-                denB = (k == 1) ? bB : bB - aB * cpB_prev;
-                cpB_prev = cB / denB;
-                cpB[k - 1] = cpB_prev;
-            }
-#pragma unroll
-            for (int t = 0; t < NTR; ++t) {
-                if (t < ntr) {
-                    const bool useA = !TWO || (t == iT);
-                    const double a = useA ? aA : aB;
-                    const double den = useA ? denA : denB;
-                    const double x = trc[t][P * (size_t)(k - 1)];
-                    r[t][k - 1] = (k == 1) ? x / den : (x - a * r[t][k - 2]) / den;
-                }
-            }
-            h_m = h_c;
-            h_c = h_p;
-            h_p = (k + 2 <= nz) ? HH(k + 2) : 0.0;
-            KA_k = KA_kp1;
-            KA_kp1 = (k + 2 <= nz + 1) ? __ldg(KA + P * (size_t)(k + 1)) : 0.0;
-            if (TWO) {
-                KB_k = KB_kp1;
-                KB_kp1 = (k + 2 <= nz + 1) ? __ldg(KB + P * (size_t)(k + 1)) : 0.0;
-            }
-        }
+    z += 0x9e3779b97f4a7c15ull;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+__device__ __forceinline__ double st_make(unsigned long long r, int emin, int erange)
+{
+    unsigned long long mant = r & 0xFFFFFFFFFFFFFull;
+    const int sel = (int)((r >> 52) & 15);
+    if (sel == 0) mant = 0xFFFFFFFFFFFFFull;
+    if (sel == 1) mant = 0;
+    const int e = emin + (int)((r >> 56) % (unsigned long long)erange);
+    const unsigned long long bits = ((r >> 63) << 63) | ((unsigned long long)(e + 1023) << 52) | mant;
+    if (sel == 2) return ((r >> 63) ? -0.0 : 0.0);
+    return __longlong_as_double((long long)bits);
+}
+__global__ void k_selftest_division(unsigned long long seed, long long per_thread, int emin, int erange,
+                                    unsigned long long *bad)
+{
+    const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    unsigned long long nb = 0;
+    for (long long n = 0; n < per_thread; ++n) {
+        const unsigned long long r1 = st_mix(seed ^ ((unsigned long long)tid * 0x100000001b3ull + (unsigned long long)n * 0x9e37ull));
+        const unsigned long long r2 = st_mix(r1 + 0x632be59bd9b4e019ull);
+        const unsigned long long r3 = st_mix(r2 + 0x2545f4914f6cdd1dull);
+        const double a = st_make(r1, emin, erange), b = st_make(r2, emin, erange), a2 = st_make(r3, emin, erange);
+        if (b == 0.0) continue;
+        const double ref = a / b, ref2 = a2 / b;
+        const Rcp rb = rcp_of(b);
+        const double q = qdiv(a, rb), q2 = qdiv(a2, rb), x = xdiv(a, b);
+        nb += (__double_as_longlong(q) != __double_as_longlong(ref)) + (__double_as_longlong(q2) != __double_as_longlong(ref2)) +
+              (__double_as_longlong(x) != __double_as_longlong(ref));
     }
+    if (nb) atomicAdd(bad, nb);
+}
 
-    // ---- non-local column scalars, recomputed exactly as KPP pass 2 ----
-    bool nl = nonlocal && c.use_kpp;
-    int k_sfc = nz;
-    double h_b = 0.0, q_T_kin = 0.0, q_S_kin = 0.0, cs = c.cs_nonlocal;
-    if (nl) {
-        for (int k = nz; k >= 1; --k) {
-            if (HH(k) > H_VANISHED) {
-                k_sfc = k;
-                break;
-            }
-        }
-        const double rho0 = c.rho0;
-        h_b = p.bl_depth[col];
-        const double u_star = sqrt(p.stress_mag[col] / rho0);
-        q_T_kin = p.q_heat[col] / (rho0 * c.cp);
-        q_S_kin = p.q_salt[col] / rho0;
-        const double B_0 = (GRAVITY / rho0) * (c.alpha_T * q_T_kin - c.beta_S * q_S_kin);
-        const double wstar3 = fmx(0.0, -B_0) * h_b;
-        const double w_star = sm_cbrt(wstar3);
-        const double w_s = sqrt(u_star * u_star + w_star * w_star);
-        nl = (h_b > 0.0 && w_s > 0.0 && B_0 < 0.0);
-    }
-    const bool do_nl = nonlocal && c.use_kpp;
-    double *heat = (c.budgets && diffuse && iT >= 0) ? p.heat_budget + col : nullptr;
-    double *salt = (c.budgets && diffuse && iS >= 0) ? p.salt_budget + col : nullptr;
-
-    // ---- downward pass: back-substitution, budgets, non-local, store ----
-    double x_above[NTR];
-#pragma unroll
-    for (int t = 0; t < NTR; ++t) x_above[t] = 0.0;
-    double gT_above = 0.0, gS_above = 0.0;   // gamma at the top interface of layer k
-    double d_run = 0.0;
-    double h_c = HH(nz), h_a = 0.0;
-    for (int k = nz; k >= 1; --k) {
-        const double h_b_layer = (k > 1) ? HH(k - 1) : 0.0;   // layer below
-        double gT = 0.0, gS = 0.0;
-        if (nl) {
-            if (k <= k_sfc) d_run = d_run + h_c;
-            if (k > 1 && k <= k_sfc && d_run < h_b) {
-                const double sigma = d_run / h_b;
-                const double g_shape = sigma * (1.0 - sigma) * (1.0 - sigma);
-                const double gamma_factor = cs * g_shape;
-                gT = gamma_factor * q_T_kin;
-                gS = gamma_factor * q_S_kin;
-            }
-        }
-        double fT = 0.0, fS = 0.0;
-        if (do_nl) {
-            double fT_up = 0.0, fT_dn = 0.0, fS_up = 0.0, fS_dn = 0.0;
-            if (k < nz) {
-                fT_up = nonlocal_face_flux(gT_above, h_c, h_a);
-                fS_up = nonlocal_face_flux(gS_above, h_c, h_a);
-            }
-            if (k > 1) {
-                fT_dn = nonlocal_face_flux(gT, h_b_layer, h_c);
-                fS_dn = nonlocal_face_flux(gS, h_b_layer, h_c);
-            }
-            fT = dt * (fT_up - fT_dn);
-            fS = dt * (fS_up - fS_dn);
-        }
-        const size_t off = P * (size_t)(k - 1);
-#pragma unroll
-        for (int t = 0; t < NTR; ++t) {
-            if (t < ntr && (diffuse || t == iT || t == iS || t == iPS)) {
-                double x;
-                double x_old = trc[t][off];
-                if (diffuse) {
-                    const bool useA = !TWO || (t == iT);
-                    const double cpk = useA ? cpA[k - 1] : cpB[TWO ? k - 1 : 0];
-                    x = (k == nz) ? r[t][k - 1] : r[t][k - 1] - cpk * x_above[t];
-                    x_above[t] = x;
-                    if (t == iT && heat) {
-                        const double p_new = h_c * x, p_old = h_c * x_old;
-                        heat[off] = heat[off] + (p_new - p_old);
-                    } else if (t == iS && salt) {
-                        const double p_new = h_c * x, p_old = h_c * x_old;
-                        salt[off] = salt[off] + (p_new - p_old);
-                    }
-                } else {
-                    x = x_old;
-                }
-                if (do_nl) {
-                    if (t == iT) x = conc_add_source(x, h_c, fT);
-                    else if (t == iS || t == iPS) x = conc_add_source(x, h_c, fS);
-                }
-                trc[t][off] = x;
-            }
-        }
-        gT_above = gT;
-        gS_above = gS;
-        h_a = h_c;
-        h_c = h_b_layer;
-    }
-#undef HH
+void launch_selftest_division(unsigned long long seed, long long per_thread, int emin, int erange,
+                              unsigned long long *bad, cudaStream_t stream)
+{
+    k_selftest_division<<<148 * 4, 256, 0, stream>>>(seed, per_thread, emin, erange, bad);
 }
 
 // ---------------------------------------------------------------------------
@@ -830,30 +702,14 @@ void launch_smooth(const Params &p, double *fld, double *scratch, cudaStream_t s
 
 void launch_momentum(const Params &p, double dt, cudaStream_t stream)
 {
-    dim3 grid((p.nx + 1 + MOM_THREADS - 1) / MOM_THREADS, p.ny + 1);
-    k_momentum<<<grid, MOM_THREADS, 0, stream>>>(p, dt);
-}
-
-template <int NTR>
-static void launch_tracers_n(const Params &p, double dt, bool diffuse, bool nonlocal, cudaStream_t stream)
-{
-    dim3 grid((p.nx + TR_THREADS - 1) / TR_THREADS, p.ny);
-    if (p.ks_equals_kt)
-        k_tracers<NTR, false><<<grid, TR_THREADS, 0, stream>>>(p, dt, diffuse ? 1 : 0, nonlocal ? 1 : 0);
-    else
-        k_tracers<NTR, true><<<grid, TR_THREADS, 0, stream>>>(p, dt, diffuse ? 1 : 0, nonlocal ? 1 : 0);
-}
-
-void launch_tracers(const Params &p, double dt, bool diffuse, bool nonlocal, cudaStream_t stream)
-{
-    if (p.ntr <= 2)
-        launch_tracers_n<2>(p, dt, diffuse, nonlocal, stream);
-    else if (p.ntr <= 4)
-        launch_tracers_n<4>(p, dt, diffuse, nonlocal, stream);
-    else if (p.ntr <= 8)
-        launch_tracers_n<8>(p, dt, diffuse, nonlocal, stream);
-    else
-        launch_tracers_n<16>(p, dt, diffuse, nonlocal, stream);
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_momentum, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)((size_t)VPHYS_NZ_MAX * MOM_THREADS * sizeof(double)));
+        attr_set = true;
+    }
+    dim3 grid((p.nx + 1 + MOM_THREADS - 1) / MOM_THREADS, p.ny + 1, 2);
+    k_momentum<<<grid, MOM_THREADS, (size_t)p.nz * MOM_THREADS * sizeof(double), stream>>>(p, dt);
 }
 
 }  // namespace vphys

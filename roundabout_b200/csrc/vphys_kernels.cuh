@@ -28,6 +28,7 @@ struct Params {
     double *visc_rem_u, *visc_rem_v;
     double *gamma_t, *gamma_s;       // nullptr: not written
     double *heat_budget, *salt_budget;
+    double *budget_scratch;          // 2 planes x nz: forward-swept T and S when budgets are on
     const int *k_top_u, *k_top_v, *k_bot_u, *k_bot_v;   // nullptr: nz / 1
     double *tr[NTR_MAX];
     unsigned long long *guard_count;  // vmix_guard counter (device)
@@ -42,5 +43,7 @@ void launch_assemble(const Params &p, cudaStream_t stream);
 void launch_smooth(const Params &p, double *fld, double *scratch, cudaStream_t stream);
 void launch_momentum(const Params &p, double dt, cudaStream_t stream);
 void launch_tracers(const Params &p, double dt, bool diffuse, bool nonlocal, cudaStream_t stream);
+void launch_selftest_division(unsigned long long seed, long long per_thread, int emin, int erange,
+                              unsigned long long *bad, cudaStream_t stream);
 
 }  // namespace vphys

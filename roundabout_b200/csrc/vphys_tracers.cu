@@ -1,0 +1,346 @@
+// vphys_tracers.cu -- implicit vertical diffusion of every tracer with the KPP
+// non-local tendency fused into the store (rdb_ocean_vdiff.F90:1107-1414,
+// rdb_ocean_vmix.F90:1605-1714).
+//
+// One thread per cell column; the block's 128 columns are consecutive in i,
+// so every per-level access of a warp is one coalesced 256-B segment.
+//
+// * Only the column's live span [k_lo, k_hi] (first live layer from the bed,
+//   first live layer from the surface) is solved: every row outside it is an
+//   identity row of the reference's matrix (both couplings gated to zero by
+//   H_VANISHED), whose solution is its input, its budget increment zero and
+//   its non-local deposit refused -- the values are unchanged (up to the sign
+//   of a zero), so those cells are neither read nor written.  Land columns
+//   cost one scan of h.
+// * The matrix is factorised once per diffusivity (kt, and ks when it differs)
+//   in the same upward pass that forward-sweeps every tracer.  The pivots'
+//   c' live in shared memory; the forward-swept right-hand sides are written
+//   in place into the tracer arrays with an L2 evict_last hint and read back
+//   by the downward pass, so the round trip stays in L2 and HBM sees each
+//   tracer value read once and written once.
+// * Loads are issued a block of U levels ahead of the arithmetic, so each
+//   thread keeps several independent loads in flight under the serial
+//   Thomas recurrence.
+#include <cuda_runtime.h>
+
+#include "vphys_device.cuh"
+#include "vphys_kernels.cuh"
+
+namespace vphys {
+
+
+// Row k (1-based) of the tracer matrix (build_factorize_tracer_matrix,
+// rdb_ocean_vdiff.F90:1285-1341); hm/hc/hp are the raw thicknesses of layers
+// k-1, k, k+1, K_k / K_kp1 the diffusivity at interfaces k and k+1.
+__device__ __forceinline__ void tracer_row(int k, int nz, bool use_harmonic, double dt, double hm_raw, double hc_raw,
+                                           double hp_raw, double K_k, double K_kp1, double &a, double &b, double &cc)
+{
+    if (k == 1) {
+        const double hc = fmx(hc_raw, H_VANISHED);
+        double alpha = 0.0;
+        if (nz > 1) {
+            const double hp = fmx(hp_raw, H_VANISHED);
+            const double dz_face = face_thick(hc, hp, use_harmonic);
+            alpha = xdiv(dt * K_kp1, hc * dz_face);
+            if (hc_raw <= H_VANISHED || hp_raw <= H_VANISHED) alpha = 0.0;
+        }
+        a = 0.0;
+        cc = -alpha;
+        b = 1.0 + alpha;
+    } else if (k < nz) {
+        const double hm = fmx(hm_raw, H_VANISHED);
+        const double hc = fmx(hc_raw, H_VANISHED);
+        const double hp = fmx(hp_raw, H_VANISHED);
+        double beta = xdiv(dt * K_k, hc * face_thick(hm, hc, use_harmonic));
+        double alpha = xdiv(dt * K_kp1, hc * face_thick(hc, hp, use_harmonic));
+        if (hc_raw <= H_VANISHED || hm_raw <= H_VANISHED) beta = 0.0;
+        if (hc_raw <= H_VANISHED || hp_raw <= H_VANISHED) alpha = 0.0;
+        a = -beta;
+        cc = -alpha;
+        b = 1.0 + alpha + beta;
+    } else {
+        const double hm = fmx(hm_raw, H_VANISHED);
+        const double hc = fmx(hc_raw, H_VANISHED);
+        const double dz_face = face_thick(hm, hc, use_harmonic);
+        double beta = xdiv(dt * K_k, hc * dz_face);
+        if (hc_raw <= H_VANISHED || hm_raw <= H_VANISHED) beta = 0.0;
+        a = -beta;
+        cc = 0.0;
+        b = 1.0 + beta;
+    }
+}
+
+template <int NTR, bool TWO>
+__global__ void __launch_bounds__(128) k_tracers(const Params p, double dt, int diffuse, int nonlocal)
+{
+    constexpr int TR_U = NTR <= 4 ? 4 : (NTR <= 8 ? 2 : 1);   // levels per load block
+    extern __shared__ double smem[];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    const vphys_config &c = p.cfg;
+    const int nx = p.nx, nz = p.nz, ntr = p.ntr;
+    const size_t P = p.plane;
+    const bool in_grid = i < nx;
+    const size_t col = (size_t)(in_grid ? i : 0) + (size_t)nx * j;
+    const double *__restrict__ hp = p.h + col;
+    const int iT = c.idx_temperature, iS = c.idx_salinity, iPS = c.idx_pseudo_salt;
+    const int bs = blockDim.x;
+    double *cpA = smem + threadIdx.x;                       // cpA[(k-1)*bs]
+    double *cpB = smem + (size_t)nz * bs + threadIdx.x;     // only when TWO
+    const unsigned long long pol_keep = l2_policy_evict_last();
+    const unsigned long long pol_once = l2_policy_evict_first();
+#define HH(k) __ldg(hp + P * (size_t)((k) - 1))
+
+    // ---- this column's live span; rows outside it are identity rows ----
+    int k_lo = 0, k_hi = 0;
+    double h_below = 0.0, h_lo = 0.0, h_hi = 0.0;
+    if (in_grid) {
+        for (int k = 1; k <= nz; ++k) {
+            const double hk = HH(k);
+            if (hk > H_VANISHED) {
+                k_lo = k;
+                h_lo = hk;
+                break;
+            }
+            h_below = hk;
+        }
+        if (k_lo > 0) {
+            k_hi = k_lo;
+            h_hi = h_lo;
+            for (int k = nz; k > k_lo; --k) {
+                const double hk = HH(k);
+                if (hk > H_VANISHED) {
+                    k_hi = k;
+                    h_hi = hk;
+                    break;
+                }
+            }
+        }
+    }
+    const bool live = k_lo > 0;
+    // the warp sweeps the union of its lanes' spans with a uniform k, so its
+    // loads stay coalesced and the row-type branches stay uniform; a lane
+    // outside its own span is predicated off (no load, no store)
+    const unsigned full = 0xffffffffu;
+    const int w_lo = __reduce_min_sync(full, live ? k_lo : 0x7fffffff);
+    const int w_hi = __reduce_max_sync(full, live ? k_hi : 0);
+    if (w_hi == 0) return;   // no live layer anywhere in this warp
+
+    double *trc[NTR];
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) trc[t] = (t < ntr) ? p.tr[t] + col : nullptr;
+    // With heat/salt budgets the reference needs h*c_new - h*c_old, so the
+    // forward-swept values of T and S go to a scratch plane instead of over
+    // the input (rbuf); every other tracer is swept in place.
+    double *heat = (c.budgets && diffuse && iT >= 0) ? p.heat_budget + col : nullptr;
+    double *salt = (c.budgets && diffuse && iS >= 0) ? p.salt_budget + col : nullptr;
+    double *rbuf[NTR];
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) {
+        rbuf[t] = trc[t];
+        if (t < ntr && heat && t == iT) rbuf[t] = p.budget_scratch + col;
+        if (t < ntr && salt && t == iS) rbuf[t] = p.budget_scratch + P * (size_t)nz + col;
+    }
+
+    if (diffuse) {
+        // ---- upward pass: rows, factorisation, forward sweep of every tracer ----
+        const double *__restrict__ KA = p.kt + col;
+        const double *__restrict__ KB = p.ks + col;
+        double h_m = h_below, h_c = h_lo;
+        double KA_k = 0.0, KB_k = 0.0;   // interface k_lo: gated off when k_lo > 1
+        double cpA_prev = 0.0, cpB_prev = 0.0;
+        double r_prev[NTR];
+#pragma unroll
+        for (int t = 0; t < NTR; ++t) r_prev[t] = 0.0;
+        for (int k0 = w_lo; k0 <= w_hi; k0 += TR_U) {
+            double xs[TR_U][NTR], hps[TR_U], kap[TR_U], kbp[TR_U];
+#pragma unroll
+            for (int u = 0; u < TR_U; ++u) {
+                const int k = k0 + u;
+                const bool act = live && k >= k_lo && k <= k_hi;
+                const size_t off = P * (size_t)(k - 1);
+                hps[u] = (act && k < nz) ? __ldg(hp + off + P) : 0.0;
+                kap[u] = (act && k < nz) ? ld_hint(KA + off + P, pol_once) : 0.0;
+                if (TWO) kbp[u] = (act && k < nz) ? ld_hint(KB + off + P, pol_once) : 0.0;
+#pragma unroll
+                for (int t = 0; t < NTR; ++t) xs[u][t] = (act && t < ntr) ? trc[t][off] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < TR_U; ++u) {
+                const int k = k0 + u;
+                if (k > w_hi) break;
+                const bool act = live && k >= k_lo && k <= k_hi;
+                if (act) {
+                    const size_t off = P * (size_t)(k - 1);
+                    const double h_p = hps[u];
+                    double aA, bA, cA;
+                    tracer_row(k, nz, c.use_harmonic, dt, h_m, h_c, h_p, KA_k, kap[u], aA, bA, cA);
+                    const Rcp denA = rcp_of((k == 1) ? bA : bA - aA * cpA_prev);
+                    cpA_prev = qdiv(cA, denA);
+                    cpA[(size_t)(k - 1) * bs] = cpA_prev;
+                    double aB = 0.0;
+                    Rcp denB = denA;
+                    if (TWO) {
+                        double bB, cB;
+                        tracer_row(k, nz, c.use_harmonic, dt, h_m, h_c, h_p, KB_k, kbp[u], aB, bB, cB);
+                        denB = rcp_of((k == 1) ? bB : bB - aB * cpB_prev);
+                        cpB_prev = qdiv(cB, denB);
+                        cpB[(size_t)(k - 1) * bs] = cpB_prev;
+                        KB_k = kbp[u];
+                    }
+#pragma unroll
+                    for (int t = 0; t < NTR; ++t) {
+                        if (t < ntr) {
+                            const bool useA = !TWO || (t == iT);
+                            const double a = useA ? aA : aB;
+                            const double num = (k == 1) ? xs[u][t] : xs[u][t] - a * r_prev[t];
+                            const double r = qdiv(num, useA ? denA : denB);
+                            r_prev[t] = r;
+                            st_hint(rbuf[t] + off, r, pol_keep);
+                        }
+                    }
+                    KA_k = kap[u];
+                    h_m = h_c;
+                    h_c = h_p;
+                }
+            }
+        }
+    }
+
+    // ---- non-local column scalars, recomputed exactly as KPP pass 2 ----
+    const bool do_nl = nonlocal && c.use_kpp;
+    bool nl = do_nl && live;
+    double h_b = 0.0, q_T_kin = 0.0, q_S_kin = 0.0;
+    if (nl) {
+        const double rho0 = c.rho0;
+        h_b = p.bl_depth[col];
+        const double u_star = sqrt(xdiv(p.stress_mag[col], rho0));
+        q_T_kin = xdiv(p.q_heat[col], rho0 * c.cp);
+        q_S_kin = xdiv(p.q_salt[col], rho0);
+        const double B_0 = (GRAVITY / rho0) * (c.alpha_T * q_T_kin - c.beta_S * q_S_kin);
+        const double wstar3 = fmx(0.0, -B_0) * h_b;
+        const double w_star = sm_cbrt(wstar3);
+        const double w_s = sqrt(u_star * u_star + w_star * w_star);
+        nl = (h_b > 0.0 && w_s > 0.0 && B_0 < 0.0);
+    }
+
+    // ---- downward pass: back-substitution, budgets, non-local deposit and
+    //      the store (the reference's k_sfc is this column's k_hi) ----
+    double x_above[NTR];
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) x_above[t] = 0.0;
+    double gT_above = 0.0, gS_above = 0.0;
+    double d_run = 0.0;
+    double h_c = h_hi, h_a = 0.0;   // layer above k_hi is vanished: its flux is closed
+    for (int k0 = w_hi; k0 >= w_lo; k0 -= TR_U) {
+        double rs[TR_U][NTR], hbs[TR_U];
+#pragma unroll
+        for (int u = 0; u < TR_U; ++u) {
+            const int k = k0 - u;
+            const bool act = live && k >= k_lo && k <= k_hi;
+            const size_t off = P * (size_t)(k - 1);
+            hbs[u] = (act && k > 1) ? __ldg(hp + off - P) : 0.0;
+#pragma unroll
+            for (int t = 0; t < NTR; ++t)
+                rs[u][t] = (act && t < ntr && (diffuse || t == iT || t == iS || t == iPS))
+                               ? ld_hint((diffuse ? rbuf[t] : trc[t]) + off, pol_keep)
+                               : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < TR_U; ++u) {
+            const int k = k0 - u;
+            if (k < w_lo) break;
+            const bool act = live && k >= k_lo && k <= k_hi;
+            if (act) {
+                const size_t off = P * (size_t)(k - 1);
+                const double h_bl = hbs[u];
+                double gT = 0.0, gS = 0.0;
+                if (nl) {
+                    d_run = d_run + h_c;
+                    if (k > 1 && d_run < h_b) {
+                        const double sigma = xdiv(d_run, h_b);
+                        const double g_shape = sigma * (1.0 - sigma) * (1.0 - sigma);
+                        const double gamma_factor = c.cs_nonlocal * g_shape;
+                        gT = gamma_factor * q_T_kin;
+                        gS = gamma_factor * q_S_kin;
+                    }
+                }
+                double fT = 0.0, fS = 0.0;
+                if (do_nl) {
+                    double fT_up = 0.0, fT_dn = 0.0, fS_up = 0.0, fS_dn = 0.0;
+                    if (k < nz) {
+                        fT_up = nonlocal_face_flux(gT_above, h_c, h_a);
+                        fS_up = nonlocal_face_flux(gS_above, h_c, h_a);
+                    }
+                    if (k > 1) {
+                        fT_dn = nonlocal_face_flux(gT, h_bl, h_c);
+                        fS_dn = nonlocal_face_flux(gS, h_bl, h_c);
+                    }
+                    fT = dt * (fT_up - fT_dn);
+                    fS = dt * (fS_up - fS_dn);
+                }
+#pragma unroll
+                for (int t = 0; t < NTR; ++t) {
+                    if (t < ntr && (diffuse || t == iT || t == iS || t == iPS)) {
+                        double x = rs[u][t];
+                        if (diffuse) {
+                            const bool useA = !TWO || (t == iT);
+                            const double cpk = useA ? cpA[(size_t)(k - 1) * bs] : cpB[(size_t)(k - 1) * bs];
+                            x = x - cpk * x_above[t];   // x_above = 0 at k_hi: the top row
+                            x_above[t] = x;
+                            if ((t == iT && heat) || (t == iS && salt)) {
+                                double *bud = (t == iT) ? heat : salt;
+                                const double x_old = trc[t][off];
+                                const double p_new = h_c * x, p_old = h_c * x_old;
+                                bud[off] = bud[off] + (p_new - p_old);
+                            }
+                        }
+                        if (do_nl) {
+                            if (t == iT) x = conc_add_source(x, h_c, fT);
+                            else if (t == iS || t == iPS) x = conc_add_source(x, h_c, fS);
+                        }
+                        trc[t][off] = x;
+                    }
+                }
+                gT_above = gT;
+                gS_above = gS;
+                h_a = h_c;
+                h_c = h_bl;
+            }
+        }
+    }
+#undef HH
+}
+
+template <int NTR, bool TWO>
+static void launch_tracers_n(const Params &p, double dt, bool diffuse, bool nonlocal, cudaStream_t stream)
+{
+    // two factorisations keep two c' arrays: halve the block to stay within
+    // the 227 KB of shared memory per block at nz = VPHYS_NZ_MAX
+    const int bs = TWO ? 64 : 128;
+    const size_t smem = (size_t)p.nz * bs * sizeof(double) * (TWO ? 2 : 1);
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_tracers<NTR, TWO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)((size_t)VPHYS_NZ_MAX * bs * sizeof(double) * (TWO ? 2 : 1)));
+        attr_set = true;
+    }
+    dim3 grid((p.nx + bs - 1) / bs, p.ny);
+    k_tracers<NTR, TWO><<<grid, bs, smem, stream>>>(p, dt, diffuse ? 1 : 0, nonlocal ? 1 : 0);
+}
+
+void launch_tracers(const Params &p, double dt, bool diffuse, bool nonlocal, cudaStream_t stream)
+{
+    const bool two = !p.ks_equals_kt;
+    if (p.ntr <= 2) {
+        two ? launch_tracers_n<2, true>(p, dt, diffuse, nonlocal, stream) : launch_tracers_n<2, false>(p, dt, diffuse, nonlocal, stream);
+    } else if (p.ntr <= 4) {
+        two ? launch_tracers_n<4, true>(p, dt, diffuse, nonlocal, stream) : launch_tracers_n<4, false>(p, dt, diffuse, nonlocal, stream);
+    } else if (p.ntr <= 8) {
+        two ? launch_tracers_n<8, true>(p, dt, diffuse, nonlocal, stream) : launch_tracers_n<8, false>(p, dt, diffuse, nonlocal, stream);
+    } else {
+        two ? launch_tracers_n<16, true>(p, dt, diffuse, nonlocal, stream) : launch_tracers_n<16, false>(p, dt, diffuse, nonlocal, stream);
+    }
+}
+
+}  // namespace vphys
