@@ -59,6 +59,7 @@ extern "C" {
                                        rdb_ocean_vmix.F90:2264-2277) */
 #define VPHYS_ERR_TOO_DEEP 32       /* nz > VPHYS_NZ_MAX */
 #define VPHYS_ERR_ALLOC 33          /* device allocation failed */
+#define VPHYS_ERR_TOO_LARGE 34      /* request beyond a fixed capacity */
 
 /* Largest nz the column kernels accept; the reference's own per-column
  * stack bound NZ_STACK_MAX (src/core/rdb_constants.F90:107-124) is 128 and
@@ -285,6 +286,25 @@ const char *vphys_version(void);
  * patterns to *mismatches (0 expected).  Synchronous. */
 int vphys_selftest_division(long long n_pairs, unsigned long long seed, int emin, int erange,
                             unsigned long long *mismatches);
+
+/* Allocation-free 1-2-1 smoothing.  No counterpart in the reference: it is
+ * the masked 1-2-1 horizontal smoothing of the assembly gate
+ * (vmix_smooth_121_impl, rdb_ocean_vmix.F90:2699-2748, which the reference
+ * runs through its own smooth_scratch) offered to callers that cannot call
+ * cudaMalloc -- a host that owns all device memory through its own pool
+ * (an OpenACC/Fortran model, a framework caching allocator) or code running
+ * where allocating is not allowed.  `fld` is a device (nx, ny, nz+1)
+ * interface field (kv, kt or ks), smoothed in place on interfaces 2..nz for
+ * `iterations` passes; `wet` the device (nx, ny) wet mask; `stream` a
+ * cudaStream_t (NULL: legacy default stream).  The copy of a plane that the
+ * stencil reads lives in a fixed device array of 2^23 doubles (64 MiB) that
+ * every GPU loading the library holds until exit; nx*ny above 2^23 returns
+ * VPHYS_ERR_TOO_LARGE.  Nothing is allocated or freed.  The first call on a
+ * device looks up that array's device address (once per device); make it
+ * before any stream capture.  All calls share the array, so calls whose work
+ * overlaps on the GPU race.  Asynchronous. */
+int vphys_smooth_121_static(double *fld, const double *wet, int nx, int ny, int nz, int iterations,
+                            void *stream);
 
 /* sizeof(vphys_config) as compiled into the library, so a binding in another
  * language can verify its mirror of the struct before passing one. */

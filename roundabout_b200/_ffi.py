@@ -28,6 +28,7 @@ ERR_CUDA = 30
 ERR_GUARD = 31
 ERR_TOO_DEEP = 32
 ERR_ALLOC = 33
+ERR_TOO_LARGE = 34
 
 NZ_MAX = 127
 INTERIOR_PP81 = 1
@@ -173,6 +174,8 @@ _PROTOTYPES = {
     "vphys_last_error": (ctypes.c_int, [ctypes.c_int, ctypes.c_char_p, ctypes.c_int]),
     "vphys_version": (ctypes.c_char_p, []),
     "vphys_config_sizeof": (ctypes.c_size_t, []),
+    "vphys_smooth_121_static": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                                ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
     "vphys_selftest_division": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_ulonglong, ctypes.c_int, ctypes.c_int,
                                                 ctypes.POINTER(ctypes.c_ulonglong)]),
 }

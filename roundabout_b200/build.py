@@ -17,7 +17,7 @@ from pathlib import Path
 CSRC = Path(__file__).resolve().parent / "csrc"
 OUT = CSRC / "_build"
 LIB = OUT / "libvphys.so"
-SOURCES = ["vphys_api.cu", "vphys_kernels.cu", "vphys_tracers.cu"]
+SOURCES = ["vphys_api.cu", "vphys_kernels.cu", "vphys_tracers.cu", "vphys_static.cu"]
 HEADERS = ["vphys_device.cuh", "vphys_kernels.cuh", "../../include/vphys.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

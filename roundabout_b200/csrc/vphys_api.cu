@@ -333,6 +333,8 @@ int read_guard(vphys_handle h, int *status)
 
 }  // namespace
 
+int vphys::report_error(int status, const char *msg) { return push_error(status, "%s", msg); }
+
 // ===========================================================================
 // C ABI
 // ===========================================================================

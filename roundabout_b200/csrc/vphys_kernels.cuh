@@ -36,6 +36,9 @@ struct Params {
     int write_gamma;
 };
 
+// Push a message onto the library's error ring and return `status` (vphys_api.cu).
+int report_error(int status, const char *msg);
+
 // Launchers (vphys_kernels.cu); all asynchronous on `stream`.
 void launch_eos_wright(const Params &p, cudaStream_t stream);
 void launch_stress_mag(const Params &p, cudaStream_t stream);
