@@ -1,0 +1,81 @@
+"""The C ABI without a GPU: libvphys.so loads, exports every entry point that
+include/vphys.h declares, agrees with the Python mirror of its config struct
+and its defaults, and fails cleanly (status + error-ring message, no abort)
+where a device would be needed."""
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from roundabout_b200 import build as b
+
+    b.build()
+    from roundabout_b200 import _ffi
+
+    return _ffi.get_lib()
+
+
+def declared_symbols():
+    text = (ROOT / "include" / "vphys.h").read_text()
+    return sorted(set(re.findall(r"^\s*(?:int|size_t|const char \*)\s*(vphys_\w+)\s*\(", text, re.M)))
+
+
+def test_every_declared_symbol_is_exported(lib):
+    from roundabout_b200 import _ffi
+
+    syms = declared_symbols()
+    assert len(syms) >= 20
+    for s in syms:
+        assert hasattr(lib, s), f"{s} declared in include/vphys.h but not exported"
+        assert s in _ffi.EXPORTED_SYMBOLS, f"{s} has no ctypes prototype in _ffi.py"
+
+
+def test_config_struct_layout_and_defaults(lib):
+    from roundabout_b200 import _ffi
+    from roundabout_b200.config import default_config
+
+    assert lib.vphys_config_sizeof() == ctypes.sizeof(_ffi.VphysConfig)
+    c = _ffi.VphysConfig()
+    assert lib.vphys_config_default(ctypes.byref(c)) == _ffi.OK
+    py = default_config()
+    assert c.as_dict() == py.as_dict()
+
+
+def test_errors_are_reported_not_raised(lib):
+    from roundabout_b200 import _ffi
+
+    h = ctypes.c_void_p()
+    st = lib.vphys_create(4, 4, 200, 2, None, ctypes.byref(h))
+    assert st == _ffi.ERR_TOO_DEEP and h.value is None
+    assert "VPHYS_NZ_MAX" in _ffi.last_error(0)
+    bad = _ffi.VphysConfig()
+    lib.vphys_config_default(ctypes.byref(bad))
+    bad.use_closure = 0
+    assert lib.vphys_create(4, 4, 4, 2, ctypes.byref(bad), ctypes.byref(h)) == _ffi.ERR_CONFIG
+    assert "scalar" in _ffi.last_error(0)
+    assert lib.vphys_step(None, 1.0, 1) == _ffi.ERR_BAD_HANDLE
+    nothing = ctypes.c_void_p()
+    assert lib.vphys_destroy(ctypes.byref(nothing)) == _ffi.OK
+    buf = ctypes.create_string_buffer(4)
+    n = lib.vphys_last_error(0, buf, 4)
+    assert n > 3 and len(buf.value) == 3          # snprintf-style truncation
+    assert lib.vphys_last_error(10_000, buf, 4) == 0
+
+
+def test_create_without_a_device_fails_cleanly(lib):
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    from roundabout_b200 import _ffi
+
+    h = ctypes.c_void_p()
+    st = lib.vphys_create(8, 8, 4, 2, None, ctypes.byref(h))
+    assert st in (_ffi.ERR_ALLOC, _ffi.ERR_CUDA) and h.value is None
+    assert _ffi.last_error(0)

@@ -1,0 +1,342 @@
+"""The CPU oracle against the reference's own known-answer tests for the path,
+re-expressed here (the Fortran tests cannot run: no Fortran compiler).
+
+Cases follow, in order: tests/test_ocean_pp81.F90:42-53, test_ocean_kpp.F90:40-57
+(no wind, unstratified h_b, shape function, collapsed top layer),
+test_ocean_kpp_nonlocal.F90 (stabilising flux, column heat),
+test_ocean_vdiff.F90:42-69 (constancy, K = 0, conservation, vanishing layer,
+relax-to-mean, kt = ks), test_ocean_vmix_assembly.F90:39-55 (pass-through,
+ceilings, floors), test_ocean_bkgnd_mixing.F90:114-132 (Bryan-Lewis shape),
+and test_ocean_wright_eos.F90:87-130 (Wright reference values).  Tolerances are the
+reference tests' own.
+"""
+import numpy as np
+import pytest
+
+from roundabout_b200.config import default_config
+
+NZ = 5
+
+
+def state(oracle, nx=12, ny=10, nz=NZ, ntr=2, h=10.0):
+    st = oracle.OracleState(nx, ny, nz, ntr)
+    st.h[...] = h
+    return st
+
+
+def cfg_pp81(**kw):
+    c = default_config()
+    for k, v in kw.items():
+        setattr(c, k, v)
+    return c
+
+
+# ---------------------------------------------------------------- PP81 ----
+def test_pp81_quiescent_stratified(oracle):
+    c = cfg_pp81()
+    st = state(oracle)
+    for k in range(NZ):
+        st.rho[:, :, k] = 1030.0 - 1.0 * k
+    st.call("vpo_pp81", c)
+    assert np.abs(st.kv[6, 5, 1:NZ] - c.pp81_nu_bg).max() < 1e-6
+    assert np.abs(st.kt[6, 5, 1:NZ] - c.pp81_kappa_bg).max() < 1e-6
+
+
+def test_pp81_shear_without_stratification_is_full_mixing(oracle):
+    c = cfg_pp81()
+    st = state(oracle)
+    st.rho[...] = 1030.0
+    for k in range(NZ):
+        st.u[:, :, k] = 1.0 * k / (NZ - 1)
+    st.call("vpo_pp81", c)
+    assert np.abs(st.kv[6, 5, 1:NZ] - (c.pp81_nu_bg + c.pp81_nu0)).max() < 1e-12
+    assert np.abs(st.kt[6, 5, 1:NZ] - (c.pp81_kappa_bg + c.pp81_nu0)).max() < 1e-12
+
+
+def test_pp81_strong_stratification_clamps(oracle):
+    c = cfg_pp81()
+    st = state(oracle)
+    for k in range(NZ):
+        st.u[:, :, k] = 1.0e-3 * k / (NZ - 1)
+        st.rho[:, :, k] = 1030.0 - 5.0 * k
+    st.call("vpo_pp81", c)
+    assert st.kv[6, 5, 1:NZ].max() < 0.1 * (c.pp81_nu_bg + c.pp81_nu0)
+
+
+def test_pp81_unstable_ri_clipped(oracle):
+    c = cfg_pp81()
+    st = state(oracle)
+    for k in range(NZ):
+        st.rho[:, :, k] = 1030.0 + 1.0 * k
+    st.call("vpo_pp81", c)
+    assert np.abs(st.kv[6, 5, 1:NZ] - (c.pp81_nu_bg + c.pp81_nu0)).max() < 1e-12
+
+
+def test_pp81_boundary_interfaces_zero(oracle):
+    c = cfg_pp81()
+    st = state(oracle)
+    st.u[...] = 0.5
+    for k in range(NZ):
+        st.rho[:, :, k] = 1030.0 - 0.5 * k
+    st.kv[...] = 7.0
+    st.kt[...] = 7.0
+    st.call("vpo_pp81", c)
+    for a in (st.kv, st.kt):
+        assert np.abs(a[:, :, 0]).max() < 1e-15 and np.abs(a[:, :, -1]).max() < 1e-15
+
+
+# ----------------------------------------------------------------- KPP ----
+def kpp_state(oracle, nz=10, h=10.0, tau=0.1, strat=0.0):
+    st = state(oracle, nz=nz, h=h)
+    for k in range(nz):
+        st.rho[:, :, k] = 1030.0 - strat * k
+    st.stress_mag[...] = tau
+    return st
+
+
+def test_kpp_no_wind_is_no_op(oracle):
+    c = cfg_pp81(use_kpp=1)
+    st = kpp_state(oracle, nz=NZ, h=5.0, tau=0.0, strat=0.5)
+    ref = st.copy()
+    ref.call("vpo_pp81", c)
+    st.call("vpo_pp81", c)
+    st.call("vpo_kpp_overlay", c)
+    assert np.abs(st.kv - ref.kv).max() <= 1e-14
+    assert np.abs(st.kt - ref.kt).max() <= 1e-14
+
+
+def test_kpp_unstratified_bl_fills_column(oracle):
+    c = cfg_pp81(use_kpp=1)
+    nz, h = 8, 10.0
+    st = kpp_state(oracle, nz=nz, h=h, tau=0.1, strat=0.0)
+    st.call("vpo_pp81", c)
+    st.call("vpo_kpp_overlay", c)
+    assert np.abs(st.bl_depth - nz * h).max() < 1e-9
+
+
+def test_kpp_shape_function_matches_closed_form(oracle):
+    c = cfg_pp81(use_kpp=1)
+    nz, h, tau = 8, 10.0, 0.1
+    st = kpp_state(oracle, nz=nz, h=h, tau=tau, strat=0.0)
+    st.call("vpo_pp81", c)
+    st.call("vpo_kpp_overlay", c)
+    hb = nz * h
+    u_star = np.sqrt(tau / c.rho0)
+    for k in range(1, nz):            # interface k (0-based) is the bottom of layer k
+        d = (nz - k) * h              # depth of that interface below the surface
+        sig = d / hb
+        want = max(c.pp81_nu_bg + c.pp81_nu0, hb * u_star * sig * (1 - sig) ** 2)
+        assert abs(st.kv[6, 5, k] - want) < 1e-9
+
+
+def test_kpp_vt2_never_shallows_the_bl(oracle):
+    base = dict(use_kpp=1)
+    depths = []
+    for cvt2 in (0.0, 1.8, 4.0):
+        c = cfg_pp81(c_vt2=cvt2, **base)
+        st = kpp_state(oracle, nz=20, h=5.0, tau=0.05, strat=0.02)
+        st.q_heat[...] = -200.0
+        st.bl_depth[...] = 30.0       # lagged h_b feeds w_s into V_t^2
+        st.call("vpo_pp81", c)
+        st.call("vpo_kpp_overlay", c)
+        depths.append(st.bl_depth[6, 5])
+    assert depths[0] <= depths[1] <= depths[2]
+
+
+def test_kpp_collapsed_top_layer_equals_column_without_it(oracle):
+    c = cfg_pp81(use_kpp=1)
+    nz = 9
+    a = kpp_state(oracle, nz=nz, h=10.0, tau=0.1, strat=0.2)
+    b = kpp_state(oracle, nz=nz + 1, h=10.0, tau=0.1, strat=0.2)
+    for k in range(nz):
+        b.rho[:, :, k] = a.rho[:, :, k]
+    b.h[:, :, nz] = 1.0e-4            # a collapsed (vanished) top layer
+    b.rho[:, :, nz] = c.rho0
+    for s_ in (a, b):
+        s_.call("vpo_pp81", c)
+        s_.call("vpo_kpp_overlay", c)
+    assert abs(a.bl_depth[6, 5] - b.bl_depth[6, 5]) < 1e-9
+    np.testing.assert_allclose(b.kv[6, 5, 1:nz], a.kv[6, 5, 1:nz], rtol=0, atol=1e-12)
+
+
+# -------------------------------------------------------- non-local KPP ----
+def test_nonlocal_zero_under_stabilising_flux(oracle):
+    c = cfg_pp81(use_kpp=1, alpha_T=0.2, beta_S=0.77)
+    st = kpp_state(oracle, nz=10, h=10.0, tau=0.1, strat=0.05)
+    st.q_heat[...] = +150.0           # heating: B0 > 0
+    st.call("vpo_pp81", c)
+    st.call("vpo_kpp_overlay", c)
+    assert np.abs(st.gamma_t).max() == 0.0 and np.abs(st.gamma_s).max() == 0.0
+
+
+def test_nonlocal_conserves_column_heat(oracle):
+    c = cfg_pp81(use_kpp=1, alpha_T=0.2, beta_S=0.77)
+    st = kpp_state(oracle, nz=12, h=8.0, tau=0.05, strat=0.01)
+    st.h[:, :, 0] = 0.0                # a vanished bed filler
+    st.q_heat[...] = -300.0            # cooling: B0 < 0
+    st.tracers[1][...] = 10.0 + np.arange(12)[None, None, :] * 0.5
+    st.call("vpo_pp81", c)
+    st.call("vpo_kpp_overlay", c)
+    assert np.abs(st.gamma_t).max() > 0.0
+    heat0 = (st.h * st.tracers[1]).sum(axis=2)
+    st.call("vpo_nonlocal", c, 3600.0)
+    heat1 = (st.h * st.tracers[1]).sum(axis=2)
+    assert np.abs(heat1 - heat0).max() <= 1e-12 * np.abs(heat0).max()
+    assert np.abs(st.gamma_t[:, :, 0]).max() == 0.0 and np.abs(st.gamma_t[:, :, -1]).max() == 0.0
+
+
+# --------------------------------------------------------------- vdiff ----
+def vdiff_state(oracle, nz=8, K=1e-3, h=10.0):
+    c = cfg_pp81()
+    st = state(oracle, nz=nz, h=h, ntr=2)
+    st.kt[...] = K
+    st.kt[:, :, 0] = 0.0
+    st.kt[:, :, -1] = 0.0
+    st.ks[...] = st.kt
+    return c, st
+
+
+def test_vdiff_uniform_tracer_stays_uniform(oracle):
+    c, st = vdiff_state(oracle)
+    st.tracers[0][...] = 35.0
+    st.tracers[1][...] = 12.0
+    st.call("vpo_vdiff_tracers", c, 3600.0)
+    assert np.abs(st.tracers[0] - 35.0).max() <= 1e-12
+    assert np.abs(st.tracers[1] - 12.0).max() <= 1e-12
+
+
+def test_vdiff_zero_diffusivity_is_no_op(oracle):
+    c, st = vdiff_state(oracle, K=0.0)
+    rng = np.random.default_rng(0)
+    st.tracers[1][...] = rng.uniform(0, 20, st.tracers[1].shape)
+    t0 = st.tracers[1].copy()
+    st.call("vpo_vdiff_tracers", c, 3600.0)
+    assert np.array_equal(st.tracers[1], t0)
+
+
+def test_vdiff_conserves_column_content(oracle):
+    c, st = vdiff_state(oracle, K=5e-2)
+    rng = np.random.default_rng(1)
+    st.h[...] = rng.uniform(1.0, 50.0, st.h.shape)
+    st.tracers[1][...] = rng.uniform(0, 20, st.h.shape)
+    c0 = (st.h * st.tracers[1]).sum(axis=2)
+    st.call("vpo_vdiff_tracers", c, 3600.0)
+    c1 = (st.h * st.tracers[1]).sum(axis=2)
+    assert np.abs(c1 - c0).max() <= 1e-12 * np.abs(c0).max()
+
+
+def test_vdiff_vanishing_layer_is_frozen_and_live_layers_conserve(oracle):
+    c, st = vdiff_state(oracle, K=5e-2)
+    st.h[:, :, 3] = 1.0e-5              # vanishing (<= H_VANISHED) mid-column layer
+    rng = np.random.default_rng(2)
+    st.tracers[1][...] = rng.uniform(0, 20, st.h.shape)
+    frozen = st.tracers[1][:, :, 3].copy()
+    live = st.h > 1.5e-4
+    c0 = (st.h * st.tracers[1] * live).sum(axis=2)
+    st.call("vpo_vdiff_tracers", c, 3600.0)
+    c1 = (st.h * st.tracers[1] * live).sum(axis=2)
+    assert np.abs(c1 - c0).max() <= 1e-12 * np.abs(c0).max()
+    assert np.abs(st.tracers[1][:, :, 3] - frozen).max() <= 1e-10
+
+
+def test_vdiff_strong_mixing_relaxes_to_the_mean(oracle):
+    # test_ocean_vdiff.F90:310-362: h = 1, dt = 1, K = 1e6
+    c, st = vdiff_state(oracle, K=1.0e6, h=1.0)
+    st.tracers[1][...] = np.arange(8)[None, None, :] * 1.0
+    st.call("vpo_vdiff_tracers", c, 1.0)
+    assert np.abs(st.tracers[1] - 3.5).max() < 1e-4
+
+
+def test_vdiff_kt_equal_ks_gives_identical_tracers(oracle):
+    c, st = vdiff_state(oracle, K=2e-3)
+    rng = np.random.default_rng(3)
+    st.h[...] = rng.uniform(1.0, 50.0, st.h.shape)
+    st.tracers[0][...] = rng.uniform(0, 20, st.h.shape)
+    st.tracers[1][...] = st.tracers[0]
+    st.call("vpo_vdiff_tracers", c, 3600.0)
+    assert np.array_equal(st.tracers[0], st.tracers[1])
+
+
+def test_momentum_uniform_velocity_stays_uniform(oracle):
+    c = cfg_pp81()
+    st = state(oracle, nz=8, h=10.0)
+    st.kv[...] = 1e-2
+    st.kv[:, :, 0] = 0.0
+    st.kv[:, :, -1] = 0.0
+    st.u[...] = 0.3
+    st.v[...] = -0.2
+    st.call("vpo_vdiff_momentum", c, 3600.0)
+    assert np.abs(st.u - 0.3).max() <= 1e-12
+    assert np.abs(st.v + 0.2).max() <= 1e-12
+
+
+# ------------------------------------------------------------- assembly ----
+def test_assembly_defaults_pass_pp81_through(oracle):
+    c = cfg_pp81()
+    st = state(oracle)
+    for k in range(NZ):
+        st.rho[:, :, k] = 1030.0 - 0.1 * k
+        st.u[:, :, k] = 0.01 * k
+    st.call("vpo_pp81", c)
+    kv0 = st.kv.copy()
+    st.call("vpo_split", c)
+    assert st.call("vpo_assemble_gate", c) == 0
+    assert np.array_equal(st.kv, kv0)
+    assert np.array_equal(st.ks, st.kt)
+
+
+def test_assembly_ceiling_and_floor(oracle):
+    c = cfg_pp81(kd_max=2.0e-5, kv_max=3.0e-4, kt_bg=1.5e-5, ks_bg=1.5e-5)
+    st = state(oracle)
+    st.rho[...] = 1030.0
+    for k in range(NZ):
+        st.u[:, :, k] = 0.05 * k
+    st.call("vpo_pp81", c)
+    st.call("vpo_split", c)
+    st.call("vpo_assemble_gate", c)
+    assert st.kt[:, :, 1:NZ].max() <= 2.0e-5 and st.kv[:, :, 1:NZ].max() <= 3.0e-4
+    assert st.kt[:, :, 1:NZ].min() >= 1.5e-5
+
+
+def test_guard_flags_negative_before_the_clip(oracle):
+    c = cfg_pp81(vmix_guard=1)
+    st = state(oracle)
+    st.kv[:, :, 2] = -1.0
+    assert st.call("vpo_assemble_gate", c) == 1
+    assert st.kv[:, :, 2].min() >= c.kv_bg        # then floored, as the reference does
+
+
+def test_bryan_lewis_profile_shape(oracle):
+    c = cfg_pp81(bkgnd_profile=1)
+    nz = 60
+    st = state(oracle, nz=nz, h=100.0)
+    st.kv[...] = 0.0
+    st.kt[...] = 0.0
+    st.ks[...] = 0.0
+    st.call("vpo_assemble_gate", c)
+    depth = np.array([(nz - k) * 100.0 for k in range(nz + 1)])
+    kd = st.kt[6, 5, :]
+    assert abs(kd[nz - 1] - c.bkgnd_kd_sfc) < 0.05 * (c.bkgnd_kd_deep - c.bkgnd_kd_sfc)
+    assert abs(kd[1] - c.bkgnd_kd_deep) < 0.1 * (c.bkgnd_kd_deep - c.bkgnd_kd_sfc)
+    kz = int(np.argmin(np.abs(depth - c.bkgnd_z0)))
+    assert abs(kd[kz] - 0.5 * (c.bkgnd_kd_sfc + c.bkgnd_kd_deep)) < 1e-12
+    assert np.all(np.diff(kd[1:nz]) <= 0.0)        # deeper -> larger
+    np.testing.assert_array_equal(st.kv[6, 5, 1:nz], kd[1:nz])   # kv floor = 1 * kd_bg
+
+
+def test_wright_eos_reference_value(oracle):
+    c = cfg_pp81()
+    st = state(oracle, nz=1, ntr=2)
+    st.tracers[0][...] = 35.0
+    st.tracers[1][...] = 10.0
+    st.call("vpo_eos_wright", c)
+    # test_ocean_wright_eos.F90:87-107: within 0.5 of 1027 kg/m3 at (10 C, 35 psu, 0 Pa)
+    assert abs(st.rho[0, 0, 0] - 1027.0) < 0.5
+    st.tracers[0][...] = 0.0
+    st.tracers[1][...] = 0.0
+    st.call("vpo_eos_wright", c)
+    # test_ocean_wright_eos.F90:125-130: pure water at 0 C within 0.5 of 999.7 kg/m3
+    assert abs(st.rho[0, 0, 0] - 999.7) < 0.5
+    st.h[...] = 0.0
+    st.call("vpo_eos_wright", c)
+    assert np.all(st.rho == c.rho0)
