@@ -95,13 +95,19 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
 
     const double rho0 = c.rho0;
 
-    // first live layer from the top (rdb_vl_first_live)
+    // first live layer from the top (rdb_vl_first_live); a column whose every
+    // layer is exactly 0 m thick (land) is noted: its pass-1 walk finds no
+    // crossing whatever rho holds (every delta_d is 0), so h_b = sum(h) = 0
     int k_sfc = nz;
+    bool all_zero = true;
     for (int k = nz; k >= 1; --k) {
-        if (HH(k) > H_VANISHED) {
+        const double hk = HH(k);
+        if (hk > H_VANISHED) {
             k_sfc = k;
+            all_zero = false;
             break;
         }
+        all_zero = all_zero && (hk == 0.0);
     }
 
     double h_b = p.bl_depth[col];   // lagged BL depth (state)
@@ -118,47 +124,49 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
             const double wstar3_lagged = fmx(0.0, -B_0) * h_b;
             const double cb = sm_cbrt(wstar3_lagged);
             const double w_s_col = sqrt(u_star * u_star + cb * cb);
-            const double u_ref = UC(k_sfc);
-            const double v_ref = VC(k_sfc);
-            const double b_ref = -(GRAVITY * RR(k_sfc) / rho0);
-            const double h_sfc = HH(k_sfc);
-            const double d_centre_ref = 0.5 * h_sfc;
-            const double vt2_coef = c.c_vt2 / c.ri_crit;
-            double ri_prev = 0.0, d_prev = d_centre_ref, d_centre_k = d_centre_ref;
-            double h_above = h_sfc;
-            bool crossing_found = false;
-            double hb_new = 0.0;
-            for (int k = k_sfc - 1; k >= 1; --k) {
-                const double h_k = HH(k);
-                d_centre_k = d_centre_k + 0.5 * (h_above + h_k);
-                const double u_k = UC(k);
-                const double v_k = VC(k);
-                const double b_k = -(GRAVITY * RR(k) / rho0);
-                const double delta_d = d_centre_k - d_centre_ref;
-                const double delta_b = b_ref - b_k;
-                const double n_brunt = sqrt(fmx(0.0, xdiv(delta_b, delta_d)));
-                const double vt2 = vt2_coef * d_centre_k * n_brunt * w_s_col;
-                const double shear2 =
-                    fmx((u_k - u_ref) * (u_k - u_ref) + (v_k - v_ref) * (v_k - v_ref) + vt2, c.shear2_floor);
-                const double ri_bulk = xdiv(delta_b * delta_d, shear2);
-                if (ri_bulk >= c.ri_crit) {
-                    const double denom = ri_bulk - ri_prev;
-                    double frac;
-                    if (fabs(denom) > 1.0e-12)
-                        frac = xdiv(c.ri_crit - ri_prev, denom);
-                    else
-                        frac = 0.5;
-                    hb_new = d_prev + frac * (d_centre_k - d_prev);
-                    crossing_found = true;
-                    break;
+            double hb_new = 0.0;   // all-zero column: no crossing, sum of zeros
+            if (!all_zero) {
+                const double u_ref = UC(k_sfc);
+                const double v_ref = VC(k_sfc);
+                const double b_ref = -(GRAVITY * RR(k_sfc) / rho0);
+                const double h_sfc = HH(k_sfc);
+                const double d_centre_ref = 0.5 * h_sfc;
+                const double vt2_coef = c.c_vt2 / c.ri_crit;
+                double ri_prev = 0.0, d_prev = d_centre_ref, d_centre_k = d_centre_ref;
+                double h_above = h_sfc;
+                bool crossing_found = false;
+                for (int k = k_sfc - 1; k >= 1; --k) {
+                    const double h_k = HH(k);
+                    d_centre_k = d_centre_k + 0.5 * (h_above + h_k);
+                    const double u_k = UC(k);
+                    const double v_k = VC(k);
+                    const double b_k = -(GRAVITY * RR(k) / rho0);
+                    const double delta_d = d_centre_k - d_centre_ref;
+                    const double delta_b = b_ref - b_k;
+                    const double n_brunt = sqrt(fmx(0.0, xdiv(delta_b, delta_d)));
+                    const double vt2 = vt2_coef * d_centre_k * n_brunt * w_s_col;
+                    const double shear2 =
+                        fmx((u_k - u_ref) * (u_k - u_ref) + (v_k - v_ref) * (v_k - v_ref) + vt2, c.shear2_floor);
+                    const double ri_bulk = xdiv(delta_b * delta_d, shear2);
+                    if (ri_bulk >= c.ri_crit) {
+                        const double denom = ri_bulk - ri_prev;
+                        double frac;
+                        if (fabs(denom) > 1.0e-12)
+                            frac = xdiv(c.ri_crit - ri_prev, denom);
+                        else
+                            frac = 0.5;
+                        hb_new = d_prev + frac * (d_centre_k - d_prev);
+                        crossing_found = true;
+                        break;
+                    }
+                    ri_prev = ri_bulk;
+                    d_prev = d_centre_k;
+                    h_above = h_k;
                 }
-                ri_prev = ri_bulk;
-                d_prev = d_centre_k;
-                h_above = h_k;
-            }
-            if (!crossing_found) {
-                hb_new = 0.0;
-                for (int k = 1; k <= k_sfc; ++k) hb_new = hb_new + HH(k);
+                if (!crossing_found) {
+                    hb_new = 0.0;
+                    for (int k = 1; k <= k_sfc; ++k) hb_new = hb_new + HH(k);
+                }
             }
             h_b = hb_new;
             p.bl_depth[col] = h_b;
@@ -193,24 +201,50 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
 
     double depth = 0.0;   // sum of h over layers nz..q (interface q's depth)
     double d_run = 0.0;   // sum of h over layers k_sfc..q (KPP pass 2)
-    double h_c = HH(nz), r_c = RR(nz), uc_c = UC(nz), vc_c = VC(nz);
+    // Layer values (rho, cell-centred u and v) are loaded only for interfaces
+    // that use them: an interface between two 0-thickness layers (land,
+    // below-bathymetry fillers) takes PP81's background branch and never
+    // reads them.  The Bryan-Lewis value depends on the interface depth
+    // alone, so it is re-evaluated only when the depth changes (it stays
+    // constant through the fillers under the bathymetry).
+    double h_c = HH(nz), r_c = 0.0, uc_c = 0.0, vc_c = 0.0;
+    bool have_c = false;
+    double kdb_depth = 0.0, kdb_cached = 0.0;
+    bool kdb_valid = false;
     unsigned bad = 0;
     for (int q = nz; q >= 1; --q) {
         depth = depth + h_c;
         if (q <= k_sfc) d_run = d_run + h_c;
         double kvq = 0.0, ktq = 0.0, kdb = 0.0;
         double h_m = 0.0, r_m = 0.0, uc_m = 0.0, vc_m = 0.0;
+        bool have_m = false;
         if (q >= 2) {
             h_m = HH(q - 1);
-            r_m = RR(q - 1);
-            if (c.bkgnd_profile)
-                kdb = c.bkgnd_kd_sfc +
-                      (c.bkgnd_kd_deep - c.bkgnd_kd_sfc) * (0.5 + sm_atan(xdiv(depth - c.bkgnd_z0, c.bkgnd_delta)) * inv_pi);
-            if (pp81) {
-                // ---- PP81 (rdb_ocean_vmix.F90:1046-1073) ----
+            if (c.bkgnd_profile) {
+                if (!(kdb_valid && depth == kdb_depth)) {
+                    kdb_cached = c.bkgnd_kd_sfc + (c.bkgnd_kd_deep - c.bkgnd_kd_sfc) *
+                                                      (0.5 + sm_atan(xdiv(depth - c.bkgnd_z0, c.bkgnd_delta)) * inv_pi);
+                    kdb_depth = depth;
+                    kdb_valid = true;
+                }
+                kdb = kdb_cached;
+            }
+            const double dz_face = 0.5 * (h_m + h_c);
+            const bool need_layers = (pp81 && !(dz_face <= 0.0)) || (c.conv_enable && !(dz_face <= H_VANISHED));
+            if (need_layers) {
+                if (!have_c) {
+                    r_c = RR(q);
+                    uc_c = UC(q);
+                    vc_c = VC(q);
+                    have_c = true;
+                }
+                r_m = RR(q - 1);
                 uc_m = UC(q - 1);
                 vc_m = VC(q - 1);
-                const double dz_face = 0.5 * (h_m + h_c);
+                have_m = true;
+            }
+            if (pp81) {
+                // ---- PP81 (rdb_ocean_vmix.F90:1046-1073) ----
                 if (dz_face <= 0.0) {
                     kvq = c.pp81_nu_bg;
                     ktq = c.pp81_kappa_bg;
@@ -301,6 +335,7 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
         r_c = r_m;
         uc_c = uc_m;
         vc_c = vc_m;
+        have_c = have_m;
     }
     if (bad) atomicAdd(p.guard_count, (unsigned long long)bad);
 #undef HH
@@ -458,6 +493,14 @@ __device__ __forceinline__ void solve_face(const Params &p, double dt, int i, in
     // value can never index outside it (valid input: a no-op)
     const int kb = kbp ? min(max(kbp[f], 1), nz) : 1;
     const int ktop = ktp ? min(max(ktp[f], 1), nz) : nz;
+    // A face touching land whose velocity is zero in every layer keeps it:
+    // with a zero right-hand side every Thomas quantity is a zero, so the
+    // solve is skipped (unless the remnant or the stress fold is wanted).
+    if (!c.remnant && !c.implicit_stress && fmn(p.wet[cl], p.wet[cr]) == 0.0) {
+        bool zero = true;
+        for (int k = 1; k <= nz && zero; ++k) zero = (uf[PF * (size_t)(k - 1)] == 0.0);
+        if (zero) return;
+    }
     double kv_bbl = 0.0, bbl_thick = c.hbbl_visc;
     if (c.bbl_glue) {
         kv_bbl = c.bbl_piston * c.hbbl_visc;
