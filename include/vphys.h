@@ -141,6 +141,10 @@ typedef struct vphys_config {
     int eos_in_step;          /* 1: vphys_step runs the Wright EOS first */
     int remnant;              /* 1: momentum also writes visc_rem_u/v */
     int budgets;              /* 1: tracers accumulate heat/salt budgets */
+    int mixed_precision;      /* 0: FP64 throughout (bitwise the reference's arithmetic);
+                                 1: FP64 assembly, FP32 Thomas sweeps + FP64 residual correction;
+                                 2: as 1 with the assembly's interface sweep in FP32 too */
+    int pad1;
 } vphys_config;
 
 /* ---- field ids (vphys_bind / vphys_set_field / vphys_get_field) ----- */

@@ -119,10 +119,11 @@ class VphysConfig(ctypes.Structure):
         ("hbbl_visc", ctypes.c_double), ("bbl_piston", ctypes.c_double), ("kv_bbl_bg", ctypes.c_double),
         ("idx_temperature", ctypes.c_int), ("idx_salinity", ctypes.c_int), ("idx_pseudo_salt", ctypes.c_int),
         ("eos_in_step", ctypes.c_int), ("remnant", ctypes.c_int), ("budgets", ctypes.c_int),
+        ("mixed_precision", ctypes.c_int), ("pad1", ctypes.c_int),
     ]
 
     def as_dict(self):
-        return {n: getattr(self, n) for n, _ in self._fields_ if n != "pad0"}
+        return {n: getattr(self, n) for n, _ in self._fields_ if n not in ("pad0", "pad1")}
 
 
 class LibraryNotFoundError(FileNotFoundError):

@@ -2,9 +2,11 @@
 
     python -m roundabout_b200.build [--verbose]
 
-The kernels are compiled with -fmad=false: no a*b+c contraction, so every
-column's FP64 result is bit-identical to the CPU restatement of the
-reference (which its CPU builds compile with -ffp-contract=off).
+The exact kernels are compiled with -fmad=false: no a*b+c contraction, so
+every column's FP64 result is bit-identical to the CPU restatement of the
+reference (which its CPU builds compile with -ffp-contract=off).  The
+mixed-precision solves (vphys_mixed.cu) have no bitwise contract and keep
+FMA contraction.
 """
 from __future__ import annotations
 
@@ -17,12 +19,13 @@ from pathlib import Path
 CSRC = Path(__file__).resolve().parent / "csrc"
 OUT = CSRC / "_build"
 LIB = OUT / "libvphys.so"
-SOURCES = ["vphys_api.cu", "vphys_kernels.cu", "vphys_tracers.cu", "vphys_static.cu"]
-HEADERS = ["vphys_device.cuh", "vphys_kernels.cuh", "../../include/vphys.h"]
+SOURCES = ["vphys_api.cu", "vphys_kernels.cu", "vphys_tracers.cu", "vphys_static.cu", "vphys_mixed.cu"]
+HEADERS = ["vphys_device.cuh", "vphys_faces.cuh", "vphys_kernels.cuh", "../../include/vphys.h"]
+# the mixed-precision solves carry no bitwise contract: FMA contraction allowed
+CONTRACT_OK = {"vphys_mixed.cu"}
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
-         "--expt-relaxed-constexpr"]
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2", "--expt-relaxed-constexpr"]
 
 
 def nvcc() -> str:
@@ -46,7 +49,8 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     objs = []
     for s in SOURCES:
         obj = OUT / (Path(s).stem + ".o")
-        cmd = [nvcc(), *ARCH, *FLAGS, "-c", str(CSRC / s), "-o", str(obj)]
+        fmad = "-fmad=true" if s in CONTRACT_OK else "-fmad=false"
+        cmd = [nvcc(), *ARCH, *FLAGS, fmad, "-c", str(CSRC / s), "-o", str(obj)]
         if verbose:
             cmd += ["-Xptxas", "-v"]
         r = subprocess.run(cmd, capture_output=True, text=True)

@@ -75,6 +75,7 @@ def default_config() -> VphysConfig:
     c.eos_in_step = 0
     c.remnant = 0
     c.budgets = 0
+    c.mixed_precision = 0
     return c
 
 

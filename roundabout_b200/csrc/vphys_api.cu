@@ -204,6 +204,9 @@ int validate(const vphys_config *c, int ntr)
     if (c->idx_temperature >= 0 && c->idx_temperature == c->idx_salinity)
         return push_error(VPHYS_ERR_CONFIG, "temperature and salinity must be different tracers");
     if (c->kd_smooth_iterations < 0) return push_error(VPHYS_ERR_CONFIG, "kd_smooth_iterations < 0");
+    if (c->mixed_precision < 0 || c->mixed_precision > 2)
+        return push_error(VPHYS_ERR_CONFIG, "mixed_precision %d: 0 (FP64), 1 (mixed solves) or 2 (mixed solves and assembly)",
+                          c->mixed_precision);
     if (c->rho0 <= 0.0 || c->cp <= 0.0) return push_error(VPHYS_ERR_CONFIG, "rho0 and cp must be positive");
     if (c->use_kpp && c->ri_crit <= 0.0) return push_error(VPHYS_ERR_CONFIG, "ri_crit must be positive");
     if (c->bkgnd_profile && c->bkgnd_delta == 0.0) return push_error(VPHYS_ERR_CONFIG, "bkgnd_delta must be nonzero");

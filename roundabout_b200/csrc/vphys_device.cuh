@@ -68,6 +68,19 @@ __device__ __forceinline__ double qdiv(double a, const Rcp &r)
 // Fortran MAX/MIN (finite operands); the same ternary as the CPU restatement.
 __device__ __forceinline__ double fmx(double a, double b) { return a > b ? a : b; }
 __device__ __forceinline__ double fmn(double a, double b) { return a < b ? a : b; }
+__device__ __forceinline__ float fmx(float a, float b) { return a > b ? a : b; }
+__device__ __forceinline__ float fmn(float a, float b) { return a < b ? a : b; }
+
+// Precision-generic spellings used by the templated kernels: for double they
+// are the exact helpers above (value-identical to a/b); for float (the
+// mixed-precision path, no bitwise contract) the hardware fast forms.
+__device__ __forceinline__ double rdiv(double a, double b) { return xdiv(a, b); }
+__device__ __forceinline__ float rdiv(float a, float b) { return __fdividef(a, b); }
+struct RcpF {
+    float y;
+};
+__device__ __forceinline__ RcpF rcp_of(float b) { return RcpF{__frcp_rn(b)}; }
+__device__ __forceinline__ float qdiv(float a, const RcpF &r) { return a * r.y; }
 
 // ---- position-independent cube root: rdb_sm_cbrt
 // (rdb_safe_math_pow.inc:107-142): exponent split modulo 3, degree-4 seed on
@@ -128,6 +141,9 @@ __device__ __forceinline__ double sm_atan(double x)
     return y;
 }
 
+__device__ __forceinline__ double ratan(double x) { return sm_atan(x); }
+__device__ __forceinline__ float ratan(float x) { return atanf(x); }
+
 // face_thick (rdb_ocean_vdiff.F90:1928-1962)
 __device__ __forceinline__ double face_thick(double ha, double hb, bool use_harmonic)
 {
@@ -137,6 +153,15 @@ __device__ __forceinline__ double face_thick(double ha, double hb, bool use_harm
         return 0.5 * sum_h;
     }
     return 0.5 * (ha + hb);
+}
+__device__ __forceinline__ float face_thick(float ha, float hb, bool use_harmonic)
+{
+    if (use_harmonic) {
+        const float sum_h = ha + hb;
+        if (sum_h > 1.0e-30f) return __fdividef(2.0f * ha * hb, sum_h);
+        return 0.5f * sum_h;
+    }
+    return 0.5f * (ha + hb);
 }
 
 // rdb_conc_add_source (rdb_tracer_conc.inc:36-53)

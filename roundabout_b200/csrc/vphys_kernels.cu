@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include "vphys_device.cuh"
+#include "vphys_faces.cuh"
 #include "vphys_kernels.cuh"
 
 namespace vphys {
@@ -72,6 +73,7 @@ __global__ void k_stress_mag(const Params p, double *out)
 // ---------------------------------------------------------------------------
 constexpr int ASM_THREADS = 128;
 
+template <typename R>
 __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -180,15 +182,25 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
         kpp_active = (h_b > 0.0 && w_s > 0.0);
     }
 
+    // ---- the interface sweep, in R (double: the exact path; float: the
+    //      mixed-precision path, whose KPP pass 1 above stays FP64) ----
+    const R r0 = (R)rho0, G = (R)GRAVITY;
+    const R nu_bg = (R)c.pp81_nu_bg, kap_bg = (R)c.pp81_kappa_bg, nu0 = (R)c.pp81_nu0, alpha81 = (R)c.pp81_alpha;
+    const R shear2_floor = (R)c.shear2_floor;
+    const R kd_sfc = (R)c.bkgnd_kd_sfc, kd_deep = (R)c.bkgnd_kd_deep, z0 = (R)c.bkgnd_z0, bdelta = (R)c.bkgnd_delta;
+    const R kv_max = (R)c.kv_max, kd_max = (R)c.kd_max, kt_bg = (R)c.kt_bg, ks_bg = (R)c.ks_bg;
+    const R cs = (R)c.cs_nonlocal, qT = (R)q_T_kin, qS = (R)q_S_kin, hbR = (R)h_b, wsR = (R)w_s;
+    const R invz2 = (R)c.kv_ml_invz2, conv_kd = (R)c.conv_kd, conv_pr = (R)c.conv_prandtl, conv_n2 = (R)c.conv_n2_thresh;
     // gate constants (vmix_assemble, rdb_ocean_vmix.F90:2279-2348)
-    const double pr_bl = (c.bkgnd_prandtl > 0.0) ? c.bkgnd_prandtl : 1.0;
-    const double kv_floor_scalar = (c.bkgnd_prandtl > 0.0) ? c.bkgnd_prandtl * c.kt_bg + c.kv_bg : c.kv_bg;
-    const double inv_pi = 1.0 / PI_D;
+    const R pr_bl = (R)((c.bkgnd_prandtl > 0.0) ? c.bkgnd_prandtl : 1.0);
+    const R kv_floor_scalar = (R)((c.bkgnd_prandtl > 0.0) ? c.bkgnd_prandtl * c.kt_bg + c.kv_bg : c.kv_bg);
+    const R inv_pi = (R)(1.0 / PI_D);
     const bool pp81 = (c.interior_closure == VPHYS_INTERIOR_PP81);
     bool invz2_on = (c.kv_ml_invz2 > 0.0 && c.hmix_fixed > 0.0);
-    const double hmix = c.hmix_fixed;
-    const double hmix_sq = hmix * hmix;
-    const double dz_min_safe = 0.5 * hmix / (double)(nz > 1 ? nz : 1);
+    const R hmix = (R)c.hmix_fixed;
+    const R hmix_sq = hmix * hmix;
+    const R dz_min_safe = rdiv(R(0.5) * hmix, (R)(nz > 1 ? nz : 1));
+    const R HV = (R)H_VANISHED;
 
     // surface interface (k = nz+1): closed, every contributor leaves it at 0
     kvp[P * (size_t)nz] = 0.0;
@@ -199,38 +211,42 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
         p.gamma_s[col + P * (size_t)nz] = 0.0;
     }
 
-    double depth = 0.0;   // sum of h over layers nz..q (interface q's depth)
-    double d_run = 0.0;   // sum of h over layers k_sfc..q (KPP pass 2)
+    R depth = 0;   // sum of h over layers nz..q (interface q's depth)
+    R d_run = 0;   // sum of h over layers k_sfc..q (KPP pass 2)
     // Layer values (rho, cell-centred u and v) are loaded only for interfaces
     // that use them: an interface between two 0-thickness layers (land,
     // below-bathymetry fillers) takes PP81's background branch and never
     // reads them.  The Bryan-Lewis value depends on the interface depth
     // alone, so it is re-evaluated only when the depth changes (it stays
     // constant through the fillers under the bathymetry).
-    double h_c = HH(nz), r_c = 0.0, uc_c = 0.0, vc_c = 0.0;
+    // rho and the cell-centred velocities stay FP64 in either precision: their
+    // differences across an interface are formed in FP64 (a density step of
+    // 1e-3 on 1027 would keep only 3 digits in FP32) and only then rounded to R
+    R h_c = (R)HH(nz);
+    double r_c = 0, uc_c = 0, vc_c = 0;
     bool have_c = false;
-    double kdb_depth = 0.0, kdb_cached = 0.0;
+    R kdb_depth = 0, kdb_cached = 0;
     bool kdb_valid = false;
     unsigned bad = 0;
     for (int q = nz; q >= 1; --q) {
         depth = depth + h_c;
         if (q <= k_sfc) d_run = d_run + h_c;
-        double kvq = 0.0, ktq = 0.0, kdb = 0.0;
-        double h_m = 0.0, r_m = 0.0, uc_m = 0.0, vc_m = 0.0;
+        R kvq = 0, ktq = 0, kdb = 0;
+        R h_m = 0;
+        double r_m = 0, uc_m = 0, vc_m = 0;
         bool have_m = false;
         if (q >= 2) {
-            h_m = HH(q - 1);
+            h_m = (R)HH(q - 1);
             if (c.bkgnd_profile) {
                 if (!(kdb_valid && depth == kdb_depth)) {
-                    kdb_cached = c.bkgnd_kd_sfc + (c.bkgnd_kd_deep - c.bkgnd_kd_sfc) *
-                                                      (0.5 + sm_atan(xdiv(depth - c.bkgnd_z0, c.bkgnd_delta)) * inv_pi);
+                    kdb_cached = kd_sfc + (kd_deep - kd_sfc) * (R(0.5) + ratan(rdiv(depth - z0, bdelta)) * inv_pi);
                     kdb_depth = depth;
                     kdb_valid = true;
                 }
                 kdb = kdb_cached;
             }
-            const double dz_face = 0.5 * (h_m + h_c);
-            const bool need_layers = (pp81 && !(dz_face <= 0.0)) || (c.conv_enable && !(dz_face <= H_VANISHED));
+            const R dz_face = R(0.5) * (h_m + h_c);
+            const bool need_layers = (pp81 && !(dz_face <= R(0))) || (c.conv_enable && !(dz_face <= HV));
             if (need_layers) {
                 if (!have_c) {
                     r_c = RR(q);
@@ -245,20 +261,20 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
             }
             if (pp81) {
                 // ---- PP81 (rdb_ocean_vmix.F90:1046-1073) ----
-                if (dz_face <= 0.0) {
-                    kvq = c.pp81_nu_bg;
-                    ktq = c.pp81_kappa_bg;
+                if (dz_face <= R(0)) {
+                    kvq = nu_bg;
+                    ktq = kap_bg;
                 } else {
-                    const Rcp rdz = rcp_of(dz_face);
-                    const double du_dz = qdiv(uc_c - uc_m, rdz);
-                    const double dv_dz = qdiv(vc_c - vc_m, rdz);
-                    const double shear2 = fmx(du_dz * du_dz + dv_dz * dv_dz, c.shear2_floor);
-                    const double n2 = -xdiv(GRAVITY * (r_c - r_m), rho0 * dz_face);
-                    const double ri = xdiv(n2, shear2);
-                    const double denom = 1.0 + c.pp81_alpha * fmx(ri, 0.0);
-                    const double ri_factor = 1.0 / (denom * denom);
-                    kvq = c.pp81_nu_bg + c.pp81_nu0 * ri_factor;
-                    ktq = c.pp81_kappa_bg + c.pp81_nu0 * ri_factor / denom;
+                    const auto rdz = rcp_of(dz_face);
+                    const R du_dz = qdiv((R)(uc_c - uc_m), rdz);
+                    const R dv_dz = qdiv((R)(vc_c - vc_m), rdz);
+                    const R shear2 = fmx(du_dz * du_dz + dv_dz * dv_dz, shear2_floor);
+                    const R n2 = -rdiv(G * (R)(r_c - r_m), r0 * dz_face);
+                    const R ri = rdiv(n2, shear2);
+                    const R denom = R(1) + alpha81 * fmx(ri, R(0));
+                    const R ri_factor = rdiv(R(1), denom * denom);
+                    kvq = nu_bg + nu0 * ri_factor;
+                    ktq = kap_bg + rdiv(nu0 * ri_factor, denom);
                 }
             } else if (c.bkgnd_profile) {
                 // ---- interior "none" seed (rdb_ocean_vmix.F90:779-797) ----
@@ -266,21 +282,21 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
                 ktq = kdb;
             } else {
                 kvq = kv_floor_scalar;
-                ktq = c.kt_bg;
+                ktq = kt_bg;
             }
         }
         // ---- KPP overlay (rdb_ocean_vmix.F90:1496-1514) ----
-        double gt = 0.0, gs = 0.0;
-        if (kpp_active && q > 1 && q <= k_sfc && d_run < h_b) {
-            const double sigma = xdiv(d_run, h_b);
-            const double g_shape = sigma * (1.0 - sigma) * (1.0 - sigma);
-            const double kv_kpp = h_b * w_s * g_shape;
+        R gt = 0, gs = 0;
+        if (kpp_active && q > 1 && q <= k_sfc && d_run < hbR) {
+            const R sigma = rdiv(d_run, hbR);
+            const R g_shape = sigma * (R(1) - sigma) * (R(1) - sigma);
+            const R kv_kpp = hbR * wsR * g_shape;
             kvq = fmx(kvq, kv_kpp);
             ktq = fmx(ktq, kv_kpp);
             if (destabilizing) {
-                const double gamma_factor = c.cs_nonlocal * g_shape;
-                gt = gamma_factor * q_T_kin;
-                gs = gamma_factor * q_S_kin;
+                const R gamma_factor = cs * g_shape;
+                gt = gamma_factor * qT;
+                gs = gamma_factor * qS;
             }
         }
         if (q >= 2) {
@@ -289,47 +305,47 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
                 if (depth >= hmix) {
                     invz2_on = false;
                 } else {
-                    const double zz = fmx(depth, dz_min_safe);
-                    kvq = kvq + c.kv_ml_invz2 * hmix_sq / (zz * zz);
+                    const R zz = fmx(depth, dz_min_safe);
+                    kvq = kvq + rdiv(invz2 * hmix_sq, zz * zz);
                 }
             }
             // ---- convection (rdb_ocean_vmix.F90:1835-1848) ----
             if (c.conv_enable) {
-                const double dz_face = 0.5 * (h_m + h_c);
-                if (!(dz_face <= H_VANISHED) && !(depth < h_b)) {
-                    const double n2 = -xdiv(GRAVITY * (r_c - r_m), rho0 * dz_face);
-                    if (n2 < c.conv_n2_thresh) {
-                        ktq = fmx(ktq, c.conv_kd);
-                        kvq = fmx(kvq, c.conv_prandtl * c.conv_kd);
+                const R dz_face = R(0.5) * (h_m + h_c);
+                if (!(dz_face <= HV) && !(depth < hbR)) {
+                    const R n2 = -rdiv(G * (R)(r_c - r_m), r0 * dz_face);
+                    if (n2 < conv_n2) {
+                        ktq = fmx(ktq, conv_kd);
+                        kvq = fmx(kvq, conv_pr * conv_kd);
                     }
                 }
             }
         }
         // ---- split ks := kt, then the gate on interior interfaces ----
-        double ksq = ktq;
+        R ksq = ktq;
         if (q >= 2 && q <= nz) {
             if (c.vmix_guard) {
-                bad += (kvq < 0.0 || kvq != kvq);
-                bad += (ktq < 0.0 || ktq != ktq);
-                bad += (ksq < 0.0 || ksq != ksq);
+                bad += (kvq < R(0) || kvq != kvq);
+                bad += (ktq < R(0) || ktq != ktq);
+                bad += (ksq < R(0) || ksq != ksq);
             }
             if (c.bkgnd_profile) {
-                kvq = fmn(fmx(kvq, pr_bl * kdb), c.kv_max);
-                ktq = fmn(fmx(ktq, kdb), c.kd_max);
-                ksq = fmn(fmx(ksq, kdb), c.kd_max);
+                kvq = fmn(fmx(kvq, pr_bl * kdb), kv_max);
+                ktq = fmn(fmx(ktq, kdb), kd_max);
+                ksq = fmn(fmx(ksq, kdb), kd_max);
             } else {
-                kvq = fmn(fmx(kvq, kv_floor_scalar), c.kv_max);
-                ktq = fmn(fmx(ktq, c.kt_bg), c.kd_max);
-                ksq = fmn(fmx(ksq, c.ks_bg), c.kd_max);
+                kvq = fmn(fmx(kvq, kv_floor_scalar), kv_max);
+                ktq = fmn(fmx(ktq, kt_bg), kd_max);
+                ksq = fmn(fmx(ksq, ks_bg), kd_max);
             }
         }
         const size_t off = P * (size_t)(q - 1);
-        kvp[off] = kvq;
-        ktp[off] = ktq;
-        ksp[off] = ksq;
+        kvp[off] = (double)kvq;
+        ktp[off] = (double)ktq;
+        ksp[off] = (double)ksq;
         if (p.write_gamma) {
-            p.gamma_t[col + off] = gt;
-            p.gamma_s[col + off] = gs;
+            p.gamma_t[col + off] = (double)gt;
+            p.gamma_s[col + off] = (double)gs;
         }
         h_c = h_m;
         r_c = r_m;
@@ -389,67 +405,6 @@ __global__ void k_smooth(const Params p, double *__restrict__ fld, const double 
 // Momentum: one thread per (u face, v face) pair.
 // ---------------------------------------------------------------------------
 constexpr int MOM_THREADS = 128;
-
-__device__ __forceinline__ void face_layer(const vphys_config &c, double hl_c, double hr_c, double u_k, int k, int kb,
-                                           double d_min, double i_hbbl, double &zacc, double &zcol_l,
-                                           double &zcol_r, double &hvel, double &zint)
-{
-    // vdiff_face_layer (rdb_ocean_vdiff.F90:1964-2056)
-    zint = 0.0;
-    if (c.hvel_mom6 && !c.hvel_harmonic) {
-        const double h_harm = xdiv(2.0 * hl_c * hr_c, hl_c + hr_c + EPS_HVEL);
-        const double h_arith = 0.5 * (hl_c + hr_c);
-        const double h_delta = hr_c - hl_c;
-        zcol_l = zcol_l + hl_c;
-        zcol_r = zcol_r + hr_c;
-        if (k >= kb) zacc = zacc + h_harm;
-        const double z_clear = fmx(zcol_l, zcol_r) + d_min;
-        zint = fmx(zacc, z_clear) * i_hbbl;
-        hvel = h_arith;
-        if (u_k * h_delta > 0.0) {
-            const double z2 = zint;
-            const double botfn = 1.0 / (1.0 + 0.09 * z2 * z2 * z2 * z2 * z2 * z2);
-            hvel = (1.0 - botfn) * h_arith + botfn * h_harm;
-        }
-    } else if (c.hvel_mom6) {
-        const double h_harm = xdiv(2.0 * hl_c * hr_c, hl_c + hr_c + EPS_HVEL);
-        const double h_arith = 0.5 * (hl_c + hr_c);
-        const double h_delta = hr_c - hl_c;
-        hvel = h_harm;
-        if (c.hvel_upwind && u_k * h_delta < 0.0) {
-            const double z2 = zacc;
-            const double botfn = 1.0 / (1.0 + 0.09 * z2 * z2 * z2 * z2 * z2 * z2);
-            hvel = (1.0 - botfn) * h_harm + botfn * h_arith;
-        }
-        if (k >= kb) zacc = zacc + h_harm * i_hbbl;
-        zint = zacc;
-    } else {
-        hvel = 0.5 * (hl_c + hr_c);
-    }
-    if (c.zlevel_faces) hvel = fmn(hl_c, hr_c);
-}
-
-__device__ __forceinline__ void interface_coupling(const vphys_config &c, double hv_lo, double hv_hi, double zint_lo,
-                                                   double dt, double kv_bbl, double bbl_thick, double kv_l,
-                                                   double kv_r, double &num, double &dz, bool &cut)
-{
-    // vdiff_interface_coupling (rdb_ocean_vdiff.F90:2058-2115)
-    const double hf_lo = fmx(hv_lo, H_VANISHED);
-    const double hf_hi = fmx(hv_hi, H_VANISHED);
-    if (c.hvel_mom6)
-        dz = 0.5 * (hf_lo + hf_hi);
-    else
-        dz = face_thick(hf_lo, hf_hi, c.use_harmonic);
-    double nu_f = 0.5 * (kv_l + kv_r);
-    if (c.bbl_glue) {
-        const double z = zint_lo;
-        const double botfn_int = 1.0 / (1.0 + 0.09 * z * z * z * z * z * z);
-        nu_f = fmx(0.0, nu_f + (kv_bbl - c.kv_bbl_bg) * botfn_int);
-        if (dz > bbl_thick) dz = (1.0 - botfn_int) * dz + botfn_int * bbl_thick;
-    }
-    num = dt * nu_f;
-    cut = c.zlevel_faces && (hv_lo <= H_VANISHED || hv_hi <= H_VANISHED);
-}
 
 constexpr int MOM_U = 4;   // levels per load block
 
@@ -526,7 +481,7 @@ __device__ __forceinline__ void solve_face(const Params &p, double dt, int i, in
     }
     double hv_p, zi_p;
     double u_k = uf[0];
-    face_layer(c, __ldg(hl), __ldg(hr), u_k, 1, kb, d_min, i_hbbl, zacc, zcol_l, zcol_r, hv_p, zi_p);
+    face_layer<double>(c, __ldg(hl), __ldg(hr), u_k, 1, kb, d_min, i_hbbl, zacc, zcol_l, zcol_r, hv_p, zi_p);
     double num_t = 0.0, dz_t = 1.0;
     bool cut_t = false;
     double cp_prev = 0.0, dp_prev = 0.0, gp_prev = 0.0;
@@ -556,9 +511,9 @@ __device__ __forceinline__ void solve_face(const Params &p, double dt, int i, in
                 double u_kp1 = 0.0;
                 if (k < nz) {
                     u_kp1 = un[q];
-                    face_layer(c, hln[q], hrn[q], u_kp1, k + 1, kb, d_min, i_hbbl, zacc, zcol_l, zcol_r, hv_p, zi_p);
+                    face_layer<double>(c, hln[q], hrn[q], u_kp1, k + 1, kb, d_min, i_hbbl, zacc, zcol_l, zcol_r, hv_p, zi_p);
                     if (k >= kb_live && k <= ktop)
-                        interface_coupling(c, hv_0, hv_p, zi_0, dt, kv_bbl, bbl_thick, kvln[q], kvrn[q], num_t, dz_t,
+                        interface_coupling<double>(c, hv_0, hv_p, zi_0, dt, kv_bbl, bbl_thick, kvln[q], kvrn[q], num_t, dz_t,
                                            cut_t);
                 }
                 double a_k = 0.0, b_k = 1.0, c_k = 0.0;
@@ -730,7 +685,10 @@ void launch_stress_mag(const Params &p, cudaStream_t stream)
 void launch_assemble(const Params &p, cudaStream_t stream)
 {
     dim3 grid((p.nx + ASM_THREADS - 1) / ASM_THREADS, p.ny);
-    k_assemble<<<grid, ASM_THREADS, 0, stream>>>(p);
+    if (p.cfg.mixed_precision >= 2)
+        k_assemble<float><<<grid, ASM_THREADS, 0, stream>>>(p);
+    else
+        k_assemble<double><<<grid, ASM_THREADS, 0, stream>>>(p);
 }
 
 void launch_smooth(const Params &p, double *fld, double *scratch, cudaStream_t stream)
@@ -745,6 +703,10 @@ void launch_smooth(const Params &p, double *fld, double *scratch, cudaStream_t s
 
 void launch_momentum(const Params &p, double dt, cudaStream_t stream)
 {
+    if (p.cfg.mixed_precision) {
+        launch_momentum_mp(p, dt, stream);
+        return;
+    }
     static bool attr_set = false;
     if (!attr_set) {
         cudaFuncSetAttribute(k_momentum, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -46,6 +46,9 @@ void launch_assemble(const Params &p, cudaStream_t stream);
 void launch_smooth(const Params &p, double *fld, double *scratch, cudaStream_t stream);
 void launch_momentum(const Params &p, double dt, cudaStream_t stream);
 void launch_tracers(const Params &p, double dt, bool diffuse, bool nonlocal, cudaStream_t stream);
+// mixed-precision solves (vphys_mixed.cu), dispatched by the two above when cfg.mixed_precision
+void launch_momentum_mp(const Params &p, double dt, cudaStream_t stream);
+void launch_tracers_mp(const Params &p, double dt, bool nonlocal, cudaStream_t stream);
 void launch_selftest_division(unsigned long long seed, long long per_thread, int emin, int erange,
                               unsigned long long *bad, cudaStream_t stream);
 

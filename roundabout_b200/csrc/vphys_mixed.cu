@@ -1,0 +1,506 @@
+// vphys_mixed.cu -- the mixed-precision form of the implicit solves: FP32
+// factorisation and sweeps, FP64 residual and FP64 forward accumulation.
+//
+// Each column solves A x = d (A = I + dt * vertical diffusion operator:
+// rdb_ocean_vdiff.F90:1248-1349 for tracers, 1611-1925 for momentum) for the
+// INCREMENT x = d + delta.  Row k scaled by its thickness H_k is the
+// conservative form
+//     (H_k + E_k + F_k + F_{k+1}) x_k - F_k x_{k-1} - F_{k+1} x_{k+1} = H_k rhs_k
+// with F_k = dt K_k / dz_k the coupling of interface k (alpha_k = F_{k+1}/H_k,
+// beta_k = F_k/H_k in the reference's rows) and E_k a diagonal extra (bottom
+// drag, BBL glue).  The increment solves the same matrix with the FP64
+// residual b = H rhs - (H + E + G) d, i.e. b_k = F_k (d_{k-1} - d_k) +
+// F_{k+1} (d_{k+1} - d_k) - E_k d_k (+ the wind stress), built from the SAME
+// FP32 couplings the factorisation uses, so the telescoping sum of the
+// internal fluxes cancels exactly and FP32 rounding only perturbs delta.
+//
+// The factorisation keeps, per row, the pivot p_k = s_k + F_{k+1}, its excess
+//     s_k = H_k + E_k + F_k q_{k-1}         (a sum of positive terms)
+// and BOTH complementary ratios u_k = F_{k+1}/p_k and q_k = s_k/p_k
+// (u + q = 1): across a stiff interface (F >> s: a 1 mm layer under KPP
+// mixing) u rounds to 1 in FP32 and only q carries the information, across a
+// weak one (F << s) it is the other way round, so each multiplication by
+// u_k is done as (1 - q_k)*z = z - q_k z when q_k < 1/2 and as u_k z
+// otherwise (t_k below: -q_k or u_k).  Then
+//     forward (FP64):  w_k = b_k + u_{k-1} w_{k-1},   v_k = w_k / p_k
+//     backward (FP32): delta_k = v_k + u_k delta_{k+1},   x_k = d_k + delta_k (FP64)
+//
+// Tracers: one warp per block, one lane per column.  The column's live span
+// of every tracer is staged into shared memory with per-lane asynchronous
+// copies (cp.async, 8 B per level, each warp-level copy one 256-B segment),
+// double-buffered so that tracer t+1 is in flight while tracer t is swept;
+// h and the diffusivity are staged the same way for the factorisation.
+// Every lane reads only its own column's shared-memory slots, so the kernel
+// needs no block barrier.
+//
+// Momentum: one thread per u or v face column; t and v in shared memory, the
+// velocity read again from L2 (evict_last) by the back-substitution.
+#include <cuda_runtime.h>
+
+#include "vphys_device.cuh"
+#include "vphys_faces.cuh"
+#include "vphys_kernels.cuh"
+
+namespace vphys {
+
+constexpr int MP_TR_COLS = 32;      // columns (lanes) per tracer block
+constexpr int MP_MOM_THREADS = 64;  // face columns per momentum block
+constexpr int MP_MOM_U = 4;         // levels per momentum load block
+
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Stage levels [lo, hi] (1-based) of one lane's column of a level-major
+// field into its shared-memory slots buf[(k-1)*32].  The loop runs over the
+// warp's union [w_lo, w_hi] so that each level is one coalesced warp copy.
+__device__ __forceinline__ void stage_column(double *buf, const double *col, size_t P, int w_lo, int w_hi, int lo,
+                                             int hi)
+{
+    for (int k = w_lo; k <= w_hi; ++k)
+        if (k >= lo && k <= hi) cp_async8(buf + (size_t)(k - 1) * MP_TR_COLS, col + P * (size_t)(k - 1));
+}
+
+// One row of the factorisation: given the excess inputs, the pivot's
+// reciprocal and the signed multiplier t (-q when q < 1/2, else u).
+__device__ __forceinline__ void pivot_row(float s, float f_up, float &ip, float &t, float &q)
+{
+    const float p = s + f_up;
+    ip = __frcp_rn(p);
+    if (f_up == 0.0f) {
+        q = 1.0f;
+        t = 0.0f;
+    } else {
+        q = s * ip;
+        t = (q < 0.5f) ? -q : f_up * ip;
+    }
+}
+// u * z from the signed multiplier
+__device__ __forceinline__ double mul_u(float t, double z) { return (t < 0.0f) ? z + (double)t * z : (double)t * z; }
+__device__ __forceinline__ float mul_u(float t, float z) { return (t < 0.0f) ? z + t * z : t * z; }
+
+// FP32 couplings, pivots and multipliers of one diffusivity over the lane's
+// live span (build_factorize_tracer_matrix: rdb_ocean_vdiff.F90:1285-1341;
+// gates in FP64 on the raw thicknesses, which makes the coupling of an
+// interface the same for the two rows it joins).  hs holds h at layer slots,
+// ks the diffusivity of interface k (1-based, the bottom of layer k) at slot
+// k-1, for k in (k_lo, k_hi].  Out: fu[k] = F_{k+1} (the coupling above
+// layer k), ip[k] = 1/p_k, tu[k] = t_k.
+__device__ __forceinline__ void tracer_factors(const double *hs, const double *ks, int w_lo, int w_hi, int k_lo,
+                                               int k_hi, bool use_harmonic, float dtf, float *fu, float *ipv, float *tu)
+{
+    const float HV = (float)H_VANISHED;
+    float f_dn = 0.0f, q_prev = 1.0f;
+    for (int k = w_lo; k <= w_hi; ++k) {
+        if (k < k_lo || k > k_hi) continue;
+        const size_t s = (size_t)(k - 1) * MP_TR_COLS;
+        const double hc_raw = hs[s];
+        const float H = fmx((float)hc_raw, HV);
+        float f_up = 0.0f;
+        if (k < k_hi) {
+            const double hp_raw = hs[s + MP_TR_COLS];
+            if (!(hc_raw <= H_VANISHED || hp_raw <= H_VANISHED))
+                f_up = __fdividef(dtf * (float)ks[s + MP_TR_COLS], face_thick(H, fmx((float)hp_raw, HV), use_harmonic));
+        }
+        const float sx = H + f_dn * q_prev;
+        float ip, t, q;
+        pivot_row(sx, f_up, ip, t, q);
+        fu[s] = f_up;
+        ipv[s] = ip;
+        tu[s] = t;
+        f_dn = f_up;
+        q_prev = q;
+    }
+}
+
+template <bool TWO>
+__global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, double dt, int nonlocal)
+{
+    extern __shared__ __align__(16) double smd[];
+    const int lane = threadIdx.x;
+    const int i = blockIdx.x * MP_TR_COLS + lane;
+    const int j = blockIdx.y;
+    const vphys_config &c = p.cfg;
+    const int nx = p.nx, nz = p.nz, ntr = p.ntr;
+    const size_t P = p.plane;
+    const bool in_grid = i < nx;
+    const size_t col = (size_t)(in_grid ? i : 0) + (size_t)nx * j;
+    const double *__restrict__ hp = p.h + col;
+    const int iT = c.idx_temperature, iS = c.idx_salinity, iPS = c.idx_pseudo_salt;
+    const size_t NB = (size_t)nz * MP_TR_COLS;
+    // per lane and level: two FP64 staging buffers, then FP32 F, 1/p, t per
+    // diffusivity and the forward result v
+    double *buf0 = smd + lane, *buf1 = smd + NB + lane;
+    float *fA = reinterpret_cast<float *>(smd + 2 * NB) + lane;
+    float *ipA = fA + NB, *tA = ipA + NB;
+    float *fB = TWO ? tA + NB : fA;
+    float *ipB = TWO ? fB + NB : ipA;
+    float *tB = TWO ? ipB + NB : tA;
+    float *vv = (TWO ? tB : tA) + NB;
+
+    // ---- this column's live span; rows outside it are identity rows ----
+    int k_lo = 0, k_hi = 0;
+    if (in_grid) {
+        for (int k = 1; k <= nz; ++k)
+            if (__ldg(hp + P * (size_t)(k - 1)) > H_VANISHED) {
+                k_lo = k;
+                break;
+            }
+        if (k_lo > 0) {
+            k_hi = k_lo;
+            for (int k = nz; k > k_lo; --k)
+                if (__ldg(hp + P * (size_t)(k - 1)) > H_VANISHED) {
+                    k_hi = k;
+                    break;
+                }
+        }
+    }
+    const bool live = k_lo > 0;
+    const int w_lo = __reduce_min_sync(0xffffffffu, live ? k_lo : 0x7fffffff);
+    const int w_hi = __reduce_max_sync(0xffffffffu, live ? k_hi : 0);
+    if (w_hi == 0) return;
+    const int lo = live ? k_lo : 1, hi = live ? k_hi : 0;   // empty range for a dead lane
+    const float dtf = (float)dt;
+
+    // ---- factorisation: h -> buf1, interfaces (k_lo, k_hi] of kt (then ks) -> buf0 ----
+    stage_column(buf1, hp, P, w_lo, w_hi, lo, hi);
+    stage_column(buf0, p.kt + col, P, w_lo + 1, w_hi, lo + 1, hi);
+    cp_async_commit();
+    cp_async_wait<0>();
+    tracer_factors(buf1, buf0, w_lo, w_hi, lo, hi, c.use_harmonic, dtf, fA, ipA, tA);
+    if (TWO) {
+        stage_column(buf0, p.ks + col, P, w_lo + 1, w_hi, lo + 1, hi);
+        cp_async_commit();
+        cp_async_wait<0>();
+        tracer_factors(buf1, buf0, w_lo, w_hi, lo, hi, c.use_harmonic, dtf, fB, ipB, tB);
+    }
+
+    // ---- non-local column scalars (FP64, as KPP pass 2) ----
+    const bool do_nl = nonlocal && c.use_kpp;
+    bool nl = do_nl && live;
+    double h_b = 0.0, q_T_kin = 0.0, q_S_kin = 0.0;
+    if (nl) {
+        const double rho0 = c.rho0;
+        h_b = p.bl_depth[col];
+        const double u_star = sqrt(xdiv(p.stress_mag[col], rho0));
+        q_T_kin = xdiv(p.q_heat[col], rho0 * c.cp);
+        q_S_kin = xdiv(p.q_salt[col], rho0);
+        const double B_0 = (GRAVITY / rho0) * (c.alpha_T * q_T_kin - c.beta_S * q_S_kin);
+        const double wstar3 = fmx(0.0, -B_0) * h_b;
+        const double w_star = sm_cbrt(wstar3);
+        const double w_s = sqrt(u_star * u_star + w_star * w_star);
+        nl = (h_b > 0.0 && w_s > 0.0 && B_0 < 0.0);
+    }
+    double *heat = (c.budgets && iT >= 0) ? p.heat_budget + col : nullptr;
+    double *salt = (c.budgets && iS >= 0) ? p.salt_budget + col : nullptr;
+
+    // ---- tracers: double-buffered staging, forward and backward sweeps ----
+    stage_column(buf0, p.tr[0] + col, P, w_lo, w_hi, lo, hi);
+    cp_async_commit();
+    for (int t = 0; t < ntr; ++t) {
+        const double *cur = (t & 1) ? buf1 : buf0;
+        if (t + 1 < ntr) {
+            stage_column((t & 1) ? buf0 : buf1, p.tr[t + 1] + col, P, w_lo, w_hi, lo, hi);
+            cp_async_commit();
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        const bool useA = !TWO || (t == iT);
+        const float *fu = useA ? fA : fB;
+        const float *ipv = useA ? ipA : ipB;
+        const float *tu = useA ? tA : tB;
+        double *__restrict__ trc = p.tr[t] + col;
+
+        // forward: FP64 residual and accumulation, v = w / p
+        {
+            double d_m = 0.0, d_c = live ? cur[(size_t)(lo - 1) * MP_TR_COLS] : 0.0, w = 0.0;
+            float f_dn = 0.0f, t_prev = 0.0f;
+            for (int k = w_lo; k <= w_hi; ++k) {
+                if (k < lo || k > hi) continue;
+                const size_t s = (size_t)(k - 1) * MP_TR_COLS;
+                const double d_p = (k < hi) ? cur[s + MP_TR_COLS] : d_c;
+                const float f_up = fu[s];
+                const double b = (double)f_dn * (d_m - d_c) + (double)f_up * (d_p - d_c);
+                w = b + mul_u(t_prev, w);
+                vv[s] = (float)(w * (double)ipv[s]);
+                t_prev = tu[s];
+                f_dn = f_up;
+                d_m = d_c;
+                d_c = d_p;
+            }
+        }
+        // back-substitution, FP64 update, budgets, non-local deposit, store
+        const bool nl_t = do_nl && (t == iT || t == iS || t == iPS);
+        const double qk = (t == iT) ? q_T_kin : q_S_kin;
+        double *bud = (t == iT) ? heat : ((t == iS) ? salt : nullptr);
+        float delta = 0.0f;
+        double g_above = 0.0, d_run = 0.0;
+        double h_c = live ? __ldg(hp + P * (size_t)(hi - 1)) : 0.0, h_a = 0.0;
+        for (int k = w_hi; k >= w_lo; --k) {
+            if (k < lo || k > hi) continue;
+            const size_t s = (size_t)(k - 1) * MP_TR_COLS;
+            const size_t off = P * (size_t)(k - 1);
+            delta = vv[s] + mul_u(tu[s], delta);
+            const double d_k = cur[s];
+            double x = d_k + (double)delta;
+            if (bud) bud[off] = bud[off] + (h_c * x - h_c * d_k);
+            if (nl_t || bud) {
+                const double h_bl = (k > 1) ? __ldg(hp + off - P) : 0.0;
+                if (nl_t) {
+                    double gk = 0.0;
+                    if (nl) {
+                        d_run = d_run + h_c;
+                        if (k > 1 && d_run < h_b) {
+                            const double sigma = xdiv(d_run, h_b);
+                            gk = c.cs_nonlocal * (sigma * (1.0 - sigma) * (1.0 - sigma)) * qk;
+                        }
+                    }
+                    double f_up = 0.0, f_dn = 0.0;
+                    if (k < nz) f_up = nonlocal_face_flux(g_above, h_c, h_a);
+                    if (k > 1) f_dn = nonlocal_face_flux(gk, h_bl, h_c);
+                    x = conc_add_source(x, h_c, dt * (f_up - f_dn));
+                    g_above = gk;
+                }
+                h_a = h_c;
+                h_c = h_bl;
+            }
+            trc[off] = x;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// momentum: one thread per u or v face column
+// ---------------------------------------------------------------------------
+template <bool XF>
+__device__ __forceinline__ void solve_face_mp(const Params &p, double dt, int i, int j, float *st, float *sv,
+                                              float *sr, int bs)
+{
+    const vphys_config &c = p.cfg;
+    const int nx = p.nx, ny = p.ny, nz = p.nz;
+    const int nu = XF ? nx + 1 : nx;
+    const size_t P = p.plane;
+    const size_t PF = XF ? p.plane_u : p.plane_v;
+    const size_t f = (size_t)i + (size_t)nu * j;
+    double *__restrict__ uf = (XF ? p.u : p.v) + f;
+    double *__restrict__ vrem = c.remnant ? ((XF ? p.visc_rem_u : p.visc_rem_v) + f) : nullptr;
+    const unsigned long long pol_keep = l2_policy_evict_last();
+    int il, ir, jb, ja;
+    if (XF) {
+        il = i - 1 > 0 ? i - 1 : 0;
+        ir = i < nx - 1 ? i : nx - 1;
+        jb = j;
+        ja = j;
+    } else {
+        il = i;
+        ir = i;
+        jb = j - 1 > 0 ? j - 1 : 0;
+        ja = j < ny - 1 ? j : ny - 1;
+    }
+    const size_t cl = (size_t)il + (size_t)nx * jb;
+    const size_t cr = (size_t)ir + (size_t)nx * ja;
+    if (!c.remnant && !c.implicit_stress && fmn(p.wet[cl], p.wet[cr]) == 0.0) {
+        bool zero = true;
+        for (int k = 1; k <= nz && zero; ++k) zero = (uf[PF * (size_t)(k - 1)] == 0.0);
+        if (zero) return;
+    }
+    const double *__restrict__ hl = p.h + cl;
+    const double *__restrict__ hr = p.h + cr;
+    const double *__restrict__ kvl = p.kv + cl;
+    const double *__restrict__ kvr = p.kv + cr;
+    const int *ktp = XF ? p.k_top_u : p.k_top_v;
+    const int *kbp = XF ? p.k_bot_u : p.k_bot_v;
+    const int kb = kbp ? min(max(kbp[f], 1), nz) : 1;
+    const int ktop = ktp ? min(max(ktp[f], 1), nz) : nz;
+    const float bbl_thick = (float)c.hbbl_visc;
+    const float kv_bbl = c.bbl_glue ? (float)(c.bbl_piston * c.hbbl_visc) : 0.0f;
+    const float i_hbbl = __frcp_rn(bbl_thick + (float)EPS_HVEL);
+    const float dtf = (float)dt;
+    float zacc = 0.0f, zcol_l = 0.0f, zcol_r = 0.0f;
+    if (c.hvel_mom6 && !c.hvel_harmonic) {
+        for (int k = 1; k <= nz; ++k) {
+            zcol_l = zcol_l - (float)__ldg(hl + P * (size_t)(k - 1));
+            zcol_r = zcol_r - (float)__ldg(hr + P * (size_t)(k - 1));
+        }
+    }
+    const float d_min = fmn(-zcol_l, -zcol_r);
+    int kb_live = kb;
+    if (c.zlevel_faces) {
+        for (int k = kb; k <= nz; ++k) {
+            if (fmn(__ldg(hl + P * (size_t)(k - 1)), __ldg(hr + P * (size_t)(k - 1))) > H_VANISHED) {
+                kb_live = k;
+                break;
+            }
+        }
+    }
+    float hv_p, zi_p;
+    double u_c = ld_hint(uf, pol_keep), u_m = 0.0;
+    face_layer<float>(c, (float)__ldg(hl), (float)__ldg(hr), (float)u_c, 1, kb, d_min, i_hbbl, zacc, zcol_l, zcol_r,
+                      hv_p, zi_p);
+    float num_t = 0.0f, dz_t = 1.0f;
+    bool cut_t = false;
+    const float lam = (c.implicit_drag && !c.bbl_glue) ? (float)(XF ? p.lambda_bot_u : p.lambda_bot_v)[f] : 0.0f;
+    double stress = 0.0;
+    if (c.implicit_stress) {
+        const double tau = (XF ? p.tau_x : p.tau_y)[f];
+        stress = dt * tau * fmn(p.wet[cl], p.wet[cr]) * (1.0 / c.rho0);
+    }
+    // carried between rows: the coupling above the previous row, its q and t,
+    // and the FP64 forward accumulations of the increment and of the remnant
+    float f_prev = 0.0f, q_prev = 1.0f, t_prev = 0.0f;
+    double w = 0.0, wr = 0.0;
+    for (int k0 = 1; k0 <= nz; k0 += MP_MOM_U) {
+        double hln[MP_MOM_U], hrn[MP_MOM_U], un[MP_MOM_U], kvln[MP_MOM_U], kvrn[MP_MOM_U];
+#pragma unroll
+        for (int q = 0; q < MP_MOM_U; ++q) {
+            const int k = k0 + q;
+            if (k < nz) {
+                const size_t o = P * (size_t)k;
+                hln[q] = __ldg(hl + o);
+                hrn[q] = __ldg(hr + o);
+                kvln[q] = __ldg(kvl + o);
+                kvrn[q] = __ldg(kvr + o);
+                un[q] = ld_hint(uf + PF * (size_t)k, pol_keep);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < MP_MOM_U; ++q) {
+            const int k = k0 + q;
+            if (k > nz) break;
+            const float hv_0 = hv_p, zi_0 = zi_p;
+            const float num_b = num_t, dz_b = dz_t;
+            const bool cut_b = cut_t;
+            double u_p = 0.0;
+            if (k < nz) {
+                u_p = un[q];
+                face_layer<float>(c, (float)hln[q], (float)hrn[q], (float)u_p, k + 1, kb, d_min, i_hbbl, zacc,
+                                  zcol_l, zcol_r, hv_p, zi_p);
+                if (k >= kb_live && k <= ktop)
+                    interface_coupling<float>(c, hv_0, hv_p, zi_0, dtf, kv_bbl, bbl_thick, (float)kvln[q],
+                                              (float)kvrn[q], num_t, dz_t, cut_t);
+            }
+            // the row in conservative form (row k of the reference times hf_k)
+            const float H = fmx(hv_0, (float)H_VANISHED);
+            float f_up = 0.0f, f_dn = 0.0f, ex = 0.0f;
+            if (k == kb_live && k <= ktop) {
+                if (kb_live < nz && !cut_t) f_up = __fdividef(num_t, dz_t);
+                if (c.bbl_glue) ex = __fdividef(dtf * kv_bbl, fmn(0.5f * hv_0, bbl_thick) + (float)EPS_HVEL);
+                if (c.implicit_drag && !c.bbl_glue) ex = H * (dtf * lam);
+            }
+            if (k == ktop && k > kb_live && !cut_b) f_dn = __fdividef(num_b, dz_b);
+            if (k > kb_live && k < ktop) {
+                if (!cut_b) f_dn = __fdividef(num_b, dz_b);
+                if (!cut_t) f_up = __fdividef(num_t, dz_t);
+            }
+            // FP64 residual of the old velocity (+ the wind stress of the top row)
+            double b = (double)f_dn * (u_m - u_c) + (double)f_up * (u_p - u_c) - (double)ex * u_c;
+            if (k == ktop && c.implicit_stress) b = b + (double)H * (stress / fmx((double)H, STRESS_H_MIN));
+            // the row below couples into this one only through a shared interface
+            const float t_in = (f_dn != 0.0f) ? t_prev : 0.0f;
+            const float sx = H + ex + f_dn * q_prev;
+            float ip, t, qq;
+            pivot_row(sx, f_up, ip, t, qq);
+            w = b + mul_u(t_in, w);
+            const size_t s = (size_t)(k - 1) * bs;
+            sv[s] = (float)(w * (double)ip);
+            st[s] = t;
+            if (vrem) {
+                wr = (double)H + mul_u(t_in, wr);
+                sr[s] = (float)(wr * (double)ip);
+            }
+            f_prev = f_up;
+            q_prev = qq;
+            t_prev = t;
+            u_m = u_c;
+            u_c = u_p;
+        }
+    }
+    (void)f_prev;
+    // back-substitution: increment (+ the remnant, RHS 1, clipped at 1 as it goes)
+    float delta = 0.0f, gam = 0.0f;
+    for (int k0 = nz; k0 >= 1; k0 -= MP_MOM_U) {
+        double uo[MP_MOM_U];
+#pragma unroll
+        for (int q = 0; q < MP_MOM_U; ++q) {
+            const int k = k0 - q;
+            if (k >= 1) uo[q] = ld_hint(uf + PF * (size_t)(k - 1), pol_keep);
+        }
+#pragma unroll
+        for (int q = 0; q < MP_MOM_U; ++q) {
+            const int k = k0 - q;
+            if (k < 1) break;
+            const size_t s = (size_t)(k - 1) * bs;
+            const float tk = st[s];
+            delta = sv[s] + mul_u(tk, delta);
+            const size_t o = PF * (size_t)(k - 1);
+            uf[o] = uo[q] + (double)delta;
+            if (vrem) {
+                gam = fminf(sr[s] + mul_u(tk, gam), 1.0f);
+                vrem[o] = (double)gam;
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(MP_MOM_THREADS) k_momentum_mp(const Params p, double dt)
+{
+    extern __shared__ float smf[];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    const size_t NB = (size_t)p.nz * blockDim.x;
+    float *st = smf + threadIdx.x, *sv = st + NB, *sr = sv + NB;
+    if (blockIdx.z == 0) {
+        if (i <= p.nx && j < p.ny) solve_face_mp<true>(p, dt, i, j, st, sv, sr, blockDim.x);
+    } else {
+        if (i < p.nx && j <= p.ny) solve_face_mp<false>(p, dt, i, j, st, sv, sr, blockDim.x);
+    }
+}
+
+static size_t tracers_mp_smem(int nz, bool two)
+{
+    // two FP64 staging buffers + (F, 1/p, t) per diffusivity + v, per lane and level
+    return (size_t)nz * MP_TR_COLS * (2 * sizeof(double) + (two ? 7 : 4) * sizeof(float));
+}
+
+template <bool TWO>
+static void launch_tracers_mp_t(const Params &p, double dt, bool nonlocal, cudaStream_t stream)
+{
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_tracers_mp<TWO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)tracers_mp_smem(VPHYS_NZ_MAX, TWO));
+        attr_set = true;
+    }
+    dim3 grid((p.nx + MP_TR_COLS - 1) / MP_TR_COLS, p.ny);
+    k_tracers_mp<TWO><<<grid, MP_TR_COLS, tracers_mp_smem(p.nz, TWO), stream>>>(p, dt, nonlocal ? 1 : 0);
+}
+
+void launch_tracers_mp(const Params &p, double dt, bool nonlocal, cudaStream_t stream)
+{
+    if (p.ks_equals_kt)
+        launch_tracers_mp_t<false>(p, dt, nonlocal, stream);
+    else
+        launch_tracers_mp_t<true>(p, dt, nonlocal, stream);
+}
+
+void launch_momentum_mp(const Params &p, double dt, cudaStream_t stream)
+{
+    const int bs = MP_MOM_THREADS;
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_momentum_mp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)((size_t)VPHYS_NZ_MAX * bs * sizeof(float) * 3));
+        attr_set = true;
+    }
+    const size_t smem = (size_t)p.nz * bs * sizeof(float) * (p.cfg.remnant ? 3 : 2);
+    dim3 grid((p.nx + 1 + bs - 1) / bs, p.ny + 1, 2);
+    k_momentum_mp<<<grid, bs, smem, stream>>>(p, dt);
+}
+
+}  // namespace vphys

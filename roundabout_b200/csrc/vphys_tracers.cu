@@ -331,6 +331,10 @@ static void launch_tracers_n(const Params &p, double dt, bool diffuse, bool nonl
 
 void launch_tracers(const Params &p, double dt, bool diffuse, bool nonlocal, cudaStream_t stream)
 {
+    if (diffuse && p.cfg.mixed_precision) {
+        launch_tracers_mp(p, dt, nonlocal, stream);
+        return;
+    }
     const bool two = !p.ks_equals_kt;
     if (p.ntr <= 2) {
         two ? launch_tracers_n<2, true>(p, dt, diffuse, nonlocal, stream) : launch_tracers_n<2, false>(p, dt, diffuse, nonlocal, stream);
