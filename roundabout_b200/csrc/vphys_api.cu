@@ -73,6 +73,7 @@ struct vphys_handle_s {
     unsigned long long *guard_dev = nullptr;
     double *smooth_scratch = nullptr;
     double *budget_scratch = nullptr;
+    int *span = nullptr;              // live spans of the columns (mixed-precision tracer solve)
 };
 
 namespace {
@@ -258,6 +259,7 @@ Params make_params(vphys_handle h)
     for (int t = 0; t < h->ntr && t < vphys::NTR_MAX; ++t) p.tr[t] = (double *)h->f[NFIXED + t].ptr();
     p.guard_count = h->guard_dev;
     p.budget_scratch = h->budget_scratch;
+    p.span = h->span;
     p.ks_equals_kt = (h->cfg.bkgnd_profile || h->cfg.kt_bg == h->cfg.ks_bg) ? 1 : 0;
     p.write_gamma = (p.gamma_t && p.gamma_s) ? 1 : 0;
     return p;
@@ -281,6 +283,14 @@ int prepare_momentum(vphys_handle h)
 int prepare_tracers(vphys_handle h)
 {
     int st = VPHYS_OK;
+    if (h->cfg.mixed_precision && !h->span) {
+        cudaError_t e = cudaMalloc(&h->span, (size_t)h->nx * h->ny * sizeof(int));
+        if (e != cudaSuccess) {
+            h->span = nullptr;
+            cudaGetLastError();
+            return push_error(VPHYS_ERR_ALLOC, "cudaMalloc of the column spans failed");
+        }
+    }
     if (h->cfg.budgets) {
         if ((st = ensure(h, VPHYS_FIELD_HEAT_BUDGET))) return st;
         if ((st = ensure(h, VPHYS_FIELD_SALT_BUDGET))) return st;
@@ -491,6 +501,7 @@ int vphys_destroy(vphys_handle *hp)
     if (h->guard_dev) cudaFree(h->guard_dev);
     if (h->smooth_scratch) cudaFree(h->smooth_scratch);
     if (h->budget_scratch) cudaFree(h->budget_scratch);
+    if (h->span) cudaFree(h->span);
     h->magic = 0;
     delete h;
     return VPHYS_OK;

@@ -32,6 +32,7 @@ struct Params {
     const int *k_top_u, *k_top_v, *k_bot_u, *k_bot_v;   // nullptr: nz / 1
     double *tr[NTR_MAX];
     unsigned long long *guard_count;  // vmix_guard counter (device)
+    int *span;                        // per column: first | last live layer << 16 (0: none), scratch
     int ks_equals_kt;                 // ks is bitwise kt after the gate
     int write_gamma;
 };

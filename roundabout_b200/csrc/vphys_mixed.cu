@@ -25,13 +25,13 @@
 //     forward (FP64):  w_k = b_k + u_{k-1} w_{k-1},   v_k = w_k / p_k
 //     backward (FP32): delta_k = v_k + u_k delta_{k+1},   x_k = d_k + delta_k (FP64)
 //
-// Tracers: one warp per block, one lane per column.  The column's live span
-// of every tracer is staged into shared memory with per-lane asynchronous
-// copies (cp.async, 8 B per level, each warp-level copy one 256-B segment),
-// double-buffered so that tracer t+1 is in flight while tracer t is swept;
-// h and the diffusivity are staged the same way for the factorisation.
-// Every lane reads only its own column's shared-memory slots, so the kernel
-// needs no block barrier.
+// Tracers: one warp per block, 32 columns (the lanes) x one tracer; the grid
+// runs the tracers of a column group back to back (adjacent blocks), so
+// h and K, read by each of them, come from L2 after the first.  Each warp
+// factorises in its own upward pass (FP32 arithmetic is cheap next to the
+// loads; no warp waits for another), keeps t and v (8 B per level and lane)
+// in shared memory, and reads d again from L2 in the back-substitution.  All
+// loads of a pass are issued MP_TR_U levels ahead of the arithmetic.
 //
 // Momentum: one thread per u or v face column; t and v in shared memory, the
 // velocity read again from L2 (evict_last) by the back-substitution.
@@ -44,213 +44,103 @@
 namespace vphys {
 
 constexpr int MP_TR_COLS = 32;      // columns (lanes) per tracer block
+constexpr int MP_TR_U = 8;          // levels per tracer load block
 constexpr int MP_MOM_THREADS = 64;  // face columns per momentum block
 constexpr int MP_MOM_U = 4;         // levels per momentum load block
 
-__device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
+// Hardware reciprocal (MUFU, within 1 ulp): the FP32 factors carry no
+// bitwise contract, and their rounding is a consistent perturbation of the
+// couplings that the FP64 residual then sees.
+__device__ __forceinline__ float rcp_approx(float x)
 {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
-
-// Stage levels [lo, hi] (1-based) of one lane's column of a level-major
-// field into its shared-memory slots buf[(k-1)*32].  The loop runs over the
-// warp's union [w_lo, w_hi] so that each level is one coalesced warp copy.
-__device__ __forceinline__ void stage_column(double *buf, const double *col, size_t P, int w_lo, int w_hi, int lo,
-                                             int hi)
-{
-    for (int k = w_lo; k <= w_hi; ++k)
-        if (k >= lo && k <= hi) cp_async8(buf + (size_t)(k - 1) * MP_TR_COLS, col + P * (size_t)(k - 1));
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
 }
 
-// One row of the factorisation: given the excess inputs, the pivot's
-// reciprocal and the signed multiplier t (-q when q < 1/2, else u).
+// One row of the factorisation: the pivot's reciprocal and the signed
+// multiplier t (-q when q < 1/2, else u) from the excess s and the coupling
+// above; q = 1, t = 0 exactly for a row not coupled upward.
 __device__ __forceinline__ void pivot_row(float s, float f_up, float &ip, float &t, float &q)
 {
-    const float p = s + f_up;
-    ip = __frcp_rn(p);
-    if (f_up == 0.0f) {
-        q = 1.0f;
-        t = 0.0f;
-    } else {
-        q = s * ip;
-        t = (q < 0.5f) ? -q : f_up * ip;
-    }
+    ip = rcp_approx(s + f_up);
+    const float qq = s * ip;
+    q = (f_up == 0.0f) ? 1.0f : qq;
+    t = (f_up == 0.0f) ? 0.0f : ((qq < 0.5f) ? -qq : f_up * ip);
 }
 // u * z from the signed multiplier
 __device__ __forceinline__ double mul_u(float t, double z) { return (t < 0.0f) ? z + (double)t * z : (double)t * z; }
 __device__ __forceinline__ float mul_u(float t, float z) { return (t < 0.0f) ? z + t * z : t * z; }
 
-// FP32 couplings, pivots and multipliers of one diffusivity over the lane's
-// live span (build_factorize_tracer_matrix: rdb_ocean_vdiff.F90:1285-1341;
-// gates in FP64 on the raw thicknesses, which makes the coupling of an
-// interface the same for the two rows it joins).  hs holds h at layer slots,
-// ks the diffusivity of interface k (1-based, the bottom of layer k) at slot
-// k-1, for k in (k_lo, k_hi].  Out: fu[k] = F_{k+1} (the coupling above
-// layer k), ip[k] = 1/p_k, tu[k] = t_k.
-__device__ __forceinline__ void tracer_factors(const double *hs, const double *ks, int w_lo, int w_hi, int k_lo,
-                                               int k_hi, bool use_harmonic, float dtf, float *fu, float *ipv, float *tu)
+// Live span of every column: the first live layer from the bed and from the
+// surface (rdb_vl_first_live's test h > H_VANISHED), packed lo | hi << 16,
+// 0 for a column without one.  Loads go MP_TR_U levels at a time, so a column
+// with many fillers under its bathymetry costs a few load latencies, not one
+// per filler.
+__global__ void k_spans(const Params p)
 {
-    const float HV = (float)H_VANISHED;
-    float f_dn = 0.0f, q_prev = 1.0f;
-    for (int k = w_lo; k <= w_hi; ++k) {
-        if (k < k_lo || k > k_hi) continue;
-        const size_t s = (size_t)(k - 1) * MP_TR_COLS;
-        const double hc_raw = hs[s];
-        const float H = fmx((float)hc_raw, HV);
-        float f_up = 0.0f;
-        if (k < k_hi) {
-            const double hp_raw = hs[s + MP_TR_COLS];
-            if (!(hc_raw <= H_VANISHED || hp_raw <= H_VANISHED))
-                f_up = __fdividef(dtf * (float)ks[s + MP_TR_COLS], face_thick(H, fmx((float)hp_raw, HV), use_harmonic));
-        }
-        const float sx = H + f_dn * q_prev;
-        float ip, t, q;
-        pivot_row(sx, f_up, ip, t, q);
-        fu[s] = f_up;
-        ipv[s] = ip;
-        tu[s] = t;
-        f_dn = f_up;
-        q_prev = q;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (i >= p.nx) return;
+    const size_t col = (size_t)i + (size_t)p.nx * j;
+    const double *__restrict__ hp = p.h + col;
+    const size_t P = p.plane;
+    const int nz = p.nz;
+    int lo = 0, hi = 0;
+    for (int k0 = 1; k0 <= nz && lo == 0; k0 += MP_TR_U) {
+        double hv[MP_TR_U];
+#pragma unroll
+        for (int u = 0; u < MP_TR_U; ++u) hv[u] = (k0 + u <= nz) ? __ldg(hp + P * (size_t)(k0 + u - 1)) : 0.0;
+#pragma unroll
+        for (int u = MP_TR_U - 1; u >= 0; --u)
+            if (hv[u] > H_VANISHED) lo = k0 + u;
     }
+    if (lo > 0) {
+        for (int k0 = nz; k0 >= lo && hi == 0; k0 -= MP_TR_U) {
+            double hv[MP_TR_U];
+#pragma unroll
+            for (int u = 0; u < MP_TR_U; ++u) hv[u] = (k0 - u >= lo) ? __ldg(hp + P * (size_t)(k0 - u - 1)) : 0.0;
+#pragma unroll
+            for (int u = MP_TR_U - 1; u >= 0; --u)
+                if (hv[u] > H_VANISHED) hi = k0 - u;
+        }
+    }
+    p.span[col] = lo | (hi << 16);
 }
 
-template <bool TWO>
-__global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, double dt, int nonlocal)
+// Back-substitution of one tracer column from the t and v rows; with FULL the
+// heat/salt budgets and the KPP non-local deposit (nonlocal_face_flux,
+// rdb_ocean_vmix.F90:1605-1714) ride along.
+template <bool FULL>
+__device__ __forceinline__ void tracer_back(const Params &p, double dt, double *__restrict__ trc,
+                                            const double *__restrict__ hp, const float *tu, const float *vv, int w_lo,
+                                            int w_hi, int lo, int hi, double *bud, bool nl_t, bool nl, double h_b,
+                                            double q_kin, unsigned long long pol)
 {
-    extern __shared__ __align__(16) double smd[];
-    const int lane = threadIdx.x;
-    const int i = blockIdx.x * MP_TR_COLS + lane;
-    const int j = blockIdx.y;
-    const vphys_config &c = p.cfg;
-    const int nx = p.nx, nz = p.nz, ntr = p.ntr;
     const size_t P = p.plane;
-    const bool in_grid = i < nx;
-    const size_t col = (size_t)(in_grid ? i : 0) + (size_t)nx * j;
-    const double *__restrict__ hp = p.h + col;
-    const int iT = c.idx_temperature, iS = c.idx_salinity, iPS = c.idx_pseudo_salt;
-    const size_t NB = (size_t)nz * MP_TR_COLS;
-    // per lane and level: two FP64 staging buffers, then FP32 F, 1/p, t per
-    // diffusivity and the forward result v
-    double *buf0 = smd + lane, *buf1 = smd + NB + lane;
-    float *fA = reinterpret_cast<float *>(smd + 2 * NB) + lane;
-    float *ipA = fA + NB, *tA = ipA + NB;
-    float *fB = TWO ? tA + NB : fA;
-    float *ipB = TWO ? fB + NB : ipA;
-    float *tB = TWO ? ipB + NB : tA;
-    float *vv = (TWO ? tB : tA) + NB;
-
-    // ---- this column's live span; rows outside it are identity rows ----
-    int k_lo = 0, k_hi = 0;
-    if (in_grid) {
-        for (int k = 1; k <= nz; ++k)
-            if (__ldg(hp + P * (size_t)(k - 1)) > H_VANISHED) {
-                k_lo = k;
-                break;
-            }
-        if (k_lo > 0) {
-            k_hi = k_lo;
-            for (int k = nz; k > k_lo; --k)
-                if (__ldg(hp + P * (size_t)(k - 1)) > H_VANISHED) {
-                    k_hi = k;
-                    break;
-                }
+    const int nz = p.nz;
+    float delta = 0.0f;
+    double g_above = 0.0, d_run = 0.0, h_a = 0.0;
+    double h_c = (FULL && lo <= hi) ? __ldg(hp + P * (size_t)(hi - 1)) : 0.0;
+    for (int k0 = w_hi; k0 >= w_lo; k0 -= MP_TR_U) {
+        double dk[MP_TR_U];
+#pragma unroll
+        for (int u = 0; u < MP_TR_U; ++u) {
+            const int k = k0 - u;
+            dk[u] = (k >= lo && k <= hi) ? ld_hint(trc + P * (size_t)(k - 1), pol) : 0.0;
         }
-    }
-    const bool live = k_lo > 0;
-    const int w_lo = __reduce_min_sync(0xffffffffu, live ? k_lo : 0x7fffffff);
-    const int w_hi = __reduce_max_sync(0xffffffffu, live ? k_hi : 0);
-    if (w_hi == 0) return;
-    const int lo = live ? k_lo : 1, hi = live ? k_hi : 0;   // empty range for a dead lane
-    const float dtf = (float)dt;
-
-    // ---- factorisation: h -> buf1, interfaces (k_lo, k_hi] of kt (then ks) -> buf0 ----
-    stage_column(buf1, hp, P, w_lo, w_hi, lo, hi);
-    stage_column(buf0, p.kt + col, P, w_lo + 1, w_hi, lo + 1, hi);
-    cp_async_commit();
-    cp_async_wait<0>();
-    tracer_factors(buf1, buf0, w_lo, w_hi, lo, hi, c.use_harmonic, dtf, fA, ipA, tA);
-    if (TWO) {
-        stage_column(buf0, p.ks + col, P, w_lo + 1, w_hi, lo + 1, hi);
-        cp_async_commit();
-        cp_async_wait<0>();
-        tracer_factors(buf1, buf0, w_lo, w_hi, lo, hi, c.use_harmonic, dtf, fB, ipB, tB);
-    }
-
-    // ---- non-local column scalars (FP64, as KPP pass 2) ----
-    const bool do_nl = nonlocal && c.use_kpp;
-    bool nl = do_nl && live;
-    double h_b = 0.0, q_T_kin = 0.0, q_S_kin = 0.0;
-    if (nl) {
-        const double rho0 = c.rho0;
-        h_b = p.bl_depth[col];
-        const double u_star = sqrt(xdiv(p.stress_mag[col], rho0));
-        q_T_kin = xdiv(p.q_heat[col], rho0 * c.cp);
-        q_S_kin = xdiv(p.q_salt[col], rho0);
-        const double B_0 = (GRAVITY / rho0) * (c.alpha_T * q_T_kin - c.beta_S * q_S_kin);
-        const double wstar3 = fmx(0.0, -B_0) * h_b;
-        const double w_star = sm_cbrt(wstar3);
-        const double w_s = sqrt(u_star * u_star + w_star * w_star);
-        nl = (h_b > 0.0 && w_s > 0.0 && B_0 < 0.0);
-    }
-    double *heat = (c.budgets && iT >= 0) ? p.heat_budget + col : nullptr;
-    double *salt = (c.budgets && iS >= 0) ? p.salt_budget + col : nullptr;
-
-    // ---- tracers: double-buffered staging, forward and backward sweeps ----
-    stage_column(buf0, p.tr[0] + col, P, w_lo, w_hi, lo, hi);
-    cp_async_commit();
-    for (int t = 0; t < ntr; ++t) {
-        const double *cur = (t & 1) ? buf1 : buf0;
-        if (t + 1 < ntr) {
-            stage_column((t & 1) ? buf0 : buf1, p.tr[t + 1] + col, P, w_lo, w_hi, lo, hi);
-            cp_async_commit();
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
-        }
-        const bool useA = !TWO || (t == iT);
-        const float *fu = useA ? fA : fB;
-        const float *ipv = useA ? ipA : ipB;
-        const float *tu = useA ? tA : tB;
-        double *__restrict__ trc = p.tr[t] + col;
-
-        // forward: FP64 residual and accumulation, v = w / p
-        {
-            double d_m = 0.0, d_c = live ? cur[(size_t)(lo - 1) * MP_TR_COLS] : 0.0, w = 0.0;
-            float f_dn = 0.0f, t_prev = 0.0f;
-            for (int k = w_lo; k <= w_hi; ++k) {
-                if (k < lo || k > hi) continue;
-                const size_t s = (size_t)(k - 1) * MP_TR_COLS;
-                const double d_p = (k < hi) ? cur[s + MP_TR_COLS] : d_c;
-                const float f_up = fu[s];
-                const double b = (double)f_dn * (d_m - d_c) + (double)f_up * (d_p - d_c);
-                w = b + mul_u(t_prev, w);
-                vv[s] = (float)(w * (double)ipv[s]);
-                t_prev = tu[s];
-                f_dn = f_up;
-                d_m = d_c;
-                d_c = d_p;
-            }
-        }
-        // back-substitution, FP64 update, budgets, non-local deposit, store
-        const bool nl_t = do_nl && (t == iT || t == iS || t == iPS);
-        const double qk = (t == iT) ? q_T_kin : q_S_kin;
-        double *bud = (t == iT) ? heat : ((t == iS) ? salt : nullptr);
-        float delta = 0.0f;
-        double g_above = 0.0, d_run = 0.0;
-        double h_c = live ? __ldg(hp + P * (size_t)(hi - 1)) : 0.0, h_a = 0.0;
-        for (int k = w_hi; k >= w_lo; --k) {
-            if (k < lo || k > hi) continue;
+#pragma unroll
+        for (int u = 0; u < MP_TR_U; ++u) {
+            const int k = k0 - u;
+            if (k < w_lo) break;
             const size_t s = (size_t)(k - 1) * MP_TR_COLS;
+            delta = vv[s] + mul_u(tu[s], delta);   // rows outside the span: v = t = 0
+            if (k < lo || k > hi) continue;
             const size_t off = P * (size_t)(k - 1);
-            delta = vv[s] + mul_u(tu[s], delta);
-            const double d_k = cur[s];
+            const double d_k = dk[u];
             double x = d_k + (double)delta;
-            if (bud) bud[off] = bud[off] + (h_c * x - h_c * d_k);
-            if (nl_t || bud) {
+            if (FULL) {
+                if (bud) bud[off] = bud[off] + (h_c * x - h_c * d_k);
                 const double h_bl = (k > 1) ? __ldg(hp + off - P) : 0.0;
                 if (nl_t) {
                     double gk = 0.0;
@@ -258,7 +148,7 @@ __global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, doubl
                         d_run = d_run + h_c;
                         if (k > 1 && d_run < h_b) {
                             const double sigma = xdiv(d_run, h_b);
-                            gk = c.cs_nonlocal * (sigma * (1.0 - sigma) * (1.0 - sigma)) * qk;
+                            gk = p.cfg.cs_nonlocal * (sigma * (1.0 - sigma) * (1.0 - sigma)) * q_kin;
                         }
                     }
                     double f_up = 0.0, f_dn = 0.0;
@@ -273,6 +163,115 @@ __global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, doubl
             trc[off] = x;
         }
     }
+}
+
+template <bool TWO>
+__global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, double dt, int nonlocal, int ngx)
+{
+    extern __shared__ __align__(16) float smf[];
+    const int lane = threadIdx.x;
+    const int tr = blockIdx.x % p.ntr;   // the tracers of a column group are adjacent blocks
+    const unsigned g = blockIdx.x / p.ntr;
+    const int gi = g % ngx, j = g / ngx;
+    const int i = gi * MP_TR_COLS + lane;
+    const vphys_config &c = p.cfg;
+    const int nx = p.nx, nz = p.nz;
+    const size_t P = p.plane;
+    const bool in_grid = i < nx;
+    const size_t col = (size_t)(in_grid ? i : 0) + (size_t)nx * j;
+    const double *__restrict__ hp = p.h + col;
+    const int iT = c.idx_temperature, iS = c.idx_salinity, iPS = c.idx_pseudo_salt;
+    const size_t NB = (size_t)nz * MP_TR_COLS;
+    float *tu = smf + lane, *vv = tu + NB;   // t and v per level, this lane's column
+    const float HV = (float)H_VANISHED;
+
+    // ---- this column's live span (k_spans); rows outside it are identity rows ----
+    const int sp = in_grid ? p.span[col] : 0;
+    const bool live = (sp & 0xffff) > 0;
+    const int lo = live ? (sp & 0xffff) : nz + 1, hi = live ? (sp >> 16) : 0;
+    const int w_lo = __reduce_min_sync(0xffffffffu, live ? lo : 0x7fffffff);
+    const int w_hi = __reduce_max_sync(0xffffffffu, hi);
+    if (w_hi == 0) return;
+
+    const double *__restrict__ Kp = ((TWO && tr != iT) ? p.ks : p.kt) + col;
+    double *__restrict__ trc = p.tr[tr] + col;
+    const unsigned long long pol_keep = l2_policy_evict_last();
+    const float dtf = (float)dt;
+
+    // ---- upward: factorisation (FP32) + FP64 residual and accumulation.
+    //      Branch-free rows: outside [lo, hi] nothing is loaded, h = 0 gates
+    //      both couplings off and the row solves to an increment of 0 ----
+    {
+        const bool first = (w_lo == lo);   // the lane's span starts at the warp's first row
+        double h_c = first ? __ldg(hp + P * (size_t)(w_lo - 1)) : 0.0;
+        double d_c = first ? ld_hint(trc + P * (size_t)(w_lo - 1), pol_keep) : 0.0;
+        double d_m = 0.0, w = 0.0;
+        float f_dn = 0.0f, q_prev = 1.0f, t_prev = 0.0f;
+        for (int k0 = w_lo; k0 <= w_hi; k0 += MP_TR_U) {
+            double hn[MP_TR_U], kn[MP_TR_U], dn[MP_TR_U];
+#pragma unroll
+            for (int u = 0; u < MP_TR_U; ++u) {
+                const int k = k0 + u;   // row k reads h, K and d one level up
+                const bool need = k + 1 >= lo && k + 1 <= hi;
+                const size_t o = P * (size_t)k;
+                hn[u] = need ? __ldg(hp + o) : 0.0;
+                kn[u] = need ? __ldg(Kp + o) : 0.0;
+                dn[u] = need ? ld_hint(trc + o, pol_keep) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < MP_TR_U; ++u) {
+                const int k = k0 + u;
+                if (k > w_hi) break;
+                // row k (build_factorize_tracer_matrix: rdb_ocean_vdiff.F90:1285-1341;
+                // gates on the raw FP64 thicknesses)
+                const float H = fmx((float)h_c, HV);
+                const float Hp = fmx((float)hn[u], HV);
+                const bool coupled = h_c > H_VANISHED && hn[u] > H_VANISHED;
+                const float f_up = coupled ? __fdividef(dtf * (float)kn[u], face_thick(H, Hp, c.use_harmonic)) : 0.0f;
+                float ip, t, q;
+                pivot_row(H + f_dn * q_prev, f_up, ip, t, q);
+                const double b = (double)f_dn * (d_m - d_c) + (double)f_up * (dn[u] - d_c);
+                w = b + mul_u(t_prev, w);
+                const size_t s = (size_t)(k - 1) * MP_TR_COLS;
+                vv[s] = (float)(w * (double)ip);
+                tu[s] = t;
+                t_prev = t;
+                q_prev = q;
+                f_dn = f_up;
+                d_m = d_c;
+                d_c = dn[u];
+                h_c = hn[u];
+            }
+        }
+    }
+
+    // ---- non-local column scalars (FP64, as KPP pass 2) ----
+    const bool nl_t = nonlocal && c.use_kpp && (tr == iT || tr == iS || tr == iPS);
+    bool nl = nl_t && live;
+    double h_b = 0.0, q_kin = 0.0;
+    if (nl) {
+        const double rho0 = c.rho0;
+        h_b = p.bl_depth[col];
+        const double u_star = sqrt(xdiv(p.stress_mag[col], rho0));
+        const double q_T_kin = xdiv(p.q_heat[col], rho0 * c.cp);
+        const double q_S_kin = xdiv(p.q_salt[col], rho0);
+        const double B_0 = (GRAVITY / rho0) * (c.alpha_T * q_T_kin - c.beta_S * q_S_kin);
+        const double wstar3 = fmx(0.0, -B_0) * h_b;
+        const double w_star = sm_cbrt(wstar3);
+        const double w_s = sqrt(u_star * u_star + w_star * w_star);
+        nl = (h_b > 0.0 && w_s > 0.0 && B_0 < 0.0);
+        q_kin = (tr == iT) ? q_T_kin : q_S_kin;
+    }
+    double *bud = nullptr;
+    if (c.budgets && tr == iT) bud = p.heat_budget + col;
+    if (c.budgets && tr == iS) bud = p.salt_budget + col;
+
+    // ---- back-substitution, FP64 update (+ budgets, non-local deposit), store ----
+    const unsigned long long pol_once = l2_policy_evict_first();
+    if (nl_t || (c.budgets && (tr == iT || tr == iS)))
+        tracer_back<true>(p, dt, trc, hp, tu, vv, w_lo, w_hi, lo, hi, bud, nl_t, nl, h_b, q_kin, pol_once);
+    else
+        tracer_back<false>(p, dt, trc, hp, tu, vv, w_lo, w_hi, lo, hi, nullptr, false, false, 0.0, 0.0, pol_once);
 }
 
 // ---------------------------------------------------------------------------
@@ -462,23 +461,20 @@ __global__ void __launch_bounds__(MP_MOM_THREADS) k_momentum_mp(const Params p, 
     }
 }
 
-static size_t tracers_mp_smem(int nz, bool two)
-{
-    // two FP64 staging buffers + (F, 1/p, t) per diffusivity + v, per lane and level
-    return (size_t)nz * MP_TR_COLS * (2 * sizeof(double) + (two ? 7 : 4) * sizeof(float));
-}
-
 template <bool TWO>
 static void launch_tracers_mp_t(const Params &p, double dt, bool nonlocal, cudaStream_t stream)
 {
+    const size_t smem = (size_t)p.nz * MP_TR_COLS * 2 * sizeof(float);
     static bool attr_set = false;
     if (!attr_set) {
         cudaFuncSetAttribute(k_tracers_mp<TWO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)tracers_mp_smem(VPHYS_NZ_MAX, TWO));
+                             (int)((size_t)VPHYS_NZ_MAX * MP_TR_COLS * 2 * sizeof(float)));
         attr_set = true;
     }
-    dim3 grid((p.nx + MP_TR_COLS - 1) / MP_TR_COLS, p.ny);
-    k_tracers_mp<TWO><<<grid, MP_TR_COLS, tracers_mp_smem(p.nz, TWO), stream>>>(p, dt, nonlocal ? 1 : 0);
+    k_spans<<<dim3((p.nx + 127) / 128, p.ny), 128, 0, stream>>>(p);
+    const int ngx = (p.nx + MP_TR_COLS - 1) / MP_TR_COLS;
+    const unsigned blocks = (unsigned)ngx * (unsigned)p.ny * (unsigned)p.ntr;
+    k_tracers_mp<TWO><<<blocks, MP_TR_COLS, smem, stream>>>(p, dt, nonlocal ? 1 : 0, ngx);
 }
 
 void launch_tracers_mp(const Params &p, double dt, bool nonlocal, cudaStream_t stream)
