@@ -8,10 +8,17 @@ coefficient assembly (PP81 + KPP + Bryan-Lewis gate) -> implicit momentum
 viscosity (u, v) -> implicit tracer diffusion of every tracer with the KPP
 non-local tendency.  The metric is cells/s (nx*ny*nz per step, the
 reference's Mcells/s convention, benchmarks/bench_ocean.F90:149-150) on the
-1440x1080x75 eddy-permitting configuration with T, S and 2 passives, FP64.
+1440x1080x75 eddy-permitting configuration with T, S and 2 passives; the
+state is FP64 at the interface in every form.
+
+Forms (--form): "mixed" (default) runs the Thomas sweeps in FP32 with the
+FP64 residual correction (cfg.mixed_precision = 1); "plain" is FP64
+throughout and bitwise the reference's arithmetic.  The line's "forms" object
+carries both forms' cells/s and the mixed form's error against the plain FP64
+GPU path after one step from the same state, over the whole domain.
 
 One JSON line from rank 0:
-  value        device-resident cells/s (state in HBM before timing)
+  value        device-resident cells/s of the selected form (state in HBM before timing)
   e2e          cells/s through the C ABI with host buffers: every step
                uploads the state (h, u, v, tracers, forcing) from pinned host
                memory with vphys_set_field and downloads the results (u, v,
@@ -55,6 +62,10 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-sample", default="360x270", help="nx x ny of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--form", default="mixed", choices=["mixed", "plain"],
+                    help="mixed: FP32 Thomas sweeps + FP64 residual (cfg.mixed_precision=1); "
+                         "plain: FP64 throughout, bitwise the reference's arithmetic")
+    ap.add_argument("--no-compare", action="store_true", help="skip the plain-FP64 timing and error check")
     return ap.parse_args()
 
 
@@ -242,10 +253,13 @@ def main():
     gen_spec = dict(spec)
     gen_spec.pop("ntracers")
     cols = make_columns(ntracers=ntr, seed=1234 + rank, **gen_spec)
+    mixed = args.form == "mixed"
     cfg = hot_path_config(ntracers=ntr)
+    cfg.mixed_precision = 1 if mixed else 0
     vp = VerticalPhysics(nx, ny, nz, ntr, cfg)
     vp.load_columns(cols)
     torch.cuda.synchronize()
+    config_out["form"] = args.form
 
     def barrier():
         if dist is not None:
@@ -260,21 +274,56 @@ def main():
         return float(t.item())
 
     dt = 3600.0
-    for _ in range(max(3, args.warmup)):
-        vp.step(dt, 1)
-    barrier()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        barrier()
-        ev0.record()
-        for _ in range(args.steps):
-            vp.step(dt, 1)
-        ev1.record()
-        barrier()
-    ms = ev0.elapsed_time(ev1)
-    ms = max_over_ranks(ms)
     cells = nx * ny * nz
+
+    def timed(handle, steps, warm):
+        for _ in range(max(3, warm)):
+            handle.step(dt, 1)
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        e0.record()
+        for _ in range(steps):
+            handle.step(dt, 1)
+        e1.record()
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1))
+
+    # ---- the mixed form against the plain FP64 GPU path: one step from the
+    #      same state, max |difference| over the whole domain ----
+    forms = {}
+    vp_plain = None
+    if mixed and not args.no_compare:
+        cfg_plain = hot_path_config(ntracers=ntr)
+        vp_plain = VerticalPhysics(nx, ny, nz, ntr, cfg_plain)
+        vp_plain.load_columns(cols)
+        vp.step(dt, 1)
+        vp_plain.step(dt, 1)
+        torch.cuda.synchronize()
+        iT, iS = cfg.idx_temperature, cfg.idx_salinity
+        err = {"T": 0.0, "S": 0.0, "passive": 0.0, "u": 0.0, "v": 0.0}
+        for t in range(ntr):
+            d = float(np.abs(np.asarray(vp.get_tracer(t)) - np.asarray(vp_plain.get_tracer(t))).max())
+            key = "T" if t == iT else ("S" if t == iS else "passive")
+            err[key] = max(err[key], d)
+        for n in ("u", "v"):
+            err[n] = float(np.abs(np.asarray(vp.get(n)) - np.asarray(vp_plain.get(n))).max())
+        forms["mixed_max_abs_err_vs_plain_fp64_1step"] = {k: float(f"{v:.3e}") for k, v in err.items()}
+        forms["error_bar"] = "|dT|, |dS|, tracers <= 1e-6 after one step from the same state"
+        ms_plain = timed(vp_plain, args.steps, args.warmup)
+        forms["plain_fp64"] = {"cells_per_s": cells * args.steps * world / (ms_plain / 1e3),
+                               "ms_per_step": ms_plain / args.steps}
+        vp_plain.close()
+        vp_plain = None
+        vp.load_columns(cols)
+
+    with ClockSampler(local) as clk:
+        ms = timed(vp, args.steps, args.warmup)
     value = cells * args.steps * world / (ms / 1e3)
+    if mixed:
+        forms["mixed"] = {"cells_per_s": value, "ms_per_step": ms / args.steps}
+        if "plain_fp64" in forms:
+            forms["mixed_over_plain"] = round(value / forms["plain_fp64"]["cells_per_s"], 3)
 
     # ---- per-kernel device times (same stream, CUDA events) ----
     reps = 5
@@ -296,8 +345,9 @@ def main():
         torch.cuda.synchronize()
         stage_ms[name] = a.elapsed_time(b) / reps
     bpc = bytes_per_cell(ntr, nz)
-    kernel_of = {"eos": "k_eos_wright", "assemble": "k_assemble", "momentum": "k_momentum",
-                 "tracers": "k_tracers"}
+    kernel_of = {"eos": "k_eos_wright", "assemble": "k_assemble",
+                 "momentum": "k_momentum_mp" if mixed else "k_momentum",
+                 "tracers": "k_tracers_mp" if mixed else "k_tracers"}
     dom = max(("assemble", "momentum", "tracers", "eos"), key=lambda k: stage_ms[k])
     peak, peak_kind = peaks()
     achieved = bpc[dom] * cells / (stage_ms[dom] / 1e3) / 1e9
@@ -366,10 +416,11 @@ def main():
     clocks = clk.summary()
     line = {"metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config_out,
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": 4 * args.steps, "clocks": clocks,
-            "mode": "plain FP64, bit-identical to the CPU restatement"}
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if mixed else "f64", "data": "synthetic",
+            "config": config_out, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": (5 if mixed else 4) * args.steps, "clocks": clocks, "forms": forms,
+            "mode": ("FP64 state, FP32 Thomas sweeps with FP64 residual correction (mixed_precision=1)" if mixed
+                     else "plain FP64, bit-identical to the CPU restatement")}
     vp.close()
     if dist is not None:
         dist.barrier()
