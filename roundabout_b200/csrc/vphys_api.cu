@@ -74,6 +74,7 @@ struct vphys_handle_s {
     double *smooth_scratch = nullptr;
     double *budget_scratch = nullptr;
     int *span = nullptr;              // live spans of the columns (mixed-precision tracer solve)
+    double *zcol = nullptr;           // column depths for the momentum face thickness
 };
 
 namespace {
@@ -260,6 +261,7 @@ Params make_params(vphys_handle h)
     p.guard_count = h->guard_dev;
     p.budget_scratch = h->budget_scratch;
     p.span = h->span;
+    p.zcol = h->zcol;
     p.ks_equals_kt = (h->cfg.bkgnd_profile || h->cfg.kt_bg == h->cfg.ks_bg) ? 1 : 0;
     p.write_gamma = (p.gamma_t && p.gamma_s) ? 1 : 0;
     return p;
@@ -269,6 +271,14 @@ Params make_params(vphys_handle h)
 int prepare_momentum(vphys_handle h)
 {
     int st = VPHYS_OK;
+    if (h->cfg.hvel_mom6 && !h->cfg.hvel_harmonic && !h->zcol) {
+        cudaError_t e = cudaMalloc(&h->zcol, (size_t)h->nx * h->ny * sizeof(double));
+        if (e != cudaSuccess) {
+            h->zcol = nullptr;
+            cudaGetLastError();
+            return push_error(VPHYS_ERR_ALLOC, "cudaMalloc of the column depths failed");
+        }
+    }
     if (h->cfg.remnant) {
         if ((st = ensure(h, VPHYS_FIELD_VISC_REM_U))) return st;
         if ((st = ensure(h, VPHYS_FIELD_VISC_REM_V))) return st;
@@ -502,6 +512,7 @@ int vphys_destroy(vphys_handle *hp)
     if (h->smooth_scratch) cudaFree(h->smooth_scratch);
     if (h->budget_scratch) cudaFree(h->budget_scratch);
     if (h->span) cudaFree(h->span);
+    if (h->zcol) cudaFree(h->zcol);
     h->magic = 0;
     delete h;
     return VPHYS_OK;

@@ -462,12 +462,11 @@ __device__ __forceinline__ void solve_face(const Params &p, double dt, int i, in
         bbl_thick = c.hbbl_visc;
     }
     const double i_hbbl = 1.0 / (bbl_thick + EPS_HVEL);
+    // column depths (k_column_depth: the same k = 1..nz accumulation)
     double zacc = 0.0, zcol_l = 0.0, zcol_r = 0.0;
     if (c.hvel_mom6 && !c.hvel_harmonic) {
-        for (int k = 1; k <= nz; ++k) {
-            zcol_l = zcol_l - __ldg(hl + P * (size_t)(k - 1));
-            zcol_r = zcol_r - __ldg(hr + P * (size_t)(k - 1));
-        }
+        zcol_l = p.zcol[cl];
+        zcol_r = p.zcol[cr];
     }
     const double d_min = fmn(-zcol_l, -zcol_r);
     int kb_live = kb;
@@ -701,8 +700,38 @@ void launch_smooth(const Params &p, double *fld, double *scratch, cudaStream_t s
     }
 }
 
+// -sum_{k=1..nz} h of every column, accumulated in the order of
+// diffuse_velocity_columns_impl's z_clear pre-pass (rdb_ocean_vdiff.F90:1621-1700),
+// so the momentum kernels read two numbers per face instead of 2*nz.
+__global__ void k_column_depth(const Params p)
+{
+    constexpr int U = 8;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (i >= p.nx) return;
+    const size_t col = (size_t)i + (size_t)p.nx * j;
+    const double *__restrict__ hp = p.h + col;
+    const size_t P = p.plane;
+    double z = 0.0;
+    for (int k0 = 0; k0 < p.nz; k0 += U) {
+        double hv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) hv[u] = (k0 + u < p.nz) ? __ldg(hp + P * (size_t)(k0 + u)) : 0.0;
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (k0 + u < p.nz) z = z - hv[u];
+    }
+    p.zcol[col] = z;
+}
+
+void launch_column_depth(const Params &p, cudaStream_t stream)
+{
+    k_column_depth<<<dim3((p.nx + 127) / 128, p.ny), 128, 0, stream>>>(p);
+}
+
 void launch_momentum(const Params &p, double dt, cudaStream_t stream)
 {
+    if (p.cfg.hvel_mom6 && !p.cfg.hvel_harmonic) launch_column_depth(p, stream);
     if (p.cfg.mixed_precision) {
         launch_momentum_mp(p, dt, stream);
         return;

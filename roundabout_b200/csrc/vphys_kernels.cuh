@@ -33,6 +33,7 @@ struct Params {
     double *tr[NTR_MAX];
     unsigned long long *guard_count;  // vmix_guard counter (device)
     int *span;                        // per column: first | last live layer << 16 (0: none), scratch
+    double *zcol;                     // per column: -sum_k h, k = 1..nz in order (momentum z_clear), scratch
     int ks_equals_kt;                 // ks is bitwise kt after the gate
     int write_gamma;
 };
@@ -46,6 +47,8 @@ void launch_stress_mag(const Params &p, cudaStream_t stream);
 void launch_assemble(const Params &p, cudaStream_t stream);
 void launch_smooth(const Params &p, double *fld, double *scratch, cudaStream_t stream);
 void launch_momentum(const Params &p, double dt, cudaStream_t stream);
+// -sum of h over each column, accumulated k = 1..nz as vdiff's z_clear does (into p.zcol)
+void launch_column_depth(const Params &p, cudaStream_t stream);
 void launch_tracers(const Params &p, double dt, bool diffuse, bool nonlocal, cudaStream_t stream);
 // mixed-precision solves (vphys_mixed.cu), dispatched by the two above when cfg.mixed_precision
 void launch_momentum_mp(const Params &p, double dt, cudaStream_t stream);

@@ -322,11 +322,9 @@ __device__ __forceinline__ void solve_face_mp(const Params &p, double dt, int i,
     const float i_hbbl = __frcp_rn(bbl_thick + (float)EPS_HVEL);
     const float dtf = (float)dt;
     float zacc = 0.0f, zcol_l = 0.0f, zcol_r = 0.0f;
-    if (c.hvel_mom6 && !c.hvel_harmonic) {
-        for (int k = 1; k <= nz; ++k) {
-            zcol_l = zcol_l - (float)__ldg(hl + P * (size_t)(k - 1));
-            zcol_r = zcol_r - (float)__ldg(hr + P * (size_t)(k - 1));
-        }
+    if (c.hvel_mom6 && !c.hvel_harmonic) {   // column depths (k_column_depth)
+        zcol_l = (float)p.zcol[cl];
+        zcol_r = (float)p.zcol[cr];
     }
     const float d_min = fmn(-zcol_l, -zcol_r);
     int kb_live = kb;
