@@ -314,6 +314,25 @@ int vphys_smooth_121_static(double *fld, const double *wet, int nx, int ny, int 
  * language can verify its mirror of the struct before passing one. */
 size_t vphys_config_sizeof(void);
 
+/* ---- learned KPP surrogate: building blocks ---------------------------------
+ * No counterpart in the reference (whose KPP is the bulk-Richardson search of
+ * vmix_kpp_overlay_impl, rdb_ocean_vmix.F90:1121-1516); these serve the MLP
+ * that stands in for it when cfg.learned_kpp is set.  All pointers are device
+ * pointers; all calls are asynchronous on `stream` (cudaStream_t, NULL: the
+ * legacy default stream).
+ *
+ * vphys_gemm_tn_bf16: C[M,N] = alpha * A[M,K] . B[N,K]^T on the tcgen05 tensor
+ * cores, BF16 operands (row-major, K contiguous, 16-byte aligned, K % 8 == 0),
+ * FP32 accumulation, 16 <= N <= 256 with N % 16 == 0.  Epilogue, per element:
+ * v = alpha*acc (+ bias[col]) (* GELU'(zin[row*ld_z+col]) when zin);
+ * out_f32[row*ld_f32+col] = v; a = act ? GELU(v) : v (tanh form);
+ * out_bf16[row*ld_bf16+col] = bf16(a); out_bf16_t[col*ld_t+row] = bf16(a).
+ * Every output may be NULL.  A stalled pipeline writes a non-zero code to
+ * *err (device int) instead of hanging. */
+int vphys_gemm_tn_bf16(const void *A, const void *B, int M, int N, int K, float alpha, const float *bias,
+                       const float *zin, int ld_z, int act, float *out_f32, int ld_f32, void *out_bf16,
+                       int ld_bf16, void *out_bf16_t, int ld_t, int *err, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -179,6 +179,10 @@ _PROTOTYPES = {
                                                 ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
     "vphys_selftest_division": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_ulonglong, ctypes.c_int, ctypes.c_int,
                                                 ctypes.POINTER(ctypes.c_ulonglong)]),
+    "vphys_gemm_tn_bf16": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                          ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                          ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]),
 }
 
 EXPORTED_SYMBOLS = tuple(_PROTOTYPES)

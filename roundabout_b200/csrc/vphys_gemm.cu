@@ -1,0 +1,341 @@
+// vphys_gemm.cu -- BF16 x BF16 -> FP32 GEMM on the 5th-generation tensor
+// cores (tcgen05), the building block of the learned KPP surrogate's forward
+// and backward passes.
+//
+//   C[M, N] = alpha * A[M, K] . B[N, K]^T      (both operands K-contiguous, "TN")
+//
+// followed by a fused epilogue: + bias[N], optional multiplication by
+// GELU'(z) of a saved pre-activation (the backward of a GELU layer), storing
+// FP32 (pre-activation or plain), BF16 of GELU(v) or v, and/or a transposed
+// BF16 copy (the operand layout the weight-gradient GEMMs read).
+//
+// One CTA computes a 128-row tile against all N <= 256 output columns:
+//   * warp 0 lane 0 streams K in 64-element steps with TMA
+//     (cp.async.bulk.tensor, 128-byte swizzle) into a 4-stage ring,
+//   * warp 1 lane 0 issues tcgen05.mma (M=128, N, K=16) from the shared-memory
+//     descriptors into an FP32 accumulator in tensor memory and releases each
+//     stage with tcgen05.commit,
+//   * all four warps read their 32 accumulator lanes back with tcgen05.ld.
+// Every mbarrier wait is bounded: on expiry the CTA records an error code in
+// *err, skips the rest of its work and still frees its tensor memory.
+// No load is multicast; the kernel runs on the calling GPU's memory only.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <cstdint>
+#include <mutex>
+
+#include "../../include/vphys.h"
+#include "vphys_kernels.cuh"
+
+namespace vphys {
+
+constexpr int GM = 128;        // rows per CTA (tcgen05 M)
+constexpr int GK = 64;         // K per stage: one 128-byte swizzle row of BF16
+constexpr int GSTAGES = 4;
+constexpr int GN_MAX = 256;    // N per CTA (tcgen05 N <= 256)
+constexpr int GEMM_THREADS = 128;
+constexpr uint32_t TMEM_COLS = 256;
+constexpr size_t GEMM_SMEM = (size_t)GSTAGES * (GM + GN_MAX) * GK * 2 + 1024 /* barriers */ + 1024 /* align */;
+constexpr long long WAIT_LIMIT = 1LL << 24;   // try_wait polls before a wait is declared lost
+
+struct GemmEpi {
+    int M, N, K;
+    float alpha;
+    const float *bias;      // [N] or null
+    const float *zin;       // [M, ld_z] pre-activation: multiply by GELU'(z), or null
+    int ld_z;
+    int act;                // 1: the BF16 outputs hold GELU(v), 0: v
+    float *out_f32;         // [M, ld_f32] v (before the activation), or null
+    int ld_f32;
+    __nv_bfloat16 *out_bf16;    // [M, ld_bf16], or null
+    int ld_bf16;
+    __nv_bfloat16 *out_bf16_t;  // [N, ld_t] transposed, or null
+    int ld_t;
+    int *err;
+};
+
+// ---- small PTX wrappers ----------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// bounded wait for the phase of parity `parity` to complete; false on expiry
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+{
+    const uint32_t a = smem_u32(bar);
+    for (long long it = 0; it < WAIT_LIMIT; ++it) {
+        uint32_t ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(smem_u32(dst)), "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
+// 1024 B apart (SBO), descriptor version 1 (sm_100)
+__device__ __forceinline__ uint64_t smem_desc_sw128(const void *p)
+{
+    const uint64_t addr = smem_u32(p);
+    uint64_t d = 0;
+    d |= (addr >> 4) & 0x3FFFull;            // start address, bits [0,14)
+    d |= (uint64_t)(16 >> 4) << 16;          // leading byte offset (unused with this swizzle), bits [16,30)
+    d |= (uint64_t)(1024 >> 4) << 32;        // stride byte offset, bits [32,46)
+    d |= (uint64_t)1 << 46;                  // version, bits [46,48)
+    d |= (uint64_t)2 << 61;                  // layout: 128-byte swizzle, bits [61,64)
+    return d;
+}
+// instruction descriptor, kind::f16: BF16 A and B, FP32 D, both K-major
+__device__ __forceinline__ uint32_t idesc_bf16(int m, int n)
+{
+    uint32_t d = 0;
+    d |= 1u << 4;                        // D format: F32
+    d |= 1u << 7;                        // A format: BF16
+    d |= 1u << 10;                       // B format: BF16
+    d |= (uint32_t)(n >> 3) << 17;       // N / 8
+    d |= (uint32_t)(m >> 4) << 24;       // M / 16
+    return d;
+}
+
+__device__ __forceinline__ float gelu_tanh(float x)
+{
+    // GELU, tanh form (Hendrycks & Gimpel 2016)
+    const float c = 0.7978845608028654f;   // sqrt(2/pi)
+    const float t = tanhf(c * (x + 0.044715f * x * x * x));
+    return 0.5f * x * (1.0f + t);
+}
+__device__ __forceinline__ float gelu_tanh_grad(float x)
+{
+    const float c = 0.7978845608028654f;
+    const float t = tanhf(c * (x + 0.044715f * x * x * x));
+    return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * c * (1.0f + 3.0f * 0.044715f * x * x);
+}
+
+__global__ void __launch_bounds__(GEMM_THREADS, 1)
+    k_gemm_tn(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const GemmEpi g)
+{
+    extern __shared__ uint8_t smraw[];
+    uint8_t *sm = reinterpret_cast<uint8_t *>(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
+    __nv_bfloat16 *sa = reinterpret_cast<__nv_bfloat16 *>(sm);
+    __nv_bfloat16 *sb = sa + (size_t)GSTAGES * GM * GK;
+    uint64_t *full = reinterpret_cast<uint64_t *>(sb + (size_t)GSTAGES * GN_MAX * GK);
+    uint64_t *empty = full + GSTAGES;
+    uint64_t *done = empty + GSTAGES;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
+    int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.x * GM;
+    const int N = g.N;
+    const int nk = (g.K + GK - 1) / GK;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < GSTAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(done, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // ---- TMA producer ----
+        const uint32_t bytes = (uint32_t)(GM + N) * GK * 2;
+        for (int kt = 0; kt < nk; ++kt) {
+            const int s = kt % GSTAGES;
+            const uint32_t round = kt / GSTAGES;
+            if (!mbar_wait(&empty[s], (round & 1) ^ 1)) {
+                atomicExch(g.err, 1);
+                *(volatile int *)abort_flag = 1;
+                break;
+            }
+            mbar_expect_tx(&full[s], bytes);
+            tma_load_2d(sa + (size_t)s * GM * GK, &tmA, kt * GK, m0, &full[s]);
+            tma_load_2d(sb + (size_t)s * GN_MAX * GK, &tmB, kt * GK, 0, &full[s]);
+        }
+    } else if (warp == 1 && lane == 0) {
+        // ---- MMA issuer ----
+        const uint32_t idesc = idesc_bf16(GM, N);
+        int issued = 0;
+        for (int kt = 0; kt < nk; ++kt) {
+            const int s = kt % GSTAGES;
+            const uint32_t round = kt / GSTAGES;
+            if (!mbar_wait(&full[s], round & 1)) {
+                atomicExch(g.err, 2);
+                *(volatile int *)abort_flag = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const __nv_bfloat16 *as = sa + (size_t)s * GM * GK;
+            const __nv_bfloat16 *bs = sb + (size_t)s * GN_MAX * GK;
+#pragma unroll
+            for (int kk = 0; kk < GK / 16; ++kk) {
+                const uint64_t ad = smem_desc_sw128(as + kk * 16);
+                const uint64_t bd = smem_desc_sw128(bs + kk * 16);
+                const uint32_t acc = (kt > 0 || kk > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                    " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+                    "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(&empty[s]))
+                         : "memory");
+            ++issued;
+        }
+        // signals when every MMA issued so far has completed (also after an abort)
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_u32(done))
+                     : "memory");
+        (void)issued;
+    }
+
+    // ---- epilogue: every warp reads its 32 accumulator lanes ----
+    __syncwarp();
+    const bool ok = mbar_wait(done, 0);
+    if (!ok && threadIdx.x == 0) atomicExch(g.err, 3);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const bool skip = !ok || *(volatile int *)abort_flag;
+    const int row = m0 + warp * 32 + lane;
+    if (!skip) {
+        for (int c0 = 0; c0 < N; c0 += 16) {
+            uint32_t r[16];
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (row < g.M) {
+#pragma unroll
+                for (int q = 0; q < 16; ++q) {
+                    const int col = c0 + q;
+                    if (col >= N) break;
+                    float v = g.alpha * __uint_as_float(r[q]);
+                    if (g.bias) v += g.bias[col];
+                    if (g.zin) v *= gelu_tanh_grad(g.zin[(size_t)row * g.ld_z + col]);
+                    if (g.out_f32) g.out_f32[(size_t)row * g.ld_f32 + col] = v;
+                    const float a = g.act ? gelu_tanh(v) : v;
+                    const __nv_bfloat16 ab = __float2bfloat16_rn(a);
+                    if (g.out_bf16) g.out_bf16[(size_t)row * g.ld_bf16 + col] = ab;
+                    if (g.out_bf16_t) g.out_bf16_t[(size_t)col * g.ld_t + row] = ab;
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+}
+
+// ---- host side ---------------------------------------------------------------
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// 2-D BF16 row-major [rows, cols] (cols contiguous) tiled {64, box_rows}, 128-byte swizzle
+static bool make_map(CUtensorMap *m, const void *base, int rows, int cols, int box_rows)
+{
+    auto fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
+    cuuint32_t box[2] = {(cuuint32_t)GK, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+int gemm_tn_bf16(const void *A, const void *B, int M, int N, int K, float alpha, const float *bias, const float *zin,
+                 int ld_z, int act, float *out_f32, int ld_f32, void *out_bf16, int ld_bf16, void *out_bf16_t, int ld_t,
+                 int *err, cudaStream_t stream)
+{
+    if (M <= 0 || N < 16 || N > GN_MAX || (N % 16) != 0 || K <= 0 || (K % 8) != 0)
+        return report_error(VPHYS_ERR_BAD_SHAPE, "vphys_gemm_tn_bf16: need M > 0, 16 <= N <= 256 with N % 16 == 0, "
+                                                 "K > 0 with K % 8 == 0");
+    if (((uintptr_t)A | (uintptr_t)B) & 15)
+        return report_error(VPHYS_ERR_BAD_SHAPE, "vphys_gemm_tn_bf16: A and B must be 16-byte aligned");
+    CUtensorMap ma, mb;
+    if (!make_map(&ma, A, M, K, GM) || !make_map(&mb, B, N, K, N))
+        return report_error(VPHYS_ERR_CUDA, "vphys_gemm_tn_bf16: cuTensorMapEncodeTiled failed");
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_gemm_tn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM);
+        attr_set = true;
+    }
+    GemmEpi g{};
+    g.M = M;
+    g.N = N;
+    g.K = K;
+    g.alpha = alpha;
+    g.bias = bias;
+    g.zin = zin;
+    g.ld_z = ld_z;
+    g.act = act;
+    g.out_f32 = out_f32;
+    g.ld_f32 = ld_f32;
+    g.out_bf16 = reinterpret_cast<__nv_bfloat16 *>(out_bf16);
+    g.ld_bf16 = ld_bf16;
+    g.out_bf16_t = reinterpret_cast<__nv_bfloat16 *>(out_bf16_t);
+    g.ld_t = ld_t;
+    g.err = err;
+    k_gemm_tn<<<(M + GM - 1) / GM, GEMM_THREADS, GEMM_SMEM, stream>>>(ma, mb, g);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return report_error(VPHYS_ERR_CUDA, cudaGetErrorString(e));
+    return VPHYS_OK;
+}
+
+}  // namespace vphys
+
+extern "C" int vphys_gemm_tn_bf16(const void *A, const void *B, int M, int N, int K, float alpha, const float *bias,
+                                  const float *zin, int ld_z, int act, float *out_f32, int ld_f32, void *out_bf16,
+                                  int ld_bf16, void *out_bf16_t, int ld_t, int *err, void *stream)
+{
+    return vphys::gemm_tn_bf16(A, B, M, N, K, alpha, bias, zin, ld_z, act, out_f32, ld_f32, out_bf16, ld_bf16,
+                               out_bf16_t, ld_t, err, reinterpret_cast<cudaStream_t>(stream));
+}

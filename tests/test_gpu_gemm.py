@@ -1,0 +1,104 @@
+"""The tcgen05 BF16 GEMM (vphys_gemm_tn_bf16) against a torch FP32 matmul of
+the same BF16 operands.  FP32 accumulation in a different order: relative
+tolerance 2e-3 of the output's scale (bf16 outputs: one bf16 ulp more)."""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def env():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from roundabout_b200 import _ffi
+
+    return torch, _ffi.get_lib(), _ffi
+
+
+def P(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def gelu(x):
+    import torch
+
+    return 0.5 * x * (1.0 + torch.tanh(0.7978845608028654 * (x + 0.044715 * x ** 3)))
+
+
+def gelu_grad(x):
+    import torch
+
+    t = torch.tanh(0.7978845608028654 * (x + 0.044715 * x ** 3))
+    return 0.5 * (1 + t) + 0.5 * x * (1 - t * t) * 0.7978845608028654 * (1 + 3 * 0.044715 * x * x)
+
+
+def run(env, A, B, alpha=1.0, bias=None, zin=None, act=0, f32=True, bf16=False, bf16_t=False):
+    torch, lib, _ffi = env
+    M, K = A.shape
+    N = B.shape[0]
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    o32 = torch.full((M, N), float("nan"), device="cuda") if f32 else None
+    o16 = torch.zeros((M, N), dtype=torch.bfloat16, device="cuda") if bf16 else None
+    o16t = torch.zeros((N, M), dtype=torch.bfloat16, device="cuda") if bf16_t else None
+    st = lib.vphys_gemm_tn_bf16(P(A), P(B), M, N, K, float(alpha), P(bias), P(zin), N, act, P(o32), N, P(o16), N,
+                                P(o16t), M, P(err), None)
+    assert st == 0, _ffi.last_error()
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    return o32, o16, o16t
+
+
+@pytest.mark.parametrize("M,N,K", [(128, 256, 160), (300, 80, 256), (1000, 160, 64), (77, 16, 8), (4096, 256, 256),
+                                   (80, 256, 16384), (256, 160, 4104)])
+def test_gemm_plain(env, M, N, K):
+    torch = env[0]
+    g = torch.Generator(device="cuda").manual_seed(M * 7 + N * 3 + K)
+    A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
+    B = torch.randn(N, K, device="cuda", generator=g).to(torch.bfloat16)
+    o32, _, _ = run(env, A, B, alpha=0.5)
+    ref = 0.5 * (A.float() @ B.float().T)
+    scale = float(ref.abs().max())
+    diff = float((o32 - ref).abs().max())
+    assert diff <= 2e-3 * scale, (diff, scale)
+
+
+def test_gemm_epilogue_gelu_bias_transposed(env):
+    torch = env[0]
+    M, N, K = 520, 256, 160
+    g = torch.Generator(device="cuda").manual_seed(11)
+    A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
+    B = (0.1 * torch.randn(N, K, device="cuda", generator=g)).to(torch.bfloat16)
+    bias = torch.randn(N, device="cuda", generator=g)
+    o32, o16, o16t = run(env, A, B, bias=bias, act=1, f32=True, bf16=True, bf16_t=True)
+    z = A.float() @ B.float().T + bias
+    assert float((o32 - z).abs().max()) <= 2e-3 * float(z.abs().max())
+    a = gelu(z)
+    tol = 2e-3 * float(a.abs().max()) + 1e-2 * float(a.abs().max()) / 128
+    assert float((o16.float() - a).abs().max()) <= tol
+    assert torch.equal(o16t, o16.T.contiguous())
+
+
+def test_gemm_epilogue_gelu_backward(env):
+    torch = env[0]
+    M, N, K = 333, 256, 80
+    g = torch.Generator(device="cuda").manual_seed(12)
+    A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
+    B = torch.randn(N, K, device="cuda", generator=g).to(torch.bfloat16)
+    zin = torch.randn(M, N, device="cuda", generator=g)
+    o32, _, _ = run(env, A, B, zin=zin)
+    ref = (A.float() @ B.float().T) * gelu_grad(zin)
+    assert float((o32 - ref).abs().max()) <= 2e-3 * float(ref.abs().max())
+
+
+def test_gemm_rejects_bad_shapes(env):
+    torch, lib, _ffi = env
+    A = torch.zeros(128, 64, dtype=torch.bfloat16, device="cuda")
+    B = torch.zeros(24, 64, dtype=torch.bfloat16, device="cuda")   # N % 16 != 0
+    st = lib.vphys_gemm_tn_bf16(P(A), P(B), 128, 24, 64, 1.0, None, None, 0, 0, None, 0, None, 0, None, 0, None,
+                                None)
+    assert st == _ffi.ERR_BAD_SHAPE
