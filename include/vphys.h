@@ -144,7 +144,9 @@ typedef struct vphys_config {
     int mixed_precision;      /* 0: FP64 throughout (bitwise the reference's arithmetic);
                                  1: FP64 assembly, FP32 Thomas sweeps + FP64 residual correction;
                                  2: as 1 with the assembly's interface sweep in FP32 too */
-    int pad1;
+    int learned_kpp;          /* 1: the KPP boundary-layer depth comes from the attached MLP surrogate
+                                 (vphys_kpp_attach), with the range gate and the sampled plain-KPP
+                                 check; 0: the reference's bulk-Richardson search */
 } vphys_config;
 
 /* ---- field ids (vphys_bind / vphys_set_field / vphys_get_field) ----- */
@@ -176,6 +178,7 @@ enum vphys_field {
     VPHYS_FIELD_K_TOP_V = 24,   /* in int32 (nx, ny+1) */
     VPHYS_FIELD_K_BOT_U = 25,   /* in int32 (nx+1, ny), 1-based (default 1) */
     VPHYS_FIELD_K_BOT_V = 26,   /* in int32 (nx, ny+1) */
+    VPHYS_FIELD_CORIOLIS = 27,  /* in      (nx, ny)  f, 1/s: read only by the learned KPP's features */
     VPHYS_FIELD_TRACER0 = 64    /* in/out  (nx, ny, nz); tracer t is
                                    VPHYS_FIELD_TRACER0 + t */
 };
@@ -322,16 +325,65 @@ size_t vphys_config_sizeof(void);
  * legacy default stream).
  *
  * vphys_gemm_tn_bf16: C[M,N] = alpha * A[M,K] . B[N,K]^T on the tcgen05 tensor
- * cores, BF16 operands (row-major, K contiguous, 16-byte aligned, K % 8 == 0),
+ * cores, BF16 operands (row-major, K contiguous, rows lda / ldb elements apart,
+ * 16-byte aligned, K, lda, ldb multiples of 8),
  * FP32 accumulation, 16 <= N <= 256 with N % 16 == 0.  Epilogue, per element:
  * v = alpha*acc (+ bias[col]) (* GELU'(zin[row*ld_z+col]) when zin);
  * out_f32[row*ld_f32+col] = v; a = act ? GELU(v) : v (tanh form);
  * out_bf16[row*ld_bf16+col] = bf16(a); out_bf16_t[col*ld_t+row] = bf16(a).
  * Every output may be NULL.  A stalled pipeline writes a non-zero code to
  * *err (device int) instead of hanging. */
-int vphys_gemm_tn_bf16(const void *A, const void *B, int M, int N, int K, float alpha, const float *bias,
-                       const float *zin, int ld_z, int act, float *out_f32, int ld_f32, void *out_bf16,
-                       int ld_bf16, void *out_bf16_t, int ld_t, int *err, void *stream);
+/* The surrogate's weights and settings (device pointers stay owned by the
+ * caller and must outlive the attachment).  Shapes: w1 BF16 [256, 160]
+ * (inputs beyond 154 zero), w2 [256, 256], w3 [80, 256] (outputs beyond 77
+ * unused), each row-major [out, in]; b1, b2 [256], b3 [80] FP32; feat_mean /
+ * feat_istd [160] FP32 (features are (x - mean) * istd); the OBL-depth output
+ * y0 is de-standardised as h_b = 10 m * exp(y0 * target_std0 + target_mean0). */
+typedef struct vphys_kpp_model {
+    const void *w1, *w2, *w3;
+    const float *b1, *b2, *b3;
+    const float *feat_mean, *feat_istd;
+    float target_mean0, target_std0;
+    float gate_limit;       /* |standardised feature| beyond which a column takes the plain KPP (e.g. 6) */
+    float check_fraction;   /* fraction of columns re-run by the plain KPP each step (e.g. 0.01) */
+    float check_tolerance;  /* relative h_b error counted as a failed check (e.g. 0.25) */
+    float fail_fraction;    /* failed share of the checked columns that sends the next step to the plain KPP */
+} vphys_kpp_model;
+
+/* Attach (m != NULL) or detach (m == NULL) the surrogate; allocates one
+ * inference's scratch (about 1.7 kB per column).  With cfg.learned_kpp and
+ * cfg.use_kpp, vphys_assemble and vphys_step then run features -> MLP ->
+ * gate/check before the assembly, whose pass 1 runs only where needed. */
+int vphys_kpp_attach(vphys_handle h, const vphys_kpp_model *m);
+/* Counters (synchronises the handle's stream): [0] checked in the last step,
+ * [1] failed, [2] fallback flag of the last step, [3] gated in the last step,
+ * [4] checked in total, [5] failed in total, [6] fallback steps, [7] gated in
+ * total, [8] sum of squared relative h_b errors of the checks * 1e6, [9]
+ * steps, [10] tensor-core GEMM error code (0).  n: entries wanted (<= 16). */
+int vphys_kpp_stats(vphys_handle h, unsigned long long *out, int n);
+/* Features of the handle's current state: raw FP32 [ncols, 154] and/or
+ * standardised BF16 X [ncols, 160] / XT [160, ld_t] (mean, istd NULL: raw
+ * values), the per-column gate flag and column depth (-1: no live layer). */
+int vphys_kpp_features(vphys_handle h, const float *mean, const float *istd, float gate_limit, float *raw, void *X,
+                       void *XT, long long ld_t, unsigned char *gate, float *colH);
+/* Training targets [ncols, 80] FP32 from the state left by a plain assembly. */
+int vphys_kpp_targets(vphys_handle h, float *T);
+/* Training helpers: dY = scale*w*(Y - T) (+ loss += sum w (Y-T)^2); column
+ * sums; column sums and sums of squares (FP64); standardisation into BF16 /
+ * transposed BF16 / FP32; one Adam step (step >= 1) refreshing BF16 copies. */
+int vphys_mlp_loss(const float *Y, const float *T, const float *w, int rows, int cols, float scale, float *dY32,
+                   void *dY, void *dYT, float *loss, void *stream);
+int vphys_mlp_colsum(const float *G, int rows, int cols, int ld, float *out, void *stream);
+int vphys_mlp_colstats(const float *X, long long rows, int cols, int ld, double *sum, double *sumsq, void *stream);
+int vphys_mlp_standardize(const float *raw, long long rows, int cols_in, int ld_in, const float *mean,
+                          const float *istd, int cols_out, void *X, void *XT, long long ld_t, float *out32,
+                          void *stream);
+int vphys_mlp_adam(float *w, float *m, float *v, const float *g, int rows, int cols, float lr, float b1, float b2,
+                   float eps, int step, void *wb, void *wbt, void *stream);
+
+int vphys_gemm_tn_bf16(const void *A, long long lda, const void *B, long long ldb, int M, int N, int K,
+                       float alpha, const float *bias, const float *zin, int ld_z, int act, float *out_f32,
+                       int ld_f32, void *out_bf16, int ld_bf16, void *out_bf16_t, int ld_t, int *err, void *stream);
 
 #ifdef __cplusplus
 }

@@ -62,6 +62,7 @@ FIELD_K_TOP_U = 23
 FIELD_K_TOP_V = 24
 FIELD_K_BOT_U = 25
 FIELD_K_BOT_V = 26
+FIELD_CORIOLIS = 27
 FIELD_TRACER0 = 64
 
 FIELD_NAMES = {
@@ -72,7 +73,7 @@ FIELD_NAMES = {
     "visc_rem_u": FIELD_VISC_REM_U, "visc_rem_v": FIELD_VISC_REM_V, "gamma_t": FIELD_GAMMA_T,
     "gamma_s": FIELD_GAMMA_S, "heat_budget": FIELD_HEAT_BUDGET, "salt_budget": FIELD_SALT_BUDGET,
     "k_top_u": FIELD_K_TOP_U, "k_top_v": FIELD_K_TOP_V, "k_bot_u": FIELD_K_BOT_U,
-    "k_bot_v": FIELD_K_BOT_V,
+    "k_bot_v": FIELD_K_BOT_V, "coriolis": FIELD_CORIOLIS,
 }
 INT_FIELDS = (FIELD_K_TOP_U, FIELD_K_TOP_V, FIELD_K_BOT_U, FIELD_K_BOT_V)
 
@@ -87,7 +88,7 @@ def field_shape(field: int, nx: int, ny: int, nz: int):
         return (nx, ny + 1, nz)
     if field in (FIELD_KV, FIELD_KT, FIELD_KS, FIELD_GAMMA_T, FIELD_GAMMA_S):
         return (nx, ny, nz + 1)
-    if field in (FIELD_BL_DEPTH, FIELD_B0, FIELD_STRESS_MAG, FIELD_Q_HEAT, FIELD_Q_SALT, FIELD_WET):
+    if field in (FIELD_BL_DEPTH, FIELD_B0, FIELD_STRESS_MAG, FIELD_Q_HEAT, FIELD_Q_SALT, FIELD_WET, FIELD_CORIOLIS):
         return (nx, ny)
     if field in (FIELD_TAU_X, FIELD_LAMBDA_BOT_U, FIELD_K_TOP_U, FIELD_K_BOT_U):
         return (nx + 1, ny)
@@ -119,11 +120,11 @@ class VphysConfig(ctypes.Structure):
         ("hbbl_visc", ctypes.c_double), ("bbl_piston", ctypes.c_double), ("kv_bbl_bg", ctypes.c_double),
         ("idx_temperature", ctypes.c_int), ("idx_salinity", ctypes.c_int), ("idx_pseudo_salt", ctypes.c_int),
         ("eos_in_step", ctypes.c_int), ("remnant", ctypes.c_int), ("budgets", ctypes.c_int),
-        ("mixed_precision", ctypes.c_int), ("pad1", ctypes.c_int),
+        ("mixed_precision", ctypes.c_int), ("learned_kpp", ctypes.c_int),
     ]
 
     def as_dict(self):
-        return {n: getattr(self, n) for n, _ in self._fields_ if n not in ("pad0", "pad1")}
+        return {n: getattr(self, n) for n, _ in self._fields_ if n not in ("pad0",)}
 
 
 class LibraryNotFoundError(FileNotFoundError):
@@ -149,6 +150,22 @@ def find_library() -> Path:
         f"{p} not found: build it with `python -c 'import __graft_entry__ as g; g.build()'` "
         "or `python -m roundabout_b200.build`")
 
+
+class KppModel(ctypes.Structure):
+    """Mirror of `struct vphys_kpp_model` (include/vphys.h)."""
+
+    _fields_ = [("w1", ctypes.c_void_p), ("w2", ctypes.c_void_p), ("w3", ctypes.c_void_p),
+                ("b1", ctypes.c_void_p), ("b2", ctypes.c_void_p), ("b3", ctypes.c_void_p),
+                ("feat_mean", ctypes.c_void_p), ("feat_istd", ctypes.c_void_p),
+                ("target_mean0", ctypes.c_float), ("target_std0", ctypes.c_float),
+                ("gate_limit", ctypes.c_float), ("check_fraction", ctypes.c_float),
+                ("check_tolerance", ctypes.c_float), ("fail_fraction", ctypes.c_float)]
+
+
+_V = ctypes.c_void_p
+_I = ctypes.c_int
+_F = ctypes.c_float
+_LL = ctypes.c_longlong
 
 _PROTOTYPES = {
     "vphys_config_default": (ctypes.c_int, [ctypes.POINTER(VphysConfig)]),
@@ -179,7 +196,17 @@ _PROTOTYPES = {
                                                 ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
     "vphys_selftest_division": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_ulonglong, ctypes.c_int, ctypes.c_int,
                                                 ctypes.POINTER(ctypes.c_ulonglong)]),
-    "vphys_gemm_tn_bf16": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+    "vphys_kpp_attach": (_I, [_V, ctypes.POINTER(KppModel)]),
+    "vphys_kpp_stats": (_I, [_V, ctypes.POINTER(ctypes.c_ulonglong), _I]),
+    "vphys_kpp_features": (_I, [_V, _V, _V, _F, _V, _V, _V, _LL, _V, _V]),
+    "vphys_kpp_targets": (_I, [_V, _V]),
+    "vphys_mlp_loss": (_I, [_V, _V, _V, _I, _I, _F, _V, _V, _V, _V, _V]),
+    "vphys_mlp_colsum": (_I, [_V, _I, _I, _I, _V, _V]),
+    "vphys_mlp_colstats": (_I, [_V, _LL, _I, _I, _V, _V, _V]),
+    "vphys_mlp_standardize": (_I, [_V, _LL, _I, _I, _V, _V, _I, _V, _V, _LL, _V, _V]),
+    "vphys_mlp_adam": (_I, [_V, _V, _V, _V, _I, _I, _F, _F, _F, _F, _I, _V, _V, _V]),
+    "vphys_gemm_tn_bf16": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_void_p, ctypes.c_longlong,
+                                          ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                           ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                           ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
                                           ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]),

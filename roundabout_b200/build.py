@@ -20,10 +20,10 @@ CSRC = Path(__file__).resolve().parent / "csrc"
 OUT = CSRC / "_build"
 LIB = OUT / "libvphys.so"
 SOURCES = ["vphys_api.cu", "vphys_kernels.cu", "vphys_tracers.cu", "vphys_static.cu", "vphys_mixed.cu",
-           "vphys_gemm.cu"]
+           "vphys_gemm.cu", "vphys_learned.cu"]
 HEADERS = ["vphys_device.cuh", "vphys_faces.cuh", "vphys_kernels.cuh", "../../include/vphys.h"]
 # the mixed-precision solves carry no bitwise contract: FMA contraction allowed
-CONTRACT_OK = {"vphys_mixed.cu", "vphys_gemm.cu"}
+CONTRACT_OK = {"vphys_mixed.cu", "vphys_gemm.cu", "vphys_learned.cu"}
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2", "--expt-relaxed-constexpr"]

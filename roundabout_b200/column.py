@@ -137,6 +137,8 @@ class VerticalPhysics:
         self.set("q_heat", cols.q_heat)
         self.set("q_salt", cols.q_salt)
         self.set("wet", cols.wet)
+        if getattr(cols, "coriolis", None) is not None:
+            self.set("coriolis", cols.coriolis)
         self.stress_mag()
 
     # ---- the hot path --------------------------------------------------------

@@ -76,6 +76,7 @@ def default_config() -> VphysConfig:
     c.remnant = 0
     c.budgets = 0
     c.mixed_precision = 0
+    c.learned_kpp = 0
     return c
 
 

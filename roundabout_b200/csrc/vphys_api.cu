@@ -49,7 +49,7 @@ int cuda_status(cudaError_t e, const char *where)
     return push_error(VPHYS_ERR_CUDA, "%s: CUDA error %d (%s)", where, (int)e, cudaGetErrorString(e));
 }
 
-constexpr int NFIXED = 27;
+constexpr int NFIXED = 28;
 constexpr unsigned MAGIC = 0x56504859u;   // "VPHY"
 
 struct Field {
@@ -75,6 +75,15 @@ struct vphys_handle_s {
     double *budget_scratch = nullptr;
     int *span = nullptr;              // live spans of the columns (mixed-precision tracer solve)
     double *zcol = nullptr;           // column depths for the momentum face thickness
+    // learned KPP surrogate (vphys_kpp_attach): the caller's weights and the scratch of one inference
+    vphys_kpp_model kpp{};
+    bool kpp_attached = false;
+    void *kX = nullptr, *kH1 = nullptr, *kH2 = nullptr;
+    float *kY = nullptr, *kcolH = nullptr, *kpred = nullptr, *kcheck = nullptr;
+    unsigned char *kgate = nullptr;
+    unsigned long long *kstats = nullptr;
+    int *kerr = nullptr;
+    unsigned kgen = 0;
 };
 
 namespace {
@@ -112,7 +121,8 @@ size_t field_count(int nx, int ny, int nz, int field, bool *is_int)
     case VPHYS_FIELD_STRESS_MAG:
     case VPHYS_FIELD_Q_HEAT:
     case VPHYS_FIELD_Q_SALT:
-    case VPHYS_FIELD_WET: return X * Y;
+    case VPHYS_FIELD_WET:
+    case VPHYS_FIELD_CORIOLIS: return X * Y;
     case VPHYS_FIELD_TAU_X:
     case VPHYS_FIELD_LAMBDA_BOT_U: return (X + 1) * Y;
     case VPHYS_FIELD_TAU_Y:
@@ -262,6 +272,7 @@ Params make_params(vphys_handle h)
     p.budget_scratch = h->budget_scratch;
     p.span = h->span;
     p.zcol = h->zcol;
+    p.coriolis = D(VPHYS_FIELD_CORIOLIS);
     p.ks_equals_kt = (h->cfg.bkgnd_profile || h->cfg.kt_bg == h->cfg.ks_bg) ? 1 : 0;
     p.write_gamma = (p.gamma_t && p.gamma_s) ? 1 : 0;
     return p;
@@ -329,6 +340,52 @@ int prepare_assemble(vphys_handle h)
         }
     }
     return VPHYS_OK;
+}
+
+// The learned KPP pre-stage of an assembly: counters, features, the MLP on the
+// tensor cores, the gate/check/fallback decision per column.  Afterwards the
+// assembly reads p.kpp_pred / p.kpp_check.
+int run_learned_kpp(vphys_handle h, Params &p)
+{
+    if (!h->cfg.learned_kpp || !h->cfg.use_kpp) return VPHYS_OK;
+    if (!h->kpp_attached)
+        return push_error(VPHYS_ERR_NOT_INITIALISED, "learned_kpp = 1 but no surrogate attached (vphys_kpp_attach)");
+    const vphys_kpp_model &m = h->kpp;
+    cudaStream_t s = h->stream;
+    const int ncols = h->nx * h->ny;
+    vphys::launch_kpp_roll(h->kstats, m.fail_fraction, s);
+    vphys::launch_kpp_features(p, nullptr, h->kX, nullptr, 0, m.feat_mean, m.feat_istd, m.gate_limit, h->kgate,
+                               h->kcolH, s);
+    int st;
+    if ((st = vphys::gemm_tn_bf16(h->kX, vphys::LK_INP, m.w1, vphys::LK_INP, ncols, vphys::LK_HID, vphys::LK_INP,
+                                  1.0f, m.b1, nullptr, 0, 1, nullptr, 0, h->kH1, vphys::LK_HID, nullptr, 0, h->kerr, s)))
+        return st;
+    if ((st = vphys::gemm_tn_bf16(h->kH1, vphys::LK_HID, m.w2, vphys::LK_HID, ncols, vphys::LK_HID, vphys::LK_HID,
+                                  1.0f, m.b2, nullptr, 0, 1, nullptr, 0, h->kH2, vphys::LK_HID, nullptr, 0, h->kerr, s)))
+        return st;
+    if ((st = vphys::gemm_tn_bf16(h->kH2, vphys::LK_HID, m.w3, vphys::LK_HID, ncols, vphys::LK_OUTP, vphys::LK_HID,
+                                  1.0f, m.b3, nullptr, 0, 0, h->kY, vphys::LK_OUTP, nullptr, 0, nullptr, 0, h->kerr, s)))
+        return st;
+    vphys::launch_kpp_apply((size_t)ncols, h->kY, m.target_mean0, m.target_std0, h->kgate, h->kcolH, h->kpred,
+                            h->kcheck, h->kstats, h->kgen++, m.check_fraction, s);
+    p.kpp_pred = h->kpred;
+    p.kpp_check = h->kcheck;
+    p.kpp_stats = h->kstats;
+    p.kpp_tol = m.check_tolerance;
+    return cuda_status(cudaGetLastError(), "learned KPP launch");
+}
+
+void free_kpp(vphys_handle h)
+{
+    void *bufs[] = {h->kX, h->kH1, h->kH2, h->kY, h->kcolH, h->kpred, h->kcheck, h->kgate, h->kstats, h->kerr};
+    for (void *b : bufs)
+        if (b) cudaFree(b);
+    h->kX = h->kH1 = h->kH2 = nullptr;
+    h->kY = h->kcolH = h->kpred = h->kcheck = nullptr;
+    h->kgate = nullptr;
+    h->kstats = nullptr;
+    h->kerr = nullptr;
+    h->kpp_attached = false;
 }
 
 int run_assemble(vphys_handle h, const Params &p)
@@ -513,6 +570,7 @@ int vphys_destroy(vphys_handle *hp)
     if (h->budget_scratch) cudaFree(h->budget_scratch);
     if (h->span) cudaFree(h->span);
     if (h->zcol) cudaFree(h->zcol);
+    free_kpp(h);
     h->magic = 0;
     delete h;
     return VPHYS_OK;
@@ -636,6 +694,7 @@ int vphys_assemble(vphys_handle h)
         if (e != cudaSuccess) return cuda_status(e, "vphys_assemble guard reset");
     }
     Params p = make_params(h);
+    if ((st = run_learned_kpp(h, p))) return st;
     if ((st = run_assemble(h, p))) return st;
     if (h->cfg.vmix_guard) {
         int gs = VPHYS_OK;
@@ -690,7 +749,9 @@ int vphys_step(vphys_handle h, double dt, int n_steps)
     Params p = make_params(h);
     for (int n = 0; n < n_steps; ++n) {
         if (h->cfg.eos_in_step) vphys::launch_eos_wright(p, h->stream);
-        if ((st = run_assemble(h, p))) return st;
+        Params pa = p;
+        if ((st = run_learned_kpp(h, pa))) return st;
+        if ((st = run_assemble(h, pa))) return st;
         vphys::launch_momentum(p, dt, h->stream);
         if (h->ntr > 0) vphys::launch_tracers(p, dt, true, h->cfg.use_kpp != 0, h->stream);
         h->gen += 1;
@@ -708,6 +769,87 @@ int vphys_synchronize(vphys_handle h)
 {
     if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_synchronize: bad handle");
     return cuda_status(cudaStreamSynchronize(h->stream), "vphys_synchronize");
+}
+
+int vphys_kpp_attach(vphys_handle h, const vphys_kpp_model *m)
+{
+    if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_kpp_attach: bad handle");
+    if (!m) {
+        free_kpp(h);
+        return VPHYS_OK;
+    }
+    if (!m->w1 || !m->w2 || !m->w3 || !m->b1 || !m->b2 || !m->b3 || !m->feat_mean || !m->feat_istd)
+        return push_error(VPHYS_ERR_CONFIG, "vphys_kpp_attach: a weight, bias or standardisation pointer is NULL");
+    if (!(m->target_std0 > 0.0f) || !(m->gate_limit > 0.0f) || m->check_fraction < 0.0f || m->check_fraction > 1.0f)
+        return push_error(VPHYS_ERR_CONFIG, "vphys_kpp_attach: target_std0 and gate_limit must be > 0, "
+                                            "check_fraction in [0, 1]");
+    if ((((uintptr_t)m->w1) | ((uintptr_t)m->w2) | ((uintptr_t)m->w3)) & 15)
+        return push_error(VPHYS_ERR_BAD_SHAPE, "vphys_kpp_attach: weights must be 16-byte aligned");
+    free_kpp(h);
+    const size_t nc = (size_t)h->nx * h->ny;
+    struct {
+        void **p;
+        size_t bytes;
+    } want[] = {{&h->kX, nc * vphys::LK_INP * 2},
+                {&h->kH1, nc * vphys::LK_HID * 2},
+                {&h->kH2, nc * vphys::LK_HID * 2},
+                {(void **)&h->kY, nc * vphys::LK_OUTP * sizeof(float)},
+                {(void **)&h->kcolH, nc * sizeof(float)},
+                {(void **)&h->kpred, nc * sizeof(float)},
+                {(void **)&h->kcheck, nc * sizeof(float)},
+                {(void **)&h->kgate, nc},
+                {(void **)&h->kstats, 16 * sizeof(unsigned long long)},
+                {(void **)&h->kerr, sizeof(int)}};
+    for (auto &w : want) {
+        if (cudaMalloc(w.p, w.bytes) != cudaSuccess) {
+            cudaGetLastError();
+            free_kpp(h);
+            return push_error(VPHYS_ERR_ALLOC, "vphys_kpp_attach: cudaMalloc of the surrogate's scratch failed");
+        }
+    }
+    cudaMemsetAsync(h->kstats, 0, 16 * sizeof(unsigned long long), h->stream);
+    cudaMemsetAsync(h->kerr, 0, sizeof(int), h->stream);
+    h->kpp = *m;
+    h->kpp_attached = true;
+    h->kgen = 0;
+    return cuda_status(cudaGetLastError(), "vphys_kpp_attach");
+}
+
+int vphys_kpp_stats(vphys_handle h, unsigned long long *out, int n)
+{
+    if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_kpp_stats: bad handle");
+    if (!h->kpp_attached) return push_error(VPHYS_ERR_NOT_INITIALISED, "vphys_kpp_stats: no surrogate attached");
+    if (!out || n <= 0) return VPHYS_OK;
+    unsigned long long tmp[16];
+    int gemm_err = 0;
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e == cudaSuccess) e = cudaMemcpy(tmp, h->kstats, sizeof tmp, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(&gemm_err, h->kerr, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_status(e, "vphys_kpp_stats");
+    tmp[10] = (unsigned long long)gemm_err;
+    for (int i = 0; i < n && i < 16; ++i) out[i] = tmp[i];
+    if (gemm_err) return push_error(VPHYS_ERR_CUDA, "learned KPP: a tensor-core GEMM gave up waiting (code %d)", gemm_err);
+    return VPHYS_OK;
+}
+
+int vphys_kpp_features(vphys_handle h, const float *mean, const float *istd, float gate_limit, float *raw, void *X,
+                       void *XT, long long ld_t, unsigned char *gate, float *colH)
+{
+    if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_kpp_features: bad handle");
+    if ((mean == nullptr) != (istd == nullptr))
+        return push_error(VPHYS_ERR_CONFIG, "vphys_kpp_features: mean and istd go together");
+    Params p = make_params(h);
+    vphys::launch_kpp_features(p, raw, X, XT, ld_t, mean, istd, gate_limit, gate, colH, h->stream);
+    return cuda_status(cudaGetLastError(), "vphys_kpp_features launch");
+}
+
+int vphys_kpp_targets(vphys_handle h, float *T)
+{
+    if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_kpp_targets: bad handle");
+    if (!T) return push_error(VPHYS_ERR_CONFIG, "vphys_kpp_targets: NULL");
+    Params p = make_params(h);
+    vphys::launch_kpp_targets(p, T, h->stream);
+    return cuda_status(cudaGetLastError(), "vphys_kpp_targets launch");
 }
 
 }  // extern "C"

@@ -277,13 +277,14 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
     return fn;
 }
 
-// 2-D BF16 row-major [rows, cols] (cols contiguous) tiled {64, box_rows}, 128-byte swizzle
-static bool make_map(CUtensorMap *m, const void *base, int rows, int cols, int box_rows)
+// 2-D BF16 row-major [rows, cols] (cols contiguous, rows `ld` elements
+// apart) tiled {64, box_rows}, 128-byte swizzle
+static bool make_map(CUtensorMap *m, const void *base, int rows, int cols, long long ld, int box_rows)
 {
     auto fn = encode_fn();
     if (!fn) return false;
     cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
+    cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
     cuuint32_t box[2] = {(cuuint32_t)GK, (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
     return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box, estr,
@@ -291,17 +292,19 @@ static bool make_map(CUtensorMap *m, const void *base, int rows, int cols, int b
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-int gemm_tn_bf16(const void *A, const void *B, int M, int N, int K, float alpha, const float *bias, const float *zin,
-                 int ld_z, int act, float *out_f32, int ld_f32, void *out_bf16, int ld_bf16, void *out_bf16_t, int ld_t,
-                 int *err, cudaStream_t stream)
+int gemm_tn_bf16(const void *A, long long lda, const void *B, long long ldb, int M, int N, int K, float alpha,
+                 const float *bias, const float *zin, int ld_z, int act, float *out_f32, int ld_f32, void *out_bf16,
+                 int ld_bf16, void *out_bf16_t, int ld_t, int *err, cudaStream_t stream)
 {
     if (M <= 0 || N < 16 || N > GN_MAX || (N % 16) != 0 || K <= 0 || (K % 8) != 0)
         return report_error(VPHYS_ERR_BAD_SHAPE, "vphys_gemm_tn_bf16: need M > 0, 16 <= N <= 256 with N % 16 == 0, "
                                                  "K > 0 with K % 8 == 0");
+    if (lda < K || ldb < K || (lda % 8) != 0 || (ldb % 8) != 0)
+        return report_error(VPHYS_ERR_BAD_SHAPE, "vphys_gemm_tn_bf16: lda, ldb must be >= K and multiples of 8");
     if (((uintptr_t)A | (uintptr_t)B) & 15)
         return report_error(VPHYS_ERR_BAD_SHAPE, "vphys_gemm_tn_bf16: A and B must be 16-byte aligned");
     CUtensorMap ma, mb;
-    if (!make_map(&ma, A, M, K, GM) || !make_map(&mb, B, N, K, N))
+    if (!make_map(&ma, A, M, K, lda, GM) || !make_map(&mb, B, N, K, ldb, N))
         return report_error(VPHYS_ERR_CUDA, "vphys_gemm_tn_bf16: cuTensorMapEncodeTiled failed");
     static bool attr_set = false;
     if (!attr_set) {
@@ -332,10 +335,11 @@ int gemm_tn_bf16(const void *A, const void *B, int M, int N, int K, float alpha,
 
 }  // namespace vphys
 
-extern "C" int vphys_gemm_tn_bf16(const void *A, const void *B, int M, int N, int K, float alpha, const float *bias,
-                                  const float *zin, int ld_z, int act, float *out_f32, int ld_f32, void *out_bf16,
-                                  int ld_bf16, void *out_bf16_t, int ld_t, int *err, void *stream)
+extern "C" int vphys_gemm_tn_bf16(const void *A, long long lda, const void *B, long long ldb, int M, int N, int K,
+                                  float alpha, const float *bias, const float *zin, int ld_z, int act, float *out_f32,
+                                  int ld_f32, void *out_bf16, int ld_bf16, void *out_bf16_t, int ld_t, int *err,
+                                  void *stream)
 {
-    return vphys::gemm_tn_bf16(A, B, M, N, K, alpha, bias, zin, ld_z, act, out_f32, ld_f32, out_bf16, ld_bf16,
-                               out_bf16_t, ld_t, err, reinterpret_cast<cudaStream_t>(stream));
+    return vphys::gemm_tn_bf16(A, lda, B, ldb, M, N, K, alpha, bias, zin, ld_z, act, out_f32, ld_f32, out_bf16,
+                               ld_bf16, out_bf16_t, ld_t, err, reinterpret_cast<cudaStream_t>(stream));
 }

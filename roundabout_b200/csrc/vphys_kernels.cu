@@ -127,7 +127,12 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
             const double cb = sm_cbrt(wstar3_lagged);
             const double w_s_col = sqrt(u_star * u_star + cb * cb);
             double hb_new = 0.0;   // all-zero column: no crossing, sum of zeros
-            if (!all_zero) {
+            // learned KPP: the surrogate's h_b replaces the walk unless the
+            // column is gated, sampled for the check, or in a fallback step
+            const float pred = p.kpp_pred ? p.kpp_pred[col] : -1.0f;
+            if (pred >= 0.0f) {
+                hb_new = (double)pred;
+            } else if (!all_zero) {
                 const double u_ref = UC(k_sfc);
                 const double v_ref = VC(k_sfc);
                 const double b_ref = -(GRAVITY * RR(k_sfc) / rho0);
@@ -168,6 +173,15 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
                 if (!crossing_found) {
                     hb_new = 0.0;
                     for (int k = 1; k <= k_sfc; ++k) hb_new = hb_new + HH(k);
+                }
+                if (p.kpp_check) {
+                    const float ck = p.kpp_check[col];
+                    if (ck >= 0.0f) {   // sampled column: the network's h_b against pass 1
+                        const double rel = fabs((double)ck - hb_new) / fmx(hb_new, 1.0);
+                        atomicAdd(p.kpp_stats + 0, 1ull);
+                        if (rel > (double)p.kpp_tol) atomicAdd(p.kpp_stats + 1, 1ull);
+                        atomicAdd(p.kpp_stats + 8, (unsigned long long)(fmn(rel * rel, 1.0e6) * 1.0e6));
+                    }
                 }
             }
             h_b = hb_new;

@@ -12,6 +12,15 @@ namespace vphys {
 constexpr int NZ_MAX = VPHYS_NZ_MAX + 1;   // per-column local arrays (>= nz + 1)
 constexpr int NTR_MAX = 16;                // tracers a handle may carry
 
+// learned KPP surrogate: 75 feature levels below the surface layer,
+// 154 inputs (K padded to 160), 256 hidden, 77 outputs (padded to 80)
+constexpr int LK_LEV = 75;
+constexpr int LK_IN = 154;
+constexpr int LK_INP = 160;
+constexpr int LK_HID = 256;
+constexpr int LK_OUT = 77;
+constexpr int LK_OUTP = 80;
+
 // Everything a kernel needs: the grid, the knobs and the device pointers.
 struct Params {
     int nx, ny, nz, ntr;
@@ -34,6 +43,11 @@ struct Params {
     unsigned long long *guard_count;  // vmix_guard counter (device)
     int *span;                        // per column: first | last live layer << 16 (0: none), scratch
     double *zcol;                     // per column: -sum_k h, k = 1..nz in order (momentum z_clear), scratch
+    const double *coriolis;           // (nx, ny) f, or nullptr (learned KPP features only)
+    const float *kpp_pred;            // per column: the surrogate's h_b, < 0: run pass 1; nullptr: plain KPP
+    const float *kpp_check;           // per column: h_b to compare with pass 1 (>= 0), or nullptr
+    unsigned long long *kpp_stats;    // learned KPP counters (k_kpp_roll)
+    float kpp_tol;                    // relative h_b difference counted as a failed check
     int ks_equals_kt;                 // ks is bitwise kt after the gate
     int write_gamma;
 };
@@ -53,6 +67,18 @@ void launch_tracers(const Params &p, double dt, bool diffuse, bool nonlocal, cud
 // mixed-precision solves (vphys_mixed.cu), dispatched by the two above when cfg.mixed_precision
 void launch_momentum_mp(const Params &p, double dt, cudaStream_t stream);
 void launch_tracers_mp(const Params &p, double dt, bool nonlocal, cudaStream_t stream);
+// learned KPP (vphys_learned.cu)
+void launch_kpp_features(const Params &p, float *raw, void *X, void *XT, long long ld_t, const float *mean,
+                         const float *istd, float limit, unsigned char *gate, float *colH, cudaStream_t s);
+void launch_kpp_targets(const Params &p, float *T, cudaStream_t s);
+void launch_kpp_roll(unsigned long long *st, float fail_fraction, cudaStream_t s);
+void launch_kpp_apply(size_t ncols, const float *Y, float tmean0, float tstd0, const unsigned char *gate,
+                      const float *colH, float *pred, float *check, unsigned long long *st, unsigned gen,
+                      float check_fraction, cudaStream_t s);
+// tcgen05 GEMM (vphys_gemm.cu)
+int gemm_tn_bf16(const void *A, long long lda, const void *B, long long ldb, int M, int N, int K, float alpha,
+                 const float *bias, const float *zin, int ld_z, int act, float *out_f32, int ld_f32, void *out_bf16,
+                 int ld_bf16, void *out_bf16_t, int ld_t, int *err, cudaStream_t stream);
 void launch_selftest_division(unsigned long long seed, long long per_thread, int emin, int erange,
                               unsigned long long *bad, cudaStream_t stream);
 

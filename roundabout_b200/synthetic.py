@@ -20,6 +20,7 @@ synthetic columns with the stated shapes and value distributions:
   faces, zero on faces touching land;
 * passives: ideal age = 0, pseudo-salt = S (`passive_init="age_ps"`) or
   U[0, 1] (`passive_init="uniform"`);
+* f = 1e-4 + 2e-11 y 1/s (not read by the path; an input of the learned KPP);
 * forcing: tau_x = 0.1 sin(pi y / Ly) N/m2, tau_y = 0;
   Q_heat ~ U[-100, 100] W/m2; freshwater F ~ U[-1e-7, 1e-7] m/s turned into
   the reference's salt flux as Q_salt = -rho0 * 35 * F.
@@ -51,6 +52,7 @@ class Columns:
     q_salt: np.ndarray
     wet: np.ndarray
     kbot: np.ndarray = field(repr=False)   # 1-based index of the deepest live layer (0 on land)
+    coriolis: np.ndarray = field(default=None, repr=False)   # f = 1e-4 + 2e-11 y (read by the learned KPP only)
 
     @property
     def ncells(self) -> int:
@@ -165,7 +167,8 @@ def make_columns(nx, ny, nz, ntracers=2, seed=1234, land_frac=0.0, thin_frac=0.0
     q_heat = np.asfortranarray(rng.uniform(-100.0, 100.0, size=(nx, ny)))
     fw = rng.uniform(-1.0e-7, 1.0e-7, size=(nx, ny))
     q_salt = np.asfortranarray(-rho0 * 35.0 * fw)
-    return Columns(nx, ny, nz, h, u, v, tracers, tau_x, tau_y, q_heat, q_salt, wet, kbot)
+    coriolis = np.asfortranarray(np.broadcast_to((1.0e-4 + 2.0e-11 * y)[None, :], (nx, ny)).copy())
+    return Columns(nx, ny, nz, h, u, v, tracers, tau_x, tau_y, q_heat, q_salt, wet, kbot, coriolis)
 
 
 # Benchmark configurations (shapes of the reference's north-star configs).

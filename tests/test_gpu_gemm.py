@@ -45,8 +45,8 @@ def run(env, A, B, alpha=1.0, bias=None, zin=None, act=0, f32=True, bf16=False, 
     o32 = torch.full((M, N), float("nan"), device="cuda") if f32 else None
     o16 = torch.zeros((M, N), dtype=torch.bfloat16, device="cuda") if bf16 else None
     o16t = torch.zeros((N, M), dtype=torch.bfloat16, device="cuda") if bf16_t else None
-    st = lib.vphys_gemm_tn_bf16(P(A), P(B), M, N, K, float(alpha), P(bias), P(zin), N, act, P(o32), N, P(o16), N,
-                                P(o16t), M, P(err), None)
+    st = lib.vphys_gemm_tn_bf16(P(A), A.stride(0), P(B), B.stride(0), M, N, K, float(alpha), P(bias), P(zin), N,
+                                act, P(o32), N, P(o16), N, P(o16t), M, P(err), None)
     assert st == 0, _ffi.last_error()
     torch.cuda.synchronize()
     assert int(err.item()) == 0
@@ -95,10 +95,22 @@ def test_gemm_epilogue_gelu_backward(env):
     assert float((o32 - ref).abs().max()) <= 2e-3 * float(ref.abs().max())
 
 
+def test_gemm_strided_operands(env):
+    """Operands that are column slices of wider matrices (row stride > K)."""
+    torch = env[0]
+    g = torch.Generator(device="cuda").manual_seed(13)
+    Afull = torch.randn(256, 4096, device="cuda", generator=g).to(torch.bfloat16)
+    Bfull = torch.randn(160, 4096, device="cuda", generator=g).to(torch.bfloat16)
+    A, B = Afull[:, 1024:1024 + 2048], Bfull[:, 1024:1024 + 2048]
+    o32, _, _ = run(env, A, B)
+    ref = A.float() @ B.float().T
+    assert float((o32 - ref).abs().max()) <= 2e-3 * float(ref.abs().max())
+
+
 def test_gemm_rejects_bad_shapes(env):
     torch, lib, _ffi = env
     A = torch.zeros(128, 64, dtype=torch.bfloat16, device="cuda")
     B = torch.zeros(24, 64, dtype=torch.bfloat16, device="cuda")   # N % 16 != 0
-    st = lib.vphys_gemm_tn_bf16(P(A), P(B), 128, 24, 64, 1.0, None, None, 0, 0, None, 0, None, 0, None, 0, None,
-                                None)
+    st = lib.vphys_gemm_tn_bf16(P(A), 64, P(B), 64, 128, 24, 64, 1.0, None, None, 0, 0, None, 0, None, 0, None, 0,
+                                None, None)
     assert st == _ffi.ERR_BAD_SHAPE
