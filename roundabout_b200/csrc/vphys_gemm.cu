@@ -9,13 +9,16 @@
 // FP32 (pre-activation or plain), BF16 of GELU(v) or v, and/or a transposed
 // BF16 copy (the operand layout the weight-gradient GEMMs read).
 //
-// One CTA computes a 128-row tile against all N <= 256 output columns:
+// Persistent kernel, one CTA per SM, looping over 128-row tiles (each against
+// all N <= 256 output columns), warp-specialised:
 //   * warp 0 lane 0 streams K in 64-element steps with TMA
 //     (cp.async.bulk.tensor, 128-byte swizzle) into a 4-stage ring,
 //   * warp 1 lane 0 issues tcgen05.mma (M=128, N, K=16) from the shared-memory
-//     descriptors into an FP32 accumulator in tensor memory and releases each
-//     stage with tcgen05.commit,
-//   * all four warps read their 32 accumulator lanes back with tcgen05.ld.
+//     descriptors into one of two FP32 accumulators in tensor memory (all 512
+//     columns), releasing each stage with tcgen05.commit,
+//   * warps 2-9 drain the other accumulator with tcgen05.ld (two warps per
+//     32-lane quarter, alternate 16-column chunks), so the epilogue of tile i
+//     overlaps the loads and MMAs of tile i+1.
 // Every mbarrier wait is bounded: on expiry the CTA records an error code in
 // *err, skips the rest of its work and still frees its tensor memory.
 // No load is multicast; the kernel runs on the calling GPU's memory only.
@@ -36,8 +39,9 @@ constexpr int GM = 128;        // rows per CTA (tcgen05 M)
 constexpr int GK = 64;         // K per stage: one 128-byte swizzle row of BF16
 constexpr int GSTAGES = 4;
 constexpr int GN_MAX = 256;    // N per CTA (tcgen05 N <= 256)
-constexpr int GEMM_THREADS = 128;
-constexpr uint32_t TMEM_COLS = 256;
+constexpr int GEMM_THREADS = 320;   // producer, MMA, 8 epilogue warps
+constexpr int EPI_WARPS = 8;
+constexpr uint32_t TMEM_COLS = 512;  // two 256-column accumulators
 constexpr size_t GEMM_SMEM = (size_t)GSTAGES * (GM + GN_MAX) * GK * 2 + 1024 /* barriers */ + 1024 /* align */;
 constexpr long long WAIT_LIMIT = 1LL << 24;   // try_wait polls before a wait is declared lost
 
@@ -54,6 +58,7 @@ struct GemmEpi {
     int ld_bf16;
     __nv_bfloat16 *out_bf16_t;  // [N, ld_t] transposed, or null
     int ld_t;
+    int vec;                // row-major outputs 16-byte aligned with ld % 8 == 0: vector stores
     int *err;
 };
 
@@ -116,18 +121,88 @@ __device__ __forceinline__ uint32_t idesc_bf16(int m, int n)
     return d;
 }
 
+// hardware tanh (MUFU, relative error about 2^-11: below the BF16 rounding
+// every activation then goes through)
+__device__ __forceinline__ float tanh_hw(float x)
+{
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
 __device__ __forceinline__ float gelu_tanh(float x)
 {
     // GELU, tanh form (Hendrycks & Gimpel 2016)
     const float c = 0.7978845608028654f;   // sqrt(2/pi)
-    const float t = tanhf(c * (x + 0.044715f * x * x * x));
+    const float t = tanh_hw(c * (x + 0.044715f * x * x * x));
     return 0.5f * x * (1.0f + t);
 }
 __device__ __forceinline__ float gelu_tanh_grad(float x)
 {
     const float c = 0.7978845608028654f;
-    const float t = tanhf(c * (x + 0.044715f * x * x * x));
+    const float t = tanh_hw(c * (x + 0.044715f * x * x * x));
     return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * c * (1.0f + 3.0f * 0.044715f * x * x);
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// epilogue of one 16-column chunk of one row (v[] = accumulator values)
+__device__ __forceinline__ void epilogue16(const GemmEpi &g, int row, int c0, const uint32_t (&r)[16])
+{
+    float v[16], a[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+        const int col = c0 + q;
+        float x = g.alpha * __uint_as_float(r[q]);
+        if (g.bias) x += __ldg(g.bias + col);
+        if (g.zin) x *= gelu_tanh_grad(__ldg(g.zin + (size_t)row * g.ld_z + col));
+        v[q] = x;
+        a[q] = g.act ? gelu_tanh(x) : x;
+    }
+    if (g.out_f32) {
+        float *o = g.out_f32 + (size_t)row * g.ld_f32 + c0;
+        if (g.vec) {
+#pragma unroll
+            for (int q = 0; q < 16; q += 4) *reinterpret_cast<float4 *>(o + q) = make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]);
+        } else {
+#pragma unroll
+            for (int q = 0; q < 16; ++q) o[q] = v[q];
+        }
+    }
+    if (g.out_bf16 || g.out_bf16_t) {
+        __nv_bfloat162 pk[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) pk[q] = __floats2bfloat162_rn(a[2 * q], a[2 * q + 1]);
+        if (g.out_bf16) {
+            __nv_bfloat16 *o = g.out_bf16 + (size_t)row * g.ld_bf16 + c0;
+            if (g.vec) {
+                uint4 *o4 = reinterpret_cast<uint4 *>(o);
+                o4[0] = *reinterpret_cast<uint4 *>(&pk[0]);
+                o4[1] = *reinterpret_cast<uint4 *>(&pk[4]);
+            } else {
+#pragma unroll
+                for (int q = 0; q < 8; ++q) *reinterpret_cast<__nv_bfloat162 *>(o + 2 * q) = pk[q];
+            }
+        }
+        if (g.out_bf16_t) {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                g.out_bf16_t[(size_t)(c0 + 2 * q) * g.ld_t + row] = pk[q].x;
+                g.out_bf16_t[(size_t)(c0 + 2 * q + 1) * g.ld_t + row] = pk[q].y;
+            }
+        }
+    }
 }
 
 __global__ void __launch_bounds__(GEMM_THREADS, 1)
@@ -139,21 +214,26 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
     __nv_bfloat16 *sb = sa + (size_t)GSTAGES * GM * GK;
     uint64_t *full = reinterpret_cast<uint64_t *>(sb + (size_t)GSTAGES * GN_MAX * GK);
     uint64_t *empty = full + GSTAGES;
-    uint64_t *done = empty + GSTAGES;
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
+    uint64_t *acc_full = empty + GSTAGES;     // [2] MMA -> epilogue
+    uint64_t *acc_empty = acc_full + 2;       // [2] epilogue -> MMA
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(acc_empty + 2);
     int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.x * GM;
     const int N = g.N;
     const int nk = (g.K + GK - 1) / GK;
+    const int tiles = (g.M + GM - 1) / GM;
+    const int my_tiles = (tiles > (int)blockIdx.x) ? (tiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < GSTAGES; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
-        mbar_init(done, 1);
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(&acc_full[a], 1);
+            mbar_init(&acc_empty[a], EPI_WARPS);
+        }
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -167,99 +247,108 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
+    volatile int *abort_v = abort_flag;
 
-    if (warp == 0 && lane == 0) {
-        // ---- TMA producer ----
-        const uint32_t bytes = (uint32_t)(GM + N) * GK * 2;
-        for (int kt = 0; kt < nk; ++kt) {
-            const int s = kt % GSTAGES;
-            const uint32_t round = kt / GSTAGES;
-            if (!mbar_wait(&empty[s], (round & 1) ^ 1)) {
-                atomicExch(g.err, 1);
-                *(volatile int *)abort_flag = 1;
-                break;
-            }
-            mbar_expect_tx(&full[s], bytes);
-            tma_load_2d(sa + (size_t)s * GM * GK, &tmA, kt * GK, m0, &full[s]);
-            tma_load_2d(sb + (size_t)s * GN_MAX * GK, &tmB, kt * GK, 0, &full[s]);
-        }
-    } else if (warp == 1 && lane == 0) {
-        // ---- MMA issuer ----
-        const uint32_t idesc = idesc_bf16(GM, N);
-        int issued = 0;
-        for (int kt = 0; kt < nk; ++kt) {
-            const int s = kt % GSTAGES;
-            const uint32_t round = kt / GSTAGES;
-            if (!mbar_wait(&full[s], round & 1)) {
-                atomicExch(g.err, 2);
-                *(volatile int *)abort_flag = 1;
-                break;
-            }
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const __nv_bfloat16 *as = sa + (size_t)s * GM * GK;
-            const __nv_bfloat16 *bs = sb + (size_t)s * GN_MAX * GK;
-#pragma unroll
-            for (int kk = 0; kk < GK / 16; ++kk) {
-                const uint64_t ad = smem_desc_sw128(as + kk * 16);
-                const uint64_t bd = smem_desc_sw128(bs + kk * 16);
-                const uint32_t acc = (kt > 0 || kk > 0) ? 1u : 0u;
-                asm volatile(
-                    "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-                    " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
-                    "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
-                    : "memory");
-            }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                             smem_u32(&empty[s]))
-                         : "memory");
-            ++issued;
-        }
-        // signals when every MMA issued so far has completed (also after an abort)
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                         smem_u32(done))
-                     : "memory");
-        (void)issued;
-    }
-
-    // ---- epilogue: every warp reads its 32 accumulator lanes ----
-    __syncwarp();
-    const bool ok = mbar_wait(done, 0);
-    if (!ok && threadIdx.x == 0) atomicExch(g.err, 3);
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const bool skip = !ok || *(volatile int *)abort_flag;
-    const int row = m0 + warp * 32 + lane;
-    if (!skip) {
-        for (int c0 = 0; c0 < N; c0 += 16) {
-            uint32_t r[16];
-            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
-                  "=r"(r[15])
-                : "r"(taddr));
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (row < g.M) {
-#pragma unroll
-                for (int q = 0; q < 16; ++q) {
-                    const int col = c0 + q;
-                    if (col >= N) break;
-                    float v = g.alpha * __uint_as_float(r[q]);
-                    if (g.bias) v += g.bias[col];
-                    if (g.zin) v *= gelu_tanh_grad(g.zin[(size_t)row * g.ld_z + col]);
-                    if (g.out_f32) g.out_f32[(size_t)row * g.ld_f32 + col] = v;
-                    const float a = g.act ? gelu_tanh(v) : v;
-                    const __nv_bfloat16 ab = __float2bfloat16_rn(a);
-                    if (g.out_bf16) g.out_bf16[(size_t)row * g.ld_bf16 + col] = ab;
-                    if (g.out_bf16_t) g.out_bf16_t[(size_t)col * g.ld_t + row] = ab;
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---- TMA producer ----
+            const uint32_t bytes = (uint32_t)(GM + N) * GK * 2;
+            long long it = 0;
+            for (int t = 0; t < my_tiles && !*abort_v; ++t) {
+                const int m0 = ((int)blockIdx.x + t * (int)gridDim.x) * GM;
+                for (int kt = 0; kt < nk; ++kt, ++it) {
+                    const int s = (int)(it % GSTAGES);
+                    const uint32_t round = (uint32_t)(it / GSTAGES);
+                    if (!mbar_wait(&empty[s], (round & 1) ^ 1)) {
+                        atomicExch(g.err, 1);
+                        *abort_v = 1;
+                        break;
+                    }
+                    mbar_expect_tx(&full[s], bytes);
+                    tma_load_2d(sa + (size_t)s * GM * GK, &tmA, kt * GK, m0, &full[s]);
+                    tma_load_2d(sb + (size_t)s * GN_MAX * GK, &tmB, kt * GK, 0, &full[s]);
                 }
             }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---- MMA issuer ----
+            const uint32_t idesc = idesc_bf16(GM, N);
+            long long it = 0;
+            for (int t = 0; t < my_tiles && !*abort_v; ++t) {
+                const int a = t & 1;
+                if (!mbar_wait(&acc_empty[a], ((t >> 1) & 1) ^ 1)) {
+                    atomicExch(g.err, 4);
+                    *abort_v = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t d = tmem + (uint32_t)(a * GN_MAX);
+                bool ok = true;
+                for (int kt = 0; kt < nk; ++kt, ++it) {
+                    const int s = (int)(it % GSTAGES);
+                    const uint32_t round = (uint32_t)(it / GSTAGES);
+                    if (!mbar_wait(&full[s], round & 1)) {
+                        atomicExch(g.err, 2);
+                        *abort_v = 1;
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const __nv_bfloat16 *as = sa + (size_t)s * GM * GK;
+                    const __nv_bfloat16 *bs = sb + (size_t)s * GN_MAX * GK;
+#pragma unroll
+                    for (int kk = 0; kk < GK / 16; ++kk) {
+                        const uint64_t ad = smem_desc_sw128(as + kk * 16);
+                        const uint64_t bd = smem_desc_sw128(bs + kk * 16);
+                        const uint32_t acc = (kt > 0 || kk > 0) ? 1u : 0u;
+                        asm volatile(
+                            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
+                            "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+                            : "memory");
+                    }
+                    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                     smem_u32(&empty[s]))
+                                 : "memory");
+                }
+                // the accumulator is ready (or, after an abort, every MMA issued has finished)
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 smem_u32(&acc_full[a]))
+                             : "memory");
+                if (!ok) break;
+            }
+        }
+    } else {
+        // ---- epilogue warps 2..9: quarter (warp % 4) of the lanes, alternate chunks ----
+        const int quarter = warp & 3;
+        const int half = (warp - 2) >> 2;
+        for (int t = 0; t < my_tiles; ++t) {
+            const int a = t & 1;
+            const bool ok = mbar_wait(&acc_full[a], (t >> 1) & 1);
+            if (!ok) {
+                if (lane == 0) atomicExch(g.err, 3);
+                *abort_v = 1;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            if (!ok || *abort_v) break;
+            const int row = ((int)blockIdx.x + t * (int)gridDim.x) * GM + quarter * 32 + lane;
+            for (int c0 = half * 16; c0 < N; c0 += 32) {
+                uint32_t r[16];
+                tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(a * GN_MAX + c0), r);
+                if (row < g.M) epilogue16(g, row, c0, r);
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acc_empty[a]);
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (warp == 0)
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+    }
 }
 
 // ---- host side ---------------------------------------------------------------
@@ -327,7 +416,18 @@ int gemm_tn_bf16(const void *A, long long lda, const void *B, long long ldb, int
     g.out_bf16_t = reinterpret_cast<__nv_bfloat16 *>(out_bf16_t);
     g.ld_t = ld_t;
     g.err = err;
-    k_gemm_tn<<<(M + GM - 1) / GM, GEMM_THREADS, GEMM_SMEM, stream>>>(ma, mb, g);
+    const bool f32_vec = !out_f32 || ((((uintptr_t)out_f32) & 15) == 0 && (ld_f32 % 4) == 0);
+    const bool b16_vec = !out_bf16 || ((((uintptr_t)out_bf16) & 15) == 0 && (ld_bf16 % 8) == 0);
+    g.vec = (f32_vec && b16_vec) ? 1 : 0;
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    const int tiles = (M + GM - 1) / GM;
+    k_gemm_tn<<<tiles < sms ? tiles : sms, GEMM_THREADS, GEMM_SMEM, stream>>>(ma, mb, g);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return report_error(VPHYS_ERR_CUDA, cudaGetErrorString(e));
     return VPHYS_OK;

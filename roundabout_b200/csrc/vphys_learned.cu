@@ -45,21 +45,31 @@ struct FeatOut {
 
 __device__ __forceinline__ float slog6(float x) { return copysignf(log1pf(fabsf(x) * 1.0e6f), x); }
 
-__device__ __forceinline__ void emit(const FeatOut &o, size_t col, int m, float x, bool &oor)
+constexpr int FEAT_THREADS = 128;
+constexpr int FEAT_LD = LK_INP + 2;   // shared row stride (BF16): odd word stride, no bank conflicts
+
+// feature m of this thread's column: raw (training), standardised BF16 into the
+// block's shared rows (copied out coalesced) and/or transposed (coalesced as is)
+__device__ __forceinline__ void emit(const FeatOut &o, __nv_bfloat16 *srow, size_t col, int m, float x, bool &oor)
 {
     if (o.raw) o.raw[col * LK_IN + m] = x;
     const float v = o.mean ? (x - o.mean[m]) * o.istd[m] : x;
     oor = oor || !(fabsf(v) <= o.limit);
     const __nv_bfloat16 b = __float2bfloat16_rn(v);
-    if (o.X) o.X[col * LK_INP + m] = b;
+    srow[m] = b;
     if (o.XT) o.XT[(size_t)m * o.ld_t + col] = b;
 }
 
-__global__ void k_kpp_features(const Params p, const FeatOut o, unsigned char *gate, float *colH)
+__global__ void __launch_bounds__(FEAT_THREADS) k_kpp_features(const Params p, const FeatOut o, unsigned char *gate,
+                                                               float *colH)
 {
+    __shared__ __nv_bfloat16 tile[FEAT_THREADS * FEAT_LD];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
-    if (i >= p.nx) return;
+    __nv_bfloat16 *srow = tile + threadIdx.x * FEAT_LD;
+    const int i0 = blockIdx.x * blockDim.x;
+    const int rows = min((int)blockDim.x, p.nx - i0);   // columns of this block (consecutive in memory)
+    if (i < p.nx) {
     const vphys_config &c = p.cfg;
     const int nx = p.nx, nz = p.nz;
     const size_t P = p.plane, PU = p.plane_u, PV = p.plane_v;
@@ -94,10 +104,10 @@ __global__ void k_kpp_features(const Params p, const FeatOut o, unsigned char *g
     const double B_0 = (GRAVITY / rho0) * (c.alpha_T * q_T_kin - c.beta_S * q_S_kin);
     const double f = p.coriolis ? p.coriolis[col] : 0.0;
     bool oor = false;
-    emit(o, col, 0, (float)(u_star * 100.0), oor);
-    emit(o, col, 1, (float)(B_0 * 1.0e8), oor);
-    emit(o, col, 2, (float)(f * 1.0e4), oor);
-    emit(o, col, 3, (float)(H * 1.0e-3), oor);
+    emit(o, srow, col, 0, (float)(u_star * 100.0), oor);
+    emit(o, srow, col, 1, (float)(B_0 * 1.0e8), oor);
+    emit(o, srow, col, 2, (float)(f * 1.0e4), oor);
+    emit(o, srow, col, 3, (float)(H * 1.0e-3), oor);
 
     double u_ref = 0, v_ref = 0, b_ref = 0, d_ref = 0, d_c = 0, h_above = 0;
     if (!all_zero) {
@@ -123,15 +133,29 @@ __global__ void k_kpp_features(const Params p, const FeatOut o, unsigned char *g
             }
             h_above = h_k;
         }
-        emit(o, col, 4 + m, slog6(n2), oor);
-        emit(o, col, 4 + LK_LEV + m, slog6(s2), oor);
+        emit(o, srow, col, 4 + m, slog6(n2), oor);
+        emit(o, srow, col, 4 + LK_LEV + m, slog6(s2), oor);
     }
     for (int m = LK_IN; m < LK_INP; ++m) {   // K padding
-        if (o.X) o.X[col * LK_INP + m] = __float2bfloat16_rn(0.0f);
+        srow[m] = __float2bfloat16_rn(0.0f);
         if (o.XT) o.XT[(size_t)m * o.ld_t + col] = __float2bfloat16_rn(0.0f);
     }
     if (gate) gate[col] = oor ? 1 : 0;
     if (colH) colH[col] = all_zero ? -1.0f : (float)H;
+    }
+    __syncthreads();
+    if (o.X && rows > 0) {
+        // the block's rows are consecutive columns: one contiguous run of
+        // rows * 160 BF16, written as 4-byte words by consecutive threads
+        const size_t col0 = (size_t)i0 + (size_t)p.nx * j;
+        uint32_t *dst = reinterpret_cast<uint32_t *>(o.X + col0 * LK_INP);
+        const int words = rows * (LK_INP / 2);
+        for (int w = threadIdx.x; w < words; w += blockDim.x) {
+            const int r = w / (LK_INP / 2), c2 = w % (LK_INP / 2);
+            const __nv_bfloat162 v = *reinterpret_cast<const __nv_bfloat162 *>(tile + r * FEAT_LD + 2 * c2);
+            dst[w] = *reinterpret_cast<const uint32_t *>(&v);
+        }
+    }
 }
 
 // ---- training targets from the plain KPP's state ------------------------------
@@ -343,7 +367,7 @@ void launch_kpp_features(const Params &p, float *raw, void *X, void *XT, long lo
 {
     FeatOut o{raw, reinterpret_cast<__nv_bfloat16 *>(X), reinterpret_cast<__nv_bfloat16 *>(XT), ld_t, mean, istd,
               limit};
-    k_kpp_features<<<dim3((p.nx + 127) / 128, p.ny), 128, 0, s>>>(p, o, gate, colH);
+    k_kpp_features<<<dim3((p.nx + FEAT_THREADS - 1) / FEAT_THREADS, p.ny), FEAT_THREADS, 0, s>>>(p, o, gate, colH);
 }
 
 void launch_kpp_targets(const Params &p, float *T, cudaStream_t s)
