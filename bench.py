@@ -66,6 +66,8 @@ def parse():
                     help="mixed: FP32 Thomas sweeps + FP64 residual (cfg.mixed_precision=1); "
                          "plain: FP64 throughout, bitwise the reference's arithmetic")
     ap.add_argument("--no-compare", action="store_true", help="skip the plain-FP64 timing and error check")
+    ap.add_argument("--learned-cols", type=int, default=1_048_576,
+                    help="training columns of the learned-KPP surrogate timed beside the mixed form (0: skip)")
     return ap.parse_args()
 
 
@@ -316,6 +318,35 @@ def main():
         vp_plain.close()
         vp_plain = None
         vp.load_columns(cols)
+
+    # ---- learned KPP + mixed solves: trained here on the plain KPP's columns ----
+    if mixed and not args.no_compare and args.learned_cols > 0:
+        from roundabout_b200 import learned as L
+
+        sur, _ = L.train_surrogate(args.learned_cols, nz=nz, seed=100, epochs=4)
+        cfg_l = hot_path_config(ntracers=ntr)
+        cfg_l.mixed_precision = 1
+        cfg_l.learned_kpp = 1
+        vl = VerticalPhysics(nx, ny, nz, ntr, cfg_l)
+        vl.load_columns(cols)
+        sur.attach(vl)
+        vpp = VerticalPhysics(nx, ny, nz, ntr, hot_path_config(ntracers=ntr))
+        vpp.load_columns(cols)
+        vl.step(dt, 1)
+        vpp.step(dt, 1)
+        torch.cuda.synchronize()
+        bl, blp = np.asarray(vl.get("bl_depth")), np.asarray(vpp.get("bl_depth"))
+        wetm = np.asarray(cols.wet) > 0
+        r = ((bl - blp) / np.maximum(blp, 1.0))[wetm]
+        vpp.close()
+        ms_l = timed(vl, args.steps, args.warmup)
+        forms["learned_kpp_mixed"] = {
+            "cells_per_s": cells * args.steps * world / (ms_l / 1e3), "ms_per_step": ms_l / args.steps,
+            "obl_rms_rel_vs_plain_1step": float(np.sqrt(np.mean(r * r))),
+            "train_columns": int(sur.ntrain), "collect_s": round(sur.collect_seconds, 2),
+            "train_s": round(sur.train_seconds, 2), "kpp": L.kpp_stats(vl)}
+        vl.close()
+        del sur
 
     with ClockSampler(local) as clk:
         ms = timed(vp, args.steps, args.warmup)

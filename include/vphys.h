@@ -274,6 +274,14 @@ int vphys_nonlocal(vphys_handle h, double dt);
  * buffers are allocated.  n_steps <= 0 is a successful no-op. */
 int vphys_step(vphys_handle h, double dt, int n_steps);
 
+/* vphys_step as one CUDA graph: the launches of n_steps steps are captured
+ * once (on a private stream) and replayed with cudaGraphLaunch on the
+ * handle's stream; a change of any bound pointer, of the configuration, of
+ * dt, n_steps or of the attached surrogate recaptures.  Results are those of
+ * vphys_step(h, dt, n_steps).  (The learned KPP's sampled-check columns are
+ * fixed per capture.)  Asynchronous. */
+int vphys_step_graph(vphys_handle h, double dt, int n_steps);
+
 /* Block until the handle's stream is idle; VPHYS_ERR_CUDA on a CUDA error. */
 int vphys_synchronize(vphys_handle h);
 

@@ -196,6 +196,7 @@ _PROTOTYPES = {
                                                 ctypes.c_int, ctypes.c_int, ctypes.c_void_p]),
     "vphys_selftest_division": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_ulonglong, ctypes.c_int, ctypes.c_int,
                                                 ctypes.POINTER(ctypes.c_ulonglong)]),
+    "vphys_step_graph": (_I, [_V, ctypes.c_double, _I]),
     "vphys_kpp_attach": (_I, [_V, ctypes.POINTER(KppModel)]),
     "vphys_kpp_stats": (_I, [_V, ctypes.POINTER(ctypes.c_ulonglong), _I]),
     "vphys_kpp_features": (_I, [_V, _V, _V, _F, _V, _V, _V, _LL, _V, _V]),

@@ -167,6 +167,10 @@ class VerticalPhysics:
     def step(self, dt, n_steps=1):
         _ffi.check(self.lib.vphys_step(self._h, float(dt), int(n_steps)), "vphys_step")
 
+    def step_graph(self, dt, n_steps=1):
+        """vphys_step_graph: the n steps captured once as a CUDA graph and replayed."""
+        _ffi.check(self.lib.vphys_step_graph(self._h, float(dt), int(n_steps)), "vphys_step_graph")
+
     def step_status(self, dt, n_steps=1):
         return self.lib.vphys_step(self._h, float(dt), int(n_steps))
 

@@ -84,6 +84,10 @@ struct vphys_handle_s {
     unsigned long long *kstats = nullptr;
     int *kerr = nullptr;
     unsigned kgen = 0;
+    // vphys_step_graph: the captured launches of n steps and what they were captured with
+    cudaStream_t cap_stream = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    unsigned char gsig[sizeof(Params) + sizeof(vphys_kpp_model) + 32] = {};
 };
 
 namespace {
@@ -388,6 +392,26 @@ void free_kpp(vphys_handle h)
     h->kpp_attached = false;
 }
 
+int run_assemble(vphys_handle h, const Params &p);
+
+// The launches of n whole steps (vmix_apply_in_stage on a thermo step,
+// rdb_ocean_dyn.F90:1636-1900): EOS, [learned KPP], assembly, momentum,
+// tracers with the non-local tendency.  All asynchronous on h->stream.
+int launch_steps(vphys_handle h, const Params &p, double dt, int n_steps)
+{
+    int st;
+    for (int n = 0; n < n_steps; ++n) {
+        if (h->cfg.eos_in_step) vphys::launch_eos_wright(p, h->stream);
+        Params pa = p;
+        if ((st = run_learned_kpp(h, pa))) return st;
+        if ((st = run_assemble(h, pa))) return st;
+        vphys::launch_momentum(p, dt, h->stream);
+        if (h->ntr > 0) vphys::launch_tracers(p, dt, true, h->cfg.use_kpp != 0, h->stream);
+        h->gen += 1;
+    }
+    return VPHYS_OK;
+}
+
 int run_assemble(vphys_handle h, const Params &p)
 {
     vphys::launch_assemble(p, h->stream);
@@ -571,6 +595,8 @@ int vphys_destroy(vphys_handle *hp)
     if (h->span) cudaFree(h->span);
     if (h->zcol) cudaFree(h->zcol);
     free_kpp(h);
+    if (h->gexec) cudaGraphExecDestroy(h->gexec);
+    if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
     h->magic = 0;
     delete h;
     return VPHYS_OK;
@@ -747,16 +773,73 @@ int vphys_step(vphys_handle h, double dt, int n_steps)
         if (e != cudaSuccess) return cuda_status(e, "vphys_step guard reset");
     }
     Params p = make_params(h);
-    for (int n = 0; n < n_steps; ++n) {
-        if (h->cfg.eos_in_step) vphys::launch_eos_wright(p, h->stream);
-        Params pa = p;
-        if ((st = run_learned_kpp(h, pa))) return st;
-        if ((st = run_assemble(h, pa))) return st;
-        vphys::launch_momentum(p, dt, h->stream);
-        if (h->ntr > 0) vphys::launch_tracers(p, dt, true, h->cfg.use_kpp != 0, h->stream);
-        h->gen += 1;
-    }
+    if ((st = launch_steps(h, p, dt, n_steps))) return st;
     if ((st = cuda_status(cudaGetLastError(), "vphys_step launch"))) return st;
+    if (h->cfg.vmix_guard) {
+        int gs = VPHYS_OK;
+        if ((st = read_guard(h, &gs))) return st;
+        return gs;
+    }
+    return VPHYS_OK;
+}
+
+int vphys_step_graph(vphys_handle h, double dt, int n_steps)
+{
+    if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_step_graph: bad handle");
+    if (n_steps <= 0) return VPHYS_OK;
+    int st;
+    if ((st = prepare_assemble(h)) || (st = prepare_momentum(h)) || (st = prepare_tracers(h))) return st;
+    if (h->cfg.eos_in_step && (h->cfg.idx_temperature < 0 || h->cfg.idx_salinity < 0))
+        return push_error(VPHYS_ERR_CONFIG, "vphys_step_graph: eos_in_step needs temperature and salinity tracers");
+    if (h->cfg.vmix_guard) {
+        cudaError_t e = cudaMemsetAsync(h->guard_dev, 0, sizeof(unsigned long long), h->stream);
+        if (e != cudaSuccess) return cuda_status(e, "vphys_step_graph guard reset");
+    }
+    Params p = make_params(h);
+    // what the launches depend on: every pointer and knob (Params), dt, n and
+    // the surrogate; any change (a bind, a new config, an attach) recaptures
+    unsigned char sig[sizeof h->gsig] = {};
+    memcpy(sig, &p, sizeof p);
+    memcpy(sig + sizeof p, &h->kpp, sizeof h->kpp);
+    memcpy(sig + sizeof p + sizeof h->kpp, &dt, sizeof dt);
+    memcpy(sig + sizeof p + sizeof h->kpp + 8, &n_steps, sizeof n_steps);
+    sig[sizeof p + sizeof h->kpp + 12] = h->kpp_attached ? 1 : 0;
+    if (!h->gexec || memcmp(sig, h->gsig, sizeof sig) != 0) {
+        if (h->gexec) {
+            cudaGraphExecDestroy(h->gexec);
+            h->gexec = nullptr;
+        }
+        cudaError_t e = cudaSuccess;
+        if (!h->cap_stream) e = cudaStreamCreateWithFlags(&h->cap_stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return cuda_status(e, "vphys_step_graph stream");
+        cudaStream_t user = h->stream;
+        const int gen0 = h->gen;
+        const unsigned kgen0 = h->kgen;
+        h->stream = h->cap_stream;
+        e = cudaStreamBeginCapture(h->cap_stream, cudaStreamCaptureModeRelaxed);
+        int lst = (e == cudaSuccess) ? launch_steps(h, p, dt, n_steps) : VPHYS_OK;
+        cudaGraph_t graph = nullptr;
+        cudaError_t e2 = (e == cudaSuccess) ? cudaStreamEndCapture(h->cap_stream, &graph) : e;
+        h->stream = user;
+        h->gen = gen0;
+        h->kgen = kgen0 + (unsigned)n_steps;
+        if (e != cudaSuccess || e2 != cudaSuccess || lst != VPHYS_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            cudaGetLastError();
+            if (lst != VPHYS_OK) return lst;
+            return cuda_status(e != cudaSuccess ? e : e2, "vphys_step_graph capture");
+        }
+        e = cudaGraphInstantiate(&h->gexec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            h->gexec = nullptr;
+            return cuda_status(e, "vphys_step_graph instantiate");
+        }
+        memcpy(h->gsig, sig, sizeof sig);
+    }
+    cudaError_t e = cudaGraphLaunch(h->gexec, h->stream);
+    if (e != cudaSuccess) return cuda_status(e, "vphys_step_graph launch");
+    h->gen += n_steps;
     if (h->cfg.vmix_guard) {
         int gs = VPHYS_OK;
         if ((st = read_guard(h, &gs))) return st;

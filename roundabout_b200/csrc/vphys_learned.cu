@@ -96,7 +96,13 @@ __global__ void __launch_bounds__(FEAT_THREADS) k_kpp_features(const Params p, c
         all_zero = all_zero && (hk == 0.0);
     }
     double H = 0.0;
-    for (int k = 1; k <= k_sfc; ++k) H += HH(k);
+    for (int k0 = 1; k0 <= k_sfc; k0 += 8) {
+        double hv[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) hv[q] = (k0 + q <= k_sfc) ? HH(k0 + q) : 0.0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) H += hv[q];
+    }
 
     const double u_star = sqrt(xdiv(p.stress_mag[col], rho0));
     const double q_T_kin = xdiv(p.q_heat[col], rho0 * c.cp);
@@ -118,23 +124,42 @@ __global__ void __launch_bounds__(FEAT_THREADS) k_kpp_features(const Params p, c
         d_ref = 0.5 * h_above;
         d_c = d_ref;
     }
-    for (int m = 0; m < LK_LEV; ++m) {
-        const int k = k_sfc - 1 - m;
-        float n2 = 0.0f, s2 = 0.0f;
-        if (!all_zero && k >= 1) {
-            const double h_k = HH(k);
-            d_c = d_c + 0.5 * (h_above + h_k);
-            const double dd = d_c - d_ref;
-            const double db = b_ref - (-(GRAVITY * __ldg(rp + P * (size_t)(k - 1)) / rho0));
-            const double du = UC(k) - u_ref, dv = VC(k) - v_ref;
-            if (dd > 0.0) {
-                n2 = (float)(db / dd);
-                s2 = (float)((du * du + dv * dv) / (dd * dd));
-            }
-            h_above = h_k;
+    // the walk down from the surface layer; loads go FEAT_U levels ahead
+    constexpr int FEAT_U = 4;
+    for (int m0 = 0; m0 < LK_LEV; m0 += FEAT_U) {
+        double hk[FEAT_U], rk[FEAT_U], ua[FEAT_U], ub[FEAT_U], va[FEAT_U], vb[FEAT_U];
+#pragma unroll
+        for (int q = 0; q < FEAT_U; ++q) {
+            const int k = k_sfc - 1 - (m0 + q);
+            const bool in = !all_zero && k >= 1 && m0 + q < LK_LEV;
+            const size_t o = P * (size_t)(k - 1), ou = PU * (size_t)(k - 1), ov = PV * (size_t)(k - 1);
+            hk[q] = in ? __ldg(hp + o) : 0.0;
+            rk[q] = in ? __ldg(rp + o) : 0.0;
+            ua[q] = in ? __ldg(up + ou) : 0.0;
+            ub[q] = in ? __ldg(up + ou + 1) : 0.0;
+            va[q] = in ? __ldg(vp + ov) : 0.0;
+            vb[q] = in ? __ldg(vp + ov + nx) : 0.0;
         }
-        emit(o, srow, col, 4 + m, slog6(n2), oor);
-        emit(o, srow, col, 4 + LK_LEV + m, slog6(s2), oor);
+#pragma unroll
+        for (int q = 0; q < FEAT_U; ++q) {
+            const int m = m0 + q;
+            if (m >= LK_LEV) break;
+            const int k = k_sfc - 1 - m;
+            float n2 = 0.0f, s2 = 0.0f;
+            if (!all_zero && k >= 1) {
+                d_c = d_c + 0.5 * (h_above + hk[q]);
+                const double dd = d_c - d_ref;
+                const double db = b_ref - (-(GRAVITY * rk[q] / rho0));
+                const double du = 0.5 * (ua[q] + ub[q]) - u_ref, dv = 0.5 * (va[q] + vb[q]) - v_ref;
+                if (dd > 0.0) {
+                    n2 = (float)(db / dd);
+                    s2 = (float)((du * du + dv * dv) / (dd * dd));
+                }
+                h_above = hk[q];
+            }
+            emit(o, srow, col, 4 + m, slog6(n2), oor);
+            emit(o, srow, col, 4 + LK_LEV + m, slog6(s2), oor);
+        }
     }
     for (int m = LK_IN; m < LK_INP; ++m) {   // K padding
         srow[m] = __float2bfloat16_rn(0.0f);

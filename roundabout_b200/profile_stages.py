@@ -2,6 +2,11 @@
 
     python -m roundabout_b200.profile_stages --nx 512 --ny 384 --nz 75 --ntr 4 --reps 3
     python -m roundabout_b200.profile_stages --config batched_1440x1080x75 --mixed 1
+    python -m roundabout_b200.profile_stages --nx 512 --ny 384 --stages features,mlp
+
+Stages: eos, assemble, momentum, tracers, step (the path) and features, mlp
+(the learned KPP's feature extraction and its three tensor-core GEMMs, with
+untrained weights: the time does not depend on their values).
 
 Prints, per stage, the mean device time and the algorithmic GB/s; used as the
 driver of the ncu captures kept under profiles/.
@@ -55,6 +60,27 @@ def main():
            "step": 8 * (4 + args.ntr) + 8 * (2 + args.ntr) + 24 * ifc}
     fns = {"eos": vp.eos, "assemble": vp.assemble, "momentum": lambda: vp.vdiff_momentum(dt),
            "tracers": lambda: vp.vdiff_tracers(dt), "step": lambda: vp.step(dt, 1)}
+    ncols = args.nx * args.ny
+    if "features" in args.stages or "mlp" in args.stages:
+        import ctypes
+
+        from . import _ffi
+        from . import learned as L
+
+        sur = L.KPPSurrogate(seed=1)
+        X = torch.empty(ncols, L.NINP, dtype=torch.bfloat16, device="cuda")
+        gate = torch.empty(ncols, dtype=torch.uint8, device="cuda")
+        colH = torch.empty(ncols, device="cuda")
+
+        def features():
+            _ffi.check(vp.lib.vphys_kpp_features(vp.handle, L._p(sur.feat_mean), L._p(sur.feat_istd),
+                                                 ctypes.c_float(8.0), None, L._p(X), None, 0, L._p(gate),
+                                                 L._p(colH)), "vphys_kpp_features")
+
+        fns["features"] = features
+        fns["mlp"] = lambda: sur.forward(X)
+        bpc["features"] = 40.0 + L.NINP * 2.0 / args.nz   # h, rho, u, v (two faces each) -> X
+        bpc["mlp"] = (L.NINP * 2 + 4 * L.NHID * 2 + L.NOUTP * 4) / args.nz   # X in, H1/H2 out+in, Y out
     out = {}
     for name in args.stages.split(","):
         fn = fns[name]

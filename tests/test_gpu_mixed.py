@@ -191,3 +191,21 @@ def test_exact_path_unchanged_after_mixed(VP, oracle):
         assert_bitwise(f"tracer{t}", vp.get_tracer(t), st.tracers[t])
     assert_bitwise("u", vp.get("u"), st.u)
     assert_bitwise("kv", vp.get("kv"), st.kv)
+
+
+@pytest.mark.parametrize("level", [0, 1])
+def test_step_graph_equals_steps(VP, level):
+    """vphys_step_graph replays the captured launches: the same state as
+    vphys_step, bit for bit, and a rebind recaptures."""
+    cols = columns(nx=40, ny=24, nz=30, seed=36, ntr=4, thin_frac=0.15)
+    a = VP(cols.nx, cols.ny, cols.nz, 4, hot_cfg(ntr=4, mixed_precision=level))
+    b = VP(cols.nx, cols.ny, cols.nz, 4, hot_cfg(ntr=4, mixed_precision=level))
+    a.load_columns(cols)
+    b.load_columns(cols)
+    a.step(DT, 6)
+    b.step_graph(DT, 3)
+    b.step_graph(DT, 3)
+    for t in range(4):
+        assert_bitwise(f"tracer{t}", b.get_tracer(t), a.get_tracer(t))
+    for n in ("u", "v", "kv", "kt", "bl_depth"):
+        assert_bitwise(n, b.get(n), a.get(n))
