@@ -254,7 +254,9 @@ def main():
 
     gen_spec = dict(spec)
     gen_spec.pop("ntracers")
-    cols = make_columns(ntracers=ntr, seed=1234 + rank, **gen_spec)
+    from roundabout_b200.ranks import rank_seed
+
+    cols = make_columns(ntracers=ntr, seed=rank_seed(1234, rank), **gen_spec)
     mixed = args.form == "mixed"
     cfg = hot_path_config(ntracers=ntr)
     cfg.mixed_precision = 1 if mixed else 0
@@ -268,12 +270,10 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
+    from roundabout_b200.ranks import max_over_ranks as _mor, rank_seed, weak_scaling_value
+
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return _mor(x, dist)
 
     dt = 3600.0
     cells = nx * ny * nz
@@ -350,7 +350,7 @@ def main():
 
     with ClockSampler(local) as clk:
         ms = timed(vp, args.steps, args.warmup)
-    value = cells * args.steps * world / (ms / 1e3)
+    value = weak_scaling_value(cells, args.steps, world, ms)
     if mixed:
         forms["mixed"] = {"cells_per_s": value, "ms_per_step": ms / args.steps}
         if "plain_fp64" in forms:

@@ -37,6 +37,8 @@
 // velocity read again from L2 (evict_last) by the back-substitution.
 #include <cuda_runtime.h>
 
+#include <cstdlib>
+
 #include "vphys_device.cuh"
 #include "vphys_faces.cuh"
 #include "vphys_kernels.cuh"
@@ -165,13 +167,26 @@ __device__ __forceinline__ void tracer_back(const Params &p, double dt, double *
     }
 }
 
-template <bool TWO>
-__global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, double dt, int nonlocal, int ngx)
+// Tracer groups of a launch: the first `single` groups hold one tracer each
+// (those with a non-local deposit or a budget, whose back-substitution is
+// their own), the rest up to TPW tracers in the order of `perm`.
+struct TracerGroups {
+    int single, ngroups;
+    signed char perm[NTR_MAX];
+};
+
+// TPW tracers per warp share one factorisation and one t array (TWO, a
+// separate ks, keeps one tracer per warp); their forward chains interleave.
+template <bool TWO, int TPW>
+__global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, double dt, int nonlocal, int ngx,
+                                                           const TracerGroups tg)
 {
+    const int ngroups = tg.ngroups;
+    constexpr int U = (TPW >= 4) ? 4 : MP_TR_U;   // levels per load block
     extern __shared__ __align__(16) float smf[];
     const int lane = threadIdx.x;
-    const int tr = blockIdx.x % p.ntr;   // the tracers of a column group are adjacent blocks
-    const unsigned g = blockIdx.x / p.ntr;
+    const int grp = blockIdx.x % ngroups;          // the tracer groups of a column group are adjacent blocks
+    const unsigned g = blockIdx.x / ngroups;
     const int gi = g % ngx, j = g / ngx;
     const int i = gi * MP_TR_COLS + lane;
     const vphys_config &c = p.cfg;
@@ -182,7 +197,26 @@ __global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, doubl
     const double *__restrict__ hp = p.h + col;
     const int iT = c.idx_temperature, iS = c.idx_salinity, iPS = c.idx_pseudo_salt;
     const size_t NB = (size_t)nz * MP_TR_COLS;
-    float *tu = smf + lane, *vv = tu + NB;   // t and v per level, this lane's column
+    int nt, tix[TPW];   // tracers of this group
+    if (grp < tg.single) {
+        nt = 1;
+        tix[0] = tg.perm[grp];
+    } else {
+        const int base = tg.single + (grp - tg.single) * TPW;
+        nt = min(TPW, p.ntr - base);
+#pragma unroll
+        for (int q = 0; q < TPW; ++q) tix[q] = tg.perm[base + (q < nt ? q : 0)];
+    }
+    if (grp >= tg.single) {
+#pragma unroll
+        for (int q = 1; q < TPW; ++q)
+            if (q >= nt) tix[q] = tix[0];
+    } else {
+#pragma unroll
+        for (int q = 1; q < TPW; ++q) tix[q] = tix[0];
+    }
+    float *tu = smf + lane;                        // t per level, this lane's column
+    float *vv = tu + NB;                           // v per level and tracer (stride NB)
     const float HV = (float)H_VANISHED;
 
     // ---- this column's live span (k_spans); rows outside it are identity rows ----
@@ -193,33 +227,42 @@ __global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, doubl
     const int w_hi = __reduce_max_sync(0xffffffffu, hi);
     if (w_hi == 0) return;
 
-    const double *__restrict__ Kp = ((TWO && tr != iT) ? p.ks : p.kt) + col;
-    double *__restrict__ trc = p.tr[tr] + col;
+    const double *__restrict__ Kp = ((TWO && tix[0] != iT) ? p.ks : p.kt) + col;
+    double *trc[TPW];
+#pragma unroll
+    for (int q = 0; q < TPW; ++q) trc[q] = p.tr[tix[q]] + col;
     const unsigned long long pol_keep = l2_policy_evict_last();
     const float dtf = (float)dt;
 
-    // ---- upward: factorisation (FP32) + FP64 residual and accumulation.
-    //      Branch-free rows: outside [lo, hi] nothing is loaded, h = 0 gates
-    //      both couplings off and the row solves to an increment of 0 ----
+    // ---- upward: factorisation (FP32, once for the group) + FP64 residual and
+    //      accumulation of every tracer.  Branch-free rows: outside [lo, hi]
+    //      nothing is loaded, h = 0 gates both couplings off and the row
+    //      solves to an increment of 0 ----
     {
         const bool first = (w_lo == lo);   // the lane's span starts at the warp's first row
         double h_c = first ? __ldg(hp + P * (size_t)(w_lo - 1)) : 0.0;
-        double d_c = first ? ld_hint(trc + P * (size_t)(w_lo - 1), pol_keep) : 0.0;
-        double d_m = 0.0, w = 0.0;
-        float f_dn = 0.0f, q_prev = 1.0f, t_prev = 0.0f;
-        for (int k0 = w_lo; k0 <= w_hi; k0 += MP_TR_U) {
-            double hn[MP_TR_U], kn[MP_TR_U], dn[MP_TR_U];
+        double d_c[TPW], d_m[TPW], w[TPW];
 #pragma unroll
-            for (int u = 0; u < MP_TR_U; ++u) {
+        for (int q = 0; q < TPW; ++q) {
+            d_c[q] = (first && q < nt) ? ld_hint(trc[q] + P * (size_t)(w_lo - 1), pol_keep) : 0.0;
+            d_m[q] = 0.0;
+            w[q] = 0.0;
+        }
+        float f_dn = 0.0f, q_prev = 1.0f, t_prev = 0.0f;
+        for (int k0 = w_lo; k0 <= w_hi; k0 += U) {
+            double hn[U], kn[U], dn[U][TPW];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
                 const int k = k0 + u;   // row k reads h, K and d one level up
                 const bool need = k + 1 >= lo && k + 1 <= hi;
                 const size_t o = P * (size_t)k;
                 hn[u] = need ? __ldg(hp + o) : 0.0;
                 kn[u] = need ? __ldg(Kp + o) : 0.0;
-                dn[u] = need ? ld_hint(trc + o, pol_keep) : 0.0;
+#pragma unroll
+                for (int q = 0; q < TPW; ++q) dn[u][q] = (need && q < nt) ? ld_hint(trc[q] + o, pol_keep) : 0.0;
             }
 #pragma unroll
-            for (int u = 0; u < MP_TR_U; ++u) {
+            for (int u = 0; u < U; ++u) {
                 const int k = k0 + u;
                 if (k > w_hi) break;
                 // row k (build_factorize_tracer_matrix: rdb_ocean_vdiff.F90:1285-1341;
@@ -228,50 +271,98 @@ __global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, doubl
                 const float Hp = fmx((float)hn[u], HV);
                 const bool coupled = h_c > H_VANISHED && hn[u] > H_VANISHED;
                 const float f_up = coupled ? __fdividef(dtf * (float)kn[u], face_thick(H, Hp, c.use_harmonic)) : 0.0f;
-                float ip, t, q;
-                pivot_row(H + f_dn * q_prev, f_up, ip, t, q);
-                const double b = (double)f_dn * (d_m - d_c) + (double)f_up * (dn[u] - d_c);
-                w = b + mul_u(t_prev, w);
+                float ip, t, qq;
+                pivot_row(H + f_dn * q_prev, f_up, ip, t, qq);
                 const size_t s = (size_t)(k - 1) * MP_TR_COLS;
-                vv[s] = (float)(w * (double)ip);
+                const double fd = (double)f_dn, fu = (double)f_up, ipd = (double)ip;
+#pragma unroll
+                for (int q = 0; q < TPW; ++q) {
+                    const double b = fd * (d_m[q] - d_c[q]) + fu * (dn[u][q] - d_c[q]);
+                    w[q] = b + mul_u(t_prev, w[q]);
+                    vv[(size_t)q * NB + s] = (float)(w[q] * ipd);
+                    d_m[q] = d_c[q];
+                    d_c[q] = dn[u][q];
+                }
                 tu[s] = t;
                 t_prev = t;
-                q_prev = q;
+                q_prev = qq;
                 f_dn = f_up;
-                d_m = d_c;
-                d_c = dn[u];
                 h_c = hn[u];
             }
         }
     }
 
-    // ---- non-local column scalars (FP64, as KPP pass 2) ----
-    const bool nl_t = nonlocal && c.use_kpp && (tr == iT || tr == iS || tr == iPS);
-    bool nl = nl_t && live;
-    double h_b = 0.0, q_kin = 0.0;
-    if (nl) {
-        const double rho0 = c.rho0;
-        h_b = p.bl_depth[col];
-        const double u_star = sqrt(xdiv(p.stress_mag[col], rho0));
-        const double q_T_kin = xdiv(p.q_heat[col], rho0 * c.cp);
-        const double q_S_kin = xdiv(p.q_salt[col], rho0);
-        const double B_0 = (GRAVITY / rho0) * (c.alpha_T * q_T_kin - c.beta_S * q_S_kin);
-        const double wstar3 = fmx(0.0, -B_0) * h_b;
-        const double w_star = sm_cbrt(wstar3);
-        const double w_s = sqrt(u_star * u_star + w_star * w_star);
-        nl = (h_b > 0.0 && w_s > 0.0 && B_0 < 0.0);
-        q_kin = (tr == iT) ? q_T_kin : q_S_kin;
-    }
-    double *bud = nullptr;
-    if (c.budgets && tr == iT) bud = p.heat_budget + col;
-    if (c.budgets && tr == iS) bud = p.salt_budget + col;
-
-    // ---- back-substitution, FP64 update (+ budgets, non-local deposit), store ----
+    // ---- back-substitution ----
     const unsigned long long pol_once = l2_policy_evict_first();
-    if (nl_t || (c.budgets && (tr == iT || tr == iS)))
-        tracer_back<true>(p, dt, trc, hp, tu, vv, w_lo, w_hi, lo, hi, bud, nl_t, nl, h_b, q_kin, pol_once);
-    else
-        tracer_back<false>(p, dt, trc, hp, tu, vv, w_lo, w_hi, lo, hi, nullptr, false, false, 0.0, 0.0, pol_once);
+    bool any_full = false;
+#pragma unroll
+    for (int q = 0; q < TPW; ++q) {
+        const int tr = tix[q];
+        if (q < nt && (((nonlocal && c.use_kpp) && (tr == iT || tr == iS || tr == iPS)) ||
+                       (c.budgets && (tr == iT || tr == iS))))
+            any_full = true;
+    }
+    if (!any_full) {
+        // every tracer of the group is a plain diffusion: one fused downward pass
+        float delta[TPW];
+#pragma unroll
+        for (int q = 0; q < TPW; ++q) delta[q] = 0.0f;
+        for (int k0 = w_hi; k0 >= w_lo; k0 -= U) {
+            double dk[U][TPW];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int k = k0 - u;
+#pragma unroll
+                for (int q = 0; q < TPW; ++q)
+                    dk[u][q] = (k >= lo && k <= hi && q < nt) ? ld_hint(trc[q] + P * (size_t)(k - 1), pol_once) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int k = k0 - u;
+                if (k < w_lo) break;
+                const size_t s = (size_t)(k - 1) * MP_TR_COLS;
+                const float tk = tu[s];
+#pragma unroll
+                for (int q = 0; q < TPW; ++q) delta[q] = vv[(size_t)q * NB + s] + mul_u(tk, delta[q]);
+                if (k < lo || k > hi) continue;
+                const size_t off = P * (size_t)(k - 1);
+#pragma unroll
+                for (int q = 0; q < TPW; ++q)
+                    if (q < nt) trc[q][off] = dk[u][q] + (double)delta[q];
+            }
+        }
+        return;
+    }
+    for (int q = 0; q < nt; ++q) {
+        const int tr = tix[q];
+        // ---- non-local column scalars (FP64, as KPP pass 2) ----
+        const bool nl_t = nonlocal && c.use_kpp && (tr == iT || tr == iS || tr == iPS);
+        bool nl = nl_t && live;
+        double h_b = 0.0, q_kin = 0.0;
+        if (nl) {
+            const double rho0 = c.rho0;
+            h_b = p.bl_depth[col];
+            const double u_star = sqrt(xdiv(p.stress_mag[col], rho0));
+            const double q_T_kin = xdiv(p.q_heat[col], rho0 * c.cp);
+            const double q_S_kin = xdiv(p.q_salt[col], rho0);
+            const double B_0 = (GRAVITY / rho0) * (c.alpha_T * q_T_kin - c.beta_S * q_S_kin);
+            const double wstar3 = fmx(0.0, -B_0) * h_b;
+            const double w_star = sm_cbrt(wstar3);
+            const double w_s = sqrt(u_star * u_star + w_star * w_star);
+            nl = (h_b > 0.0 && w_s > 0.0 && B_0 < 0.0);
+            q_kin = (tr == iT) ? q_T_kin : q_S_kin;
+        }
+        double *bud = nullptr;
+        if (c.budgets && tr == iT) bud = p.heat_budget + col;
+        if (c.budgets && tr == iS) bud = p.salt_budget + col;
+        double *t_ptr = p.tr[tr] + col;
+        const float *vq = vv + (size_t)q * NB;
+        if (nl_t || bud)
+            tracer_back<true>(p, dt, t_ptr, hp, tu, vq, w_lo, w_hi, lo, hi, bud, nl_t, nl, h_b, q_kin, pol_once);
+        else
+            tracer_back<false>(p, dt, t_ptr, hp, tu, vq, w_lo, w_hi, lo, hi, nullptr, false, false, 0.0, 0.0,
+                               pol_once);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -459,28 +550,68 @@ __global__ void __launch_bounds__(MP_MOM_THREADS) k_momentum_mp(const Params p, 
     }
 }
 
-template <bool TWO>
+template <bool TWO, int TPW>
 static void launch_tracers_mp_t(const Params &p, double dt, bool nonlocal, cudaStream_t stream)
 {
-    const size_t smem = (size_t)p.nz * MP_TR_COLS * 2 * sizeof(float);
+    const size_t smem = (size_t)p.nz * MP_TR_COLS * (1 + TPW) * sizeof(float);
     static bool attr_set = false;
     if (!attr_set) {
-        cudaFuncSetAttribute(k_tracers_mp<TWO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)((size_t)VPHYS_NZ_MAX * MP_TR_COLS * 2 * sizeof(float)));
+        cudaFuncSetAttribute(k_tracers_mp<TWO, TPW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)((size_t)VPHYS_NZ_MAX * MP_TR_COLS * (1 + TPW) * sizeof(float)));
         attr_set = true;
     }
-    k_spans<<<dim3((p.nx + 127) / 128, p.ny), 128, 0, stream>>>(p);
+    // tracers with a non-local deposit or a budget first, one per group; the
+    // plain diffusions after them, TPW per group
+    const vphys_config &c = p.cfg;
+    TracerGroups tg{};
+    int n = 0;
+    for (int t = 0; t < p.ntr; ++t) {
+        const bool full = (nonlocal && c.use_kpp &&
+                           (t == c.idx_temperature || t == c.idx_salinity || t == c.idx_pseudo_salt)) ||
+                          (c.budgets && (t == c.idx_temperature || t == c.idx_salinity));
+        if (full || TPW == 1) tg.perm[n++] = (signed char)t;
+    }
+    tg.single = n;
+    for (int t = 0; t < p.ntr && TPW > 1; ++t) {
+        const bool full = (nonlocal && c.use_kpp &&
+                           (t == c.idx_temperature || t == c.idx_salinity || t == c.idx_pseudo_salt)) ||
+                          (c.budgets && (t == c.idx_temperature || t == c.idx_salinity));
+        if (!full) tg.perm[n++] = (signed char)t;
+    }
+    tg.ngroups = tg.single + (p.ntr - tg.single + TPW - 1) / TPW;
     const int ngx = (p.nx + MP_TR_COLS - 1) / MP_TR_COLS;
-    const unsigned blocks = (unsigned)ngx * (unsigned)p.ny * (unsigned)p.ntr;
-    k_tracers_mp<TWO><<<blocks, MP_TR_COLS, smem, stream>>>(p, dt, nonlocal ? 1 : 0, ngx);
+    const unsigned blocks = (unsigned)ngx * (unsigned)p.ny * (unsigned)tg.ngroups;
+    k_tracers_mp<TWO, TPW><<<blocks, MP_TR_COLS, smem, stream>>>(p, dt, nonlocal ? 1 : 0, ngx, tg);
+}
+
+// Tracers per warp: VPHYS_MP_TRACERS_PER_WARP (1, 2 or 4) when set, else 1
+// (measured on 1440x1080x75: sharing a warp saves the repeated factorisation
+// but the larger register and shared-memory footprint costs more warps per
+// SM than it gains).  A separate ks keeps one per warp.
+static int tracers_per_warp(int ntr)
+{
+    static int forced = -1;
+    if (forced < 0) {
+        const char *e = getenv("VPHYS_MP_TRACERS_PER_WARP");
+        forced = e ? atoi(e) : 0;
+        if (forced != 1 && forced != 2 && forced != 4) forced = 0;
+    }
+    (void)ntr;
+    return forced ? forced : 1;
 }
 
 void launch_tracers_mp(const Params &p, double dt, bool nonlocal, cudaStream_t stream)
 {
-    if (p.ks_equals_kt)
-        launch_tracers_mp_t<false>(p, dt, nonlocal, stream);
-    else
-        launch_tracers_mp_t<true>(p, dt, nonlocal, stream);
+    k_spans<<<dim3((p.nx + 127) / 128, p.ny), 128, 0, stream>>>(p);
+    if (!p.ks_equals_kt) {
+        launch_tracers_mp_t<true, 1>(p, dt, nonlocal, stream);
+        return;
+    }
+    switch (tracers_per_warp(p.ntr)) {
+    case 4: launch_tracers_mp_t<false, 4>(p, dt, nonlocal, stream); break;
+    case 2: launch_tracers_mp_t<false, 2>(p, dt, nonlocal, stream); break;
+    default: launch_tracers_mp_t<false, 1>(p, dt, nonlocal, stream); break;
+    }
 }
 
 void launch_momentum_mp(const Params &p, double dt, cudaStream_t stream)
