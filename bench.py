@@ -11,9 +11,10 @@ reference's Mcells/s convention, benchmarks/bench_ocean.F90:149-150) on the
 1440x1080x75 eddy-permitting configuration with T, S and 2 passives; the
 state is FP64 at the interface in every form.
 
-Forms (--form): "mixed" (default) runs the Thomas sweeps in FP32 with the
-FP64 residual correction (cfg.mixed_precision = 1); "plain" is FP64
-throughout and bitwise the reference's arithmetic.  The line's "forms" object
+Forms (--form): "mixed" (default) runs the assembly's interface sweep and
+the Thomas sweeps in FP32 with the FP64 residual correction
+(cfg.mixed_precision = 2; --mixed-level 1 keeps the assembly FP64); "plain"
+is FP64 throughout and bitwise the reference's arithmetic.  The line's "forms" object
 carries both forms' cells/s and the mixed form's error against the plain FP64
 GPU path after one step from the same state, over the whole domain.
 
@@ -63,8 +64,10 @@ def parse():
     ap.add_argument("--cpu-sample", default="360x270", help="nx x ny of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--form", default="mixed", choices=["mixed", "plain"],
-                    help="mixed: FP32 Thomas sweeps + FP64 residual (cfg.mixed_precision=1); "
+                    help="mixed: FP32 assembly and Thomas sweeps + FP64 residual (cfg.mixed_precision=2); "
                          "plain: FP64 throughout, bitwise the reference's arithmetic")
+    ap.add_argument("--mixed-level", type=int, default=2, choices=[1, 2],
+                    help="1: FP64 assembly, FP32 sweeps; 2: FP32 assembly too (the default)")
     ap.add_argument("--no-compare", action="store_true", help="skip the plain-FP64 timing and error check")
     ap.add_argument("--learned-cols", type=int, default=1_048_576,
                     help="training columns of the learned-KPP surrogate timed beside the mixed form (0: skip)")
@@ -259,7 +262,7 @@ def main():
     cols = make_columns(ntracers=ntr, seed=rank_seed(1234, rank), **gen_spec)
     mixed = args.form == "mixed"
     cfg = hot_path_config(ntracers=ntr)
-    cfg.mixed_precision = 1 if mixed else 0
+    cfg.mixed_precision = args.mixed_level if mixed else 0
     vp = VerticalPhysics(nx, ny, nz, ntr, cfg)
     vp.load_columns(cols)
     torch.cuda.synchronize()
@@ -325,7 +328,7 @@ def main():
 
         sur, _ = L.train_surrogate(args.learned_cols, nz=nz, seed=100, epochs=4)
         cfg_l = hot_path_config(ntracers=ntr)
-        cfg_l.mixed_precision = 1
+        cfg_l.mixed_precision = args.mixed_level
         cfg_l.learned_kpp = 1
         vl = VerticalPhysics(nx, ny, nz, ntr, cfg_l)
         vl.load_columns(cols)
@@ -450,7 +453,8 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if mixed else "f64", "data": "synthetic",
             "config": config_out, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": (5 if mixed else 4) * args.steps, "clocks": clocks, "forms": forms,
-            "mode": ("FP64 state, FP32 Thomas sweeps with FP64 residual correction (mixed_precision=1)" if mixed
+            "mode": (f"FP64 state, FP32 assembly and Thomas sweeps with FP64 residual correction "
+                     f"(mixed_precision={args.mixed_level})" if mixed
                      else "plain FP64, bit-identical to the CPU restatement")}
     vp.close()
     if dist is not None:

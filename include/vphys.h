@@ -211,8 +211,10 @@ int vphys_get_config(vphys_handle h, vphys_config *cfg);
 int vphys_set_stream(vphys_handle h, void *stream);
 
 /* Zero-copy: use the caller's device array for `field` from now on.
- * The pointer must stay valid while the handle uses it; NULL restores the
- * handle-owned buffer. */
+ * The pointer must stay valid while the handle uses it.  The handle's own
+ * buffer for the field is freed (a bound state is never held twice); NULL
+ * unbinds and gives the field a fresh handle-owned buffer with its default
+ * contents.  Synchronises the device when a buffer is freed. */
 int vphys_bind(vphys_handle h, int field, void *device_ptr);
 
 /* Synchronous host<->device copies of a whole field (n = element count,

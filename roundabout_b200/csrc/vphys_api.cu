@@ -633,6 +633,13 @@ int vphys_bind(vphys_handle h, int field, void *device_ptr)
     int sl = slot_of(h, field);
     if (sl < 0) return push_error(VPHYS_ERR_NOT_FOUND, "vphys_bind: unknown field id %d", field);
     h->f[sl].bound = device_ptr;
+    if (device_ptr && h->f[sl].own) {
+        // the caller's array replaces the handle's own buffer: free it (a
+        // later unbind allocates a fresh one), so binding every large field
+        // does not hold two copies of the state
+        cudaFree(h->f[sl].own);
+        h->f[sl].own = nullptr;
+    }
     if (!device_ptr && !h->f[sl].own) {
         // restore a handle-owned buffer only for core fields / tracers
         if (sl < VPHYS_FIELD_LAMBDA_BOT_U || sl >= NFIXED) return ensure(h, field);

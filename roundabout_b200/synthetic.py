@@ -177,4 +177,96 @@ CONFIGS = {
     "eddy_1440x1080x75": dict(nx=1440, ny=1080, nz=75, ntracers=4, land_frac=0.3, thin_frac=0.0),
     "batched_1440x1080x75": dict(nx=1440, ny=1080, nz=75, ntracers=10, land_frac=0.3, thin_frac=0.15,
                                  passive_init="uniform"),
+    # built on the device (make_columns_device): T, S + 4 passives
+    "combined_3600x2700x75": dict(nx=3600, ny=2700, nz=75, ntracers=6, land_frac=0.3, thin_frac=0.0,
+                                  passive_init="uniform"),
 }
+
+
+# ---------------------------------------------------------------------------
+# Device-side generator for the shapes too large to build on the host
+# ---------------------------------------------------------------------------
+def make_columns_device(nx, ny, nz, ntracers=6, seed=1234, land_frac=0.3, passive_init="uniform", rho0=1035.0):
+    """The same distributions as `make_columns`, drawn on the GPU with torch's
+    seeded Philox generator (a different random stream, so not the same
+    numbers), returned as contiguous CUDA float64 tensors in the reference's
+    layout (torch shape (nz, ny, nx) is Fortran (nx, ny, nz)) ready for
+    VerticalPhysics.bind.  For 3600x2700x75 no field ever exists on the host.
+    Returns a dict: h, u, v, tracers (list), tau_x, tau_y, q_heat, q_salt,
+    wet, coriolis."""
+    import math
+
+    import torch
+
+    dev = "cuda"
+    g = torch.Generator(device=dev).manual_seed(seed)
+    f64 = torch.float64
+
+    def smooth():
+        x = (torch.arange(nx, device=dev, dtype=f64) + 0.5) / nx
+        y = (torch.arange(ny, device=dev, dtype=f64) + 0.5) / ny
+        f = torch.zeros(ny, nx, device=dev, dtype=f64)
+        for _ in range(8):
+            kx = int(torch.randint(0, 5, (1,), generator=g, device=dev))
+            ky = int(torch.randint(0, 5, (1,), generator=g, device=dev))
+            amp = float(torch.randn(1, generator=g, device=dev))
+            ph = float(torch.rand(1, generator=g, device=dev)) * 2 * math.pi
+            f += amp * torch.cos(2 * math.pi * (kx * x[None, :] + ky * y[:, None]) + ph)
+        return f
+
+    bathy = smooth()
+    bmin, bmax = float(bathy.min()), float(bathy.max())
+    bathy = 500.0 + (bathy - bmin) * (4500.0 / max(bmax - bmin, 1e-30))
+    wet = torch.ones(ny, nx, device=dev, dtype=f64)
+    if land_frac > 0:
+        lf = smooth()
+        flat = lf.flatten()
+        sample = flat[torch.randperm(flat.numel(), generator=g, device=dev)[: min(flat.numel(), 1 << 22)]]
+        thr = float(torch.quantile(sample, land_frac))
+        wet = (lf > thr).to(f64)
+
+    dz_td = torch.tensor(layer_stack(nz), device=dev, dtype=f64)
+    edges = torch.cat([torch.zeros(1, device=dev, dtype=f64), torch.cumsum(dz_td, 0)])
+    h = torch.empty(nz, ny, nx, device=dev, dtype=f64)
+    for kt in range(nz):   # surface-first index kt -> bottom-up k = nz - 1 - kt
+        h[nz - 1 - kt] = torch.clamp(torch.minimum(edges[kt + 1], bathy) - edges[kt], min=0.0) * wet
+    zc = -(edges[:-1] + 0.5 * dz_td).flip(0)   # layer-centre depth, bottom-up
+    T = 2.0 + 18.0 * torch.exp(zc / 500.0)[:, None, None] + 0.05 * torch.randn(nz, ny, nx, generator=g, device=dev,
+                                                                              dtype=f64)
+    S = 35.0 + 0.1 * torch.randn(nz, ny, nx, generator=g, device=dev, dtype=f64)
+    decay = torch.exp(zc / 300.0)[:, None, None]
+    wu = torch.zeros(ny, nx + 1, device=dev, dtype=f64)
+    wu[:, 1:nx] = torch.minimum(wet[:, :-1], wet[:, 1:])
+    wv = torch.zeros(ny + 1, nx, device=dev, dtype=f64)
+    wv[1:ny, :] = torch.minimum(wet[:-1, :], wet[1:, :])
+    u = 0.1 * torch.randn(nz, ny, nx + 1, generator=g, device=dev, dtype=f64) * decay * wu[None]
+    v = 0.1 * torch.randn(nz, ny + 1, nx, generator=g, device=dev, dtype=f64) * decay * wv[None]
+    tracers = [S, T]
+    for n in range(2, ntracers):
+        if passive_init == "uniform":
+            tracers.append(torch.rand(nz, ny, nx, generator=g, device=dev, dtype=f64))
+        elif n == 2:
+            tracers.append(torch.zeros(nz, ny, nx, device=dev, dtype=f64))
+        else:
+            tracers.append(S.clone())
+    y = (torch.arange(ny, device=dev, dtype=f64) + 0.5) * DX
+    Ly = ny * DX
+    tau_x = (0.1 * torch.sin(math.pi * y / Ly))[:, None].expand(ny, nx + 1).contiguous()
+    tau_y = torch.zeros(ny + 1, nx, device=dev, dtype=f64)
+    q_heat = torch.rand(ny, nx, generator=g, device=dev, dtype=f64) * 200.0 - 100.0
+    fw = (torch.rand(ny, nx, generator=g, device=dev, dtype=f64) * 2.0 - 1.0) * 1.0e-7
+    q_salt = -rho0 * 35.0 * fw
+    coriolis = (1.0e-4 + 2.0e-11 * y)[:, None].expand(ny, nx).contiguous()
+    return {"h": h.contiguous(), "u": u.contiguous(), "v": v.contiguous(), "tracers": tracers, "tau_x": tau_x,
+            "tau_y": tau_y, "q_heat": q_heat.contiguous(), "q_salt": q_salt.contiguous(), "wet": wet.contiguous(),
+            "coriolis": coriolis}
+
+
+def bind_device_columns(vp, d):
+    """Bind a `make_columns_device` dict to a VerticalPhysics handle (zero
+    copy) and derive the stress magnitude."""
+    for name in ("h", "u", "v", "tau_x", "tau_y", "q_heat", "q_salt", "wet", "coriolis"):
+        vp.bind(name, d[name])
+    for t, a in enumerate(d["tracers"][: vp.ntr]):
+        vp.bind(f"tracer{t}", a)
+    vp.stress_mag()
