@@ -418,7 +418,10 @@ __global__ void k_smooth(const Params p, double *__restrict__ fld, const double 
 // ---------------------------------------------------------------------------
 // Momentum: one thread per (u face, v face) pair.
 // ---------------------------------------------------------------------------
-constexpr int MOM_THREADS = 128;
+#ifndef VPHYS_MOM_THREADS
+#define VPHYS_MOM_THREADS 128
+#endif
+constexpr int MOM_THREADS = VPHYS_MOM_THREADS;   // face columns per block (c' of each in shared memory)
 
 constexpr int MOM_U = 4;   // levels per load block
 

@@ -46,9 +46,19 @@
 namespace vphys {
 
 constexpr int MP_TR_COLS = 32;      // columns (lanes) per tracer block
-constexpr int MP_TR_U = 8;          // levels per tracer load block
-constexpr int MP_MOM_THREADS = 64;  // face columns per momentum block
-constexpr int MP_MOM_U = 4;         // levels per momentum load block
+#ifndef VPHYS_MP_TR_U
+#define VPHYS_MP_TR_U 4
+#endif
+#ifndef VPHYS_MP_MOM_THREADS
+#define VPHYS_MP_MOM_THREADS 32
+#endif
+#ifndef VPHYS_MP_MOM_U
+#define VPHYS_MP_MOM_U 4
+#endif
+constexpr int MP_TR_U = VPHYS_MP_TR_U;                // levels per tracer load block
+constexpr int MP_TR_UF = 4;   // levels per load block of the back-substitution with the non-local deposit
+constexpr int MP_MOM_THREADS = VPHYS_MP_MOM_THREADS;  // face columns per momentum block
+constexpr int MP_MOM_U = VPHYS_MP_MOM_U;              // levels per momentum load block
 
 // Hardware reciprocal (MUFU, within 1 ulp): the FP32 factors carry no
 // bitwise contract, and their rounding is a consistent perturbation of the
@@ -124,15 +134,16 @@ __device__ __forceinline__ void tracer_back(const Params &p, double dt, double *
     float delta = 0.0f;
     double g_above = 0.0, d_run = 0.0, h_a = 0.0;
     double h_c = (FULL && lo <= hi) ? __ldg(hp + P * (size_t)(hi - 1)) : 0.0;
-    for (int k0 = w_hi; k0 >= w_lo; k0 -= MP_TR_U) {
-        double dk[MP_TR_U];
+    constexpr int BU = FULL ? MP_TR_UF : MP_TR_U;   // the deposit's registers leave room for fewer loads
+    for (int k0 = w_hi; k0 >= w_lo; k0 -= BU) {
+        double dk[BU];
 #pragma unroll
-        for (int u = 0; u < MP_TR_U; ++u) {
+        for (int u = 0; u < BU; ++u) {
             const int k = k0 - u;
             dk[u] = (k >= lo && k <= hi) ? ld_hint(trc + P * (size_t)(k - 1), pol) : 0.0;
         }
 #pragma unroll
-        for (int u = 0; u < MP_TR_U; ++u) {
+        for (int u = 0; u < BU; ++u) {
             const int k = k0 - u;
             if (k < w_lo) break;
             const size_t s = (size_t)(k - 1) * MP_TR_COLS;

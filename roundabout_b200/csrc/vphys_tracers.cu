@@ -26,6 +26,10 @@
 #include "vphys_device.cuh"
 #include "vphys_kernels.cuh"
 
+#ifndef VPHYS_TR_THREADS
+#define VPHYS_TR_THREADS 128
+#endif
+
 namespace vphys {
 
 
@@ -317,7 +321,7 @@ static void launch_tracers_n(const Params &p, double dt, bool diffuse, bool nonl
 {
     // two factorisations keep two c' arrays: halve the block to stay within
     // the 227 KB of shared memory per block at nz = VPHYS_NZ_MAX
-    const int bs = TWO ? 64 : 128;
+    const int bs = TWO ? VPHYS_TR_THREADS / 2 : VPHYS_TR_THREADS;
     const size_t smem = (size_t)p.nz * bs * sizeof(double) * (TWO ? 2 : 1);
     static bool attr_set = false;
     if (!attr_set) {
