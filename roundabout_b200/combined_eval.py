@@ -83,6 +83,8 @@ def main():
     keep = {0: d["tracers"][0].clone(), 1: d["tracers"][1].clone()}
     bl_c = np.asarray(vp.get("bl_depth"))
     out["kpp"] = L.kpp_stats(vp)
+    out["obl_rms_rel_on_own_states"] = float(np.sqrt(out["kpp"]["sum_rel_err2_e6"] / 1e6 /
+                                                     max(out["kpp"]["checked"], 1)))
 
     # the same initial state, plain FP64
     d["u"].copy_(init["u"])

@@ -237,10 +237,14 @@ def kpp_stats(vp):
     return {n: int(out[i]) for i, n in enumerate(names)}
 
 
-def collect(nx, ny, nz, domains, snapshots, seed=100, dt=3600.0, log=None):
-    """(raw features [N, 154], targets [N, 80]) from plain-KPP trajectories of
-    seeded domains (all wet, the benchmark's generators), one sample per column
-    and snapshot step."""
+def collect(nx, ny, nz, domains, snapshots, seed=100, dt=3600.0, log=None, surrogate=None):
+    """(raw features [N, 154], targets [N, 80]) from trajectories of seeded
+    domains (all wet, the benchmark's generators), one sample per column and
+    snapshot step.  Without `surrogate` the trajectories are the plain
+    KPP's; with one they are the learned form's own (the surrogate attached),
+    and each snapshot is still labelled by the plain KPP pass 1 on that state
+    (the lagged h_b put back afterwards, so the trajectory is the learned
+    one's)."""
     import torch
 
     from .column import VerticalPhysics
@@ -252,8 +256,14 @@ def collect(nx, ny, nz, domains, snapshots, seed=100, dt=3600.0, log=None):
     ncols = nx * ny
     for d in range(domains):
         cols = make_columns(nx, ny, nz, ntracers=2, seed=seed + d, land_frac=0.0, thin_frac=0.0)
-        vp = VerticalPhysics(nx, ny, nz, 2, hot_path_config(ntracers=2))
+        cfg_plain = hot_path_config(ntracers=2)
+        cfg_run = hot_path_config(ntracers=2)
+        if surrogate is not None:
+            cfg_run.learned_kpp = 1
+        vp = VerticalPhysics(nx, ny, nz, 2, cfg_run)
         vp.load_columns(cols)
+        if surrogate is not None:
+            surrogate.attach(vp)
         step = 0
         for snap in sorted(snapshots):
             if snap > step:
@@ -264,13 +274,19 @@ def collect(nx, ny, nz, domains, snapshots, seed=100, dt=3600.0, log=None):
             vp.eos()
             _ffi.check(lib.vphys_kpp_features(vp.handle, None, None, ctypes.c_float(1e30), _p(raw), None, None, 0,
                                               None, None), "vphys_kpp_features")
+            lagged = vp.get("bl_depth") if surrogate is not None else None
+            if surrogate is not None:
+                vp.set_config(cfg_plain)
             vp.assemble()
             _ffi.check(lib.vphys_kpp_targets(vp.handle, _p(T)), "vphys_kpp_targets")
+            if surrogate is not None:
+                vp.set("bl_depth", lagged)
+                vp.set_config(cfg_run)
             raws.append(raw)
             tgts.append(T)
         vp.close()
         if log:
-            log(f"domain {d}: {len(snapshots)} snapshots")
+            log(f"domain {d}: {len(snapshots)} snapshots" + (" (learned trajectory)" if surrogate is not None else ""))
     raw = torch.cat(raws)
     T = torch.cat(tgts)
     g = torch.Generator(device="cuda").manual_seed(seed)
@@ -279,10 +295,15 @@ def collect(nx, ny, nz, domains, snapshots, seed=100, dt=3600.0, log=None):
 
 
 def train_surrogate(ncols_target=4_000_000, nz=75, seed=100, epochs=4, batch=8192, snaps=(0, 23, 167, 719),
-                    domain=(256, 1024), log=None):
-    """Collect about `ncols_target` training columns (256 x 1024 domains, so
-    that f and the wind stress span the 1080-row benchmark's ranges;
-    snapshots after 0, 23, 167 and 719 plain steps) and train a surrogate."""
+                    domain=(256, 1024), rounds=1, log=None):
+    """Collect about `ncols_target` training columns (256 x 1024 domains,
+    so that f and the wind stress span the 1080-row benchmark's ranges;
+    snapshots after 0, 23, 167 and 719 plain steps) and train a surrogate.
+    With rounds = 2 the trained network then runs its own trajectories on
+    fresh domains, the plain KPP labels their snapshots, and training goes on
+    over both sets (the network learns the states it actually produces)."""
+    import torch
+
     per = domain[0] * domain[1]
     domains = max(1, round(ncols_target / (per * len(snaps))))
     t0 = time.perf_counter()
@@ -292,6 +313,26 @@ def train_surrogate(ncols_target=4_000_000, nz=75, seed=100, epochs=4, batch=819
     s.fit_standardisation(raw, T)
     X, XT, Ts = s.standardise(raw, T)
     hist = s.train(X, XT, Ts, epochs=epochs, batch=batch, log=log)
+    t_train = s.train_seconds
+    for r in range(1, rounds):
+        del X, XT, Ts
+        t0 = time.perf_counter()
+        raw2, T2 = collect(domain[0], domain[1], nz, domains, list(snaps), seed=seed + 1000 * r, log=log,
+                           surrogate=s)
+        t_collect += time.perf_counter() - t0
+        raw = torch.cat([raw, raw2])
+        T = torch.cat([T, T2])
+        g = torch.Generator(device="cuda").manual_seed(seed + r)
+        perm = torch.randperm(raw.shape[0], generator=g, device="cuda")
+        raw, T = raw[perm].contiguous(), T[perm].contiguous()
+        del raw2, T2
+        X, XT, Ts = s.standardise(raw, T)   # the first round's standardisation stays
+        s.adam_step = 0
+        s.m = [torch.zeros_like(t) for t in s.m]
+        s.v = [torch.zeros_like(t) for t in s.v]
+        hist += s.train(X, XT, Ts, epochs=epochs, batch=batch, lr=1e-3, log=log)
+        t_train += s.train_seconds
     s.collect_seconds = t_collect
+    s.train_seconds = t_train
     s.ntrain = X.shape[0]
     return s, hist
