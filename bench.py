@@ -314,6 +314,7 @@ def main():
         for n in ("u", "v"):
             err[n] = float(np.abs(np.asarray(vp.get(n)) - np.asarray(vp_plain.get(n))).max())
         forms["mixed_max_abs_err_vs_plain_fp64_1step"] = {k: float(f"{v:.3e}") for k, v in err.items()}
+        forms["fp64_resolved_groups_1step"] = vp.mixed_redo_count()
         forms["error_bar"] = "|dT|, |dS|, tracers <= 1e-6 after one step from the same state"
         ms_plain = timed(vp_plain, args.steps, args.warmup)
         forms["plain_fp64"] = {"cells_per_s": cells * args.steps * world / (ms_plain / 1e3),
@@ -355,7 +356,9 @@ def main():
         ms = timed(vp, args.steps, args.warmup)
     value = weak_scaling_value(cells, args.steps, world, ms)
     if mixed:
-        forms["mixed"] = {"cells_per_s": value, "ms_per_step": ms / args.steps}
+        forms["mixed"] = {"cells_per_s": value, "ms_per_step": ms / args.steps,
+                          "fp64_resolved_groups_last_step": vp.mixed_redo_count(),
+                          "groups_per_step": ((nx + 31) // 32) * ny * ntr}
         if "plain_fp64" in forms:
             forms["mixed_over_plain"] = round(value / forms["plain_fp64"]["cells_per_s"], 3)
 
@@ -452,7 +455,7 @@ def main():
             "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if mixed else "f64", "data": "synthetic",
             "config": config_out, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": (5 if mixed else 4) * args.steps, "clocks": clocks, "forms": forms,
+            "gpu_launches": (6 if mixed else 4) * args.steps, "clocks": clocks, "forms": forms,
             "mode": (f"FP64 state, FP32 assembly and Thomas sweeps with FP64 residual correction "
                      f"(mixed_precision={args.mixed_level})" if mixed
                      else "plain FP64, bit-identical to the CPU restatement")}

@@ -84,7 +84,8 @@ typedef struct vphys_config {
     int vmix_guard;           /* negative/NaN guard before the clip (0) */
     int kd_smooth_iterations; /* 1-2-1 smoothing passes (0) */
     int conv_enable;          /* convective adjustment contributor (0) */
-    int pad0;
+    int surface_flux;         /* 1: vphys_step deposits q_heat / q_salt into the top live layer of
+                                 T, S and pseudo-salt after the EOS (ocean_surface_flux_apply_tracers) */
     /* PP81 (rdb_ocean_vmix.F90:233-265) */
     double pp81_nu0;          /* 1e-2 */
     double pp81_nu_bg;        /* 1e-4 */
@@ -179,6 +180,8 @@ enum vphys_field {
     VPHYS_FIELD_K_BOT_U = 25,   /* in int32 (nx+1, ny), 1-based (default 1) */
     VPHYS_FIELD_K_BOT_V = 26,   /* in int32 (nx, ny+1) */
     VPHYS_FIELD_CORIOLIS = 27,  /* in      (nx, ny)  f, 1/s: read only by the learned KPP's features */
+    VPHYS_FIELD_HEAT_BUDGET_SURFACE = 28, /* in/out (nx, ny, nz) the surface deposit's heat contributor */
+    VPHYS_FIELD_SALT_BUDGET_SURFACE = 29, /* in/out (nx, ny, nz) */
     VPHYS_FIELD_TRACER0 = 64    /* in/out  (nx, ny, nz); tracer t is
                                    VPHYS_FIELD_TRACER0 + t */
 };
@@ -240,6 +243,23 @@ int vphys_eos_wright(vphys_handle h);
  * Replaces ocean_surfstress_derived_impl
  * (rdb_ocean_surface_stress.F90:858-875). */
 int vphys_stress_mag(vphys_handle h);
+
+/* The surface heat and salt fluxes deposited on the first live layer from
+ * the top: T += dt*Q_HEAT*WET/(rho0*cp)/(h+eps), S and pseudo-salt +=
+ * dt*Q_SALT*WET/rho0/(h+eps) (rdb_conc_add_source; a vanished layer takes
+ * nothing).  With budgets on, HEAT_BUDGET_SURFACE / SALT_BUDGET_SURFACE book
+ * the accepted content (pseudo-salt books none).  Replaces
+ * ocean_surface_flux_apply_tracers (rdb_ocean_surface_flux.F90:959-1070,
+ * apply_surface_src_2d_impl 1093-1142, the nobudget twin 1175-1203), called
+ * after the EOS at rdb_ocean_dyn.F90:1363; vphys_step runs it there when
+ * surface_flux is 1. */
+int vphys_surface_flux(vphys_handle h, double dt);
+
+/* Mixed-precision tracer solves (mixed_precision >= 1): the number of
+ * (32-column group, tracer) pairs whose one-step increment reached 2 units
+ * in the last solve and were re-solved on the FP64 path (bitwise the exact
+ * results).  Synchronises the handle's stream; 0 when nothing is mixed. */
+int vphys_mixed_redo_count(vphys_handle h, unsigned *groups);
 
 /* The whole coefficient build: interior closure (PP81 or background seed),
  * KPP overlay (+ bl_depth, b0, gamma_t/gamma_s), KV_ML_INVZ2, convection,

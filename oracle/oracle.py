@@ -26,7 +26,8 @@ class VpoState(ctypes.Structure):
         (n, _dp) for n in ("h", "rho", "u", "v", "kv", "kt", "ks", "kd_bg", "bl_depth", "b0", "stress_mag",
                           "q_heat", "q_salt", "wet", "tau_x", "tau_y", "lambda_bot_u", "lambda_bot_v",
                           "visc_rem_u", "visc_rem_v", "gamma_t", "gamma_s", "heat_budget", "salt_budget")
-    ] + [(n, _ip) for n in ("k_top_u", "k_top_v", "k_bot_u", "k_bot_v")] + [("tr", ctypes.POINTER(_dp))]
+    ] + [(n, _ip) for n in ("k_top_u", "k_top_v", "k_bot_u", "k_bot_v")] + [("tr", ctypes.POINTER(_dp))] + [
+        (n, _dp) for n in ("heat_budget_surface", "salt_budget_surface")]
 
 
 def build(force: bool = False) -> Path:
@@ -60,7 +61,7 @@ def lib():
         for name in ("vpo_assemble_gate", "vpo_build_coefficients"):
             getattr(L, name).argtypes = [ctypes.c_void_p, ctypes.POINTER(VpoState)]
             getattr(L, name).restype = ctypes.c_int
-        for name in ("vpo_vdiff_momentum", "vpo_vdiff_tracers", "vpo_nonlocal"):
+        for name in ("vpo_vdiff_momentum", "vpo_vdiff_tracers", "vpo_nonlocal", "vpo_surface_flux"):
             getattr(L, name).argtypes = [ctypes.c_void_p, ctypes.POINTER(VpoState), ctypes.c_double]
             getattr(L, name).restype = None
         L.vpo_step.argtypes = [ctypes.c_void_p, ctypes.POINTER(VpoState), ctypes.c_double, ctypes.c_int]
@@ -104,6 +105,8 @@ class OracleState:
         self.gamma_s = f(nx, ny, nz + 1)
         self.heat_budget = f(nx, ny, nz)
         self.salt_budget = f(nx, ny, nz)
+        self.heat_budget_surface = f(nx, ny, nz)
+        self.salt_budget_surface = f(nx, ny, nz)
         self.k_top_u = np.full((nx + 1, ny), nz, dtype=np.int32, order="F")
         self.k_top_v = np.full((nx, ny + 1), nz, dtype=np.int32, order="F")
         self.k_bot_u = np.ones((nx + 1, ny), dtype=np.int32, order="F")
@@ -121,20 +124,15 @@ class OracleState:
             a[:, :, -1] = 0.0
 
     def _struct(self) -> VpoState:
-        for name in ("h", "rho", "u", "v", "kv", "kt", "ks", "kd_bg", "bl_depth", "b0", "stress_mag", "q_heat",
-                     "q_salt", "wet", "tau_x", "tau_y", "lambda_bot_u", "lambda_bot_v", "visc_rem_u",
-                     "visc_rem_v", "gamma_t", "gamma_s", "heat_budget", "salt_budget", "k_top_u", "k_top_v",
-                     "k_bot_u", "k_bot_v"):
-            a = getattr(self, name)
-            assert a.flags.f_contiguous, name
         for t in self.tracers:
             assert t.flags.f_contiguous
         s = VpoState()
         s.nx, s.ny, s.nz, s.ntr = self.nx, self.ny, self.nz, self.ntr
-        for name, _ in VpoState._fields_[4:-5]:
-            setattr(s, name, getattr(self, name).ctypes.data_as(_dp))
-        for name in ("k_top_u", "k_top_v", "k_bot_u", "k_bot_v"):
-            setattr(s, name, getattr(self, name).ctypes.data_as(_ip))
+        for name, typ in VpoState._fields_[4:]:
+            if typ is _dp or typ is _ip:
+                a = getattr(self, name)
+                assert a.flags.f_contiguous, name
+                setattr(s, name, a.ctypes.data_as(typ))
         self._trp = (_dp * max(1, self.ntr))(*[t.ctypes.data_as(_dp) for t in self.tracers])
         s.tr = ctypes.cast(self._trp, ctypes.POINTER(_dp))
         return s

@@ -950,11 +950,52 @@ void vpo_vdiff_momentum(const vphys_config *c, vpo_state *s, double dt)
 }
 
 /* One vmix_apply_in_stage on a thermo step (rdb_ocean_dyn.F90:1636-1900). */
+/* ocean_surface_flux_apply_tracers (rdb_ocean_surface_flux.F90:959-1070):
+ * the surface heat and salt fluxes stamped onto the first live layer from the
+ * top (rdb_vl_first_live from k_top = nz) of T, S and the pseudo-salt mirror,
+ * apply_surface_src_2d_impl (1093-1142) with its budget contributor and the
+ * nobudget twin (1175-1203) for pseudo-salt; content -> concentration through
+ * rdb_conc_add_source, the budget books rdb_conc_accepted_source
+ * (rdb_tracer_conc.inc:33-63). */
+void vpo_surface_flux(const vphys_config *c, vpo_state *s, double dt)
+{
+    const int nx = s->nx, ny = s->ny, nz = s->nz;
+    const double inv_heat = dt / (c->rho0 * c->cp);
+    const double inv_salt = dt / c->rho0;
+    const int iT = c->idx_temperature, iS = c->idx_salinity, iPS = c->idx_pseudo_salt;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int j = 1; j <= ny; ++j) {
+        for (int i = 1; i <= nx; ++i) {
+            const int kt = first_live(s->h, nx, ny, i, j, nz);
+            const double hk = C3(s->h, i, j, kt);
+            const double w = C2(s->wet, i, j);
+            if (iT >= 0) {
+                const double cell = inv_heat * C2(s->q_heat, i, j) * w;
+                double *T = s->tr[iT];
+                C3(T, i, j, kt) = conc_add_source(C3(T, i, j, kt), hk, cell);
+                if (c->budgets) C3(s->heat_budget_surface, i, j, kt) += (hk > H_VANISHED) ? cell : 0.0;
+            }
+            if (iS >= 0) {
+                const double cell = inv_salt * C2(s->q_salt, i, j) * w;
+                double *S = s->tr[iS];
+                C3(S, i, j, kt) = conc_add_source(C3(S, i, j, kt), hk, cell);
+                if (c->budgets) C3(s->salt_budget_surface, i, j, kt) += (hk > H_VANISHED) ? cell : 0.0;
+            }
+            if (iPS >= 0) {
+                const double cell = inv_salt * C2(s->q_salt, i, j) * w;
+                double *PS = s->tr[iPS];
+                C3(PS, i, j, kt) = conc_add_source(C3(PS, i, j, kt), hk, cell);
+            }
+        }
+    }
+}
+
 int vpo_step(const vphys_config *c, vpo_state *s, double dt, int n_steps)
 {
     int st = 0;
     for (int n = 0; n < n_steps; ++n) {
         if (c->eos_in_step) vpo_eos_wright(c, s);
+        if (c->surface_flux) vpo_surface_flux(c, s, dt);
         st |= vpo_build_coefficients(c, s);
         vpo_vdiff_momentum(c, s, dt);
         vpo_vdiff_tracers(c, s, dt);

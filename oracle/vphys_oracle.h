@@ -38,6 +38,7 @@ typedef struct vpo_state {
     double *heat_budget, *salt_budget;
     int *k_top_u, *k_top_v, *k_bot_u, *k_bot_v;   /* 1-based */
     double **tr;                            /* ntr pointers */
+    double *heat_budget_surface, *salt_budget_surface;
 } vpo_state;
 
 void vpo_set_threads(int n);
@@ -61,6 +62,7 @@ int vpo_build_coefficients(const vphys_config *c, vpo_state *s);
 void vpo_vdiff_momentum(const vphys_config *c, vpo_state *s, double dt);
 void vpo_vdiff_tracers(const vphys_config *c, vpo_state *s, double dt);
 void vpo_nonlocal(const vphys_config *c, vpo_state *s, double dt);
+void vpo_surface_flux(const vphys_config *c, vpo_state *s, double dt);
 
 int vpo_step(const vphys_config *c, vpo_state *s, double dt, int n_steps);
 

@@ -63,6 +63,8 @@ FIELD_K_TOP_V = 24
 FIELD_K_BOT_U = 25
 FIELD_K_BOT_V = 26
 FIELD_CORIOLIS = 27
+FIELD_HEAT_BUDGET_SURFACE = 28
+FIELD_SALT_BUDGET_SURFACE = 29
 FIELD_TRACER0 = 64
 
 FIELD_NAMES = {
@@ -74,13 +76,15 @@ FIELD_NAMES = {
     "gamma_s": FIELD_GAMMA_S, "heat_budget": FIELD_HEAT_BUDGET, "salt_budget": FIELD_SALT_BUDGET,
     "k_top_u": FIELD_K_TOP_U, "k_top_v": FIELD_K_TOP_V, "k_bot_u": FIELD_K_BOT_U,
     "k_bot_v": FIELD_K_BOT_V, "coriolis": FIELD_CORIOLIS,
+    "heat_budget_surface": FIELD_HEAT_BUDGET_SURFACE, "salt_budget_surface": FIELD_SALT_BUDGET_SURFACE,
 }
 INT_FIELDS = (FIELD_K_TOP_U, FIELD_K_TOP_V, FIELD_K_BOT_U, FIELD_K_BOT_V)
 
 
 def field_shape(field: int, nx: int, ny: int, nz: int):
     """Fortran-order shape of a field (matches vphys_field_shape in C)."""
-    if field >= FIELD_TRACER0 or field in (FIELD_H, FIELD_RHO, FIELD_HEAT_BUDGET, FIELD_SALT_BUDGET):
+    if field >= FIELD_TRACER0 or field in (FIELD_H, FIELD_RHO, FIELD_HEAT_BUDGET, FIELD_SALT_BUDGET,
+                                           FIELD_HEAT_BUDGET_SURFACE, FIELD_SALT_BUDGET_SURFACE):
         return (nx, ny, nz)
     if field in (FIELD_U, FIELD_VISC_REM_U):
         return (nx + 1, ny, nz)
@@ -102,7 +106,7 @@ class VphysConfig(ctypes.Structure):
     _fields_ = [
         ("use_closure", ctypes.c_int), ("interior_closure", ctypes.c_int), ("use_kpp", ctypes.c_int),
         ("bkgnd_profile", ctypes.c_int), ("vmix_guard", ctypes.c_int), ("kd_smooth_iterations", ctypes.c_int),
-        ("conv_enable", ctypes.c_int), ("pad0", ctypes.c_int),
+        ("conv_enable", ctypes.c_int), ("surface_flux", ctypes.c_int),
         ("pp81_nu0", ctypes.c_double), ("pp81_nu_bg", ctypes.c_double), ("pp81_kappa_bg", ctypes.c_double),
         ("pp81_alpha", ctypes.c_double), ("rho0", ctypes.c_double), ("shear2_floor", ctypes.c_double),
         ("ri_crit", ctypes.c_double), ("cs_nonlocal", ctypes.c_double), ("c_vt2", ctypes.c_double),
@@ -124,7 +128,7 @@ class VphysConfig(ctypes.Structure):
     ]
 
     def as_dict(self):
-        return {n: getattr(self, n) for n, _ in self._fields_ if n not in ("pad0",)}
+        return {n: getattr(self, n) for n, _ in self._fields_ if n not in ()}
 
 
 class LibraryNotFoundError(FileNotFoundError):
@@ -183,6 +187,8 @@ _PROTOTYPES = {
                                      ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     "vphys_eos_wright": (ctypes.c_int, [ctypes.c_void_p]),
     "vphys_stress_mag": (ctypes.c_int, [ctypes.c_void_p]),
+    "vphys_surface_flux": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    "vphys_mixed_redo_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint)]),
     "vphys_assemble": (ctypes.c_int, [ctypes.c_void_p]),
     "vphys_vdiff_momentum": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "vphys_vdiff_tracers": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),

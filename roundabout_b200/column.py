@@ -148,6 +148,10 @@ class VerticalPhysics:
     def stress_mag(self):
         _ffi.check(self.lib.vphys_stress_mag(self._h), "vphys_stress_mag")
 
+    def surface_flux(self, dt):
+        """ocean_surface_flux_apply_tracers (rdb_ocean_surface_flux.F90:959-1070)."""
+        _ffi.check(self.lib.vphys_surface_flux(self._h, float(dt)), "vphys_surface_flux")
+
     def assemble(self):
         return _ffi.check(self.lib.vphys_assemble(self._h), "vphys_assemble")
 
@@ -170,6 +174,12 @@ class VerticalPhysics:
     def step_graph(self, dt, n_steps=1):
         """vphys_step_graph: the n steps captured once as a CUDA graph and replayed."""
         _ffi.check(self.lib.vphys_step_graph(self._h, float(dt), int(n_steps)), "vphys_step_graph")
+
+    def mixed_redo_count(self):
+        """(32-column group, tracer) pairs of the last mixed tracer solve re-solved in FP64."""
+        n = ctypes.c_uint(0)
+        _ffi.check(self.lib.vphys_mixed_redo_count(self._h, ctypes.byref(n)), "vphys_mixed_redo_count")
+        return int(n.value)
 
     def step_status(self, dt, n_steps=1):
         return self.lib.vphys_step(self._h, float(dt), int(n_steps))

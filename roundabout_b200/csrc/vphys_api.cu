@@ -49,7 +49,7 @@ int cuda_status(cudaError_t e, const char *where)
     return push_error(VPHYS_ERR_CUDA, "%s: CUDA error %d (%s)", where, (int)e, cudaGetErrorString(e));
 }
 
-constexpr int NFIXED = 28;
+constexpr int NFIXED = 30;
 constexpr unsigned MAGIC = 0x56504859u;   // "VPHY"
 
 struct Field {
@@ -74,6 +74,7 @@ struct vphys_handle_s {
     double *smooth_scratch = nullptr;
     double *budget_scratch = nullptr;
     int *span = nullptr;              // live spans of the columns (mixed-precision tracer solve)
+    unsigned *mp_redo = nullptr;      // the mixed tracer solve's FP64 re-solve list (count + entries)
     double *zcol = nullptr;           // column depths for the momentum face thickness
     // learned KPP surrogate (vphys_kpp_attach): the caller's weights and the scratch of one inference
     vphys_kpp_model kpp{};
@@ -110,7 +111,9 @@ size_t field_count(int nx, int ny, int nz, int field, bool *is_int)
     case VPHYS_FIELD_H:
     case VPHYS_FIELD_RHO:
     case VPHYS_FIELD_HEAT_BUDGET:
-    case VPHYS_FIELD_SALT_BUDGET: return X * Y * Z;
+    case VPHYS_FIELD_SALT_BUDGET:
+    case VPHYS_FIELD_HEAT_BUDGET_SURFACE:
+    case VPHYS_FIELD_SALT_BUDGET_SURFACE: return X * Y * Z;
     case VPHYS_FIELD_U:
     case VPHYS_FIELD_VISC_REM_U: return (X + 1) * Y * Z;
     case VPHYS_FIELD_V:
@@ -223,6 +226,7 @@ int validate(const vphys_config *c, int ntr)
     if (c->mixed_precision < 0 || c->mixed_precision > 2)
         return push_error(VPHYS_ERR_CONFIG, "mixed_precision %d: 0 (FP64), 1 (mixed solves) or 2 (mixed solves and assembly)",
                           c->mixed_precision);
+    if (c->surface_flux < 0 || c->surface_flux > 1) return push_error(VPHYS_ERR_CONFIG, "surface_flux must be 0 or 1");
     if (c->rho0 <= 0.0 || c->cp <= 0.0) return push_error(VPHYS_ERR_CONFIG, "rho0 and cp must be positive");
     if (c->use_kpp && c->ri_crit <= 0.0) return push_error(VPHYS_ERR_CONFIG, "ri_crit must be positive");
     if (c->bkgnd_profile && c->bkgnd_delta == 0.0) return push_error(VPHYS_ERR_CONFIG, "bkgnd_delta must be nonzero");
@@ -267,6 +271,8 @@ Params make_params(vphys_handle h)
     p.gamma_s = D(VPHYS_FIELD_GAMMA_S);
     p.heat_budget = D(VPHYS_FIELD_HEAT_BUDGET);
     p.salt_budget = D(VPHYS_FIELD_SALT_BUDGET);
+    p.heat_budget_surface = D(VPHYS_FIELD_HEAT_BUDGET_SURFACE);
+    p.salt_budget_surface = D(VPHYS_FIELD_SALT_BUDGET_SURFACE);
     p.k_top_u = I(VPHYS_FIELD_K_TOP_U);
     p.k_top_v = I(VPHYS_FIELD_K_TOP_V);
     p.k_bot_u = I(VPHYS_FIELD_K_BOT_U);
@@ -275,6 +281,7 @@ Params make_params(vphys_handle h)
     p.guard_count = h->guard_dev;
     p.budget_scratch = h->budget_scratch;
     p.span = h->span;
+    p.mp_redo = h->mp_redo;
     p.zcol = h->zcol;
     p.coriolis = D(VPHYS_FIELD_CORIOLIS);
     p.ks_equals_kt = (h->cfg.bkgnd_profile || h->cfg.kt_bg == h->cfg.ks_bg) ? 1 : 0;
@@ -316,6 +323,17 @@ int prepare_tracers(vphys_handle h)
             return push_error(VPHYS_ERR_ALLOC, "cudaMalloc of the column spans failed");
         }
     }
+    if (h->cfg.mixed_precision && !h->mp_redo) {
+        const size_t n = 1 + (size_t)((h->nx + 31) / 32) * h->ny * (size_t)(h->ntr > 0 ? h->ntr : 1);
+        cudaError_t e = cudaMalloc(&h->mp_redo, n * sizeof(unsigned));
+        if (e == cudaSuccess) e = cudaMemsetAsync(h->mp_redo, 0, sizeof(unsigned), h->stream);
+        if (e != cudaSuccess) {
+            if (h->mp_redo) cudaFree(h->mp_redo);
+            h->mp_redo = nullptr;
+            cudaGetLastError();
+            return push_error(VPHYS_ERR_ALLOC, "cudaMalloc of the mixed-solve re-solve list failed");
+        }
+    }
     if (h->cfg.budgets) {
         if ((st = ensure(h, VPHYS_FIELD_HEAT_BUDGET))) return st;
         if ((st = ensure(h, VPHYS_FIELD_SALT_BUDGET))) return st;
@@ -330,6 +348,24 @@ int prepare_tracers(vphys_handle h)
         }
     }
     return st;
+}
+
+int prepare_surface_flux(vphys_handle h)
+{
+    int st = VPHYS_OK;
+    if (h->cfg.budgets) {
+        if ((st = ensure(h, VPHYS_FIELD_HEAT_BUDGET_SURFACE))) return st;
+        if ((st = ensure(h, VPHYS_FIELD_SALT_BUDGET_SURFACE))) return st;
+    }
+    return st;
+}
+
+// dt/(rho0 cp) and dt/rho0, the deposit's column-invariant multipliers
+// (rdb_ocean_surface_flux.F90:1048-1064), divided on the host in IEEE double
+void surface_flux_scales(const vphys_config &c, double dt, double *inv_heat, double *inv_salt)
+{
+    *inv_heat = dt / (c.rho0 * c.cp);
+    *inv_salt = dt / c.rho0;
 }
 
 int prepare_assemble(vphys_handle h)
@@ -395,13 +431,17 @@ void free_kpp(vphys_handle h)
 int run_assemble(vphys_handle h, const Params &p);
 
 // The launches of n whole steps (vmix_apply_in_stage on a thermo step,
-// rdb_ocean_dyn.F90:1636-1900): EOS, [learned KPP], assembly, momentum,
-// tracers with the non-local tendency.  All asynchronous on h->stream.
+// rdb_ocean_dyn.F90:1636-1900): EOS, [surface deposit], [learned KPP],
+// assembly, momentum, tracers with the non-local tendency.  All asynchronous
+// on h->stream.
 int launch_steps(vphys_handle h, const Params &p, double dt, int n_steps)
 {
     int st;
+    double inv_heat, inv_salt;
+    surface_flux_scales(h->cfg, dt, &inv_heat, &inv_salt);
     for (int n = 0; n < n_steps; ++n) {
         if (h->cfg.eos_in_step) vphys::launch_eos_wright(p, h->stream);
+        if (h->cfg.surface_flux) vphys::launch_surface_flux(p, inv_heat, inv_salt, h->stream);
         Params pa = p;
         if ((st = run_learned_kpp(h, pa))) return st;
         if ((st = run_assemble(h, pa))) return st;
@@ -593,6 +633,7 @@ int vphys_destroy(vphys_handle *hp)
     if (h->smooth_scratch) cudaFree(h->smooth_scratch);
     if (h->budget_scratch) cudaFree(h->budget_scratch);
     if (h->span) cudaFree(h->span);
+    if (h->mp_redo) cudaFree(h->mp_redo);
     if (h->zcol) cudaFree(h->zcol);
     free_kpp(h);
     if (h->gexec) cudaGraphExecDestroy(h->gexec);
@@ -709,6 +750,29 @@ int vphys_eos_wright(vphys_handle h)
     return cuda_status(cudaGetLastError(), "vphys_eos_wright launch");
 }
 
+int vphys_surface_flux(vphys_handle h, double dt)
+{
+    if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_surface_flux: bad handle");
+    int st = prepare_surface_flux(h);
+    if (st) return st;
+    double inv_heat, inv_salt;
+    surface_flux_scales(h->cfg, dt, &inv_heat, &inv_salt);
+    Params p = make_params(h);
+    vphys::launch_surface_flux(p, inv_heat, inv_salt, h->stream);
+    return cuda_status(cudaGetLastError(), "vphys_surface_flux launch");
+}
+
+int vphys_mixed_redo_count(vphys_handle h, unsigned *groups)
+{
+    if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_mixed_redo_count: bad handle");
+    if (!groups) return VPHYS_OK;
+    *groups = 0;
+    if (!h->mp_redo) return VPHYS_OK;
+    cudaError_t e = cudaMemcpyAsync(groups, h->mp_redo, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    return cuda_status(e, "vphys_mixed_redo_count");
+}
+
 int vphys_stress_mag(vphys_handle h)
 {
     if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_stress_mag: bad handle");
@@ -772,7 +836,9 @@ int vphys_step(vphys_handle h, double dt, int n_steps)
     if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_step: bad handle");
     if (n_steps <= 0) return VPHYS_OK;
     int st;
-    if ((st = prepare_assemble(h)) || (st = prepare_momentum(h)) || (st = prepare_tracers(h))) return st;
+    if ((st = prepare_assemble(h)) || (st = prepare_momentum(h)) || (st = prepare_tracers(h)) ||
+        (h->cfg.surface_flux && (st = prepare_surface_flux(h))))
+        return st;
     if (h->cfg.eos_in_step && (h->cfg.idx_temperature < 0 || h->cfg.idx_salinity < 0))
         return push_error(VPHYS_ERR_CONFIG, "vphys_step: eos_in_step needs temperature and salinity tracers");
     if (h->cfg.vmix_guard) {
@@ -795,7 +861,9 @@ int vphys_step_graph(vphys_handle h, double dt, int n_steps)
     if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_step_graph: bad handle");
     if (n_steps <= 0) return VPHYS_OK;
     int st;
-    if ((st = prepare_assemble(h)) || (st = prepare_momentum(h)) || (st = prepare_tracers(h))) return st;
+    if ((st = prepare_assemble(h)) || (st = prepare_momentum(h)) || (st = prepare_tracers(h)) ||
+        (h->cfg.surface_flux && (st = prepare_surface_flux(h))))
+        return st;
     if (h->cfg.eos_in_step && (h->cfg.idx_temperature < 0 || h->cfg.idx_salinity < 0))
         return push_error(VPHYS_ERR_CONFIG, "vphys_step_graph: eos_in_step needs temperature and salinity tracers");
     if (h->cfg.vmix_guard) {

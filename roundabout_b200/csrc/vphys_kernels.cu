@@ -9,6 +9,7 @@
 //
 // Kernels (one launch each, all asynchronous):
 //   k_eos_wright   rho from (T, S)                     rdb_eos.F90:909-959
+//   k_surface_flux surface heat/salt deposit           rdb_ocean_surface_flux.F90:959-1230
 //   k_stress_mag   |tau| at cell centres               rdb_ocean_surface_stress.F90:858-875
 //   k_assemble     PP81 / seed, KPP passes 1 + 2, KV_ML_INVZ2, convection,
 //                  split, guard, Bryan-Lewis or scalar gate: every interface
@@ -54,6 +55,48 @@ __global__ void __launch_bounds__(256) k_eos_wright(const Params p)
             r = rho0;
         }
         p.rho[idx] = r;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Surface heat / salt deposit (ocean_surface_flux_apply_tracers,
+// rdb_ocean_surface_flux.F90:959-1070 with apply_surface_src_2d_impl
+// 1093-1142 and its nobudget twin for pseudo-salt 1175-1203): the content
+// inv * Q(i,j) * wet(i,j) enters the first live layer from the top through
+// rdb_conc_add_source; the budget books rdb_conc_accepted_source.  One thread
+// per column; the walk reads one plane per vanished top layer.
+// ---------------------------------------------------------------------------
+__global__ void k_surface_flux(const Params p, double inv_heat, double inv_salt)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (i >= p.nx) return;
+    const size_t col = (size_t)i + (size_t)p.nx * j;
+    const size_t P = p.plane;
+    int kt = p.nz;
+    for (int k = p.nz; k >= 1; --k) {
+        if (__ldg(p.h + col + P * (size_t)(k - 1)) > H_VANISHED) {
+            kt = k;
+            break;
+        }
+    }
+    const size_t idx = col + P * (size_t)(kt - 1);
+    const double hk = __ldg(p.h + idx);
+    const double w = __ldg(p.wet + col);
+    const int iT = p.cfg.idx_temperature, iS = p.cfg.idx_salinity, iPS = p.cfg.idx_pseudo_salt;
+    const bool book = p.cfg.budgets && hk > H_VANISHED;
+    if (iT >= 0) {
+        const double cell = inv_heat * __ldg(p.q_heat + col) * w;
+        p.tr[iT][idx] = conc_add_source(p.tr[iT][idx], hk, cell);
+        if (p.cfg.budgets) p.heat_budget_surface[idx] += book ? cell : 0.0;
+    }
+    if (iS >= 0 || iPS >= 0) {
+        const double cell = inv_salt * __ldg(p.q_salt + col) * w;
+        if (iS >= 0) {
+            p.tr[iS][idx] = conc_add_source(p.tr[iS][idx], hk, cell);
+            if (p.cfg.budgets) p.salt_budget_surface[idx] += book ? cell : 0.0;
+        }
+        if (iPS >= 0) p.tr[iPS][idx] = conc_add_source(p.tr[iPS][idx], hk, cell);
     }
 }
 
@@ -690,6 +733,12 @@ static int grid_1d(size_t n, int threads)
 void launch_eos_wright(const Params &p, cudaStream_t stream)
 {
     k_eos_wright<<<grid_1d(p.plane * (size_t)p.nz, 256), 256, 0, stream>>>(p);
+}
+
+void launch_surface_flux(const Params &p, double inv_heat, double inv_salt, cudaStream_t stream)
+{
+    dim3 grid((p.nx + 127) / 128, p.ny);
+    k_surface_flux<<<grid, 128, 0, stream>>>(p, inv_heat, inv_salt);
 }
 
 void launch_stress_mag(const Params &p, cudaStream_t stream)

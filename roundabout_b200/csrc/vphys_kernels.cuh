@@ -37,11 +37,13 @@ struct Params {
     double *visc_rem_u, *visc_rem_v;
     double *gamma_t, *gamma_s;       // nullptr: not written
     double *heat_budget, *salt_budget;
+    double *heat_budget_surface, *salt_budget_surface;   // surface-flux deposit books (budgets on)
     double *budget_scratch;          // 2 planes x nz: forward-swept T and S when budgets are on
     const int *k_top_u, *k_top_v, *k_bot_u, *k_bot_v;   // nullptr: nz / 1
     double *tr[NTR_MAX];
     unsigned long long *guard_count;  // vmix_guard counter (device)
     int *span;                        // per column: first | last live layer << 16 (0: none), scratch
+    unsigned *mp_redo;                // mixed solves: count, then (group << 5 | tracer) re-solved in FP64
     double *zcol;                     // per column: -sum_k h, k = 1..nz in order (momentum z_clear), scratch
     const double *coriolis;           // (nx, ny) f, or nullptr (learned KPP features only)
     const float *kpp_pred;            // per column: the surrogate's h_b, < 0: run pass 1; nullptr: plain KPP
@@ -57,6 +59,8 @@ int report_error(int status, const char *msg);
 
 // Launchers (vphys_kernels.cu); all asynchronous on `stream`.
 void launch_eos_wright(const Params &p, cudaStream_t stream);
+// surface heat/salt deposit on the first live layer; inv_heat = dt/(rho0 cp), inv_salt = dt/rho0
+void launch_surface_flux(const Params &p, double inv_heat, double inv_salt, cudaStream_t stream);
 void launch_stress_mag(const Params &p, cudaStream_t stream);
 void launch_assemble(const Params &p, cudaStream_t stream);
 void launch_smooth(const Params &p, double *fld, double *scratch, cudaStream_t stream);
@@ -67,6 +71,8 @@ void launch_tracers(const Params &p, double dt, bool diffuse, bool nonlocal, cud
 // mixed-precision solves (vphys_mixed.cu), dispatched by the two above when cfg.mixed_precision
 void launch_momentum_mp(const Params &p, double dt, cudaStream_t stream);
 void launch_tracers_mp(const Params &p, double dt, bool nonlocal, cudaStream_t stream);
+// the FP64 re-solve of the groups the mixed tracer kernel listed in p.mp_redo (vphys_tracers.cu)
+void launch_tracers_redo(const Params &p, double dt, bool nonlocal, cudaStream_t stream);
 // learned KPP (vphys_learned.cu)
 void launch_kpp_features(const Params &p, float *raw, void *X, void *XT, long long ld_t, const float *mean,
                          const float *istd, float limit, unsigned char *gate, float *colH, cudaStream_t s);

@@ -59,6 +59,12 @@ constexpr int MP_TR_U = VPHYS_MP_TR_U;                // levels per tracer load 
 constexpr int MP_TR_UF = 4;   // levels per load block of the back-substitution with the non-local deposit
 constexpr int MP_MOM_THREADS = VPHYS_MP_MOM_THREADS;  // face columns per momentum block
 constexpr int MP_MOM_U = VPHYS_MP_MOM_U;              // levels per momentum load block
+// Largest tracer increment (in the tracer's units) a mixed solve keeps.  The
+// FP32 couplings and the FP32 back-substitution leave an error of about
+// 3 eps_32 |delta| (eps_32 = 6e-8): 2 units keep it under 4e-7.  A column
+// group with a larger increment in one step -- a 1 mm top layer taking a
+// surface heat flux warms by tens of kelvin -- is re-solved in FP64.
+constexpr float MP_DELTA_MAX = 2.0f;
 
 // Hardware reciprocal (MUFU, within 1 ulp): the FP32 factors carry no
 // bitwise contract, and their rounding is a consistent perturbation of the
@@ -118,6 +124,7 @@ __global__ void k_spans(const Params p)
         }
     }
     p.span[col] = lo | (hi << 16);
+    if (p.mp_redo && col == 0) p.mp_redo[0] = 0;   // the re-solve list of the tracer kernel that follows
 }
 
 // Back-substitution of one tracer column from the t and v rows; with FULL the
@@ -245,6 +252,7 @@ __global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, doubl
     const unsigned long long pol_keep = l2_policy_evict_last();
     const float dtf = (float)dt;
 
+    float vsum = 0.0f;   // sum of |v| over rows and tracers: a bound on every |delta| below
     // ---- upward: factorisation (FP32, once for the group) + FP64 residual and
     //      accumulation of every tracer.  Branch-free rows: outside [lo, hi]
     //      nothing is loaded, h = 0 gates both couplings off and the row
@@ -290,7 +298,9 @@ __global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, doubl
                 for (int q = 0; q < TPW; ++q) {
                     const double b = fd * (d_m[q] - d_c[q]) + fu * (dn[u][q] - d_c[q]);
                     w[q] = b + mul_u(t_prev, w[q]);
-                    vv[(size_t)q * NB + s] = (float)(w[q] * ipd);
+                    const float vq = (float)(w[q] * ipd);
+                    vv[(size_t)q * NB + s] = vq;
+                    vsum += fabsf(vq);
                     d_m[q] = d_c[q];
                     d_c[q] = dn[u][q];
                 }
@@ -300,6 +310,30 @@ __global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, doubl
                 f_dn = f_up;
                 h_c = hn[u];
             }
+        }
+    }
+
+    // ---- a group whose increment reaches MP_DELTA_MAX goes to the FP64 re-solve ----
+    // delta_k = v_k + u_k delta_{k+1} with 0 <= u_k <= 1, so max |delta| <= sum |v|;
+    // only when that bound is exceeded does the warp run the exact recurrence
+    // (shared memory only) for max |delta|.  A listed group writes nothing.
+    if (p.mp_redo && __any_sync(0xffffffffu, vsum > MP_DELTA_MAX)) {
+        float dmax = 0.0f;
+        for (int q = 0; q < nt; ++q) {
+            const float *vq = vv + (size_t)q * NB;
+            float delta = 0.0f;
+            for (int k = w_hi; k >= w_lo; --k) {
+                const size_t s = (size_t)(k - 1) * MP_TR_COLS;
+                delta = vq[s] + mul_u(tu[s], delta);
+                dmax = fmaxf(dmax, fabsf(delta));
+            }
+        }
+        if (__any_sync(0xffffffffu, dmax > MP_DELTA_MAX)) {
+            if (lane == 0) {
+                const unsigned base = atomicAdd(p.mp_redo, (unsigned)nt);
+                for (int q = 0; q < nt; ++q) p.mp_redo[1 + base + q] = (g << 5) | (unsigned)tix[q];
+            }
+            return;
         }
     }
 
@@ -593,6 +627,7 @@ static void launch_tracers_mp_t(const Params &p, double dt, bool nonlocal, cudaS
     const int ngx = (p.nx + MP_TR_COLS - 1) / MP_TR_COLS;
     const unsigned blocks = (unsigned)ngx * (unsigned)p.ny * (unsigned)tg.ngroups;
     k_tracers_mp<TWO, TPW><<<blocks, MP_TR_COLS, smem, stream>>>(p, dt, nonlocal ? 1 : 0, ngx, tg);
+    if (p.mp_redo) launch_tracers_redo(p, dt, nonlocal, stream);
 }
 
 // Tracers per warp: VPHYS_MP_TRACERS_PER_WARP (1, 2 or 4) when set, else 1

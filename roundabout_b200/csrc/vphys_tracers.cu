@@ -74,13 +74,13 @@ __device__ __forceinline__ void tracer_row(int k, int nz, bool use_harmonic, dou
     }
 }
 
+// The columns of one warp: column (i, j) on this lane, `tid` its slot in the
+// block's shared memory of `bs` columns.
 template <int NTR, bool TWO>
-__global__ void __launch_bounds__(128) k_tracers(const Params p, double dt, int diffuse, int nonlocal)
+__device__ __forceinline__ void tracer_columns(const Params &p, double dt, int diffuse, int nonlocal, int i, int j,
+                                               double *smem, int tid, int bs)
 {
     constexpr int TR_U = NTR <= 4 ? 4 : (NTR <= 8 ? 2 : 1);   // levels per load block
-    extern __shared__ double smem[];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y;
     const vphys_config &c = p.cfg;
     const int nx = p.nx, nz = p.nz, ntr = p.ntr;
     const size_t P = p.plane;
@@ -88,9 +88,8 @@ __global__ void __launch_bounds__(128) k_tracers(const Params p, double dt, int 
     const size_t col = (size_t)(in_grid ? i : 0) + (size_t)nx * j;
     const double *__restrict__ hp = p.h + col;
     const int iT = c.idx_temperature, iS = c.idx_salinity, iPS = c.idx_pseudo_salt;
-    const int bs = blockDim.x;
-    double *cpA = smem + threadIdx.x;                       // cpA[(k-1)*bs]
-    double *cpB = smem + (size_t)nz * bs + threadIdx.x;     // only when TWO
+    double *cpA = smem + tid;                       // cpA[(k-1)*bs]
+    double *cpB = smem + (size_t)nz * bs + tid;     // only when TWO
     const unsigned long long pol_keep = l2_policy_evict_last();
     const unsigned long long pol_once = l2_policy_evict_first();
 #define HH(k) __ldg(hp + P * (size_t)((k) - 1))
@@ -314,6 +313,55 @@ __global__ void __launch_bounds__(128) k_tracers(const Params p, double dt, int 
         }
     }
 #undef HH
+}
+
+template <int NTR, bool TWO>
+__global__ void __launch_bounds__(128) k_tracers(const Params p, double dt, int diffuse, int nonlocal)
+{
+    extern __shared__ double smem[];
+    tracer_columns<NTR, TWO>(p, dt, diffuse, nonlocal, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y, smem,
+                             threadIdx.x, blockDim.x);
+}
+
+// The FP64 re-solve of the (32-column group, tracer) pairs that the
+// mixed-precision kernel listed (mp_redo[0] entries after the count, each
+// group << 5 | tracer) and left untouched: each runs the exact path above as
+// a one-tracer problem -- the tracer's roles (T, S, pseudo-salt) and its
+// diffusivity carried over -- so those columns come out bitwise as on the
+// FP64 path.  One warp per entry, the grid strides over the list.
+__global__ void __launch_bounds__(32) k_tracers_redo(const Params p, double dt, int nonlocal, int ngx)
+{
+    extern __shared__ double smem[];
+    const unsigned n = *(volatile const unsigned *)p.mp_redo;
+    for (unsigned e = blockIdx.x; e < n; e += gridDim.x) {
+        const unsigned ent = p.mp_redo[1 + e];
+        const int tix = (int)(ent & 31u);
+        const unsigned g = ent >> 5;
+        const int gi = (int)(g % (unsigned)ngx), j = (int)(g / (unsigned)ngx);
+        Params q = p;
+        const vphys_config &c = p.cfg;
+        q.ntr = 1;
+        q.tr[0] = p.tr[tix];
+        q.cfg.idx_temperature = (tix == c.idx_temperature) ? 0 : -1;
+        q.cfg.idx_salinity = (tix == c.idx_salinity) ? 0 : -1;
+        q.cfg.idx_pseudo_salt = (tix == c.idx_pseudo_salt) ? 0 : -1;
+        if (!p.ks_equals_kt && tix != c.idx_temperature) q.kt = p.ks;   // the second factorisation's tracers
+        tracer_columns<1, false>(q, dt, 1, nonlocal, gi * 32 + (int)threadIdx.x, j, smem, threadIdx.x, 32);
+        __syncwarp();
+    }
+}
+
+void launch_tracers_redo(const Params &p, double dt, bool nonlocal, cudaStream_t stream)
+{
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_tracers_redo, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)((size_t)VPHYS_NZ_MAX * 32 * sizeof(double)));
+        attr_set = true;
+    }
+    const int ngx = (p.nx + 31) / 32;
+    const size_t smem = (size_t)p.nz * 32 * sizeof(double);
+    k_tracers_redo<<<148 * 8, 32, smem, stream>>>(p, dt, nonlocal ? 1 : 0, ngx);
 }
 
 template <int NTR, bool TWO>

@@ -126,6 +126,61 @@ def test_momentum_options_mixed(VP, oracle, over):
         assert maxabs(vp.get("visc_rem_v"), st.visc_rem_v) <= 1e-5
 
 
+@pytest.mark.parametrize("case", ["ks_eq_kt", "ks_ne_kt", "budgets"])
+def test_large_increment_resolved_in_fp64(VP, oracle, case):
+    """A column group whose one-step increment reaches 2 units (here a 15 K
+    cold anomaly in the top layer, mixed down by convection) is re-solved on
+    the FP64 path: those groups come out bitwise, every tracer within 1e-6."""
+    ntr = 4
+    cols = columns(nx=72, ny=12, nz=30, seed=37, ntr=ntr, thin_frac=0.15, passive_init="uniform")
+    cols.tracers[1][:8, :, -1] -= 15.0
+    cfg = hot_cfg(ntr=ntr, **TRACER_CASES[case])
+    st = oracle_state(oracle, cols, cfg)
+    vp = VP(cols.nx, cols.ny, cols.nz, ntr, cfg)
+    vp.load_columns(cols)
+    st.call("vpo_eos_wright", cfg)
+    st.call("vpo_build_coefficients", cfg)
+    vp.eos()
+    vp.assemble()
+    vp.set_config(hot_cfg(ntr=ntr, mixed_precision=1, **TRACER_CASES[case]))
+    T0 = st.tracers[1].copy()
+    st.call("vpo_vdiff_tracers", cfg, DT)
+    dT = np.abs(st.tracers[1] - T0)
+    st.call("vpo_nonlocal", cfg, DT)
+    vp.vdiff_tracers(DT)
+    assert vp.mixed_redo_count() > 0
+    vp.nonlocal_tendencies(DT)
+    errs = [maxabs(vp.get_tracer(t), st.tracers[t]) for t in range(ntr)]
+    assert max(errs) <= TOL_TS, errs
+    T = np.asarray(vp.get_tracer(1))
+    group_max = dT[:32].max(axis=(0, 2))          # columns 0..31 of each row j: one group
+    sure = np.flatnonzero(group_max > 2.2)
+    assert sure.size > 0
+    for j in sure:
+        assert_bitwise(f"T, re-solved group j={j}", T[:32, j], st.tracers[1][:32, j])
+    if cfg.budgets:
+        want = st.heat_budget
+        assert maxabs(vp.get("heat_budget"), want) <= 1e-6 * max(1.0, float(np.abs(want).max()))
+
+
+def test_resolve_is_rare_once_mixed(VP, oracle):
+    """The first step from the stratified synthetic state homogenises mixed
+    layers spanning a few kelvin (|delta| ~ 2 K): a few groups go to FP64.
+    Once mixed, the increments stay small and (almost) nothing is re-solved."""
+    ntr = 4
+    cols = columns(nx=96, ny=32, nz=40, seed=38, ntr=ntr, thin_frac=0.15)
+    vp = VP(cols.nx, cols.ny, cols.nz, ntr, hot_cfg(ntr=ntr, mixed_precision=1))
+    vp.load_columns(cols)
+    groups = 3 * 32 * ntr
+    counts = []
+    for _ in range(6):
+        vp.step(DT, 1)
+        counts.append(vp.mixed_redo_count())
+    print("re-solved groups per step:", counts, "of", groups)
+    assert counts[0] <= 0.1 * groups
+    assert counts[-1] <= 0.02 * groups
+
+
 @pytest.mark.parametrize("level,tol", [(1, TOL_TS), (2, 2e-5)])
 def test_mixed_one_step(VP, oracle, level, tol):
     """One whole step (EOS, assembly, momentum, tracers, non-local) from the

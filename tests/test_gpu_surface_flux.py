@@ -1,0 +1,119 @@
+"""Parity of the surface heat/salt deposit (vphys_surface_flux, and inside
+vphys_step with surface_flux = 1) with the CPU oracle.
+
+The deposit is ocean_surface_flux_apply_tracers (rdb_ocean_surface_flux.F90:
+959-1070): bitwise on the FP64 path, standalone and in a whole step; the
+mixed-precision step keeps its 1e-6 per-step bar with the deposit on.
+"""
+import numpy as np
+import pytest
+
+from tests._cases import assert_bitwise, columns, hot_cfg, oracle_state
+
+pytestmark = pytest.mark.gpu
+
+DT = 3600.0
+
+
+@pytest.fixture(scope="module")
+def VP():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from roundabout_b200.column import VerticalPhysics
+
+    return VerticalPhysics
+
+
+def loaded(VP, cols, cfg):
+    vp = VP(cols.nx, cols.ny, cols.nz, len(cols.tracers), cfg)
+    vp.load_columns(cols)
+    return vp
+
+
+@pytest.mark.parametrize("shape", [(24, 20, 12), (7, 5, 1), (130, 9, 20)])
+@pytest.mark.parametrize("budgets", [0, 1])
+def test_surface_flux_standalone(VP, oracle, shape, budgets):
+    nx, ny, nz = shape
+    cols = columns(nx=nx, ny=ny, nz=nz, seed=nx + 3 * nz, thin_frac=0.2)
+    cols.h[: nx // 3, :, -1] = 1.0e-4          # vanished top filler on part of the domain
+    if nz > 2:
+        cols.h[: nx // 5, :, -2] = 0.0          # and a second one on some of it
+    cfg = hot_cfg(budgets=budgets, surface_flux=1)
+    st = oracle_state(oracle, cols, cfg)
+    vp = loaded(VP, cols, cfg)
+    for _ in range(3):
+        st.call("vpo_surface_flux", cfg, DT)
+        vp.surface_flux(DT)
+    for t in range(st.ntr):
+        assert_bitwise(f"tracer{t}", vp.get_tracer(t), st.tracers[t])
+    if budgets:
+        assert_bitwise("heat_budget_surface", vp.get("heat_budget_surface"), st.heat_budget_surface)
+        assert_bitwise("salt_budget_surface", vp.get("salt_budget_surface"), st.salt_budget_surface)
+        assert np.abs(st.heat_budget_surface).max() > 0.0
+
+
+def test_surface_flux_content_equals_budget(VP, oracle):
+    """The column heat content gained is the booked contribution (the
+    contributors-match-analytic case, test_ocean_surface_flux.F90:220-300)."""
+    cols = columns(nx=32, ny=16, nz=10, seed=41, land_frac=0.2)
+    cfg = hot_cfg(budgets=1, surface_flux=1)
+    vp = loaded(VP, cols, cfg)
+    T0 = np.asarray(vp.get_tracer(1)).copy()
+    for _ in range(4):
+        vp.surface_flux(DT)
+    gained = ((np.asarray(vp.get_tracer(1)) - T0) * cols.h).sum()
+    booked = np.asarray(vp.get("heat_budget_surface")).sum()
+    assert abs(gained - booked) <= 1e-9 * max(abs(booked), 1e-30)
+
+
+@pytest.mark.parametrize("shape", [(24, 20, 12), (33, 17, 3)])
+def test_step_with_surface_flux(VP, oracle, shape):
+    nx, ny, nz = shape
+    cols = columns(nx=nx, ny=ny, nz=nz, seed=nx + ny, thin_frac=0.1)
+    cfg = hot_cfg(budgets=1, surface_flux=1)
+    st = oracle_state(oracle, cols, cfg)
+    vp = loaded(VP, cols, cfg)
+    assert st.call("vpo_step", cfg, DT, 3) == 0
+    vp.step(DT, 3)
+    for t in range(st.ntr):
+        assert_bitwise(f"tracer{t}", vp.get_tracer(t), st.tracers[t])
+    for n in ("kv", "kt", "ks", "u", "v", "bl_depth", "b0", "rho", "heat_budget", "heat_budget_surface",
+              "salt_budget_surface"):
+        assert_bitwise(n, vp.get(n), getattr(st, n))
+
+
+def test_step_graph_with_surface_flux(VP, oracle):
+    cols = columns(nx=40, ny=24, nz=16, seed=43, thin_frac=0.1)
+    cfg = hot_cfg(surface_flux=1)
+    st = oracle_state(oracle, cols, cfg)
+    vp = loaded(VP, cols, cfg)
+    assert st.call("vpo_step", cfg, DT, 4) == 0
+    vp.step_graph(DT, 2)
+    vp.step_graph(DT, 2)
+    for t in range(st.ntr):
+        assert_bitwise(f"tracer{t}", vp.get_tracer(t), st.tracers[t])
+
+
+def test_mixed_step_with_surface_flux(VP, oracle):
+    """A 1 mm top layer under 100 W/m2 warms by ~87 K: its column group is
+    re-solved in FP64, and the step keeps the 1e-6 bar."""
+    ntr = 6
+    cols = columns(nx=48, ny=32, nz=40, seed=44, ntr=ntr, thin_frac=0.15, passive_init="uniform")
+    cfg = hot_cfg(ntr=ntr, surface_flux=1)
+    st = oracle_state(oracle, cols, cfg)
+    vp = loaded(VP, cols, hot_cfg(ntr=ntr, surface_flux=1, mixed_precision=1))
+    assert st.call("vpo_step", cfg, DT, 1) == 0
+    vp.step(DT, 1)
+    assert vp.mixed_redo_count() > 0
+    err = max(float(np.abs(np.asarray(vp.get_tracer(t)) - st.tracers[t]).max()) for t in range(ntr))
+    assert err <= 1.0e-6, err
+
+
+def test_surface_flux_rejects_bad_flag(VP):
+    from roundabout_b200 import _ffi
+
+    cols = columns(nx=8, ny=4, nz=3, seed=45)
+    with pytest.raises(_ffi.VphysError):
+        loaded(VP, cols, hot_cfg(surface_flux=2))

@@ -340,3 +340,105 @@ def test_wright_eos_reference_value(oracle):
     st.h[...] = 0.0
     st.call("vpo_eos_wright", c)
     assert np.all(st.rho == c.rho0)
+
+
+# ------------------------------------------------------- surface fluxes ----
+# test_ocean_surface_flux.F90: zero flux is a no-op (82-117), heat warms the
+# top layer by dt*Q/(rho0*cp*h) and leaves the rest (119-169), salt likewise
+# with dt*Q/rho0 (171-218), the contributors integrate to the analytic deposit
+# (220-300), a non-uniform Q field acts per column (302-364); plus the
+# first-live-layer rule (apply_surface_src_2d_impl's k_top walk) and the
+# pseudo-salt mirror that books no budget.
+def flux_state(oracle, nz=4, h=10.0, ntr=3):
+    st = state(oracle, nx=6, ny=4, nz=nz, ntr=ntr, h=h)
+    st.tracers[0][...] = 35.0    # salinity
+    st.tracers[1][...] = 10.0    # temperature
+    return st
+
+
+def test_surface_flux_zero_is_no_op(oracle):
+    c = cfg_pp81(budgets=1)
+    st = flux_state(oracle)
+    T0, S0 = st.tracers[1].copy(), st.tracers[0].copy()
+    for _ in range(5):
+        st.call("vpo_surface_flux", c, 3600.0)
+    assert np.abs(st.tracers[1] - T0).max() < 1e-14 and np.abs(st.tracers[0] - S0).max() < 1e-14
+    assert np.abs(st.heat_budget_surface).max() == 0.0
+
+
+def test_surface_heat_flux_warms_top(oracle):
+    c = cfg_pp81()
+    st = flux_state(oracle)
+    st.q_heat[...] = 100.0
+    st.call("vpo_surface_flux", c, 3600.0)
+    dhT = 3600.0 * 100.0 / (c.rho0 * c.cp)
+    assert np.abs(st.tracers[1][:, :, -1] - (10.0 + dhT / 10.0)).max() < 1e-10
+    assert np.abs(st.tracers[1][:, :, :-1] - 10.0).max() < 1e-14
+    assert np.abs(st.tracers[0] - 35.0).max() < 1e-14
+
+
+def test_surface_salt_flux_salinifies_top(oracle):
+    c = cfg_pp81()
+    st = flux_state(oracle)
+    st.q_salt[...] = 1.0e-3
+    st.call("vpo_surface_flux", c, 3600.0)
+    dhS = 3600.0 * 1.0e-3 / c.rho0
+    assert np.abs(st.tracers[0][:, :, -1] - (35.0 + dhS / 10.0)).max() < 1e-10
+    assert np.abs(st.tracers[0][:, :, :-1] - 35.0).max() < 1e-14
+    assert np.abs(st.tracers[1] - 10.0).max() < 1e-14
+
+
+def test_surface_flux_contributors_match_analytic(oracle):
+    c = cfg_pp81(budgets=1)
+    st = flux_state(oracle)
+    st.q_heat[...] = 100.0
+    st.q_salt[...] = 1.0e-3
+    n = 7
+    for _ in range(n):
+        st.call("vpo_surface_flux", c, 3600.0)
+    cells = st.nx * st.ny
+    want_heat = n * 3600.0 * 100.0 / (c.rho0 * c.cp) * cells
+    want_salt = n * 3600.0 * 1.0e-3 / c.rho0 * cells
+    assert abs(st.heat_budget_surface.sum() - want_heat) < 1e-10 * want_heat
+    assert abs(st.salt_budget_surface.sum() - want_salt) < 1e-10 * want_salt
+    # the booked content is what the top layer gained
+    gained = ((st.tracers[1] - 10.0) * st.h).sum()
+    assert abs(gained - want_heat) < 1e-10 * want_heat
+
+
+def test_surface_flux_nonuniform_field_per_column(oracle):
+    c = cfg_pp81()
+    st = flux_state(oracle)
+    st.q_heat[:3, :] = 100.0       # west half heated, east half not
+    st.call("vpo_surface_flux", c, 3600.0)
+    dhT = 3600.0 * 100.0 / (c.rho0 * c.cp)
+    assert np.abs(st.tracers[1][:3, :, -1] - (10.0 + dhT / 10.0)).max() < 1e-10
+    assert np.abs(st.tracers[1][3:, :, -1] - 10.0).max() < 1e-14
+
+
+def test_surface_flux_lands_on_first_live_layer_and_spares_land(oracle):
+    c = cfg_pp81(budgets=1)
+    st = flux_state(oracle, nz=6)
+    st.h[:, :, -1] = 1.0e-4        # vanished top filler everywhere
+    st.h[:2, :, -2] = 0.0          # and a second one on two columns
+    st.wet[5, 3] = 0.0             # a land cell
+    st.q_heat[...] = 100.0
+    st.call("vpo_surface_flux", c, 3600.0)
+    T = st.tracers[1]
+    assert np.all(T[:, :, -1] == 10.0)                     # the filler takes nothing
+    assert np.all(T[2:, :, -2][~(st.wet[2:, :] == 0.0)] > 10.0)
+    assert np.all(T[:2, :, -3] > 10.0) and np.all(T[:2, :, -2] == 10.0)
+    assert np.all(T[5, 3, :] == 10.0)                      # land: wet = 0
+    assert st.heat_budget_surface[5, 3, :].sum() == 0.0
+    assert np.all(st.heat_budget_surface[:, :, -1] == 0.0)
+
+
+def test_surface_flux_pseudo_salt_mirrors_salt_without_budget(oracle):
+    c = cfg_pp81(budgets=1, idx_pseudo_salt=2)
+    st = flux_state(oracle)
+    st.tracers[2][...] = 35.0
+    st.q_salt[...] = 1.0e-3
+    st.call("vpo_surface_flux", c, 3600.0)
+    np.testing.assert_array_equal(st.tracers[2], st.tracers[0])
+    dhS = 3600.0 * 1.0e-3 / c.rho0
+    assert abs(st.salt_budget_surface.sum() - dhS * st.nx * st.ny) < 1e-10 * dhS * st.nx * st.ny
