@@ -167,7 +167,21 @@ def traffic_from_profiles(kernel: str):
 # ---------------------------------------------------------------------------
 # CPU arm (the oracle: the C restatement of the reference)
 # ---------------------------------------------------------------------------
-def cpu_run(cfg_name: str, sample: str, steps: int, warmup: int):
+def host_cpu():
+    """nproc and the CPU model of this host (/proc/cpuinfo)."""
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"nproc": os.cpu_count(), "model": model}
+
+
+def cpu_run(cfg_name: str, sample: str, steps: int, warmup: int, threads: int = 0):
     from oracle import oracle as o
     from roundabout_b200.config import hot_path_config
     from roundabout_b200.synthetic import CONFIGS, make_columns
@@ -192,7 +206,7 @@ def cpu_run(cfg_name: str, sample: str, steps: int, warmup: int):
     st.q_salt[...] = cols.q_salt
     st.wet[...] = cols.wet
     st.stress_mag_from_tau()
-    threads = os.cpu_count() or 1
+    threads = threads if threads > 0 else (os.cpu_count() or 1)
     o.set_threads(threads)
     for _ in range(warmup):
         st.call("vpo_step", cfg, 3600.0, 1)
@@ -449,6 +463,9 @@ def main():
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_run(args.config, args.cpu_sample, 2, 1)
         cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        one = cpu_run(args.config, args.cpu_sample, 1, 1, threads=1)
+        cpu["single_thread"] = {"value": one["value"], "unit": "cells/s", "cores": 1}
+        cpu["host"] = host_cpu()
 
     clocks = clk.summary()
     line = {"metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,

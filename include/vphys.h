@@ -148,6 +148,12 @@ typedef struct vphys_config {
     int learned_kpp;          /* 1: the KPP boundary-layer depth comes from the attached MLP surrogate
                                  (vphys_kpp_attach), with the range gate and the sampled plain-KPP
                                  check; 0: the reference's bulk-Richardson search */
+    int buoyancy_coeffs;      /* KPP surface buoyancy flux coefficients (&ocean_vmix_nml buoyancy_coeffs):
+                                 0 "constant": alpha_T / beta_S above; 1 "eos": -d(rho)/dT and d(rho)/dS of
+                                 the Wright EOS at the first live layer's (T, S) and eos_p_ref
+                                 (eos_buoyancy_coeffs, rdb_eos.F90:1624-1736; the constants on a vanished
+                                 surface layer) */
+    int pad0;
 } vphys_config;
 
 /* ---- field ids (vphys_bind / vphys_set_field / vphys_get_field) ----- */

@@ -64,6 +64,8 @@ def lib():
         for name in ("vpo_vdiff_momentum", "vpo_vdiff_tracers", "vpo_nonlocal", "vpo_surface_flux"):
             getattr(L, name).argtypes = [ctypes.c_void_p, ctypes.POINTER(VpoState), ctypes.c_double]
             getattr(L, name).restype = None
+        L.vpo_eos_buoyancy_coeffs.argtypes = [ctypes.c_double] * 3 + [ctypes.POINTER(ctypes.c_double)] * 2
+        L.vpo_eos_buoyancy_coeffs.restype = None
         L.vpo_step.argtypes = [ctypes.c_void_p, ctypes.POINTER(VpoState), ctypes.c_double, ctypes.c_int]
         L.vpo_step.restype = ctypes.c_int
         _lib = L
@@ -166,3 +168,10 @@ def sm_cbrt(x: float) -> float:
 
 def sm_atan(x: float) -> float:
     return lib().vpo_sm_atan(float(x))
+
+
+def eos_buoyancy_coeffs(T: float, S: float, p: float):
+    """(alpha_T, beta_S) = (-d rho/dT, +d rho/dS) of the Wright EOS at (T, S, p)."""
+    a, b = ctypes.c_double(), ctypes.c_double()
+    lib().vpo_eos_buoyancy_coeffs(float(T), float(S), float(p), ctypes.byref(a), ctypes.byref(b))
+    return a.value, b.value

@@ -164,6 +164,27 @@ void vpo_eos_wright(const vphys_config *c, vpo_state *s)
             }
 }
 
+/* eos_buoyancy_coeffs, Wright branch (rdb_eos.F90:1624-1736, the Wright arm
+ * 1716-1733): alpha_T = -d(rho)/dT, beta_S = +d(rho)/dS of rho = P/D with
+ * P = p + p0(T,S), D = lambda(T,S) + alpha0(T,S) P, by the quotient rule. */
+void vpo_eos_buoyancy_coeffs(double T, double S, double p, double *alpha_T, double *beta_S)
+{
+    double T_sq = T * T;
+    double alpha_0 = WRIGHT_A0 + WRIGHT_A1 * T + WRIGHT_A2 * S;
+    double p_0 = WRIGHT_B0 + WRIGHT_B1 * T + WRIGHT_B2 * T_sq + WRIGHT_B3 * T_sq * T + WRIGHT_B4 * S + WRIGHT_B5 * S * T;
+    double lambda = WRIGHT_C0 + WRIGHT_C1 * T + WRIGHT_C2 * T_sq + WRIGHT_C3 * T_sq * T + WRIGHT_C4 * S +
+                    WRIGHT_C5 * S * T;
+    double dp0_dt = WRIGHT_B1 + 2.0 * WRIGHT_B2 * T + 3.0 * WRIGHT_B3 * T_sq + WRIGHT_B5 * S;
+    double dlam_dt = WRIGHT_C1 + 2.0 * WRIGHT_C2 * T + 3.0 * WRIGHT_C3 * T_sq + WRIGHT_C5 * S;
+    double dp0_ds = WRIGHT_B4 + WRIGHT_B5 * T;
+    double dlam_ds = WRIGHT_C4 + WRIGHT_C5 * T;
+    double big_p = p + p_0;
+    double denom = lambda + alpha_0 * big_p;
+    double inv_d2 = 1.0 / (denom * denom);
+    *alpha_T = -(dp0_dt * denom - big_p * (dlam_dt + WRIGHT_A1 * big_p + alpha_0 * dp0_dt)) * inv_d2;
+    *beta_S = (dp0_ds * denom - big_p * (dlam_ds + WRIGHT_A2 * big_p + alpha_0 * dp0_ds)) * inv_d2;
+}
+
 /* |tau| at cell centres (rdb_ocean_surface_stress.F90:858-875). */
 void vpo_stress_mag(vpo_state *s)
 {
@@ -294,6 +315,20 @@ static inline double kpp_b0(double alpha_T, double beta_S, double rho0, double q
     return (GRAVITY / rho0) * (alpha_T * qT - beta_S * qS);
 }
 
+/* The coefficient pair of B0 (rdb_ocean_vmix.F90:1357-1376, 1469-1488): the
+ * constants, or with buoyancy_coeffs = "eos" the Wright derivatives at the
+ * first live layer's (T, S) and p_ref when that layer is live. */
+static inline double kpp_b0_col(const vphys_config *c, const vpo_state *s, int i, int j, int k_sfc, double qT,
+                                double qS)
+{
+    const int nx = s->nx, ny = s->ny;
+    double a = c->alpha_T, b = c->beta_S;
+    if (c->buoyancy_coeffs && C3(s->h, i, j, k_sfc) > H_VANISHED)
+        vpo_eos_buoyancy_coeffs(C3(s->tr[c->idx_temperature], i, j, k_sfc), C3(s->tr[c->idx_salinity], i, j, k_sfc),
+                                c->eos_p_ref, &a, &b);
+    return kpp_b0(a, b, c->rho0, qT, qS);
+}
+
 /* =====================================================================
  * KPP overlay (rdb_ocean_vmix.F90:1121-1516), constant buoyancy
  * coefficients, no penetrating shortwave (sw_active = .false.).
@@ -321,7 +356,7 @@ void vpo_kpp_overlay(const vphys_config *c, vpo_state *s)
             double h_b_lagged = C2(s->bl_depth, i, j);
             double q_T_kin = C2(s->q_heat, i, j) / (rho0 * c->cp);
             double q_S_kin = C2(s->q_salt, i, j) / rho0;
-            double B_0 = kpp_b0(c->alpha_T, c->beta_S, rho0, q_T_kin, q_S_kin);
+            double B_0 = kpp_b0_col(c, s, i, j, k_sfc, q_T_kin, q_S_kin);
             double wstar3_lagged = fmx(0.0, -B_0) * h_b_lagged;
             double cb = vpo_sm_cbrt(wstar3_lagged);
             double w_s_col = sqrt(u_star * u_star + cb * cb);
@@ -371,7 +406,7 @@ void vpo_kpp_overlay(const vphys_config *c, vpo_state *s)
             double h_b = C2(s->bl_depth, i, j);
             double q_T_kin = C2(s->q_heat, i, j) / (rho0 * c->cp);
             double q_S_kin = C2(s->q_salt, i, j) / rho0;
-            double B_0 = kpp_b0(c->alpha_T, c->beta_S, rho0, q_T_kin, q_S_kin);
+            double B_0 = kpp_b0_col(c, s, i, j, k_sfc, q_T_kin, q_S_kin);
             C2(s->b0, i, j) = B_0;
             int destabilizing = B_0 < 0.0;
             double wstar3 = fmx(0.0, -B_0) * h_b;

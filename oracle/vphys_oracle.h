@@ -63,6 +63,7 @@ void vpo_vdiff_momentum(const vphys_config *c, vpo_state *s, double dt);
 void vpo_vdiff_tracers(const vphys_config *c, vpo_state *s, double dt);
 void vpo_nonlocal(const vphys_config *c, vpo_state *s, double dt);
 void vpo_surface_flux(const vphys_config *c, vpo_state *s, double dt);
+void vpo_eos_buoyancy_coeffs(double T, double S, double p, double *alpha_T, double *beta_S);
 
 int vpo_step(const vphys_config *c, vpo_state *s, double dt, int n_steps);
 

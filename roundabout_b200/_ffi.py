@@ -125,10 +125,11 @@ class VphysConfig(ctypes.Structure):
         ("idx_temperature", ctypes.c_int), ("idx_salinity", ctypes.c_int), ("idx_pseudo_salt", ctypes.c_int),
         ("eos_in_step", ctypes.c_int), ("remnant", ctypes.c_int), ("budgets", ctypes.c_int),
         ("mixed_precision", ctypes.c_int), ("learned_kpp", ctypes.c_int),
+        ("buoyancy_coeffs", ctypes.c_int), ("pad0", ctypes.c_int),
     ]
 
     def as_dict(self):
-        return {n: getattr(self, n) for n, _ in self._fields_ if n not in ()}
+        return {n: getattr(self, n) for n, _ in self._fields_ if n not in ("pad0",)}
 
 
 class LibraryNotFoundError(FileNotFoundError):

@@ -31,6 +31,7 @@ def default_config() -> VphysConfig:
     c.kd_smooth_iterations = 0
     c.conv_enable = 0
     c.surface_flux = 0
+    c.buoyancy_coeffs = 0
     c.pp81_nu0 = 1.0e-2
     c.pp81_nu_bg = 1.0e-4
     c.pp81_kappa_bg = 1.0e-5

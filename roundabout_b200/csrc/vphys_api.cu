@@ -227,6 +227,10 @@ int validate(const vphys_config *c, int ntr)
         return push_error(VPHYS_ERR_CONFIG, "mixed_precision %d: 0 (FP64), 1 (mixed solves) or 2 (mixed solves and assembly)",
                           c->mixed_precision);
     if (c->surface_flux < 0 || c->surface_flux > 1) return push_error(VPHYS_ERR_CONFIG, "surface_flux must be 0 or 1");
+    if (c->buoyancy_coeffs < 0 || c->buoyancy_coeffs > 1)
+        return push_error(VPHYS_ERR_CONFIG, "buoyancy_coeffs must be 0 (constant) or 1 (eos)");
+    if (c->buoyancy_coeffs && c->use_kpp && (c->idx_temperature < 0 || c->idx_salinity < 0))
+        return push_error(VPHYS_ERR_CONFIG, "buoyancy_coeffs = eos needs temperature and salinity tracers");
     if (c->rho0 <= 0.0 || c->cp <= 0.0) return push_error(VPHYS_ERR_CONFIG, "rho0 and cp must be positive");
     if (c->use_kpp && c->ri_crit <= 0.0) return push_error(VPHYS_ERR_CONFIG, "ri_crit must be positive");
     if (c->bkgnd_profile && c->bkgnd_delta == 0.0) return push_error(VPHYS_ERR_CONFIG, "bkgnd_delta must be nonzero");

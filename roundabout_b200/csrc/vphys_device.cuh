@@ -8,6 +8,8 @@
 
 #include <cstdint>
 
+#include "../../include/vphys.h"
+
 namespace vphys {
 
 constexpr double GRAVITY = 9.80665;        // rdb_constants.F90:37
@@ -17,6 +19,13 @@ constexpr double PI_D = 3.141592653589793115997963468544185161590576171875;  // 
 constexpr double EPS_HVEL = 1.0e-30;       // rdb_ocean_vdiff.F90 diffuse_velocity_columns_impl
 constexpr double STRESS_H_MIN = 1.0e-3;
 constexpr double DBL_TINY = 2.2250738585072014e-308;
+
+// Wright (1997) reduced-range coefficients (rdb_eos.F90:200-217, Table A1)
+constexpr double WRIGHT_A0 = 7.057924e-4, WRIGHT_A1 = 3.480336e-7, WRIGHT_A2 = -1.112733e-7;
+constexpr double WRIGHT_B0 = 5.790749e8, WRIGHT_B1 = 3.516535e6, WRIGHT_B2 = -4.002714e4, WRIGHT_B3 = 2.084372e2,
+                 WRIGHT_B4 = 5.944068e5, WRIGHT_B5 = -9.643486e3;
+constexpr double WRIGHT_C0 = 1.704853e5, WRIGHT_C1 = 7.904722e2, WRIGHT_C2 = -7.984422e0, WRIGHT_C3 = 5.140652e-2,
+                 WRIGHT_C4 = -2.302158e2, WRIGHT_C5 = -3.079464e0;
 
 // ---- exact division helpers ----------------------------------------------
 // xdiv(a, b) == a / b for every input.  A zero numerator is answered directly
@@ -201,6 +210,42 @@ __device__ __forceinline__ double ld_hint(const double *ptr, unsigned long long 
 __device__ __forceinline__ void st_hint(double *ptr, double v, unsigned long long pol)
 {
     asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(ptr), "d"(v), "l"(pol) : "memory");
+}
+
+// eos_buoyancy_coeffs, Wright branch (rdb_eos.F90:1716-1733): alpha_T =
+// -d(rho)/dT and beta_S = +d(rho)/dS of rho = P/D, P = p + p0(T,S),
+// D = lambda(T,S) + alpha0(T,S) P, by the quotient rule, in the reference's
+// operation order.
+__device__ __forceinline__ void wright_buoyancy_coeffs(double T, double S, double p, double &alpha_T, double &beta_S)
+{
+    const double T_sq = T * T;
+    const double alpha_0 = WRIGHT_A0 + WRIGHT_A1 * T + WRIGHT_A2 * S;
+    const double p_0 = WRIGHT_B0 + WRIGHT_B1 * T + WRIGHT_B2 * T_sq + WRIGHT_B3 * T_sq * T + WRIGHT_B4 * S +
+                       WRIGHT_B5 * S * T;
+    const double lambda = WRIGHT_C0 + WRIGHT_C1 * T + WRIGHT_C2 * T_sq + WRIGHT_C3 * T_sq * T + WRIGHT_C4 * S +
+                          WRIGHT_C5 * S * T;
+    const double dp0_dt = WRIGHT_B1 + 2.0 * WRIGHT_B2 * T + 3.0 * WRIGHT_B3 * T_sq + WRIGHT_B5 * S;
+    const double dlam_dt = WRIGHT_C1 + 2.0 * WRIGHT_C2 * T + 3.0 * WRIGHT_C3 * T_sq + WRIGHT_C5 * S;
+    const double dp0_ds = WRIGHT_B4 + WRIGHT_B5 * T;
+    const double dlam_ds = WRIGHT_C4 + WRIGHT_C5 * T;
+    const double big_p = p + p_0;
+    const double denom = lambda + alpha_0 * big_p;
+    const double inv_d2 = xdiv(1.0, denom * denom);
+    alpha_T = -(dp0_dt * denom - big_p * (dlam_dt + WRIGHT_A1 * big_p + alpha_0 * dp0_dt)) * inv_d2;
+    beta_S = (dp0_ds * denom - big_p * (dlam_ds + WRIGHT_A2 * big_p + alpha_0 * dp0_ds)) * inv_d2;
+}
+
+// The KPP surface buoyancy flux B0 (kpp_surface_buoyancy_flux,
+// rdb_ocean_vmix.F90:1518-1559) with the coefficient pair of
+// buoyancy_coeffs (1357-1376): the constants, or with "eos" the Wright
+// derivatives at the first live layer's (T_sfc, S_sfc) and p_ref when that
+// layer is live (h_sfc > H_VANISHED).
+__device__ __forceinline__ double kpp_surface_b0(const vphys_config &c, double q_T_kin, double q_S_kin, double h_sfc,
+                                                 double T_sfc, double S_sfc)
+{
+    double a = c.alpha_T, b = c.beta_S;
+    if (c.buoyancy_coeffs && h_sfc > H_VANISHED) wright_buoyancy_coeffs(T_sfc, S_sfc, c.eos_p_ref, a, b);
+    return (GRAVITY / c.rho0) * (a * q_T_kin - b * q_S_kin);
 }
 
 }  // namespace vphys

@@ -43,11 +43,11 @@ __global__ void __launch_bounds__(256) k_eos_wright(const Params p)
             double S_k = __ldg(S + idx), T_k = __ldg(T + idx);
             double T_sq = T_k * T_k;
             double T_cu = T_sq * T_k;
-            double alpha_0 = 7.057924e-4 + 3.480336e-7 * T_k + -1.112733e-7 * S_k;
-            double p_0 = 5.790749e8 + 3.516535e6 * T_k + -4.002714e4 * T_sq + 2.084372e2 * T_cu + 5.944068e5 * S_k +
-                         -9.643486e3 * S_k * T_k;
-            double lambda = 1.704853e5 + 7.904722e2 * T_k + -7.984422e0 * T_sq + 5.140652e-2 * T_cu +
-                            -2.302158e2 * S_k + -3.079464e0 * S_k * T_k;
+            double alpha_0 = WRIGHT_A0 + WRIGHT_A1 * T_k + WRIGHT_A2 * S_k;
+            double p_0 = WRIGHT_B0 + WRIGHT_B1 * T_k + WRIGHT_B2 * T_sq + WRIGHT_B3 * T_cu + WRIGHT_B4 * S_k +
+                         WRIGHT_B5 * S_k * T_k;
+            double lambda = WRIGHT_C0 + WRIGHT_C1 * T_k + WRIGHT_C2 * T_sq + WRIGHT_C3 * T_cu + WRIGHT_C4 * S_k +
+                            WRIGHT_C5 * S_k * T_k;
             double p_plus_p0 = p_ref + p_0;
             double denom = lambda + alpha_0 * p_plus_p0;
             r = p_plus_p0 / denom;
@@ -164,7 +164,12 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
         const double u_star = sqrt(xdiv(tau_mag, rho0));
         q_T_kin = xdiv(p.q_heat[col], rho0 * c.cp);
         q_S_kin = xdiv(p.q_salt[col], rho0);
-        const double B_0 = (GRAVITY / rho0) * (c.alpha_T * q_T_kin - c.beta_S * q_S_kin);
+        double T_sfc = 0.0, S_sfc = 0.0;
+        if (c.buoyancy_coeffs) {   // "eos": the surface layer's (T, S) (rdb_ocean_vmix.F90:1357-1376)
+            T_sfc = p.tr[c.idx_temperature][col + P * (size_t)(k_sfc - 1)];
+            S_sfc = p.tr[c.idx_salinity][col + P * (size_t)(k_sfc - 1)];
+        }
+        const double B_0 = kpp_surface_b0(c, q_T_kin, q_S_kin, HH(k_sfc), T_sfc, S_sfc);
         {
             const double wstar3_lagged = fmx(0.0, -B_0) * h_b;
             const double cb = sm_cbrt(wstar3_lagged);

@@ -107,7 +107,12 @@ __global__ void __launch_bounds__(FEAT_THREADS) k_kpp_features(const Params p, c
     const double u_star = sqrt(xdiv(p.stress_mag[col], rho0));
     const double q_T_kin = xdiv(p.q_heat[col], rho0 * c.cp);
     const double q_S_kin = xdiv(p.q_salt[col], rho0);
-    const double B_0 = (GRAVITY / rho0) * (c.alpha_T * q_T_kin - c.beta_S * q_S_kin);
+    double T_sfc = 0.0, S_sfc = 0.0;
+    if (c.buoyancy_coeffs) {   // the same surface (T, S) the assembly's B0 will use
+        T_sfc = p.tr[c.idx_temperature][col + P * (size_t)(k_sfc - 1)];
+        S_sfc = p.tr[c.idx_salinity][col + P * (size_t)(k_sfc - 1)];
+    }
+    const double B_0 = kpp_surface_b0(c, q_T_kin, q_S_kin, HH(k_sfc), T_sfc, S_sfc);
     const double f = p.coriolis ? p.coriolis[col] : 0.0;
     bool oor = false;
     emit(o, srow, col, 0, (float)(u_star * 100.0), oor);
@@ -205,7 +210,9 @@ __global__ void k_kpp_targets(const Params p, float *T)
     const double u_star = sqrt(xdiv(p.stress_mag[col], rho0));
     const double q_T_kin = xdiv(p.q_heat[col], rho0 * c.cp);
     const double q_S_kin = xdiv(p.q_salt[col], rho0);
-    const double B_0 = (GRAVITY / rho0) * (c.alpha_T * q_T_kin - c.beta_S * q_S_kin);
+    // with "eos" coefficients, the B0 of the assembly that set this h_b
+    const double B_0 = c.buoyancy_coeffs ? p.b0[col]
+                                         : (GRAVITY / rho0) * (c.alpha_T * q_T_kin - c.beta_S * q_S_kin);
     const double w_star = sm_cbrt(fmx(0.0, -B_0) * h_b);
     const double w_s = sqrt(u_star * u_star + w_star * w_star);
     float *t = T + col * LK_OUTP;

@@ -64,6 +64,7 @@ ASSEMBLE_CASES = {
     "ceilings": dict(kv_max=2e-3, kd_max=5e-4),
     "smoothing": dict(kd_smooth_iterations=2),
     "no_vt2": dict(c_vt2=0.0),
+    "eos_buoyancy_coeffs": dict(buoyancy_coeffs=1),
 }
 
 
@@ -142,6 +143,7 @@ TRACER_CASES = {
     "budgets": dict(budgets=1),
     "use_harmonic": dict(use_harmonic=1),
     "no_kpp": dict(use_kpp=0),
+    "eos_buoyancy_coeffs": dict(buoyancy_coeffs=1),
 }
 
 
@@ -150,6 +152,8 @@ TRACER_CASES = {
 def test_tracers_and_nonlocal(VP, oracle, case, ntr):
     cols = columns(seed=21, ntr=ntr, thin_frac=0.15, passive_init="uniform")
     over = dict(TRACER_CASES[case])
+    if ntr < 2 and over.get("buoyancy_coeffs"):
+        pytest.skip("the eos coefficients need T and S")
     cfg = hot_cfg(ntr=ntr, **over)
     if ntr < 2:
         cfg.idx_temperature = -1
@@ -253,3 +257,61 @@ def test_bind_torch_zero_copy(VP, oracle):
     vp.synchronize()
     assert_bitwise("u (bound tensor)", u_t.cpu().numpy().T, st.u)
     compare_all(vp, st, names=("kv", "v"))
+
+
+def test_tracer_solve_conserves_column_content(VP, oracle):
+    """Column sum of h~ * T and h~ * S (h~ = max(h, H_VANISHED) as the matrix
+    weights rows) before and after the tracer solve: the drift is round-off,
+    summed exactly (math.fsum) per column -- the conservation metric of the
+    path, on the GPU's own output, with thin stiff layers present."""
+    import math
+
+    cols = columns(nx=40, ny=24, nz=30, seed=12, thin_frac=0.15)
+    cfg = hot_cfg()
+    vp = gpu_state(VP, cols, cfg)
+    vp.eos()
+    vp.assemble()
+    ht = np.maximum(cols.h, 1.5e-4)
+    live = cols.h > 1.5e-4
+    before = [np.asarray(vp.get_tracer(t)).copy() for t in (0, 1)]
+    vp.vdiff_tracers(DT)
+    worst = 0.0
+    for t, b in zip((0, 1), before):
+        a = np.asarray(vp.get_tracer(t))
+        for i in range(cols.nx):
+            for j in range(cols.ny):
+                m = live[i, j]
+                if not m.any():
+                    continue
+                s0 = math.fsum((ht[i, j, m] * b[i, j, m]).tolist())
+                s1 = math.fsum((ht[i, j, m] * a[i, j, m]).tolist())
+                scale = math.fsum(np.abs(ht[i, j, m] * b[i, j, m]).tolist())
+                worst = max(worst, abs(s1 - s0) / scale)
+    # the reference's own bar for the column sum is 1e-12 (test_ocean_vdiff.F90:270-308)
+    assert worst <= 1e-12, worst
+
+
+@pytest.mark.parametrize("mixed", [0, 1, 2])
+def test_full_step_eos_buoyancy_coeffs(VP, oracle, mixed):
+    """KPP's B0 from the Wright derivatives at the surface (T, S): bitwise
+    on the FP64 path over 3 steps (assembly, solves, the non-local deposit
+    from the stored b0); the mixed forms within their one-step bars."""
+    cols = columns(nx=40, ny=24, nz=20, seed=19, thin_frac=0.1)
+    cfg = hot_cfg(budgets=1, buoyancy_coeffs=1)
+    st = oracle_state(oracle, cols, cfg)
+    vp = gpu_state(VP, cols, hot_cfg(budgets=1, buoyancy_coeffs=1, mixed_precision=mixed))
+    n = 3 if mixed == 0 else 1
+    assert st.call("vpo_step", cfg, DT, n) == 0
+    vp.step(DT, n)
+    if mixed == 0:
+        compare_all(vp, st)
+        assert_bitwise("heat_budget", vp.get("heat_budget"), st.heat_budget)
+    else:
+        tol = 1.0e-6 if mixed == 1 else 2.0e-5
+        for t in range(st.ntr):
+            assert float(np.abs(np.asarray(vp.get_tracer(t)) - st.tracers[t]).max()) <= tol
+    # the eos pair really changed the answer
+    c0 = hot_cfg(budgets=1)
+    st0 = oracle_state(oracle, cols, c0)
+    st0.call("vpo_step", c0, DT, n)
+    assert np.abs(st0.b0 - st.b0).max() > 0.0

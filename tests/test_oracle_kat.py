@@ -442,3 +442,71 @@ def test_surface_flux_pseudo_salt_mirrors_salt_without_budget(oracle):
     np.testing.assert_array_equal(st.tracers[2], st.tracers[0])
     dhS = 3600.0 * 1.0e-3 / c.rho0
     assert abs(st.salt_budget_surface.sum() - dhS * st.nx * st.ny) < 1e-10 * dhS * st.nx * st.ny
+
+
+# ------------------------------------------- buoyancy_coeffs = "eos" ----
+# test_ocean_eos_buoyancy.F90: the Wright derivatives against centred
+# differences of the EOS itself (points 99-110, steps and tolerances 112-122,
+# check 169-201), alpha_T rising with temperature toward 20 C (283-313) and
+# with pressure at the freezing point (315-339), and KPP's kv scaling as the
+# cube root of the B0 ratio in the closed-form column (462-556).
+EOS_PTS = [(-2.0, 33.0, 0.0), (-1.9, 34.5, 0.0), (-1.0, 34.0, 2.5e6), (0.0, 35.0, 5.0e6), (1.0, 33.5, 7.5e6),
+           (2.0, 34.5, 1.0e7), (-2.0, 34.5, 1.0e7), (-1.9, 33.0, 5.0e6), (2.0, 35.0, 0.0), (10.0, 35.0, 0.0),
+           (18.0, 36.0, 2.0e6), (25.0, 34.0, 4.0e7)]
+
+
+def eos_rho(oracle, T, S, p):
+    c = cfg_pp81(eos_p_ref=p)
+    st = state(oracle, nx=1, ny=1, nz=1, ntr=2)
+    st.tracers[0][...] = S
+    st.tracers[1][...] = T
+    st.call("vpo_eos_wright", c)
+    return float(st.rho[0, 0, 0])
+
+
+def test_eos_buoyancy_coeffs_match_finite_differences(oracle):
+    eps = 1.0e-4
+    for T, S, p in EOS_PTS:
+        a, b = oracle.eos_buoyancy_coeffs(T, S, p)
+        fd_t = (eos_rho(oracle, T + eps, S, p) - eos_rho(oracle, T - eps, S, p)) / (2.0 * eps)
+        fd_s = (eos_rho(oracle, T, S + eps, p) - eos_rho(oracle, T, S - eps, p)) / (2.0 * eps)
+        assert abs(-a - fd_t) <= max(1.0e-7 * abs(fd_t), 1.0e-9), (T, S, p, a, fd_t)
+        assert abs(b - fd_s) <= max(1.0e-7 * abs(fd_s), 1.0e-9), (T, S, p, b, fd_s)
+
+
+def test_eos_alpha_grows_with_temperature_and_pressure(oracle):
+    a = [oracle.eos_buoyancy_coeffs(-2.0 + n, 34.5, 0.0)[0] for n in range(23)]
+    assert all(a[n] > a[n - 1] for n in range(1, 23))
+    assert a[12] > 3.0 * a[0] and a[0] > 0.0
+    ap = [oracle.eos_buoyancy_coeffs(-1.9, 34.5, n * 1.0e6)[0] for n in range(11)]
+    assert all(ap[n] > ap[n - 1] for n in range(1, 11))
+    assert ap[10] > 1.5 * ap[0]
+
+
+def test_kpp_eos_coeffs_scale_kv_as_cube_root_of_b0(oracle):
+    nz, H, T0, S0, QH, QS = 8, 40.0, -1.9, 34.5, -200.0, 3.0e-5
+    runs = {}
+    for mode in (0, 1):
+        c = cfg_pp81(use_kpp=1, alpha_T=0.17, beta_S=0.78, buoyancy_coeffs=mode)
+        st = state(oracle, nx=6, ny=4, nz=nz, ntr=2, h=H)
+        st.tracers[0][...] = S0
+        st.tracers[1][...] = T0
+        st.rho[...] = 1027.8
+        st.q_heat[...] = QH
+        st.q_salt[...] = QS
+        st.seed_backgrounds(c)
+        st.call("vpo_pp81", c)
+        st.call("vpo_kpp_overlay", c)
+        runs[mode] = st
+    a_e, b_e = oracle.eos_buoyancy_coeffs(T0, S0, 0.0)
+    qt, qs = QH / (1035.0 * 3992.0), QS / 1035.0
+    b0_c = 0.17 * qt - 0.78 * qs
+    b0_e = a_e * qt - b_e * qs
+    assert b0_c < 0.0 and b0_e < 0.0 and a_e < 0.5 * 0.17
+    ratio = (b0_e / b0_c) ** (1.0 / 3.0)
+    assert abs(ratio - 1.0) > 0.1
+    for k in range(1, nz):
+        kv_c, kv_e = runs[0].kv[3, 2, k], runs[1].kv[3, 2, k]
+        assert kv_c > 1.0e-3
+        assert abs(kv_e / kv_c - ratio) < 1.0e-10 * ratio
+    assert runs[1].b0[3, 2] == (9.80665 / 1035.0) * (a_e * qt - b_e * qs)
