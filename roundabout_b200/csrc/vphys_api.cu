@@ -75,7 +75,6 @@ struct vphys_handle_s {
     double *budget_scratch = nullptr;
     int *span = nullptr;              // live spans of the columns (mixed-precision tracer solve)
     unsigned *mp_redo = nullptr;      // the mixed tracer solve's FP64 re-solve list (count + entries)
-    float2 *hk32 = nullptr;           // the mixed momentum solve's FP32 (h, kv) pairs
     double *zcol = nullptr;           // column depths for the momentum face thickness
     // learned KPP surrogate (vphys_kpp_attach): the caller's weights and the scratch of one inference
     vphys_kpp_model kpp{};
@@ -287,7 +286,6 @@ Params make_params(vphys_handle h)
     p.budget_scratch = h->budget_scratch;
     p.span = h->span;
     p.mp_redo = h->mp_redo;
-    p.hk32 = h->cfg.mixed_precision ? h->hk32 : nullptr;
     p.zcol = h->zcol;
     p.coriolis = D(VPHYS_FIELD_CORIOLIS);
     p.ks_equals_kt = (h->cfg.bkgnd_profile || h->cfg.kt_bg == h->cfg.ks_bg) ? 1 : 0;
@@ -305,14 +303,6 @@ int prepare_momentum(vphys_handle h)
             h->zcol = nullptr;
             cudaGetLastError();
             return push_error(VPHYS_ERR_ALLOC, "cudaMalloc of the column depths failed");
-        }
-    }
-    if (h->cfg.mixed_precision && !h->hk32) {
-        cudaError_t e = cudaMalloc(&h->hk32, (size_t)h->nx * h->ny * h->nz * sizeof(float2));
-        if (e != cudaSuccess) {
-            h->hk32 = nullptr;
-            cudaGetLastError();
-            return push_error(VPHYS_ERR_ALLOC, "cudaMalloc of the FP32 (h, kv) pairs failed");
         }
     }
     if (h->cfg.remnant) {
@@ -343,7 +333,6 @@ int prepare_tracers(vphys_handle h)
         if (e == cudaSuccess) e = cudaMemsetAsync(h->mp_redo, 0, sizeof(unsigned), h->stream);
         if (e != cudaSuccess) {
             if (h->mp_redo) cudaFree(h->mp_redo);
-    if (h->hk32) cudaFree(h->hk32);
             h->mp_redo = nullptr;
             cudaGetLastError();
             return push_error(VPHYS_ERR_ALLOC, "cudaMalloc of the mixed-solve re-solve list failed");

@@ -774,11 +774,6 @@ void launch_smooth(const Params &p, double *fld, double *scratch, cudaStream_t s
 // -sum_{k=1..nz} h of every column, accumulated in the order of
 // diffuse_velocity_columns_impl's z_clear pre-pass (rdb_ocean_vdiff.F90:1621-1700),
 // so the momentum kernels read two numbers per face instead of 2*nz.
-// With p.hk32 the same pass also writes each level's ((float)h, (float)kv)
-// pair: the mixed momentum solve converts both to FP32 on use anyway, and one
-// 8-byte load per cell and level instead of two halves its load instructions
-// and the registers its prefetched levels hold.
-template <bool PACK>
 __global__ void k_column_depth(const Params p)
 {
     constexpr int U = 8;
@@ -787,38 +782,27 @@ __global__ void k_column_depth(const Params p)
     if (i >= p.nx) return;
     const size_t col = (size_t)i + (size_t)p.nx * j;
     const double *__restrict__ hp = p.h + col;
-    const double *__restrict__ kp = p.kv + col;
     const size_t P = p.plane;
     double z = 0.0;
     for (int k0 = 0; k0 < p.nz; k0 += U) {
-        double hv[U], kv[U];
+        double hv[U];
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            hv[u] = (k0 + u < p.nz) ? __ldg(hp + P * (size_t)(k0 + u)) : 0.0;
-            if (PACK) kv[u] = (k0 + u < p.nz) ? __ldg(kp + P * (size_t)(k0 + u)) : 0.0;
-        }
+        for (int u = 0; u < U; ++u) hv[u] = (k0 + u < p.nz) ? __ldg(hp + P * (size_t)(k0 + u)) : 0.0;
 #pragma unroll
         for (int u = 0; u < U; ++u)
-            if (k0 + u < p.nz) {
-                z = z - hv[u];
-                if (PACK) p.hk32[col + P * (size_t)(k0 + u)] = make_float2((float)hv[u], (float)kv[u]);
-            }
+            if (k0 + u < p.nz) z = z - hv[u];
     }
-    if (p.zcol) p.zcol[col] = z;
+    p.zcol[col] = z;
 }
 
 void launch_column_depth(const Params &p, cudaStream_t stream)
 {
-    const dim3 grid((p.nx + 127) / 128, p.ny);
-    if (p.hk32)
-        k_column_depth<true><<<grid, 128, 0, stream>>>(p);
-    else
-        k_column_depth<false><<<grid, 128, 0, stream>>>(p);
+    k_column_depth<<<dim3((p.nx + 127) / 128, p.ny), 128, 0, stream>>>(p);
 }
 
 void launch_momentum(const Params &p, double dt, cudaStream_t stream)
 {
-    if ((p.cfg.hvel_mom6 && !p.cfg.hvel_harmonic) || (p.cfg.mixed_precision && p.hk32)) launch_column_depth(p, stream);
+    if (p.cfg.hvel_mom6 && !p.cfg.hvel_harmonic) launch_column_depth(p, stream);
     if (p.cfg.mixed_precision) {
         launch_momentum_mp(p, dt, stream);
         return;

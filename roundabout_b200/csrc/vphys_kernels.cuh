@@ -5,8 +5,6 @@
 #include <cstddef>
 #include <cstdint>
 
-#include <vector_types.h>
-
 #include "../../include/vphys.h"
 
 namespace vphys {
@@ -47,8 +45,6 @@ struct Params {
     int *span;                        // per column: first | last live layer << 16 (0: none), scratch
     unsigned *mp_redo;                // mixed solves: count, then (group << 5 | tracer) re-solved in FP64
     double *zcol;                     // per column: -sum_k h, k = 1..nz in order (momentum z_clear), scratch
-    float2 *hk32;                     // per cell and level: ((float)h, (float)kv) at the same offset, written
-                                      // by k_column_depth for the mixed momentum solve (nullptr: not mixed)
     const double *coriolis;           // (nx, ny) f, or nullptr (learned KPP features only)
     const float *kpp_pred;            // per column: the surrogate's h_b, < 0: run pass 1; nullptr: plain KPP
     const float *kpp_check;           // per column: h_b to compare with pass 1 (>= 0), or nullptr
@@ -69,8 +65,7 @@ void launch_stress_mag(const Params &p, cudaStream_t stream);
 void launch_assemble(const Params &p, cudaStream_t stream);
 void launch_smooth(const Params &p, double *fld, double *scratch, cudaStream_t stream);
 void launch_momentum(const Params &p, double dt, cudaStream_t stream);
-// -sum of h over each column, accumulated k = 1..nz as vdiff's z_clear does (into p.zcol when set),
-// and the FP32 (h, kv) pairs of the mixed momentum solve (into p.hk32 when set)
+// -sum of h over each column, accumulated k = 1..nz as vdiff's z_clear does (into p.zcol)
 void launch_column_depth(const Params &p, cudaStream_t stream);
 void launch_tracers(const Params &p, double dt, bool diffuse, bool nonlocal, cudaStream_t stream);
 // mixed-precision solves (vphys_mixed.cu), dispatched by the two above when cfg.mixed_precision

@@ -34,8 +34,7 @@
 // loads of a pass are issued MP_TR_U levels ahead of the arithmetic.
 //
 // Momentum: one thread per u or v face column; t and v in shared memory, the
-// velocity read again from L2 (evict_last) by the back-substitution; h and kv
-// of the two cells come as one FP32 pair per cell and level (k_column_depth).
+// velocity read again from L2 (evict_last) by the back-substitution.
 #include <cuda_runtime.h>
 
 #include <cstdlib>
@@ -452,8 +451,8 @@ __device__ __forceinline__ void solve_face_mp(const Params &p, double dt, int i,
     }
     const double *__restrict__ hl = p.h + cl;
     const double *__restrict__ hr = p.h + cr;
-    const float2 *__restrict__ pl = p.hk32 + cl;   // (h, kv) of the two cells, FP32 (k_column_depth)
-    const float2 *__restrict__ pr = p.hk32 + cr;
+    const double *__restrict__ kvl = p.kv + cl;
+    const double *__restrict__ kvr = p.kv + cr;
     const int *ktp = XF ? p.k_top_u : p.k_top_v;
     const int *kbp = XF ? p.k_bot_u : p.k_bot_v;
     const int kb = kbp ? min(max(kbp[f], 1), nz) : 1;
@@ -479,8 +478,8 @@ __device__ __forceinline__ void solve_face_mp(const Params &p, double dt, int i,
     }
     float hv_p, zi_p;
     double u_c = ld_hint(uf, pol_keep), u_m = 0.0;
-    face_layer<float>(c, __ldg(pl).x, __ldg(pr).x, (float)u_c, 1, kb, d_min, i_hbbl, zacc, zcol_l, zcol_r, hv_p,
-                      zi_p);
+    face_layer<float>(c, (float)__ldg(hl), (float)__ldg(hr), (float)u_c, 1, kb, d_min, i_hbbl, zacc, zcol_l, zcol_r,
+                      hv_p, zi_p);
     float num_t = 0.0f, dz_t = 1.0f;
     bool cut_t = false;
     const float lam = (c.implicit_drag && !c.bbl_glue) ? (float)(XF ? p.lambda_bot_u : p.lambda_bot_v)[f] : 0.0f;
@@ -494,15 +493,16 @@ __device__ __forceinline__ void solve_face_mp(const Params &p, double dt, int i,
     float f_prev = 0.0f, q_prev = 1.0f, t_prev = 0.0f;
     double w = 0.0, wr = 0.0;
     for (int k0 = 1; k0 <= nz; k0 += MP_MOM_U) {
-        float2 pln[MP_MOM_U], prn[MP_MOM_U];
-        double un[MP_MOM_U];
+        double hln[MP_MOM_U], hrn[MP_MOM_U], un[MP_MOM_U], kvln[MP_MOM_U], kvrn[MP_MOM_U];
 #pragma unroll
         for (int q = 0; q < MP_MOM_U; ++q) {
             const int k = k0 + q;
             if (k < nz) {
                 const size_t o = P * (size_t)k;
-                pln[q] = __ldg(pl + o);
-                prn[q] = __ldg(pr + o);
+                hln[q] = __ldg(hl + o);
+                hrn[q] = __ldg(hr + o);
+                kvln[q] = __ldg(kvl + o);
+                kvrn[q] = __ldg(kvr + o);
                 un[q] = ld_hint(uf + PF * (size_t)k, pol_keep);
             }
         }
@@ -516,11 +516,11 @@ __device__ __forceinline__ void solve_face_mp(const Params &p, double dt, int i,
             double u_p = 0.0;
             if (k < nz) {
                 u_p = un[q];
-                face_layer<float>(c, pln[q].x, prn[q].x, (float)u_p, k + 1, kb, d_min, i_hbbl, zacc, zcol_l, zcol_r,
-                                  hv_p, zi_p);
+                face_layer<float>(c, (float)hln[q], (float)hrn[q], (float)u_p, k + 1, kb, d_min, i_hbbl, zacc,
+                                  zcol_l, zcol_r, hv_p, zi_p);
                 if (k >= kb_live && k <= ktop)
-                    interface_coupling<float>(c, hv_0, hv_p, zi_0, dtf, kv_bbl, bbl_thick, pln[q].y, prn[q].y, num_t,
-                                              dz_t, cut_t);
+                    interface_coupling<float>(c, hv_0, hv_p, zi_0, dtf, kv_bbl, bbl_thick, (float)kvln[q],
+                                              (float)kvrn[q], num_t, dz_t, cut_t);
             }
             // the row in conservative form (row k of the reference times hf_k)
             const float H = fmx(hv_0, (float)H_VANISHED);
