@@ -150,18 +150,23 @@ class ClockSampler:
 
 
 def traffic_from_profiles(kernel: str):
-    """dram bytes per launch of `kernel` from the committed ncu summary, if any."""
+    """dram bytes per launch of `kernel` ("a+b": the sum over the stage's
+    launches) from the committed ncu summary, if every one is there."""
     p = ROOT / "profiles" / "traffic.txt"
     if not p.exists():
         return None
+    table = {}
     for line in p.read_text().splitlines():
         parts = line.split()
-        if len(parts) >= 2 and parts[0] == kernel:
+        if len(parts) >= 2 and not parts[0].startswith("#"):
             try:
-                return float(parts[1])
+                table[parts[0]] = float(parts[1])
             except ValueError:
-                return None
-    return None
+                pass
+    names = kernel.split("+")
+    if not all(n in table for n in names):
+        return None
+    return sum(table[n] for n in names)
 
 
 # ---------------------------------------------------------------------------
@@ -397,8 +402,9 @@ def main():
         stage_ms[name] = a.elapsed_time(b) / reps
     bpc = bytes_per_cell(ntr, nz)
     kernel_of = {"eos": "k_eos_wright", "assemble": "k_assemble",
-                 "momentum": "k_momentum_mp" if mixed else "k_momentum",
-                 "tracers": "k_tracers_mp" if mixed else "k_tracers"}
+                 # the stage's launches: the column-depth pass and the face solve
+                 "momentum": "k_column_depth+k_momentum_mp" if mixed else "k_column_depth+k_momentum",
+                 "tracers": "k_spans+k_tracers_mp" if mixed else "k_tracers"}
     dom = max(("assemble", "momentum", "tracers", "eos"), key=lambda k: stage_ms[k])
     peak, peak_kind = peaks()
     achieved = bpc[dom] * cells / (stage_ms[dom] / 1e3) / 1e9
