@@ -115,6 +115,14 @@ __global__ void k_stress_mag(const Params p, double *out)
 // Coefficient assembly: one thread per cell column.
 // ---------------------------------------------------------------------------
 constexpr int ASM_THREADS = 128;
+// Layers per load block of the FP32 interface sweep (1440x1080x75: 1.97 ms
+// loading each layer when its interface needs it, 1.60 ms with 2, more
+// with 3, 4 or 8 whose registers cost warps).  The FP64 sweep keeps the
+// on-demand loads: its exact divisions already cover the load latency, and
+// blocks measured slower (2.65 -> 2.75 ms with 2).
+#ifndef VPHYS_ASM_U_F
+#define VPHYS_ASM_U_F 2
+#endif
 
 template <typename R>
 __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
@@ -290,130 +298,172 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
     R kdb_depth = 0, kdb_cached = 0;
     bool kdb_valid = false;
     unsigned bad = 0;
-    for (int q = nz; q >= 1; --q) {
-        depth = depth + h_c;
-        if (q <= k_sfc) d_run = d_run + h_c;
-        R kvq = 0, ktq = 0, kdb = 0;
-        R h_m = 0;
-        double r_m = 0, uc_m = 0, vc_m = 0;
-        bool have_m = false;
-        if (q >= 2) {
-            h_m = (R)HH(q - 1);
-            if (c.bkgnd_profile) {
-                if (!(kdb_valid && depth == kdb_depth)) {
-                    kdb_cached = kd_sfc + (kd_deep - kd_sfc) * (R(0.5) + ratan(rdiv(depth - z0, bdelta)) * inv_pi);
-                    kdb_depth = depth;
-                    kdb_valid = true;
+    // FP32 (PREF): the sweep's loads come ASM_U layers at a time, issued
+    // before the block's arithmetic, so a column waits on memory once per
+    // block instead of once per layer.  Layer values are read only from
+    // k_lo - 1 up (k_lo: the lowest layer with h > 0): an interface q reads
+    // layers q and q-1 only when h_{q-1} + h_q > 0, so no needed layer lies
+    // lower, and the 0-thickness fillers under the bathymetry and land columns
+    // load nothing.  The loaded values are the same either way.
+    constexpr bool PREF = sizeof(R) == sizeof(float);
+    constexpr int ASM_U = PREF ? VPHYS_ASM_U_F : 1;
+    int k_lo = nz + 2;
+    if (PREF && !all_zero) {
+        for (int k0 = 1; k0 <= nz && k_lo > nz; k0 += 8) {
+            double hv[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) hv[u] = (k0 + u <= nz) ? HH(k0 + u) : 0.0;
+#pragma unroll
+            for (int u = 7; u >= 0; --u)
+                if (hv[u] > 0.0) k_lo = k0 + u;
+        }
+    }
+    const int k_need = k_lo - 1;
+    for (int q0 = nz; q0 >= 1; q0 -= ASM_U) {
+        double hb[ASM_U], rb[ASM_U], ub0[ASM_U], ub1[ASM_U], vb0[ASM_U], vb1[ASM_U];   // layer q0-1-u
+#pragma unroll
+        for (int u = 0; u < ASM_U; ++u) {
+            const int L = q0 - 1 - u;
+            hb[u] = rb[u] = ub0[u] = ub1[u] = vb0[u] = vb1[u] = 0.0;
+            if (PREF && L >= 1) {
+                hb[u] = HH(L);
+                if (L >= k_need) {
+                    rb[u] = RR(L);
+                    ub0[u] = __ldg(up + PU * (size_t)(L - 1));
+                    ub1[u] = __ldg(up + PU * (size_t)(L - 1) + 1);
+                    vb0[u] = __ldg(vp + PV * (size_t)(L - 1));
+                    vb1[u] = __ldg(vp + PV * (size_t)(L - 1) + nx);
                 }
-                kdb = kdb_cached;
-            }
-            const R dz_face = R(0.5) * (h_m + h_c);
-            const bool need_layers = (pp81 && !(dz_face <= R(0))) || (c.conv_enable && !(dz_face <= HV));
-            if (need_layers) {
-                if (!have_c) {
-                    r_c = RR(q);
-                    uc_c = UC(q);
-                    vc_c = VC(q);
-                    have_c = true;
-                }
-                r_m = RR(q - 1);
-                uc_m = UC(q - 1);
-                vc_m = VC(q - 1);
-                have_m = true;
-            }
-            if (pp81) {
-                // ---- PP81 (rdb_ocean_vmix.F90:1046-1073) ----
-                if (dz_face <= R(0)) {
-                    kvq = nu_bg;
-                    ktq = kap_bg;
-                } else {
-                    const auto rdz = rcp_of(dz_face);
-                    const R du_dz = qdiv((R)(uc_c - uc_m), rdz);
-                    const R dv_dz = qdiv((R)(vc_c - vc_m), rdz);
-                    const R shear2 = fmx(du_dz * du_dz + dv_dz * dv_dz, shear2_floor);
-                    const R n2 = -rdiv(G * (R)(r_c - r_m), r0 * dz_face);
-                    const R ri = rdiv(n2, shear2);
-                    const R denom = R(1) + alpha81 * fmx(ri, R(0));
-                    const R ri_factor = rdiv(R(1), denom * denom);
-                    kvq = nu_bg + nu0 * ri_factor;
-                    ktq = kap_bg + rdiv(nu0 * ri_factor, denom);
-                }
-            } else if (c.bkgnd_profile) {
-                // ---- interior "none" seed (rdb_ocean_vmix.F90:779-797) ----
-                kvq = pr_bl * kdb;
-                ktq = kdb;
-            } else {
-                kvq = kv_floor_scalar;
-                ktq = kt_bg;
             }
         }
-        // ---- KPP overlay (rdb_ocean_vmix.F90:1496-1514) ----
-        R gt = 0, gs = 0;
-        if (kpp_active && q > 1 && q <= k_sfc && d_run < hbR) {
-            const R sigma = rdiv(d_run, hbR);
-            const R g_shape = sigma * (R(1) - sigma) * (R(1) - sigma);
-            const R kv_kpp = hbR * wsR * g_shape;
-            kvq = fmx(kvq, kv_kpp);
-            ktq = fmx(ktq, kv_kpp);
-            if (destabilizing) {
-                const R gamma_factor = cs * g_shape;
-                gt = gamma_factor * qT;
-                gs = gamma_factor * qS;
-            }
-        }
-        if (q >= 2) {
-            // ---- KV_ML_INVZ2 (rdb_ocean_vmix.F90:1757-1765) ----
-            if (invz2_on) {
-                if (depth >= hmix) {
-                    invz2_on = false;
-                } else {
-                    const R zz = fmx(depth, dz_min_safe);
-                    kvq = kvq + rdiv(invz2 * hmix_sq, zz * zz);
+#pragma unroll
+        for (int u = 0; u < ASM_U; ++u) {
+            const int q = q0 - u;
+            if (q < 1) break;
+            depth = depth + h_c;
+            if (q <= k_sfc) d_run = d_run + h_c;
+            R kvq = 0, ktq = 0, kdb = 0;
+            R h_m = 0;
+            double r_m = 0, uc_m = 0, vc_m = 0;
+            bool have_m = false;
+            if (q >= 2) {
+                h_m = PREF ? (R)hb[u] : (R)HH(q - 1);
+                if (c.bkgnd_profile) {
+                    if (!(kdb_valid && depth == kdb_depth)) {
+                        kdb_cached = kd_sfc + (kd_deep - kd_sfc) * (R(0.5) + ratan(rdiv(depth - z0, bdelta)) * inv_pi);
+                        kdb_depth = depth;
+                        kdb_valid = true;
+                    }
+                    kdb = kdb_cached;
                 }
-            }
-            // ---- convection (rdb_ocean_vmix.F90:1835-1848) ----
-            if (c.conv_enable) {
                 const R dz_face = R(0.5) * (h_m + h_c);
-                if (!(dz_face <= HV) && !(depth < hbR)) {
-                    const R n2 = -rdiv(G * (R)(r_c - r_m), r0 * dz_face);
-                    if (n2 < conv_n2) {
-                        ktq = fmx(ktq, conv_kd);
-                        kvq = fmx(kvq, conv_pr * conv_kd);
+                const bool need_layers = (pp81 && !(dz_face <= R(0))) || (c.conv_enable && !(dz_face <= HV));
+                if (need_layers) {
+                    if (!have_c) {
+                        r_c = RR(q);
+                        uc_c = UC(q);
+                        vc_c = VC(q);
+                        have_c = true;
+                    }
+                    r_m = PREF ? rb[u] : RR(q - 1);
+                    uc_m = PREF ? 0.5 * (ub0[u] + ub1[u]) : UC(q - 1);
+                    vc_m = PREF ? 0.5 * (vb0[u] + vb1[u]) : VC(q - 1);
+                    have_m = true;
+                }
+                if (pp81) {
+                    // ---- PP81 (rdb_ocean_vmix.F90:1046-1073) ----
+                    if (dz_face <= R(0)) {
+                        kvq = nu_bg;
+                        ktq = kap_bg;
+                    } else {
+                        const auto rdz = rcp_of(dz_face);
+                        const R du_dz = qdiv((R)(uc_c - uc_m), rdz);
+                        const R dv_dz = qdiv((R)(vc_c - vc_m), rdz);
+                        const R shear2 = fmx(du_dz * du_dz + dv_dz * dv_dz, shear2_floor);
+                        const R n2 = -rdiv(G * (R)(r_c - r_m), r0 * dz_face);
+                        const R ri = rdiv(n2, shear2);
+                        const R denom = R(1) + alpha81 * fmx(ri, R(0));
+                        const R ri_factor = rdiv(R(1), denom * denom);
+                        kvq = nu_bg + nu0 * ri_factor;
+                        ktq = kap_bg + rdiv(nu0 * ri_factor, denom);
+                    }
+                } else if (c.bkgnd_profile) {
+                    // ---- interior "none" seed (rdb_ocean_vmix.F90:779-797) ----
+                    kvq = pr_bl * kdb;
+                    ktq = kdb;
+                } else {
+                    kvq = kv_floor_scalar;
+                    ktq = kt_bg;
+                }
+            }
+            // ---- KPP overlay (rdb_ocean_vmix.F90:1496-1514) ----
+            R gt = 0, gs = 0;
+            if (kpp_active && q > 1 && q <= k_sfc && d_run < hbR) {
+                const R sigma = rdiv(d_run, hbR);
+                const R g_shape = sigma * (R(1) - sigma) * (R(1) - sigma);
+                const R kv_kpp = hbR * wsR * g_shape;
+                kvq = fmx(kvq, kv_kpp);
+                ktq = fmx(ktq, kv_kpp);
+                if (destabilizing) {
+                    const R gamma_factor = cs * g_shape;
+                    gt = gamma_factor * qT;
+                    gs = gamma_factor * qS;
+                }
+            }
+            if (q >= 2) {
+                // ---- KV_ML_INVZ2 (rdb_ocean_vmix.F90:1757-1765) ----
+                if (invz2_on) {
+                    if (depth >= hmix) {
+                        invz2_on = false;
+                    } else {
+                        const R zz = fmx(depth, dz_min_safe);
+                        kvq = kvq + rdiv(invz2 * hmix_sq, zz * zz);
+                    }
+                }
+                // ---- convection (rdb_ocean_vmix.F90:1835-1848) ----
+                if (c.conv_enable) {
+                    const R dz_face = R(0.5) * (h_m + h_c);
+                    if (!(dz_face <= HV) && !(depth < hbR)) {
+                        const R n2 = -rdiv(G * (R)(r_c - r_m), r0 * dz_face);
+                        if (n2 < conv_n2) {
+                            ktq = fmx(ktq, conv_kd);
+                            kvq = fmx(kvq, conv_pr * conv_kd);
+                        }
                     }
                 }
             }
-        }
-        // ---- split ks := kt, then the gate on interior interfaces ----
-        R ksq = ktq;
-        if (q >= 2 && q <= nz) {
-            if (c.vmix_guard) {
-                bad += (kvq < R(0) || kvq != kvq);
-                bad += (ktq < R(0) || ktq != ktq);
-                bad += (ksq < R(0) || ksq != ksq);
+            // ---- split ks := kt, then the gate on interior interfaces ----
+            R ksq = ktq;
+            if (q >= 2 && q <= nz) {
+                if (c.vmix_guard) {
+                    bad += (kvq < R(0) || kvq != kvq);
+                    bad += (ktq < R(0) || ktq != ktq);
+                    bad += (ksq < R(0) || ksq != ksq);
+                }
+                if (c.bkgnd_profile) {
+                    kvq = fmn(fmx(kvq, pr_bl * kdb), kv_max);
+                    ktq = fmn(fmx(ktq, kdb), kd_max);
+                    ksq = fmn(fmx(ksq, kdb), kd_max);
+                } else {
+                    kvq = fmn(fmx(kvq, kv_floor_scalar), kv_max);
+                    ktq = fmn(fmx(ktq, kt_bg), kd_max);
+                    ksq = fmn(fmx(ksq, ks_bg), kd_max);
+                }
             }
-            if (c.bkgnd_profile) {
-                kvq = fmn(fmx(kvq, pr_bl * kdb), kv_max);
-                ktq = fmn(fmx(ktq, kdb), kd_max);
-                ksq = fmn(fmx(ksq, kdb), kd_max);
-            } else {
-                kvq = fmn(fmx(kvq, kv_floor_scalar), kv_max);
-                ktq = fmn(fmx(ktq, kt_bg), kd_max);
-                ksq = fmn(fmx(ksq, ks_bg), kd_max);
+            const size_t off = P * (size_t)(q - 1);
+            kvp[off] = (double)kvq;
+            ktp[off] = (double)ktq;
+            ksp[off] = (double)ksq;
+            if (p.write_gamma) {
+                p.gamma_t[col + off] = (double)gt;
+                p.gamma_s[col + off] = (double)gs;
             }
+            h_c = h_m;
+            r_c = r_m;
+            uc_c = uc_m;
+            vc_c = vc_m;
+            have_c = have_m;
         }
-        const size_t off = P * (size_t)(q - 1);
-        kvp[off] = (double)kvq;
-        ktp[off] = (double)ktq;
-        ksp[off] = (double)ksq;
-        if (p.write_gamma) {
-            p.gamma_t[col + off] = (double)gt;
-            p.gamma_s[col + off] = (double)gs;
-        }
-        h_c = h_m;
-        r_c = r_m;
-        uc_c = uc_m;
-        vc_c = vc_m;
-        have_c = have_m;
     }
     if (bad) atomicAdd(p.guard_count, (unsigned long long)bad);
 #undef HH
