@@ -521,7 +521,10 @@ __global__ void k_smooth(const Params p, double *__restrict__ fld, const double 
 #endif
 constexpr int MOM_THREADS = VPHYS_MOM_THREADS;   // face columns per block (c' of each in shared memory)
 
-constexpr int MOM_U = 4;   // levels per load block
+#ifndef VPHYS_MOM_U
+#define VPHYS_MOM_U 4
+#endif
+constexpr int MOM_U = VPHYS_MOM_U;   // levels per load block
 
 // diffuse_velocity_columns_impl for one face column (rdb_ocean_vdiff.F90:1611-1925).
 // The Thomas c' of every level sits in shared memory (cpp[(k-1)*bs]); the

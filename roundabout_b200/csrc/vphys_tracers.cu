@@ -80,7 +80,15 @@ template <int NTR, bool TWO>
 __device__ __forceinline__ void tracer_columns(const Params &p, double dt, int diffuse, int nonlocal, int i, int j,
                                                double *smem, int tid, int bs)
 {
-    constexpr int TR_U = NTR <= 4 ? 4 : (NTR <= 8 ? 2 : 1);   // levels per load block
+    // levels per load block: 2 up to 8 tracers, else 1 (1440x1080x75, 4
+    // tracers: 5.25 ms with 4, 4.18 with 2, 4.37 with 1 -- the larger
+    // unrolled body costs more in instruction-cache misses and registers than
+    // the deeper prefetch gains)
+#ifdef VPHYS_TR_U
+    constexpr int TR_U = VPHYS_TR_U;
+#else
+    constexpr int TR_U = NTR <= 8 ? 2 : 1;
+#endif
     const vphys_config &c = p.cfg;
     const int nx = p.nx, nz = p.nz, ntr = p.ntr;
     const size_t P = p.plane;
