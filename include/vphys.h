@@ -153,8 +153,23 @@ typedef struct vphys_config {
                                  the Wright EOS at the first live layer's (T, S) and eos_p_ref
                                  (eos_buoyancy_coeffs, rdb_eos.F90:1624-1736; the constants on a vanished
                                  surface layer) */
-    int pad0;
+    int kpp_sw_method;        /* which shortwave KPP's B0 charges (kpp_sw_method, rdb_ocean_vmix.F90:132-136,
+                                 335): VPHYS_KPP_SW_ALL 1 (all of Q_heat), _MXL 2 (default: Q_heat minus the
+                                 penetrating part that passes the boundary layer), _LV1 (minus what passes
+                                 the surface layer); read only when sw_pen_frac != 0 */
+    /* two-band shortwave penetration (ocean_surface_flux_t, rdb_ocean_surface_flux.F90:229-258):
+     * the penetrating irradiance I0 = sw_pen_frac * Q_heat, transmission
+     * T(d) = R exp(-d/zeta1) + (1-R) exp(-d/zeta2).  sw_pen_frac = 0 (default)
+     * turns both the KPP correction and the deposit off. */
+    double sw_pen_frac;       /* 0 */
+    double sw_band_ratio;     /* R, 0.58 */
+    double sw_zeta1;          /* m, 0.35 */
+    double sw_zeta2;          /* m, 23 */
 } vphys_config;
+
+#define VPHYS_KPP_SW_ALL 1
+#define VPHYS_KPP_SW_MXL 2
+#define VPHYS_KPP_SW_LV1 3
 
 /* ---- field ids (vphys_bind / vphys_set_field / vphys_get_field) ----- */
 enum vphys_field {
@@ -260,6 +275,18 @@ int vphys_stress_mag(vphys_handle h);
  * after the EOS at rdb_ocean_dyn.F90:1363; vphys_step runs it there when
  * surface_flux is 1. */
 int vphys_surface_flux(vphys_handle h, double dt);
+
+/* The penetrating shortwave moved down the column after the surface
+ * deposit: I0 = sw_pen_frac * Q_HEAT * WET leaves the first live layer and
+ * each live layer takes I0 (T(d_top) - T(d_bottom)) * dt/(rho0 cp), the
+ * deepest live layer the rest (an opaque bed); vanished layers pass the light
+ * on.  Column heat is unchanged; HEAT_BUDGET_SURFACE books the moves when
+ * budgets are on.  A no-op when sw_pen_frac is 0 or there is no temperature
+ * tracer.  Replaces ocean_surface_flux_apply_sw_penetration with
+ * apply_sw_penetration_impl (rdb_ocean_surface_flux.F90:1255-1530), called
+ * at rdb_ocean_dyn.F90:1375 right after the surface deposit; vphys_step runs
+ * it there when surface_flux is 1. */
+int vphys_sw_penetration(vphys_handle h, double dt);
 
 /* Mixed-precision tracer solves (mixed_precision >= 1): the number of
  * (32-column group, tracer) pairs whose one-step increment reached 2 units

@@ -51,6 +51,8 @@ def lib():
         L.vpo_sm_cbrt.argtypes = [ctypes.c_double]
         L.vpo_sm_atan.restype = ctypes.c_double
         L.vpo_sm_atan.argtypes = [ctypes.c_double]
+        L.vpo_sm_exp.restype = ctypes.c_double
+        L.vpo_sm_exp.argtypes = [ctypes.c_double]
         L.vpo_set_threads.argtypes = [ctypes.c_int]
         L.vpo_get_threads.restype = ctypes.c_int
         for name in ("vpo_eos_wright", "vpo_pp81", "vpo_seed_interior_none", "vpo_kpp_overlay",
@@ -61,7 +63,8 @@ def lib():
         for name in ("vpo_assemble_gate", "vpo_build_coefficients"):
             getattr(L, name).argtypes = [ctypes.c_void_p, ctypes.POINTER(VpoState)]
             getattr(L, name).restype = ctypes.c_int
-        for name in ("vpo_vdiff_momentum", "vpo_vdiff_tracers", "vpo_nonlocal", "vpo_surface_flux"):
+        for name in ("vpo_vdiff_momentum", "vpo_vdiff_tracers", "vpo_nonlocal", "vpo_surface_flux",
+                     "vpo_sw_penetration"):
             getattr(L, name).argtypes = [ctypes.c_void_p, ctypes.POINTER(VpoState), ctypes.c_double]
             getattr(L, name).restype = None
         L.vpo_eos_buoyancy_coeffs.argtypes = [ctypes.c_double] * 3 + [ctypes.POINTER(ctypes.c_double)] * 2
@@ -168,6 +171,10 @@ def sm_cbrt(x: float) -> float:
 
 def sm_atan(x: float) -> float:
     return lib().vpo_sm_atan(float(x))
+
+
+def sm_exp(x: float) -> float:
+    return lib().vpo_sm_exp(float(x))
 
 
 def eos_buoyancy_coeffs(T: float, S: float, p: float):

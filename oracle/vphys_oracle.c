@@ -72,6 +72,38 @@ static const double SM_PIO6_HI = 0.52359877559829892668;
 static const double SM_PIO6_LO = -5.3604088322554549242e-17;
 static const double SM_TAN_PIO12 = 0.2679491924311226958;
 
+/* rdb_sm_exp (rdb_safe_math_core.inc:81-137) with its constants
+ * (rdb_safe_math_consts.inc:39-52): k = nearest integer to x/ln2 (halves away
+ * from zero), r = x - k ln2 with ln2 split so k*LN2_HI is exact, degree-13
+ * Taylor polynomial (coefficients 1/i!), scaled by 2**k; results below the
+ * smallest normal are exactly 0. */
+static const double SM_LN2_HI = 0.69314718060195446014;
+static const double SM_LN2_LO = -4.2009150726810845979e-11;
+static const double SM_INV_LN2 = 1.442695040888963387;
+static const double SM_EXP_MAX = 709.78271289338399679;
+static const double SM_EXP_MIN = -745.1332191019412;
+static const double SM_EXP_C[14] = {1.0,           1.0,              1.0 / 2.0,         1.0 / 6.0,
+                                    1.0 / 24.0,    1.0 / 120.0,      1.0 / 720.0,       1.0 / 5040.0,
+                                    1.0 / 40320.0, 1.0 / 362880.0,   1.0 / 3628800.0,   1.0 / 39916800.0,
+                                    1.0 / 479001600.0, 1.0 / 6227020800.0};
+
+double vpo_sm_exp(double x)
+{
+    if (isnan(x)) return x;
+    if (x > SM_EXP_MAX) return INFINITY;
+    if (x < SM_EXP_MIN) return 0.0;
+    double kr = round(x * SM_INV_LN2);
+    int k = (int)kr;
+    double r = x - kr * SM_LN2_HI;
+    r = r - kr * SM_LN2_LO;
+    r = r + 0.0;
+    double p = SM_EXP_C[13];
+    for (int i = 12; i >= 0; --i) p = p * r + SM_EXP_C[i];
+    double y = (k > 1000) ? 2.0 * ldexp(p, k - 1) : ldexp(p, k);
+    if (y < DBL_MIN) y = 0.0;
+    return y;
+}
+
 static inline double sm_flush(double r)
 {
     /* rdb_sm_flush (rdb_safe_math_core.inc:40-51) */
@@ -315,6 +347,31 @@ static inline double kpp_b0(double alpha_T, double beta_S, double rho0, double q
     return (GRAVITY / rho0) * (alpha_T * qT - beta_S * qS);
 }
 
+/* sw_transmission (rdb_ocean_surface_flux.F90:1401-1415): the two-band
+ * normalised downward irradiance at depth d, R e^(-d/zeta1) + (1-R) e^(-d/zeta2). */
+static inline double sw_transmission(const vphys_config *c, double d)
+{
+    return c->sw_band_ratio * vpo_sm_exp(-d / c->sw_zeta1) + (1.0 - c->sw_band_ratio) * vpo_sm_exp(-d / c->sw_zeta2);
+}
+
+/* The kinematic heat flux B0 charges (rdb_ocean_vmix.F90:1321-1348 in pass 1
+ * with the lagged h_b, 1440-1466 in pass 2 with the new one): with
+ * shortwave penetration on, Q_heat minus the penetrating part that passes
+ * the boundary layer (MXL) or the surface layer (LV1); all of it otherwise. */
+static inline double kpp_q_t_kin(const vphys_config *c, const vpo_state *s, int i, int j, int k_sfc, double h_b)
+{
+    const int nx = s->nx, ny = s->ny;
+    if (c->sw_pen_frac != 0.0) {
+        double q_bl = C2(s->q_heat, i, j);
+        if (c->kpp_sw_method == VPHYS_KPP_SW_MXL)
+            q_bl = q_bl - c->sw_pen_frac * C2(s->q_heat, i, j) * sw_transmission(c, h_b);
+        else if (c->kpp_sw_method == VPHYS_KPP_SW_LV1)
+            q_bl = q_bl - c->sw_pen_frac * C2(s->q_heat, i, j) * sw_transmission(c, C3(s->h, i, j, k_sfc));
+        return q_bl / (c->rho0 * c->cp);
+    }
+    return C2(s->q_heat, i, j) / (c->rho0 * c->cp);
+}
+
 /* The coefficient pair of B0 (rdb_ocean_vmix.F90:1357-1376, 1469-1488): the
  * constants, or with buoyancy_coeffs = "eos" the Wright derivatives at the
  * first live layer's (T, S) and p_ref when that layer is live. */
@@ -354,7 +411,7 @@ void vpo_kpp_overlay(const vphys_config *c, vpo_state *s)
             double tau_mag = C2(s->stress_mag, i, j);
             double u_star = sqrt(tau_mag / rho0);
             double h_b_lagged = C2(s->bl_depth, i, j);
-            double q_T_kin = C2(s->q_heat, i, j) / (rho0 * c->cp);
+            double q_T_kin = kpp_q_t_kin(c, s, i, j, k_sfc, h_b_lagged);
             double q_S_kin = C2(s->q_salt, i, j) / rho0;
             double B_0 = kpp_b0_col(c, s, i, j, k_sfc, q_T_kin, q_S_kin);
             double wstar3_lagged = fmx(0.0, -B_0) * h_b_lagged;
@@ -404,7 +461,7 @@ void vpo_kpp_overlay(const vphys_config *c, vpo_state *s)
             double tau_mag = C2(s->stress_mag, i, j);
             double u_star = sqrt(tau_mag / rho0);
             double h_b = C2(s->bl_depth, i, j);
-            double q_T_kin = C2(s->q_heat, i, j) / (rho0 * c->cp);
+            double q_T_kin = kpp_q_t_kin(c, s, i, j, k_sfc, h_b);
             double q_S_kin = C2(s->q_salt, i, j) / rho0;
             double B_0 = kpp_b0_col(c, s, i, j, k_sfc, q_T_kin, q_S_kin);
             C2(s->b0, i, j) = B_0;
@@ -1025,12 +1082,59 @@ void vpo_surface_flux(const vphys_config *c, vpo_state *s, double dt)
     }
 }
 
+/* ocean_surface_flux_apply_sw_penetration -> apply_sw_penetration_impl
+ * (rdb_ocean_surface_flux.F90:1255-1370, 1451-1530) with k_top = nz and
+ * k_bot = 1: the penetrating part I0 of the surface lump leaves the first
+ * live layer and is spread as I0 (T(d_top) - T(d_bottom)) over the live
+ * layers, the deepest live layer taking the rest (opaque bed); vanished
+ * layers pass the light on. */
+void vpo_sw_penetration(const vphys_config *c, vpo_state *s, double dt)
+{
+    if (c->sw_pen_frac == 0.0 || c->idx_temperature < 0) return;
+    const int nx = s->nx, ny = s->ny, nz = s->nz;
+    const double inv_scale = dt / (c->rho0 * c->cp);
+    double *T = s->tr[c->idx_temperature];
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int j = 1; j <= ny; ++j) {
+        for (int i = 1; i <= nx; ++i) {
+            const int kt = first_live(s->h, nx, ny, i, j, nz);
+            const double i0col = c->sw_pen_frac * C2(s->q_heat, i, j) * C2(s->wet, i, j);
+            int k_dep = 1;
+            for (int k = 1; k <= nz; ++k) {
+                if (C3(s->h, i, j, k) > H_VANISHED) {
+                    k_dep = k;
+                    break;
+                }
+            }
+            double d_top = 0.0;
+            double trans_top = sw_transmission(c, d_top);
+            for (int k = nz; k >= k_dep; --k) {
+                const double hk = C3(s->h, i, j, k);
+                const double d_bot = d_top + hk;
+                const double trans_bot = (k > k_dep) ? sw_transmission(c, d_bot) : 0.0;
+                if (hk > H_VANISHED) {
+                    const double absorbed = i0col * (trans_top - trans_bot);
+                    double add = inv_scale * absorbed;
+                    if (k == kt) add = add - inv_scale * i0col;
+                    C3(T, i, j, k) = conc_add_source(C3(T, i, j, k), hk, add);
+                    if (c->budgets) C3(s->heat_budget_surface, i, j, k) += add;
+                    trans_top = trans_bot;
+                }
+                d_top = d_bot;
+            }
+        }
+    }
+}
+
 int vpo_step(const vphys_config *c, vpo_state *s, double dt, int n_steps)
 {
     int st = 0;
     for (int n = 0; n < n_steps; ++n) {
         if (c->eos_in_step) vpo_eos_wright(c, s);
-        if (c->surface_flux) vpo_surface_flux(c, s, dt);
+        if (c->surface_flux) {
+            vpo_surface_flux(c, s, dt);
+            vpo_sw_penetration(c, s, dt);
+        }
         st |= vpo_build_coefficients(c, s);
         vpo_vdiff_momentum(c, s, dt);
         vpo_vdiff_tracers(c, s, dt);

@@ -64,6 +64,8 @@ void vpo_vdiff_tracers(const vphys_config *c, vpo_state *s, double dt);
 void vpo_nonlocal(const vphys_config *c, vpo_state *s, double dt);
 void vpo_surface_flux(const vphys_config *c, vpo_state *s, double dt);
 void vpo_eos_buoyancy_coeffs(double T, double S, double p, double *alpha_T, double *beta_S);
+double vpo_sm_exp(double x);
+void vpo_sw_penetration(const vphys_config *c, vpo_state *s, double dt);
 
 int vpo_step(const vphys_config *c, vpo_state *s, double dt, int n_steps);
 

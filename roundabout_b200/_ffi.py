@@ -125,11 +125,13 @@ class VphysConfig(ctypes.Structure):
         ("idx_temperature", ctypes.c_int), ("idx_salinity", ctypes.c_int), ("idx_pseudo_salt", ctypes.c_int),
         ("eos_in_step", ctypes.c_int), ("remnant", ctypes.c_int), ("budgets", ctypes.c_int),
         ("mixed_precision", ctypes.c_int), ("learned_kpp", ctypes.c_int),
-        ("buoyancy_coeffs", ctypes.c_int), ("pad0", ctypes.c_int),
+        ("buoyancy_coeffs", ctypes.c_int), ("kpp_sw_method", ctypes.c_int),
+        ("sw_pen_frac", ctypes.c_double), ("sw_band_ratio", ctypes.c_double), ("sw_zeta1", ctypes.c_double),
+        ("sw_zeta2", ctypes.c_double),
     ]
 
     def as_dict(self):
-        return {n: getattr(self, n) for n, _ in self._fields_ if n not in ("pad0",)}
+        return {n: getattr(self, n) for n, _ in self._fields_ if n not in ()}
 
 
 class LibraryNotFoundError(FileNotFoundError):
@@ -189,6 +191,7 @@ _PROTOTYPES = {
     "vphys_eos_wright": (ctypes.c_int, [ctypes.c_void_p]),
     "vphys_stress_mag": (ctypes.c_int, [ctypes.c_void_p]),
     "vphys_surface_flux": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    "vphys_sw_penetration": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "vphys_mixed_redo_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint)]),
     "vphys_assemble": (ctypes.c_int, [ctypes.c_void_p]),
     "vphys_vdiff_momentum": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),

@@ -32,6 +32,11 @@ def default_config() -> VphysConfig:
     c.conv_enable = 0
     c.surface_flux = 0
     c.buoyancy_coeffs = 0
+    c.kpp_sw_method = 2
+    c.sw_pen_frac = 0.0
+    c.sw_band_ratio = 0.58
+    c.sw_zeta1 = 0.35
+    c.sw_zeta2 = 23.0
     c.pp81_nu0 = 1.0e-2
     c.pp81_nu_bg = 1.0e-4
     c.pp81_kappa_bg = 1.0e-5

@@ -227,6 +227,12 @@ int validate(const vphys_config *c, int ntr)
         return push_error(VPHYS_ERR_CONFIG, "mixed_precision %d: 0 (FP64), 1 (mixed solves) or 2 (mixed solves and assembly)",
                           c->mixed_precision);
     if (c->surface_flux < 0 || c->surface_flux > 1) return push_error(VPHYS_ERR_CONFIG, "surface_flux must be 0 or 1");
+    if (c->sw_pen_frac != 0.0) {
+        if (c->kpp_sw_method < VPHYS_KPP_SW_ALL || c->kpp_sw_method > VPHYS_KPP_SW_LV1)
+            return push_error(VPHYS_ERR_CONFIG, "kpp_sw_method must be 1 (all), 2 (mxl) or 3 (lv1)");
+        if (!(c->sw_zeta1 > 0.0) || !(c->sw_zeta2 > 0.0))
+            return push_error(VPHYS_ERR_CONFIG, "sw_zeta1 and sw_zeta2 must be positive");
+    }
     if (c->buoyancy_coeffs < 0 || c->buoyancy_coeffs > 1)
         return push_error(VPHYS_ERR_CONFIG, "buoyancy_coeffs must be 0 (constant) or 1 (eos)");
     if (c->buoyancy_coeffs && c->use_kpp && (c->idx_temperature < 0 || c->idx_salinity < 0))
@@ -435,7 +441,7 @@ void free_kpp(vphys_handle h)
 int run_assemble(vphys_handle h, const Params &p);
 
 // The launches of n whole steps (vmix_apply_in_stage on a thermo step,
-// rdb_ocean_dyn.F90:1636-1900): EOS, [surface deposit], [learned KPP],
+// rdb_ocean_dyn.F90:1636-1900): EOS, [surface deposit + shortwave], [learned KPP],
 // assembly, momentum, tracers with the non-local tendency.  All asynchronous
 // on h->stream.
 int launch_steps(vphys_handle h, const Params &p, double dt, int n_steps)
@@ -445,7 +451,11 @@ int launch_steps(vphys_handle h, const Params &p, double dt, int n_steps)
     surface_flux_scales(h->cfg, dt, &inv_heat, &inv_salt);
     for (int n = 0; n < n_steps; ++n) {
         if (h->cfg.eos_in_step) vphys::launch_eos_wright(p, h->stream);
-        if (h->cfg.surface_flux) vphys::launch_surface_flux(p, inv_heat, inv_salt, h->stream);
+        if (h->cfg.surface_flux) {
+            vphys::launch_surface_flux(p, inv_heat, inv_salt, h->stream);
+            if (h->cfg.sw_pen_frac != 0.0 && h->cfg.idx_temperature >= 0)
+                vphys::launch_sw_penetration(p, inv_heat, h->stream);
+        }
         Params pa = p;
         if ((st = run_learned_kpp(h, pa))) return st;
         if ((st = run_assemble(h, pa))) return st;
@@ -538,6 +548,10 @@ int vphys_config_default(vphys_config *c)
     c->ri_crit = 0.3;
     c->cs_nonlocal = 6.3;
     c->c_vt2 = 1.8;
+    c->kpp_sw_method = VPHYS_KPP_SW_MXL;
+    c->sw_band_ratio = 0.58;
+    c->sw_zeta1 = 0.35;
+    c->sw_zeta2 = 23.0;
     c->alpha_T = 1.7e-4;
     c->beta_S = 7.6e-4;
     c->cp = 3992.0;
@@ -764,6 +778,19 @@ int vphys_surface_flux(vphys_handle h, double dt)
     Params p = make_params(h);
     vphys::launch_surface_flux(p, inv_heat, inv_salt, h->stream);
     return cuda_status(cudaGetLastError(), "vphys_surface_flux launch");
+}
+
+int vphys_sw_penetration(vphys_handle h, double dt)
+{
+    if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_sw_penetration: bad handle");
+    if (h->cfg.sw_pen_frac == 0.0 || h->cfg.idx_temperature < 0) return VPHYS_OK;
+    int st = prepare_surface_flux(h);
+    if (st) return st;
+    double inv_heat, inv_salt;
+    surface_flux_scales(h->cfg, dt, &inv_heat, &inv_salt);
+    Params p = make_params(h);
+    vphys::launch_sw_penetration(p, inv_heat, h->stream);
+    return cuda_status(cudaGetLastError(), "vphys_sw_penetration launch");
 }
 
 int vphys_mixed_redo_count(vphys_handle h, unsigned *groups)

@@ -118,6 +118,40 @@ __device__ __forceinline__ double sm_cbrt(double x)
     return x < 0.0 ? -y : y;
 }
 
+// ---- position-independent exponential: rdb_sm_exp
+// (rdb_safe_math_core.inc:81-137, constants rdb_safe_math_consts.inc:39-52):
+// k = nearest integer to x/ln2 (halves away from zero), r = x - k ln2 with
+// ln2 split so k*LN2_HI is exact, degree-13 Taylor polynomial (1/i!), 2**k;
+// results below the smallest normal are exactly 0.
+__device__ __forceinline__ double sm_exp(double x)
+{
+    if (isnan(x)) return x;
+    if (x > 709.78271289338399679) return __longlong_as_double(0x7ff0000000000000LL);
+    if (x < -745.1332191019412) return 0.0;
+    const double kr = round(x * 1.442695040888963387);
+    const int k = (int)kr;
+    double r = x - kr * 0.69314718060195446014;
+    r = r - kr * -4.2009150726810845979e-11;
+    r = r + 0.0;
+    double p = 1.0 / 6227020800.0;
+    p = p * r + 1.0 / 479001600.0;
+    p = p * r + 1.0 / 39916800.0;
+    p = p * r + 1.0 / 3628800.0;
+    p = p * r + 1.0 / 362880.0;
+    p = p * r + 1.0 / 40320.0;
+    p = p * r + 1.0 / 5040.0;
+    p = p * r + 1.0 / 720.0;
+    p = p * r + 1.0 / 120.0;
+    p = p * r + 1.0 / 24.0;
+    p = p * r + 1.0 / 6.0;
+    p = p * r + 1.0 / 2.0;
+    p = p * r + 1.0;
+    p = p * r + 1.0;
+    double y = (k > 1000) ? 2.0 * ldexp(p, k - 1) : ldexp(p, k);
+    if (y < DBL_TINY) y = 0.0;
+    return y;
+}
+
 // ---- position-independent arctangent: rdb_sm_atan
 // (rdb_safe_math_atan.inc:7-44, Cody & Waite reduction, fitted degree-11
 // polynomial of rdb_safe_math_consts.inc:85-89).
@@ -246,6 +280,30 @@ __device__ __forceinline__ double kpp_surface_b0(const vphys_config &c, double q
     double a = c.alpha_T, b = c.beta_S;
     if (c.buoyancy_coeffs && h_sfc > H_VANISHED) wright_buoyancy_coeffs(T_sfc, S_sfc, c.eos_p_ref, a, b);
     return (GRAVITY / c.rho0) * (a * q_T_kin - b * q_S_kin);
+}
+
+// sw_transmission (rdb_ocean_surface_flux.F90:1401-1415): the two-band
+// normalised downward irradiance at depth d.
+__device__ __forceinline__ double sw_transmission(const vphys_config &c, double d)
+{
+    return c.sw_band_ratio * sm_exp(xdiv(-d, c.sw_zeta1)) + (1.0 - c.sw_band_ratio) * sm_exp(xdiv(-d, c.sw_zeta2));
+}
+
+// The kinematic heat flux KPP's B0 charges (rdb_ocean_vmix.F90:1321-1348 in
+// pass 1 with the lagged h_b, 1440-1466 in pass 2 with the new one): with
+// shortwave penetration on, Q_heat minus the penetrating part that passes the
+// boundary layer (MXL) or the surface layer h_sfc (LV1).
+__device__ __forceinline__ double kpp_q_t_kin(const vphys_config &c, double q_heat, double h_b, double h_sfc)
+{
+    if (c.sw_pen_frac != 0.0) {
+        double q_bl = q_heat;
+        if (c.kpp_sw_method == VPHYS_KPP_SW_MXL)
+            q_bl = q_bl - c.sw_pen_frac * q_heat * sw_transmission(c, h_b);
+        else if (c.kpp_sw_method == VPHYS_KPP_SW_LV1)
+            q_bl = q_bl - c.sw_pen_frac * q_heat * sw_transmission(c, h_sfc);
+        return xdiv(q_bl, c.rho0 * c.cp);
+    }
+    return xdiv(q_heat, c.rho0 * c.cp);
 }
 
 }  // namespace vphys

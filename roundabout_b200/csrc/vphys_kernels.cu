@@ -10,6 +10,7 @@
 // Kernels (one launch each, all asynchronous):
 //   k_eos_wright   rho from (T, S)                     rdb_eos.F90:909-959
 //   k_surface_flux surface heat/salt deposit           rdb_ocean_surface_flux.F90:959-1230
+//   k_sw_penetration shortwave moved down the column   rdb_ocean_surface_flux.F90:1255-1530
 //   k_stress_mag   |tau| at cell centres               rdb_ocean_surface_stress.F90:858-875
 //   k_assemble     PP81 / seed, KPP passes 1 + 2, KV_ML_INVZ2, convection,
 //                  split, guard, Bryan-Lewis or scalar gate: every interface
@@ -100,6 +101,58 @@ __global__ void k_surface_flux(const Params p, double inv_heat, double inv_salt)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Shortwave penetration (ocean_surface_flux_apply_sw_penetration ->
+// apply_sw_penetration_impl, rdb_ocean_surface_flux.F90:1255-1370,
+// 1451-1530, with k_top = nz and k_bot = 1): the penetrating part
+// I0 = sw_pen_frac Q_heat wet of the surface lump leaves the first live layer
+// and each live layer takes I0 (T(d_top) - T(d_bottom)), the deepest live
+// layer the rest (opaque bed); vanished layers pass the light on.  One thread
+// per column.
+// ---------------------------------------------------------------------------
+__global__ void k_sw_penetration(const Params p, double inv_scale)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (i >= p.nx) return;
+    const vphys_config &c = p.cfg;
+    const int nz = p.nz;
+    const size_t col = (size_t)i + (size_t)p.nx * j;
+    const size_t P = p.plane;
+    const double *__restrict__ hp = p.h + col;
+    double *__restrict__ T = p.tr[c.idx_temperature] + col;
+    int kt = nz;
+    for (int k = nz; k >= 1; --k)
+        if (__ldg(hp + P * (size_t)(k - 1)) > H_VANISHED) {
+            kt = k;
+            break;
+        }
+    int k_dep = 1;
+    for (int k = 1; k <= nz; ++k)
+        if (__ldg(hp + P * (size_t)(k - 1)) > H_VANISHED) {
+            k_dep = k;
+            break;
+        }
+    const double i0col = c.sw_pen_frac * __ldg(p.q_heat + col) * __ldg(p.wet + col);
+    double d_top = 0.0;
+    double trans_top = sw_transmission(c, d_top);
+    for (int k = nz; k >= k_dep; --k) {
+        const size_t off = P * (size_t)(k - 1);
+        const double hk = __ldg(hp + off);
+        const double d_bot = d_top + hk;
+        const double trans_bot = (k > k_dep) ? sw_transmission(c, d_bot) : 0.0;
+        if (hk > H_VANISHED) {
+            const double absorbed = i0col * (trans_top - trans_bot);
+            double add = inv_scale * absorbed;
+            if (k == kt) add = add - inv_scale * i0col;
+            T[off] = conc_add_source(T[off], hk, add);
+            if (c.budgets) p.heat_budget_surface[col + off] += add;
+            trans_top = trans_bot;
+        }
+        d_top = d_bot;
+    }
+}
+
 __global__ void k_stress_mag(const Params p, double *out)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -170,14 +223,15 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
         // ---- KPP pass 1 (rdb_ocean_vmix.F90:1288-1426) ----
         const double tau_mag = p.stress_mag[col];
         const double u_star = sqrt(xdiv(tau_mag, rho0));
-        q_T_kin = xdiv(p.q_heat[col], rho0 * c.cp);
+        // pass 1 charges the shortwave that passes the lagged boundary layer
+        q_T_kin = kpp_q_t_kin(c, p.q_heat[col], h_b, HH(k_sfc));
         q_S_kin = xdiv(p.q_salt[col], rho0);
         double T_sfc = 0.0, S_sfc = 0.0;
         if (c.buoyancy_coeffs) {   // "eos": the surface layer's (T, S) (rdb_ocean_vmix.F90:1357-1376)
             T_sfc = p.tr[c.idx_temperature][col + P * (size_t)(k_sfc - 1)];
             S_sfc = p.tr[c.idx_salinity][col + P * (size_t)(k_sfc - 1)];
         }
-        const double B_0 = kpp_surface_b0(c, q_T_kin, q_S_kin, HH(k_sfc), T_sfc, S_sfc);
+        double B_0 = kpp_surface_b0(c, q_T_kin, q_S_kin, HH(k_sfc), T_sfc, S_sfc);
         {
             const double wstar3_lagged = fmx(0.0, -B_0) * h_b;
             const double cb = sm_cbrt(wstar3_lagged);
@@ -244,6 +298,10 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
             p.bl_depth[col] = h_b;
         }
         // ---- KPP pass 2 scalars (rdb_ocean_vmix.F90:1429-1491) ----
+        if (c.sw_pen_frac != 0.0) {   // pass 2 charges what passes the new boundary layer
+            q_T_kin = kpp_q_t_kin(c, p.q_heat[col], h_b, HH(k_sfc));
+            B_0 = kpp_surface_b0(c, q_T_kin, q_S_kin, HH(k_sfc), T_sfc, S_sfc);
+        }
         p.b0[col] = B_0;
         destabilizing = B_0 < 0.0;
         const double wstar3 = fmx(0.0, -B_0) * h_b;
@@ -797,6 +855,12 @@ void launch_surface_flux(const Params &p, double inv_heat, double inv_salt, cuda
 {
     dim3 grid((p.nx + 127) / 128, p.ny);
     k_surface_flux<<<grid, 128, 0, stream>>>(p, inv_heat, inv_salt);
+}
+
+void launch_sw_penetration(const Params &p, double inv_scale, cudaStream_t stream)
+{
+    dim3 grid((p.nx + 127) / 128, p.ny);
+    k_sw_penetration<<<grid, 128, 0, stream>>>(p, inv_scale);
 }
 
 void launch_stress_mag(const Params &p, cudaStream_t stream)

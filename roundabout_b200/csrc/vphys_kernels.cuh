@@ -61,6 +61,8 @@ int report_error(int status, const char *msg);
 void launch_eos_wright(const Params &p, cudaStream_t stream);
 // surface heat/salt deposit on the first live layer; inv_heat = dt/(rho0 cp), inv_salt = dt/rho0
 void launch_surface_flux(const Params &p, double inv_heat, double inv_salt, cudaStream_t stream);
+// the penetrating shortwave spread down the column; inv_scale = dt/(rho0 cp)
+void launch_sw_penetration(const Params &p, double inv_scale, cudaStream_t stream);
 void launch_stress_mag(const Params &p, cudaStream_t stream);
 void launch_assemble(const Params &p, cudaStream_t stream);
 void launch_smooth(const Params &p, double *fld, double *scratch, cudaStream_t stream);

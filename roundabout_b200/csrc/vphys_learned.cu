@@ -105,7 +105,8 @@ __global__ void __launch_bounds__(FEAT_THREADS) k_kpp_features(const Params p, c
     }
 
     const double u_star = sqrt(xdiv(p.stress_mag[col], rho0));
-    const double q_T_kin = xdiv(p.q_heat[col], rho0 * c.cp);
+    // the B0 of KPP pass 1: with shortwave, the part passing the lagged h_b is not charged
+    const double q_T_kin = kpp_q_t_kin(c, p.q_heat[col], p.bl_depth[col], HH(k_sfc));
     const double q_S_kin = xdiv(p.q_salt[col], rho0);
     double T_sfc = 0.0, S_sfc = 0.0;
     if (c.buoyancy_coeffs) {   // the same surface (T, S) the assembly's B0 will use
@@ -210,9 +211,10 @@ __global__ void k_kpp_targets(const Params p, float *T)
     const double u_star = sqrt(xdiv(p.stress_mag[col], rho0));
     const double q_T_kin = xdiv(p.q_heat[col], rho0 * c.cp);
     const double q_S_kin = xdiv(p.q_salt[col], rho0);
-    // with "eos" coefficients, the B0 of the assembly that set this h_b
-    const double B_0 = c.buoyancy_coeffs ? p.b0[col]
-                                         : (GRAVITY / rho0) * (c.alpha_T * q_T_kin - c.beta_S * q_S_kin);
+    // with "eos" coefficients or shortwave, the B0 of the assembly that set this h_b
+    const double B_0 = (c.buoyancy_coeffs || c.sw_pen_frac != 0.0)
+                           ? p.b0[col]
+                           : (GRAVITY / rho0) * (c.alpha_T * q_T_kin - c.beta_S * q_S_kin);
     const double w_star = sm_cbrt(fmx(0.0, -B_0) * h_b);
     const double w_s = sqrt(u_star * u_star + w_star * w_star);
     float *t = T + col * LK_OUTP;

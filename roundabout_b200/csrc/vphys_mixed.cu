@@ -388,13 +388,16 @@ __global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, doubl
             const double rho0 = c.rho0;
             h_b = p.bl_depth[col];
             const double u_star = sqrt(xdiv(p.stress_mag[col], rho0));
-            const double q_T_kin = xdiv(p.q_heat[col], rho0 * c.cp);
+            // the heat flux pass 2 charged (shortwave: what passes h_b, or the
+            // surface layer hi)
+            const double q_T_kin = kpp_q_t_kin(c, p.q_heat[col], h_b, __ldg(hp + P * (size_t)(hi - 1)));
             const double q_S_kin = xdiv(p.q_salt[col], rho0);
-            // with "eos" coefficients B0 is the assembly's (pass 2 stored it before
-        // the solve changed the surface T and S); the constants give the same
-        // number recomputed
-        const double B_0 = c.buoyancy_coeffs ? p.b0[col]
-                                             : (GRAVITY / rho0) * (c.alpha_T * q_T_kin - c.beta_S * q_S_kin);
+            // with "eos" coefficients or shortwave B0 is the assembly's (pass 2
+            // stored it before the solve changed the surface T and S); otherwise
+            // the same number recomputed
+            const double B_0 = (c.buoyancy_coeffs || c.sw_pen_frac != 0.0)
+                                   ? p.b0[col]
+                                   : (GRAVITY / rho0) * (c.alpha_T * q_T_kin - c.beta_S * q_S_kin);
             const double wstar3 = fmx(0.0, -B_0) * h_b;
             const double w_star = sm_cbrt(wstar3);
             const double w_s = sqrt(u_star * u_star + w_star * w_star);

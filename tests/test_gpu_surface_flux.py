@@ -117,3 +117,79 @@ def test_surface_flux_rejects_bad_flag(VP):
     cols = columns(nx=8, ny=4, nz=3, seed=45)
     with pytest.raises(_ffi.VphysError):
         loaded(VP, cols, hot_cfg(surface_flux=2))
+
+
+SW = dict(sw_pen_frac=0.5, sw_band_ratio=0.58, sw_zeta1=0.35, sw_zeta2=23.0)
+
+
+@pytest.mark.parametrize("budgets", [0, 1])
+def test_sw_penetration_standalone(VP, oracle, budgets):
+    """ocean_surface_flux_apply_sw_penetration after the surface deposit,
+    bitwise, with vanished top fillers and thin layers."""
+    cols = columns(nx=40, ny=12, nz=20, seed=46, thin_frac=0.2)
+    cols.h[:10, :, -1] = 1.0e-4
+    cfg = hot_cfg(budgets=budgets, surface_flux=1, **SW)
+    st = oracle_state(oracle, cols, cfg)
+    vp = loaded(VP, cols, cfg)
+    for _ in range(2):
+        st.call("vpo_surface_flux", cfg, DT)
+        st.call("vpo_sw_penetration", cfg, DT)
+        vp.surface_flux(DT)
+        vp.sw_penetration(DT)
+    for t in range(st.ntr):
+        assert_bitwise(f"tracer{t}", vp.get_tracer(t), st.tracers[t])
+    if budgets:
+        assert_bitwise("heat_budget_surface", vp.get("heat_budget_surface"), st.heat_budget_surface)
+
+
+@pytest.mark.parametrize("method", [1, 2, 3])
+def test_assemble_with_shortwave(VP, oracle, method):
+    """KPP's B0 charging only the absorbed shortwave (MXL: inside the
+    boundary layer, LV1: inside the surface layer): the assembly bitwise."""
+    cols = columns(seed=47)
+    cfg = hot_cfg(kpp_sw_method=method, **SW)
+    st = oracle_state(oracle, cols, cfg)
+    st.q_heat[...] = np.abs(st.q_heat) + 50.0    # sunlit: a penetrating part to subtract
+    st.call("vpo_eos_wright", cfg)
+    st.bl_depth[...] = np.abs(np.sin(np.arange(st.bl_depth.size))).reshape(st.bl_depth.shape, order="F") * 60.0
+    vp = loaded(VP, cols, cfg)
+    vp.set("q_heat", st.q_heat)
+    vp.eos()
+    vp.set("bl_depth", st.bl_depth)
+    vp.get("gamma_t")
+    assert st.call("vpo_build_coefficients", cfg) == 0
+    vp.assemble()
+    for n in ("kv", "kt", "ks", "bl_depth", "b0", "gamma_t"):
+        assert_bitwise(n, vp.get(n), getattr(st, n))
+
+
+@pytest.mark.parametrize("eos_coeffs", [0, 1])
+def test_step_with_shortwave(VP, oracle, eos_coeffs):
+    """Whole steps with the surface deposit, the shortwave moved down the
+    column and KPP's corrected B0 (and its non-local deposit): bitwise."""
+    cols = columns(nx=30, ny=18, nz=16, seed=48, thin_frac=0.1)
+    cfg = hot_cfg(budgets=1, surface_flux=1, buoyancy_coeffs=eos_coeffs, **SW)
+    st = oracle_state(oracle, cols, cfg)
+    vp = loaded(VP, cols, cfg)
+    assert st.call("vpo_step", cfg, DT, 3) == 0
+    vp.step(DT, 3)
+    for t in range(st.ntr):
+        assert_bitwise(f"tracer{t}", vp.get_tracer(t), st.tracers[t])
+    for n in ("kv", "kt", "u", "bl_depth", "b0", "heat_budget", "heat_budget_surface"):
+        assert_bitwise(n, vp.get(n), getattr(st, n))
+    c0 = hot_cfg(budgets=1, surface_flux=1, buoyancy_coeffs=eos_coeffs)
+    s0 = oracle_state(oracle, cols, c0)
+    s0.call("vpo_step", c0, DT, 3)
+    assert np.abs(s0.tracers[1] - st.tracers[1]).max() > 1e-6   # the shortwave changed the answer
+
+
+def test_mixed_step_with_shortwave(VP, oracle):
+    ntr = 6
+    cols = columns(nx=48, ny=32, nz=40, seed=49, ntr=ntr, thin_frac=0.15, passive_init="uniform")
+    cfg = hot_cfg(ntr=ntr, surface_flux=1, **SW)
+    st = oracle_state(oracle, cols, cfg)
+    vp = loaded(VP, cols, hot_cfg(ntr=ntr, surface_flux=1, mixed_precision=1, **SW))
+    assert st.call("vpo_step", cfg, DT, 1) == 0
+    vp.step(DT, 1)
+    err = max(float(np.abs(np.asarray(vp.get_tracer(t)) - st.tracers[t]).max()) for t in range(ntr))
+    assert err <= 1.0e-6, err

@@ -510,3 +510,99 @@ def test_kpp_eos_coeffs_scale_kv_as_cube_root_of_b0(oracle):
         assert kv_c > 1.0e-3
         assert abs(kv_e / kv_c - ratio) < 1.0e-10 * ratio
     assert runs[1].b0[3, 2] == (9.80665 / 1035.0) * (a_e * qt - b_e * qs)
+
+
+# ------------------------------------------------- shortwave penetration ----
+# test_ocean_sw_penetration.F90: 6 layers of 5 m, Q_heat = 200 W/m2, half of it
+# penetrating, two bands R = 0.58, zeta = 0.35 / 23 m (39-47).  The correction
+# redistributes (column sum 0, 150-189), follows the two-band closed form
+# layer by layer (124-148, 191-218), absorbs most at the top and decays with
+# depth (220-268), and is byte-for-byte nothing at sw_pen_frac = 0 (270-290).
+SW = dict(sw_pen_frac=0.5, sw_band_ratio=0.58, sw_zeta1=0.35, sw_zeta2=23.0)
+
+
+def sw_state(oracle, nz=6, h=5.0):
+    st = flux_state(oracle, nz=nz, h=h)
+    st.q_heat[...] = 200.0
+    return st
+
+
+def sw_closed_form(nz, h, c, dt=3600.0, q=200.0):
+    import math
+
+    inv = dt / (c.rho0 * c.cp)
+    i0 = c.sw_pen_frac * q
+    tr = lambda d: c.sw_band_ratio * math.exp(-d / c.sw_zeta1) + (1 - c.sw_band_ratio) * math.exp(-d / c.sw_zeta2)
+    corr = np.zeros(nz)
+    d_top = 0.0
+    for k in range(nz - 1, -1, -1):
+        d_bot = d_top + h
+        tb = tr(d_bot) if k > 0 else 0.0
+        corr[k] = inv * i0 * (tr(d_top) - tb) - (inv * i0 if k == nz - 1 else 0.0)
+        d_top = d_bot
+    return corr
+
+
+def test_sw_penetration_conserves_and_matches_two_band(oracle):
+    c = cfg_pp81(**SW)
+    st = sw_state(oracle)
+    st.call("vpo_sw_penetration", c, 3600.0)
+    got = st.h[3, 2, :] * (st.tracers[1][3, 2, :] - 10.0)
+    assert abs(got.sum()) < 1e-12
+    np.testing.assert_allclose(got, sw_closed_form(6, 5.0, c), rtol=0, atol=1e-12)
+    absorbed = got.copy()
+    absorbed[-1] += 3600.0 / (c.rho0 * c.cp) * 0.5 * 200.0
+    assert np.all(absorbed >= 0.0) and np.all(absorbed[-1] > absorbed[:-1])
+    assert np.all(absorbed[2:-1] > absorbed[1:-2])   # interior decays; the opaque bed takes the rest
+
+
+def test_sw_penetration_off_is_identity(oracle):
+    c = cfg_pp81(**dict(SW, sw_pen_frac=0.0))
+    st = sw_state(oracle)
+    T0 = st.tracers[1].copy()
+    st.call("vpo_sw_penetration", c, 3600.0)
+    np.testing.assert_array_equal(st.tracers[1], T0)
+
+
+def test_sw_penetration_skips_vanished_layers_and_books_the_move(oracle):
+    """A vanished top filler and a vanished bed layer pass the light on; the
+    lump leaves the first live layer; the budget books every move (sum 0)."""
+    c = cfg_pp81(budgets=1, **SW)
+    st = sw_state(oracle, nz=8)
+    st.h[:, :, -1] = 1.0e-4
+    st.h[:, :, 0] = 0.0
+    st.call("vpo_sw_penetration", c, 3600.0)
+    T = st.tracers[1]
+    assert np.all(T[:, :, -1] == 10.0) and np.all(T[:, :, 0] == 10.0)
+    assert np.all(T[:, :, -2] < 10.0)            # the surface lump left the first live layer
+    bud = st.heat_budget_surface
+    assert abs(bud.sum()) < 1e-10 and np.abs(bud).max() > 0.0
+    np.testing.assert_allclose((st.h * (T - 10.0)).sum(axis=2), bud.sum(axis=2), rtol=0, atol=1e-12)
+
+
+@pytest.mark.parametrize("method", [1, 2, 3])
+def test_kpp_b0_charges_the_absorbed_shortwave(oracle, method):
+    """Pass 2's B0 (the stored b0) takes Q_heat minus what passes the new
+    boundary layer (MXL) or the surface layer (LV1), all of it with ALL
+    (rdb_ocean_vmix.F90:1440-1466)."""
+    import math
+
+    c = cfg_pp81(use_kpp=1, alpha_T=0.2, beta_S=0.77, kpp_sw_method=method, **SW)
+    st = kpp_state(oracle, nz=10, h=8.0, tau=0.05, strat=0.01)
+    st.q_heat[...] = 150.0
+    st.call("vpo_pp81", c)
+    st.call("vpo_kpp_overlay", c)
+    h_b = st.bl_depth[4, 3]
+    tr = lambda d: 0.58 * math.exp(-d / 0.35) + 0.42 * math.exp(-d / 23.0)
+    q = 150.0 - {1: 0.0, 2: 0.5 * 150.0 * tr(h_b), 3: 0.5 * 150.0 * tr(st.h[4, 3, -1])}[method]
+    want = (9.80665 / 1035.0) * (0.2 * q / (1035.0 * 3992.0))
+    assert abs(st.b0[4, 3] - want) <= 1e-13 * abs(want)
+    c0 = cfg_pp81(use_kpp=1, alpha_T=0.2, beta_S=0.77, kpp_sw_method=method)
+    s0 = kpp_state(oracle, nz=10, h=8.0, tau=0.05, strat=0.01)
+    s0.q_heat[...] = 150.0
+    s0.call("vpo_pp81", c0)
+    s0.call("vpo_kpp_overlay", c0)
+    if method == 1:
+        np.testing.assert_array_equal(st.b0, s0.b0)
+    else:
+        assert np.all(st.b0 < s0.b0)
