@@ -60,7 +60,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="eddy_1440x1080x75")
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=4)
     ap.add_argument("--cpu-sample", default="360x270", help="nx x ny of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--form", default="mixed", choices=["mixed", "plain"],
@@ -419,51 +419,85 @@ def main():
                 "path_achieved_gbs": round(bpc["path"] * cells / (ms / args.steps / 1e3) / 1e9, 1)}
 
     # ---- end to end through the C ABI with host buffers ----
+    # Every step uploads its inputs from pinned host memory and downloads its
+    # results.  Serial: one handle, synchronous copies, upload -> step ->
+    # download.  Pipelined (the reported e2e): two handles on two streams take
+    # alternate steps with the asynchronous copies, so one handle's download
+    # overlaps the other's upload on the full-duplex host link; each handle
+    # has its own pinned result buffers.
     e2e = None
     if args.e2e_steps > 0:
+        import ctypes
+
         pin = lambda a: torch.from_numpy(np.ascontiguousarray(a.T)).pin_memory()  # noqa: E731
         host_in = {"h": pin(cols.h), "u": pin(cols.u), "v": pin(cols.v), "q_heat": pin(cols.q_heat),
                    "q_salt": pin(cols.q_salt), "tau_x": pin(cols.tau_x), "tau_y": pin(cols.tau_y)}
         host_tr = [pin(t) for t in cols.tracers]
-        host_out = {n: torch.empty(tuple(reversed(vp.shape(n))), dtype=torch.float64).pin_memory()
-                    for n in ("kv", "kt", "ks", "bl_depth")}
-        lib, hdl = vp.lib, vp.handle
-        import ctypes
+        out_names = ("u", "v", "kv", "kt", "ks", "bl_depth")
 
-        def put(fid, t):
-            _ffi.check(lib.vphys_set_field(hdl, fid, ctypes.c_void_p(t.data_ptr()), t.numel()), "set_field")
+        def outputs(h):
+            o = {n: torch.empty(tuple(reversed(h.shape(n))), dtype=torch.float64).pin_memory() for n in out_names}
+            o["tracers"] = [torch.empty_like(t).pin_memory() for t in host_tr]
+            return o
 
-        def take(fid, t):
-            _ffi.check(lib.vphys_get_field(hdl, fid, ctypes.c_void_p(t.data_ptr()), t.numel()), "get_field")
-
-        def e2e_step():
+        def e2e_step(h, out, sync):
+            lib, hdl = h.lib, h.handle
+            setf = lib.vphys_set_field if sync else lib.vphys_set_field_async
+            getf = lib.vphys_get_field if sync else lib.vphys_get_field_async
             for n, t in host_in.items():
-                put(_ffi.FIELD_NAMES[n], t)
+                _ffi.check(setf(hdl, _ffi.FIELD_NAMES[n], ctypes.c_void_p(t.data_ptr()), t.numel()), "set_field")
             for k, t in enumerate(host_tr):
-                put(_ffi.FIELD_TRACER0 + k, t)
+                _ffi.check(setf(hdl, _ffi.FIELD_TRACER0 + k, ctypes.c_void_p(t.data_ptr()), t.numel()), "set_field")
             _ffi.check(lib.vphys_stress_mag(hdl), "stress_mag")
             _ffi.check(lib.vphys_step(hdl, dt, 1), "step")
-            take(_ffi.FIELD_U, host_in["u"])
-            take(_ffi.FIELD_V, host_in["v"])
-            for k, t in enumerate(host_tr):
-                take(_ffi.FIELD_TRACER0 + k, t)
-            for n, t in host_out.items():
-                take(_ffi.FIELD_NAMES[n], t)
+            for n in out_names:
+                t = out[n]
+                _ffi.check(getf(hdl, _ffi.FIELD_NAMES[n], ctypes.c_void_p(t.data_ptr()), t.numel()), "get_field")
+            for k, t in enumerate(out["tracers"]):
+                _ffi.check(getf(hdl, _ffi.FIELD_TRACER0 + k, ctypes.c_void_p(t.data_ptr()), t.numel()), "get_field")
 
         h2d = sum(t.numel() * 8 for t in host_in.values()) + sum(t.numel() * 8 for t in host_tr)
-        d2h = (host_in["u"].numel() + host_in["v"].numel()) * 8 + sum(t.numel() * 8 for t in host_tr) + \
-            sum(t.numel() * 8 for t in host_out.values())
-        e2e_step()
+        out0 = outputs(vp)
+        d2h = sum(out0[n].numel() * 8 for n in out_names) + sum(t.numel() * 8 for t in out0["tracers"])
+
+        # serial, one handle
+        e2e_step(vp, out0, True)
         barrier()
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
-            e2e_step()
+            e2e_step(vp, out0, True)
+        barrier()
+        el_serial = max_over_ranks(time.perf_counter() - t0)
+
+        # pipelined, two handles on their own streams
+        vp2 = VerticalPhysics(nx, ny, nz, ntr, cfg)
+        vp2.load_columns(cols)
+        pair = [(vp, out0, torch.cuda.Stream()), (vp2, outputs(vp2), torch.cuda.Stream())]
+        for h, _, s in pair:
+            h.set_stream(s.cuda_stream)
+        for h, o, _ in pair:
+            e2e_step(h, o, False)
+        for h, _, _ in pair:
+            h.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        for i in range(args.e2e_steps):
+            h, o, _ = pair[i % 2]
+            e2e_step(h, o, False)
+        for h, _, _ in pair:
+            h.synchronize()
         barrier()
         el = max_over_ranks(time.perf_counter() - t0)
+        vp.set_stream(0)
+        vp2.close()
         e2e = {"value": cells * args.e2e_steps * world / el, "unit": "cells/s", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "ms_per_step": el / args.e2e_steps * 1e3,
-               "what": "C-ABI vphys_set_field (pinned host -> HBM) of h, u, v, tracers, forcing; vphys_step; "
-                       "vphys_get_field of u, v, tracers, kv, kt, ks, bl_depth"}
+               "serial_ms_per_step": el_serial / args.e2e_steps * 1e3,
+               "serial_cells_per_s": cells * args.e2e_steps * world / el_serial,
+               "what": "C ABI: vphys_set_field_async (pinned host -> HBM) of h, u, v, tracers, forcing; vphys_step; "
+                       "vphys_get_field_async of u, v, tracers, kv, kt, ks, bl_depth; two handles on two streams "
+                       "take alternate steps so one's download overlaps the other's upload (serial: one handle, "
+                       "synchronous vphys_set_field / vphys_get_field)"}
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:

@@ -247,6 +247,17 @@ int vphys_bind(vphys_handle h, int field, void *device_ptr);
 int vphys_set_field(vphys_handle h, int field, const void *host, size_t n);
 int vphys_get_field(vphys_handle h, int field, void *host, size_t n);
 
+/* The same copies enqueued on the handle's stream without waiting (the
+ * counterparts of the setters and getters above, include/rdb_ocean.h:419-447,
+ * made asynchronous): they return once the copy is queued, in stream order
+ * with vphys_step.  The host buffer must stay valid, and untouched by the
+ * caller, until vphys_synchronize(h) returns; page-locked (pinned) host
+ * memory lets the copy run while the host and other streams work, so a
+ * caller with two handles on two streams can overlap one domain's upload
+ * with another's download. */
+int vphys_set_field_async(vphys_handle h, int field, const void *host, size_t n);
+int vphys_get_field_async(vphys_handle h, int field, void *host, size_t n);
+
 /* Current device pointer and shape of a field, like
  * rdb_ocean_get_kv_ptr(handle, ptr, nx, ny, nz, gen)
  * (include/rdb_ocean.h:378-385); *gen = number of completed vphys_step

@@ -736,6 +736,51 @@ int vphys_get_field(vphys_handle h, int field, void *host, size_t n)
     return cuda_status(e, "vphys_get_field");
 }
 
+namespace {
+// Checks shared by the asynchronous copies; returns the slot or a status < 0.
+int copy_slot(vphys_handle h, int field, const void *host, size_t n, const char *who, int *st)
+{
+    *st = VPHYS_OK;
+    if (!valid(h)) {
+        *st = push_error(VPHYS_ERR_BAD_HANDLE, "%s: bad handle", who);
+        return -1;
+    }
+    int sl = slot_of(h, field);
+    if (sl < 0) {
+        *st = push_error(VPHYS_ERR_NOT_FOUND, "%s: unknown field id %d", who, field);
+        return -1;
+    }
+    if (n != h->f[sl].n) {
+        *st = push_error(VPHYS_ERR_BAD_SHAPE, "%s: field %d holds %zu elements, got %zu", who, field, h->f[sl].n, n);
+        return -1;
+    }
+    if (!host) {
+        *st = push_error(VPHYS_ERR_BAD_SHAPE, "%s: NULL host buffer", who);
+        return -1;
+    }
+    if ((*st = ensure(h, field))) return -1;
+    return sl;
+}
+}  // namespace
+
+int vphys_set_field_async(vphys_handle h, int field, const void *host, size_t n)
+{
+    int st;
+    const int sl = copy_slot(h, field, host, n, "vphys_set_field_async", &st);
+    if (sl < 0) return st;
+    return cuda_status(cudaMemcpyAsync(h->f[sl].ptr(), host, h->f[sl].bytes(), cudaMemcpyHostToDevice, h->stream),
+                       "vphys_set_field_async");
+}
+
+int vphys_get_field_async(vphys_handle h, int field, void *host, size_t n)
+{
+    int st;
+    const int sl = copy_slot(h, field, host, n, "vphys_get_field_async", &st);
+    if (sl < 0) return st;
+    return cuda_status(cudaMemcpyAsync(host, h->f[sl].ptr(), h->f[sl].bytes(), cudaMemcpyDeviceToHost, h->stream),
+                       "vphys_get_field_async");
+}
+
 int vphys_get_ptr(vphys_handle h, int field, void **ptr, int *nx, int *ny, int *nz, int *gen)
 {
     if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_get_ptr: bad handle");
