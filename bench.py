@@ -401,7 +401,8 @@ def main():
         torch.cuda.synchronize()
         stage_ms[name] = a.elapsed_time(b) / reps
     bpc = bytes_per_cell(ntr, nz)
-    kernel_of = {"eos": "k_eos_wright", "assemble": "k_assemble",
+    kernel_of = {"eos": "k_eos_wright",
+                 "assemble": "k_assemble<float>" if (mixed and args.mixed_level >= 2) else "k_assemble<double>",
                  # the stage's launches: the column-depth pass and the face solve
                  "momentum": "k_column_depth+k_momentum_mp" if mixed else "k_column_depth+k_momentum",
                  "tracers": "k_spans+k_tracers_mp" if mixed else "k_tracers"}
