@@ -8,6 +8,24 @@
 
 namespace vphys {
 
+// The momentum knobs of the default (benchmark) configuration; a face solve
+// instantiated for them folds the other options' branches out.
+__host__ __device__ __forceinline__ bool is_default_face_knobs(const vphys_config &c)
+{
+    return c.hvel_mom6 && !c.hvel_harmonic && !c.remnant && !c.bbl_glue && !c.implicit_stress &&
+           !c.implicit_drag && !c.zlevel_faces;
+}
+__host__ __device__ __forceinline__ void default_face_knobs(vphys_config &c)
+{
+    c.hvel_mom6 = 1;
+    c.hvel_harmonic = 0;
+    c.remnant = 0;
+    c.bbl_glue = 0;
+    c.implicit_stress = 0;
+    c.implicit_drag = 0;
+    c.zlevel_faces = 0;
+}
+
 template <typename R>
 __device__ __forceinline__ void face_layer(const vphys_config &c, R hl_c, R hr_c, R u_k, int k, int kb, R d_min,
                                            R i_hbbl, R &zacc, R &zcol_l, R &zcol_r, R &hvel, R &zint)

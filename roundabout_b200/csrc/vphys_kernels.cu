@@ -588,10 +588,15 @@ constexpr int MOM_U = VPHYS_MOM_U;   // levels per load block
 // The Thomas c' of every level sits in shared memory (cpp[(k-1)*bs]); the
 // forward-swept d' is written in place over u with an L2 evict_last hint and
 // read back by the back-substitution.
-template <bool XF>
+template <bool XF, bool DEF>
 __device__ __forceinline__ void solve_face(const Params &p, double dt, int i, int j, double *cpp, int bs)
 {
-    const vphys_config &c = p.cfg;
+    // DEF: the default momentum knobs (hvel_mom6 z_clear, no remnant, BBL
+    // glue, implicit stress or drag, z-level faces) as compile-time
+    // constants, so their branches fold out of the per-level code
+    vphys_config cd = p.cfg;
+    if (DEF) default_face_knobs(cd);
+    const vphys_config &c = cd;
     const int nx = p.nx, ny = p.ny, nz = p.nz;
     const int nu = XF ? nx + 1 : nx;
     const size_t P = p.plane;
@@ -774,6 +779,7 @@ __device__ __forceinline__ void solve_face(const Params &p, double dt, int i, in
 }
 
 // blockIdx.z = 0: u faces (i <= nx, j < ny); 1: v faces (i < nx, j <= ny)
+template <bool DEF>
 __global__ void __launch_bounds__(MOM_THREADS) k_momentum(const Params p, double dt)
 {
     extern __shared__ double smem[];
@@ -781,9 +787,9 @@ __global__ void __launch_bounds__(MOM_THREADS) k_momentum(const Params p, double
     const int j = blockIdx.y;
     double *cpp = smem + threadIdx.x;
     if (blockIdx.z == 0) {
-        if (i <= p.nx && j < p.ny) solve_face<true>(p, dt, i, j, cpp, blockDim.x);
+        if (i <= p.nx && j < p.ny) solve_face<true, DEF>(p, dt, i, j, cpp, blockDim.x);
     } else {
-        if (i < p.nx && j <= p.ny) solve_face<false>(p, dt, i, j, cpp, blockDim.x);
+        if (i < p.nx && j <= p.ny) solve_face<false, DEF>(p, dt, i, j, cpp, blockDim.x);
     }
 }
 
@@ -926,12 +932,17 @@ void launch_momentum(const Params &p, double dt, cudaStream_t stream)
     }
     static bool attr_set = false;
     if (!attr_set) {
-        cudaFuncSetAttribute(k_momentum, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)((size_t)VPHYS_NZ_MAX * MOM_THREADS * sizeof(double)));
+        const int mx = (int)((size_t)VPHYS_NZ_MAX * MOM_THREADS * sizeof(double));
+        cudaFuncSetAttribute(k_momentum<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+        cudaFuncSetAttribute(k_momentum<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
         attr_set = true;
     }
     dim3 grid((p.nx + 1 + MOM_THREADS - 1) / MOM_THREADS, p.ny + 1, 2);
-    k_momentum<<<grid, MOM_THREADS, (size_t)p.nz * MOM_THREADS * sizeof(double), stream>>>(p, dt);
+    const size_t smem = (size_t)p.nz * MOM_THREADS * sizeof(double);
+    if (is_default_face_knobs(p.cfg))
+        k_momentum<true><<<grid, MOM_THREADS, smem, stream>>>(p, dt);
+    else
+        k_momentum<false><<<grid, MOM_THREADS, smem, stream>>>(p, dt);
 }
 
 }  // namespace vphys

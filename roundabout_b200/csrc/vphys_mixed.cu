@@ -420,11 +420,13 @@ __global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, doubl
 // ---------------------------------------------------------------------------
 // momentum: one thread per u or v face column
 // ---------------------------------------------------------------------------
-template <bool XF>
+template <bool XF, bool DEF>
 __device__ __forceinline__ void solve_face_mp(const Params &p, double dt, int i, int j, float *st, float *sv,
                                               float *sr, int bs)
 {
-    const vphys_config &c = p.cfg;
+    vphys_config cd = p.cfg;   // DEF: the default knobs folded in (is_default_face_knobs)
+    if (DEF) default_face_knobs(cd);
+    const vphys_config &c = cd;
     const int nx = p.nx, ny = p.ny, nz = p.nz;
     const int nu = XF ? nx + 1 : nx;
     const size_t P = p.plane;
@@ -588,6 +590,7 @@ __device__ __forceinline__ void solve_face_mp(const Params &p, double dt, int i,
     }
 }
 
+template <bool DEF>
 __global__ void __launch_bounds__(MP_MOM_THREADS) k_momentum_mp(const Params p, double dt)
 {
     extern __shared__ float smf[];
@@ -596,9 +599,9 @@ __global__ void __launch_bounds__(MP_MOM_THREADS) k_momentum_mp(const Params p, 
     const size_t NB = (size_t)p.nz * blockDim.x;
     float *st = smf + threadIdx.x, *sv = st + NB, *sr = sv + NB;
     if (blockIdx.z == 0) {
-        if (i <= p.nx && j < p.ny) solve_face_mp<true>(p, dt, i, j, st, sv, sr, blockDim.x);
+        if (i <= p.nx && j < p.ny) solve_face_mp<true, DEF>(p, dt, i, j, st, sv, sr, blockDim.x);
     } else {
-        if (i < p.nx && j <= p.ny) solve_face_mp<false>(p, dt, i, j, st, sv, sr, blockDim.x);
+        if (i < p.nx && j <= p.ny) solve_face_mp<false, DEF>(p, dt, i, j, st, sv, sr, blockDim.x);
     }
 }
 
@@ -672,13 +675,17 @@ void launch_momentum_mp(const Params &p, double dt, cudaStream_t stream)
     const int bs = MP_MOM_THREADS;
     static bool attr_set = false;
     if (!attr_set) {
-        cudaFuncSetAttribute(k_momentum_mp, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)((size_t)VPHYS_NZ_MAX * bs * sizeof(float) * 3));
+        const int mx = (int)((size_t)VPHYS_NZ_MAX * bs * sizeof(float) * 3);
+        cudaFuncSetAttribute(k_momentum_mp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+        cudaFuncSetAttribute(k_momentum_mp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
         attr_set = true;
     }
     const size_t smem = (size_t)p.nz * bs * sizeof(float) * (p.cfg.remnant ? 3 : 2);
     dim3 grid((p.nx + 1 + bs - 1) / bs, p.ny + 1, 2);
-    k_momentum_mp<<<grid, bs, smem, stream>>>(p, dt);
+    if (is_default_face_knobs(p.cfg))
+        k_momentum_mp<true><<<grid, bs, smem, stream>>>(p, dt);
+    else
+        k_momentum_mp<false><<<grid, bs, smem, stream>>>(p, dt);
 }
 
 }  // namespace vphys
