@@ -177,13 +177,37 @@ constexpr int ASM_THREADS = 128;
 #define VPHYS_ASM_U_F 2
 #endif
 
-template <typename R>
+// The assembly knobs of the default (benchmark) configuration: PP81, KPP
+// with constant buoyancy coefficients and no shortwave, Bryan-Lewis, no
+// KV_ML_INVZ2, convection or guard.
+__host__ __device__ __forceinline__ bool is_default_assembly_knobs(const vphys_config &c)
+{
+    return c.interior_closure == VPHYS_INTERIOR_PP81 && c.use_kpp && c.bkgnd_profile && !(c.kv_ml_invz2 > 0.0) &&
+           !c.conv_enable && !c.vmix_guard && !c.buoyancy_coeffs && c.sw_pen_frac == 0.0;
+}
+__device__ __forceinline__ void default_assembly_knobs(vphys_config &c)
+{
+    c.interior_closure = VPHYS_INTERIOR_PP81;
+    c.use_kpp = 1;
+    c.bkgnd_profile = 1;
+    c.kv_ml_invz2 = 0.0;
+    c.conv_enable = 0;
+    c.vmix_guard = 0;
+    c.buoyancy_coeffs = 0;
+    c.sw_pen_frac = 0.0;
+}
+
+template <typename R, bool DEF>
 __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
     if (i >= p.nx) return;
-    const vphys_config &c = p.cfg;
+    // DEF: the default assembly knobs (is_default_assembly_knobs) as
+    // compile-time constants, so the other options' branches fold out
+    vphys_config cd = p.cfg;
+    if (DEF) default_assembly_knobs(cd);
+    const vphys_config &c = cd;
     const int nx = p.nx, nz = p.nz;
     const size_t P = p.plane, PU = p.plane_u, PV = p.plane_v;
     const size_t col = (size_t)i + (size_t)nx * j;
@@ -878,10 +902,18 @@ void launch_stress_mag(const Params &p, cudaStream_t stream)
 void launch_assemble(const Params &p, cudaStream_t stream)
 {
     dim3 grid((p.nx + ASM_THREADS - 1) / ASM_THREADS, p.ny);
-    if (p.cfg.mixed_precision >= 2)
-        k_assemble<float><<<grid, ASM_THREADS, 0, stream>>>(p);
-    else
-        k_assemble<double><<<grid, ASM_THREADS, 0, stream>>>(p);
+    const bool def = is_default_assembly_knobs(p.cfg);
+    if (p.cfg.mixed_precision >= 2) {
+        if (def)
+            k_assemble<float, true><<<grid, ASM_THREADS, 0, stream>>>(p);
+        else
+            k_assemble<float, false><<<grid, ASM_THREADS, 0, stream>>>(p);
+    } else {
+        if (def)
+            k_assemble<double, true><<<grid, ASM_THREADS, 0, stream>>>(p);
+        else
+            k_assemble<double, false><<<grid, ASM_THREADS, 0, stream>>>(p);
+    }
 }
 
 void launch_smooth(const Params &p, double *fld, double *scratch, cudaStream_t stream)
