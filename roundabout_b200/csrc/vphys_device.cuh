@@ -308,4 +308,19 @@ __device__ __forceinline__ double kpp_q_t_kin(const vphys_config &c, double q_he
     return xdiv(q_heat, c.rho0 * c.cp);
 }
 
+// The tracer-solve knobs of the default (benchmark) configuration: no
+// budgets, arithmetic face thickness, constant buoyancy coefficients, no
+// shortwave; a solve instantiated for them folds the other branches out.
+__host__ __device__ __forceinline__ bool is_default_tracer_knobs(const vphys_config &c)
+{
+    return !c.budgets && !c.use_harmonic && !c.buoyancy_coeffs && c.sw_pen_frac == 0.0;
+}
+__device__ __forceinline__ void default_tracer_knobs(vphys_config &c)
+{
+    c.budgets = 0;
+    c.use_harmonic = 0;
+    c.buoyancy_coeffs = 0;
+    c.sw_pen_frac = 0.0;
+}
+
 }  // namespace vphys

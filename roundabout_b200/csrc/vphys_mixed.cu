@@ -195,7 +195,7 @@ struct TracerGroups {
 
 // TPW tracers per warp share one factorisation and one t array (TWO, a
 // separate ks, keeps one tracer per warp); their forward chains interleave.
-template <bool TWO, int TPW>
+template <bool TWO, int TPW, bool DEF>
 __global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, double dt, int nonlocal, int ngx,
                                                            const TracerGroups tg)
 {
@@ -207,7 +207,9 @@ __global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, doubl
     const unsigned g = blockIdx.x / ngroups;
     const int gi = g % ngx, j = g / ngx;
     const int i = gi * MP_TR_COLS + lane;
-    const vphys_config &c = p.cfg;
+    vphys_config cd = p.cfg;   // DEF: the default knobs folded in (is_default_tracer_knobs)
+    if (DEF) default_tracer_knobs(cd);
+    const vphys_config &c = cd;
     const int nx = p.nx, nz = p.nz;
     const size_t P = p.plane;
     const bool in_grid = i < nx;
@@ -611,8 +613,9 @@ static void launch_tracers_mp_t(const Params &p, double dt, bool nonlocal, cudaS
     const size_t smem = (size_t)p.nz * MP_TR_COLS * (1 + TPW) * sizeof(float);
     static bool attr_set = false;
     if (!attr_set) {
-        cudaFuncSetAttribute(k_tracers_mp<TWO, TPW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)((size_t)VPHYS_NZ_MAX * MP_TR_COLS * (1 + TPW) * sizeof(float)));
+        const int mx = (int)((size_t)VPHYS_NZ_MAX * MP_TR_COLS * (1 + TPW) * sizeof(float));
+        cudaFuncSetAttribute(k_tracers_mp<TWO, TPW, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+        cudaFuncSetAttribute(k_tracers_mp<TWO, TPW, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
         attr_set = true;
     }
     // tracers with a non-local deposit or a budget first, one per group; the
@@ -636,7 +639,10 @@ static void launch_tracers_mp_t(const Params &p, double dt, bool nonlocal, cudaS
     tg.ngroups = tg.single + (p.ntr - tg.single + TPW - 1) / TPW;
     const int ngx = (p.nx + MP_TR_COLS - 1) / MP_TR_COLS;
     const unsigned blocks = (unsigned)ngx * (unsigned)p.ny * (unsigned)tg.ngroups;
-    k_tracers_mp<TWO, TPW><<<blocks, MP_TR_COLS, smem, stream>>>(p, dt, nonlocal ? 1 : 0, ngx, tg);
+    if (is_default_tracer_knobs(p.cfg))
+        k_tracers_mp<TWO, TPW, true><<<blocks, MP_TR_COLS, smem, stream>>>(p, dt, nonlocal ? 1 : 0, ngx, tg);
+    else
+        k_tracers_mp<TWO, TPW, false><<<blocks, MP_TR_COLS, smem, stream>>>(p, dt, nonlocal ? 1 : 0, ngx, tg);
     if (p.mp_redo) launch_tracers_redo(p, dt, nonlocal, stream);
 }
 

@@ -76,7 +76,7 @@ __device__ __forceinline__ void tracer_row(int k, int nz, bool use_harmonic, dou
 
 // The columns of one warp: column (i, j) on this lane, `tid` its slot in the
 // block's shared memory of `bs` columns.
-template <int NTR, bool TWO>
+template <int NTR, bool TWO, bool DEF>
 __device__ __forceinline__ void tracer_columns(const Params &p, double dt, int diffuse, int nonlocal, int i, int j,
                                                double *smem, int tid, int bs)
 {
@@ -89,7 +89,9 @@ __device__ __forceinline__ void tracer_columns(const Params &p, double dt, int d
 #else
     constexpr int TR_U = NTR <= 8 ? 2 : 1;
 #endif
-    const vphys_config &c = p.cfg;
+    vphys_config cd = p.cfg;   // DEF: the default knobs folded in (is_default_tracer_knobs)
+    if (DEF) default_tracer_knobs(cd);
+    const vphys_config &c = cd;
     const int nx = p.nx, nz = p.nz, ntr = p.ntr;
     const size_t P = p.plane;
     const bool in_grid = i < nx;
@@ -330,11 +332,11 @@ __device__ __forceinline__ void tracer_columns(const Params &p, double dt, int d
 #undef HH
 }
 
-template <int NTR, bool TWO>
+template <int NTR, bool TWO, bool DEF>
 __global__ void __launch_bounds__(128) k_tracers(const Params p, double dt, int diffuse, int nonlocal)
 {
     extern __shared__ double smem[];
-    tracer_columns<NTR, TWO>(p, dt, diffuse, nonlocal, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y, smem,
+    tracer_columns<NTR, TWO, DEF>(p, dt, diffuse, nonlocal, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y, smem,
                              threadIdx.x, blockDim.x);
 }
 
@@ -361,7 +363,7 @@ __global__ void __launch_bounds__(32) k_tracers_redo(const Params p, double dt, 
         q.cfg.idx_salinity = (tix == c.idx_salinity) ? 0 : -1;
         q.cfg.idx_pseudo_salt = (tix == c.idx_pseudo_salt) ? 0 : -1;
         if (!p.ks_equals_kt && tix != c.idx_temperature) q.kt = p.ks;   // the second factorisation's tracers
-        tracer_columns<1, false>(q, dt, 1, nonlocal, gi * 32 + (int)threadIdx.x, j, smem, threadIdx.x, 32);
+        tracer_columns<1, false, false>(q, dt, 1, nonlocal, gi * 32 + (int)threadIdx.x, j, smem, threadIdx.x, 32);
         __syncwarp();
     }
 }
@@ -388,12 +390,16 @@ static void launch_tracers_n(const Params &p, double dt, bool diffuse, bool nonl
     const size_t smem = (size_t)p.nz * bs * sizeof(double) * (TWO ? 2 : 1);
     static bool attr_set = false;
     if (!attr_set) {
-        cudaFuncSetAttribute(k_tracers<NTR, TWO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)((size_t)VPHYS_NZ_MAX * bs * sizeof(double) * (TWO ? 2 : 1)));
+        const int mx = (int)((size_t)VPHYS_NZ_MAX * bs * sizeof(double) * (TWO ? 2 : 1));
+        cudaFuncSetAttribute(k_tracers<NTR, TWO, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+        cudaFuncSetAttribute(k_tracers<NTR, TWO, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
         attr_set = true;
     }
     dim3 grid((p.nx + bs - 1) / bs, p.ny);
-    k_tracers<NTR, TWO><<<grid, bs, smem, stream>>>(p, dt, diffuse ? 1 : 0, nonlocal ? 1 : 0);
+    if (is_default_tracer_knobs(p.cfg))
+        k_tracers<NTR, TWO, true><<<grid, bs, smem, stream>>>(p, dt, diffuse ? 1 : 0, nonlocal ? 1 : 0);
+    else
+        k_tracers<NTR, TWO, false><<<grid, bs, smem, stream>>>(p, dt, diffuse ? 1 : 0, nonlocal ? 1 : 0);
 }
 
 void launch_tracers(const Params &p, double dt, bool diffuse, bool nonlocal, cudaStream_t stream)
