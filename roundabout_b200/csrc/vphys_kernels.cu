@@ -169,12 +169,12 @@ __global__ void k_stress_mag(const Params p, double *out)
 // ---------------------------------------------------------------------------
 constexpr int ASM_THREADS = 128;
 // Layers per load block of the FP32 interface sweep (1440x1080x75: 1.97 ms
-// loading each layer when its interface needs it, 1.60 ms with 2, more
-// with 3, 4 or 8 whose registers cost warps).  The FP64 sweep keeps the
-// on-demand loads: its exact divisions already cover the load latency, and
-// blocks measured slower (2.65 -> 2.75 ms with 2).
+// loading each layer when its interface needs it, 1.60 ms with 2, 1.50 ms
+// with 3 once the default-knob instantiation freed registers).  The FP64 sweep
+// keeps the on-demand loads: its exact divisions already cover the load
+// latency, and blocks measured slower there (2.65 -> 2.75 ms with 2).
 #ifndef VPHYS_ASM_U_F
-#define VPHYS_ASM_U_F 2
+#define VPHYS_ASM_U_F 3
 #endif
 
 // The assembly knobs of the default (benchmark) configuration: PP81, KPP
