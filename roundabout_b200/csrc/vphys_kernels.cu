@@ -172,7 +172,8 @@ constexpr int ASM_THREADS = 128;
 // loading each layer when its interface needs it, 1.60 ms with 2, 1.50 ms
 // with 3 once the default-knob instantiation freed registers).  The FP64 sweep
 // keeps the on-demand loads: its exact divisions already cover the load
-// latency, and blocks measured slower there (2.65 -> 2.75 ms with 2).
+// latency, and blocks measured slower there (default-knob instantiation:
+// 2.14 ms on demand, 2.46 with 2, 2.43 with 3; VPHYS_ASM_U_D sets it).
 #ifndef VPHYS_ASM_U_F
 #define VPHYS_ASM_U_F 3
 #endif
@@ -387,8 +388,11 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
     // layers q and q-1 only when h_{q-1} + h_q > 0, so no needed layer lies
     // lower, and the 0-thickness fillers under the bathymetry and land columns
     // load nothing.  The loaded values are the same either way.
-    constexpr bool PREF = sizeof(R) == sizeof(float);
-    constexpr int ASM_U = PREF ? VPHYS_ASM_U_F : 1;
+#ifndef VPHYS_ASM_U_D
+#define VPHYS_ASM_U_D 1   // FP64 sweep: on-demand loads (1) or blocks of this many layers
+#endif
+    constexpr bool PREF = sizeof(R) == sizeof(float) || VPHYS_ASM_U_D > 1;
+    constexpr int ASM_U = (sizeof(R) == sizeof(float)) ? VPHYS_ASM_U_F : (PREF ? VPHYS_ASM_U_D : 1);
     int k_lo = nz + 2;
     if (PREF && !all_zero) {
         for (int k0 = 1; k0 <= nz && k_lo > nz; k0 += 8) {
