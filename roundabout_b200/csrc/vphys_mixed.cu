@@ -56,7 +56,10 @@ constexpr int MP_TR_COLS = 32;      // columns (lanes) per tracer block
 #define VPHYS_MP_MOM_U 6   // 1440x1080x75 default-knob solve: 3.10 ms with 4, 2.87 with 6 or 8 (still 11 warps/SM)
 #endif
 constexpr int MP_TR_U = VPHYS_MP_TR_U;                // levels per tracer load block
-constexpr int MP_TR_UF = 4;   // levels per load block of the back-substitution with the non-local deposit
+#ifndef VPHYS_MP_TR_UF
+#define VPHYS_MP_TR_UF 6   // 1440x1080x75 step: 8.955 ms with 4, 8.898 with 6, 9.40 with 8
+#endif
+constexpr int MP_TR_UF = VPHYS_MP_TR_UF;   // levels per load block of the back-substitution with the non-local deposit
 constexpr int MP_MOM_THREADS = VPHYS_MP_MOM_THREADS;  // face columns per momentum block
 constexpr int MP_MOM_U = VPHYS_MP_MOM_U;              // levels per momentum load block
 // Largest tracer increment (in the tracer's units) a mixed solve keeps.  The
