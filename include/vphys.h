@@ -165,6 +165,36 @@ typedef struct vphys_config {
     double sw_band_ratio;     /* R, 0.58 */
     double sw_zeta1;          /* m, 0.35 */
     double sw_zeta2;          /* m, 23 */
+    /* kappa-shear interior closure, column form (ocean_kappa_shear_t,
+     * rdb_ocean_kappa_shear.F90:86-224; Jackson, Hallberg & Legg 2008).
+     * kappa_shear = 1: vphys_step refreshes kd_shear once a step
+     * (vphys_kappa_shear, kappa_shear_compute) and every assembly adds
+     * kd_shear to kt and ks_prandtl_turb * kd_shear to kv after KPP, before
+     * the split and the floors (kappa_shear_merge_into_kv_kt,
+     * rdb_ocean_dyn.F90:1564-1583).  The vertex form (at_vertex) and the
+     * massless merge are not built. */
+    int kappa_shear;          /* 0 */
+    int ks_max_inner_it;      /* Picard iterations, 50 (MAX_RINO_IT) */
+    int ks_max_substep_it;    /* adaptive substeps, 13 (MAX_KAPPA_SHEAR_IT) */
+    int ks_eos;               /* buoyancy derivatives from: 0 the Wright 1997 EOS, 1 a linear EOS
+                                 (ks_alpha_t, ks_beta_s, rho0) -- eos_specvol_derivs, rdb_eos.F90:1551-1622 */
+    double ks_ri_crit;        /* 0.25 */
+    double ks_shearmix_rate;  /* 0.089 */
+    double ks_fri_curvature;  /* -0.97 */
+    double ks_c_n;            /* 0.24 */
+    double ks_c_s;            /* 0.14 */
+    double ks_lambda;         /* 0.82 */
+    double ks_lz_rescale;     /* 1 */
+    double ks_kappa_0;        /* 1e-7 m2/s */
+    double ks_kappa_seed;     /* 1 m2/s */
+    double ks_kappa_trunc;    /* 1e-9 m2/s */
+    double ks_tke_bg;         /* 0 m2/s2 */
+    double ks_tol_err;        /* 0.1 */
+    double ks_src_max_chg;    /* 10 */
+    double ks_prandtl_turb;   /* 1 */
+    double ks_vel_underflow;  /* 0 m/s */
+    double ks_alpha_t;        /* linear EOS only: kg m-3 K-1 */
+    double ks_beta_s;         /* linear EOS only: kg m-3 psu-1 */
 } vphys_config;
 
 #define VPHYS_KPP_SW_ALL 1
@@ -200,9 +230,12 @@ enum vphys_field {
     VPHYS_FIELD_K_TOP_V = 24,   /* in int32 (nx, ny+1) */
     VPHYS_FIELD_K_BOT_U = 25,   /* in int32 (nx+1, ny), 1-based (default 1) */
     VPHYS_FIELD_K_BOT_V = 26,   /* in int32 (nx, ny+1) */
-    VPHYS_FIELD_CORIOLIS = 27,  /* in      (nx, ny)  f, 1/s: read only by the learned KPP's features */
+    VPHYS_FIELD_CORIOLIS = 27,  /* in      (nx, ny)  f at cell centres, 1/s: read by the learned KPP's
+                                   features and by kappa-shear (f^2) */
     VPHYS_FIELD_HEAT_BUDGET_SURFACE = 28, /* in/out (nx, ny, nz) the surface deposit's heat contributor */
     VPHYS_FIELD_SALT_BUDGET_SURFACE = 29, /* in/out (nx, ny, nz) */
+    VPHYS_FIELD_KD_SHEAR = 30,  /* in/out  (nx, ny, nz+1) kappa-shear diffusivity kd_int, 0 at bed and surface */
+    VPHYS_FIELD_TKE_SHEAR = 31, /* out     (nx, ny, nz+1) kappa-shear time-mean TKE tke_int */
     VPHYS_FIELD_TRACER0 = 64    /* in/out  (nx, ny, nz); tracer t is
                                    VPHYS_FIELD_TRACER0 + t */
 };
@@ -299,6 +332,20 @@ int vphys_surface_flux(vphys_handle h, double dt);
  * it there when surface_flux is 1. */
 int vphys_sw_penetration(vphys_handle h, double dt);
 
+/* Kappa-shear, column form: per wet column, the JHL08 steady (kappa, TKE)
+ * pair solved surface-down on the interfaces with adaptive substepping over
+ * dt (a kappa_0 background pre-step, frozen EOS buoyancy derivatives at the
+ * hydrostatic pressure, predictor-corrector substeps, Picard inner solves),
+ * from H, U and V averaged to cell centres, the temperature and salinity
+ * tracers, and CORIOLIS (f^2).  Writes KD_SHEAR (the time-mean diffusivity,
+ * 0 on the bed and surface interfaces and in land columns) and TKE_SHEAR.
+ * Layers thinner than H_VANISHED enter at H_VANISHED.  A no-op without a
+ * temperature or salinity tracer.  Replaces kappa_shear_compute ->
+ * kappa_shear_column_kernel (rdb_ocean_kappa_shear.F90:427-648, the solver
+ * 953-1909); vphys_step runs it before the assembly when kappa_shear is 1,
+ * and the assembly adds KD_SHEAR (rdb_ocean_dyn.F90:1564-1583). */
+int vphys_kappa_shear(vphys_handle h, double dt);
+
 /* Mixed-precision tracer solves (mixed_precision >= 1): the number of
  * (32-column group, tracer) pairs whose one-step increment reached 2 units
  * in the last solve and were re-solved on the FP64 path (bitwise the exact
@@ -306,7 +353,9 @@ int vphys_sw_penetration(vphys_handle h, double dt);
 int vphys_mixed_redo_count(vphys_handle h, unsigned *groups);
 
 /* The whole coefficient build: interior closure (PP81 or background seed),
- * KPP overlay (+ bl_depth, b0, gamma_t/gamma_s), KV_ML_INVZ2, convection,
+ * KPP overlay (+ bl_depth, b0, gamma_t/gamma_s), the kappa-shear merge
+ * (kt += KD_SHEAR, kv += ks_prandtl_turb * KD_SHEAR when kappa_shear is 1),
+ * KV_ML_INVZ2, convection,
  * heat/salt split, assembly gate (guard, Bryan-Lewis or scalar floors,
  * ceilings, optional 1-2-1 smoothing).  Replaces vmix_build_coefficients
  * (rdb_ocean_dyn.F90:1473-1634) with vmix_compute_pp81

@@ -636,8 +636,9 @@ int vpo_assemble_gate(const vphys_config *c, vpo_state *s)
     return status;
 }
 
-/* vmix_build_coefficients (rdb_ocean_dyn.F90:1473-1634), default
- * contributors only (no EPBL / kappa-shear / tidal / BBL mixing). */
+/* vmix_build_coefficients (rdb_ocean_dyn.F90:1473-1634) with the
+ * kappa-shear merge of the kd_shear last computed (1564-1583); no EPBL /
+ * tidal / BBL mixing. */
 int vpo_build_coefficients(const vphys_config *c, vpo_state *s)
 {
     if (c->interior_closure == VPHYS_INTERIOR_PP81)
@@ -645,6 +646,7 @@ int vpo_build_coefficients(const vphys_config *c, vpo_state *s)
     else
         vpo_seed_interior_none(c, s);
     if (c->use_kpp) vpo_kpp_overlay(c, s);
+    if (c->kappa_shear) vpo_kappa_shear_merge(c, s);
     vpo_kv_ml_invz2(c, s);
     if (c->conv_enable) vpo_convection(c, s);
     vpo_split(c, s);
@@ -1135,6 +1137,7 @@ int vpo_step(const vphys_config *c, vpo_state *s, double dt, int n_steps)
             vpo_surface_flux(c, s, dt);
             vpo_sw_penetration(c, s, dt);
         }
+        if (c->kappa_shear) vpo_kappa_shear(c, s, dt);
         st |= vpo_build_coefficients(c, s);
         vpo_vdiff_momentum(c, s, dt);
         vpo_vdiff_tracers(c, s, dt);

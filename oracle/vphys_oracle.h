@@ -39,6 +39,8 @@ typedef struct vpo_state {
     int *k_top_u, *k_top_v, *k_bot_u, *k_bot_v;   /* 1-based */
     double **tr;                            /* ntr pointers */
     double *heat_budget_surface, *salt_budget_surface;
+    double *coriolis;                       /* (nx,ny) f; NULL reads as 0 */
+    double *kd_shear, *tke_shear;           /* (nx,ny,nz+1) kappa-shear kd_int, tke_int */
 } vpo_state;
 
 void vpo_set_threads(int n);
@@ -66,6 +68,10 @@ void vpo_surface_flux(const vphys_config *c, vpo_state *s, double dt);
 void vpo_eos_buoyancy_coeffs(double T, double S, double p, double *alpha_T, double *beta_S);
 double vpo_sm_exp(double x);
 void vpo_sw_penetration(const vphys_config *c, vpo_state *s, double dt);
+
+/* kappa-shear, column form (vphys_oracle_kshear.c) */
+void vpo_kappa_shear(const vphys_config *c, vpo_state *s, double dt);
+void vpo_kappa_shear_merge(const vphys_config *c, vpo_state *s);
 
 int vpo_step(const vphys_config *c, vpo_state *s, double dt, int n_steps);
 

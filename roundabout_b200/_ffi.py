@@ -65,6 +65,8 @@ FIELD_K_BOT_V = 26
 FIELD_CORIOLIS = 27
 FIELD_HEAT_BUDGET_SURFACE = 28
 FIELD_SALT_BUDGET_SURFACE = 29
+FIELD_KD_SHEAR = 30
+FIELD_TKE_SHEAR = 31
 FIELD_TRACER0 = 64
 
 FIELD_NAMES = {
@@ -77,6 +79,7 @@ FIELD_NAMES = {
     "k_top_u": FIELD_K_TOP_U, "k_top_v": FIELD_K_TOP_V, "k_bot_u": FIELD_K_BOT_U,
     "k_bot_v": FIELD_K_BOT_V, "coriolis": FIELD_CORIOLIS,
     "heat_budget_surface": FIELD_HEAT_BUDGET_SURFACE, "salt_budget_surface": FIELD_SALT_BUDGET_SURFACE,
+    "kd_shear": FIELD_KD_SHEAR, "tke_shear": FIELD_TKE_SHEAR,
 }
 INT_FIELDS = (FIELD_K_TOP_U, FIELD_K_TOP_V, FIELD_K_BOT_U, FIELD_K_BOT_V)
 
@@ -90,7 +93,7 @@ def field_shape(field: int, nx: int, ny: int, nz: int):
         return (nx + 1, ny, nz)
     if field in (FIELD_V, FIELD_VISC_REM_V):
         return (nx, ny + 1, nz)
-    if field in (FIELD_KV, FIELD_KT, FIELD_KS, FIELD_GAMMA_T, FIELD_GAMMA_S):
+    if field in (FIELD_KV, FIELD_KT, FIELD_KS, FIELD_GAMMA_T, FIELD_GAMMA_S, FIELD_KD_SHEAR, FIELD_TKE_SHEAR):
         return (nx, ny, nz + 1)
     if field in (FIELD_BL_DEPTH, FIELD_B0, FIELD_STRESS_MAG, FIELD_Q_HEAT, FIELD_Q_SALT, FIELD_WET, FIELD_CORIOLIS):
         return (nx, ny)
@@ -128,6 +131,14 @@ class VphysConfig(ctypes.Structure):
         ("buoyancy_coeffs", ctypes.c_int), ("kpp_sw_method", ctypes.c_int),
         ("sw_pen_frac", ctypes.c_double), ("sw_band_ratio", ctypes.c_double), ("sw_zeta1", ctypes.c_double),
         ("sw_zeta2", ctypes.c_double),
+        ("kappa_shear", ctypes.c_int), ("ks_max_inner_it", ctypes.c_int), ("ks_max_substep_it", ctypes.c_int),
+        ("ks_eos", ctypes.c_int),
+        ("ks_ri_crit", ctypes.c_double), ("ks_shearmix_rate", ctypes.c_double), ("ks_fri_curvature", ctypes.c_double),
+        ("ks_c_n", ctypes.c_double), ("ks_c_s", ctypes.c_double), ("ks_lambda", ctypes.c_double),
+        ("ks_lz_rescale", ctypes.c_double), ("ks_kappa_0", ctypes.c_double), ("ks_kappa_seed", ctypes.c_double),
+        ("ks_kappa_trunc", ctypes.c_double), ("ks_tke_bg", ctypes.c_double), ("ks_tol_err", ctypes.c_double),
+        ("ks_src_max_chg", ctypes.c_double), ("ks_prandtl_turb", ctypes.c_double),
+        ("ks_vel_underflow", ctypes.c_double), ("ks_alpha_t", ctypes.c_double), ("ks_beta_s", ctypes.c_double),
     ]
 
     def as_dict(self):
@@ -194,6 +205,7 @@ _PROTOTYPES = {
     "vphys_stress_mag": (ctypes.c_int, [ctypes.c_void_p]),
     "vphys_surface_flux": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "vphys_sw_penetration": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    "vphys_kappa_shear": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "vphys_mixed_redo_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint)]),
     "vphys_assemble": (ctypes.c_int, [ctypes.c_void_p]),
     "vphys_vdiff_momentum": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),

@@ -156,6 +156,11 @@ class VerticalPhysics:
         """ocean_surface_flux_apply_sw_penetration (rdb_ocean_surface_flux.F90:1255-1370)."""
         _ffi.check(self.lib.vphys_sw_penetration(self._h, float(dt)), "vphys_sw_penetration")
 
+    def kappa_shear(self, dt):
+        """kappa_shear_compute, column form (rdb_ocean_kappa_shear.F90:427-648):
+        fills the kd_shear / tke_shear fields."""
+        _ffi.check(self.lib.vphys_kappa_shear(self._h, float(dt)), "vphys_kappa_shear")
+
     def assemble(self):
         return _ffi.check(self.lib.vphys_assemble(self._h), "vphys_assemble")
 

@@ -84,6 +84,27 @@ def default_config() -> VphysConfig:
     c.budgets = 0
     c.mixed_precision = 0
     c.learned_kpp = 0
+    c.kappa_shear = 0
+    c.ks_max_inner_it = 50
+    c.ks_max_substep_it = 13
+    c.ks_eos = 0
+    c.ks_ri_crit = 0.25
+    c.ks_shearmix_rate = 0.089
+    c.ks_fri_curvature = -0.97
+    c.ks_c_n = 0.24
+    c.ks_c_s = 0.14
+    c.ks_lambda = 0.82
+    c.ks_lz_rescale = 1.0
+    c.ks_kappa_0 = 1.0e-7
+    c.ks_kappa_seed = 1.0
+    c.ks_kappa_trunc = 1.0e-9
+    c.ks_tke_bg = 0.0
+    c.ks_tol_err = 0.1
+    c.ks_src_max_chg = 10.0
+    c.ks_prandtl_turb = 1.0
+    c.ks_vel_underflow = 0.0
+    c.ks_alpha_t = 0.0
+    c.ks_beta_s = 0.0
     return c
 
 
@@ -205,6 +226,25 @@ class ConvectiveAdjustment:
         cfg.conv_kd = float(self.kd)
         cfg.conv_prandtl = float(self.prandtl)
         cfg.conv_n2_thresh = float(self.n2_threshold)
+        return cfg
+
+
+class KappaShear:
+    """JHL08 prognostic interior shear turbulence, column form
+    (python/rdb/closures.py:152-180: `KappaShear(ri_crit=0.25, prandtl=1.0,
+    at_vertex=False, ...)`).  The vertex (corner) form is not built here:
+    `at_vertex=True` raises.  The iteration-control knobs are the `ks_*`
+    fields of the config."""
+
+    def __init__(self, ri_crit=0.25, prandtl=1.0, at_vertex=False, vertex_geometric_mean=False, vertex_kdmin=0.0):
+        if at_vertex or vertex_geometric_mean:
+            raise NotImplementedError("KappaShear: the vertex (corner) form is not built; use the column form")
+        self.ri_crit, self.prandtl = ri_crit, prandtl
+
+    def apply(self, cfg):
+        cfg.kappa_shear = 1
+        cfg.ks_ri_crit = float(self.ri_crit)
+        cfg.ks_prandtl_turb = float(self.prandtl)
         return cfg
 
 

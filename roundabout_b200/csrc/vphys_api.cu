@@ -50,7 +50,7 @@ int cuda_status(cudaError_t e, const char *where)
     return push_error(VPHYS_ERR_CUDA, "%s: CUDA error %d (%s)", where, (int)e, cudaGetErrorString(e));
 }
 
-constexpr int NFIXED = 30;
+constexpr int NFIXED = 32;
 constexpr unsigned MAGIC = 0x56504859u;   // "VPHY"
 
 struct Field {
@@ -125,7 +125,9 @@ size_t field_count(int nx, int ny, int nz, int field, bool *is_int)
     case VPHYS_FIELD_KT:
     case VPHYS_FIELD_KS:
     case VPHYS_FIELD_GAMMA_T:
-    case VPHYS_FIELD_GAMMA_S: return X * Y * (Z + 1);
+    case VPHYS_FIELD_GAMMA_S:
+    case VPHYS_FIELD_KD_SHEAR:
+    case VPHYS_FIELD_TKE_SHEAR: return X * Y * (Z + 1);
     case VPHYS_FIELD_BL_DEPTH:
     case VPHYS_FIELD_B0:
     case VPHYS_FIELD_STRESS_MAG:
@@ -245,6 +247,16 @@ int validate(const vphys_config *c, int ntr)
     if (c->bkgnd_profile && c->bkgnd_delta == 0.0) return push_error(VPHYS_ERR_CONFIG, "bkgnd_delta must be nonzero");
     if (c->bkgnd_prandtl == 0.0)
         return push_error(VPHYS_ERR_CONFIG, "bkgnd_prandtl = 0 is refused (use -1 for off), as the reference does");
+    if (c->kappa_shear < 0 || c->kappa_shear > 1) return push_error(VPHYS_ERR_CONFIG, "kappa_shear must be 0 or 1");
+    // the inner solve must run at least once (the substep's adaptive-dt bands
+    // read its decay lengths); both caps bound the per-column work
+    if (c->ks_max_inner_it < 1 || c->ks_max_inner_it > 10000)
+        return push_error(VPHYS_ERR_CONFIG, "ks_max_inner_it must be in [1, 10000]");
+    if (c->ks_max_substep_it < 0 || c->ks_max_substep_it > 10000)
+        return push_error(VPHYS_ERR_CONFIG, "ks_max_substep_it must be in [0, 10000]");
+    if (c->ks_eos < 0 || c->ks_eos > 1) return push_error(VPHYS_ERR_CONFIG, "ks_eos must be 0 (Wright) or 1 (linear)");
+    if (c->ks_lambda == 0.0 || c->ks_lz_rescale == 0.0 || c->ks_src_max_chg == 0.0)
+        return push_error(VPHYS_ERR_CONFIG, "ks_lambda, ks_lz_rescale and ks_src_max_chg must be nonzero");
     return VPHYS_OK;
 }
 
@@ -297,6 +309,8 @@ Params make_params(vphys_handle h)
     p.mp_redo = h->mp_redo;
     p.zcol = h->zcol;
     p.coriolis = D(VPHYS_FIELD_CORIOLIS);
+    p.kd_shear = D(VPHYS_FIELD_KD_SHEAR);
+    p.tke_shear = D(VPHYS_FIELD_TKE_SHEAR);
     p.ks_equals_kt = (h->cfg.bkgnd_profile || h->cfg.kt_bg == h->cfg.ks_bg) ? 1 : 0;
     p.write_gamma = (p.gamma_t && p.gamma_s) ? 1 : 0;
     return p;
@@ -381,8 +395,19 @@ void surface_flux_scales(const vphys_config &c, double dt, double *inv_heat, dou
     *inv_salt = dt / c.rho0;
 }
 
+int prepare_kappa_shear(vphys_handle h)
+{
+    int st = VPHYS_OK;
+    if ((st = ensure(h, VPHYS_FIELD_KD_SHEAR))) return st;
+    return ensure(h, VPHYS_FIELD_TKE_SHEAR);
+}
+
 int prepare_assemble(vphys_handle h)
 {
+    if (h->cfg.kappa_shear) {
+        int st = prepare_kappa_shear(h);
+        if (st) return st;
+    }
     if (h->cfg.kd_smooth_iterations > 0 && !h->smooth_scratch) {
         size_t n = (size_t)h->nx * h->ny * (h->nz + 1);
         cudaError_t e = cudaMalloc(&h->smooth_scratch, n * sizeof(double));
@@ -444,8 +469,9 @@ void free_kpp(vphys_handle h)
 int run_assemble(vphys_handle h, const Params &p);
 
 // The launches of n whole steps (vmix_apply_in_stage on a thermo step,
-// rdb_ocean_dyn.F90:1636-1900): EOS, [surface deposit + shortwave], [learned KPP],
-// assembly, momentum, tracers with the non-local tendency.  All asynchronous
+// rdb_ocean_dyn.F90:1636-1900): EOS, [surface deposit + shortwave],
+// [kappa-shear], [learned KPP], assembly (with the kappa-shear merge), momentum,
+// tracers with the non-local tendency.  All asynchronous
 // on h->stream.
 // The momentum and tracer solves after the assembly touch disjoint data
 // (u, v, kv / tracers, kt, ks, b0), so the momentum solve runs on an
@@ -486,6 +512,8 @@ int launch_steps(vphys_handle h, const Params &p, double dt, int n_steps)
             if (h->cfg.sw_pen_frac != 0.0 && h->cfg.idx_temperature >= 0)
                 vphys::launch_sw_penetration(p, inv_heat, h->stream);
         }
+        if (h->cfg.kappa_shear && h->cfg.idx_temperature >= 0 && h->cfg.idx_salinity >= 0)
+            vphys::launch_kappa_shear(p, dt, h->stream);
         Params pa = p;
         if ((st = run_learned_kpp(h, pa))) return st;
         if ((st = run_assemble(h, pa))) return st;
@@ -615,6 +643,21 @@ int vphys_config_default(vphys_config *c)
     c->idx_temperature = 1;
     c->idx_salinity = 0;
     c->idx_pseudo_salt = -1;
+    c->ks_max_inner_it = 50;
+    c->ks_max_substep_it = 13;
+    c->ks_ri_crit = 0.25;
+    c->ks_shearmix_rate = 0.089;
+    c->ks_fri_curvature = -0.97;
+    c->ks_c_n = 0.24;
+    c->ks_c_s = 0.14;
+    c->ks_lambda = 0.82;
+    c->ks_lz_rescale = 1.0;
+    c->ks_kappa_0 = 1.0e-7;
+    c->ks_kappa_seed = 1.0;
+    c->ks_kappa_trunc = 1.0e-9;
+    c->ks_tol_err = 0.1;
+    c->ks_src_max_chg = 10.0;
+    c->ks_prandtl_turb = 1.0;
     return VPHYS_OK;
 }
 
@@ -878,6 +921,17 @@ int vphys_sw_penetration(vphys_handle h, double dt)
     Params p = make_params(h);
     vphys::launch_sw_penetration(p, inv_heat, h->stream);
     return cuda_status(cudaGetLastError(), "vphys_sw_penetration launch");
+}
+
+int vphys_kappa_shear(vphys_handle h, double dt)
+{
+    if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_kappa_shear: bad handle");
+    if (h->cfg.idx_temperature < 0 || h->cfg.idx_salinity < 0) return VPHYS_OK;
+    int st = prepare_kappa_shear(h);
+    if (st) return st;
+    Params p = make_params(h);
+    vphys::launch_kappa_shear(p, dt, h->stream);
+    return cuda_status(cudaGetLastError(), "vphys_kappa_shear launch");
 }
 
 int vphys_mixed_redo_count(vphys_handle h, unsigned *groups)

@@ -184,10 +184,11 @@ constexpr int ASM_THREADS = 128;
 __host__ __device__ __forceinline__ bool is_default_assembly_knobs(const vphys_config &c)
 {
     return c.interior_closure == VPHYS_INTERIOR_PP81 && c.use_kpp && c.bkgnd_profile && !(c.kv_ml_invz2 > 0.0) &&
-           !c.conv_enable && !c.vmix_guard && !c.buoyancy_coeffs && c.sw_pen_frac == 0.0;
+           !c.conv_enable && !c.vmix_guard && !c.buoyancy_coeffs && c.sw_pen_frac == 0.0 && !c.kappa_shear;
 }
 __device__ __forceinline__ void default_assembly_knobs(vphys_config &c)
 {
+    c.kappa_shear = 0;
     c.interior_closure = VPHYS_INTERIOR_PP81;
     c.use_kpp = 1;
     c.bkgnd_profile = 1;
@@ -344,6 +345,7 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
     const R kv_max = (R)c.kv_max, kd_max = (R)c.kd_max, kt_bg = (R)c.kt_bg, ks_bg = (R)c.ks_bg;
     const R cs = (R)c.cs_nonlocal, qT = (R)q_T_kin, qS = (R)q_S_kin, hbR = (R)h_b, wsR = (R)w_s;
     const R invz2 = (R)c.kv_ml_invz2, conv_kd = (R)c.conv_kd, conv_pr = (R)c.conv_prandtl, conv_n2 = (R)c.conv_n2_thresh;
+    const R ks_pr = (R)c.ks_prandtl_turb;
     // gate constants (vmix_assemble, rdb_ocean_vmix.F90:2279-2348)
     const R pr_bl = (R)((c.bkgnd_prandtl > 0.0) ? c.bkgnd_prandtl : 1.0);
     const R kv_floor_scalar = (R)((c.bkgnd_prandtl > 0.0) ? c.bkgnd_prandtl * c.kt_bg + c.kv_bg : c.kv_bg);
@@ -497,6 +499,13 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
                 }
             }
             if (q >= 2) {
+                // ---- kappa-shear merge after KPP, interior interfaces only
+                //      (kappa_shear_merge_into_kv_kt, rdb_ocean_kappa_shear.F90:381-421) ----
+                if (c.kappa_shear) {
+                    const R kd = (R)p.kd_shear[col + P * (size_t)(q - 1)];
+                    ktq = ktq + kd;
+                    kvq = kvq + ks_pr * kd;
+                }
                 // ---- KV_ML_INVZ2 (rdb_ocean_vmix.F90:1757-1765) ----
                 if (invz2_on) {
                     if (depth >= hmix) {

@@ -45,7 +45,8 @@ struct Params {
     int *span;                        // per column: first | last live layer << 16 (0: none), scratch
     unsigned *mp_redo;                // mixed solves: count, then (group << 5 | tracer) re-solved in FP64
     double *zcol;                     // per column: -sum_k h, k = 1..nz in order (momentum z_clear), scratch
-    const double *coriolis;           // (nx, ny) f, or nullptr (learned KPP features only)
+    const double *coriolis;           // (nx, ny) f, or nullptr (learned KPP features, kappa-shear f^2)
+    double *kd_shear, *tke_shear;     // (nx, ny, nz+1) kappa-shear diffusivity and TKE, or nullptr
     const float *kpp_pred;            // per column: the surrogate's h_b, < 0: run pass 1; nullptr: plain KPP
     const float *kpp_check;           // per column: h_b to compare with pass 1 (>= 0), or nullptr
     unsigned long long *kpp_stats;    // learned KPP counters (k_kpp_roll)
@@ -64,6 +65,8 @@ void launch_surface_flux(const Params &p, double inv_heat, double inv_salt, cuda
 // the penetrating shortwave spread down the column; inv_scale = dt/(rho0 cp)
 void launch_sw_penetration(const Params &p, double inv_scale, cudaStream_t stream);
 void launch_stress_mag(const Params &p, cudaStream_t stream);
+// kappa-shear column solve into p.kd_shear / p.tke_shear (vphys_kshear.cu)
+void launch_kappa_shear(const Params &p, double dt, cudaStream_t stream);
 void launch_assemble(const Params &p, cudaStream_t stream);
 void launch_smooth(const Params &p, double *fld, double *scratch, cudaStream_t stream);
 void launch_momentum(const Params &p, double dt, cudaStream_t stream);

@@ -79,3 +79,21 @@ def test_create_without_a_device_fails_cleanly(lib):
     st = lib.vphys_create(8, 8, 4, 2, None, ctypes.byref(h))
     assert st in (_ffi.ERR_ALLOC, _ffi.ERR_CUDA) and h.value is None
     assert _ffi.last_error(0)
+
+
+def test_kappa_shear_knobs_are_validated(lib):
+    """The kappa-shear knobs are checked at create, before any device work."""
+    from roundabout_b200 import _ffi
+    from roundabout_b200.config import KappaShear, default_config
+
+    h = ctypes.c_void_p()
+    for name, value in (("ks_max_inner_it", 0), ("ks_max_substep_it", -1), ("ks_eos", 2), ("ks_lambda", 0.0),
+                        ("kappa_shear", 2)):
+        bad = default_config()
+        setattr(bad, name, value)
+        assert lib.vphys_create(4, 4, 4, 2, ctypes.byref(bad), ctypes.byref(h)) == _ffi.ERR_CONFIG, name
+        assert h.value is None
+    cfg = KappaShear(ri_crit=0.3, prandtl=0.8).apply(default_config())
+    assert cfg.kappa_shear == 1 and cfg.ks_ri_crit == 0.3 and cfg.ks_prandtl_turb == 0.8
+    with pytest.raises(NotImplementedError):
+        KappaShear(at_vertex=True)
