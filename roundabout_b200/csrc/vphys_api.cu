@@ -91,6 +91,9 @@ struct vphys_handle_s {
     cudaStream_t aux_stream = nullptr;   // the momentum solve, forked from `stream` after the assembly
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaGraphExec_t gexec = nullptr;
+    int *ks_work = nullptr;            // kappa-shear: each column's cost in the last solve
+    int *ks_order = nullptr;           // kappa-shear: the solve order built from ks_work
+    unsigned *ks_hist = nullptr;       // kappa-shear: cost-bucket counts / offsets (1024)
     unsigned char gsig[sizeof(Params) + sizeof(vphys_kpp_model) + 32] = {};
 };
 
@@ -399,7 +402,29 @@ int prepare_kappa_shear(vphys_handle h)
 {
     int st = VPHYS_OK;
     if ((st = ensure(h, VPHYS_FIELD_KD_SHEAR))) return st;
-    return ensure(h, VPHYS_FIELD_TKE_SHEAR);
+    if ((st = ensure(h, VPHYS_FIELD_TKE_SHEAR))) return st;
+    if (!h->ks_work) {
+        const size_t n = (size_t)h->nx * h->ny;
+        cudaError_t e = cudaMalloc(&h->ks_work, n * sizeof(int));
+        if (e == cudaSuccess) e = cudaMalloc(&h->ks_order, n * sizeof(int));
+        if (e == cudaSuccess) e = cudaMalloc(&h->ks_hist, 1024 * sizeof(unsigned));
+        if (e == cudaSuccess) e = cudaMemsetAsync(h->ks_work, 0, n * sizeof(int), h->stream);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            cudaFree(h->ks_work);
+            cudaFree(h->ks_order);
+            cudaFree(h->ks_hist);
+            h->ks_work = h->ks_order = nullptr;
+            h->ks_hist = nullptr;
+            return push_error(VPHYS_ERR_ALLOC, "cudaMalloc of the kappa-shear scheduling arrays failed");
+        }
+    }
+    return st;
+}
+
+void launch_kappa_shear(vphys_handle h, const Params &p, double dt)
+{
+    vphys::launch_kappa_shear(p, dt, h->ks_work, h->ks_order, h->ks_hist, true, h->stream);
 }
 
 int prepare_assemble(vphys_handle h)
@@ -513,7 +538,7 @@ int launch_steps(vphys_handle h, const Params &p, double dt, int n_steps)
                 vphys::launch_sw_penetration(p, inv_heat, h->stream);
         }
         if (h->cfg.kappa_shear && h->cfg.idx_temperature >= 0 && h->cfg.idx_salinity >= 0)
-            vphys::launch_kappa_shear(p, dt, h->stream);
+            launch_kappa_shear(h, p, dt);
         Params pa = p;
         if ((st = run_learned_kpp(h, pa))) return st;
         if ((st = run_assemble(h, pa))) return st;
@@ -735,6 +760,9 @@ int vphys_destroy(vphys_handle *hp)
     if (h->span) cudaFree(h->span);
     if (h->mp_redo) cudaFree(h->mp_redo);
     if (h->zcol) cudaFree(h->zcol);
+    if (h->ks_work) cudaFree(h->ks_work);
+    if (h->ks_order) cudaFree(h->ks_order);
+    if (h->ks_hist) cudaFree(h->ks_hist);
     free_kpp(h);
     if (h->gexec) cudaGraphExecDestroy(h->gexec);
     if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
@@ -930,7 +958,7 @@ int vphys_kappa_shear(vphys_handle h, double dt)
     int st = prepare_kappa_shear(h);
     if (st) return st;
     Params p = make_params(h);
-    vphys::launch_kappa_shear(p, dt, h->stream);
+    launch_kappa_shear(h, p, dt);
     return cuda_status(cudaGetLastError(), "vphys_kappa_shear launch");
 }
 

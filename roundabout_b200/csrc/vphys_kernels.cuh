@@ -65,8 +65,12 @@ void launch_surface_flux(const Params &p, double inv_heat, double inv_salt, cuda
 // the penetrating shortwave spread down the column; inv_scale = dt/(rho0 cp)
 void launch_sw_penetration(const Params &p, double inv_scale, cudaStream_t stream);
 void launch_stress_mag(const Params &p, cudaStream_t stream);
-// kappa-shear column solve into p.kd_shear / p.tke_shear (vphys_kshear.cu)
-void launch_kappa_shear(const Params &p, double dt, cudaStream_t stream);
+// kappa-shear column solve into p.kd_shear / p.tke_shear (vphys_kshear.cu).
+// work (per column, zeroed before the first call) carries each column's cost
+// from one call to the next; with `ordered`, the columns are solved heaviest
+// first through order (per column) bucketed in hist (1024 counts).
+void launch_kappa_shear(const Params &p, double dt, int *work, int *order, unsigned *hist, bool ordered,
+                        cudaStream_t stream);
 void launch_assemble(const Params &p, cudaStream_t stream);
 void launch_smooth(const Params &p, double *fld, double *scratch, cudaStream_t stream);
 void launch_momentum(const Params &p, double dt, cudaStream_t stream);

@@ -48,6 +48,7 @@ struct KsCol {
     double u_ps[N], v_ps[N], t_ps[N], s_ps[N], c1[N], n2p[N], s2p[N];
     // predictor / corrector
     double tke_pred[N], kappa_pred[N], kappa_mid[N], tke_fin[N], kappa_pred2[N];
+    int nwork;   // 4 per Picard iteration + 1 per projected-state sweep: the column's cost, for scheduling
 };
 
 // eos_specvol_derivs (rdb_eos.F90:1551-1622)
@@ -88,20 +89,22 @@ __device__ __forceinline__ double src_func(const KsPar &p, double n2, double s2)
 
 // ks_projected_state (:1034-1171): mix (u_c, v_c, t_c, s_c) with kap over
 // dt_now inside layers [ks, ke] into the _ps arrays; N2, S2 into n2o, s2o.
+//
+// The reference first copies the whole input column into the outputs and
+// zeroes c1; on the band path neither is observable (levels outside the band
+// read the inputs, and every c1 the back-substitution reads is written by the
+// forward sweep), so only the no-band path copies.
 template <int N>
 __device__ __noinline__ void projected_state(KsCol<N> &w, int nz, double dt_now, int ks, int ke, double vel_underflow,
-                                             const double *kap, double *n2o, double *s2o)
+                                             const double *__restrict__ kap, double *__restrict__ n2o,
+                                             double *__restrict__ s2o)
 {
-    const double *h = w.h, *idz_int = w.idz_int;
-    const double *u0 = w.u_c, *v0 = w.v_c, *t0 = w.t_c, *s0 = w.s_c;
-    double *u_o = w.u_ps, *v_o = w.v_ps, *t_o = w.t_ps, *s_o = w.s_ps, *c1 = w.c1;
-    for (int k = 1; k <= nz; ++k) {
-        u_o[k] = u0[k];
-        v_o[k] = v0[k];
-        t_o[k] = t0[k];
-        s_o[k] = s0[k];
-    }
-    for (int k = 1; k <= nz + 1; ++k) c1[k] = 0.0;
+    w.nwork += 1;
+    const double *__restrict__ h = w.h;
+    const double *__restrict__ idz_int = w.idz_int;
+    const double *__restrict__ u0 = w.u_c, *__restrict__ v0 = w.v_c, *__restrict__ t0 = w.t_c, *__restrict__ s0 = w.s_c;
+    double *__restrict__ u_o = w.u_ps, *__restrict__ v_o = w.v_ps, *__restrict__ t_o = w.t_ps, *__restrict__ s_o = w.s_ps;
+    double *__restrict__ c1 = w.c1;
 
     if (ks <= ke && dt_now > 0.0) {
         double a_b = dt_now * kap[ks + 1] * idz_int[ks + 1];
@@ -154,8 +157,10 @@ __device__ __noinline__ void projected_state(KsCol<N> &w, int nz, double dt_now,
         }
     } else {
         for (int k = 1; k <= nz; ++k) {
-            if (fabs(u_o[k]) < vel_underflow) u_o[k] = 0.0;
-            if (fabs(v_o[k]) < vel_underflow) v_o[k] = 0.0;
+            u_o[k] = (fabs(u0[k]) < vel_underflow) ? 0.0 : u0[k];
+            v_o[k] = (fabs(v0[k]) < vel_underflow) ? 0.0 : v0[k];
+            t_o[k] = t0[k];
+            s_o[k] = s0[k];
         }
     }
 
@@ -182,15 +187,21 @@ __device__ __noinline__ void projected_state(KsCol<N> &w, int nz, double dt_now,
 // pair for the buoyancy/shear profile (n2_in, s2_in), seeded from kseed and
 // k_q; writes tke_o, kappa_o, updates k_q in place.  Uses w.ksrc, w.tkedec,
 // w.ild2 and the aq..ck scratch.
+// Every array argument is a different member of w from the ones the solve
+// uses directly (the callers pass n2/s2 or n2p/s2p, kappa or kappa_out,
+// k_q or kq_tmp, and the tke/kappa outputs of that call), hence __restrict__.
 template <int N>
-__device__ __noinline__ void find_kappa_tke(KsCol<N> &w, const KsPar &p, int nz, double f2_val, const double *n2_in,
-                                            const double *s2_in, const double *kseed, double *k_q, double *tke_o,
-                                            double *kappa_o)
+__device__ __noinline__ void find_kappa_tke(KsCol<N> &w, const KsPar &p, int nz, double f2_val,
+                                            const double *__restrict__ n2_in, const double *__restrict__ s2_in,
+                                            const double *__restrict__ kseed, double *__restrict__ k_q,
+                                            double *__restrict__ tke_o, double *__restrict__ kappa_o)
 {
     const double kappa_0 = p.kappa_0, kappa_trunc = p.kappa_trunc, tke_bg = p.tke_bg, tke_min = p.tke_min;
-    const double *idz = w.idz, *hint = w.hint, *e1 = w.e1;
-    double *ksrc = w.ksrc, *tkedec = w.tkedec, *ild2 = w.ild2;
-    double *aq = w.aq, *dq = w.dq, *cq = w.cq, *dk = w.dk, *ck = w.ck;
+    const double *__restrict__ idz = w.idz, *__restrict__ hint = w.hint, *__restrict__ e1 = w.e1;
+    double *__restrict__ ksrc = w.ksrc, *__restrict__ tkedec = w.tkedec, *__restrict__ ild2 = w.ild2;
+    double *__restrict__ aq = w.aq, *__restrict__ dq = w.dq, *__restrict__ cq = w.cq, *__restrict__ dk = w.dk;
+    double *__restrict__ ck = w.ck;
+    const double *__restrict__ il2 = w.il2;
     int ks_src = nz + 2, ke_src = 0;
     ksrc[1] = 0.0;
     ksrc[nz + 1] = 0.0;
@@ -220,10 +231,12 @@ __device__ __noinline__ void find_kappa_tke(KsCol<N> &w, const KsPar &p, int nz,
 
     int ks_kap = 2, ke_kap = nz, ks_kp = 2, ke_kp = nz;
     for (int it = 1; it <= p.max_inner_it; ++it) {
+        w.nwork += 4;
         // (a) TKE sweep (ke_tke: an interface index, nz+1 = the bed)
         int ke_tke = (ke_kap > ke_kp ? ke_kap : ke_kp) + 1;
         if (ke_tke > nz + 1) ke_tke = nz + 1;
         const int kmax = ke_tke < nz ? ke_tke : nz;
+#pragma unroll 4
         for (int k = 1; k <= kmax; ++k) aq[k] = (0.5 * (kappa_o[k] + kappa_o[k + 1]) + kappa_0) * idz[k];
         dq[1] = -tke_o[1];
         tke_o[1] = tke_bg;
@@ -268,8 +281,9 @@ __device__ __noinline__ void find_kappa_tke(KsCol<N> &w, const KsPar &p, int nz,
         // (b) kappa sweep with the truncation ramp and range tracking
         ks_kp = ks_kap;
         ke_kp = ke_kap;
+#pragma unroll 4
         for (int kk = 2; kk <= nz; ++kk)
-            ild2[kk] = (tke_o[kk] > 0.0) ? xdiv(n2_in[kk] * p.ilambda2 + f2_val, tke_o[kk]) + w.il2[kk] : 1.0e30;
+            ild2[kk] = (tke_o[kk] > 0.0) ? xdiv(n2_in[kk] * p.ilambda2 + f2_val, tke_o[kk]) + il2[kk] : 1.0e30;
         dk[1] = 0.0;
         ck[2] = 0.0;
         double ckc_l = 1.0;
@@ -575,7 +589,6 @@ __device__ __noinline__ void solve_column(KsCol<N> &w, const KsPar &p, int nz, d
                 ke_src = kk;
             }
         }
-        for (int kk = 1; kk <= nz + 1; ++kk) kappa_out[kk] = kappa[kk];
         if (ks_src > ke_src) {
             // no source: the TKE seed is what the step averages
             double *tke = w.tke;
@@ -585,10 +598,10 @@ __device__ __noinline__ void solve_column(KsCol<N> &w, const KsPar &p, int nz, d
             for (int kk = 1; kk <= nz + 1; ++kk) kappa_out[kk] = 0.0;
             for (int kk = 2; kk <= nz; ++kk) w.ild2[kk] = 0.0;
         } else {
-            // (find_kappa_tke re-forms the same source, decay and TKE seed)
-            for (int kk = 1; kk <= nz + 1; ++kk) w.kq_tmp[kk] = k_q[kk];
-            find_kappa_tke(w, p, nz, f2_val, n2, s2, kappa, w.kq_tmp, w.tke, kappa_out);
-            for (int kk = 1; kk <= nz + 1; ++kk) k_q[kk] = w.kq_tmp[kk];
+            // find_kappa_tke re-forms the same source, decay and TKE seed,
+            // seeds kappa_out from kappa, and leaves in k_q what the
+            // reference copies back from its k_q copy
+            find_kappa_tke(w, p, nz, f2_val, n2, s2, kappa, k_q, w.tke, kappa_out);
         }
 
         // local_src of the adaptive-dt bands
@@ -671,11 +684,25 @@ __device__ __noinline__ void solve_column(KsCol<N> &w, const KsPar &p, int nz, d
     }
 }
 
+// Minimum resident 64-thread blocks per SM: 16 caps the solve at 64
+// registers (a few bytes of spill) for 32 warps per SM.  The solve waits on
+// its local-memory columns (the working sets of the resident threads far
+// exceed L1 and L2), so warps in flight buy more than registers:
+// 1440x1080x75, ordered columns: 824 ms at 128 registers (16 warps/SM),
+// 666 ms at 80, 588 ms at 64.
+#ifndef VPHYS_KS_MINB
+#define VPHYS_KS_MINB 16
+#endif
+
+// Thread t solves column order[t] (t itself without an order) and records
+// the column's cost in work[col] (0 for land) for the next call's ordering.
 template <int N>
-__global__ void __launch_bounds__(64) k_kappa_shear(Params p, KsPar kp, double dt)
+__global__ void __launch_bounds__(64, VPHYS_KS_MINB) k_kappa_shear(Params p, KsPar kp, double dt,
+                                                                    const int *__restrict__ order, int *work)
 {
-    const size_t col = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-    if (col >= p.plane) return;
+    const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (t >= p.plane) return;
+    const size_t col = order ? (size_t)order[t] : t;
     const int nx = p.nx, nz = p.nz;
     const int i = (int)(col % (size_t)nx), j = (int)(col / (size_t)nx);
     double *kd = p.kd_shear, *tke = p.tke_shear;
@@ -685,9 +712,11 @@ __global__ void __launch_bounds__(64) k_kappa_shear(Params p, KsPar kp, double d
             kd[col + (size_t)k * plane] = 0.0;
             tke[col + (size_t)k * plane] = 0.0;
         }
+        if (work) work[col] = 0;
         return;
     }
     KsCol<N> w;
+    w.nwork = 0;
     const double *T = p.tr[p.cfg.idx_temperature], *S = p.tr[p.cfg.idx_salinity];
     const size_t ucol = (size_t)j * (nx + 1) + i, vcol = col;
     for (int k = 1; k <= nz; ++k) {
@@ -707,6 +736,60 @@ __global__ void __launch_bounds__(64) k_kappa_shear(Params p, KsPar kp, double d
         const bool edge = (k == 1 || k == nz + 1);
         kd[col + kg * plane] = edge ? 0.0 : w.kappa_avg[k];
         tke[col + kg * plane] = edge ? 0.0 : w.tke_avg[k];
+    }
+    if (work) work[col] = w.nwork;
+}
+
+// ---- the solve order: columns bucketed by their last cost, heaviest first.
+// A warp then carries columns of like cost (a warp runs as long as its
+// slowest lane) and the long columns start first.  Which thread solves which
+// column changes nothing in any column's result.
+constexpr int KS_NB = 1024;
+
+__device__ __forceinline__ int ks_bucket(int work)
+{
+    const int key = work >> 3;
+    return KS_NB - 1 - (key < KS_NB - 1 ? key : KS_NB - 1);
+}
+
+__global__ void k_ks_hist(const int *__restrict__ work, size_t n, unsigned *hist)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int b = ks_bucket(work[i]);
+        // one atomic per distinct bucket of the warp (land comes in runs)
+        const unsigned peers = __match_any_sync(__activemask(), b);
+        if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&hist[b], (unsigned)__popc(peers));
+    }
+}
+
+// exclusive scan of the KS_NB bucket counts, in place (one block of KS_NB threads)
+__global__ void __launch_bounds__(KS_NB) k_ks_scan(unsigned *hist)
+{
+    __shared__ unsigned sh[KS_NB];
+    const int t = threadIdx.x;
+    const unsigned v = hist[t];
+    sh[t] = v;
+    __syncthreads();
+    for (int off = 1; off < KS_NB; off <<= 1) {
+        const unsigned a = (t >= off) ? sh[t - off] : 0u;
+        __syncthreads();
+        sh[t] += a;
+        __syncthreads();
+    }
+    hist[t] = sh[t] - v;
+}
+
+__global__ void k_ks_scatter(const int *__restrict__ work, size_t n, unsigned *offs, int *order)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int b = ks_bucket(work[i]);
+        const unsigned peers = __match_any_sync(__activemask(), b);
+        const int lane = threadIdx.x & 31;
+        const int leader = __ffs(peers) - 1;
+        unsigned base = 0;
+        if (lane == leader) base = atomicAdd(&offs[b], (unsigned)__popc(peers));
+        base = __shfl_sync(peers, base, leader);
+        order[base + __popc(peers & ((1u << lane) - 1u))] = (int)i;
     }
 }
 
@@ -742,17 +825,28 @@ KsPar ks_par_of(const vphys_config &c)
 
 }  // namespace
 
-void launch_kappa_shear(const Params &p, double dt, cudaStream_t stream)
+void launch_kappa_shear(const Params &p, double dt, int *work, int *order, unsigned *hist, bool ordered,
+                        cudaStream_t stream)
 {
     const KsPar kp = ks_par_of(p.cfg);
+    const size_t n = p.plane;
+    const int *ord = nullptr;
+    if (ordered && work && order && hist) {
+        const int fill = (int)((n + 255) / 256 < 1184 ? (n + 255) / 256 : 1184);
+        cudaMemsetAsync(hist, 0, KS_NB * sizeof(unsigned), stream);
+        k_ks_hist<<<fill, 256, 0, stream>>>(work, n, hist);
+        k_ks_scan<<<1, KS_NB, 0, stream>>>(hist);
+        k_ks_scatter<<<fill, 256, 0, stream>>>(work, n, hist, order);
+        ord = order;
+    }
     const int threads = 64;
-    const unsigned blocks = (unsigned)((p.plane + threads - 1) / threads);
+    const unsigned blocks = (unsigned)((n + threads - 1) / threads);
     if (p.nz <= 32)
-        k_kappa_shear<34><<<blocks, threads, 0, stream>>>(p, kp, dt);
+        k_kappa_shear<34><<<blocks, threads, 0, stream>>>(p, kp, dt, ord, work);
     else if (p.nz <= 80)
-        k_kappa_shear<82><<<blocks, threads, 0, stream>>>(p, kp, dt);
+        k_kappa_shear<82><<<blocks, threads, 0, stream>>>(p, kp, dt, ord, work);
     else
-        k_kappa_shear<NZ_MAX + 2><<<blocks, threads, 0, stream>>>(p, kp, dt);
+        k_kappa_shear<NZ_MAX + 2><<<blocks, threads, 0, stream>>>(p, kp, dt, ord, work);
 }
 
 }  // namespace vphys

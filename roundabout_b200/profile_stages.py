@@ -4,9 +4,10 @@
     python -m roundabout_b200.profile_stages --config batched_1440x1080x75 --mixed 1
     python -m roundabout_b200.profile_stages --nx 512 --ny 384 --stages features,mlp
 
-Stages: eos, assemble, momentum, tracers, step (the path) and features, mlp
-(the learned KPP's feature extraction and its three tensor-core GEMMs, with
-untrained weights: the time does not depend on their values).
+Stages: eos, assemble, momentum, tracers, step (the path), kshear (the
+kappa-shear column solve, vphys_kappa_shear, default knobs, Wright EOS), and
+features, mlp (the learned KPP's feature extraction and its three tensor-core
+GEMMs, with untrained weights: the time does not depend on their values).
 
 Prints, per stage, the mean device time and the algorithmic GB/s; used as the
 driver of the ncu captures kept under profiles/.
@@ -53,13 +54,18 @@ def main():
     vp.load_columns(cols)
     dt = 3600.0
     vp.step(dt, args.warmup)
+    if "kshear" in args.stages:
+        for _ in range(args.warmup):
+            vp.kappa_shear(dt)
     torch.cuda.synchronize()
     cells = args.nx * args.ny * args.nz
     ifc = (args.nz + 1) / args.nz
     bpc = {"eos": 32.0, "assemble": 32.0 + 24 * ifc, "momentum": 48.0, "tracers": 16.0 + 16.0 * args.ntr,
-           "step": 8 * (4 + args.ntr) + 8 * (2 + args.ntr) + 24 * ifc}
+           "step": 8 * (4 + args.ntr) + 8 * (2 + args.ntr) + 24 * ifc,
+           "kshear": 8.0 * 7 + 16 * ifc}   # h, u and v (two faces each), T, S in; kd, tke out
     fns = {"eos": vp.eos, "assemble": vp.assemble, "momentum": lambda: vp.vdiff_momentum(dt),
-           "tracers": lambda: vp.vdiff_tracers(dt), "step": lambda: vp.step(dt, 1)}
+           "tracers": lambda: vp.vdiff_tracers(dt), "step": lambda: vp.step(dt, 1),
+           "kshear": lambda: vp.kappa_shear(dt)}
     ncols = args.nx * args.ny
     if "features" in args.stages or "mlp" in args.stages:
         import ctypes
@@ -91,7 +97,11 @@ def main():
         b.record()
         torch.cuda.synchronize()
         ms = a.elapsed_time(b) / args.reps
-        out[name] = {"ms": round(ms, 4), "alg_GBps": round(bpc[name] * cells / ms / 1e6, 1)}
+        out[name] = {"ms": round(ms, 4), "alg_GBps": round(bpc[name] * cells / ms / 1e6, 1),
+                     "cells_per_s": round(cells / ms * 1e3, 1)}
+        if name == "kshear":
+            kd = vp.get("kd_shear")
+            out[name]["active_columns"] = round(float((kd.max(axis=2) > 0.0).mean()), 4)
     print(json.dumps({"shape": [args.nx, args.ny, args.nz], "ntr": args.ntr, "thin": args.thin,
                       "mixed": args.mixed, "stages": out}))
     vp.close()
