@@ -176,8 +176,9 @@ typedef struct vphys_config {
     int kappa_shear;          /* 0 */
     int ks_max_inner_it;      /* Picard iterations, 50 (MAX_RINO_IT) */
     int ks_max_substep_it;    /* adaptive substeps, 13 (MAX_KAPPA_SHEAR_IT) */
-    int ks_eos;               /* buoyancy derivatives from: 0 the Wright 1997 EOS, 1 a linear EOS
-                                 (ks_alpha_t, ks_beta_s, rho0) -- eos_specvol_derivs, rdb_eos.F90:1551-1622 */
+    int eos_variant;          /* the shared EOS whose specific-volume derivatives kappa-shear and EPBL
+                                 read (eos_specvol_derivs, rdb_eos.F90:1551-1622): 0 Wright 1997, 1 linear
+                                 (eos_alpha_t, eos_beta_s, rho0).  The density precursor stays Wright. */
     double ks_ri_crit;        /* 0.25 */
     double ks_shearmix_rate;  /* 0.089 */
     double ks_fri_curvature;  /* -0.97 */
@@ -193,8 +194,46 @@ typedef struct vphys_config {
     double ks_src_max_chg;    /* 10 */
     double ks_prandtl_turb;   /* 1 */
     double ks_vel_underflow;  /* 0 m/s */
-    double ks_alpha_t;        /* linear EOS only: kg m-3 K-1 */
-    double ks_beta_s;         /* linear EOS only: kg m-3 psu-1 */
+    double eos_alpha_t;       /* linear EOS only: kg m-3 K-1 */
+    double eos_beta_s;        /* linear EOS only: kg m-3 psu-1 */
+    /* EPBL, the energetic planetary boundary layer, column form (ocean_epbl_t,
+     * rdb_ocean_epbl.F90:116-318; Reichl & Hallberg 2018).  epbl = 1 takes the
+     * boundary layer from KPP, which it switches off as the reference does
+     * (rdb_ocean_dyn.F90:1539): vphys_step refreshes KD_EPBL and MLD_EPBL
+     * once a step (vphys_epbl, epbl_compute) and every assembly merges
+     * KD_EPBL into kt and epbl_prandtl * KD_EPBL into kv (epbl_combine);
+     * convection then masks below MLD_EPBL.  Not built (refused): the
+     * penetrating-shortwave TKE ledger (sw_pen_frac != 0), Langmuir
+     * enhancement, the RH18 mstar fit and a mixing-length exponent other
+     * than 2. */
+    int epbl;                 /* 0 */
+    int epbl_mstar_scheme;    /* 1 constant, 2 OM4 (default) */
+    int epbl_vstar_scheme;    /* 1 cube root (default), 2 RH18 */
+    int epbl_combine;         /* 1 add (default), 2 max, 3 max_shear (needs kappa_shear: shear merged first) */
+    int epbl_mld_iteration;   /* 1 */
+    int epbl_mld_max_its;     /* 20 */
+    int epbl_mld_bisection;   /* 0: false position with a bisection fallback */
+    int epbl_mld_use_prev_guess; /* 0 */
+    double epbl_mstar_const;  /* 1.2 */
+    double epbl_mstar_cap;    /* -1 (off) */
+    double epbl_mstar_coef1;  /* 0.3 */
+    double epbl_c_ek;         /* 0.085 */
+    double epbl_mstar_conv_adj; /* 0 */
+    double epbl_nstar;        /* 0.2 */
+    double epbl_tke_decay;    /* 2.5 */
+    double epbl_wstar_ustar_coef; /* 1 */
+    double epbl_vstar_scale_fac; /* 1 */
+    double epbl_vstar_surf_fac; /* 1.2 */
+    double epbl_von_karman;   /* 0.41 */
+    double epbl_ekman_scale_coef; /* 1 */
+    double epbl_min_mix_len;  /* 0 m */
+    double epbl_mixlen_exponent; /* 2 */
+    double epbl_translay_scale; /* 0.1 */
+    double epbl_mld_tol;      /* 1 m */
+    double epbl_omega;        /* 7.2921e-5 1/s */
+    double epbl_omega_frac;   /* 0 */
+    double epbl_ustar_min;    /* 1e-8 m/s */
+    double epbl_prandtl;      /* 1 */
 } vphys_config;
 
 #define VPHYS_KPP_SW_ALL 1
@@ -236,6 +275,9 @@ enum vphys_field {
     VPHYS_FIELD_SALT_BUDGET_SURFACE = 29, /* in/out (nx, ny, nz) */
     VPHYS_FIELD_KD_SHEAR = 30,  /* in/out  (nx, ny, nz+1) kappa-shear diffusivity kd_int, 0 at bed and surface */
     VPHYS_FIELD_TKE_SHEAR = 31, /* out     (nx, ny, nz+1) kappa-shear time-mean TKE tke_int */
+    VPHYS_FIELD_KD_EPBL = 32,   /* in/out  (nx, ny, nz+1) EPBL diffusivity kd_int, 0 at bed and surface */
+    VPHYS_FIELD_MLD_EPBL = 33,  /* in/out  (nx, ny) EPBL mixed-layer depth (the previous one seeds the
+                                   iteration when epbl_mld_use_prev_guess) */
     VPHYS_FIELD_TRACER0 = 64    /* in/out  (nx, ny, nz); tracer t is
                                    VPHYS_FIELD_TRACER0 + t */
 };
@@ -345,6 +387,19 @@ int vphys_sw_penetration(vphys_handle h, double dt);
  * 953-1909); vphys_step runs it before the assembly when kappa_shear is 1,
  * and the assembly adds KD_SHEAR (rdb_ocean_dyn.F90:1564-1583). */
 int vphys_kappa_shear(vphys_handle h, double dt);
+
+/* EPBL, column form: per wet column the energetics of the surface forcing
+ * (mstar u*^3 of wind work, the convective release of the surface buoyancy
+ * loss) spent down the column on the largest diffusivity each interface can
+ * afford (a closed-form energy solve with an embedded forward elimination),
+ * iterated on the mixed-layer depth (false position, up to
+ * epbl_mld_max_its).  Reads H, T, S, STRESS_MAG, Q_HEAT, Q_SALT, WET,
+ * CORIOLIS; writes KD_EPBL (0 on the bed and surface interfaces and in land
+ * columns) and MLD_EPBL.  A no-op without a temperature or salinity tracer.
+ * Replaces epbl_compute -> epbl_column_kernel (rdb_ocean_epbl.F90:864-1659);
+ * vphys_step runs it before the assembly when epbl is 1, and the assembly
+ * merges KD_EPBL (epbl_merge_into_kv_kt / epbl_merge_max_shear, 1661-1718). */
+int vphys_epbl(vphys_handle h, double dt);
 
 /* Mixed-precision tracer solves (mixed_precision >= 1): the number of
  * (32-column group, tracer) pairs whose one-step increment reached 2 units

@@ -27,12 +27,14 @@ class VpoState(ctypes.Structure):
                           "q_heat", "q_salt", "wet", "tau_x", "tau_y", "lambda_bot_u", "lambda_bot_v",
                           "visc_rem_u", "visc_rem_v", "gamma_t", "gamma_s", "heat_budget", "salt_budget")
     ] + [(n, _ip) for n in ("k_top_u", "k_top_v", "k_bot_u", "k_bot_v")] + [("tr", ctypes.POINTER(_dp))] + [
-        (n, _dp) for n in ("heat_budget_surface", "salt_budget_surface", "coriolis", "kd_shear", "tke_shear")]
+        (n, _dp) for n in ("heat_budget_surface", "salt_budget_surface", "coriolis", "kd_shear", "tke_shear", "kd_epbl",
+                          "mld_epbl")]
 
 
 def build(force: bool = False) -> Path:
     """Compile the oracle with its Makefile (gcc, -ffp-contract=off)."""
-    srcs = [HERE / n for n in ("vphys_oracle.c", "vphys_oracle_kshear.c", "vphys_oracle.h", "Makefile")]
+    srcs = [HERE / n for n in ("vphys_oracle.c", "vphys_oracle_kshear.c", "vphys_oracle_epbl.c", "vphys_oracle.h",
+                               "Makefile")]
     srcs.append(HERE.parent / "include" / "vphys.h")
     if force or not LIB_PATH.exists() or LIB_PATH.stat().st_mtime < max(p.stat().st_mtime for p in srcs):
         env = dict(os.environ)
@@ -54,10 +56,12 @@ def lib():
         L.vpo_sm_atan.argtypes = [ctypes.c_double]
         L.vpo_sm_exp.restype = ctypes.c_double
         L.vpo_sm_exp.argtypes = [ctypes.c_double]
+        L.vpo_sm_log.restype = ctypes.c_double
+        L.vpo_sm_log.argtypes = [ctypes.c_double]
         L.vpo_set_threads.argtypes = [ctypes.c_int]
         L.vpo_get_threads.restype = ctypes.c_int
         for name in ("vpo_eos_wright", "vpo_pp81", "vpo_seed_interior_none", "vpo_kpp_overlay",
-                     "vpo_kv_ml_invz2", "vpo_convection", "vpo_split", "vpo_kappa_shear_merge"):
+                     "vpo_kv_ml_invz2", "vpo_convection", "vpo_split", "vpo_kappa_shear_merge", "vpo_epbl_merge"):
             getattr(L, name).argtypes = [ctypes.c_void_p, ctypes.POINTER(VpoState)]
             getattr(L, name).restype = None
         L.vpo_stress_mag.argtypes = [ctypes.POINTER(VpoState)]
@@ -65,7 +69,7 @@ def lib():
             getattr(L, name).argtypes = [ctypes.c_void_p, ctypes.POINTER(VpoState)]
             getattr(L, name).restype = ctypes.c_int
         for name in ("vpo_vdiff_momentum", "vpo_vdiff_tracers", "vpo_nonlocal", "vpo_surface_flux",
-                     "vpo_sw_penetration", "vpo_kappa_shear"):
+                     "vpo_sw_penetration", "vpo_kappa_shear", "vpo_epbl"):
             getattr(L, name).argtypes = [ctypes.c_void_p, ctypes.POINTER(VpoState), ctypes.c_double]
             getattr(L, name).restype = None
         L.vpo_eos_buoyancy_coeffs.argtypes = [ctypes.c_double] * 3 + [ctypes.POINTER(ctypes.c_double)] * 2
@@ -116,6 +120,8 @@ class OracleState:
         self.coriolis = f(nx, ny)
         self.kd_shear = f(nx, ny, nz + 1)
         self.tke_shear = f(nx, ny, nz + 1)
+        self.kd_epbl = f(nx, ny, nz + 1)
+        self.mld_epbl = f(nx, ny)
         self.k_top_u = np.full((nx + 1, ny), nz, dtype=np.int32, order="F")
         self.k_top_v = np.full((nx, ny + 1), nz, dtype=np.int32, order="F")
         self.k_bot_u = np.ones((nx + 1, ny), dtype=np.int32, order="F")
@@ -179,6 +185,10 @@ def sm_atan(x: float) -> float:
 
 def sm_exp(x: float) -> float:
     return lib().vpo_sm_exp(float(x))
+
+
+def sm_log(x: float) -> float:
+    return lib().vpo_sm_log(float(x))
 
 
 def eos_buoyancy_coeffs(T: float, S: float, p: float):

@@ -104,6 +104,44 @@ double vpo_sm_exp(double x)
     return y;
 }
 
+/* rdb_sm_log (rdb_safe_math_core.inc:139-206): x = m 2^k with m in
+ * [sqrt(1/2), sqrt(2)), log m = 2 atanh f, f = (m-1)/(m+1), the odd series
+ * in f to 1/19 (Cody & Waite 1980, ch. 5), k ln 2 added as head + tail. */
+static const double SM_LOG_C[10] = {1.0,        1.0 / 3.0,  1.0 / 5.0,  1.0 / 7.0,  1.0 / 9.0,
+                                    1.0 / 11.0, 1.0 / 13.0, 1.0 / 15.0, 1.0 / 17.0, 1.0 / 19.0};
+static const double SM_SQRT_HALF = 0.70710678118654757274;
+static const double SM_TWO54 = 18014398509481984.0;
+
+double vpo_sm_log(double x)
+{
+    if (isnan(x)) return x;
+    if (x < 0.0) return NAN;
+    if (x == 0.0) return -INFINITY;
+    if (x < DBL_MIN && x * SM_TWO54 == 0.0) return -INFINITY;
+    if (!isfinite(x)) return x;
+    double xs = x;
+    int kadj = 0;
+    if (x < DBL_MIN) {
+        xs = x * SM_TWO54;
+        kadj = -54;
+    }
+    int e;
+    double m = frexp(xs, &e);   /* Fortran fraction / exponent: m in [1/2, 1) */
+    int k = e + kadj;
+    if (m < SM_SQRT_HALF) {
+        m = 2.0 * m;
+        k = k - 1;
+    }
+    const double f = (m - 1.0) / (m + 1.0);
+    const double u = f * f;
+    double p = SM_LOG_C[9];
+    for (int i = 8; i >= 1; --i) p = p * u + SM_LOG_C[i];
+    const double kr = (double)k;
+    const double s = kr * SM_LN2_HI + 2.0 * f;
+    const double w = (2.0 * f) * u * p + kr * SM_LN2_LO;
+    return s + w;
+}
+
 static inline double sm_flush(double r)
 {
     /* rdb_sm_flush (rdb_safe_math_core.inc:40-51) */
@@ -528,7 +566,7 @@ void vpo_convection(const vphys_config *c, vpo_state *s)
                 z = z + C3(s->h, i, j, k);
                 double dz_face = 0.5 * (C3(s->h, i, j, k - 1) + C3(s->h, i, j, k));
                 if (dz_face <= H_VANISHED) continue;
-                if (z < C2(s->bl_depth, i, j)) continue;
+                if (z < (c->epbl ? C2(s->mld_epbl, i, j) : C2(s->bl_depth, i, j))) continue;
                 double n2 = -(GRAVITY * (C3(s->rho, i, j, k) - C3(s->rho, i, j, k - 1)) / (c->rho0 * dz_face));
                 if (n2 < c->conv_n2_thresh) {
                     C3(s->kt, i, j, k) = fmx(C3(s->kt, i, j, k), c->conv_kd);
@@ -636,8 +674,8 @@ int vpo_assemble_gate(const vphys_config *c, vpo_state *s)
     return status;
 }
 
-/* vmix_build_coefficients (rdb_ocean_dyn.F90:1473-1634) with the
- * kappa-shear merge of the kd_shear last computed (1564-1583); no EPBL /
+/* vmix_build_coefficients (rdb_ocean_dyn.F90:1473-1634) with the EPBL and
+ * kappa-shear merges of the kd_epbl / kd_shear last computed (1546-1583); no
  * tidal / BBL mixing. */
 int vpo_build_coefficients(const vphys_config *c, vpo_state *s)
 {
@@ -645,8 +683,9 @@ int vpo_build_coefficients(const vphys_config *c, vpo_state *s)
         vpo_pp81(c, s);
     else
         vpo_seed_interior_none(c, s);
-    if (c->use_kpp) vpo_kpp_overlay(c, s);
-    if (c->kappa_shear) vpo_kappa_shear_merge(c, s);
+    if (c->use_kpp && !c->epbl) vpo_kpp_overlay(c, s);   /* EPBL replaces KPP (rdb_ocean_dyn.F90:1539) */
+    if (c->epbl) vpo_epbl_merge(c, s);   /* with combine = max_shear it merges kappa-shear first */
+    if (c->kappa_shear && !(c->epbl && c->epbl_combine == 3)) vpo_kappa_shear_merge(c, s);
     vpo_kv_ml_invz2(c, s);
     if (c->conv_enable) vpo_convection(c, s);
     vpo_split(c, s);
@@ -1137,11 +1176,12 @@ int vpo_step(const vphys_config *c, vpo_state *s, double dt, int n_steps)
             vpo_surface_flux(c, s, dt);
             vpo_sw_penetration(c, s, dt);
         }
+        if (c->epbl) vpo_epbl(c, s, dt);
         if (c->kappa_shear) vpo_kappa_shear(c, s, dt);
         st |= vpo_build_coefficients(c, s);
         vpo_vdiff_momentum(c, s, dt);
         vpo_vdiff_tracers(c, s, dt);
-        if (c->use_kpp) vpo_nonlocal(c, s, dt);
+        if (c->use_kpp && !c->epbl) vpo_nonlocal(c, s, dt);   /* under EPBL its gamma is 0: a no-op */
     }
     return st;
 }

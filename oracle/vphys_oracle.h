@@ -43,6 +43,8 @@ typedef struct vpo_state {
     double *heat_budget_surface, *salt_budget_surface;
     double *coriolis;                       /* (nx,ny) f; NULL reads as 0 */
     double *kd_shear, *tke_shear;           /* (nx,ny,nz+1) kappa-shear kd_int, tke_int */
+    double *kd_epbl;                        /* (nx,ny,nz+1) EPBL kd_int */
+    double *mld_epbl;                       /* (nx,ny) EPBL mixed-layer depth */
 } vpo_state;
 
 void vpo_set_threads(int n);
@@ -69,11 +71,16 @@ void vpo_nonlocal(const vphys_config *c, vpo_state *s, double dt);
 void vpo_surface_flux(const vphys_config *c, vpo_state *s, double dt);
 void vpo_eos_buoyancy_coeffs(double T, double S, double p, double *alpha_T, double *beta_S);
 double vpo_sm_exp(double x);
+double vpo_sm_log(double x);
 void vpo_sw_penetration(const vphys_config *c, vpo_state *s, double dt);
 
 /* kappa-shear, column form (vphys_oracle_kshear.c) */
 void vpo_kappa_shear(const vphys_config *c, vpo_state *s, double dt);
 void vpo_kappa_shear_merge(const vphys_config *c, vpo_state *s);
+
+/* EPBL, column form (vphys_oracle_epbl.c) */
+void vpo_epbl(const vphys_config *c, vpo_state *s, double dt);
+void vpo_epbl_merge(const vphys_config *c, vpo_state *s);
 
 int vpo_step(const vphys_config *c, vpo_state *s, double dt, int n_steps);
 

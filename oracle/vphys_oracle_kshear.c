@@ -756,11 +756,11 @@ static void ks_params(const vphys_config *c, ks_par *p)
     p->src_max_chg = c->ks_src_max_chg;
     p->vel_underflow = c->ks_vel_underflow;
     p->rho0 = c->rho0;
-    p->alpha_t = c->ks_alpha_t;
-    p->beta_s = c->ks_beta_s;
+    p->alpha_t = c->eos_alpha_t;
+    p->beta_s = c->eos_beta_s;
     p->max_inner_it = c->ks_max_inner_it;
     p->max_substep_it = c->ks_max_substep_it;
-    p->eos_linear = c->ks_eos == 1;
+    p->eos_linear = c->eos_variant == 1;
 }
 
 /* kappa_shear_compute -> kappa_shear_column_kernel (:427-648), massless

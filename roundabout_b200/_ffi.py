@@ -67,6 +67,8 @@ FIELD_HEAT_BUDGET_SURFACE = 28
 FIELD_SALT_BUDGET_SURFACE = 29
 FIELD_KD_SHEAR = 30
 FIELD_TKE_SHEAR = 31
+FIELD_KD_EPBL = 32
+FIELD_MLD_EPBL = 33
 FIELD_TRACER0 = 64
 
 FIELD_NAMES = {
@@ -79,7 +81,7 @@ FIELD_NAMES = {
     "k_top_u": FIELD_K_TOP_U, "k_top_v": FIELD_K_TOP_V, "k_bot_u": FIELD_K_BOT_U,
     "k_bot_v": FIELD_K_BOT_V, "coriolis": FIELD_CORIOLIS,
     "heat_budget_surface": FIELD_HEAT_BUDGET_SURFACE, "salt_budget_surface": FIELD_SALT_BUDGET_SURFACE,
-    "kd_shear": FIELD_KD_SHEAR, "tke_shear": FIELD_TKE_SHEAR,
+    "kd_shear": FIELD_KD_SHEAR, "tke_shear": FIELD_TKE_SHEAR, "kd_epbl": FIELD_KD_EPBL, "mld_epbl": FIELD_MLD_EPBL,
 }
 INT_FIELDS = (FIELD_K_TOP_U, FIELD_K_TOP_V, FIELD_K_BOT_U, FIELD_K_BOT_V)
 
@@ -93,9 +95,11 @@ def field_shape(field: int, nx: int, ny: int, nz: int):
         return (nx + 1, ny, nz)
     if field in (FIELD_V, FIELD_VISC_REM_V):
         return (nx, ny + 1, nz)
-    if field in (FIELD_KV, FIELD_KT, FIELD_KS, FIELD_GAMMA_T, FIELD_GAMMA_S, FIELD_KD_SHEAR, FIELD_TKE_SHEAR):
+    if field in (FIELD_KV, FIELD_KT, FIELD_KS, FIELD_GAMMA_T, FIELD_GAMMA_S, FIELD_KD_SHEAR, FIELD_TKE_SHEAR,
+                 FIELD_KD_EPBL):
         return (nx, ny, nz + 1)
-    if field in (FIELD_BL_DEPTH, FIELD_B0, FIELD_STRESS_MAG, FIELD_Q_HEAT, FIELD_Q_SALT, FIELD_WET, FIELD_CORIOLIS):
+    if field in (FIELD_BL_DEPTH, FIELD_B0, FIELD_STRESS_MAG, FIELD_Q_HEAT, FIELD_Q_SALT, FIELD_WET, FIELD_CORIOLIS,
+                 FIELD_MLD_EPBL):
         return (nx, ny)
     if field in (FIELD_TAU_X, FIELD_LAMBDA_BOT_U, FIELD_K_TOP_U, FIELD_K_BOT_U):
         return (nx + 1, ny)
@@ -132,14 +136,21 @@ class VphysConfig(ctypes.Structure):
         ("sw_pen_frac", ctypes.c_double), ("sw_band_ratio", ctypes.c_double), ("sw_zeta1", ctypes.c_double),
         ("sw_zeta2", ctypes.c_double),
         ("kappa_shear", ctypes.c_int), ("ks_max_inner_it", ctypes.c_int), ("ks_max_substep_it", ctypes.c_int),
-        ("ks_eos", ctypes.c_int),
+        ("eos_variant", ctypes.c_int),
         ("ks_ri_crit", ctypes.c_double), ("ks_shearmix_rate", ctypes.c_double), ("ks_fri_curvature", ctypes.c_double),
         ("ks_c_n", ctypes.c_double), ("ks_c_s", ctypes.c_double), ("ks_lambda", ctypes.c_double),
         ("ks_lz_rescale", ctypes.c_double), ("ks_kappa_0", ctypes.c_double), ("ks_kappa_seed", ctypes.c_double),
         ("ks_kappa_trunc", ctypes.c_double), ("ks_tke_bg", ctypes.c_double), ("ks_tol_err", ctypes.c_double),
         ("ks_src_max_chg", ctypes.c_double), ("ks_prandtl_turb", ctypes.c_double),
-        ("ks_vel_underflow", ctypes.c_double), ("ks_alpha_t", ctypes.c_double), ("ks_beta_s", ctypes.c_double),
-    ]
+        ("ks_vel_underflow", ctypes.c_double), ("eos_alpha_t", ctypes.c_double), ("eos_beta_s", ctypes.c_double),
+        ("epbl", ctypes.c_int), ("epbl_mstar_scheme", ctypes.c_int), ("epbl_vstar_scheme", ctypes.c_int),
+        ("epbl_combine", ctypes.c_int), ("epbl_mld_iteration", ctypes.c_int), ("epbl_mld_max_its", ctypes.c_int),
+        ("epbl_mld_bisection", ctypes.c_int), ("epbl_mld_use_prev_guess", ctypes.c_int),
+    ] + [(n, ctypes.c_double) for n in (
+        "epbl_mstar_const", "epbl_mstar_cap", "epbl_mstar_coef1", "epbl_c_ek", "epbl_mstar_conv_adj", "epbl_nstar",
+        "epbl_tke_decay", "epbl_wstar_ustar_coef", "epbl_vstar_scale_fac", "epbl_vstar_surf_fac", "epbl_von_karman",
+        "epbl_ekman_scale_coef", "epbl_min_mix_len", "epbl_mixlen_exponent", "epbl_translay_scale", "epbl_mld_tol",
+        "epbl_omega", "epbl_omega_frac", "epbl_ustar_min", "epbl_prandtl")]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_ if n not in ()}
@@ -206,6 +217,7 @@ _PROTOTYPES = {
     "vphys_surface_flux": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "vphys_sw_penetration": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "vphys_kappa_shear": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    "vphys_epbl": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "vphys_mixed_redo_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint)]),
     "vphys_assemble": (ctypes.c_int, [ctypes.c_void_p]),
     "vphys_vdiff_momentum": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),

@@ -161,6 +161,11 @@ class VerticalPhysics:
         fills the kd_shear / tke_shear fields."""
         _ffi.check(self.lib.vphys_kappa_shear(self._h, float(dt)), "vphys_kappa_shear")
 
+    def epbl(self, dt):
+        """epbl_compute, column form (rdb_ocean_epbl.F90:864-1659): fills the
+        kd_epbl / mld_epbl fields."""
+        _ffi.check(self.lib.vphys_epbl(self._h, float(dt)), "vphys_epbl")
+
     def assemble(self):
         return _ffi.check(self.lib.vphys_assemble(self._h), "vphys_assemble")
 

@@ -87,7 +87,7 @@ def default_config() -> VphysConfig:
     c.kappa_shear = 0
     c.ks_max_inner_it = 50
     c.ks_max_substep_it = 13
-    c.ks_eos = 0
+    c.eos_variant = 0
     c.ks_ri_crit = 0.25
     c.ks_shearmix_rate = 0.089
     c.ks_fri_curvature = -0.97
@@ -103,8 +103,36 @@ def default_config() -> VphysConfig:
     c.ks_src_max_chg = 10.0
     c.ks_prandtl_turb = 1.0
     c.ks_vel_underflow = 0.0
-    c.ks_alpha_t = 0.0
-    c.ks_beta_s = 0.0
+    c.eos_alpha_t = 0.0
+    c.eos_beta_s = 0.0
+    c.epbl = 0
+    c.epbl_mstar_scheme = 2
+    c.epbl_vstar_scheme = 1
+    c.epbl_combine = 1
+    c.epbl_mld_iteration = 1
+    c.epbl_mld_max_its = 20
+    c.epbl_mld_bisection = 0
+    c.epbl_mld_use_prev_guess = 0
+    c.epbl_mstar_const = 1.2
+    c.epbl_mstar_cap = -1.0
+    c.epbl_mstar_coef1 = 0.3
+    c.epbl_c_ek = 0.085
+    c.epbl_mstar_conv_adj = 0.0
+    c.epbl_nstar = 0.2
+    c.epbl_tke_decay = 2.5
+    c.epbl_wstar_ustar_coef = 1.0
+    c.epbl_vstar_scale_fac = 1.0
+    c.epbl_vstar_surf_fac = 1.2
+    c.epbl_von_karman = 0.41
+    c.epbl_ekman_scale_coef = 1.0
+    c.epbl_min_mix_len = 0.0
+    c.epbl_mixlen_exponent = 2.0
+    c.epbl_translay_scale = 0.1
+    c.epbl_mld_tol = 1.0
+    c.epbl_omega = 7.2921e-05
+    c.epbl_omega_frac = 0.0
+    c.epbl_ustar_min = 1e-08
+    c.epbl_prandtl = 1.0
     return c
 
 
@@ -226,6 +254,41 @@ class ConvectiveAdjustment:
         cfg.conv_kd = float(self.kd)
         cfg.conv_prandtl = float(self.prandtl)
         cfg.conv_n2_thresh = float(self.n2_threshold)
+        return cfg
+
+
+class EPBL:
+    """Reichl-Hallberg energetics PBL, column form (python/rdb/closures.py:107-150:
+    `EPBL(mstar_scheme="om4", mstar=1.2, nstar=0.2, prandtl=1.0, combine="add",
+    mld_iteration=True, mld_use_prev_guess=False, langmuir=None)`).  Like the
+    reference it switches KPP off.  Not built here: the "rh18" mstar fit and
+    Langmuir enhancement (both raise)."""
+
+    _MSTAR = {"constant": 1, "om4": 2}
+    _COMBINE = {"add": 1, "max": 2, "max_shear": 3}
+
+    def __init__(self, mstar_scheme="om4", mstar=1.2, nstar=0.2, prandtl=1.0, combine="add", mld_iteration=True,
+                 mld_use_prev_guess=False, langmuir=None):
+        if mstar_scheme not in self._MSTAR:
+            raise NotImplementedError(f"EPBL: mstar_scheme {mstar_scheme!r} is not built (constant, om4)")
+        if combine not in self._COMBINE:
+            raise ValueError(f"EPBL: combine must be one of {sorted(self._COMBINE)}")
+        if langmuir is not None:
+            raise NotImplementedError("EPBL: Langmuir enhancement is not built")
+        self.mstar_scheme, self.mstar, self.nstar = mstar_scheme, mstar, nstar
+        self.prandtl, self.combine = prandtl, combine
+        self.mld_iteration, self.mld_use_prev_guess = mld_iteration, mld_use_prev_guess
+
+    def apply(self, cfg):
+        cfg.epbl = 1
+        cfg.use_kpp = 0
+        cfg.epbl_mstar_scheme = self._MSTAR[self.mstar_scheme]
+        cfg.epbl_mstar_const = float(self.mstar)
+        cfg.epbl_nstar = float(self.nstar)
+        cfg.epbl_prandtl = float(self.prandtl)
+        cfg.epbl_combine = self._COMBINE[self.combine]
+        cfg.epbl_mld_iteration = int(bool(self.mld_iteration))
+        cfg.epbl_mld_use_prev_guess = int(bool(self.mld_use_prev_guess))
         return cfg
 
 

@@ -50,7 +50,7 @@ int cuda_status(cudaError_t e, const char *where)
     return push_error(VPHYS_ERR_CUDA, "%s: CUDA error %d (%s)", where, (int)e, cudaGetErrorString(e));
 }
 
-constexpr int NFIXED = 32;
+constexpr int NFIXED = 34;
 constexpr unsigned MAGIC = 0x56504859u;   // "VPHY"
 
 struct Field {
@@ -130,14 +130,16 @@ size_t field_count(int nx, int ny, int nz, int field, bool *is_int)
     case VPHYS_FIELD_GAMMA_T:
     case VPHYS_FIELD_GAMMA_S:
     case VPHYS_FIELD_KD_SHEAR:
-    case VPHYS_FIELD_TKE_SHEAR: return X * Y * (Z + 1);
+    case VPHYS_FIELD_TKE_SHEAR:
+    case VPHYS_FIELD_KD_EPBL: return X * Y * (Z + 1);
     case VPHYS_FIELD_BL_DEPTH:
     case VPHYS_FIELD_B0:
     case VPHYS_FIELD_STRESS_MAG:
     case VPHYS_FIELD_Q_HEAT:
     case VPHYS_FIELD_Q_SALT:
     case VPHYS_FIELD_WET:
-    case VPHYS_FIELD_CORIOLIS: return X * Y;
+    case VPHYS_FIELD_CORIOLIS:
+    case VPHYS_FIELD_MLD_EPBL: return X * Y;
     case VPHYS_FIELD_TAU_X:
     case VPHYS_FIELD_LAMBDA_BOT_U: return (X + 1) * Y;
     case VPHYS_FIELD_TAU_Y:
@@ -257,9 +259,28 @@ int validate(const vphys_config *c, int ntr)
         return push_error(VPHYS_ERR_CONFIG, "ks_max_inner_it must be in [1, 10000]");
     if (c->ks_max_substep_it < 0 || c->ks_max_substep_it > 10000)
         return push_error(VPHYS_ERR_CONFIG, "ks_max_substep_it must be in [0, 10000]");
-    if (c->ks_eos < 0 || c->ks_eos > 1) return push_error(VPHYS_ERR_CONFIG, "ks_eos must be 0 (Wright) or 1 (linear)");
+    if (c->eos_variant < 0 || c->eos_variant > 1) return push_error(VPHYS_ERR_CONFIG, "eos_variant must be 0 (Wright) or 1 (linear)");
     if (c->ks_lambda == 0.0 || c->ks_lz_rescale == 0.0 || c->ks_src_max_chg == 0.0)
         return push_error(VPHYS_ERR_CONFIG, "ks_lambda, ks_lz_rescale and ks_src_max_chg must be nonzero");
+    if (c->epbl < 0 || c->epbl > 1) return push_error(VPHYS_ERR_CONFIG, "epbl must be 0 or 1");
+    if (c->epbl) {
+        if (c->epbl_mstar_scheme == 3)
+            return push_error(VPHYS_ERR_CONFIG, "epbl_mstar_scheme 3 (RH18) is not built: 1 constant or 2 OM4");
+        if (c->epbl_mstar_scheme < 1 || c->epbl_mstar_scheme > 2)
+            return push_error(VPHYS_ERR_CONFIG, "epbl_mstar_scheme must be 1 (constant) or 2 (OM4)");
+        if (c->epbl_vstar_scheme < 1 || c->epbl_vstar_scheme > 2)
+            return push_error(VPHYS_ERR_CONFIG, "epbl_vstar_scheme must be 1 (cube root) or 2 (RH18)");
+        if (c->epbl_combine < 1 || c->epbl_combine > 3)
+            return push_error(VPHYS_ERR_CONFIG, "epbl_combine must be 1 (add), 2 (max) or 3 (max_shear)");
+        if (c->epbl_mixlen_exponent != 2.0)
+            return push_error(VPHYS_ERR_CONFIG, "epbl_mixlen_exponent other than 2 is not built");
+        if (c->sw_pen_frac != 0.0)
+            return push_error(VPHYS_ERR_CONFIG, "EPBL's penetrating-shortwave TKE ledger is not built: sw_pen_frac must be 0");
+        if (c->learned_kpp) return push_error(VPHYS_ERR_CONFIG, "EPBL replaces KPP: learned_kpp must be 0");
+        if (c->epbl_mld_max_its < 1 || c->epbl_mld_max_its > 1000)
+            return push_error(VPHYS_ERR_CONFIG, "epbl_mld_max_its must be in [1, 1000]");
+        if (!(c->epbl_ustar_min > 0.0)) return push_error(VPHYS_ERR_CONFIG, "epbl_ustar_min must be positive");
+    }
     return VPHYS_OK;
 }
 
@@ -314,6 +335,8 @@ Params make_params(vphys_handle h)
     p.coriolis = D(VPHYS_FIELD_CORIOLIS);
     p.kd_shear = D(VPHYS_FIELD_KD_SHEAR);
     p.tke_shear = D(VPHYS_FIELD_TKE_SHEAR);
+    p.kd_epbl = D(VPHYS_FIELD_KD_EPBL);
+    p.mld_epbl = D(VPHYS_FIELD_MLD_EPBL);
     p.ks_equals_kt = (h->cfg.bkgnd_profile || h->cfg.kt_bg == h->cfg.ks_bg) ? 1 : 0;
     p.write_gamma = (p.gamma_t && p.gamma_s) ? 1 : 0;
     return p;
@@ -427,10 +450,21 @@ void launch_kappa_shear(vphys_handle h, const Params &p, double dt)
     vphys::launch_kappa_shear(p, dt, h->ks_work, h->ks_order, h->ks_hist, true, h->stream);
 }
 
+int prepare_epbl(vphys_handle h)
+{
+    int st = VPHYS_OK;
+    if ((st = ensure(h, VPHYS_FIELD_KD_EPBL))) return st;
+    return ensure(h, VPHYS_FIELD_MLD_EPBL);
+}
+
 int prepare_assemble(vphys_handle h)
 {
     if (h->cfg.kappa_shear) {
         int st = prepare_kappa_shear(h);
+        if (st) return st;
+    }
+    if (h->cfg.epbl) {
+        int st = prepare_epbl(h);
         if (st) return st;
     }
     if (h->cfg.kd_smooth_iterations > 0 && !h->smooth_scratch) {
@@ -528,6 +562,8 @@ int launch_steps(vphys_handle h, const Params &p, double dt, int n_steps)
 {
     int st;
     const bool fork = h->aux_stream && h->ntr > 0;
+    // KPP's non-local tendency; under EPBL KPP does not run and its gamma is 0
+    const bool kpp_nonlocal = h->cfg.use_kpp && !h->cfg.epbl;
     double inv_heat, inv_salt;
     surface_flux_scales(h->cfg, dt, &inv_heat, &inv_salt);
     for (int n = 0; n < n_steps; ++n) {
@@ -537,6 +573,7 @@ int launch_steps(vphys_handle h, const Params &p, double dt, int n_steps)
             if (h->cfg.sw_pen_frac != 0.0 && h->cfg.idx_temperature >= 0)
                 vphys::launch_sw_penetration(p, inv_heat, h->stream);
         }
+        if (h->cfg.epbl && h->cfg.idx_temperature >= 0 && h->cfg.idx_salinity >= 0) vphys::launch_epbl(p, dt, h->stream);
         if (h->cfg.kappa_shear && h->cfg.idx_temperature >= 0 && h->cfg.idx_salinity >= 0)
             launch_kappa_shear(h, p, dt);
         Params pa = p;
@@ -546,12 +583,12 @@ int launch_steps(vphys_handle h, const Params &p, double dt, int n_steps)
             cudaEventRecord(h->ev_fork, h->stream);
             cudaStreamWaitEvent(h->aux_stream, h->ev_fork, 0);
             vphys::launch_momentum(p, dt, h->aux_stream);
-            vphys::launch_tracers(p, dt, true, h->cfg.use_kpp != 0, h->stream);
+            vphys::launch_tracers(p, dt, true, kpp_nonlocal, h->stream);
             cudaEventRecord(h->ev_join, h->aux_stream);
             cudaStreamWaitEvent(h->stream, h->ev_join, 0);
         } else {
             vphys::launch_momentum(p, dt, h->stream);
-            if (h->ntr > 0) vphys::launch_tracers(p, dt, true, h->cfg.use_kpp != 0, h->stream);
+            if (h->ntr > 0) vphys::launch_tracers(p, dt, true, kpp_nonlocal, h->stream);
         }
         h->gen += 1;
     }
@@ -683,6 +720,28 @@ int vphys_config_default(vphys_config *c)
     c->ks_tol_err = 0.1;
     c->ks_src_max_chg = 10.0;
     c->ks_prandtl_turb = 1.0;
+    c->epbl_mstar_scheme = 2;
+    c->epbl_vstar_scheme = 1;
+    c->epbl_combine = 1;
+    c->epbl_mld_iteration = 1;
+    c->epbl_mld_max_its = 20;
+    c->epbl_mstar_const = 1.2;
+    c->epbl_mstar_cap = -1.0;
+    c->epbl_mstar_coef1 = 0.3;
+    c->epbl_c_ek = 0.085;
+    c->epbl_nstar = 0.2;
+    c->epbl_tke_decay = 2.5;
+    c->epbl_wstar_ustar_coef = 1.0;
+    c->epbl_vstar_scale_fac = 1.0;
+    c->epbl_vstar_surf_fac = 1.2;
+    c->epbl_von_karman = 0.41;
+    c->epbl_ekman_scale_coef = 1.0;
+    c->epbl_mixlen_exponent = 2.0;
+    c->epbl_translay_scale = 0.1;
+    c->epbl_mld_tol = 1.0;
+    c->epbl_omega = 7.2921e-05;
+    c->epbl_ustar_min = 1e-08;
+    c->epbl_prandtl = 1.0;
     return VPHYS_OK;
 }
 
@@ -962,6 +1021,17 @@ int vphys_kappa_shear(vphys_handle h, double dt)
     return cuda_status(cudaGetLastError(), "vphys_kappa_shear launch");
 }
 
+int vphys_epbl(vphys_handle h, double dt)
+{
+    if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_epbl: bad handle");
+    if (h->cfg.idx_temperature < 0 || h->cfg.idx_salinity < 0) return VPHYS_OK;
+    int st = prepare_epbl(h);
+    if (st) return st;
+    Params p = make_params(h);
+    vphys::launch_epbl(p, dt, h->stream);
+    return cuda_status(cudaGetLastError(), "vphys_epbl launch");
+}
+
 int vphys_mixed_redo_count(vphys_handle h, unsigned *groups)
 {
     if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_mixed_redo_count: bad handle");
@@ -1025,7 +1095,7 @@ int vphys_vdiff_tracers(vphys_handle h, double dt)
 int vphys_nonlocal(vphys_handle h, double dt)
 {
     if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_nonlocal: bad handle");
-    if (h->ntr == 0 || !h->cfg.use_kpp) return VPHYS_OK;
+    if (h->ntr == 0 || !h->cfg.use_kpp || h->cfg.epbl) return VPHYS_OK;
     Params p = make_params(h);
     vphys::launch_tracers(p, dt, false, true, h->stream);
     return cuda_status(cudaGetLastError(), "vphys_nonlocal launch");

@@ -152,6 +152,47 @@ __device__ __forceinline__ double sm_exp(double x)
     return y;
 }
 
+// ---- position-independent natural logarithm: rdb_sm_log
+// (rdb_safe_math_core.inc:139-206): x = m 2^k with m in [sqrt(1/2), sqrt(2))
+// (subnormals scaled by 2^54 first), log m = 2 atanh f with f = (m-1)/(m+1)
+// and the odd series in f to 1/19 (Cody & Waite 1980, ch. 5), k ln 2 added as
+// head + tail.  Bit-identical to the CPU restatement without FMA contraction.
+__device__ __forceinline__ double sm_log(double x)
+{
+    if (isnan(x)) return x;
+    if (x < 0.0) return __longlong_as_double(0x7ff8000000000000LL);
+    if (x == 0.0) return __longlong_as_double((long long)0xfff0000000000000ULL);
+    if (isinf(x)) return x;
+    double xs = x;
+    int kadj = 0;
+    if (x < DBL_TINY) {
+        xs = x * 18014398509481984.0;   // 2^54
+        kadj = -54;
+    }
+    int e;
+    double m = frexp(xs, &e);   // m in [1/2, 1), exact
+    int k = e + kadj;
+    if (m < 0.70710678118654757274) {
+        m = 2.0 * m;
+        k = k - 1;
+    }
+    const double f = xdiv(m - 1.0, m + 1.0);
+    const double u = f * f;
+    double p = 1.0 / 19.0;
+    p = p * u + 1.0 / 17.0;
+    p = p * u + 1.0 / 15.0;
+    p = p * u + 1.0 / 13.0;
+    p = p * u + 1.0 / 11.0;
+    p = p * u + 1.0 / 9.0;
+    p = p * u + 1.0 / 7.0;
+    p = p * u + 1.0 / 5.0;
+    p = p * u + 1.0 / 3.0;
+    const double kr = (double)k;
+    const double s = kr * 0.69314718060195446014 + 2.0 * f;
+    const double w = (2.0 * f) * u * p + kr * -4.2009150726810845979e-11;
+    return s + w;
+}
+
 // ---- position-independent arctangent: rdb_sm_atan
 // (rdb_safe_math_atan.inc:7-44, Cody & Waite reduction, fitted degree-11
 // polynomial of rdb_safe_math_consts.inc:85-89).

@@ -1,0 +1,356 @@
+// vphys_epbl.cu -- EPBL, the energetic planetary boundary layer (Reichl &
+// Hallberg 2018), column form: epbl_compute -> epbl_column_kernel
+// (src/parameterizations/vertical/rdb_ocean_epbl.F90:864-1659) with
+// epbl_find_mstar (:630-688) and epbl_mixlen_shape (:690-714).
+//
+// One thread solves one column: the prep sweep (T0, S0 and the
+// pressure-weighted potential-energy and column-height weights of each layer
+// from the EOS derivatives), the surface energetics (B0, the convective
+// release of the skin fluxes, u*, |f|), then up to epbl_mld_max_its
+// mixed-layer-depth iterations, each a downward sweep that spends the
+// wind and convective TKE on the largest diffusivity each interface can
+// afford (closed-form energy solve with an embedded forward elimination) and
+// moves the MLD guess (false position with a bisection fallback).  The
+// column's eight per-layer arrays (h and the prep weights, 1-based,
+// bottom-up as the reference stores them) live in the thread's local memory,
+// sized by a compile-time bucket of nz.  Every value is formed by the same
+// operations in the same order as the reference; built with -fmad=false it
+// is bit-identical to the CPU restatement.
+#include <cuda_runtime.h>
+
+#include "vphys_device.cuh"
+#include "vphys_kernels.cuh"
+
+namespace vphys {
+namespace {
+
+constexpr double H_NEGLECT = H_DIV_EPS;   // rdb_ocean_epbl.F90:172-178
+
+// eos_specvol_derivs (rdb_eos.F90:1551-1622)
+__device__ __forceinline__ void specvol_derivs(const vphys_config &c, double T, double S, double pres, double &dsv_dt,
+                                               double &dsv_ds)
+{
+    if (c.eos_variant == 1) {
+        dsv_dt = xdiv(c.eos_alpha_t, c.rho0 * c.rho0);
+        dsv_ds = xdiv(-c.eos_beta_s, c.rho0 * c.rho0);
+        return;
+    }
+    const double T_sq = T * T;
+    const double p_0 = WRIGHT_B0 + WRIGHT_B1 * T + WRIGHT_B2 * T_sq + WRIGHT_B3 * T_sq * T + WRIGHT_B4 * S +
+                       WRIGHT_B5 * S * T;
+    const double lambda = WRIGHT_C0 + WRIGHT_C1 * T + WRIGHT_C2 * T_sq + WRIGHT_C3 * T_sq * T + WRIGHT_C4 * S +
+                          WRIGHT_C5 * S * T;
+    const double dp0_dt = WRIGHT_B1 + 2.0 * WRIGHT_B2 * T + 3.0 * WRIGHT_B3 * T_sq + WRIGHT_B5 * S;
+    const double dlam_dt = WRIGHT_C1 + 2.0 * WRIGHT_C2 * T + 3.0 * WRIGHT_C3 * T_sq + WRIGHT_C5 * S;
+    const double dp0_ds = WRIGHT_B4 + WRIGHT_B5 * T;
+    const double dlam_ds = WRIGHT_C4 + WRIGHT_C5 * T;
+    const double big_p = pres + p_0;
+    const double inv_p = 1.0 / big_p;
+    const double inv_p2 = inv_p * inv_p;
+    dsv_dt = WRIGHT_A1 + dlam_dt * inv_p - lambda * dp0_dt * inv_p2;
+    dsv_ds = WRIGHT_A2 + dlam_ds * inv_p - lambda * dp0_ds * inv_p2;
+}
+
+// epbl_find_mstar, schemes constant (1) and OM4 (2)
+__device__ __forceinline__ double find_mstar(const vphys_config &c, double b0, double ustar, double bld, double absf)
+{
+    double mstar;
+    const double absf_floor = fmx(absf, 1.0e-20);
+    if (c.epbl_mstar_scheme == 2) {
+        const double mstar_s = c.epbl_mstar_coef1 * sqrt(xdiv(fmx(0.0, b0), ustar * ustar * absf_floor));
+        double mstar_n = 0.0;
+        if (ustar > absf_floor * bld) mstar_n = c.epbl_c_ek * sm_log(xdiv(ustar, absf_floor * fmx(bld, 1.0e-10)));
+        mstar = fmx(mstar_s, fmn(1.25, mstar_n));
+        if (c.epbl_mstar_cap > 0.0) mstar = fmn(c.epbl_mstar_cap, mstar);
+    } else {
+        mstar = c.epbl_mstar_const;
+    }
+    if (c.epbl_mstar_conv_adj > 0.0) {
+        const double t1 = -bld * fmn(0.0, b0);
+        const double t2 = 2.0 * mstar * (ustar * ustar * ustar);
+        if (t2 > 0.0)
+            mstar = xdiv(mstar * ((1.0 - c.epbl_mstar_conv_adj) * t1 + t2), t1 + t2);
+        else
+            mstar = mstar * (1.0 - c.epbl_mstar_conv_adj);
+    }
+    return mstar;
+}
+
+// the turbulent velocity scale (cube root of the TKE rate, or RH18)
+__device__ __forceinline__ double vstar_of(const vphys_config &c, double tke_here, double conv_perel, double ustar,
+                                           double htot, double mld_guess, double dt)
+{
+    if (c.epbl_vstar_scheme == 2) {
+        const double surf_scale = fmx(0.05, 1.0 - xdiv(htot, mld_guess));
+        return c.epbl_vstar_scale_fac * surf_scale *
+               (c.epbl_vstar_surf_fac * ustar + sm_cbrt(xdiv(c.epbl_wstar_ustar_coef * conv_perel, dt * c.rho0)));
+    }
+    return c.epbl_vstar_scale_fac * sm_cbrt(xdiv(tke_here, dt * c.rho0));
+}
+
+// the Ekman-limited mixing length times v* kappa
+__device__ __forceinline__ double mixlen_kd(const vphys_config &c, double vstar, double htot, double hbs, double absf)
+{
+    const double num = htot * hbs * vstar;
+    const double den = c.epbl_ekman_scale_coef * absf * htot * hbs + vstar;
+    if (c.epbl_mld_iteration) return vstar * c.epbl_von_karman * fmx(c.epbl_min_mix_len, xdiv(num, den));
+    return xdiv(vstar * c.epbl_von_karman * num, den);
+}
+
+template <int N>   // N = bucket + 2: indices 1..nz+1 with nz <= bucket
+__global__ void __launch_bounds__(128, 4) k_epbl(const Params p, double dt, double inv_rho0_cp, double inv_rho0)
+{
+    const size_t col = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (col >= p.plane) return;
+    const vphys_config &c = p.cfg;
+    const int nz = p.nz;
+    const size_t P = p.plane;
+    const double rho0 = c.rho0;
+    const double g_rho0 = GRAVITY * rho0;
+    double *kdg = p.kd_epbl + col;
+    const double *T = p.tr[c.idx_temperature] + col;
+    const double *S = p.tr[c.idx_salinity] + col;
+
+    double h[N], t0[N], s0[N], dpe_t[N], dpe_s[N], dch_t[N], dch_s[N], kd[N];
+    int k_sfc = nz;   // first live layer from the top (nz when none is live)
+    for (int k = nz; k >= 1; --k) {
+        h[k] = p.h[col + P * (size_t)(k - 1)];
+    }
+    for (int k = nz; k >= 1; --k)
+        if (h[k] > H_VANISHED) {
+            k_sfc = k;
+            break;
+        }
+    // ---- column prep (downward)
+    double pres = 0.0, h_sum = 0.0, dsv_dt_sfc = 0.0, dsv_ds_sfc = 0.0;
+    for (int k = nz; k >= 1; --k) {
+        const double hk = h[k];
+        double t0k = 0.0, s0k = 0.0;
+        if (hk > 0.0) {
+            t0k = T[P * (size_t)(k - 1)];
+            s0k = S[P * (size_t)(k - 1)];
+        }
+        const double dmass = rho0 * hk;
+        const double dpres = GRAVITY * dmass;
+        const double p_mid = pres + 0.5 * dpres;
+        double dsv_dt_k, dsv_ds_k;
+        specvol_derivs(c, t0k, s0k, p_mid, dsv_dt_k, dsv_ds_k);
+        t0[k] = t0k;
+        s0[k] = s0k;
+        dpe_t[k] = dmass * p_mid * dsv_dt_k;
+        dpe_s[k] = dmass * p_mid * dsv_ds_k;
+        dch_t[k] = dmass * dsv_dt_k;
+        dch_s[k] = dmass * dsv_ds_k;
+        if (k == k_sfc) {
+            dsv_dt_sfc = dsv_dt_k;
+            dsv_ds_sfc = dsv_ds_k;
+        }
+        if (k <= k_sfc) {
+            pres = pres + dpres;
+            h_sum = h_sum + hk;
+        }
+    }
+    h_sum = h_sum + H_NEGLECT;
+
+    // ---- surface forcing energetics
+    const double q_t_kin = inv_rho0_cp * p.q_heat[col];
+    const double q_s_kin = inv_rho0 * p.q_salt[col];
+    const double b0 = g_rho0 * (dsv_dt_sfc * q_t_kin + dsv_ds_sfc * q_s_kin);
+    const double ctke_sfc =
+        -0.5 * GRAVITY * (rho0 * rho0) * h[k_sfc] * (q_t_kin * dt * dsv_dt_sfc + q_s_kin * dt * dsv_ds_sfc);
+    const double ustar = fmx(sqrt(xdiv(p.stress_mag[col], rho0)), c.epbl_ustar_min);
+    const double f = p.coriolis ? p.coriolis[col] : 0.0;
+    const double absf = sqrt((1.0 - c.epbl_omega_frac) * (f * f) + c.epbl_omega_frac * 4.0 * (c.epbl_omega * c.epbl_omega));
+    const double idecay = xdiv(c.epbl_tke_decay * absf, ustar);
+    const double mech_in = dt * rho0 * (ustar * ustar * ustar);
+
+    double mld_found = 0.0;
+    if (p.wet[col] <= 0.0 || h_sum <= 2.0 * H_NEGLECT) {
+        for (int k = 1; k <= nz + 1; ++k) kd[k] = 0.0;
+    } else {
+        double min_mld = 0.0, max_mld = h_sum, dmld_min = 0.0, dmld_max = 0.0;
+        bool have_min = false, have_max = false;
+        double mld_guess = 0.5 * (min_mld + max_mld);
+        if (c.epbl_mld_use_prev_guess && p.mld_epbl[col] > 0.0) mld_guess = fmn(p.mld_epbl[col], max_mld);
+        const int n_its = c.epbl_mld_iteration ? c.epbl_mld_max_its : 1;
+        double dt_h = 0.0;   // carried from interface to interface, as the reference's local
+        for (int obl_it = 1; obl_it <= n_its; ++obl_it) {
+            const double mstar_val = find_mstar(c, b0, ustar, mld_guess, absf);
+            double mech_tke = mstar_val * mech_in;
+            double conv_perel;
+            if (ctke_sfc <= 0.0) {
+                mech_tke = mech_tke + fmx(ctke_sfc, -mech_tke);
+                conv_perel = 0.0;
+            } else {
+                conv_perel = ctke_sfc;
+            }
+            double h_ka = h[k_sfc] + H_NEGLECT;
+            double hp_a = h_ka;
+            double dpe_t_a = dpe_t[k_sfc], dpe_s_a = dpe_s[k_sfc], dch_t_a = dch_t[k_sfc], dch_s_a = dch_s[k_sfc];
+            double th_a = h_ka * t0[k_sfc], sh_a = h_ka * s0[k_sfc];
+            double te_lag = 0.0, se_lag = 0.0, kddt_prev = 0.0;
+            double htot = h[k_sfc], z_int = h[k_sfc], pres_int = g_rho0 * h[k_sfc], mld_output = h[k_sfc];
+            bool sfc_connected = true;
+            for (int ki = k_sfc + 1; ki <= nz + 1; ++ki) kd[ki] = 0.0;
+
+            for (int ki = k_sfc; ki >= 2; --ki) {
+                const int ka = ki, kb = ki - 1;
+                h_ka = h[ka] + H_NEGLECT;
+                const double h_kb = h[kb] + H_NEGLECT;
+                bool sfc_disconnect = false;
+                mech_tke = mech_tke * sm_exp(-h_ka * idecay);
+                double nstar_fc = c.epbl_nstar;
+                if (conv_perel > 0.0 && absf > 0.0) {
+                    const double ah = absf * htot;
+                    nstar_fc = xdiv(c.epbl_nstar * conv_perel,
+                                    conv_perel + 0.2 * sqrt(0.5 * dt * rho0 * (ah * ah * ah) * conv_perel));
+                }
+                double tot_tke = mech_tke + nstar_fc * conv_perel;
+                double kd_val;
+                if (tot_tke <= 0.0 &&
+                    0.0 <= (dch_t[kb] + dch_t[ka]) * (t0[ka] - t0[kb]) + (dch_s[kb] + dch_s[ka]) * (s0[ka] - s0[kb])) {
+                    kd_val = 0.0;
+                    sfc_disconnect = true;
+                } else {
+                    dt_h = xdiv(dt, fmx(0.5 * (h_ka + h_kb), 1.0e-15 * h_sum));
+                    double tke_here = mech_tke + c.epbl_wstar_ustar_coef * conv_perel;
+                    const double hb_hs = xdiv(h_sum - z_int, h_sum);
+                    double shape_fn = 1.0;
+                    {
+                        const double ts = c.epbl_translay_scale;
+                        if (c.epbl_mld_iteration && !(ts >= 1.0) && !(ts < 0.0) && !(mld_guess <= 0.0)) {
+                            const double fr = fmx(0.0, xdiv(mld_guess - z_int, mld_guess));
+                            shape_fn = ts + (1.0 - ts) * fr * fr;
+                        }
+                    }
+                    const double hbs = fmn(hb_hs, shape_fn);
+                    double kd_g0 = 0.0;
+                    if (tke_here > 0.0) kd_g0 = mixlen_kd(c, vstar_of(c, tke_here, conv_perel, ustar, htot, mld_guess, dt),
+                                                          htot, hbs, absf);
+                    const double hp_b = h_kb;
+                    const double th_b = h_kb * t0[kb];
+                    const double sh_b = h_kb * s0[kb];
+                    const double hps = hp_a + hp_b;
+                    const double bdt1 = hp_a * hp_b;
+                    const double dt_c = hp_a * th_b - hp_b * th_a;
+                    const double ds_c = hp_a * sh_b - hp_b * sh_a;
+                    double pec_core =
+                        hp_b * (dpe_t_a * dt_c + dpe_s_a * ds_c) - hp_a * (dpe_t[kb] * dt_c + dpe_s[kb] * ds_c);
+                    const double colht_core =
+                        hp_b * (dch_t_a * dt_c + dch_s_a * ds_c) - hp_a * (dch_t[kb] * dt_c + dch_s[kb] * ds_c);
+                    if (colht_core < 0.0) pec_core = pec_core - pres_int * colht_core;
+                    const double dkddt = kd_g0 * dt_h;
+                    const double pe_max = xdiv(pec_core, bdt1 * hps);
+                    if (pe_max < 0.0) {
+                        // convectively unstable: the Kd of the mixing length, the release banked
+                        tke_here = mech_tke + c.epbl_wstar_ustar_coef * (conv_perel - pe_max);
+                        if (tke_here > 0.0)
+                            kd_val = mixlen_kd(c, vstar_of(c, tke_here, conv_perel, ustar, htot, mld_guess, dt), htot,
+                                               hbs, absf);
+                        else
+                            kd_val = 0.0;
+                        const double pe_g0 = xdiv(pec_core * dkddt, bdt1 * (bdt1 + dkddt * hps));
+                        double dpe_conv = xdiv(pec_core * (kd_val * dt_h), bdt1 * (bdt1 + (kd_val * dt_h) * hps));
+                        if (dpe_conv > 0.0) {
+                            kd_val = kd_g0;
+                            dpe_conv = pe_g0;
+                        }
+                        conv_perel = conv_perel - dpe_conv;
+                        if (sfc_connected) mld_output = mld_output + h[kb];
+                    } else {
+                        // stable: the energy-limited Kd; the reservoirs drained
+                        double tke_used, frac_bl;
+                        if ((pec_core * dkddt <= tot_tke * (bdt1 * (bdt1 + dkddt * hps))) || (pec_core <= 0.0)) {
+                            kd_val = kd_g0;
+                            tke_used = xdiv(pec_core * dkddt, bdt1 * (bdt1 + dkddt * hps));
+                            frac_bl = 1.0;
+                        } else {
+                            kd_val = xdiv(bdt1 * bdt1 * tot_tke, dt_h * (pec_core - bdt1 * hps * tot_tke));
+                            tke_used = tot_tke;
+                            frac_bl = xdiv(tot_tke * (bdt1 * (bdt1 + dkddt * hps)), pec_core * dkddt);
+                        }
+                        if (sfc_connected) mld_output = mld_output + frac_bl * h[kb];
+                        if (frac_bl < 1.0) sfc_disconnect = true;
+                        double r_reduc = 0.0;
+                        if (tot_tke > 0.0 && tot_tke > tke_used) r_reduc = xdiv(tot_tke - tke_used, tot_tke);
+                        mech_tke = r_reduc * mech_tke;
+                        conv_perel = r_reduc * conv_perel;
+                    }
+                }
+                kd[ki] = kd_val;
+                const double kddt_cur = kd_val * dt_h;
+                const double b1 = 1.0 / (hp_a + kddt_cur);
+                const double c1 = kddt_cur * b1;
+                if (ki == k_sfc) {
+                    te_lag = b1 * (h_ka * t0[ka]);
+                    se_lag = b1 * (h_ka * s0[ka]);
+                } else {
+                    const double te_new = b1 * (h_ka * t0[ka] + kddt_prev * te_lag);
+                    const double se_new = b1 * (h_ka * s0[ka] + kddt_prev * se_lag);
+                    te_lag = te_new;
+                    se_lag = se_new;
+                }
+                hp_a = h_kb + (hp_a * b1) * kddt_cur;
+                dpe_t_a = dpe_t[kb] + c1 * dpe_t_a;
+                dpe_s_a = dpe_s[kb] + c1 * dpe_s_a;
+                dch_t_a = dch_t[kb] + c1 * dch_t_a;
+                dch_s_a = dch_s[kb] + c1 * dch_s_a;
+                th_a = h_kb * t0[kb] + kddt_cur * te_lag;
+                sh_a = h_kb * s0[kb] + kddt_cur * se_lag;
+                kddt_prev = kddt_cur;
+                if (sfc_disconnect) {
+                    htot = h[kb];
+                    sfc_connected = false;
+                } else {
+                    htot = htot + h[kb];
+                }
+                z_int = z_int + h[kb];
+                pres_int = pres_int + g_rho0 * h[kb];
+            }
+            kd[1] = 0.0;
+            mld_found = mld_output;
+            if (!c.epbl_mld_iteration) break;
+            if (fabs(mld_found - mld_guess) < c.epbl_mld_tol) break;
+            if (obl_it == n_its) break;
+            if (mld_found > mld_guess) {
+                min_mld = mld_guess;
+                dmld_min = mld_found - mld_guess;
+                have_min = true;
+            } else {
+                max_mld = mld_guess;
+                dmld_max = mld_found - mld_guess;
+                have_max = true;
+            }
+            if (c.epbl_mld_bisection)
+                mld_guess = 0.5 * (min_mld + max_mld);
+            else if (have_min && have_max && obl_it > 2 && (obl_it - 1) % 4 > 0)
+                mld_guess = min_mld + xdiv(dmld_min * (max_mld - min_mld), dmld_min - dmld_max);
+            else if (mld_found > min_mld && mld_found < max_mld)
+                mld_guess = mld_found;
+            else
+                mld_guess = 0.5 * (min_mld + max_mld);
+        }
+    }
+    for (int k = 1; k <= nz + 1; ++k) kdg[P * (size_t)(k - 1)] = kd[k];
+    p.mld_epbl[col] = mld_found;
+}
+
+}  // namespace
+
+void launch_epbl(const Params &p, double dt, cudaStream_t stream)
+{
+    // the column-invariant multipliers, divided on the host in IEEE double
+    // (epbl_compute passes 1/(rho0 cp) and 1/rho0, rdb_ocean_epbl.F90:906-927)
+    const double inv_rho0_cp = 1.0 / (p.cfg.rho0 * p.cfg.cp);
+    const double inv_rho0 = 1.0 / p.cfg.rho0;
+    const int threads = 128;
+    const unsigned blocks = (unsigned)((p.plane + threads - 1) / threads);
+    if (p.nz <= 32)
+        k_epbl<34><<<blocks, threads, 0, stream>>>(p, dt, inv_rho0_cp, inv_rho0);
+    else if (p.nz <= 80)
+        k_epbl<82><<<blocks, threads, 0, stream>>>(p, dt, inv_rho0_cp, inv_rho0);
+    else
+        k_epbl<NZ_MAX + 2><<<blocks, threads, 0, stream>>>(p, dt, inv_rho0_cp, inv_rho0);
+}
+
+}  // namespace vphys

@@ -184,11 +184,12 @@ constexpr int ASM_THREADS = 128;
 __host__ __device__ __forceinline__ bool is_default_assembly_knobs(const vphys_config &c)
 {
     return c.interior_closure == VPHYS_INTERIOR_PP81 && c.use_kpp && c.bkgnd_profile && !(c.kv_ml_invz2 > 0.0) &&
-           !c.conv_enable && !c.vmix_guard && !c.buoyancy_coeffs && c.sw_pen_frac == 0.0 && !c.kappa_shear;
+           !c.conv_enable && !c.vmix_guard && !c.buoyancy_coeffs && c.sw_pen_frac == 0.0 && !c.kappa_shear && !c.epbl;
 }
 __device__ __forceinline__ void default_assembly_knobs(vphys_config &c)
 {
     c.kappa_shear = 0;
+    c.epbl = 0;
     c.interior_closure = VPHYS_INTERIOR_PP81;
     c.use_kpp = 1;
     c.bkgnd_profile = 1;
@@ -242,10 +243,12 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
         all_zero = all_zero && (hk == 0.0);
     }
 
-    double h_b = p.bl_depth[col];   // lagged BL depth (state)
+    // lagged KPP BL depth (state); under EPBL its MLD, the depth convection
+    // masks with (rdb_ocean_dyn.F90:1606-1610)
+    double h_b = c.epbl ? p.mld_epbl[col] : p.bl_depth[col];
     double q_T_kin = 0.0, q_S_kin = 0.0, w_s = 0.0;
     bool destabilizing = false, kpp_active = false;
-    if (c.use_kpp) {
+    if (c.use_kpp && !c.epbl) {   // EPBL replaces KPP (rdb_ocean_dyn.F90:1539)
         // ---- KPP pass 1 (rdb_ocean_vmix.F90:1288-1426) ----
         const double tau_mag = p.stress_mag[col];
         const double u_star = sqrt(xdiv(tau_mag, rho0));
@@ -345,7 +348,7 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
     const R kv_max = (R)c.kv_max, kd_max = (R)c.kd_max, kt_bg = (R)c.kt_bg, ks_bg = (R)c.ks_bg;
     const R cs = (R)c.cs_nonlocal, qT = (R)q_T_kin, qS = (R)q_S_kin, hbR = (R)h_b, wsR = (R)w_s;
     const R invz2 = (R)c.kv_ml_invz2, conv_kd = (R)c.conv_kd, conv_pr = (R)c.conv_prandtl, conv_n2 = (R)c.conv_n2_thresh;
-    const R ks_pr = (R)c.ks_prandtl_turb;
+    const R ks_pr = (R)c.ks_prandtl_turb, epbl_pr = (R)c.epbl_prandtl;
     // gate constants (vmix_assemble, rdb_ocean_vmix.F90:2279-2348)
     const R pr_bl = (R)((c.bkgnd_prandtl > 0.0) ? c.bkgnd_prandtl : 1.0);
     const R kv_floor_scalar = (R)((c.bkgnd_prandtl > 0.0) ? c.bkgnd_prandtl * c.kt_bg + c.kv_bg : c.kv_bg);
@@ -501,7 +504,27 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
             if (q >= 2) {
                 // ---- kappa-shear merge after KPP, interior interfaces only
                 //      (kappa_shear_merge_into_kv_kt, rdb_ocean_kappa_shear.F90:381-421) ----
-                if (c.kappa_shear) {
+                // ---- EPBL merge (epbl_merge_into_kv_kt / epbl_merge_max_shear,
+                //      rdb_ocean_epbl.F90:1661-1718); with combine = max_shear and
+                //      kappa-shear on, kappa-shear is merged first (rdb_ocean_dyn.F90:1553-1559)
+                const bool shear_first = c.kappa_shear && c.epbl && c.epbl_combine == 3;
+                if (c.epbl) {
+                    const R kde = (R)p.kd_epbl[col + P * (size_t)(q - 1)];
+                    if (shear_first) {
+                        const R kds = (R)p.kd_shear[col + P * (size_t)(q - 1)];
+                        ktq = ktq + kds;
+                        kvq = kvq + ks_pr * kds;
+                        ktq = ktq + fmx(kde - kds, R(0));
+                        kvq = kvq + fmx(epbl_pr * kde - ks_pr * kds, R(0));
+                    } else if (c.epbl_combine == 2) {
+                        ktq = fmx(ktq, kde);
+                        kvq = fmx(kvq, epbl_pr * kde);
+                    } else {
+                        ktq = ktq + kde;
+                        kvq = kvq + epbl_pr * kde;
+                    }
+                }
+                if (c.kappa_shear && !shear_first) {
                     const R kd = (R)p.kd_shear[col + P * (size_t)(q - 1)];
                     ktq = ktq + kd;
                     kvq = kvq + ks_pr * kd;

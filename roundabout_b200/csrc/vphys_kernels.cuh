@@ -47,6 +47,7 @@ struct Params {
     double *zcol;                     // per column: -sum_k h, k = 1..nz in order (momentum z_clear), scratch
     const double *coriolis;           // (nx, ny) f, or nullptr (learned KPP features, kappa-shear f^2)
     double *kd_shear, *tke_shear;     // (nx, ny, nz+1) kappa-shear diffusivity and TKE, or nullptr
+    double *kd_epbl, *mld_epbl;       // (nx, ny, nz+1) EPBL diffusivity, (nx, ny) its MLD, or nullptr
     const float *kpp_pred;            // per column: the surrogate's h_b, < 0: run pass 1; nullptr: plain KPP
     const float *kpp_check;           // per column: h_b to compare with pass 1 (>= 0), or nullptr
     unsigned long long *kpp_stats;    // learned KPP counters (k_kpp_roll)
@@ -71,6 +72,8 @@ void launch_stress_mag(const Params &p, cudaStream_t stream);
 // first through order (per column) bucketed in hist (1024 counts).
 void launch_kappa_shear(const Params &p, double dt, int *work, int *order, unsigned *hist, bool ordered,
                         cudaStream_t stream);
+// EPBL column solve into p.kd_epbl / p.mld_epbl (vphys_epbl.cu)
+void launch_epbl(const Params &p, double dt, cudaStream_t stream);
 void launch_assemble(const Params &p, cudaStream_t stream);
 void launch_smooth(const Params &p, double *fld, double *scratch, cudaStream_t stream);
 void launch_momentum(const Params &p, double dt, cudaStream_t stream);

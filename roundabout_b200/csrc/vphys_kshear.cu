@@ -807,12 +807,12 @@ KsPar ks_par_of(const vphys_config &c)
     k.src_max_chg = c.ks_src_max_chg;
     k.vel_underflow = c.ks_vel_underflow;
     k.rho0 = c.rho0;
-    k.alpha_t = c.ks_alpha_t;
-    k.beta_s = c.ks_beta_s;
+    k.alpha_t = c.eos_alpha_t;
+    k.beta_s = c.eos_beta_s;
     k.lz_rescale = c.ks_lz_rescale;
     k.max_inner_it = c.ks_max_inner_it;
     k.max_substep_it = c.ks_max_substep_it;
-    k.eos_linear = c.ks_eos == 1;
+    k.eos_linear = c.eos_variant == 1;
     // column-invariant scalars, formed on the host in IEEE double exactly as
     // ks_solve_column (:1604-1608) and ks_adaptive_dt (:1446-1451) form them
     k.tke_min = c.ks_tke_bg > 1.0e-20 ? c.ks_tke_bg : 1.0e-20;

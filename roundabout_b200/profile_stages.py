@@ -5,7 +5,8 @@
     python -m roundabout_b200.profile_stages --nx 512 --ny 384 --stages features,mlp
 
 Stages: eos, assemble, momentum, tracers, step (the path), kshear (the
-kappa-shear column solve, vphys_kappa_shear, default knobs, Wright EOS), and
+kappa-shear column solve, vphys_kappa_shear, default knobs, Wright EOS), epbl
+(the EPBL column solve, vphys_epbl, default knobs: OM4 mstar), and
 features, mlp (the learned KPP's feature extraction and its three tensor-core
 GEMMs, with untrained weights: the time does not depend on their values).
 
@@ -57,15 +58,19 @@ def main():
     if "kshear" in args.stages:
         for _ in range(args.warmup):
             vp.kappa_shear(dt)
+    if "epbl" in args.stages:
+        for _ in range(args.warmup):
+            vp.epbl(dt)
     torch.cuda.synchronize()
     cells = args.nx * args.ny * args.nz
     ifc = (args.nz + 1) / args.nz
     bpc = {"eos": 32.0, "assemble": 32.0 + 24 * ifc, "momentum": 48.0, "tracers": 16.0 + 16.0 * args.ntr,
            "step": 8 * (4 + args.ntr) + 8 * (2 + args.ntr) + 24 * ifc,
-           "kshear": 8.0 * 7 + 16 * ifc}   # h, u and v (two faces each), T, S in; kd, tke out
+           "kshear": 8.0 * 7 + 16 * ifc,   # h, u and v (two faces each), T, S in; kd, tke out
+           "epbl": 24.0 + 8 * ifc}         # h, T, S in; kd out (the 2-D forcing and MLD ~0.1 B/cell)
     fns = {"eos": vp.eos, "assemble": vp.assemble, "momentum": lambda: vp.vdiff_momentum(dt),
            "tracers": lambda: vp.vdiff_tracers(dt), "step": lambda: vp.step(dt, 1),
-           "kshear": lambda: vp.kappa_shear(dt)}
+           "kshear": lambda: vp.kappa_shear(dt), "epbl": lambda: vp.epbl(dt)}
     ncols = args.nx * args.ny
     if "features" in args.stages or "mlp" in args.stages:
         import ctypes

@@ -2,10 +2,10 @@
 
 Reads tests/test_safe_math_golden.inc of the reference (Roundabout; the
 table generated by its tools/gen_safe_math_golden.F90 from contraction-off
-builds) and writes tests/golden/safe_math_golden.json with the CBRT, ATAN and
-EXP rows: each row is [argument_bits, result_bits] as 16-hex-digit IEEE
+builds) and writes tests/golden/safe_math_golden.json with the CBRT, ATAN,
+EXP and LOG rows: each row is [argument_bits, result_bits] as 16-hex-digit IEEE
 binary64 words.  These pin the oracle's port of rdb_sm_cbrt / rdb_sm_atan /
-rdb_sm_exp bit for bit.
+rdb_sm_exp / rdb_sm_log bit for bit.
 
 Usage (in a container where the reference tree is mounted):
     python tests/golden/make_safe_math_golden.py /path/to/roundabout
@@ -32,7 +32,8 @@ def main():
     ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
     text = (ref / "tests" / "test_safe_math_golden.inc").read_text()
     out = {"source": "tests/test_safe_math_golden.inc (reference)",
-           "cbrt": parse(text, "CBRT"), "atan": parse(text, "ATAN"), "exp": parse(text, "EXP")}
+           "cbrt": parse(text, "CBRT"), "atan": parse(text, "ATAN"), "exp": parse(text, "EXP"),
+           "log": parse(text, "LOG")}
     dst = Path(__file__).with_name("safe_math_golden.json")
     dst.write_text(json.dumps(out, indent=1) + "\n")
     print("wrote", dst, {k: len(v) for k, v in out.items() if isinstance(v, list)})

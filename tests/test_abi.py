@@ -87,7 +87,7 @@ def test_kappa_shear_knobs_are_validated(lib):
     from roundabout_b200.config import KappaShear, default_config
 
     h = ctypes.c_void_p()
-    for name, value in (("ks_max_inner_it", 0), ("ks_max_substep_it", -1), ("ks_eos", 2), ("ks_lambda", 0.0),
+    for name, value in (("ks_max_inner_it", 0), ("ks_max_substep_it", -1), ("eos_variant", 2), ("ks_lambda", 0.0),
                         ("kappa_shear", 2)):
         bad = default_config()
         setattr(bad, name, value)
@@ -97,3 +97,24 @@ def test_kappa_shear_knobs_are_validated(lib):
     assert cfg.kappa_shear == 1 and cfg.ks_ri_crit == 0.3 and cfg.ks_prandtl_turb == 0.8
     with pytest.raises(NotImplementedError):
         KappaShear(at_vertex=True)
+
+
+def test_epbl_knobs_are_validated(lib):
+    """EPBL's unbuilt options are refused at create (no device work)."""
+    from roundabout_b200 import _ffi
+    from roundabout_b200.config import EPBL, default_config
+
+    h = ctypes.c_void_p()
+    for over in (dict(epbl_mstar_scheme=3), dict(epbl_mixlen_exponent=1.5), dict(sw_pen_frac=0.5),
+                 dict(learned_kpp=1), dict(epbl_combine=4), dict(epbl_mld_max_its=0), dict(epbl_ustar_min=0.0)):
+        bad = default_config()
+        bad.epbl = 1
+        for k, v in over.items():
+            setattr(bad, k, v)
+        assert lib.vphys_create(4, 4, 4, 2, ctypes.byref(bad), ctypes.byref(h)) == _ffi.ERR_CONFIG, over
+        assert h.value is None
+    cfg = EPBL(mstar_scheme="om4", combine="max_shear", mld_use_prev_guess=True).apply(default_config())
+    assert (cfg.epbl, cfg.use_kpp, cfg.epbl_mstar_scheme, cfg.epbl_combine, cfg.epbl_mld_use_prev_guess) == (1, 0, 2, 3, 1)
+    for bad_kw in (dict(mstar_scheme="rh18"), dict(langmuir=object())):
+        with pytest.raises(NotImplementedError):
+            EPBL(**bad_kw)

@@ -45,7 +45,7 @@ def beta_plane(ny, nx):
     return np.asfortranarray(np.broadcast_to(f, (nx, ny)))
 
 
-KNOBS = dict(ks_eos=1, ks_alpha_t=0.2, ks_beta_s=0.77, ks_vel_underflow=1.0e-3, ks_tke_bg=1.0e-12,
+KNOBS = dict(eos_variant=1, eos_alpha_t=0.2, eos_beta_s=0.77, ks_vel_underflow=1.0e-3, ks_tke_bg=1.0e-12,
              ks_src_max_chg=8.0, ks_lz_rescale=0.5, ks_ri_crit=0.3, ks_max_inner_it=20, ks_max_substep_it=9)
 
 
@@ -90,7 +90,7 @@ def test_golden_column_on_the_gpu(VP, oracle):
     assert_bitwise("kd_shear", kd, st.kd_shear)
     worst = max(abs(kd[1, 1, 20 - k] - g) / g for k, g in enumerate(GOLDEN_SD) if g > 1e-10)
     assert worst < 1.0e-6, worst
-    assert (ALPHA, BETA, RHO0) == (cfg.ks_alpha_t, cfg.ks_beta_s, cfg.rho0)
+    assert (ALPHA, BETA, RHO0) == (cfg.eos_alpha_t, cfg.eos_beta_s, cfg.rho0)
 
 
 def test_assemble_merges_kd(VP, oracle):

@@ -1,0 +1,165 @@
+"""Known-answer tests of the EPBL oracle (vphys_oracle_epbl.c), re-expressed
+from the reference's tests/test_ocean_epbl.F90.  Its driver `run_epbl_steps`
+(:117-163) is restated here: per step the surface flux into T, EPBL, then the
+implicit tracer diffusion with EPBL's kd as the diffusivity.
+
+* Kraus-Turner wind deepening (:297-357): monotone MLD growth, log-log
+  exponent in [0.20, 0.47], prefactor in [0.9, 1.8] of (12 mstar u*^3 t/N^2)^(1/3);
+* a stabilising flux shoals the MLD below 95 % of the neutral one (:486-530);
+* convective deepening (:532-585): monotone, within [0.5, 1.4] of the
+  encroachment depth sqrt(2 B0 t)/N, mixing at the near-surface interface;
+* collapsed top layers (:720-790): kd and MLD equal those of the column
+  without them, no mixing on the interfaces above the first live layer;
+* the OM4 mstar (:243-281) in closed form on a neutral two-layer column,
+  including its zero-Ekman-term limit.
+"""
+import math
+
+import numpy as np
+import pytest
+
+G = 9.80665
+RHO0 = 1035.0
+ALPHA_LIN = 0.2
+BETA_LIN = 0.8
+CP = 3992.0
+
+
+def epbl_config(**over):
+    """setup_epbl (test_ocean_epbl.F90:76-97): linear EOS, constant mstar
+    1.2, nstar 0.2, f = 0."""
+    from roundabout_b200.config import default_config
+
+    c = default_config()
+    c.epbl = 1
+    c.epbl_mstar_scheme = 1
+    c.epbl_mstar_const = 1.2
+    c.epbl_nstar = 0.2
+    c.eos_variant = 1
+    c.eos_alpha_t = ALPHA_LIN
+    c.eos_beta_s = BETA_LIN
+    c.rho0 = RHO0
+    c.cp = CP
+    for k, v in over.items():
+        setattr(c, k, v)
+    return c
+
+
+def stratified(oracle, nz, dz, t_surf, dtdz, nx=2, ny=1):
+    """setup_stratified_T (:99-115)."""
+    st = oracle.OracleState(nx, ny, nz, 2)
+    st.h[...] = dz
+    for k in range(1, nz + 1):
+        z = (float(nz - k) + 0.5) * dz
+        st.tracers[1][:, :, k - 1] = t_surf - dtdz * z
+        st.tracers[0][:, :, k - 1] = 35.0
+    return st
+
+
+def run_steps(st, cfg, dt, n_steps, sample_every, stress=0.0, q_heat=0.0):
+    st.stress_mag[...] = stress
+    st.q_heat[...] = q_heat
+    st.q_salt[...] = 0.0
+    mld, t = [], []
+    for step in range(1, n_steps + 1):
+        st.call("vpo_surface_flux", cfg, dt)
+        st.call("vpo_epbl", cfg, dt)
+        st.kt[...] = st.kd_epbl
+        st.ks[...] = st.kd_epbl
+        st.call("vpo_vdiff_tracers", cfg, dt)
+        if step % sample_every == 0:
+            mld.append(float(st.mld_epbl[0, 0]))
+            t.append(step * dt)
+    return np.array(mld), np.array(t)
+
+
+def loglog_slope(t, d):
+    x, y = np.log(t), np.log(d)
+    x, y = x - x.mean(), y - y.mean()
+    return float((x * y).sum() / (x * x).sum())
+
+
+def test_wind_deepening_kraus_turner(oracle):
+    nz, dz, dt, ustar, n2 = 100, 3.0, 1800.0, 0.01, 1.0e-4
+    cfg = epbl_config()
+    st = stratified(oracle, nz, dz, 15.0, n2 * RHO0 / (G * ALPHA_LIN))
+    mld, t = run_steps(st, cfg, dt, 240, 12, stress=RHO0 * ustar ** 2)
+    assert (np.diff(mld) >= -1e-9).all(), mld
+    slope = loglog_slope(t[len(t) // 2 - 1:], mld[len(mld) // 2 - 1:])
+    assert 0.20 < slope < 0.47, slope
+    d_analytic = (12.0 * cfg.epbl_mstar_const * ustar ** 3 * t[-1] / n2) ** (1.0 / 3.0)
+    assert 0.9 < mld[-1] / d_analytic < 1.8, mld[-1] / d_analytic
+
+
+def test_stabilising_flux_shoals_the_mld(oracle):
+    nz, dz, dt = 60, 3.0, 1800.0
+    dtdz = 1.0e-4 * RHO0 / (G * ALPHA_LIN)
+    cfg = epbl_config()
+    a, _ = run_steps(stratified(oracle, nz, dz, 15.0, dtdz), cfg, dt, 96, 24, stress=RHO0 * 0.01 ** 2)
+    b, _ = run_steps(stratified(oracle, nz, dz, 15.0, dtdz), cfg, dt, 96, 24, stress=RHO0 * 0.01 ** 2, q_heat=500.0)
+    assert b[-1] < 0.95 * a[-1], (a[-1], b[-1])
+
+
+def test_convective_deepening(oracle):
+    nz, dz, dt, q, n2 = 60, 2.5, 1800.0, -200.0, 1.0e-4
+    cfg = epbl_config()
+    st = stratified(oracle, nz, dz, 15.0, n2 * RHO0 / (G * ALPHA_LIN))
+    mld, t = run_steps(st, cfg, dt, 96, 12, q_heat=q)
+    assert (np.diff(mld) >= -1e-9).all(), mld
+    b0 = abs(G * ALPHA_LIN * (q / (RHO0 * CP)) / RHO0)
+    d_enc = math.sqrt(2.0 * b0 * t[-1]) / math.sqrt(n2)
+    assert 0.5 < mld[-1] / d_enc < 1.4, mld[-1] / d_enc
+    assert st.kd_epbl[0, 0, nz - 1] > 1.0e-6
+
+
+@pytest.mark.parametrize("nlive,ndead", [(8, 1), (8, 2), (1, 1)])
+def test_collapsed_top_layers(oracle, nlive, ndead):
+    dz, dt = 5.0, 1800.0
+    cfg = epbl_config()
+    ref = stratified(oracle, nlive, dz, 15.0, 0.05)
+    dead = oracle.OracleState(2, 1, nlive + ndead, 2)
+    dead.h[:, :, :nlive] = ref.h
+    dead.tracers[0][:, :, :nlive] = ref.tracers[0]
+    dead.tracers[1][:, :, :nlive] = ref.tracers[1]
+    dead.h[:, :, nlive:] = 1.0e-5
+    dead.tracers[1][:, :, nlive:] = 40.0
+    dead.tracers[0][:, :, nlive:] = 35.0
+    for st in (ref, dead):
+        st.stress_mag[...] = 0.05
+        st.q_heat[...] = -200.0
+        st.call("vpo_epbl", cfg, dt)
+    if nlive >= 2:
+        scale = np.abs(ref.kd_epbl[0, 0, 1:nlive]).max()
+        assert scale > 0.0
+        assert np.abs(dead.kd_epbl[0, 0, 1:nlive] - ref.kd_epbl[0, 0, 1:nlive]).max() < 1e-9 * scale
+    assert abs(dead.mld_epbl[0, 0] - ref.mld_epbl[0, 0]) < 1e-6
+    assert np.abs(dead.kd_epbl[0, 0, nlive:]).max() == 0.0
+
+
+def test_om4_mstar_closed_form(oracle):
+    """epbl_find_mstar's OM4 branch (:655-662, test_ocean_epbl.F90:243-281)
+    through a neutral two-layer column, no fluxes, no TKE decay, no MLD
+    iteration: the one interior interface takes the unlimited first-guess
+    kd = v* kappa (htot hbs v*)/(f htot hbs + v*) with v* = cbrt(mstar) u*,
+    htot = h, hbs = 1/2 and the MLD guess (half the column) in
+    mstar = min(1.25, c_ek log(u*/(f BLD))).  When u* <= f BLD the Ekman
+    term is 0, so is mstar, and the interface does not mix."""
+    dz, dt, f = 10.0, 1800.0, 1.0e-4
+    for ustar in (0.01, 0.003, 1.0e-3):
+        got = {}
+        for scheme in (1, 2):
+            cfg = epbl_config(epbl_mstar_scheme=scheme, epbl_mld_iteration=0, epbl_tke_decay=0.0)
+            st = stratified(oracle, 2, dz, 15.0, 0.0)
+            st.coriolis[...] = f
+            st.stress_mag[...] = RHO0 * ustar ** 2
+            st.call("vpo_epbl", cfg, dt)
+            got[scheme] = float(st.kd_epbl[0, 0, 1])
+        bld = 0.5 * (2 * dz + 1e-20)
+        ustar_eff = math.sqrt(RHO0 * ustar ** 2 / RHO0)
+        for scheme, mstar in ((1, 1.2), (2, 0.085 * math.log(ustar_eff / (f * bld)) if ustar_eff > f * bld else 0.0)):
+            mstar = min(1.25, mstar) if scheme == 2 else mstar
+            vstar = (mstar * ustar_eff ** 3) ** (1.0 / 3.0)
+            want = vstar * 0.41 * (dz * 0.5 * vstar) / (f * dz * 0.5 + vstar) if vstar > 0 else 0.0
+            assert abs(got[scheme] - want) <= 1e-12 * max(want, 1e-300), (ustar, scheme, got[scheme], want)
+        if ustar <= f * bld:
+            assert got[2] == 0.0

@@ -40,9 +40,9 @@ def ks_config(**over):
 
     c = default_config()
     c.kappa_shear = 1
-    c.ks_eos = 1
-    c.ks_alpha_t = ALPHA
-    c.ks_beta_s = BETA
+    c.eos_variant = 1
+    c.eos_alpha_t = ALPHA
+    c.eos_beta_s = BETA
     c.rho0 = RHO0
     for k, v in over.items():
         setattr(c, k, v)

@@ -1,4 +1,4 @@
-"""The oracle's port of rdb_sm_cbrt / rdb_sm_atan / rdb_sm_exp against the reference's
+"""The oracle's port of rdb_sm_cbrt / rdb_sm_atan / rdb_sm_exp / rdb_sm_log against the reference's
 golden bit patterns (tests/test_safe_math_golden.inc, transcribed into
 tests/golden/safe_math_golden.json)."""
 import json
@@ -18,9 +18,9 @@ def d2h(x):
     return struct.pack(">d", x).hex().upper()
 
 
-@pytest.mark.parametrize("fn", ["cbrt", "atan", "exp"])
+@pytest.mark.parametrize("fn", ["cbrt", "atan", "exp", "log"])
 def test_golden_bits(oracle, fn):
-    f = {"cbrt": oracle.sm_cbrt, "atan": oracle.sm_atan, "exp": oracle.sm_exp}[fn]
+    f = {"cbrt": oracle.sm_cbrt, "atan": oracle.sm_atan, "exp": oracle.sm_exp, "log": oracle.sm_log}[fn]
     bad = []
     for arg, res in GOLD[fn]:
         got = d2h(f(h2d(arg)))
