@@ -11,7 +11,8 @@
  * test_ocean_vmix_assembly.F90, test_ocean_bkgnd_mixing.F90,
  * test_ocean_kpp_nonlocal.F90) re-expressed in tests/test_oracle_*.py;
  * kappa-shear (vphys_oracle_kshear.c) against the reference's golden kd
- * profile (tests/test_ocean_kappa_shear.F90:286-393, 1e-6 relative).
+ * profile (tests/test_ocean_kappa_shear.F90:286-393, 1e-6 relative); EPBL
+ * (vphys_oracle_epbl.c) against the physical tests of test_ocean_epbl.F90.
  * The Fortran reference itself cannot be compiled here (no Fortran
  * compiler), so bitwise parity with its binary output is unpinned.
  *
