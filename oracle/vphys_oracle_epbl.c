@@ -6,9 +6,10 @@
  * Built scope: the mstar schemes "constant" and "om4", the cube-root and
  * RH18 velocity scales, the MLD iteration (false position / bisection,
  * optionally seeded by the previous MLD), the mixing-length shape with
- * exponent 2, and the three merges (add, max, max_shear).  The penetrating
- * shortwave TKE ledger, Langmuir enhancement, the RH18 mstar fit and the TKE
- * budget diagnostics are not restated (the library refuses them).
+ * exponent 2, the two-band penetrating-shortwave TKE ledger (on whenever
+ * sw_pen_frac != 0, source Q_heat, bed row k_bot = 1), and the three merges
+ * (add, max, max_shear).  Langmuir enhancement, the RH18 mstar fit and the
+ * TKE budget diagnostics are not restated (the library refuses them).
  *
  * Parity pins: the analytic and structural tests of the reference's
  * tests/test_ocean_epbl.F90 re-expressed in tests/test_oracle_epbl.py, and
@@ -95,6 +96,16 @@ static double find_mstar(const vphys_config *c, double b0, double ustar, double 
     return mstar;
 }
 
+/* sw_pe_cost_shape (rdb_ocean_surface_flux.F90:1417-1449): the fraction of
+ * the skin PE cost that homogenising an exponentially distributed in-layer
+ * heating of optical depth tau incurs; Taylor branch below tau = 1e-2. */
+static double sw_pe_cost_shape(double tau)
+{
+    if (tau <= 1.0e-2) return (1.0 / 6.0) * tau * (1.0 - (1.0 / 60.0) * tau * tau);
+    const double em1 = 1.0 - vpo_sm_exp(-tau);
+    return (tau * (1.0 + vpo_sm_exp(-tau)) - 2.0 * em1) / (tau * em1);
+}
+
 /* epbl_mixlen_shape (:690-714), exponent 2 */
 static double mixlen_shape(const vphys_config *c, double z_depth, double mld_guess)
 {
@@ -150,8 +161,13 @@ void vpo_epbl(const vphys_config *c, vpo_state *s, double dt)
     for (int j = 1; j <= ny; ++j) {
         for (int i = 1; i <= nx; ++i) {
             const int n = nz + 2;
-            double t0[n], s0[n], dpe_t[n], dpe_s[n], dch_t[n], dch_s[n];
+            double t0[n], s0[n], dpe_t[n], dpe_s[n], dch_t[n], dch_s[n], ctke_sw[n];
             const int k_sfc = first_live(s->h, nx, ny, i, j, nz);
+            /* the penetrating-shortwave ledger (:1095-1185): irradiance I0 and the
+             * running depth of the layer top below the live surface */
+            const int sw_on = c->sw_pen_frac != 0.0;
+            const double i0_col = sw_on ? c->sw_pen_frac * C2(s->q_heat, i, j) * C2(s->wet, i, j) : 0.0;
+            double d_top_sw = 0.0, e1_top = 1.0, e2_top = 1.0;
             /* ---- column prep: T0, S0 and the pressure-weighted weights (downward) */
             double pres = 0.0, h_sum = 0.0, dsv_dt_sfc = 0.0, dsv_ds_sfc = 0.0;
             for (int k = nz; k >= 1; --k) {
@@ -172,6 +188,30 @@ void vpo_epbl(const vphys_config *c, vpo_state *s, double dt)
                 dpe_s[k] = dmass * p_mid * dsv_ds_k;
                 dch_t[k] = dmass * dsv_dt_k;
                 dch_s[k] = dmass * dsv_ds_k;
+                if (k > k_sfc) {
+                    ctke_sw[k] = 0.0;   /* dead layers above the live surface take no light */
+                } else if (sw_on) {
+                    /* absorbed heat per band, difference form, opaque bed at k = 1 */
+                    const double d_bot_sw = d_top_sw + hk;
+                    double heat_sw1, heat_sw2;
+                    if (k > 1) {
+                        const double e1_bot = vpo_sm_exp(-d_bot_sw / c->sw_zeta1);
+                        const double e2_bot = vpo_sm_exp(-d_bot_sw / c->sw_zeta2);
+                        heat_sw1 = i0_col * c->sw_band_ratio * inv_rho0_cp * dt * (e1_top - e1_bot);
+                        heat_sw2 = i0_col * (1.0 - c->sw_band_ratio) * inv_rho0_cp * dt * (e2_top - e2_bot);
+                        e1_top = e1_bot;
+                        e2_top = e2_bot;
+                    } else {
+                        heat_sw1 = i0_col * c->sw_band_ratio * inv_rho0_cp * dt * e1_top;
+                        heat_sw2 = i0_col * (1.0 - c->sw_band_ratio) * inv_rho0_cp * dt * e2_top;
+                    }
+                    ctke_sw[k] = -0.5 * GRAVITY * rho0 * dch_t[k] *
+                                 (heat_sw1 * sw_pe_cost_shape(hk / c->sw_zeta1) +
+                                  heat_sw2 * sw_pe_cost_shape(hk / c->sw_zeta2));
+                    d_top_sw = d_bot_sw;
+                } else {
+                    ctke_sw[k] = 0.0;
+                }
                 if (k == k_sfc) {
                     dsv_dt_sfc = dsv_dt_k;
                     dsv_ds_sfc = dsv_ds_k;
@@ -188,8 +228,17 @@ void vpo_epbl(const vphys_config *c, vpo_state *s, double dt)
             const double q_s_kin = inv_rho0 * C2(s->q_salt, i, j);
             const double b0 = GRAVITY * rho0 * (dsv_dt_sfc * q_t_kin + dsv_ds_sfc * q_s_kin);
             const double h_top = C3(s->h, i, j, k_sfc);
-            const double ctke_sfc =
-                -0.5 * GRAVITY * (rho0 * rho0) * h_top * (q_t_kin * dt * dsv_dt_sfc + q_s_kin * dt * dsv_ds_sfc);
+            double ctke_sfc;
+            if (sw_on) {
+                /* the skin carries only the non-penetrating heat; the shortwave
+                 * absorbed in the surface layer is its own ledger entry */
+                const double q_nonpen_kin = inv_rho0_cp * (C2(s->q_heat, i, j) - i0_col);
+                ctke_sfc = -0.5 * GRAVITY * (rho0 * rho0) * h_top *
+                               (q_nonpen_kin * dt * dsv_dt_sfc + q_s_kin * dt * dsv_ds_sfc) +
+                           ctke_sw[k_sfc];
+            } else {
+                ctke_sfc = -0.5 * GRAVITY * (rho0 * rho0) * h_top * (q_t_kin * dt * dsv_dt_sfc + q_s_kin * dt * dsv_ds_sfc);
+            }
             const double ustar = fmx(sqrt(C2(s->stress_mag, i, j) / rho0), c->epbl_ustar_min);
             const double f = s->coriolis ? C2(s->coriolis, i, j) : 0.0;
             const double absf = sqrt((1.0 - c->epbl_omega_frac) * (f * f) +
@@ -241,6 +290,13 @@ void vpo_epbl(const vphys_config *c, vpo_state *s, double dt)
                         /* (1) mechanical TKE decays across the layer above */
                         const double exp_kh = vpo_sm_exp(-h_ka * idecay);
                         mech_tke = mech_tke * exp_kh;
+                        /* (2) the layer below accrues its shortwave cost: a release
+                         * (> 0) joins the convective reservoir */
+                        double ctke_sw_kb = 0.0;
+                        if (sw_on) {
+                            ctke_sw_kb = ctke_sw[kb];
+                            if (ctke_sw_kb > 0.0) conv_perel = conv_perel + ctke_sw_kb;
+                        }
                         /* (3) rotation-reduced convective efficiency */
                         double nstar_fc = c->epbl_nstar;
                         if (conv_perel > 0.0 && absf > 0.0) {
@@ -249,6 +305,20 @@ void vpo_epbl(const vphys_config *c, vpo_state *s, double dt)
                                        (conv_perel + 0.2 * sqrt(0.5 * dt * rho0 * (ah * ah * ah) * conv_perel));
                         }
                         double tot_tke = mech_tke + nstar_fc * conv_perel;
+                        /* (3b) a shortwave sink (< 0) is paid first, both reservoirs
+                         * drained in proportion */
+                        if (sw_on && ctke_sw_kb < 0.0) {
+                            if (ctke_sw_kb + tot_tke < 0.0) {
+                                tot_tke = 0.0;
+                                mech_tke = 0.0;
+                                conv_perel = 0.0;
+                            } else {
+                                const double r_sw = (tot_tke + ctke_sw_kb) / tot_tke;
+                                tot_tke = r_sw * tot_tke;
+                                mech_tke = r_sw * mech_tke;
+                                conv_perel = r_sw * conv_perel;
+                            }
+                        }
                         double kd_val;
                         /* (5) static-stability short-circuit */
                         if (tot_tke <= 0.0 && 0.0 <= (dch_t[kb] + dch_t[ka]) * (t0[ka] - t0[kb]) +

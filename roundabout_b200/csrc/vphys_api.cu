@@ -274,8 +274,6 @@ int validate(const vphys_config *c, int ntr)
             return push_error(VPHYS_ERR_CONFIG, "epbl_combine must be 1 (add), 2 (max) or 3 (max_shear)");
         if (c->epbl_mixlen_exponent != 2.0)
             return push_error(VPHYS_ERR_CONFIG, "epbl_mixlen_exponent other than 2 is not built");
-        if (c->sw_pen_frac != 0.0)
-            return push_error(VPHYS_ERR_CONFIG, "EPBL's penetrating-shortwave TKE ledger is not built: sw_pen_frac must be 0");
         if (c->learned_kpp) return push_error(VPHYS_ERR_CONFIG, "EPBL replaces KPP: learned_kpp must be 0");
         if (c->epbl_mld_max_its < 1 || c->epbl_mld_max_its > 1000)
             return push_error(VPHYS_ERR_CONFIG, "epbl_mld_max_its must be in [1, 1000]");

@@ -10,8 +10,11 @@
 // mixed-layer-depth iterations, each a downward sweep that spends the
 // wind and convective TKE on the largest diffusivity each interface can
 // afford (closed-form energy solve with an embedded forward elimination) and
-// moves the MLD guess (false position with a bisection fallback).  The
-// column's eight per-layer arrays (h and the prep weights, 1-based,
+// moves the MLD guess (false position with a bisection fallback).  With
+// shortwave penetration on (sw_pen_frac != 0) the prep also costs each
+// layer's absorbed two-band heat (the TKE ledger of :1095-1185, opaque bed
+// row k_bot = 1) and the sweep pays it (:1373-1425).  The column's nine
+// per-layer arrays (h, the prep weights and the shortwave cost, 1-based,
 // bottom-up as the reference stores them) live in the thread's local memory,
 // sized by a compile-time bucket of nz.  Every value is formed by the same
 // operations in the same order as the reference; built with -fmad=false it
@@ -76,6 +79,16 @@ __device__ __forceinline__ double find_mstar(const vphys_config &c, double b0, d
     return mstar;
 }
 
+// sw_pe_cost_shape (rdb_ocean_surface_flux.F90:1417-1449): the share of the
+// skin PE cost that homogenising an exponential in-layer heating of optical
+// depth tau incurs; Taylor branch below tau = 1e-2
+__device__ __forceinline__ double sw_pe_cost_shape(double tau)
+{
+    if (tau <= 1.0e-2) return (1.0 / 6.0) * tau * (1.0 - (1.0 / 60.0) * tau * tau);
+    const double em1 = 1.0 - sm_exp(-tau);
+    return xdiv(tau * (1.0 + sm_exp(-tau)) - 2.0 * em1, tau * em1);
+}
+
 // the turbulent velocity scale (cube root of the TKE rate, or RH18)
 __device__ __forceinline__ double vstar_of(const vphys_config &c, double tke_here, double conv_perel, double ustar,
                                            double htot, double mld_guess, double dt)
@@ -111,7 +124,10 @@ __global__ void __launch_bounds__(128, 4) k_epbl(const Params p, double dt, doub
     const double *T = p.tr[c.idx_temperature] + col;
     const double *S = p.tr[c.idx_salinity] + col;
 
-    double h[N], t0[N], s0[N], dpe_t[N], dpe_s[N], dch_t[N], dch_s[N], kd[N];
+    double h[N], t0[N], s0[N], dpe_t[N], dpe_s[N], dch_t[N], dch_s[N], kd[N], ctke_sw[N];
+    const bool sw_on = c.sw_pen_frac != 0.0;
+    const double i0_col = sw_on ? c.sw_pen_frac * p.q_heat[col] * p.wet[col] : 0.0;
+    double d_top_sw = 0.0, e1_top = 1.0, e2_top = 1.0;
     int k_sfc = nz;   // first live layer from the top (nz when none is live)
     for (int k = nz; k >= 1; --k) {
         h[k] = p.h[col + P * (size_t)(k - 1)];
@@ -141,6 +157,27 @@ __global__ void __launch_bounds__(128, 4) k_epbl(const Params p, double dt, doub
         dpe_s[k] = dmass * p_mid * dsv_ds_k;
         dch_t[k] = dmass * dsv_dt_k;
         dch_s[k] = dmass * dsv_ds_k;
+        if (k > k_sfc || !sw_on) {
+            ctke_sw[k] = 0.0;   // dead layers above the live surface take no light
+        } else {
+            const double d_bot_sw = d_top_sw + hk;
+            double heat_sw1, heat_sw2;
+            if (k > 1) {
+                const double e1_bot = sm_exp(xdiv(-d_bot_sw, c.sw_zeta1));
+                const double e2_bot = sm_exp(xdiv(-d_bot_sw, c.sw_zeta2));
+                heat_sw1 = i0_col * c.sw_band_ratio * inv_rho0_cp * dt * (e1_top - e1_bot);
+                heat_sw2 = i0_col * (1.0 - c.sw_band_ratio) * inv_rho0_cp * dt * (e2_top - e2_bot);
+                e1_top = e1_bot;
+                e2_top = e2_bot;
+            } else {   // opaque bed: the rest of the light
+                heat_sw1 = i0_col * c.sw_band_ratio * inv_rho0_cp * dt * e1_top;
+                heat_sw2 = i0_col * (1.0 - c.sw_band_ratio) * inv_rho0_cp * dt * e2_top;
+            }
+            ctke_sw[k] = -0.5 * GRAVITY * rho0 * dch_t[k] *
+                         (heat_sw1 * sw_pe_cost_shape(xdiv(hk, c.sw_zeta1)) +
+                          heat_sw2 * sw_pe_cost_shape(xdiv(hk, c.sw_zeta2)));
+            d_top_sw = d_bot_sw;
+        }
         if (k == k_sfc) {
             dsv_dt_sfc = dsv_dt_k;
             dsv_ds_sfc = dsv_ds_k;
@@ -156,8 +193,11 @@ __global__ void __launch_bounds__(128, 4) k_epbl(const Params p, double dt, doub
     const double q_t_kin = inv_rho0_cp * p.q_heat[col];
     const double q_s_kin = inv_rho0 * p.q_salt[col];
     const double b0 = g_rho0 * (dsv_dt_sfc * q_t_kin + dsv_ds_sfc * q_s_kin);
-    const double ctke_sfc =
-        -0.5 * GRAVITY * (rho0 * rho0) * h[k_sfc] * (q_t_kin * dt * dsv_dt_sfc + q_s_kin * dt * dsv_ds_sfc);
+    // the skin carries the non-penetrating heat when the shortwave is charged per layer
+    const double q_skin_kin = sw_on ? inv_rho0_cp * (p.q_heat[col] - i0_col) : q_t_kin;
+    double ctke_sfc =
+        -0.5 * GRAVITY * (rho0 * rho0) * h[k_sfc] * (q_skin_kin * dt * dsv_dt_sfc + q_s_kin * dt * dsv_ds_sfc);
+    if (sw_on) ctke_sfc = ctke_sfc + ctke_sw[k_sfc];
     const double ustar = fmx(sqrt(xdiv(p.stress_mag[col], rho0)), c.epbl_ustar_min);
     const double f = p.coriolis ? p.coriolis[col] : 0.0;
     const double absf = sqrt((1.0 - c.epbl_omega_frac) * (f * f) + c.epbl_omega_frac * 4.0 * (c.epbl_omega * c.epbl_omega));
@@ -199,6 +239,9 @@ __global__ void __launch_bounds__(128, 4) k_epbl(const Params p, double dt, doub
                 const double h_kb = h[kb] + H_NEGLECT;
                 bool sfc_disconnect = false;
                 mech_tke = mech_tke * sm_exp(-h_ka * idecay);
+                // the layer below accrues its shortwave cost; a release joins the convective reservoir
+                const double ctke_sw_kb = ctke_sw[kb];
+                if (ctke_sw_kb > 0.0) conv_perel = conv_perel + ctke_sw_kb;
                 double nstar_fc = c.epbl_nstar;
                 if (conv_perel > 0.0 && absf > 0.0) {
                     const double ah = absf * htot;
@@ -206,6 +249,19 @@ __global__ void __launch_bounds__(128, 4) k_epbl(const Params p, double dt, doub
                                     conv_perel + 0.2 * sqrt(0.5 * dt * rho0 * (ah * ah * ah) * conv_perel));
                 }
                 double tot_tke = mech_tke + nstar_fc * conv_perel;
+                // a shortwave sink is paid first, both reservoirs drained in proportion
+                if (ctke_sw_kb < 0.0) {
+                    if (ctke_sw_kb + tot_tke < 0.0) {
+                        tot_tke = 0.0;
+                        mech_tke = 0.0;
+                        conv_perel = 0.0;
+                    } else {
+                        const double r_sw = xdiv(tot_tke + ctke_sw_kb, tot_tke);
+                        tot_tke = r_sw * tot_tke;
+                        mech_tke = r_sw * mech_tke;
+                        conv_perel = r_sw * conv_perel;
+                    }
+                }
                 double kd_val;
                 if (tot_tke <= 0.0 &&
                     0.0 <= (dch_t[kb] + dch_t[ka]) * (t0[ka] - t0[kb]) + (dch_s[kb] + dch_s[ka]) * (s0[ka] - s0[kb])) {

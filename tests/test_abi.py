@@ -105,7 +105,7 @@ def test_epbl_knobs_are_validated(lib):
     from roundabout_b200.config import EPBL, default_config
 
     h = ctypes.c_void_p()
-    for over in (dict(epbl_mstar_scheme=3), dict(epbl_mixlen_exponent=1.5), dict(sw_pen_frac=0.5),
+    for over in (dict(epbl_mstar_scheme=3), dict(epbl_mixlen_exponent=1.5),
                  dict(learned_kpp=1), dict(epbl_combine=4), dict(epbl_mld_max_its=0), dict(epbl_ustar_min=0.0)):
         bad = default_config()
         bad.epbl = 1

@@ -4,8 +4,9 @@ vphys_step with epbl = 1) with the CPU oracle.
 The column solve is epbl_compute -> epbl_column_kernel
 (rdb_ocean_epbl.F90:864-1659): bitwise on kd_epbl and mld_epbl for the
 OM4 and constant mstar, both velocity scales, the MLD iteration with false
-position, bisection, the previous-MLD seed or none, both EOS variants, nz
-from 1 to 100, vanished top layers and land; the merges (add, max,
+position, bisection, the previous-MLD seed or none, both EOS variants, the
+penetrating-shortwave TKE ledger, nz from 1 to 100, vanished top layers and
+land; the merges (add, max,
 max_shear with kappa-shear) bitwise through the assembly and whole steps,
 with convection masked below EPBL's MLD; the mixed step within 1e-6.
 """
@@ -41,6 +42,9 @@ KNOBS = {
                               epbl_vstar_scheme=2, epbl_mstar_conv_adj=0.5, epbl_omega_frac=0.3),
     "no_iteration": dict(epbl_mld_iteration=0, epbl_mstar_cap=0.8, epbl_min_mix_len=0.5),
     "bisection_prev": dict(epbl_mld_bisection=1, epbl_mld_use_prev_guess=1, epbl_mld_max_its=7),
+    "shortwave": dict(sw_pen_frac=0.6),
+    "shortwave_linear": dict(epbl_mstar_scheme=1, sw_pen_frac=1.0, eos_variant=1, eos_alpha_t=0.2, eos_beta_s=0.77,
+                             sw_zeta1=1.5, sw_zeta2=9.0),
 }
 
 
@@ -101,11 +105,11 @@ def test_assemble_merges_epbl(VP, oracle, combine, shear):
     assert (st.bl_depth == 0.0).all()          # KPP did not run
 
 
-@pytest.mark.parametrize("shear", [0, 1])
-def test_step_with_epbl(VP, oracle, shear):
+@pytest.mark.parametrize("shear,sw", [(0, 0), (1, 0), (0, 1)])
+def test_step_with_epbl(VP, oracle, shear, sw):
     cols = columns(nx=30, ny=18, nz=24, seed=62, thin_frac=0.1)
     cfg = hot_cfg(epbl=1, budgets=1, surface_flux=1, kappa_shear=shear, epbl_combine=3 if shear else 1,
-                  epbl_mld_use_prev_guess=1, conv_enable=1)
+                  epbl_mld_use_prev_guess=1, conv_enable=1, sw_pen_frac=0.5 if sw else 0.0)
     st, vp = setup(VP, oracle, cols, cfg)
     assert st.call("vpo_step", cfg, DT, 3) == 0
     vp.step(DT, 3)

@@ -163,3 +163,25 @@ def test_om4_mstar_closed_form(oracle):
             assert abs(got[scheme] - want) <= 1e-12 * max(want, 1e-300), (ustar, scheme, got[scheme], want)
         if ustar <= f * bld:
             assert got[2] == 0.0
+
+
+def test_shortwave_ledger_limits(oracle):
+    """The penetrating-shortwave TKE ledger (rdb_ocean_epbl.F90:1095-1185,
+    1373-1425): with no irradiance (Q_heat = 0) it changes nothing, bit for
+    bit; under surface heating, charging the penetrating part per layer
+    through Phi <= 1 costs less than heating the skin with all of it, so the
+    mixed layer is at least as deep."""
+    nz, dz, dt = 40, 2.0, 1800.0
+    dtdz = 1.0e-5 * RHO0 / (G * ALPHA_LIN)
+    out = {}
+    for q, frac in ((0.0, 0.0), (0.0, 0.6), (300.0, 0.0), (300.0, 0.6)):
+        cfg = epbl_config(sw_pen_frac=frac)
+        st = stratified(oracle, nz, dz, 15.0, dtdz)
+        st.stress_mag[...] = RHO0 * 0.01 ** 2
+        st.q_heat[...] = q
+        st.call("vpo_epbl", cfg, dt)
+        out[(q, frac)] = (st.kd_epbl.copy(), float(st.mld_epbl[0, 0]))
+    assert np.array_equal(out[(0.0, 0.0)][0], out[(0.0, 0.6)][0])
+    assert out[(0.0, 0.0)][1] == out[(0.0, 0.6)][1]
+    assert out[(300.0, 0.6)][1] >= out[(300.0, 0.0)][1], (out[(300.0, 0.6)][1], out[(300.0, 0.0)][1])
+    assert out[(300.0, 0.6)][1] > out[(300.0, 0.0)][1] or not np.array_equal(out[(300.0, 0.6)][0], out[(300.0, 0.0)][0])
