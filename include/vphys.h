@@ -202,10 +202,11 @@ typedef struct vphys_config {
      * (rdb_ocean_dyn.F90:1539): vphys_step refreshes KD_EPBL and MLD_EPBL
      * once a step (vphys_epbl, epbl_compute) and every assembly merges
      * KD_EPBL into kt and epbl_prandtl * KD_EPBL into kv (epbl_combine);
-     * convection then masks below MLD_EPBL.  Not built (refused): the
-     * penetrating-shortwave TKE ledger (sw_pen_frac != 0), Langmuir
-     * enhancement, the RH18 mstar fit and a mixing-length exponent other
-     * than 2. */
+     * convection then masks below MLD_EPBL.  With sw_pen_frac != 0 the
+     * two-band shortwave absorbed in each layer is charged to the TKE budget
+     * (the reference's epbl_sw_ctke ledger, source Q_HEAT).  Not built
+     * (refused): Langmuir enhancement, the RH18 mstar fit and a
+     * mixing-length exponent other than 2. */
     int epbl;                 /* 0 */
     int epbl_mstar_scheme;    /* 1 constant, 2 OM4 (default) */
     int epbl_vstar_scheme;    /* 1 cube root (default), 2 RH18 */
