@@ -204,11 +204,10 @@ typedef struct vphys_config {
      * KD_EPBL into kt and epbl_prandtl * KD_EPBL into kv (epbl_combine);
      * convection then masks below MLD_EPBL.  With sw_pen_frac != 0 the
      * two-band shortwave absorbed in each layer is charged to the TKE budget
-     * (the reference's epbl_sw_ctke ledger, source Q_HEAT).  Not built
-     * (refused): Langmuir enhancement, the RH18 mstar fit and a
-     * mixing-length exponent other than 2. */
+     * (the reference's epbl_sw_ctke ledger, source Q_HEAT).  Not built:
+     * Langmuir enhancement. */
     int epbl;                 /* 0 */
-    int epbl_mstar_scheme;    /* 1 constant, 2 OM4 (default) */
+    int epbl_mstar_scheme;    /* 1 constant, 2 OM4 (default), 3 RH18 */
     int epbl_vstar_scheme;    /* 1 cube root (default), 2 RH18 */
     int epbl_combine;         /* 1 add (default), 2 max, 3 max_shear (needs kappa_shear: shear merged first) */
     int epbl_mld_iteration;   /* 1 */
@@ -235,6 +234,13 @@ typedef struct vphys_config {
     double epbl_omega_frac;   /* 0 */
     double epbl_ustar_min;    /* 1e-8 m/s */
     double epbl_prandtl;      /* 1 */
+    /* RH18 mstar fit (epbl_mstar_scheme 3): mstar = cn1 e/(1+e) with
+     * e = cn2 exp(cn3 BLD |f|/u*), plus cs1 (B0+^2 BLD/(u*^5 |f|))^cs2 */
+    double epbl_rh18_cn1;     /* 0.275 */
+    double epbl_rh18_cn2;     /* 8 */
+    double epbl_rh18_cn3;     /* -5 */
+    double epbl_rh18_cs1;     /* 0.2 */
+    double epbl_rh18_cs2;     /* 0.4 */
 } vphys_config;
 
 #define VPHYS_KPP_SW_ALL 1

@@ -58,6 +58,8 @@ def lib():
         L.vpo_sm_exp.argtypes = [ctypes.c_double]
         L.vpo_sm_log.restype = ctypes.c_double
         L.vpo_sm_log.argtypes = [ctypes.c_double]
+        L.vpo_sm_pow.restype = ctypes.c_double
+        L.vpo_sm_pow.argtypes = [ctypes.c_double, ctypes.c_double]
         L.vpo_set_threads.argtypes = [ctypes.c_int]
         L.vpo_get_threads.restype = ctypes.c_int
         for name in ("vpo_eos_wright", "vpo_pp81", "vpo_seed_interior_none", "vpo_kpp_overlay",
@@ -189,6 +191,10 @@ def sm_exp(x: float) -> float:
 
 def sm_log(x: float) -> float:
     return lib().vpo_sm_log(float(x))
+
+
+def sm_pow(x: float, y: float) -> float:
+    return lib().vpo_sm_pow(float(x), float(y))
 
 
 def eos_buoyancy_coeffs(T: float, S: float, p: float):

@@ -87,21 +87,29 @@ static const double SM_EXP_C[14] = {1.0,           1.0,              1.0 / 2.0, 
                                     1.0 / 40320.0, 1.0 / 362880.0,   1.0 / 3628800.0,   1.0 / 39916800.0,
                                     1.0 / 479001600.0, 1.0 / 6227020800.0};
 
-double vpo_sm_exp(double x)
+/* rdb_sm_exp_core (rdb_safe_math_core.inc:81-114): exp(x + c) for finite x
+ * in range and a small correction c added to the reduced argument (0 for
+ * plain exp; the tail of a double-double exponent for pow). */
+static double sm_exp_core(double x, double c)
 {
-    if (isnan(x)) return x;
-    if (x > SM_EXP_MAX) return INFINITY;
-    if (x < SM_EXP_MIN) return 0.0;
     double kr = round(x * SM_INV_LN2);
     int k = (int)kr;
     double r = x - kr * SM_LN2_HI;
     r = r - kr * SM_LN2_LO;
-    r = r + 0.0;
+    r = r + c;
     double p = SM_EXP_C[13];
     for (int i = 12; i >= 0; --i) p = p * r + SM_EXP_C[i];
     double y = (k > 1000) ? 2.0 * ldexp(p, k - 1) : ldexp(p, k);
     if (y < DBL_MIN) y = 0.0;
     return y;
+}
+
+double vpo_sm_exp(double x)
+{
+    if (isnan(x)) return x;
+    if (x > SM_EXP_MAX) return INFINITY;
+    if (x < SM_EXP_MIN) return 0.0;
+    return sm_exp_core(x, 0.0);
 }
 
 /* rdb_sm_log (rdb_safe_math_core.inc:139-206): x = m 2^k with m in
@@ -140,6 +148,137 @@ double vpo_sm_log(double x)
     const double s = kr * SM_LN2_HI + 2.0 * f;
     const double w = (2.0 * f) * u * p + kr * SM_LN2_LO;
     return s + w;
+}
+
+/* Knuth's exact sum and Dekker's exact product without FMA (Veltkamp split
+ * by 2^27 + 1): s + e == a + b, p + e == a * b (rdb_safe_math_core.inc:53-79). */
+static const double SM_SPLIT = 134217729.0;
+static void sm_two_sum(double a, double b, double *s, double *e)
+{
+    *s = a + b;
+    const double bb = *s - a;
+    *e = (a - (*s - bb)) + (b - bb);
+}
+static void sm_two_prod(double a, double b, double *p, double *e)
+{
+    double c = SM_SPLIT * a;
+    const double ah = c - (c - a);
+    const double al = a - ah;
+    c = SM_SPLIT * b;
+    const double bh = c - (c - b);
+    const double bl = b - bh;
+    *p = a * b;
+    *e = (((ah * bh - *p) + ah * bl) + al * bh) + al * bl;
+}
+
+/* rdb_sm_log_dd (rdb_safe_math_core.inc:208-249): log x as head + tail, the
+ * quotient f = (m-1)/(m+1) carried to ~106 bits so y log x keeps its bits. */
+static void sm_log_dd(double x, double *lh, double *ll)
+{
+    if (x < DBL_MIN && x * SM_TWO54 == 0.0) {
+        *lh = -INFINITY;
+        *ll = 0.0;
+        return;
+    }
+    double xs = x;
+    int kadj = 0;
+    if (x < DBL_MIN) {
+        xs = x * SM_TWO54;
+        kadj = -54;
+    }
+    int e;
+    double m = frexp(xs, &e);
+    int k = e + kadj;
+    if (m < SM_SQRT_HALF) {
+        m = 2.0 * m;
+        k = k - 1;
+    }
+    const double a = m - 1.0;
+    double bh, bl;
+    sm_two_sum(m, 1.0, &bh, &bl);
+    const double q1 = a / bh;
+    double p1, p2;
+    sm_two_prod(q1, bh, &p1, &p2);
+    const double rr = ((a - p1) - p2) - q1 * bl;
+    const double q2 = rr / bh;
+    const double fh = q1 + q2;
+    const double fl = q2 - (fh - q1);
+    const double u = fh * fh;
+    double p = SM_LOG_C[9];
+    for (int i = 8; i >= 1; --i) p = p * u + SM_LOG_C[i];
+    const double tail = (2.0 * fh) * u * p;
+    const double kr = (double)k;
+    double ss, ee;
+    sm_two_sum(kr * SM_LN2_HI, 2.0 * fh, &ss, &ee);
+    *lh = ss;
+    *ll = ee + ((2.0 * fl + tail) + kr * SM_LN2_LO);
+}
+
+/* rdb_sm_pow (rdb_safe_math_pow.inc:6-105): the C99 pow special values
+ * except that a NaN anywhere gives NaN; for finite x > 0 exp(y log x) with
+ * the log as head + tail and y*log x formed exactly (Dekker 1971). */
+double vpo_sm_pow(double x, double y)
+{
+    if (isnan(x) || isnan(y)) return NAN;
+    if (y == 0.0 || x == 1.0) return 1.0;
+    const double ax = fabs(x), ay = fabs(y);
+    int yint, yodd;
+    if (isfinite(y)) {
+        if (ay >= 9007199254740992.0) {
+            yint = 1;
+            yodd = 0;
+        } else {
+            yint = (ay == round(ay));
+            const double h = 0.5 * ay;
+            yodd = yint && (h != round(h));
+        }
+    } else {
+        yint = 0;
+        yodd = 0;
+    }
+    const int xneg = (x < 0.0) || (x == 0.0 && signbit(x));
+    double r;
+    if (!isfinite(y)) {
+        if (ax == 1.0)
+            r = 1.0;
+        else if ((ax < 1.0) == (y > 0.0))
+            r = 0.0;
+        else
+            r = INFINITY;
+        return r;
+    }
+    if (ax == 0.0) {
+        r = (y > 0.0) ? 0.0 : INFINITY;
+        if (xneg && yodd) r = -r;
+        return r;
+    }
+    if (!isfinite(x)) {
+        r = (y > 0.0) ? INFINITY : 0.0;
+        if (xneg && yodd) r = -r;
+        return r;
+    }
+    if (xneg && !yint) return NAN;
+    double lh, ll;
+    sm_log_dd(ax, &lh, &ll);
+    const double t = y * lh;
+    if (t > 800.0) {
+        r = INFINITY;
+    } else if (t < -800.0) {
+        r = 0.0;
+    } else {
+        double ph, pl, ee, c2;
+        sm_two_prod(y, lh, &ph, &pl);
+        const double c = pl + y * ll;
+        sm_two_sum(ph, c, &ee, &c2);
+        if (ee > SM_EXP_MAX)
+            r = INFINITY;
+        else if (ee < SM_EXP_MIN)
+            r = 0.0;
+        else
+            r = sm_exp_core(ee, c2);
+    }
+    if (xneg && yodd) r = -r;
+    return r;
 }
 
 static inline double sm_flush(double r)

@@ -73,6 +73,7 @@ void vpo_surface_flux(const vphys_config *c, vpo_state *s, double dt);
 void vpo_eos_buoyancy_coeffs(double T, double S, double p, double *alpha_T, double *beta_S);
 double vpo_sm_exp(double x);
 double vpo_sm_log(double x);
+double vpo_sm_pow(double x, double y);
 void vpo_sw_penetration(const vphys_config *c, vpo_state *s, double dt);
 
 /* kappa-shear, column form (vphys_oracle_kshear.c) */

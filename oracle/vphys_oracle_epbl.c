@@ -3,13 +3,12 @@
  * restatement of src/parameterizations/vertical/rdb_ocean_epbl.F90.
  *
  * TEST INFRASTRUCTURE ONLY: the checker of vphys_epbl (see vphys_oracle.h).
- * Built scope: the mstar schemes "constant" and "om4", the cube-root and
- * RH18 velocity scales, the MLD iteration (false position / bisection,
- * optionally seeded by the previous MLD), the mixing-length shape with
- * exponent 2, the two-band penetrating-shortwave TKE ledger (on whenever
+ * Built scope: the mstar schemes "constant", "om4" and "rh18", the cube-root
+ * and RH18 velocity scales, the MLD iteration (false position / bisection,
+ * optionally seeded by the previous MLD), the mixing-length shape, the two-band penetrating-shortwave TKE ledger (on whenever
  * sw_pen_frac != 0, source Q_heat, bed row k_bot = 1), and the three merges
- * (add, max, max_shear).  Langmuir enhancement, the RH18 mstar fit and the
- * TKE budget diagnostics are not restated (the library refuses them).
+ * (add, max, max_shear).  Langmuir enhancement and the TKE budget
+ * diagnostics are not restated (the library has neither).
  *
  * Parity pins: the analytic and structural tests of the reference's
  * tests/test_ocean_epbl.F90 re-expressed in tests/test_oracle_epbl.py, and
@@ -70,7 +69,7 @@ static void specvol_derivs(const vphys_config *c, double T, double S, double pre
     *dsv_ds = W_A2 + dlam_ds * inv_p - lambda * dp0_ds * inv_p2;
 }
 
-/* epbl_find_mstar (rdb_ocean_epbl.F90:630-688), schemes constant and om4 */
+/* epbl_find_mstar (rdb_ocean_epbl.F90:630-688): constant, OM4, RH18 */
 static double find_mstar(const vphys_config *c, double b0, double ustar, double bld, double absf)
 {
     double mstar;
@@ -81,6 +80,14 @@ static double find_mstar(const vphys_config *c, double b0, double ustar, double 
         if (ustar > absf_floor * bld)
             mstar_n = c->epbl_c_ek * vpo_sm_log(ustar / (absf_floor * fmx(bld, 1.0e-10)));
         mstar = fmx(mstar_s, fmn(1.25, mstar_n));
+        if (c->epbl_mstar_cap > 0.0) mstar = fmn(c->epbl_mstar_cap, mstar);
+    } else if (c->epbl_mstar_scheme == 3) {
+        const double msn_term = c->epbl_rh18_cn2 * vpo_sm_exp(c->epbl_rh18_cn3 * bld * absf / ustar);
+        const double mstar_n = c->epbl_rh18_cn1 * msn_term / (1.0 + msn_term);
+        const double b0p = fmx(0.0, b0);
+        const double u5 = (ustar * ustar) * (ustar * ustar) * ustar;
+        const double mstar_s = c->epbl_rh18_cs1 * vpo_sm_pow(b0p * b0p * bld / (u5 * absf_floor), c->epbl_rh18_cs2);
+        mstar = mstar_n + mstar_s;
         if (c->epbl_mstar_cap > 0.0) mstar = fmn(c->epbl_mstar_cap, mstar);
     } else {
         mstar = c->epbl_mstar_const;
@@ -106,13 +113,14 @@ static double sw_pe_cost_shape(double tau)
     return (tau * (1.0 + vpo_sm_exp(-tau)) - 2.0 * em1) / (tau * em1);
 }
 
-/* epbl_mixlen_shape (:690-714), exponent 2 */
+/* epbl_mixlen_shape (:690-714) */
 static double mixlen_shape(const vphys_config *c, double z_depth, double mld_guess)
 {
     const double ts = c->epbl_translay_scale;
     if (!c->epbl_mld_iteration || ts >= 1.0 || ts < 0.0 || mld_guess <= 0.0) return 1.0;
     const double fr = fmx(0.0, (mld_guess - z_depth) / mld_guess);
-    return ts + (1.0 - ts) * fr * fr;
+    if (c->epbl_mixlen_exponent == 2.0) return ts + (1.0 - ts) * fr * fr;
+    return ts + (1.0 - ts) * vpo_sm_pow(fr, c->epbl_mixlen_exponent);
 }
 
 /* the turbulent velocity scale and the mixing-length diffusivity of sweep

@@ -150,7 +150,8 @@ class VphysConfig(ctypes.Structure):
         "epbl_mstar_const", "epbl_mstar_cap", "epbl_mstar_coef1", "epbl_c_ek", "epbl_mstar_conv_adj", "epbl_nstar",
         "epbl_tke_decay", "epbl_wstar_ustar_coef", "epbl_vstar_scale_fac", "epbl_vstar_surf_fac", "epbl_von_karman",
         "epbl_ekman_scale_coef", "epbl_min_mix_len", "epbl_mixlen_exponent", "epbl_translay_scale", "epbl_mld_tol",
-        "epbl_omega", "epbl_omega_frac", "epbl_ustar_min", "epbl_prandtl")]
+        "epbl_omega", "epbl_omega_frac", "epbl_ustar_min", "epbl_prandtl", "epbl_rh18_cn1", "epbl_rh18_cn2",
+        "epbl_rh18_cn3", "epbl_rh18_cs1", "epbl_rh18_cs2")]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_ if n not in ()}

@@ -133,6 +133,11 @@ def default_config() -> VphysConfig:
     c.epbl_omega_frac = 0.0
     c.epbl_ustar_min = 1e-08
     c.epbl_prandtl = 1.0
+    c.epbl_rh18_cn1 = 0.275
+    c.epbl_rh18_cn2 = 8.0
+    c.epbl_rh18_cn3 = -5.0
+    c.epbl_rh18_cs1 = 0.2
+    c.epbl_rh18_cs2 = 0.4
     return c
 
 
@@ -261,16 +266,16 @@ class EPBL:
     """Reichl-Hallberg energetics PBL, column form (python/rdb/closures.py:107-150:
     `EPBL(mstar_scheme="om4", mstar=1.2, nstar=0.2, prandtl=1.0, combine="add",
     mld_iteration=True, mld_use_prev_guess=False, langmuir=None)`).  Like the
-    reference it switches KPP off.  Not built here: the "rh18" mstar fit and
-    Langmuir enhancement (both raise)."""
+    reference it switches KPP off.  Langmuir enhancement is not built here
+    (raises)."""
 
-    _MSTAR = {"constant": 1, "om4": 2}
+    _MSTAR = {"constant": 1, "om4": 2, "rh18": 3}
     _COMBINE = {"add": 1, "max": 2, "max_shear": 3}
 
     def __init__(self, mstar_scheme="om4", mstar=1.2, nstar=0.2, prandtl=1.0, combine="add", mld_iteration=True,
                  mld_use_prev_guess=False, langmuir=None):
         if mstar_scheme not in self._MSTAR:
-            raise NotImplementedError(f"EPBL: mstar_scheme {mstar_scheme!r} is not built (constant, om4)")
+            raise ValueError(f"EPBL: mstar_scheme must be one of {sorted(self._MSTAR)}")
         if combine not in self._COMBINE:
             raise ValueError(f"EPBL: combine must be one of {sorted(self._COMBINE)}")
         if langmuir is not None:

@@ -264,16 +264,12 @@ int validate(const vphys_config *c, int ntr)
         return push_error(VPHYS_ERR_CONFIG, "ks_lambda, ks_lz_rescale and ks_src_max_chg must be nonzero");
     if (c->epbl < 0 || c->epbl > 1) return push_error(VPHYS_ERR_CONFIG, "epbl must be 0 or 1");
     if (c->epbl) {
-        if (c->epbl_mstar_scheme == 3)
-            return push_error(VPHYS_ERR_CONFIG, "epbl_mstar_scheme 3 (RH18) is not built: 1 constant or 2 OM4");
-        if (c->epbl_mstar_scheme < 1 || c->epbl_mstar_scheme > 2)
-            return push_error(VPHYS_ERR_CONFIG, "epbl_mstar_scheme must be 1 (constant) or 2 (OM4)");
+        if (c->epbl_mstar_scheme < 1 || c->epbl_mstar_scheme > 3)
+            return push_error(VPHYS_ERR_CONFIG, "epbl_mstar_scheme must be 1 (constant), 2 (OM4) or 3 (RH18)");
         if (c->epbl_vstar_scheme < 1 || c->epbl_vstar_scheme > 2)
             return push_error(VPHYS_ERR_CONFIG, "epbl_vstar_scheme must be 1 (cube root) or 2 (RH18)");
         if (c->epbl_combine < 1 || c->epbl_combine > 3)
             return push_error(VPHYS_ERR_CONFIG, "epbl_combine must be 1 (add), 2 (max) or 3 (max_shear)");
-        if (c->epbl_mixlen_exponent != 2.0)
-            return push_error(VPHYS_ERR_CONFIG, "epbl_mixlen_exponent other than 2 is not built");
         if (c->learned_kpp) return push_error(VPHYS_ERR_CONFIG, "EPBL replaces KPP: learned_kpp must be 0");
         if (c->epbl_mld_max_its < 1 || c->epbl_mld_max_its > 1000)
             return push_error(VPHYS_ERR_CONFIG, "epbl_mld_max_its must be in [1, 1000]");
@@ -740,6 +736,11 @@ int vphys_config_default(vphys_config *c)
     c->epbl_omega = 7.2921e-05;
     c->epbl_ustar_min = 1e-08;
     c->epbl_prandtl = 1.0;
+    c->epbl_rh18_cn1 = 0.275;
+    c->epbl_rh18_cn2 = 8.0;
+    c->epbl_rh18_cn3 = -5.0;
+    c->epbl_rh18_cs1 = 0.2;
+    c->epbl_rh18_cs2 = 0.4;
     return VPHYS_OK;
 }
 

@@ -123,16 +123,16 @@ __device__ __forceinline__ double sm_cbrt(double x)
 // k = nearest integer to x/ln2 (halves away from zero), r = x - k ln2 with
 // ln2 split so k*LN2_HI is exact, degree-13 Taylor polynomial (1/i!), 2**k;
 // results below the smallest normal are exactly 0.
-__device__ __forceinline__ double sm_exp(double x)
+// exp(x + c): the correction c joins the reduced argument (0 for plain exp;
+// the tail of a double-double exponent for sm_pow), rdb_sm_exp_core
+// (rdb_safe_math_core.inc:81-114)
+__device__ __forceinline__ double sm_exp_core(double x, double c)
 {
-    if (isnan(x)) return x;
-    if (x > 709.78271289338399679) return __longlong_as_double(0x7ff0000000000000LL);
-    if (x < -745.1332191019412) return 0.0;
     const double kr = round(x * 1.442695040888963387);
     const int k = (int)kr;
     double r = x - kr * 0.69314718060195446014;
     r = r - kr * -4.2009150726810845979e-11;
-    r = r + 0.0;
+    r = r + c;
     double p = 1.0 / 6227020800.0;
     p = p * r + 1.0 / 479001600.0;
     p = p * r + 1.0 / 39916800.0;
@@ -150,6 +150,13 @@ __device__ __forceinline__ double sm_exp(double x)
     double y = (k > 1000) ? 2.0 * ldexp(p, k - 1) : ldexp(p, k);
     if (y < DBL_TINY) y = 0.0;
     return y;
+}
+__device__ __forceinline__ double sm_exp(double x)
+{
+    if (isnan(x)) return x;
+    if (x > 709.78271289338399679) return __longlong_as_double(0x7ff0000000000000LL);
+    if (x < -745.1332191019412) return 0.0;
+    return sm_exp_core(x, 0.0);
 }
 
 // ---- position-independent natural logarithm: rdb_sm_log
@@ -191,6 +198,132 @@ __device__ __forceinline__ double sm_log(double x)
     const double s = kr * 0.69314718060195446014 + 2.0 * f;
     const double w = (2.0 * f) * u * p + kr * -4.2009150726810845979e-11;
     return s + w;
+}
+
+// ---- exact sum (Knuth) and exact product without FMA (Dekker, Veltkamp
+// split by 2^27 + 1), rdb_safe_math_core.inc:53-79: s + e == a + b,
+// p + e == a * b.  The _rn intrinsics keep every operation separately
+// rounded whatever the file's contraction setting.
+__device__ __forceinline__ void sm_two_sum(double a, double b, double &s, double &e)
+{
+    s = __dadd_rn(a, b);
+    const double bb = __dsub_rn(s, a);
+    e = __dadd_rn(__dsub_rn(a, __dsub_rn(s, bb)), __dsub_rn(b, bb));
+}
+__device__ __forceinline__ void sm_two_prod(double a, double b, double &p, double &e)
+{
+    double c = __dmul_rn(134217729.0, a);
+    const double ah = __dsub_rn(c, __dsub_rn(c, a));
+    const double al = __dsub_rn(a, ah);
+    c = __dmul_rn(134217729.0, b);
+    const double bh = __dsub_rn(c, __dsub_rn(c, b));
+    const double bl = __dsub_rn(b, bh);
+    p = __dmul_rn(a, b);
+    e = __dadd_rn(__dadd_rn(__dadd_rn(__dsub_rn(__dmul_rn(ah, bh), p), __dmul_rn(ah, bl)), __dmul_rn(al, bh)),
+                  __dmul_rn(al, bl));
+}
+
+// ---- log x as head + tail, rdb_sm_log_dd (rdb_safe_math_core.inc:208-249):
+// the quotient f = (m-1)/(m+1) carried to ~106 bits, the series tail in
+// plain double; lh + ll is good to ~1e-18 relative.
+__device__ __forceinline__ void sm_log_dd(double x, double &lh, double &ll)
+{
+    double xs = x;
+    int kadj = 0;
+    if (x < DBL_TINY) {
+        xs = x * 18014398509481984.0;   // 2^54
+        kadj = -54;
+    }
+    int e;
+    double m = frexp(xs, &e);
+    int k = e + kadj;
+    if (m < 0.70710678118654757274) {
+        m = 2.0 * m;
+        k = k - 1;
+    }
+    const double a = m - 1.0;
+    double bh, bl;
+    sm_two_sum(m, 1.0, bh, bl);
+    const double q1 = xdiv(a, bh);
+    double p1, p2;
+    sm_two_prod(q1, bh, p1, p2);
+    const double rr = ((a - p1) - p2) - q1 * bl;
+    const double q2 = xdiv(rr, bh);
+    const double fh = q1 + q2;
+    const double fl = q2 - (fh - q1);
+    const double u = fh * fh;
+    double p = 1.0 / 19.0;
+    p = p * u + 1.0 / 17.0;
+    p = p * u + 1.0 / 15.0;
+    p = p * u + 1.0 / 13.0;
+    p = p * u + 1.0 / 11.0;
+    p = p * u + 1.0 / 9.0;
+    p = p * u + 1.0 / 7.0;
+    p = p * u + 1.0 / 5.0;
+    p = p * u + 1.0 / 3.0;
+    const double tail = (2.0 * fh) * u * p;
+    const double kr = (double)k;
+    double ss, ee;
+    sm_two_sum(kr * 0.69314718060195446014, 2.0 * fh, ss, ee);
+    lh = ss;
+    ll = ee + ((2.0 * fl + tail) + kr * -4.2009150726810845979e-11);
+}
+
+// ---- position-independent power: rdb_sm_pow (rdb_safe_math_pow.inc:6-105):
+// the C99 pow special values except that a NaN anywhere gives NaN; for finite
+// x > 0, exp(y log x) with the log as head + tail and y*log x formed exactly.
+__device__ __forceinline__ double sm_pow(double x, double y)
+{
+    const double NaN = __longlong_as_double(0x7ff8000000000000LL);
+    const double Inf = __longlong_as_double(0x7ff0000000000000LL);
+    if (isnan(x) || isnan(y)) return NaN;
+    if (y == 0.0 || x == 1.0) return 1.0;
+    const double ax = fabs(x), ay = fabs(y);
+    bool yint = false, yodd = false;
+    if (isfinite(y)) {
+        if (ay >= 9007199254740992.0) {
+            yint = true;
+        } else {
+            yint = (ay == round(ay));
+            const double h = 0.5 * ay;
+            yodd = yint && (h != round(h));
+        }
+    }
+    const bool xneg = (x < 0.0) || (x == 0.0 && signbit(x));
+    double r;
+    if (!isfinite(y)) {
+        if (ax == 1.0) return 1.0;
+        return ((ax < 1.0) == (y > 0.0)) ? 0.0 : Inf;
+    }
+    if (ax == 0.0) {
+        r = (y > 0.0) ? 0.0 : Inf;
+        return (xneg && yodd) ? -r : r;
+    }
+    if (!isfinite(x)) {
+        r = (y > 0.0) ? Inf : 0.0;
+        return (xneg && yodd) ? -r : r;
+    }
+    if (xneg && !yint) return NaN;
+    double lh, ll;
+    sm_log_dd(ax, lh, ll);
+    const double t = y * lh;
+    if (t > 800.0) {
+        r = Inf;
+    } else if (t < -800.0) {
+        r = 0.0;
+    } else {
+        double ph, pl, ee, c2;
+        sm_two_prod(y, lh, ph, pl);
+        const double c = pl + y * ll;
+        sm_two_sum(ph, c, ee, c2);
+        if (ee > 709.78271289338399679)
+            r = Inf;
+        else if (ee < -745.1332191019412)
+            r = 0.0;
+        else
+            r = sm_exp_core(ee, c2);
+    }
+    return (xneg && yodd) ? -r : r;
 }
 
 // ---- position-independent arctangent: rdb_sm_atan

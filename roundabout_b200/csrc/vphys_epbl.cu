@@ -54,7 +54,7 @@ __device__ __forceinline__ void specvol_derivs(const vphys_config &c, double T, 
     dsv_ds = WRIGHT_A2 + dlam_ds * inv_p - lambda * dp0_ds * inv_p2;
 }
 
-// epbl_find_mstar, schemes constant (1) and OM4 (2)
+// epbl_find_mstar: constant (1), OM4 (2), RH18 (3)
 __device__ __forceinline__ double find_mstar(const vphys_config &c, double b0, double ustar, double bld, double absf)
 {
     double mstar;
@@ -64,6 +64,14 @@ __device__ __forceinline__ double find_mstar(const vphys_config &c, double b0, d
         double mstar_n = 0.0;
         if (ustar > absf_floor * bld) mstar_n = c.epbl_c_ek * sm_log(xdiv(ustar, absf_floor * fmx(bld, 1.0e-10)));
         mstar = fmx(mstar_s, fmn(1.25, mstar_n));
+        if (c.epbl_mstar_cap > 0.0) mstar = fmn(c.epbl_mstar_cap, mstar);
+    } else if (c.epbl_mstar_scheme == 3) {
+        const double msn_term = c.epbl_rh18_cn2 * sm_exp(xdiv(c.epbl_rh18_cn3 * bld * absf, ustar));
+        const double mstar_n = xdiv(c.epbl_rh18_cn1 * msn_term, 1.0 + msn_term);
+        const double b0p = fmx(0.0, b0);
+        const double u5 = (ustar * ustar) * (ustar * ustar) * ustar;
+        const double mstar_s = c.epbl_rh18_cs1 * sm_pow(xdiv(b0p * b0p * bld, u5 * absf_floor), c.epbl_rh18_cs2);
+        mstar = mstar_n + mstar_s;
         if (c.epbl_mstar_cap > 0.0) mstar = fmn(c.epbl_mstar_cap, mstar);
     } else {
         mstar = c.epbl_mstar_const;
@@ -276,7 +284,8 @@ __global__ void __launch_bounds__(128, 4) k_epbl(const Params p, double dt, doub
                         const double ts = c.epbl_translay_scale;
                         if (c.epbl_mld_iteration && !(ts >= 1.0) && !(ts < 0.0) && !(mld_guess <= 0.0)) {
                             const double fr = fmx(0.0, xdiv(mld_guess - z_int, mld_guess));
-                            shape_fn = ts + (1.0 - ts) * fr * fr;
+                            shape_fn = (c.epbl_mixlen_exponent == 2.0) ? ts + (1.0 - ts) * fr * fr
+                                                                       : ts + (1.0 - ts) * sm_pow(fr, c.epbl_mixlen_exponent);
                         }
                     }
                     const double hbs = fmn(hb_hs, shape_fn);

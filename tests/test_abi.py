@@ -105,8 +105,8 @@ def test_epbl_knobs_are_validated(lib):
     from roundabout_b200.config import EPBL, default_config
 
     h = ctypes.c_void_p()
-    for over in (dict(epbl_mstar_scheme=3), dict(epbl_mixlen_exponent=1.5),
-                 dict(learned_kpp=1), dict(epbl_combine=4), dict(epbl_mld_max_its=0), dict(epbl_ustar_min=0.0)):
+    for over in (dict(epbl_mstar_scheme=4), dict(learned_kpp=1), dict(epbl_combine=4), dict(epbl_mld_max_its=0),
+                 dict(epbl_ustar_min=0.0)):
         bad = default_config()
         bad.epbl = 1
         for k, v in over.items():
@@ -115,6 +115,8 @@ def test_epbl_knobs_are_validated(lib):
         assert h.value is None
     cfg = EPBL(mstar_scheme="om4", combine="max_shear", mld_use_prev_guess=True).apply(default_config())
     assert (cfg.epbl, cfg.use_kpp, cfg.epbl_mstar_scheme, cfg.epbl_combine, cfg.epbl_mld_use_prev_guess) == (1, 0, 2, 3, 1)
-    for bad_kw in (dict(mstar_scheme="rh18"), dict(langmuir=object())):
-        with pytest.raises(NotImplementedError):
-            EPBL(**bad_kw)
+    assert EPBL(mstar_scheme="rh18").apply(default_config()).epbl_mstar_scheme == 3
+    with pytest.raises(ValueError):
+        EPBL(mstar_scheme="rh19")
+    with pytest.raises(NotImplementedError):
+        EPBL(langmuir=object())

@@ -185,3 +185,45 @@ def test_shortwave_ledger_limits(oracle):
     assert out[(0.0, 0.0)][1] == out[(0.0, 0.6)][1]
     assert out[(300.0, 0.6)][1] >= out[(300.0, 0.0)][1], (out[(300.0, 0.6)][1], out[(300.0, 0.0)][1])
     assert out[(300.0, 0.6)][1] > out[(300.0, 0.0)][1] or not np.array_equal(out[(300.0, 0.6)][0], out[(300.0, 0.0)][0])
+
+
+def test_rh18_mstar_closed_form(oracle):
+    """epbl_find_mstar's RH18 branch (rdb_ocean_epbl.F90:664-670) on the same
+    neutral two-layer column: with no buoyancy flux the stabilising term is
+    cs1 * 0^cs2 = 0, so mstar = cn1 e/(1 + e) with e = cn2 exp(cn3 BLD f/u*)."""
+    dz, dt, f = 10.0, 1800.0, 1.0e-4
+    for ustar in (0.01, 0.003):
+        cfg = epbl_config(epbl_mstar_scheme=3, epbl_mld_iteration=0, epbl_tke_decay=0.0)
+        st = stratified(oracle, 2, dz, 15.0, 0.0)
+        st.coriolis[...] = f
+        st.stress_mag[...] = RHO0 * ustar ** 2
+        st.call("vpo_epbl", cfg, dt)
+        ustar_eff = math.sqrt(RHO0 * ustar ** 2 / RHO0)
+        bld = 0.5 * (2 * dz + 1e-20)
+        e = 8.0 * math.exp(-5.0 * bld * f / ustar_eff)
+        mstar = 0.275 * e / (1.0 + e)
+        vstar = (mstar * ustar_eff ** 3) ** (1.0 / 3.0)
+        want = vstar * 0.41 * (dz * 0.5 * vstar) / (f * dz * 0.5 + vstar)
+        got = float(st.kd_epbl[0, 0, 1])
+        assert abs(got - want) <= 1e-12 * want, (ustar, got, want)
+
+
+def test_mixing_length_exponent(oracle):
+    """epbl_mixlen_shape (:690-714), shape = ts + (1 - ts) fr^n: at the
+    first interface below the surface layer (no energy spent yet, f = 0,
+    the first MLD guess half the column) the diffusivity is the unlimited
+    first guess v* kappa htot hbs with hbs = the shape, so the exponent-3 /
+    exponent-2 ratio of kd there is the ratio of the two shapes; exponent 3
+    goes through rdb_sm_pow, exponent 2 through fr * fr."""
+    nz, dz, dt = 30, 2.0, 1800.0
+    kd_top = {}
+    for n in (2.0, 3.0):
+        cfg = epbl_config(epbl_mixlen_exponent=n, epbl_mld_iteration=1, epbl_mld_max_its=1)
+        st = stratified(oracle, nz, dz, 15.0, 1.0e-5 * RHO0 / (G * ALPHA_LIN))
+        st.stress_mag[...] = RHO0 * 0.01 ** 2
+        st.call("vpo_epbl", cfg, dt)
+        kd_top[n] = float(st.kd_epbl[0, 0, nz - 1])
+    fr = (0.5 * nz * dz - dz) / (0.5 * nz * dz)
+    want = (0.1 + 0.9 * fr ** 3) / (0.1 + 0.9 * fr ** 2)
+    assert kd_top[2.0] > 0.0
+    assert abs(kd_top[3.0] / kd_top[2.0] - want) < 1e-12, (kd_top, want)

@@ -1,4 +1,4 @@
-"""The oracle's port of rdb_sm_cbrt / rdb_sm_atan / rdb_sm_exp / rdb_sm_log against the reference's
+"""The oracle's port of rdb_sm_cbrt / rdb_sm_atan / rdb_sm_exp / rdb_sm_log / rdb_sm_pow against the reference's
 golden bit patterns (tests/test_safe_math_golden.inc, transcribed into
 tests/golden/safe_math_golden.json)."""
 import json
@@ -27,3 +27,13 @@ def test_golden_bits(oracle, fn):
         if got != res:
             bad.append((arg, res, got))
     assert not bad, f"{len(bad)} of {len(GOLD[fn])} {fn} rows differ: {bad[:4]}"
+
+
+@pytest.mark.parametrize("table", ["pow", "powbig"])
+def test_golden_bits_pow(oracle, table):
+    bad = []
+    for x, y, res in GOLD[table]:
+        got = d2h(oracle.sm_pow(h2d(x), h2d(y)))
+        if got != res:
+            bad.append((x, y, res, got))
+    assert not bad, f"{len(bad)} of {len(GOLD[table])} {table} rows differ: {bad[:4]}"
