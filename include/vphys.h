@@ -204,8 +204,8 @@ typedef struct vphys_config {
      * KD_EPBL into kt and epbl_prandtl * KD_EPBL into kv (epbl_combine);
      * convection then masks below MLD_EPBL.  With sw_pen_frac != 0 the
      * two-band shortwave absorbed in each layer is charged to the TKE budget
-     * (the reference's epbl_sw_ctke ledger, source Q_HEAT).  Not built:
-     * Langmuir enhancement. */
+     * (the reference's epbl_sw_ctke ledger, source Q_HEAT); epbl_use_lt adds
+     * the Langmuir enhancement of mstar. */
     int epbl;                 /* 0 */
     int epbl_mstar_scheme;    /* 1 constant, 2 OM4 (default), 3 RH18 */
     int epbl_vstar_scheme;    /* 1 cube root (default), 2 RH18 */
@@ -241,6 +241,21 @@ typedef struct vphys_config {
     double epbl_rh18_cn3;     /* -5 */
     double epbl_rh18_cs1;     /* 0.2 */
     double epbl_rh18_cs2;     /* 0.4 */
+    /* Langmuir enhancement of mstar (Reichl & Li 2019) from the LF17
+     * statistical wave state of u* alone (Li & Fox-Kemper 2017; COARE 3.5
+     * u* -> U10): epbl_lf17_wave_state, epbl_lf17_la, epbl_lt_enhance
+     * (rdb_ocean_epbl.F90:716-862) */
+    int epbl_use_lt;          /* 0 */
+    int epbl_lt_scheme;       /* 1 rescale (default), 2 additive */
+    double epbl_lt_enhance_coef; /* 0.447 */
+    double epbl_lt_enhance_exp; /* -1.33 */
+    double epbl_lt_max_enhance; /* 5 */
+    double epbl_la_frac_hbl;  /* 0.04: the surface layer the Stokes drift is averaged over, a fraction of the MLD */
+    double epbl_lt_lac1;      /* -0.87 */
+    double epbl_lt_lac2;      /* 0 */
+    double epbl_lt_lac3;      /* 0 */
+    double epbl_lt_lac4;      /* 0.95 */
+    double epbl_lt_lac5;      /* 0.95 */
 } vphys_config;
 
 #define VPHYS_KPP_SW_ALL 1
@@ -285,6 +300,8 @@ enum vphys_field {
     VPHYS_FIELD_KD_EPBL = 32,   /* in/out  (nx, ny, nz+1) EPBL diffusivity kd_int, 0 at bed and surface */
     VPHYS_FIELD_MLD_EPBL = 33,  /* in/out  (nx, ny) EPBL mixed-layer depth (the previous one seeds the
                                    iteration when epbl_mld_use_prev_guess) */
+    VPHYS_FIELD_LA_EPBL = 34,   /* out     (nx, ny) EPBL Langmuir number of the last MLD iteration (0 when
+                                   epbl_use_lt is 0) */
     VPHYS_FIELD_TRACER0 = 64    /* in/out  (nx, ny, nz); tracer t is
                                    VPHYS_FIELD_TRACER0 + t */
 };
@@ -402,7 +419,7 @@ int vphys_kappa_shear(vphys_handle h, double dt);
  * iterated on the mixed-layer depth (false position, up to
  * epbl_mld_max_its).  Reads H, T, S, STRESS_MAG, Q_HEAT, Q_SALT, WET,
  * CORIOLIS; writes KD_EPBL (0 on the bed and surface interfaces and in land
- * columns) and MLD_EPBL.  A no-op without a temperature or salinity tracer.
+ * columns), MLD_EPBL and LA_EPBL.  A no-op without a temperature or salinity tracer.
  * Replaces epbl_compute -> epbl_column_kernel (rdb_ocean_epbl.F90:864-1659);
  * vphys_step runs it before the assembly when epbl is 1, and the assembly
  * merges KD_EPBL (epbl_merge_into_kv_kt / epbl_merge_max_shear, 1661-1718). */

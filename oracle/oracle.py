@@ -28,7 +28,7 @@ class VpoState(ctypes.Structure):
                           "visc_rem_u", "visc_rem_v", "gamma_t", "gamma_s", "heat_budget", "salt_budget")
     ] + [(n, _ip) for n in ("k_top_u", "k_top_v", "k_bot_u", "k_bot_v")] + [("tr", ctypes.POINTER(_dp))] + [
         (n, _dp) for n in ("heat_budget_surface", "salt_budget_surface", "coriolis", "kd_shear", "tke_shear", "kd_epbl",
-                          "mld_epbl")]
+                          "mld_epbl", "la_epbl")]
 
 
 def build(force: bool = False) -> Path:
@@ -58,6 +58,8 @@ def lib():
         L.vpo_sm_exp.argtypes = [ctypes.c_double]
         L.vpo_sm_log.restype = ctypes.c_double
         L.vpo_sm_log.argtypes = [ctypes.c_double]
+        L.vpo_sm_erfc.restype = ctypes.c_double
+        L.vpo_sm_erfc.argtypes = [ctypes.c_double]
         L.vpo_sm_pow.restype = ctypes.c_double
         L.vpo_sm_pow.argtypes = [ctypes.c_double, ctypes.c_double]
         L.vpo_set_threads.argtypes = [ctypes.c_int]
@@ -76,6 +78,10 @@ def lib():
             getattr(L, name).restype = None
         L.vpo_eos_buoyancy_coeffs.argtypes = [ctypes.c_double] * 3 + [ctypes.POINTER(ctypes.c_double)] * 2
         L.vpo_eos_buoyancy_coeffs.restype = None
+        L.vpo_epbl_lf17.argtypes = [ctypes.c_double] * 3 + [ctypes.POINTER(ctypes.c_double)] * 2
+        L.vpo_epbl_lf17.restype = None
+        L.vpo_epbl_lt_enhance.argtypes = [ctypes.c_void_p] + [ctypes.c_double] * 6
+        L.vpo_epbl_lt_enhance.restype = ctypes.c_double
         L.vpo_step.argtypes = [ctypes.c_void_p, ctypes.POINTER(VpoState), ctypes.c_double, ctypes.c_int]
         L.vpo_step.restype = ctypes.c_int
         _lib = L
@@ -124,6 +130,7 @@ class OracleState:
         self.tke_shear = f(nx, ny, nz + 1)
         self.kd_epbl = f(nx, ny, nz + 1)
         self.mld_epbl = f(nx, ny)
+        self.la_epbl = f(nx, ny)
         self.k_top_u = np.full((nx + 1, ny), nz, dtype=np.int32, order="F")
         self.k_top_v = np.full((nx, ny + 1), nz, dtype=np.int32, order="F")
         self.k_bot_u = np.ones((nx + 1, ny), dtype=np.int32, order="F")
@@ -191,6 +198,10 @@ def sm_exp(x: float) -> float:
 
 def sm_log(x: float) -> float:
     return lib().vpo_sm_log(float(x))
+
+
+def sm_erfc(x: float) -> float:
+    return lib().vpo_sm_erfc(float(x))
 
 
 def sm_pow(x: float, y: float) -> float:

@@ -115,6 +115,7 @@ double vpo_sm_exp(double x)
 /* rdb_sm_log (rdb_safe_math_core.inc:139-206): x = m 2^k with m in
  * [sqrt(1/2), sqrt(2)), log m = 2 atanh f, f = (m-1)/(m+1), the odd series
  * in f to 1/19 (Cody & Waite 1980, ch. 5), k ln 2 added as head + tail. */
+static const double SM_SPLIT = 134217729.0;   /* 2^27 + 1, the Veltkamp split */
 static const double SM_LOG_C[10] = {1.0,        1.0 / 3.0,  1.0 / 5.0,  1.0 / 7.0,  1.0 / 9.0,
                                     1.0 / 11.0, 1.0 / 13.0, 1.0 / 15.0, 1.0 / 17.0, 1.0 / 19.0};
 static const double SM_SQRT_HALF = 0.70710678118654757274;
@@ -152,7 +153,6 @@ double vpo_sm_log(double x)
 
 /* Knuth's exact sum and Dekker's exact product without FMA (Veltkamp split
  * by 2^27 + 1): s + e == a + b, p + e == a * b (rdb_safe_math_core.inc:53-79). */
-static const double SM_SPLIT = 134217729.0;
 static void sm_two_sum(double a, double b, double *s, double *e)
 {
     *s = a + b;
@@ -279,6 +279,83 @@ double vpo_sm_pow(double x, double y)
     }
     if (xneg && yodd) r = -r;
     return r;
+}
+
+/* rdb_sm_erfc (rdb_safe_math_erfc.inc): a series in x^2 below |x| = 1/2;
+ * beyond, exp(-x^2) formed as exp(-xh^2 - xl (x + xh)) on a Veltkamp split,
+ * times a rational fit on [1/2, 2) and [2, 4) or the asymptotic form
+ * (1 + w P(w)/Q(w))/(x sqrt(pi)), w = 1/x^2, beyond 4.  The fitted tables
+ * are the reference's (rdb_safe_math_consts.inc:99-128). */
+static const double SM_ERF_C[12] = {
+    1.128379167095512559,      -0.376126389031837538,    0.1128379167095512614,
+    -0.02686617064513124181,   0.005223977625441806293,  -0.0008548327023363942604,
+    0.0001205533296923066544,  -0.00001492564916290355896, 1.64620383639705829e-6,
+    -1.636264690374603956e-7,  1.472152117638980096e-8,  -1.095865453884735107e-9};
+static const double SM_ERFC_A_P[7] = {0.9999999993850857694, 1.248626834329117141, 0.7867094724888269441,
+                                      0.2819428661917610102, 0.05719027224971907214, 0.005247572786535052193,
+                                      4.820036176802313081e-8};
+static const double SM_ERFC_A_Q[7] = {1.0, 2.377005991883625935, 2.468873583018134976, 1.443014856236056964,
+                                      0.5046949490889137691, 0.1013327241858480304, 0.009303534974169982985};
+static const double SM_ERFC_B_P[7] = {0.9999921569124016196, 1.494269944137282868, 1.086387126830294259,
+                                      0.4598879010194165118, 0.1135948493973390344, 0.01390038004034872994,
+                                      1.000103316758091609e-9};
+static const double SM_ERFC_B_Q[7] = {1.0, 2.622591678871410537, 3.045871297831376889, 2.025960043609839722,
+                                      0.8274770365185684096, 0.2013396690397278865, 0.02463786793791475013};
+static const double SM_ERFC_C_P[6] = {-0.4999999999999982792, -12.20993252402114315, -95.49719132910308872,
+                                      -273.5933562329464053, -231.8021338423288, -12.38208675658035851};
+static const double SM_ERFC_C_Q[6] = {1.0, 25.91986504803799107, 226.1241802321382579, 802.2984884770494318,
+                                      1100.222105092567517, 428.3053107970796418};
+static const double SM_INV_SQRTPI = 0.56418958354775627928;
+
+double vpo_sm_erfc(double x)
+{
+    if (isnan(x)) return x;
+    const double ax = fabs(x);
+    if (ax < 0.5) {
+        const double v = x * x;
+        double p = SM_ERF_C[11];
+        for (int i = 10; i >= 0; --i) p = p * v + SM_ERF_C[i];
+        return 1.0 - x * p;
+    }
+    double ex;
+    if (ax > 27.3) {
+        ex = 0.0;
+    } else {
+        const double c = SM_SPLIT * ax;
+        const double xh = c - (c - ax);
+        const double xl = ax - xh;
+        ex = sm_exp_core(-(xh * xh), -(xl * (ax + xh)));
+    }
+    double p, q;
+    if (ax < 2.0) {
+        p = SM_ERFC_A_P[6];
+        q = SM_ERFC_A_Q[6];
+        for (int i = 5; i >= 0; --i) {
+            p = p * ax + SM_ERFC_A_P[i];
+            q = q * ax + SM_ERFC_A_Q[i];
+        }
+        ex = ex * (p / q);
+    } else if (ax < 4.0) {
+        p = SM_ERFC_B_P[6];
+        q = SM_ERFC_B_Q[6];
+        for (int i = 5; i >= 0; --i) {
+            p = p * ax + SM_ERFC_B_P[i];
+            q = q * ax + SM_ERFC_B_Q[i];
+        }
+        ex = ex * (p / q);
+    } else {
+        const double rax = 1.0 / ax;
+        const double w = rax * rax;
+        p = SM_ERFC_C_P[5];
+        q = SM_ERFC_C_Q[5];
+        for (int i = 4; i >= 0; --i) {
+            p = p * w + SM_ERFC_C_P[i];
+            q = q * w + SM_ERFC_C_Q[i];
+        }
+        ex = ((ex * SM_INV_SQRTPI) * rax) * (1.0 + w * (p / q));
+    }
+    if (ex < DBL_MIN) ex = 0.0;
+    return (x < 0.0) ? 2.0 - ex : ex;
 }
 
 static inline double sm_flush(double r)

@@ -46,6 +46,7 @@ typedef struct vpo_state {
     double *kd_shear, *tke_shear;           /* (nx,ny,nz+1) kappa-shear kd_int, tke_int */
     double *kd_epbl;                        /* (nx,ny,nz+1) EPBL kd_int */
     double *mld_epbl;                       /* (nx,ny) EPBL mixed-layer depth */
+    double *la_epbl;                        /* (nx,ny) EPBL Langmuir number */
 } vpo_state;
 
 void vpo_set_threads(int n);
@@ -74,6 +75,7 @@ void vpo_eos_buoyancy_coeffs(double T, double S, double p, double *alpha_T, doub
 double vpo_sm_exp(double x);
 double vpo_sm_log(double x);
 double vpo_sm_pow(double x, double y);
+double vpo_sm_erfc(double x);
 void vpo_sw_penetration(const vphys_config *c, vpo_state *s, double dt);
 
 /* kappa-shear, column form (vphys_oracle_kshear.c) */
@@ -83,6 +85,10 @@ void vpo_kappa_shear_merge(const vphys_config *c, vpo_state *s);
 /* EPBL, column form (vphys_oracle_epbl.c) */
 void vpo_epbl(const vphys_config *c, vpo_state *s, double dt);
 void vpo_epbl_merge(const vphys_config *c, vpo_state *s);
+/* the LF17 wave state and Langmuir number, and the mstar enhancement, alone */
+void vpo_epbl_lf17(double ustar, double rho0, double zsl, double *u10, double *la);
+double vpo_epbl_lt_enhance(const vphys_config *c, double la, double b0, double ustar, double bld, double absf,
+                           double mstar);
 
 int vpo_step(const vphys_config *c, vpo_state *s, double dt, int n_steps);
 

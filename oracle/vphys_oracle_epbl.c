@@ -7,8 +7,8 @@
  * and RH18 velocity scales, the MLD iteration (false position / bisection,
  * optionally seeded by the previous MLD), the mixing-length shape, the two-band penetrating-shortwave TKE ledger (on whenever
  * sw_pen_frac != 0, source Q_heat, bed row k_bot = 1), and the three merges
- * (add, max, max_shear).  Langmuir enhancement and the TKE budget
- * diagnostics are not restated (the library has neither).
+ * (add, max, max_shear), and the LF17 Langmuir enhancement of mstar.  The
+ * TKE budget diagnostics are not restated (the library has none).
  *
  * Parity pins: the analytic and structural tests of the reference's
  * tests/test_ocean_epbl.F90 re-expressed in tests/test_oracle_epbl.py, and
@@ -101,6 +101,111 @@ static double find_mstar(const vphys_config *c, double b0, double ustar, double 
             mstar = mstar * (1.0 - c->epbl_mstar_conv_adj);
     }
     return mstar;
+}
+
+/* ---- Langmuir enhancement, LF17 wind-only path (rdb_ocean_epbl.F90:716-862).
+ * The empirical constants are those of the cited formulas (Li & Fox-Kemper
+ * 2017, COARE 3.5 of Edson et al. 2013), as the reference lists them at
+ * :59-71. */
+#define LT_VONKAR_WAVES 0.40
+#define LT_NU_AIR 1.0e-6
+#define LT_RHO_AIR 1.225
+#define LT_CHARNOCK_MIN 0.028
+#define LT_CHARNOCK_SLOPE 0.0017
+#define LT_CHARNOCK_ICPT -0.005
+#define LT_US_TO_U10 0.0162
+#define LT_SWH_FROM_U10SQ 0.0246
+#define LT_U19P5_TO_U10 1.075
+#define LT_FM_INTO_FP 1.296
+#define LT_R_LOSS 0.667
+static const double LT_PI = 3.141592653589793115997963468544185161590576171875;
+
+/* epbl_lf17_wave_state (:716-765): COARE fixed-point u* -> U10, then the
+ * surface Stokes drift and the Phillips peak wavenumber */
+static void lf17_wave_state(double ustar_w, double rho_ocn, double *u10, double *ustokes, double *kphil)
+{
+    const double ustar_air = ustar_w * sqrt(rho_ocn / LT_RHO_AIR);
+    const double z0_smooth = 0.11 * LT_NU_AIR / ustar_air;
+    double u = ustar_air * sqrt(1000.0);
+    int converged = 0;
+    for (int itt = 1; itt <= 20; ++itt) {
+        const double alpha_ch = fmn(LT_CHARNOCK_MIN, LT_CHARNOCK_SLOPE * u + LT_CHARNOCK_ICPT);
+        const double z0w = fmx(z0_smooth + alpha_ch * (ustar_air * ustar_air) / GRAVITY, 1.0e-10);
+        const double u_new = ustar_air * vpo_sm_log(10.0 / z0w) / LT_VONKAR_WAVES;
+        if (fabs(u_new - u) <= 1.0e-3 * u) {
+            u = u_new;
+            converged = 1;
+            break;
+        }
+        u = u_new;
+    }
+    if (!converged) u = 25.82 * ustar_air;
+    *u10 = u;
+    *ustokes = LT_US_TO_U10 * u;
+    const double hm0 = LT_SWH_FROM_U10SQ * u * u;
+    const double f_mean = LT_FM_INTO_FP * 0.877 * GRAVITY / (2.0 * LT_PI * LT_U19P5_TO_U10 * u);
+    const double vstokes = 0.125 * LT_PI * LT_R_LOSS * f_mean * hm0 * hm0;
+    *kphil = 0.176 * *ustokes / fmx(vstokes, 1.0e-30);
+}
+
+/* one_m_exp_x (:806-816): (1 - exp(-x))/x, a series below 1e-4 */
+static double one_m_exp_x(double x)
+{
+    if (x < 1.0e-4) return 1.0 - x * (0.5 - x / 6.0);
+    return (1.0 - vpo_sm_exp(-x)) / x;
+}
+
+/* epbl_lf17_la (:767-804): the Langmuir number of the Stokes drift averaged
+ * over the surface layer zsl */
+static double lf17_la(double ustar_w, double zsl, double ustokes, double kphil)
+{
+    const double xkz = kphil * zsl;
+    const double root2kz = sqrt(2.0 * xkz);
+    const double r1 = (0.302 - 1.68 * xkz) * one_m_exp_x(2.0 * xkz);
+    const double r3 = (0.1264 + 0.64 * xkz) * one_m_exp_x(5.12 * xkz);
+    double r5;
+    if (root2kz > 1.0e-3) {
+        const double ec1 = vpo_sm_erfc(root2kz);
+        const double ec2 = vpo_sm_erfc(1.6 * root2kz);
+        r5 = sqrt(LT_PI) * (root2kz * (-0.84 * ec1 + 0.2 * ec2) + 0.1182 * (ec2 - ec1) / root2kz);
+    } else {
+        r5 = -0.64 * sqrt(LT_PI) * root2kz + (-0.14184 + 1.0839648 * root2kz * root2kz);
+    }
+    const double ustokes_sl = fmx(ustokes * (0.715 + r1 + r3 + r5), 1.0e-10);
+    return sqrt(ustar_w / ustokes_sl);
+}
+
+/* epbl_lt_enhance (:818-862): La modified by the Ekman and Obukhov depth
+ * ratios, then mstar rescaled (capped) or incremented */
+static double lt_enhance(const vphys_config *c, double la, double b0, double ustar, double bld, double absf,
+                         double mstar)
+{
+    const double vonkar = c->epbl_von_karman;
+    const double mld_ek = bld * absf / ustar;
+    const double ek_ob = fabs(b0 * vonkar) / (fmx(absf, 1.0e-20) * ustar * ustar);
+    const double mld_ob = fabs(bld * b0 * vonkar) / (ustar * ustar * ustar);
+    double la_mod;
+    if (b0 >= 0.0)
+        la_mod = la * ((1.0 + fmx(-0.5, c->epbl_lt_lac1 * mld_ek)) + c->epbl_lt_lac4 * ek_ob + c->epbl_lt_lac2 * mld_ob);
+    else
+        la_mod = la * ((1.0 + fmx(-0.5, c->epbl_lt_lac1 * mld_ek)) + c->epbl_lt_lac5 * ek_ob + c->epbl_lt_lac3 * mld_ob);
+    la_mod = fmx(la_mod, 1.0e-10);
+    if (c->epbl_lt_scheme == 2) return mstar + c->epbl_lt_enhance_coef * vpo_sm_pow(la_mod, c->epbl_lt_enhance_exp);
+    const double enh = fmn(c->epbl_lt_max_enhance, 1.0 + c->epbl_lt_enhance_coef * vpo_sm_pow(la_mod, c->epbl_lt_enhance_exp));
+    return mstar * enh;
+}
+
+void vpo_epbl_lf17(double ustar, double rho0, double zsl, double *u10, double *la)
+{
+    double ustokes, kphil;
+    lf17_wave_state(ustar, rho0, u10, &ustokes, &kphil);
+    *la = lf17_la(ustar, zsl, ustokes, kphil);
+}
+
+double vpo_epbl_lt_enhance(const vphys_config *c, double la, double b0, double ustar, double bld, double absf,
+                           double mstar)
+{
+    return lt_enhance(c, la, b0, ustar, bld, absf, mstar);
 }
 
 /* sw_pe_cost_shape (rdb_ocean_surface_flux.F90:1417-1449): the fraction of
@@ -253,6 +358,9 @@ void vpo_epbl(const vphys_config *c, vpo_state *s, double dt)
                                      c->epbl_omega_frac * 4.0 * (c->epbl_omega * c->epbl_omega));
             const double idecay = c->epbl_tke_decay * absf / ustar;
             const double mech_in = dt * rho0 * (ustar * ustar * ustar);
+            /* the LF17 wave state depends on u* alone: once per column */
+            double la_val = 0.0, lt_u10 = 0.0, lt_ustokes = 0.0, lt_kphil = 0.0;
+            if (c->epbl_use_lt) lf17_wave_state(ustar, rho0, &lt_u10, &lt_ustokes, &lt_kphil);
 
             double mld_found = 0.0;
             if (C2(s->wet, i, j) <= 0.0 || h_sum <= 2.0 * H_NEGLECT) {
@@ -267,7 +375,11 @@ void vpo_epbl(const vphys_config *c, vpo_state *s, double dt)
                 const int n_its = c->epbl_mld_iteration ? c->epbl_mld_max_its : 1;
                 double dt_h = 0.0;   /* carried between interfaces (the Fortran local) */
                 for (int obl_it = 1; obl_it <= n_its; ++obl_it) {
-                    const double mstar_val = find_mstar(c, b0, ustar, mld_guess, absf);
+                    double mstar_val = find_mstar(c, b0, ustar, mld_guess, absf);
+                    if (c->epbl_use_lt) {
+                        la_val = lf17_la(ustar, c->epbl_la_frac_hbl * mld_guess, lt_ustokes, lt_kphil);
+                        mstar_val = lt_enhance(c, la_val, b0, ustar, mld_guess, absf, mstar_val);
+                    }
                     double mech_tke = mstar_val * mech_in;
                     double conv_perel;
                     if (ctke_sfc <= 0.0) {
@@ -455,6 +567,7 @@ void vpo_epbl(const vphys_config *c, vpo_state *s, double dt)
                 }
             }
             C2(s->mld_epbl, i, j) = mld_found;
+            if (s->la_epbl) C2(s->la_epbl, i, j) = la_val;
         }
     }
 }

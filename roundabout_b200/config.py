@@ -138,6 +138,17 @@ def default_config() -> VphysConfig:
     c.epbl_rh18_cn3 = -5.0
     c.epbl_rh18_cs1 = 0.2
     c.epbl_rh18_cs2 = 0.4
+    c.epbl_use_lt = 0
+    c.epbl_lt_scheme = 1
+    c.epbl_lt_enhance_coef = 0.447
+    c.epbl_lt_enhance_exp = -1.33
+    c.epbl_lt_max_enhance = 5.0
+    c.epbl_la_frac_hbl = 0.04
+    c.epbl_lt_lac1 = -0.87
+    c.epbl_lt_lac2 = 0.0
+    c.epbl_lt_lac3 = 0.0
+    c.epbl_lt_lac4 = 0.95
+    c.epbl_lt_lac5 = 0.95
     return c
 
 
@@ -262,12 +273,34 @@ class ConvectiveAdjustment:
         return cfg
 
 
+class Langmuir:
+    """Langmuir enhancement of EPBL's mstar (python/rdb/closures.py:88-105:
+    `Langmuir(scheme="rescale", coef=0.447, exponent=-1.33, max_enhance=5.0,
+    sl_fraction=0.04)`), passed as `EPBL(langmuir=...)`."""
+
+    _SCHEME = {"rescale": 1, "additive": 2}
+
+    def __init__(self, scheme="rescale", coef=0.447, exponent=-1.33, max_enhance=5.0, sl_fraction=0.04):
+        if scheme not in self._SCHEME:
+            raise ValueError(f"Langmuir: scheme must be one of {sorted(self._SCHEME)}")
+        self.scheme, self.coef, self.exponent = scheme, coef, exponent
+        self.max_enhance, self.sl_fraction = max_enhance, sl_fraction
+
+    def _apply(self, cfg):
+        cfg.epbl_use_lt = 1
+        cfg.epbl_lt_scheme = self._SCHEME[self.scheme]
+        cfg.epbl_lt_enhance_coef = float(self.coef)
+        cfg.epbl_lt_enhance_exp = float(self.exponent)
+        cfg.epbl_lt_max_enhance = float(self.max_enhance)
+        cfg.epbl_la_frac_hbl = float(self.sl_fraction)
+        return cfg
+
+
 class EPBL:
     """Reichl-Hallberg energetics PBL, column form (python/rdb/closures.py:107-150:
     `EPBL(mstar_scheme="om4", mstar=1.2, nstar=0.2, prandtl=1.0, combine="add",
     mld_iteration=True, mld_use_prev_guess=False, langmuir=None)`).  Like the
-    reference it switches KPP off.  Langmuir enhancement is not built here
-    (raises)."""
+    reference it switches KPP off; `langmuir` is a `Langmuir`."""
 
     _MSTAR = {"constant": 1, "om4": 2, "rh18": 3}
     _COMBINE = {"add": 1, "max": 2, "max_shear": 3}
@@ -278,8 +311,9 @@ class EPBL:
             raise ValueError(f"EPBL: mstar_scheme must be one of {sorted(self._MSTAR)}")
         if combine not in self._COMBINE:
             raise ValueError(f"EPBL: combine must be one of {sorted(self._COMBINE)}")
-        if langmuir is not None:
-            raise NotImplementedError("EPBL: Langmuir enhancement is not built")
+        if langmuir is not None and not isinstance(langmuir, Langmuir):
+            raise TypeError("EPBL: langmuir must be a Langmuir")
+        self.langmuir = langmuir
         self.mstar_scheme, self.mstar, self.nstar = mstar_scheme, mstar, nstar
         self.prandtl, self.combine = prandtl, combine
         self.mld_iteration, self.mld_use_prev_guess = mld_iteration, mld_use_prev_guess
@@ -294,6 +328,8 @@ class EPBL:
         cfg.epbl_combine = self._COMBINE[self.combine]
         cfg.epbl_mld_iteration = int(bool(self.mld_iteration))
         cfg.epbl_mld_use_prev_guess = int(bool(self.mld_use_prev_guess))
+        if self.langmuir is not None:
+            self.langmuir._apply(cfg)
         return cfg
 
 

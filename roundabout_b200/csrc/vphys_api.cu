@@ -50,7 +50,7 @@ int cuda_status(cudaError_t e, const char *where)
     return push_error(VPHYS_ERR_CUDA, "%s: CUDA error %d (%s)", where, (int)e, cudaGetErrorString(e));
 }
 
-constexpr int NFIXED = 34;
+constexpr int NFIXED = 35;
 constexpr unsigned MAGIC = 0x56504859u;   // "VPHY"
 
 struct Field {
@@ -139,7 +139,8 @@ size_t field_count(int nx, int ny, int nz, int field, bool *is_int)
     case VPHYS_FIELD_Q_SALT:
     case VPHYS_FIELD_WET:
     case VPHYS_FIELD_CORIOLIS:
-    case VPHYS_FIELD_MLD_EPBL: return X * Y;
+    case VPHYS_FIELD_MLD_EPBL:
+    case VPHYS_FIELD_LA_EPBL: return X * Y;
     case VPHYS_FIELD_TAU_X:
     case VPHYS_FIELD_LAMBDA_BOT_U: return (X + 1) * Y;
     case VPHYS_FIELD_TAU_Y:
@@ -271,6 +272,9 @@ int validate(const vphys_config *c, int ntr)
         if (c->epbl_combine < 1 || c->epbl_combine > 3)
             return push_error(VPHYS_ERR_CONFIG, "epbl_combine must be 1 (add), 2 (max) or 3 (max_shear)");
         if (c->learned_kpp) return push_error(VPHYS_ERR_CONFIG, "EPBL replaces KPP: learned_kpp must be 0");
+        if (c->epbl_use_lt < 0 || c->epbl_use_lt > 1) return push_error(VPHYS_ERR_CONFIG, "epbl_use_lt must be 0 or 1");
+        if (c->epbl_use_lt && (c->epbl_lt_scheme < 1 || c->epbl_lt_scheme > 2))
+            return push_error(VPHYS_ERR_CONFIG, "epbl_lt_scheme must be 1 (rescale) or 2 (additive)");
         if (c->epbl_mld_max_its < 1 || c->epbl_mld_max_its > 1000)
             return push_error(VPHYS_ERR_CONFIG, "epbl_mld_max_its must be in [1, 1000]");
         if (!(c->epbl_ustar_min > 0.0)) return push_error(VPHYS_ERR_CONFIG, "epbl_ustar_min must be positive");
@@ -331,6 +335,7 @@ Params make_params(vphys_handle h)
     p.tke_shear = D(VPHYS_FIELD_TKE_SHEAR);
     p.kd_epbl = D(VPHYS_FIELD_KD_EPBL);
     p.mld_epbl = D(VPHYS_FIELD_MLD_EPBL);
+    p.la_epbl = D(VPHYS_FIELD_LA_EPBL);
     p.ks_equals_kt = (h->cfg.bkgnd_profile || h->cfg.kt_bg == h->cfg.ks_bg) ? 1 : 0;
     p.write_gamma = (p.gamma_t && p.gamma_s) ? 1 : 0;
     return p;
@@ -448,6 +453,7 @@ int prepare_epbl(vphys_handle h)
 {
     int st = VPHYS_OK;
     if ((st = ensure(h, VPHYS_FIELD_KD_EPBL))) return st;
+    if ((st = ensure(h, VPHYS_FIELD_LA_EPBL))) return st;
     return ensure(h, VPHYS_FIELD_MLD_EPBL);
 }
 
@@ -741,6 +747,14 @@ int vphys_config_default(vphys_config *c)
     c->epbl_rh18_cn3 = -5.0;
     c->epbl_rh18_cs1 = 0.2;
     c->epbl_rh18_cs2 = 0.4;
+    c->epbl_lt_scheme = 1;
+    c->epbl_lt_enhance_coef = 0.447;
+    c->epbl_lt_enhance_exp = -1.33;
+    c->epbl_lt_max_enhance = 5.0;
+    c->epbl_la_frac_hbl = 0.04;
+    c->epbl_lt_lac1 = -0.87;
+    c->epbl_lt_lac4 = 0.95;
+    c->epbl_lt_lac5 = 0.95;
     return VPHYS_OK;
 }
 

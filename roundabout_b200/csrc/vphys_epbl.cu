@@ -87,6 +87,79 @@ __device__ __forceinline__ double find_mstar(const vphys_config &c, double b0, d
     return mstar;
 }
 
+// ---- Langmuir enhancement, LF17 wind-only path (rdb_ocean_epbl.F90:716-862);
+// the empirical constants of the cited formulas (Li & Fox-Kemper 2017,
+// COARE 3.5), as the reference lists them at :59-71
+// epbl_lf17_wave_state: COARE fixed-point u* -> U10, Stokes drift, Phillips peak wavenumber
+__device__ __forceinline__ void lf17_wave_state(double ustar_w, double rho_ocn, double &ustokes, double &kphil)
+{
+    const double ustar_air = ustar_w * sqrt(xdiv(rho_ocn, 1.225));
+    const double z0_smooth = xdiv(0.11 * 1.0e-6, ustar_air);
+    double u = ustar_air * sqrt(1000.0);
+    bool converged = false;
+    for (int itt = 1; itt <= 20; ++itt) {
+        const double alpha_ch = fmn(0.028, 0.0017 * u + -0.005);
+        const double z0w = fmx(z0_smooth + xdiv(alpha_ch * (ustar_air * ustar_air), GRAVITY), 1.0e-10);
+        const double u_new = xdiv(ustar_air * sm_log(xdiv(10.0, z0w)), 0.40);
+        if (fabs(u_new - u) <= 1.0e-3 * u) {
+            u = u_new;
+            converged = true;
+            break;
+        }
+        u = u_new;
+    }
+    if (!converged) u = 25.82 * ustar_air;
+    ustokes = 0.0162 * u;
+    const double hm0 = 0.0246 * u * u;
+    const double f_mean = xdiv(1.296 * 0.877 * GRAVITY, 2.0 * PI_D * 1.075 * u);
+    const double vstokes = 0.125 * PI_D * 0.667 * f_mean * hm0 * hm0;
+    kphil = xdiv(0.176 * ustokes, fmx(vstokes, 1.0e-30));
+}
+
+// one_m_exp_x: (1 - exp(-x))/x, a series below 1e-4
+__device__ __forceinline__ double one_m_exp_x(double x)
+{
+    if (x < 1.0e-4) return 1.0 - x * (0.5 - xdiv(x, 6.0));
+    return xdiv(1.0 - sm_exp(-x), x);
+}
+
+// epbl_lf17_la: the Langmuir number of the Stokes drift averaged over zsl
+__device__ __forceinline__ double lf17_la(double ustar_w, double zsl, double ustokes, double kphil)
+{
+    const double xkz = kphil * zsl;
+    const double root2kz = sqrt(2.0 * xkz);
+    const double r1 = (0.302 - 1.68 * xkz) * one_m_exp_x(2.0 * xkz);
+    const double r3 = (0.1264 + 0.64 * xkz) * one_m_exp_x(5.12 * xkz);
+    const double sqrt_pi = sqrt(PI_D);
+    double r5;
+    if (root2kz > 1.0e-3) {
+        const double ec1 = sm_erfc(root2kz);
+        const double ec2 = sm_erfc(1.6 * root2kz);
+        r5 = sqrt_pi * (root2kz * (-0.84 * ec1 + 0.2 * ec2) + xdiv(0.1182 * (ec2 - ec1), root2kz));
+    } else {
+        r5 = -0.64 * sqrt_pi * root2kz + (-0.14184 + 1.0839648 * root2kz * root2kz);
+    }
+    const double ustokes_sl = fmx(ustokes * (0.715 + r1 + r3 + r5), 1.0e-10);
+    return sqrt(xdiv(ustar_w, ustokes_sl));
+}
+
+// epbl_lt_enhance: La modified by the Ekman and Obukhov depth ratios, then
+// mstar rescaled (capped) or incremented
+__device__ __forceinline__ double lt_enhance(const vphys_config &c, double la, double b0, double ustar, double bld,
+                                             double absf, double mstar)
+{
+    const double vonkar = c.epbl_von_karman;
+    const double mld_ek = xdiv(bld * absf, ustar);
+    const double ek_ob = xdiv(fabs(b0 * vonkar), fmx(absf, 1.0e-20) * ustar * ustar);
+    const double mld_ob = xdiv(fabs(bld * b0 * vonkar), ustar * ustar * ustar);
+    const double lac_ek = (b0 >= 0.0) ? c.epbl_lt_lac4 : c.epbl_lt_lac5;
+    const double lac_ob = (b0 >= 0.0) ? c.epbl_lt_lac2 : c.epbl_lt_lac3;
+    double la_mod = la * ((1.0 + fmx(-0.5, c.epbl_lt_lac1 * mld_ek)) + lac_ek * ek_ob + lac_ob * mld_ob);
+    la_mod = fmx(la_mod, 1.0e-10);
+    if (c.epbl_lt_scheme == 2) return mstar + c.epbl_lt_enhance_coef * sm_pow(la_mod, c.epbl_lt_enhance_exp);
+    return mstar * fmn(c.epbl_lt_max_enhance, 1.0 + c.epbl_lt_enhance_coef * sm_pow(la_mod, c.epbl_lt_enhance_exp));
+}
+
 // sw_pe_cost_shape (rdb_ocean_surface_flux.F90:1417-1449): the share of the
 // skin PE cost that homogenising an exponential in-layer heating of optical
 // depth tau incurs; Taylor branch below tau = 1e-2
@@ -211,6 +284,9 @@ __global__ void __launch_bounds__(128, 4) k_epbl(const Params p, double dt, doub
     const double absf = sqrt((1.0 - c.epbl_omega_frac) * (f * f) + c.epbl_omega_frac * 4.0 * (c.epbl_omega * c.epbl_omega));
     const double idecay = xdiv(c.epbl_tke_decay * absf, ustar);
     const double mech_in = dt * rho0 * (ustar * ustar * ustar);
+    // the LF17 wave state depends on u* alone: once per column
+    double la_val = 0.0, lt_ustokes = 0.0, lt_kphil = 0.0;
+    if (c.epbl_use_lt) lf17_wave_state(ustar, rho0, lt_ustokes, lt_kphil);
 
     double mld_found = 0.0;
     if (p.wet[col] <= 0.0 || h_sum <= 2.0 * H_NEGLECT) {
@@ -223,7 +299,11 @@ __global__ void __launch_bounds__(128, 4) k_epbl(const Params p, double dt, doub
         const int n_its = c.epbl_mld_iteration ? c.epbl_mld_max_its : 1;
         double dt_h = 0.0;   // carried from interface to interface, as the reference's local
         for (int obl_it = 1; obl_it <= n_its; ++obl_it) {
-            const double mstar_val = find_mstar(c, b0, ustar, mld_guess, absf);
+            double mstar_val = find_mstar(c, b0, ustar, mld_guess, absf);
+            if (c.epbl_use_lt) {
+                la_val = lf17_la(ustar, c.epbl_la_frac_hbl * mld_guess, lt_ustokes, lt_kphil);
+                mstar_val = lt_enhance(c, la_val, b0, ustar, mld_guess, absf, mstar_val);
+            }
             double mech_tke = mstar_val * mech_in;
             double conv_perel;
             if (ctke_sfc <= 0.0) {
@@ -398,6 +478,7 @@ __global__ void __launch_bounds__(128, 4) k_epbl(const Params p, double dt, doub
     }
     for (int k = 1; k <= nz + 1; ++k) kdg[P * (size_t)(k - 1)] = kd[k];
     p.mld_epbl[col] = mld_found;
+    if (p.la_epbl) p.la_epbl[col] = la_val;
 }
 
 }  // namespace

@@ -48,6 +48,7 @@ struct Params {
     const double *coriolis;           // (nx, ny) f, or nullptr (learned KPP features, kappa-shear f^2)
     double *kd_shear, *tke_shear;     // (nx, ny, nz+1) kappa-shear diffusivity and TKE, or nullptr
     double *kd_epbl, *mld_epbl;       // (nx, ny, nz+1) EPBL diffusivity, (nx, ny) its MLD, or nullptr
+    double *la_epbl;                  // (nx, ny) EPBL Langmuir number, or nullptr
     const float *kpp_pred;            // per column: the surrogate's h_b, < 0: run pass 1; nullptr: plain KPP
     const float *kpp_check;           // per column: h_b to compare with pass 1 (>= 0), or nullptr
     unsigned long long *kpp_stats;    // learned KPP counters (k_kpp_roll)

@@ -3,9 +3,9 @@
 Reads tests/test_safe_math_golden.inc of the reference (Roundabout; the
 table generated by its tools/gen_safe_math_golden.F90 from contraction-off
 builds) and writes tests/golden/safe_math_golden.json with the CBRT, ATAN,
-EXP and LOG rows, each [argument_bits, result_bits], and the POW and POWBIG
+EXP, LOG and ERFC rows, each [argument_bits, result_bits], and the POW and POWBIG
 rows, each [x_bits, y_bits, result_bits], as 16-hex-digit IEEE binary64 words.  These pin the oracle's port of rdb_sm_cbrt / rdb_sm_atan /
-rdb_sm_exp / rdb_sm_log / rdb_sm_pow bit for bit.
+rdb_sm_exp / rdb_sm_log / rdb_sm_pow / rdb_sm_erfc bit for bit.
 
 Usage (in a container where the reference tree is mounted):
     python tests/golden/make_safe_math_golden.py /path/to/roundabout
@@ -33,7 +33,8 @@ def main():
     text = (ref / "tests" / "test_safe_math_golden.inc").read_text()
     out = {"source": "tests/test_safe_math_golden.inc (reference)",
            "cbrt": parse(text, "CBRT"), "atan": parse(text, "ATAN"), "exp": parse(text, "EXP"),
-           "log": parse(text, "LOG"), "pow": parse(text, "POW"), "powbig": parse(text, "POWBIG")}
+           "log": parse(text, "LOG"), "pow": parse(text, "POW"), "powbig": parse(text, "POWBIG"),
+           "erfc": parse(text, "ERFC")}
     dst = Path(__file__).with_name("safe_math_golden.json")
     dst.write_text(json.dumps(out, indent=1) + "\n")
     print("wrote", dst, {k: len(v) for k, v in out.items() if isinstance(v, list)})

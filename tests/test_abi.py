@@ -102,7 +102,7 @@ def test_kappa_shear_knobs_are_validated(lib):
 def test_epbl_knobs_are_validated(lib):
     """EPBL's unbuilt options are refused at create (no device work)."""
     from roundabout_b200 import _ffi
-    from roundabout_b200.config import EPBL, default_config
+    from roundabout_b200.config import EPBL, Langmuir, default_config
 
     h = ctypes.c_void_p()
     for over in (dict(epbl_mstar_scheme=4), dict(learned_kpp=1), dict(epbl_combine=4), dict(epbl_mld_max_its=0),
@@ -118,5 +118,7 @@ def test_epbl_knobs_are_validated(lib):
     assert EPBL(mstar_scheme="rh18").apply(default_config()).epbl_mstar_scheme == 3
     with pytest.raises(ValueError):
         EPBL(mstar_scheme="rh19")
-    with pytest.raises(NotImplementedError):
+    with pytest.raises(TypeError):
         EPBL(langmuir=object())
+    lt = EPBL(langmuir=Langmuir(scheme="additive", coef=0.3)).apply(default_config())
+    assert (lt.epbl_use_lt, lt.epbl_lt_scheme, lt.epbl_lt_enhance_coef) == (1, 2, 0.3)

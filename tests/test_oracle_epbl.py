@@ -227,3 +227,49 @@ def test_mixing_length_exponent(oracle):
     want = (0.1 + 0.9 * fr ** 3) / (0.1 + 0.9 * fr ** 2)
     assert kd_top[2.0] > 0.0
     assert abs(kd_top[3.0] / kd_top[2.0] - want) < 1e-12, (kd_top, want)
+
+
+def test_lf17_spot_values(oracle):
+    """epbl_lf17_wave_state + epbl_lf17_la against the reference's prototype
+    values (test_ocean_epbl.F90:604-627): U10 within 2 %, La within 1 %."""
+    import ctypes
+
+    L = oracle.lib()
+    for ustar, bld, la_ref, u10_ref in ((0.005, 20.0, 0.4129, 5.08), (0.01, 20.0, 0.3627, 8.51),
+                                        (0.01, 50.0, 0.4372, 8.51), (0.02, 50.0, 0.3947, 14.01)):
+        u10, la = ctypes.c_double(), ctypes.c_double()
+        L.vpo_epbl_lf17(ustar, RHO0, 0.04 * bld, ctypes.byref(u10), ctypes.byref(la))
+        assert abs(u10.value - u10_ref) < 0.02 * u10_ref, (ustar, u10.value)
+        assert abs(la.value - la_ref) < 0.01 * la_ref, (ustar, bld, la.value)
+
+
+def test_lt_enhancement_monotone(oracle):
+    """epbl_lt_enhance, rescale scheme (test_ocean_epbl.F90:629-661): a
+    smaller La enhances more, the cap holds for a tiny La, and
+    1 + 0.447 * 0.3^-1.33 by hand (all lac_i = 0, B0 = 0, f = 0)."""
+    import ctypes
+
+    L = oracle.lib()
+    cfg = epbl_config(epbl_use_lt=1, epbl_lt_scheme=1, epbl_lt_lac1=0.0, epbl_lt_lac2=0.0, epbl_lt_lac3=0.0,
+                      epbl_lt_lac4=0.0, epbl_lt_lac5=0.0)
+    m = {la: L.vpo_epbl_lt_enhance(ctypes.byref(cfg), la, 0.0, 0.01, 50.0, 0.0, 1.0) for la in (0.6, 0.3, 0.01)}
+    assert m[0.6] > 1.0
+    assert m[0.3] > m[0.6]
+    assert abs(m[0.01] - 5.0) < 1e-12
+    assert abs(m[0.3] - (1.0 + 0.447 * 0.3 ** -1.33)) < 1e-12
+
+
+def test_lt_deepens_wind_mixing(oracle):
+    """Langmuir enhancement deepens the wind-mixed layer by over 10 %, La
+    stays in the wind-sea range, and La is 0 with it off
+    (test_ocean_epbl.F90:663-716)."""
+    nz, dz, dt = 80, 3.0, 1800.0
+    dtdz = 1.0e-4 * RHO0 / (G * ALPHA_LIN)
+    off = stratified(oracle, nz, dz, 15.0, dtdz)
+    a, _ = run_steps(off, epbl_config(), dt, 48, 12, stress=RHO0 * 0.01 ** 2)
+    on = stratified(oracle, nz, dz, 15.0, dtdz)
+    cfg = epbl_config(epbl_use_lt=1, epbl_lt_scheme=1, epbl_lt_lac1=0.0, epbl_lt_lac4=0.0, epbl_lt_lac5=0.0)
+    b, _ = run_steps(on, cfg, dt, 48, 12, stress=RHO0 * 0.01 ** 2)
+    assert b[-1] > 1.1 * a[-1], (a[-1], b[-1])
+    assert 0.2 < on.la_epbl[0, 0] < 0.6, on.la_epbl[0, 0]
+    assert abs(off.la_epbl[0, 0]) < 1e-30

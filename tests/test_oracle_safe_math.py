@@ -18,9 +18,10 @@ def d2h(x):
     return struct.pack(">d", x).hex().upper()
 
 
-@pytest.mark.parametrize("fn", ["cbrt", "atan", "exp", "log"])
+@pytest.mark.parametrize("fn", ["cbrt", "atan", "exp", "log", "erfc"])
 def test_golden_bits(oracle, fn):
-    f = {"cbrt": oracle.sm_cbrt, "atan": oracle.sm_atan, "exp": oracle.sm_exp, "log": oracle.sm_log}[fn]
+    f = {"cbrt": oracle.sm_cbrt, "atan": oracle.sm_atan, "exp": oracle.sm_exp, "log": oracle.sm_log,
+         "erfc": oracle.sm_erfc}[fn]
     bad = []
     for arg, res in GOLD[fn]:
         got = d2h(f(h2d(arg)))
