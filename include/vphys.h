@@ -256,6 +256,11 @@ typedef struct vphys_config {
     double epbl_lt_lac3;      /* 0 */
     double epbl_lt_lac4;      /* 0.95 */
     double epbl_lt_lac5;      /* 0.95 */
+    /* 1: vphys_epbl also writes the TKE budget of the last MLD iteration per
+     * column, W m-2, into the EPBL_TKE_* fields (tke_diags,
+     * rdb_ocean_epbl.F90:1647-1654); wind + conv + forcing - mixing -
+     * mech_decay - conv_decay = 0 to round-off */
+    int epbl_tke_diags;       /* 0 */
 } vphys_config;
 
 #define VPHYS_KPP_SW_ALL 1
@@ -302,6 +307,12 @@ enum vphys_field {
                                    iteration when epbl_mld_use_prev_guess) */
     VPHYS_FIELD_LA_EPBL = 34,   /* out     (nx, ny) EPBL Langmuir number of the last MLD iteration (0 when
                                    epbl_use_lt is 0) */
+    VPHYS_FIELD_EPBL_TKE_WIND = 35,       /* out (nx, ny) W m-2: mstar u*^3 rho0 (epbl_tke_diags) */
+    VPHYS_FIELD_EPBL_TKE_CONV = 36,       /* out (nx, ny) convective release, nstar-weighted */
+    VPHYS_FIELD_EPBL_TKE_FORCING = 37,    /* out (nx, ny) <= 0: surface stabilisation paid from the wind */
+    VPHYS_FIELD_EPBL_TKE_MIXING = 38,     /* out (nx, ny) spent raising potential energy */
+    VPHYS_FIELD_EPBL_TKE_MECH_DECAY = 39, /* out (nx, ny) mechanical TKE decayed (and left at the bed) */
+    VPHYS_FIELD_EPBL_TKE_CONV_DECAY = 40, /* out (nx, ny) convective TKE lost to rotation (and left at the bed) */
     VPHYS_FIELD_TRACER0 = 64    /* in/out  (nx, ny, nz); tracer t is
                                    VPHYS_FIELD_TRACER0 + t */
 };

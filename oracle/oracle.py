@@ -28,7 +28,7 @@ class VpoState(ctypes.Structure):
                           "visc_rem_u", "visc_rem_v", "gamma_t", "gamma_s", "heat_budget", "salt_budget")
     ] + [(n, _ip) for n in ("k_top_u", "k_top_v", "k_bot_u", "k_bot_v")] + [("tr", ctypes.POINTER(_dp))] + [
         (n, _dp) for n in ("heat_budget_surface", "salt_budget_surface", "coriolis", "kd_shear", "tke_shear", "kd_epbl",
-                          "mld_epbl", "la_epbl")]
+                          "mld_epbl", "la_epbl")] + [("epbl_tke", _dp * 6)]
 
 
 def build(force: bool = False) -> Path:
@@ -131,6 +131,7 @@ class OracleState:
         self.kd_epbl = f(nx, ny, nz + 1)
         self.mld_epbl = f(nx, ny)
         self.la_epbl = f(nx, ny)
+        self.epbl_tke = [f(nx, ny) for _ in range(6)]   # wind, conv, forcing, mixing, mech_decay, conv_decay
         self.k_top_u = np.full((nx + 1, ny), nz, dtype=np.int32, order="F")
         self.k_top_v = np.full((nx, ny + 1), nz, dtype=np.int32, order="F")
         self.k_bot_u = np.ones((nx + 1, ny), dtype=np.int32, order="F")
@@ -157,6 +158,7 @@ class OracleState:
                 a = getattr(self, name)
                 assert a.flags.f_contiguous, name
                 setattr(s, name, a.ctypes.data_as(typ))
+        s.epbl_tke = (_dp * 6)(*[a.ctypes.data_as(_dp) for a in self.epbl_tke])
         self._trp = (_dp * max(1, self.ntr))(*[t.ctypes.data_as(_dp) for t in self.tracers])
         s.tr = ctypes.cast(self._trp, ctypes.POINTER(_dp))
         return s
@@ -177,6 +179,7 @@ class OracleState:
             if isinstance(v, np.ndarray):
                 setattr(o, k, v.copy(order="F"))
         o.tracers = [t.copy(order="F") for t in self.tracers]
+        o.epbl_tke = [t.copy(order="F") for t in self.epbl_tke]
         return o
 
 

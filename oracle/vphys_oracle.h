@@ -47,6 +47,7 @@ typedef struct vpo_state {
     double *kd_epbl;                        /* (nx,ny,nz+1) EPBL kd_int */
     double *mld_epbl;                       /* (nx,ny) EPBL mixed-layer depth */
     double *la_epbl;                        /* (nx,ny) EPBL Langmuir number */
+    double *epbl_tke[6];                    /* (nx,ny) EPBL TKE budget terms, written when epbl_tke_diags */
 } vpo_state;
 
 void vpo_set_threads(int n);

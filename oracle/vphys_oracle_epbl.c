@@ -7,8 +7,8 @@
  * and RH18 velocity scales, the MLD iteration (false position / bisection,
  * optionally seeded by the previous MLD), the mixing-length shape, the two-band penetrating-shortwave TKE ledger (on whenever
  * sw_pen_frac != 0, source Q_heat, bed row k_bot = 1), and the three merges
- * (add, max, max_shear), and the LF17 Langmuir enhancement of mstar.  The
- * TKE budget diagnostics are not restated (the library has none).
+ * (add, max, max_shear), the LF17 Langmuir enhancement of mstar and the TKE
+ * budget diagnostics.
  *
  * Parity pins: the analytic and structural tests of the reference's
  * tests/test_ocean_epbl.F90 re-expressed in tests/test_oracle_epbl.py, and
@@ -363,6 +363,8 @@ void vpo_epbl(const vphys_config *c, vpo_state *s, double dt)
             if (c->epbl_use_lt) lf17_wave_state(ustar, rho0, &lt_u10, &lt_ustokes, &lt_kphil);
 
             double mld_found = 0.0;
+            /* the TKE budget of the last MLD iteration (:1641-1654) */
+            double d_wind = 0.0, d_conv = 0.0, d_forcing = 0.0, d_mixing = 0.0, d_mdecay = 0.0, d_cdecay = 0.0;
             if (C2(s->wet, i, j) <= 0.0 || h_sum <= 2.0 * H_NEGLECT) {
                 for (int k = 1; k <= nz + 1; ++k) C3(s->kd_epbl, i, j, k) = 0.0;
             } else {
@@ -375,19 +377,23 @@ void vpo_epbl(const vphys_config *c, vpo_state *s, double dt)
                 const int n_its = c->epbl_mld_iteration ? c->epbl_mld_max_its : 1;
                 double dt_h = 0.0;   /* carried between interfaces (the Fortran local) */
                 for (int obl_it = 1; obl_it <= n_its; ++obl_it) {
+                    d_wind = d_conv = d_forcing = d_mixing = d_mdecay = d_cdecay = 0.0;
                     double mstar_val = find_mstar(c, b0, ustar, mld_guess, absf);
                     if (c->epbl_use_lt) {
                         la_val = lf17_la(ustar, c->epbl_la_frac_hbl * mld_guess, lt_ustokes, lt_kphil);
                         mstar_val = lt_enhance(c, la_val, b0, ustar, mld_guess, absf, mstar_val);
                     }
                     double mech_tke = mstar_val * mech_in;
+                    d_wind = mech_tke;
                     double conv_perel;
                     if (ctke_sfc <= 0.0) {
                         const double forcing_clip = fmx(ctke_sfc, -mech_tke);
                         mech_tke = mech_tke + forcing_clip;
                         conv_perel = 0.0;
+                        d_forcing = forcing_clip;
                     } else {
                         conv_perel = ctke_sfc;
+                        d_conv = c->epbl_nstar * ctke_sfc;
                     }
                     double h_ka = C3(s->h, i, j, k_sfc) + H_NEGLECT;
                     double hp_a = h_ka;
@@ -409,13 +415,17 @@ void vpo_epbl(const vphys_config *c, vpo_state *s, double dt)
                         int sfc_disconnect = 0;
                         /* (1) mechanical TKE decays across the layer above */
                         const double exp_kh = vpo_sm_exp(-h_ka * idecay);
+                        d_mdecay = d_mdecay + (1.0 - exp_kh) * mech_tke;
                         mech_tke = mech_tke * exp_kh;
                         /* (2) the layer below accrues its shortwave cost: a release
                          * (> 0) joins the convective reservoir */
                         double ctke_sw_kb = 0.0;
                         if (sw_on) {
                             ctke_sw_kb = ctke_sw[kb];
-                            if (ctke_sw_kb > 0.0) conv_perel = conv_perel + ctke_sw_kb;
+                            if (ctke_sw_kb > 0.0) {
+                                conv_perel = conv_perel + ctke_sw_kb;
+                                d_conv = d_conv + c->epbl_nstar * ctke_sw_kb;
+                            }
                         }
                         /* (3) rotation-reduced convective efficiency */
                         double nstar_fc = c->epbl_nstar;
@@ -429,11 +439,15 @@ void vpo_epbl(const vphys_config *c, vpo_state *s, double dt)
                          * drained in proportion */
                         if (sw_on && ctke_sw_kb < 0.0) {
                             if (ctke_sw_kb + tot_tke < 0.0) {
+                                d_mixing = d_mixing + tot_tke;
+                                d_cdecay = d_cdecay + (c->epbl_nstar - nstar_fc) * conv_perel;
                                 tot_tke = 0.0;
                                 mech_tke = 0.0;
                                 conv_perel = 0.0;
                             } else {
                                 const double r_sw = (tot_tke + ctke_sw_kb) / tot_tke;
+                                d_mixing = d_mixing - ctke_sw_kb;
+                                d_cdecay = d_cdecay + (1.0 - r_sw) * (c->epbl_nstar - nstar_fc) * conv_perel;
                                 tot_tke = r_sw * tot_tke;
                                 mech_tke = r_sw * mech_tke;
                                 conv_perel = r_sw * conv_perel;
@@ -490,6 +504,7 @@ void vpo_epbl(const vphys_config *c, vpo_state *s, double dt)
                                     dpe_conv = pe_g0;
                                 }
                                 conv_perel = conv_perel - dpe_conv;
+                                d_conv = d_conv - c->epbl_nstar * dpe_conv;
                                 if (sfc_connected) mld_output = mld_output + C3(s->h, i, j, kb);
                             } else {
                                 /* (8b) stable: energy-limited Kd; drain the reservoirs */
@@ -507,6 +522,8 @@ void vpo_epbl(const vphys_config *c, vpo_state *s, double dt)
                                 if (frac_bl < 1.0) sfc_disconnect = 1;
                                 double r_reduc = 0.0;
                                 if (tot_tke > 0.0 && tot_tke > tke_used) r_reduc = (tot_tke - tke_used) / tot_tke;
+                                d_mixing = d_mixing + tke_used;
+                                d_cdecay = d_cdecay + (1.0 - r_reduc) * (c->epbl_nstar - nstar_fc) * conv_perel;
                                 mech_tke = r_reduc * mech_tke;
                                 conv_perel = r_reduc * conv_perel;
                             }
@@ -543,6 +560,9 @@ void vpo_epbl(const vphys_config *c, vpo_state *s, double dt)
                         pres_int = pres_int + GRAVITY * rho0 * C3(s->h, i, j, kb);
                     }
                     C3(s->kd_epbl, i, j, 1) = 0.0;
+                    /* the stocks left at the bed count as dissipated */
+                    d_mdecay = d_mdecay + mech_tke;
+                    d_cdecay = d_cdecay + c->epbl_nstar * conv_perel;
                     mld_found = mld_output;
                     if (!c->epbl_mld_iteration) break;
                     if (fabs(mld_found - mld_guess) < c->epbl_mld_tol) break;
@@ -568,6 +588,11 @@ void vpo_epbl(const vphys_config *c, vpo_state *s, double dt)
             }
             C2(s->mld_epbl, i, j) = mld_found;
             if (s->la_epbl) C2(s->la_epbl, i, j) = la_val;
+            if (c->epbl_tke_diags) {
+                const double d[6] = {d_wind, d_conv, d_forcing, d_mixing, d_mdecay, d_cdecay};
+                for (int q = 0; q < 6; ++q)
+                    if (s->epbl_tke[q]) C2(s->epbl_tke[q], i, j) = d[q] / dt;
+            }
         }
     }
 }

@@ -70,6 +70,7 @@ FIELD_TKE_SHEAR = 31
 FIELD_KD_EPBL = 32
 FIELD_MLD_EPBL = 33
 FIELD_LA_EPBL = 34
+FIELD_EPBL_TKE = {"wind": 35, "conv": 36, "forcing": 37, "mixing": 38, "mech_decay": 39, "conv_decay": 40}
 FIELD_TRACER0 = 64
 
 FIELD_NAMES = {
@@ -84,6 +85,7 @@ FIELD_NAMES = {
     "heat_budget_surface": FIELD_HEAT_BUDGET_SURFACE, "salt_budget_surface": FIELD_SALT_BUDGET_SURFACE,
     "kd_shear": FIELD_KD_SHEAR, "tke_shear": FIELD_TKE_SHEAR, "kd_epbl": FIELD_KD_EPBL, "mld_epbl": FIELD_MLD_EPBL,
     "la_epbl": FIELD_LA_EPBL,
+    **{f"epbl_tke_{k}": v for k, v in FIELD_EPBL_TKE.items()},
 }
 INT_FIELDS = (FIELD_K_TOP_U, FIELD_K_TOP_V, FIELD_K_BOT_U, FIELD_K_BOT_V)
 
@@ -101,7 +103,7 @@ def field_shape(field: int, nx: int, ny: int, nz: int):
                  FIELD_KD_EPBL):
         return (nx, ny, nz + 1)
     if field in (FIELD_BL_DEPTH, FIELD_B0, FIELD_STRESS_MAG, FIELD_Q_HEAT, FIELD_Q_SALT, FIELD_WET, FIELD_CORIOLIS,
-                 FIELD_MLD_EPBL, FIELD_LA_EPBL):
+                 FIELD_MLD_EPBL, FIELD_LA_EPBL) or field in FIELD_EPBL_TKE.values():
         return (nx, ny)
     if field in (FIELD_TAU_X, FIELD_LAMBDA_BOT_U, FIELD_K_TOP_U, FIELD_K_BOT_U):
         return (nx + 1, ny)
@@ -156,7 +158,8 @@ class VphysConfig(ctypes.Structure):
         "epbl_rh18_cn3", "epbl_rh18_cs1", "epbl_rh18_cs2")] + [
         ("epbl_use_lt", ctypes.c_int), ("epbl_lt_scheme", ctypes.c_int)] + [(n, ctypes.c_double) for n in (
             "epbl_lt_enhance_coef", "epbl_lt_enhance_exp", "epbl_lt_max_enhance", "epbl_la_frac_hbl",
-            "epbl_lt_lac1", "epbl_lt_lac2", "epbl_lt_lac3", "epbl_lt_lac4", "epbl_lt_lac5")]
+            "epbl_lt_lac1", "epbl_lt_lac2", "epbl_lt_lac3", "epbl_lt_lac4", "epbl_lt_lac5")] + [
+        ("epbl_tke_diags", ctypes.c_int)]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_ if n not in ()}

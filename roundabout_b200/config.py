@@ -149,6 +149,7 @@ def default_config() -> VphysConfig:
     c.epbl_lt_lac3 = 0.0
     c.epbl_lt_lac4 = 0.95
     c.epbl_lt_lac5 = 0.95
+    c.epbl_tke_diags = 0
     return c
 
 

@@ -50,7 +50,7 @@ int cuda_status(cudaError_t e, const char *where)
     return push_error(VPHYS_ERR_CUDA, "%s: CUDA error %d (%s)", where, (int)e, cudaGetErrorString(e));
 }
 
-constexpr int NFIXED = 35;
+constexpr int NFIXED = 41;
 constexpr unsigned MAGIC = 0x56504859u;   // "VPHY"
 
 struct Field {
@@ -140,7 +140,13 @@ size_t field_count(int nx, int ny, int nz, int field, bool *is_int)
     case VPHYS_FIELD_WET:
     case VPHYS_FIELD_CORIOLIS:
     case VPHYS_FIELD_MLD_EPBL:
-    case VPHYS_FIELD_LA_EPBL: return X * Y;
+    case VPHYS_FIELD_LA_EPBL:
+    case VPHYS_FIELD_EPBL_TKE_WIND:
+    case VPHYS_FIELD_EPBL_TKE_CONV:
+    case VPHYS_FIELD_EPBL_TKE_FORCING:
+    case VPHYS_FIELD_EPBL_TKE_MIXING:
+    case VPHYS_FIELD_EPBL_TKE_MECH_DECAY:
+    case VPHYS_FIELD_EPBL_TKE_CONV_DECAY: return X * Y;
     case VPHYS_FIELD_TAU_X:
     case VPHYS_FIELD_LAMBDA_BOT_U: return (X + 1) * Y;
     case VPHYS_FIELD_TAU_Y:
@@ -273,6 +279,8 @@ int validate(const vphys_config *c, int ntr)
             return push_error(VPHYS_ERR_CONFIG, "epbl_combine must be 1 (add), 2 (max) or 3 (max_shear)");
         if (c->learned_kpp) return push_error(VPHYS_ERR_CONFIG, "EPBL replaces KPP: learned_kpp must be 0");
         if (c->epbl_use_lt < 0 || c->epbl_use_lt > 1) return push_error(VPHYS_ERR_CONFIG, "epbl_use_lt must be 0 or 1");
+        if (c->epbl_tke_diags < 0 || c->epbl_tke_diags > 1)
+            return push_error(VPHYS_ERR_CONFIG, "epbl_tke_diags must be 0 or 1");
         if (c->epbl_use_lt && (c->epbl_lt_scheme < 1 || c->epbl_lt_scheme > 2))
             return push_error(VPHYS_ERR_CONFIG, "epbl_lt_scheme must be 1 (rescale) or 2 (additive)");
         if (c->epbl_mld_max_its < 1 || c->epbl_mld_max_its > 1000)
@@ -336,6 +344,7 @@ Params make_params(vphys_handle h)
     p.kd_epbl = D(VPHYS_FIELD_KD_EPBL);
     p.mld_epbl = D(VPHYS_FIELD_MLD_EPBL);
     p.la_epbl = D(VPHYS_FIELD_LA_EPBL);
+    for (int d = 0; d < 6; ++d) p.epbl_tke[d] = h->cfg.epbl_tke_diags ? D(VPHYS_FIELD_EPBL_TKE_WIND + d) : nullptr;
     p.ks_equals_kt = (h->cfg.bkgnd_profile || h->cfg.kt_bg == h->cfg.ks_bg) ? 1 : 0;
     p.write_gamma = (p.gamma_t && p.gamma_s) ? 1 : 0;
     return p;
@@ -454,6 +463,9 @@ int prepare_epbl(vphys_handle h)
     int st = VPHYS_OK;
     if ((st = ensure(h, VPHYS_FIELD_KD_EPBL))) return st;
     if ((st = ensure(h, VPHYS_FIELD_LA_EPBL))) return st;
+    if (h->cfg.epbl_tke_diags)
+        for (int d = 0; d < 6; ++d)
+            if ((st = ensure(h, VPHYS_FIELD_EPBL_TKE_WIND + d))) return st;
     return ensure(h, VPHYS_FIELD_MLD_EPBL);
 }
 

@@ -289,6 +289,8 @@ __global__ void __launch_bounds__(128, 4) k_epbl(const Params p, double dt, doub
     if (c.epbl_use_lt) lf17_wave_state(ustar, rho0, lt_ustokes, lt_kphil);
 
     double mld_found = 0.0;
+    // the TKE budget of the last MLD iteration (:1641-1654), kept when asked for
+    double d_wind = 0.0, d_conv = 0.0, d_forcing = 0.0, d_mixing = 0.0, d_mdecay = 0.0, d_cdecay = 0.0;
     if (p.wet[col] <= 0.0 || h_sum <= 2.0 * H_NEGLECT) {
         for (int k = 1; k <= nz + 1; ++k) kd[k] = 0.0;
     } else {
@@ -299,18 +301,23 @@ __global__ void __launch_bounds__(128, 4) k_epbl(const Params p, double dt, doub
         const int n_its = c.epbl_mld_iteration ? c.epbl_mld_max_its : 1;
         double dt_h = 0.0;   // carried from interface to interface, as the reference's local
         for (int obl_it = 1; obl_it <= n_its; ++obl_it) {
+            d_wind = d_conv = d_forcing = d_mixing = d_mdecay = d_cdecay = 0.0;
             double mstar_val = find_mstar(c, b0, ustar, mld_guess, absf);
             if (c.epbl_use_lt) {
                 la_val = lf17_la(ustar, c.epbl_la_frac_hbl * mld_guess, lt_ustokes, lt_kphil);
                 mstar_val = lt_enhance(c, la_val, b0, ustar, mld_guess, absf, mstar_val);
             }
             double mech_tke = mstar_val * mech_in;
+            d_wind = mech_tke;
             double conv_perel;
             if (ctke_sfc <= 0.0) {
-                mech_tke = mech_tke + fmx(ctke_sfc, -mech_tke);
+                const double forcing_clip = fmx(ctke_sfc, -mech_tke);
+                mech_tke = mech_tke + forcing_clip;
                 conv_perel = 0.0;
+                d_forcing = forcing_clip;
             } else {
                 conv_perel = ctke_sfc;
+                d_conv = c.epbl_nstar * ctke_sfc;
             }
             double h_ka = h[k_sfc] + H_NEGLECT;
             double hp_a = h_ka;
@@ -326,10 +333,15 @@ __global__ void __launch_bounds__(128, 4) k_epbl(const Params p, double dt, doub
                 h_ka = h[ka] + H_NEGLECT;
                 const double h_kb = h[kb] + H_NEGLECT;
                 bool sfc_disconnect = false;
-                mech_tke = mech_tke * sm_exp(-h_ka * idecay);
+                const double exp_kh = sm_exp(-h_ka * idecay);
+                d_mdecay = d_mdecay + (1.0 - exp_kh) * mech_tke;
+                mech_tke = mech_tke * exp_kh;
                 // the layer below accrues its shortwave cost; a release joins the convective reservoir
                 const double ctke_sw_kb = ctke_sw[kb];
-                if (ctke_sw_kb > 0.0) conv_perel = conv_perel + ctke_sw_kb;
+                if (ctke_sw_kb > 0.0) {
+                    conv_perel = conv_perel + ctke_sw_kb;
+                    d_conv = d_conv + c.epbl_nstar * ctke_sw_kb;
+                }
                 double nstar_fc = c.epbl_nstar;
                 if (conv_perel > 0.0 && absf > 0.0) {
                     const double ah = absf * htot;
@@ -340,11 +352,15 @@ __global__ void __launch_bounds__(128, 4) k_epbl(const Params p, double dt, doub
                 // a shortwave sink is paid first, both reservoirs drained in proportion
                 if (ctke_sw_kb < 0.0) {
                     if (ctke_sw_kb + tot_tke < 0.0) {
+                        d_mixing = d_mixing + tot_tke;
+                        d_cdecay = d_cdecay + (c.epbl_nstar - nstar_fc) * conv_perel;
                         tot_tke = 0.0;
                         mech_tke = 0.0;
                         conv_perel = 0.0;
                     } else {
                         const double r_sw = xdiv(tot_tke + ctke_sw_kb, tot_tke);
+                        d_mixing = d_mixing - ctke_sw_kb;
+                        d_cdecay = d_cdecay + (1.0 - r_sw) * (c.epbl_nstar - nstar_fc) * conv_perel;
                         tot_tke = r_sw * tot_tke;
                         mech_tke = r_sw * mech_tke;
                         conv_perel = r_sw * conv_perel;
@@ -401,6 +417,7 @@ __global__ void __launch_bounds__(128, 4) k_epbl(const Params p, double dt, doub
                             dpe_conv = pe_g0;
                         }
                         conv_perel = conv_perel - dpe_conv;
+                        d_conv = d_conv - c.epbl_nstar * dpe_conv;
                         if (sfc_connected) mld_output = mld_output + h[kb];
                     } else {
                         // stable: the energy-limited Kd; the reservoirs drained
@@ -418,6 +435,8 @@ __global__ void __launch_bounds__(128, 4) k_epbl(const Params p, double dt, doub
                         if (frac_bl < 1.0) sfc_disconnect = true;
                         double r_reduc = 0.0;
                         if (tot_tke > 0.0 && tot_tke > tke_used) r_reduc = xdiv(tot_tke - tke_used, tot_tke);
+                        d_mixing = d_mixing + tke_used;
+                        d_cdecay = d_cdecay + (1.0 - r_reduc) * (c.epbl_nstar - nstar_fc) * conv_perel;
                         mech_tke = r_reduc * mech_tke;
                         conv_perel = r_reduc * conv_perel;
                     }
@@ -453,6 +472,8 @@ __global__ void __launch_bounds__(128, 4) k_epbl(const Params p, double dt, doub
                 pres_int = pres_int + g_rho0 * h[kb];
             }
             kd[1] = 0.0;
+            d_mdecay = d_mdecay + mech_tke;   // the stocks left at the bed count as dissipated
+            d_cdecay = d_cdecay + c.epbl_nstar * conv_perel;
             mld_found = mld_output;
             if (!c.epbl_mld_iteration) break;
             if (fabs(mld_found - mld_guess) < c.epbl_mld_tol) break;
@@ -479,6 +500,14 @@ __global__ void __launch_bounds__(128, 4) k_epbl(const Params p, double dt, doub
     for (int k = 1; k <= nz + 1; ++k) kdg[P * (size_t)(k - 1)] = kd[k];
     p.mld_epbl[col] = mld_found;
     if (p.la_epbl) p.la_epbl[col] = la_val;
+    if (c.epbl_tke_diags && p.epbl_tke[0]) {
+        p.epbl_tke[0][col] = xdiv(d_wind, dt);
+        p.epbl_tke[1][col] = xdiv(d_conv, dt);
+        p.epbl_tke[2][col] = xdiv(d_forcing, dt);
+        p.epbl_tke[3][col] = xdiv(d_mixing, dt);
+        p.epbl_tke[4][col] = xdiv(d_mdecay, dt);
+        p.epbl_tke[5][col] = xdiv(d_cdecay, dt);
+    }
 }
 
 }  // namespace

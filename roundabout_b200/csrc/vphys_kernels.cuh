@@ -49,6 +49,8 @@ struct Params {
     double *kd_shear, *tke_shear;     // (nx, ny, nz+1) kappa-shear diffusivity and TKE, or nullptr
     double *kd_epbl, *mld_epbl;       // (nx, ny, nz+1) EPBL diffusivity, (nx, ny) its MLD, or nullptr
     double *la_epbl;                  // (nx, ny) EPBL Langmuir number, or nullptr
+    double *epbl_tke[6];              // (nx, ny) EPBL TKE budget terms (wind, conv, forcing, mixing,
+                                      // mech_decay, conv_decay), or nullptr when not requested
     const float *kpp_pred;            // per column: the surrogate's h_b, < 0: run pass 1; nullptr: plain KPP
     const float *kpp_check;           // per column: h_b to compare with pass 1 (>= 0), or nullptr
     unsigned long long *kpp_stats;    // learned KPP counters (k_kpp_roll)

@@ -4,7 +4,8 @@ vphys_step with epbl = 1) with the CPU oracle.
 The column solve is epbl_compute -> epbl_column_kernel
 (rdb_ocean_epbl.F90:864-1659): bitwise on kd_epbl and mld_epbl for the
 OM4, RH18 and constant mstar, both velocity scales, mixing-length
-exponents 2 and 3, the LF17 Langmuir enhancement (rescale and additive), the MLD iteration with false
+exponents 2 and 3, the LF17 Langmuir enhancement (rescale and additive), the TKE budget
+diagnostics, the MLD iteration with false
 position, bisection, the previous-MLD seed or none, both EOS variants, the
 penetrating-shortwave TKE ledger, nz from 1 to 100, vanished top layers and
 land; the merges (add, max,
@@ -43,9 +44,9 @@ KNOBS = {
                               epbl_vstar_scheme=2, epbl_mstar_conv_adj=0.5, epbl_omega_frac=0.3),
     "no_iteration": dict(epbl_mld_iteration=0, epbl_mstar_cap=0.8, epbl_min_mix_len=0.5),
     "bisection_prev": dict(epbl_mld_bisection=1, epbl_mld_use_prev_guess=1, epbl_mld_max_its=7),
-    "shortwave": dict(sw_pen_frac=0.6),
+    "shortwave": dict(sw_pen_frac=0.6, epbl_tke_diags=1),
     "rh18_exponent": dict(epbl_mstar_scheme=3, epbl_mstar_cap=0.9, epbl_mixlen_exponent=3.0, epbl_vstar_scheme=2),
-    "langmuir": dict(epbl_use_lt=1),
+    "langmuir": dict(epbl_use_lt=1, epbl_tke_diags=1),
     "langmuir_additive_sw": dict(epbl_use_lt=1, epbl_lt_scheme=2, sw_pen_frac=0.5, epbl_lt_lac2=0.1),
     "shortwave_linear": dict(epbl_mstar_scheme=1, sw_pen_frac=1.0, eos_variant=1, eos_alpha_t=0.2, eos_beta_s=0.77,
                              sw_zeta1=1.5, sw_zeta2=9.0),
@@ -85,6 +86,9 @@ def test_epbl_standalone(VP, oracle, shape, thin, knobs):
     assert_bitwise("kd_epbl", vp.get("kd_epbl"), st.kd_epbl)
     assert_bitwise("mld_epbl", vp.get("mld_epbl"), st.mld_epbl)
     assert_bitwise("la_epbl", vp.get("la_epbl"), st.la_epbl)
+    if cfg.epbl_tke_diags:
+        for q, name in enumerate(("wind", "conv", "forcing", "mixing", "mech_decay", "conv_decay")):
+            assert_bitwise(f"epbl_tke_{name}", vp.get(f"epbl_tke_{name}"), st.epbl_tke[q])
     if nz >= 12:
         assert st.kd_epbl.max() > 0.0
 

@@ -273,3 +273,28 @@ def test_lt_deepens_wind_mixing(oracle):
     assert b[-1] > 1.1 * a[-1], (a[-1], b[-1])
     assert 0.2 < on.la_epbl[0, 0] < 0.6, on.la_epbl[0, 0]
     assert abs(off.la_epbl[0, 0]) < 1e-30
+
+
+@pytest.mark.parametrize("q_heat,sw", [(-300.0, 0.0), (-300.0, 1.0), (250.0, 1.0), (-50.0, 0.6)])
+def test_tke_budget_closes(oracle, q_heat, sw):
+    """The column TKE ledger closes to round-off every step
+    (test_ocean_epbl.F90:359-484): wind + conv + forcing - mixing -
+    mech_decay - conv_decay = 0 within 1e-9 of the sources, on a rotating
+    column under wind, a surface heat flux and (sw > 0) penetrating
+    shortwave charged per layer -- a heating flux drains the reservoirs
+    below the surface (the proportional and the exhausting drain), a cooling
+    one releases convective energy."""
+    nz, dz, dt = 40, 5.0, 1800.0
+    cfg = epbl_config(epbl_tke_diags=1, sw_pen_frac=sw)
+    st = stratified(oracle, nz, dz, 15.0, 0.0527, nx=3, ny=2)
+    st.coriolis[...] = 1.0e-4
+    run_steps(st, cfg, dt, 12, 12, stress=0.1, q_heat=q_heat)
+    wind, conv, forcing, mixing, mdecay, cdecay = st.epbl_tke
+    residual = wind + conv + forcing - mixing - mdecay - cdecay
+    scale = wind + conv + np.abs(forcing) + 1e-30
+    assert (np.abs(residual) < 1e-9 * scale).all(), np.abs(residual / scale).max()
+    assert (wind > 0.0).all()
+    if q_heat < 0.0:
+        assert (conv > 0.0).all()
+    else:
+        assert (forcing < 0.0).all() or (mixing > 0.0).all()
