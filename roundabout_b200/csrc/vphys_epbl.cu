@@ -54,6 +54,23 @@ __device__ __forceinline__ void specvol_derivs(const vphys_config &c, double T, 
     dsv_ds = WRIGHT_A2 + dlam_ds * inv_p - lambda * dp0_ds * inv_p2;
 }
 
+// the RH18 fit (rdb_ocean_epbl.F90:664-670)
+__device__ __noinline__ double rh18_mstar(const vphys_config &c, double b0, double ustar, double bld, double absf,
+                                          double absf_floor)
+{
+    const double msn_term = c.epbl_rh18_cn2 * sm_exp(xdiv(c.epbl_rh18_cn3 * bld * absf, ustar));
+    const double mstar_n = xdiv(c.epbl_rh18_cn1 * msn_term, 1.0 + msn_term);
+    const double b0p = fmx(0.0, b0);
+    const double u5 = (ustar * ustar) * (ustar * ustar) * ustar;
+    const double mstar_s = c.epbl_rh18_cs1 * sm_pow(xdiv(b0p * b0p * bld, u5 * absf_floor), c.epbl_rh18_cs2);
+    double mstar = mstar_n + mstar_s;
+    if (c.epbl_mstar_cap > 0.0) mstar = fmn(c.epbl_mstar_cap, mstar);
+    return mstar;
+}
+
+// fr^n for the mixing-length shape when n != 2
+__device__ __noinline__ double shape_pow(double fr, double n) { return sm_pow(fr, n); }
+
 // epbl_find_mstar: constant (1), OM4 (2), RH18 (3)
 __device__ __forceinline__ double find_mstar(const vphys_config &c, double b0, double ustar, double bld, double absf)
 {
@@ -66,13 +83,7 @@ __device__ __forceinline__ double find_mstar(const vphys_config &c, double b0, d
         mstar = fmx(mstar_s, fmn(1.25, mstar_n));
         if (c.epbl_mstar_cap > 0.0) mstar = fmn(c.epbl_mstar_cap, mstar);
     } else if (c.epbl_mstar_scheme == 3) {
-        const double msn_term = c.epbl_rh18_cn2 * sm_exp(xdiv(c.epbl_rh18_cn3 * bld * absf, ustar));
-        const double mstar_n = xdiv(c.epbl_rh18_cn1 * msn_term, 1.0 + msn_term);
-        const double b0p = fmx(0.0, b0);
-        const double u5 = (ustar * ustar) * (ustar * ustar) * ustar;
-        const double mstar_s = c.epbl_rh18_cs1 * sm_pow(xdiv(b0p * b0p * bld, u5 * absf_floor), c.epbl_rh18_cs2);
-        mstar = mstar_n + mstar_s;
-        if (c.epbl_mstar_cap > 0.0) mstar = fmn(c.epbl_mstar_cap, mstar);
+        mstar = rh18_mstar(c, b0, ustar, bld, absf, absf_floor);
     } else {
         mstar = c.epbl_mstar_const;
     }
@@ -91,7 +102,9 @@ __device__ __forceinline__ double find_mstar(const vphys_config &c, double b0, d
 // the empirical constants of the cited formulas (Li & Fox-Kemper 2017,
 // COARE 3.5), as the reference lists them at :59-71
 // epbl_lf17_wave_state: COARE fixed-point u* -> U10, Stokes drift, Phillips peak wavenumber
-__device__ __forceinline__ void lf17_wave_state(double ustar_w, double rho_ocn, double &ustokes, double &kphil)
+// The Langmuir, RH18 and general-exponent paths are off by default; they are
+// kept out of line so that their registers do not weigh on the default sweep.
+__device__ __noinline__ void lf17_wave_state(double ustar_w, double rho_ocn, double &ustokes, double &kphil)
 {
     const double ustar_air = ustar_w * sqrt(xdiv(rho_ocn, 1.225));
     const double z0_smooth = xdiv(0.11 * 1.0e-6, ustar_air);
@@ -124,7 +137,7 @@ __device__ __forceinline__ double one_m_exp_x(double x)
 }
 
 // epbl_lf17_la: the Langmuir number of the Stokes drift averaged over zsl
-__device__ __forceinline__ double lf17_la(double ustar_w, double zsl, double ustokes, double kphil)
+__device__ __noinline__ double lf17_la(double ustar_w, double zsl, double ustokes, double kphil)
 {
     const double xkz = kphil * zsl;
     const double root2kz = sqrt(2.0 * xkz);
@@ -145,8 +158,8 @@ __device__ __forceinline__ double lf17_la(double ustar_w, double zsl, double ust
 
 // epbl_lt_enhance: La modified by the Ekman and Obukhov depth ratios, then
 // mstar rescaled (capped) or incremented
-__device__ __forceinline__ double lt_enhance(const vphys_config &c, double la, double b0, double ustar, double bld,
-                                             double absf, double mstar)
+__device__ __noinline__ double lt_enhance(const vphys_config &c, double la, double b0, double ustar, double bld,
+                                          double absf, double mstar)
 {
     const double vonkar = c.epbl_von_karman;
     const double mld_ek = xdiv(bld * absf, ustar);
@@ -191,7 +204,9 @@ __device__ __forceinline__ double mixlen_kd(const vphys_config &c, double vstar,
     return xdiv(vstar * c.epbl_von_karman * num, den);
 }
 
-template <int N>   // N = bucket + 2: indices 1..nz+1 with nz <= bucket
+// N = bucket + 2 (indices 1..nz+1 with nz <= bucket); DIAG: the TKE budget
+// is kept and written (epbl_tke_diags), else its sums are dead code
+template <int N, bool DIAG>
 __global__ void __launch_bounds__(128, 4) k_epbl(const Params p, double dt, double inv_rho0_cp, double inv_rho0)
 {
     const size_t col = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
@@ -381,7 +396,7 @@ __global__ void __launch_bounds__(128, 4) k_epbl(const Params p, double dt, doub
                         if (c.epbl_mld_iteration && !(ts >= 1.0) && !(ts < 0.0) && !(mld_guess <= 0.0)) {
                             const double fr = fmx(0.0, xdiv(mld_guess - z_int, mld_guess));
                             shape_fn = (c.epbl_mixlen_exponent == 2.0) ? ts + (1.0 - ts) * fr * fr
-                                                                       : ts + (1.0 - ts) * sm_pow(fr, c.epbl_mixlen_exponent);
+                                                                       : ts + (1.0 - ts) * shape_pow(fr, c.epbl_mixlen_exponent);
                         }
                     }
                     const double hbs = fmn(hb_hs, shape_fn);
@@ -500,7 +515,7 @@ __global__ void __launch_bounds__(128, 4) k_epbl(const Params p, double dt, doub
     for (int k = 1; k <= nz + 1; ++k) kdg[P * (size_t)(k - 1)] = kd[k];
     p.mld_epbl[col] = mld_found;
     if (p.la_epbl) p.la_epbl[col] = la_val;
-    if (c.epbl_tke_diags && p.epbl_tke[0]) {
+    if (DIAG && p.epbl_tke[0]) {
         p.epbl_tke[0][col] = xdiv(d_wind, dt);
         p.epbl_tke[1][col] = xdiv(d_conv, dt);
         p.epbl_tke[2][col] = xdiv(d_forcing, dt);
@@ -520,12 +535,20 @@ void launch_epbl(const Params &p, double dt, cudaStream_t stream)
     const double inv_rho0 = 1.0 / p.cfg.rho0;
     const int threads = 128;
     const unsigned blocks = (unsigned)((p.plane + threads - 1) / threads);
-    if (p.nz <= 32)
-        k_epbl<34><<<blocks, threads, 0, stream>>>(p, dt, inv_rho0_cp, inv_rho0);
-    else if (p.nz <= 80)
-        k_epbl<82><<<blocks, threads, 0, stream>>>(p, dt, inv_rho0_cp, inv_rho0);
-    else
-        k_epbl<NZ_MAX + 2><<<blocks, threads, 0, stream>>>(p, dt, inv_rho0_cp, inv_rho0);
+    const bool diag = p.cfg.epbl_tke_diags != 0;
+#define VPHYS_EPBL_LAUNCH(NB)                                                                        \
+    if (diag)                                                                                        \
+        k_epbl<NB, true><<<blocks, threads, 0, stream>>>(p, dt, inv_rho0_cp, inv_rho0);              \
+    else                                                                                             \
+        k_epbl<NB, false><<<blocks, threads, 0, stream>>>(p, dt, inv_rho0_cp, inv_rho0)
+    if (p.nz <= 32) {
+        VPHYS_EPBL_LAUNCH(34);
+    } else if (p.nz <= 80) {
+        VPHYS_EPBL_LAUNCH(82);
+    } else {
+        VPHYS_EPBL_LAUNCH(NZ_MAX + 2);
+    }
+#undef VPHYS_EPBL_LAUNCH
 }
 
 }  // namespace vphys
