@@ -261,6 +261,13 @@ typedef struct vphys_config {
      * rdb_ocean_epbl.F90:1647-1654); wind + conv + forcing - mixing -
      * mech_decay - conv_decay = 0 to round-off */
     int epbl_tke_diags;       /* 0 */
+    /* kappa-shear: a column holding layers thinner than H_VANISHED is solved
+     * on its massive sub-grid -- vanished layers folded into a massive
+     * neighbour by thickness-weighted means, the interface results
+     * interpolated back (massless_merge, rdb_massless.F90:51-180) -- instead
+     * of flooring them at H_VANISHED; healthy columns are unchanged, bit for
+     * bit */
+    int ks_massless_merge;    /* 0 */
 } vphys_config;
 
 #define VPHYS_KPP_SW_ALL 1

@@ -82,6 +82,8 @@ def lib():
         L.vpo_epbl_lf17.restype = None
         L.vpo_epbl_lt_enhance.argtypes = [ctypes.c_void_p] + [ctypes.c_double] * 6
         L.vpo_epbl_lt_enhance.restype = ctypes.c_double
+        for name in ("vpo_massless_build_maps", "vpo_massless_merge_fields", "vpo_massless_interp_back"):
+            getattr(L, name).restype = None
         L.vpo_step.argtypes = [ctypes.c_void_p, ctypes.POINTER(VpoState), ctypes.c_double, ctypes.c_int]
         L.vpo_step.restype = ctypes.c_int
         _lib = L

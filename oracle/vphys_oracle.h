@@ -82,6 +82,11 @@ void vpo_sw_penetration(const vphys_config *c, vpo_state *s, double dt);
 /* kappa-shear, column form (vphys_oracle_kshear.c) */
 void vpo_kappa_shear(const vphys_config *c, vpo_state *s, double dt);
 void vpo_kappa_shear_merge(const vphys_config *c, vpo_state *s);
+/* the massless merge of kappa-shear, 1-based surface-down arrays */
+void vpo_massless_build_maps(const double *h, int nz, double h_min, int *nzc, double *hc, int *kc, double *kf);
+void vpo_massless_merge_fields(const double *h, const int *kc, int nz, int nzc, const double *u, const double *v,
+                               const double *t, const double *s, double *uc, double *vc, double *tc, double *sc);
+void vpo_massless_interp_back(const double *qc, const int *kc, const double *kf, int nz, double *q);
 
 /* EPBL, column form (vphys_oracle_epbl.c) */
 void vpo_epbl(const vphys_config *c, vpo_state *s, double dt);

@@ -739,6 +739,86 @@ static void ks_solve_column(const ks_par *p, int nz, double dt, double f2_val, c
     kappa_avg_sd[nz + 1] = 0.0;
 }
 
+/* ---- the massless merge (rdb_massless.F90:51-180), surface-down.  Walking
+ * down, a merged layer opens only when the current one already has mass and
+ * the incoming layer is massive: a vanished layer folds into the massive
+ * layer above it, a leading surface run into the first massive layer below,
+ * a trailing bed run into the last massive layer above. */
+static const double H_DIV_EPS = 1.0e-20;
+
+/* massless_build_maps (:51-108): merged thicknesses hc[1..nzc]; kc[k] the
+ * merged layer of layer k (kc[nz+1] = nzc+1); kf[K] the fractional position
+ * of interface K inside merged layer kc[K] (0: on a merged interface). */
+void vpo_massless_build_maps(const double *h, int nz, double h_min, int *nzc_out, double *hc, int *kc, double *kf)
+{
+    int nzc = 1;
+    hc[1] = 0.0;
+    for (int k = 1; k <= nz; ++k) {
+        if (hc[nzc] > 0.0 && h[k] > h_min) {
+            nzc = nzc + 1;
+            hc[nzc] = 0.0;
+        }
+        kc[k] = nzc;
+        hc[nzc] = hc[nzc] + h[k];
+    }
+    kc[nz + 1] = nzc + 1;
+    kf[1] = 0.0;
+    double dz_in = h[1];
+    for (int k = 2; k <= nz; ++k) {
+        if (kc[k] > kc[k - 1]) {
+            kf[k] = 0.0;
+            dz_in = h[k];
+        } else {
+            kf[k] = dz_in / fmx(hc[kc[k]], H_DIV_EPS);
+            dz_in = dz_in + h[k];
+        }
+    }
+    kf[nz + 1] = 0.0;
+    *nzc_out = nzc;
+}
+
+/* massless_merge_fields (:110-154): thickness-weighted means on the merged grid */
+void vpo_massless_merge_fields(const double *h, const int *kc, int nz, int nzc, const double *u, const double *v,
+                               const double *t, const double *s, double *uc, double *vc, double *tc, double *sc)
+{
+    double hc_acc[nzc + 2];
+    for (int kk = 1; kk <= nzc; ++kk) {
+        hc_acc[kk] = 0.0;
+        uc[kk] = 0.0;
+        vc[kk] = 0.0;
+        tc[kk] = 0.0;
+        sc[kk] = 0.0;
+    }
+    for (int k = 1; k <= nz; ++k) {
+        const int kk = kc[k];
+        hc_acc[kk] = hc_acc[kk] + h[k];
+        uc[kk] = uc[kk] + u[k] * h[k];
+        vc[kk] = vc[kk] + v[k] * h[k];
+        tc[kk] = tc[kk] + t[k] * h[k];
+        sc[kk] = sc[kk] + s[k] * h[k];
+    }
+    for (int kk = 1; kk <= nzc; ++kk) {
+        const double denom = fmx(hc_acc[kk], H_DIV_EPS);
+        uc[kk] = uc[kk] / denom;
+        vc[kk] = vc[kk] / denom;
+        tc[kk] = tc[kk] / denom;
+        sc[kk] = sc[kk] / denom;
+    }
+}
+
+/* massless_interp_back (:156-180): an interface quantity of the merged grid
+ * back on the original interfaces (lookup, or the linear blend inside a
+ * merged layer) */
+void vpo_massless_interp_back(const double *qc, const int *kc, const double *kf, int nz, double *q)
+{
+    for (int kk = 1; kk <= nz + 1; ++kk) {
+        if (kf[kk] == 0.0)
+            q[kk] = qc[kc[kk]];
+        else
+            q[kk] = (1.0 - kf[kk]) * qc[kc[kk]] + kf[kk] * qc[kc[kk] + 1];
+    }
+}
+
 static void ks_params(const vphys_config *c, ks_par *p)
 {
     p->ri_crit = c->ks_ri_crit;
@@ -795,15 +875,35 @@ void vpo_kappa_shear(const vphys_config *c, vpo_state *s, double dt)
                 }
                 double f = s->coriolis ? C2(s->coriolis, i, j) : 0.0;
                 double f2_val = f * f;
+                /* merge only when asked and the column holds a vanished layer */
+                int do_merge = 0;
+                if (c->ks_massless_merge)
+                    for (int k = 1; k <= nz; ++k)
+                        if (h_sd[k] < H_VANISHED) {
+                            do_merge = 1;
+                            break;
+                        }
                 for (int k = 1; k <= nz; ++k) {
                     int kg = nz + 1 - k;
-                    h_sd[k] = fmx(h_sd[k], H_VANISHED);
+                    if (!do_merge) h_sd[k] = fmx(h_sd[k], H_VANISHED);
                     t_sd[k] = C3(T, i, j, kg);
                     s_sd[k] = C3(S, i, j, kg);
                 }
-                ks_precompute(nz, p.lz_rescale, h_sd, idz, idz_int, hint, il2);
-                ks_solve_column(&p, nz, dt, f2_val, h_sd, u_sd, v_sd, t_sd, s_sd, idz, idz_int, hint, il2,
-                                kappa_avg_sd, tke_avg_sd);
+                if (do_merge) {
+                    int nzc, kc[n];
+                    double kf[n], hc[n], uc[n], vc[n], tc[n], sc[n], kappa_c[n], tke_c[n];
+                    vpo_massless_build_maps(h_sd, nz, H_VANISHED, &nzc, hc, kc, kf);
+                    vpo_massless_merge_fields(h_sd, kc, nz, nzc, u_sd, v_sd, t_sd, s_sd, uc, vc, tc, sc);
+                    ks_precompute(nzc, p.lz_rescale, hc, idz, idz_int, hint, il2);
+                    ks_solve_column(&p, nzc, dt, f2_val, hc, uc, vc, tc, sc, idz, idz_int, hint, il2, kappa_c,
+                                    tke_c);
+                    vpo_massless_interp_back(kappa_c, kc, kf, nz, kappa_avg_sd);
+                    vpo_massless_interp_back(tke_c, kc, kf, nz, tke_avg_sd);
+                } else {
+                    ks_precompute(nz, p.lz_rescale, h_sd, idz, idz_int, hint, il2);
+                    ks_solve_column(&p, nz, dt, f2_val, h_sd, u_sd, v_sd, t_sd, s_sd, idz, idz_int, hint, il2,
+                                    kappa_avg_sd, tke_avg_sd);
+                }
             }
             for (int k = 1; k <= nz + 1; ++k) {
                 int kg = nz + 2 - k;

@@ -159,7 +159,7 @@ class VphysConfig(ctypes.Structure):
         ("epbl_use_lt", ctypes.c_int), ("epbl_lt_scheme", ctypes.c_int)] + [(n, ctypes.c_double) for n in (
             "epbl_lt_enhance_coef", "epbl_lt_enhance_exp", "epbl_lt_max_enhance", "epbl_la_frac_hbl",
             "epbl_lt_lac1", "epbl_lt_lac2", "epbl_lt_lac3", "epbl_lt_lac4", "epbl_lt_lac5")] + [
-        ("epbl_tke_diags", ctypes.c_int)]
+        ("epbl_tke_diags", ctypes.c_int), ("ks_massless_merge", ctypes.c_int)]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_ if n not in ()}

@@ -150,6 +150,7 @@ def default_config() -> VphysConfig:
     c.epbl_lt_lac4 = 0.95
     c.epbl_lt_lac5 = 0.95
     c.epbl_tke_diags = 0
+    c.ks_massless_merge = 0
     return c
 
 

@@ -260,6 +260,8 @@ int validate(const vphys_config *c, int ntr)
     if (c->bkgnd_prandtl == 0.0)
         return push_error(VPHYS_ERR_CONFIG, "bkgnd_prandtl = 0 is refused (use -1 for off), as the reference does");
     if (c->kappa_shear < 0 || c->kappa_shear > 1) return push_error(VPHYS_ERR_CONFIG, "kappa_shear must be 0 or 1");
+    if (c->ks_massless_merge < 0 || c->ks_massless_merge > 1)
+        return push_error(VPHYS_ERR_CONFIG, "ks_massless_merge must be 0 or 1");
     // the inner solve must run at least once (the substep's adaptive-dt bands
     // read its decay lengths); both caps bound the per-column work
     if (c->ks_max_inner_it < 1 || c->ks_max_inner_it > 10000)

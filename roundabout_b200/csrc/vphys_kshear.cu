@@ -51,6 +51,110 @@ struct KsCol {
     int nwork;   // 4 per Picard iteration + 1 per projected-state sweep: the column's cost, for scheduling
 };
 
+// the massless merge's maps: the merged layer of each layer (kc[nz+1] =
+// nzc+1) and each interface's fractional position inside its merged layer.
+// Kept apart from KsCol so the solve's frame is the same with the merge off.
+template <int N>
+struct KsMap {
+    int kc[N];
+    double kf[N];
+};
+
+// ---- the massless merge (rdb_massless.F90:51-180), surface-down: walking
+// down, a merged layer opens only when the current one has mass and the
+// incoming layer is massive.  The raw column arrives in w.h, u_c, v_c, t_c,
+// s_c and is moved to scratch (w.n2p for h, u_ps, v_ps, t_ps, s_ps); the
+// merged column goes back to w.h, u_c, v_c, t_c, s_c (the thickness sums in
+// w.s2p) with the maps in m.kc / m.kf.  Returns nzc.
+template <int N>
+__device__ __noinline__ int massless_merge(KsCol<N> &w, KsMap<N> &m, int nz)
+{
+    for (int k = 1; k <= nz; ++k) {
+        w.n2p[k] = w.h[k];
+        w.u_ps[k] = w.u_c[k];
+        w.v_ps[k] = w.v_c[k];
+        w.t_ps[k] = w.t_c[k];
+        w.s_ps[k] = w.s_c[k];
+    }
+    const double *hr = w.n2p;
+    double *hc = w.h;
+    int nzc = 1;
+    hc[1] = 0.0;
+    for (int k = 1; k <= nz; ++k) {
+        if (hc[nzc] > 0.0 && hr[k] > H_VANISHED) {
+            nzc = nzc + 1;
+            hc[nzc] = 0.0;
+        }
+        m.kc[k] = nzc;
+        hc[nzc] = hc[nzc] + hr[k];
+    }
+    m.kc[nz + 1] = nzc + 1;
+    m.kf[1] = 0.0;
+    double dz_in = hr[1];
+    for (int k = 2; k <= nz; ++k) {
+        if (m.kc[k] > m.kc[k - 1]) {
+            m.kf[k] = 0.0;
+            dz_in = hr[k];
+        } else {
+            m.kf[k] = xdiv(dz_in, fmx(hc[m.kc[k]], H_DIV_EPS));
+            dz_in = dz_in + hr[k];
+        }
+    }
+    m.kf[nz + 1] = 0.0;
+    double *acc = w.s2p;
+    for (int kk = 1; kk <= nzc; ++kk) {
+        acc[kk] = 0.0;
+        w.u_c[kk] = 0.0;
+        w.v_c[kk] = 0.0;
+        w.t_c[kk] = 0.0;
+        w.s_c[kk] = 0.0;
+    }
+    for (int k = 1; k <= nz; ++k) {
+        const int kk = m.kc[k];
+        acc[kk] = acc[kk] + hr[k];
+        w.u_c[kk] = w.u_c[kk] + w.u_ps[k] * hr[k];
+        w.v_c[kk] = w.v_c[kk] + w.v_ps[k] * hr[k];
+        w.t_c[kk] = w.t_c[kk] + w.t_ps[k] * hr[k];
+        w.s_c[kk] = w.s_c[kk] + w.s_ps[k] * hr[k];
+    }
+    for (int kk = 1; kk <= nzc; ++kk) {
+        const double denom = fmx(acc[kk], H_DIV_EPS);
+        w.u_c[kk] = xdiv(w.u_c[kk], denom);
+        w.v_c[kk] = xdiv(w.v_c[kk], denom);
+        w.t_c[kk] = xdiv(w.t_c[kk], denom);
+        w.s_c[kk] = xdiv(w.s_c[kk], denom);
+    }
+    return nzc;
+}
+
+// massless_interp_back at one original interface K
+template <int N>
+__device__ __forceinline__ double interp_back(const KsMap<N> &m, const double *qc, int K)
+{
+    const int kc = m.kc[K];
+    const double kf = m.kf[K];
+    if (kf == 0.0) return qc[kc];
+    return (1.0 - kf) * qc[kc] + kf * qc[kc + 1];
+}
+
+// the scatter of a merged column: kappa and TKE interpolated back onto the
+// original interfaces, with the surface-down flip (local interface k ->
+// global 0-based nz+1-k) and 0 on the surface and the bed
+template <int N>
+__device__ __noinline__ void scatter_merged(const KsCol<N> &w, const KsMap<N> &m, int nz, double *kd, double *tke, size_t col,
+                                            size_t plane)
+{
+    kd[col + (size_t)nz * plane] = 0.0;
+    tke[col + (size_t)nz * plane] = 0.0;
+    for (int k = 2; k <= nz; ++k) {
+        const size_t kg = (size_t)(nz + 1 - k);
+        kd[col + kg * plane] = interp_back(m, w.kappa_avg, k);
+        tke[col + kg * plane] = interp_back(m, w.tke_avg, k);
+    }
+    kd[col] = 0.0;
+    tke[col] = 0.0;
+}
+
 // eos_specvol_derivs (rdb_eos.F90:1551-1622)
 __device__ __forceinline__ void specvol_derivs(const KsPar &p, double T, double S, double pres, double &dsv_dt,
                                                double &dsv_ds)
@@ -696,7 +800,9 @@ __device__ __noinline__ void solve_column(KsCol<N> &w, const KsPar &p, int nz, d
 
 // Thread t solves column order[t] (t itself without an order) and records
 // the column's cost in work[col] (0 for land) for the next call's ordering.
-template <int N>
+// MERGE instantiates the massless merge; without it the kernel carries none
+// of the merge's code (its call graph alone costs the solve registers).
+template <int N, bool MERGE>
 __global__ void __launch_bounds__(64, VPHYS_KS_MINB) k_kappa_shear(Params p, KsPar kp, double dt,
                                                                     const int *__restrict__ order, int *work)
 {
@@ -719,23 +825,47 @@ __global__ void __launch_bounds__(64, VPHYS_KS_MINB) k_kappa_shear(Params p, KsP
     w.nwork = 0;
     const double *T = p.tr[p.cfg.idx_temperature], *S = p.tr[p.cfg.idx_salinity];
     const size_t ucol = (size_t)j * (nx + 1) + i, vcol = col;
+    // the massless merge engages only when asked and the column holds a vanished layer
+    bool do_merge = false;
+    if (MERGE)
+        for (int k = 1; k <= nz; ++k)
+            if (p.h[col + (size_t)(nz - k) * plane] < H_VANISHED) {
+                do_merge = true;
+                break;
+            }
+    // gather with the flip (local k = 1 the surface) into the solve's arrays;
+    // a merged column keeps its raw thicknesses, the others the H_VANISHED floor
     for (int k = 1; k <= nz; ++k) {
         const size_t kg = (size_t)(nz - k);   // 0-based global layer of local layer k
-        w.h[k] = fmx(p.h[col + kg * plane], H_VANISHED);
+        const double hk = p.h[col + kg * plane];
+        w.h[k] = do_merge ? hk : fmx(hk, H_VANISHED);
         w.u_c[k] = 0.5 * (p.u[ucol + kg * p.plane_u] + p.u[ucol + 1 + kg * p.plane_u]);
         w.v_c[k] = 0.5 * (p.v[vcol + kg * p.plane_v] + p.v[vcol + nx + kg * p.plane_v]);
         w.t_c[k] = T[col + kg * plane];
         w.s_c[k] = S[col + kg * plane];
     }
     const double f = p.coriolis ? p.coriolis[col] : 0.0;
-    solve_column(w, kp, nz, dt, f * f);
-    // scatter with the flip: local interface k -> global interface nz+2-k
-    // (1-based), 0 on the bed and the surface
-    for (int k = 1; k <= nz + 1; ++k) {
-        const size_t kg = (size_t)(nz + 1 - k);
-        const bool edge = (k == 1 || k == nz + 1);
-        kd[col + kg * plane] = edge ? 0.0 : w.kappa_avg[k];
-        tke[col + kg * plane] = edge ? 0.0 : w.tke_avg[k];
+    KsMap<MERGE ? N : 1> m;
+    int nzs = nz;
+    if constexpr (MERGE)
+        if (do_merge) nzs = massless_merge(w, m, nz);
+    solve_column(w, kp, nzs, dt, f * f);
+    if constexpr (MERGE) {
+        if (do_merge) {
+            w.kappa_avg[1] = 0.0;   // ks_solve_column's closed top and bottom (:1905-1908), read by the interpolation
+            w.kappa_avg[nzs + 1] = 0.0;
+            scatter_merged(w, m, nz, kd, tke, col, plane);
+        }
+    }
+    if (!do_merge) {
+        // scatter with the flip: local interface k -> global interface nz+2-k
+        // (1-based), 0 on the bed and the surface
+        for (int k = 1; k <= nz + 1; ++k) {
+            const size_t kg = (size_t)(nz + 1 - k);
+            const bool edge = (k == 1 || k == nz + 1);
+            kd[col + kg * plane] = edge ? 0.0 : w.kappa_avg[k];
+            tke[col + kg * plane] = edge ? 0.0 : w.tke_avg[k];
+        }
     }
     if (work) work[col] = w.nwork;
 }
@@ -841,12 +971,19 @@ void launch_kappa_shear(const Params &p, double dt, int *work, int *order, unsig
     }
     const int threads = 64;
     const unsigned blocks = (unsigned)((n + threads - 1) / threads);
-    if (p.nz <= 32)
-        k_kappa_shear<34><<<blocks, threads, 0, stream>>>(p, kp, dt, ord, work);
-    else if (p.nz <= 80)
-        k_kappa_shear<82><<<blocks, threads, 0, stream>>>(p, kp, dt, ord, work);
-    else
-        k_kappa_shear<NZ_MAX + 2><<<blocks, threads, 0, stream>>>(p, kp, dt, ord, work);
+#define VPHYS_KS_LAUNCH(M)                                                                 \
+    if (p.nz <= 32)                                                                        \
+        k_kappa_shear<34, M><<<blocks, threads, 0, stream>>>(p, kp, dt, ord, work);        \
+    else if (p.nz <= 80)                                                                   \
+        k_kappa_shear<82, M><<<blocks, threads, 0, stream>>>(p, kp, dt, ord, work);        \
+    else                                                                                   \
+        k_kappa_shear<NZ_MAX + 2, M><<<blocks, threads, 0, stream>>>(p, kp, dt, ord, work);
+    if (p.cfg.ks_massless_merge) {
+        VPHYS_KS_LAUNCH(true)
+    } else {
+        VPHYS_KS_LAUNCH(false)
+    }
+#undef VPHYS_KS_LAUNCH
 }
 
 }  // namespace vphys

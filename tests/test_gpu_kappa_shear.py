@@ -3,8 +3,8 @@ assembly and vphys_step with kappa_shear = 1) with the CPU oracle.
 
 The column solve is kappa_shear_compute -> kappa_shear_column_kernel
 (rdb_ocean_kappa_shear.F90:427-648, solver 953-1909): bitwise on kd_shear
-and tke_shear for both EOS variants, non-default knobs, thin and vanished
-layers, land, and nz from 1 to 100; the reference's golden column
+and tke_shear for both EOS variants, non-default knobs, the massless merge of
+vanished layers, thin and vanished layers, land, and nz from 1 to 100; the reference's golden column
 (test_ocean_kappa_shear.F90:286-393) within its 1e-6 bar; the merge
 (kappa_shear_merge_into_kv_kt, :381-421) bitwise through the assembly and
 whole steps; the mixed-precision step within its 1e-6 bar.
@@ -47,17 +47,18 @@ def beta_plane(ny, nx):
 
 KNOBS = dict(eos_variant=1, eos_alpha_t=0.2, eos_beta_s=0.77, ks_vel_underflow=1.0e-3, ks_tke_bg=1.0e-12,
              ks_src_max_chg=8.0, ks_lz_rescale=0.5, ks_ri_crit=0.3, ks_max_inner_it=20, ks_max_substep_it=9)
+MERGE = dict(ks_massless_merge=1)
 
 
 @pytest.mark.parametrize("shape,thin", [((24, 20, 12), 0.0), ((30, 18, 40), 0.15), ((16, 12, 75), 0.1),
                                         ((9, 7, 1), 0.0), ((9, 7, 2), 0.0), ((11, 5, 3), 0.2), ((8, 6, 100), 0.1),
                                         ((130, 3, 33), 0.1)])
-@pytest.mark.parametrize("knobs", ["default", "knobs"])
+@pytest.mark.parametrize("knobs", ["default", "knobs", "merge"])
 def test_kappa_shear_standalone(VP, oracle, shape, thin, knobs):
     nx, ny, nz = shape
     cols = columns(nx=nx, ny=ny, nz=nz, seed=nx + 7 * nz, thin_frac=thin)
     cols.h[: nx // 4, :, -1] = 1.0e-4       # vanished top layers on part of the domain: floored at H_VANISHED
-    over = KNOBS if knobs == "knobs" else {}
+    over = {"default": {}, "knobs": KNOBS, "merge": MERGE}[knobs]
     cfg = hot_cfg(kappa_shear=1, **over)
     f = beta_plane(ny, nx) * (-1.0 if knobs == "knobs" else 1.0)
     st = oracle_state(oracle, cols, cfg)

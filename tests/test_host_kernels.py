@@ -59,7 +59,8 @@ def _beta_plane(st):
 
 @pytest.mark.parametrize("shape", [(20, 12, 12), (12, 9, 40), (10, 6, 75), (7, 5, 1), (9, 4, 3), (6, 5, 100)])
 @pytest.mark.parametrize("knobs", [{}, dict(eos_variant=1, eos_alpha_t=0.2, eos_beta_s=0.77, ks_vel_underflow=1e-3,
-                                            ks_tke_bg=1e-12, ks_src_max_chg=8.0, ks_lz_rescale=0.5)])
+                                            ks_tke_bg=1e-12, ks_src_max_chg=8.0, ks_lz_rescale=0.5),
+                                   dict(ks_massless_merge=1)])
 def test_kappa_shear_source_matches_oracle(oracle, host_libs, shape, knobs):
     nx, ny, nz = shape
     cols = columns(nx=nx, ny=ny, nz=nz, seed=nx * ny + nz, thin_frac=0.15)

@@ -159,3 +159,126 @@ def test_shallow_columns(oracle, nz):
     st.call("vpo_kappa_shear", ks_config(), DT)
     assert np.isfinite(st.kd_shear).all() and np.isfinite(st.tke_shear).all()
     assert (st.kd_shear[:, :, 0] == 0.0).all() and (st.kd_shear[:, :, nz] == 0.0).all()
+
+
+# ---- the massless merge (tests/test_ocean_massless.F90) -------------------
+H_VANISHED = 1.5e-4
+
+
+def _maps(oracle, h):
+    """vpo_massless_build_maps on a 1-based surface-down column h[1..nz]."""
+    import ctypes
+
+    nz = len(h)
+    h1 = np.zeros(nz + 2)
+    h1[1:nz + 1] = h
+    hc, kf = np.zeros(nz + 2), np.zeros(nz + 2)
+    kc = np.zeros(nz + 2, dtype=np.int32)
+    nzc = ctypes.c_int()
+    dp = ctypes.POINTER(ctypes.c_double)
+    L = oracle.lib()
+    L.vpo_massless_build_maps(h1.ctypes.data_as(dp), nz, ctypes.c_double(H_VANISHED), ctypes.byref(nzc),
+                              hc.ctypes.data_as(dp), kc.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                              kf.ctypes.data_as(dp))
+    return h1, nzc.value, hc, kc, kf
+
+
+def _merge(oracle, h1, kc, nzc, fields):
+    import ctypes
+
+    dp = ctypes.POINTER(ctypes.c_double)
+    nz = len(h1) - 2
+    ins = []
+    for f in fields:
+        a = np.zeros(nz + 2)
+        a[1:nz + 1] = f
+        ins.append(a)
+    outs = [np.zeros(nz + 2) for _ in range(4)]
+    oracle.lib().vpo_massless_merge_fields(h1.ctypes.data_as(dp), kc.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                           nz, nzc, *[a.ctypes.data_as(dp) for a in ins],
+                                           *[a.ctypes.data_as(dp) for a in outs])
+    return outs
+
+
+def test_massless_golden_maps(oracle):
+    """The worked nz = 8 example (test_ocean_massless.F90:63-140)."""
+    h = [12.0, 10.0, H_VANISHED * 0.5, 15.0, 8.0, H_VANISHED * 0.5, 6.0, 9.0]
+    h1, nzc, hc, kc, kf = _maps(oracle, h)
+    assert nzc == 6
+    assert list(kc[1:10]) == [1, 2, 2, 3, 4, 4, 5, 6, 7]
+    assert hc[1] == 12.0 and hc[3] == 15.0 and hc[5] == 6.0 and hc[6] == 9.0
+    assert abs(hc[2] - (10.0 + H_VANISHED * 0.5)) < 1e-15 and abs(hc[4] - (8.0 + H_VANISHED * 0.5)) < 1e-15
+    assert abs(kf[3] - 0.99999250005624951) < 1e-14 and abs(kf[6] - 0.99999062508788972) < 1e-14
+    assert all(kf[k] == 0.0 for k in (1, 2, 4, 5, 7, 8, 9))
+    u = [0.1, 0.2, 0.0, 0.15, 0.05, 0.0, -0.1, -0.05]
+    v = [0.0, 0.05, 0.0, -0.1, 0.1, 0.0, 0.08, 0.02]
+    t = [22.0, 20.0, 19.5, 18.0, 16.0, 15.5, 14.0, 12.0]
+    s = [35.0, 35.2, 35.3, 35.5, 35.6, 35.65, 35.7, 35.8]
+    uc, vc, tc, sc = _merge(oracle, h1, kc, nzc, (u, v, t, s))
+    assert tc[1] == 22.0 and tc[3] == 18.0 and tc[6] == 12.0
+    assert abs(tc[2] - 19.999996250028122) < 1e-12
+
+
+def test_massless_identity_and_conservation(oracle):
+    """I1 (test_ocean_massless.F90:142-205): a healthy column maps onto
+    itself bit for bit and interp_back is the identity; I2 (:207-268): the
+    merged thickness and thickness-weighted T, S integrals are conserved."""
+    import ctypes
+
+    nz = 12
+    h = [5.0 + k for k in range(1, nz + 1)]
+    h1, nzc, hc, kc, kf = _maps(oracle, h)
+    assert nzc == nz and list(kc[1:nz + 2]) == list(range(1, nz + 2))
+    assert (kf[1:nz + 2] == 0.0).all() and np.array_equal(hc[1:nz + 1], h1[1:nz + 1])
+    qc = np.zeros(nz + 2)
+    qc[1:nz + 2] = [1.0e-3 * (k * k - 3 * k) for k in range(1, nz + 2)]
+    q = np.zeros(nz + 2)
+    dp = ctypes.POINTER(ctypes.c_double)
+    oracle.lib().vpo_massless_interp_back(qc.ctypes.data_as(dp), kc.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                          kf.ctypes.data_as(dp), nz, q.ctypes.data_as(dp))
+    assert np.array_equal(q[1:nz + 2], qc[1:nz + 2])
+
+    h = [10.0, H_VANISHED * 0.4, 12.0, 8.0, H_VANISHED * 0.6, H_VANISHED * 0.2, 7.0, 9.0, H_VANISHED * 0.3, 5.0, 6.0]
+    t = [18.0 - 0.3 * k for k in range(1, 12)]
+    s = [34.5 + 0.05 * k for k in range(1, 12)]
+    h1, nzc, hc, kc, kf = _maps(oracle, h)
+    _, _, tc, sc = _merge(oracle, h1, kc, nzc, ([0.0] * 11, [0.0] * 11, t, s))
+    assert abs(sum(hc[1:nzc + 1]) - sum(h)) <= 1e-13 * sum(h)
+    assert abs(sum(tc[k] * hc[k] for k in range(1, nzc + 1)) - sum(a * b for a, b in zip(t, h))) <= 1e-12 * 1e3
+    assert abs(sum(sc[k] * hc[k] for k in range(1, nzc + 1)) - sum(a * b for a, b in zip(s, h))) <= 1e-12 * 1e4
+
+
+def _zstar_like(oracle, nz, has_vanish):
+    """setup_zstar_like_column (test_ocean_massless.F90:289-326): 10 m layers,
+    the three bed-side ones vanished when has_vanish, the golden test's tanh
+    shear and stratification."""
+    st = oracle.OracleState(2, 2, nz, 2)
+    dtdm = 3.0e-5 * RHO0 / (G * ALPHA)
+    for k in range(1, nz + 1):
+        k_sd = nz + 1 - k
+        h = H_VANISHED * 0.5 if (has_vanish and k_sd > nz - 3) else 10.0
+        z = (k_sd - 1 + 0.5) * 10.0
+        st.h[:, :, k - 1] = h
+        st.tracers[1][:, :, k - 1] = 20.0 - dtdm * z
+        st.tracers[0][:, :, k - 1] = 35.0
+        st.u[:, :, k - 1] = 0.5 * math.tanh((50.0 - z) / 20.0)
+    st.coriolis[...] = F_CORIOLIS
+    return st
+
+
+def test_massless_merge_end_to_end(oracle):
+    """T4a / T4b (test_ocean_massless.F90:328-430): on a column with vanished
+    layers the merge changes kd (and keeps 0 on the bed and surface); on a
+    healthy column merge on equals merge off bit for bit."""
+    nz = 12
+    out = {}
+    for vanish in (True, False):
+        for merge in (0, 1):
+            st = _zstar_like(oracle, nz, vanish)
+            st.call("vpo_kappa_shear", ks_config(ks_massless_merge=merge), DT)
+            out[(vanish, merge)] = (st.kd_shear.copy(), st.tke_shear.copy())
+    on = out[(True, 1)][0]
+    assert on[1, 1, 0] == 0.0 and on[1, 1, nz] == 0.0
+    assert np.abs(on - out[(True, 0)][0]).max() > 1e-9
+    assert np.array_equal(out[(False, 1)][0], out[(False, 0)][0])
+    assert np.array_equal(out[(False, 1)][1], out[(False, 0)][1])
