@@ -268,6 +268,27 @@ typedef struct vphys_config {
      * of flooring them at H_VANISHED; healthy columns are unchanged, bit for
      * bit */
     int ks_massless_merge;    /* 0 */
+    /* the shortwave source of the penetration deposit, KPP's B0 charge and
+     * EPBL's shortwave TKE ledger (sw_source, rdb_ocean_surface_flux.F90:
+     * 715-740, 1256-1399; rdb_ocean_vmix.F90:1076-1118; rdb_ocean_epbl.F90:
+     * 895-920): 0 "net_heat", I0 = sw_pen_frac Q_heat; 1 "q_sw",
+     * I0 = sw_pen_frac SW_NET (the net shortwave q_sw + sw_ice, >= 0).  The
+     * surface deposit itself always books Q_heat. */
+    int sw_source;            /* 0 */
+    /* OM3 BOUND_SALINITY: after the surface deposit, S = max(S, min_salinity)
+     * on the first live layer of every wet column whose thickness exceeds
+     * H_DIV_EPS (bound_salinity_top_impl, rdb_ocean_surface_flux.F90:
+     * 1072-1091); non-conserving, not booked in the budgets */
+    int bound_salinity;       /* 0 */
+    /* 1: the WET_DYN field (the dynamic wet/dry cell mask) multiplies the
+     * surface deposit of T, S and pseudo-salt, so a dry column takes no flux
+     * (apply_surface_src_2d_dyn_impl, rdb_ocean_surface_flux.F90:1144-1225) */
+    int use_wet_dyn;          /* 0 */
+    double min_salinity;      /* 0 */
+    /* EPBL charges the penetrating shortwave per layer in its TKE ledger
+     * (epbl_sw_ctke, rdb_ocean_epbl.F90:356-360, 905); 0 treats all of the
+     * heat flux as a skin flux even with sw_pen_frac != 0 */
+    int epbl_sw_ctke;         /* 1 */
 } vphys_config;
 
 #define VPHYS_KPP_SW_ALL 1
@@ -320,6 +341,10 @@ enum vphys_field {
     VPHYS_FIELD_EPBL_TKE_MIXING = 38,     /* out (nx, ny) spent raising potential energy */
     VPHYS_FIELD_EPBL_TKE_MECH_DECAY = 39, /* out (nx, ny) mechanical TKE decayed (and left at the bed) */
     VPHYS_FIELD_EPBL_TKE_CONV_DECAY = 40, /* out (nx, ny) convective TKE lost to rotation (and left at the bed) */
+    VPHYS_FIELD_SW_NET = 41,    /* in      (nx, ny) W m-2 >= 0: the net shortwave q_sw + sw_ice, the source
+                                   when sw_source = 1 (allocated then) */
+    VPHYS_FIELD_WET_DYN = 42,   /* in      (nx, ny) dynamic wet/dry cell mask, 1 wet, 0 dry (use_wet_dyn = 1;
+                                   allocated then, filled with 1) */
     VPHYS_FIELD_TRACER0 = 64    /* in/out  (nx, ny, nz); tracer t is
                                    VPHYS_FIELD_TRACER0 + t */
 };

@@ -611,16 +611,18 @@ static inline double sw_transmission(const vphys_config *c, double d)
 /* The kinematic heat flux B0 charges (rdb_ocean_vmix.F90:1321-1348 in pass 1
  * with the lagged h_b, 1440-1466 in pass 2 with the new one): with
  * shortwave penetration on, Q_heat minus the penetrating part that passes
- * the boundary layer (MXL) or the surface layer (LV1); all of it otherwise. */
+ * the boundary layer (MXL) or the surface layer (LV1), sw_pen_frac times the
+ * selected shortwave source (sw_src, :1102-1117); all of it otherwise. */
 static inline double kpp_q_t_kin(const vphys_config *c, const vpo_state *s, int i, int j, int k_sfc, double h_b)
 {
     const int nx = s->nx, ny = s->ny;
     if (c->sw_pen_frac != 0.0) {
+        const double *sw = vpo_sw_source(c, s);
         double q_bl = C2(s->q_heat, i, j);
         if (c->kpp_sw_method == VPHYS_KPP_SW_MXL)
-            q_bl = q_bl - c->sw_pen_frac * C2(s->q_heat, i, j) * sw_transmission(c, h_b);
+            q_bl = q_bl - c->sw_pen_frac * C2(sw, i, j) * sw_transmission(c, h_b);
         else if (c->kpp_sw_method == VPHYS_KPP_SW_LV1)
-            q_bl = q_bl - c->sw_pen_frac * C2(s->q_heat, i, j) * sw_transmission(c, C3(s->h, i, j, k_sfc));
+            q_bl = q_bl - c->sw_pen_frac * C2(sw, i, j) * sw_transmission(c, C3(s->h, i, j, k_sfc));
         return q_bl / (c->rho0 * c->cp);
     }
     return C2(s->q_heat, i, j) / (c->rho0 * c->cp);
@@ -1318,22 +1320,34 @@ void vpo_surface_flux(const vphys_config *c, vpo_state *s, double dt)
             const int kt = first_live(s->h, nx, ny, i, j, nz);
             const double hk = C3(s->h, i, j, kt);
             const double w = C2(s->wet, i, j);
+            /* apply_surface_src_2d_dyn_impl (1144-1225): the dynamic mask
+             * multiplies after the static one */
+            const int dyn = c->use_wet_dyn;
             if (iT >= 0) {
-                const double cell = inv_heat * C2(s->q_heat, i, j) * w;
+                double cell = inv_heat * C2(s->q_heat, i, j) * w;
+                if (dyn) cell = cell * C2(s->wet_dyn, i, j);
                 double *T = s->tr[iT];
                 C3(T, i, j, kt) = conc_add_source(C3(T, i, j, kt), hk, cell);
                 if (c->budgets) C3(s->heat_budget_surface, i, j, kt) += (hk > H_VANISHED) ? cell : 0.0;
             }
             if (iS >= 0) {
-                const double cell = inv_salt * C2(s->q_salt, i, j) * w;
+                double cell = inv_salt * C2(s->q_salt, i, j) * w;
+                if (dyn) cell = cell * C2(s->wet_dyn, i, j);
                 double *S = s->tr[iS];
                 C3(S, i, j, kt) = conc_add_source(C3(S, i, j, kt), hk, cell);
                 if (c->budgets) C3(s->salt_budget_surface, i, j, kt) += (hk > H_VANISHED) ? cell : 0.0;
             }
             if (iPS >= 0) {
-                const double cell = inv_salt * C2(s->q_salt, i, j) * w;
+                double cell = inv_salt * C2(s->q_salt, i, j) * w;
+                if (dyn) cell = cell * C2(s->wet_dyn, i, j);
                 double *PS = s->tr[iPS];
                 C3(PS, i, j, kt) = conc_add_source(C3(PS, i, j, kt), hk, cell);
+            }
+            /* bound_salinity_top_impl (1072-1091), after the salt deposit:
+             * the static mask, a thickness above H_DIV_EPS, not booked */
+            if (c->bound_salinity && iS >= 0 && w > 0.5 && hk > H_DIV_EPS) {
+                double *S = s->tr[iS];
+                C3(S, i, j, kt) = fmx(C3(S, i, j, kt), c->min_salinity);
             }
         }
     }
@@ -1355,7 +1369,7 @@ void vpo_sw_penetration(const vphys_config *c, vpo_state *s, double dt)
     for (int j = 1; j <= ny; ++j) {
         for (int i = 1; i <= nx; ++i) {
             const int kt = first_live(s->h, nx, ny, i, j, nz);
-            const double i0col = c->sw_pen_frac * C2(s->q_heat, i, j) * C2(s->wet, i, j);
+            const double i0col = c->sw_pen_frac * C2(vpo_sw_source(c, s), i, j) * C2(s->wet, i, j);
             int k_dep = 1;
             for (int k = 1; k <= nz; ++k) {
                 if (C3(s->h, i, j, k) > H_VANISHED) {

@@ -48,7 +48,17 @@ typedef struct vpo_state {
     double *mld_epbl;                       /* (nx,ny) EPBL mixed-layer depth */
     double *la_epbl;                        /* (nx,ny) EPBL Langmuir number */
     double *epbl_tke[6];                    /* (nx,ny) EPBL TKE budget terms, written when epbl_tke_diags */
+    double *sw_net;                         /* (nx,ny) the shortwave source under sw_source = 1 */
+    double *wet_dyn;                        /* (nx,ny) dynamic wet mask, read under use_wet_dyn */
 } vpo_state;
+
+/* The shortwave source the configuration selects (ocean_surfflux_set_sw's
+ * sw_from_qsw, rdb_ocean_surface_flux.F90:715-740): Q_heat, or the net
+ * shortwave under sw_source = 1. */
+static inline const double *vpo_sw_source(const vphys_config *c, const vpo_state *s)
+{
+    return c->sw_source ? s->sw_net : s->q_heat;
+}
 
 void vpo_set_threads(int n);
 int vpo_get_threads(void);

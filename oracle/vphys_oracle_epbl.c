@@ -278,8 +278,8 @@ void vpo_epbl(const vphys_config *c, vpo_state *s, double dt)
             const int k_sfc = first_live(s->h, nx, ny, i, j, nz);
             /* the penetrating-shortwave ledger (:1095-1185): irradiance I0 and the
              * running depth of the layer top below the live surface */
-            const int sw_on = c->sw_pen_frac != 0.0;
-            const double i0_col = sw_on ? c->sw_pen_frac * C2(s->q_heat, i, j) * C2(s->wet, i, j) : 0.0;
+            const int sw_on = c->epbl_sw_ctke && c->sw_pen_frac != 0.0;   /* sw_ctke_active (:905) */
+            const double i0_col = sw_on ? c->sw_pen_frac * C2(vpo_sw_source(c, s), i, j) * C2(s->wet, i, j) : 0.0;
             double d_top_sw = 0.0, e1_top = 1.0, e2_top = 1.0;
             /* ---- column prep: T0, S0 and the pressure-weighted weights (downward) */
             double pres = 0.0, h_sum = 0.0, dsv_dt_sfc = 0.0, dsv_ds_sfc = 0.0;

@@ -71,6 +71,8 @@ FIELD_KD_EPBL = 32
 FIELD_MLD_EPBL = 33
 FIELD_LA_EPBL = 34
 FIELD_EPBL_TKE = {"wind": 35, "conv": 36, "forcing": 37, "mixing": 38, "mech_decay": 39, "conv_decay": 40}
+FIELD_SW_NET = 41
+FIELD_WET_DYN = 42
 FIELD_TRACER0 = 64
 
 FIELD_NAMES = {
@@ -84,7 +86,7 @@ FIELD_NAMES = {
     "k_bot_v": FIELD_K_BOT_V, "coriolis": FIELD_CORIOLIS,
     "heat_budget_surface": FIELD_HEAT_BUDGET_SURFACE, "salt_budget_surface": FIELD_SALT_BUDGET_SURFACE,
     "kd_shear": FIELD_KD_SHEAR, "tke_shear": FIELD_TKE_SHEAR, "kd_epbl": FIELD_KD_EPBL, "mld_epbl": FIELD_MLD_EPBL,
-    "la_epbl": FIELD_LA_EPBL,
+    "la_epbl": FIELD_LA_EPBL, "sw_net": FIELD_SW_NET, "wet_dyn": FIELD_WET_DYN,
     **{f"epbl_tke_{k}": v for k, v in FIELD_EPBL_TKE.items()},
 }
 INT_FIELDS = (FIELD_K_TOP_U, FIELD_K_TOP_V, FIELD_K_BOT_U, FIELD_K_BOT_V)
@@ -159,7 +161,9 @@ class VphysConfig(ctypes.Structure):
         ("epbl_use_lt", ctypes.c_int), ("epbl_lt_scheme", ctypes.c_int)] + [(n, ctypes.c_double) for n in (
             "epbl_lt_enhance_coef", "epbl_lt_enhance_exp", "epbl_lt_max_enhance", "epbl_la_frac_hbl",
             "epbl_lt_lac1", "epbl_lt_lac2", "epbl_lt_lac3", "epbl_lt_lac4", "epbl_lt_lac5")] + [
-        ("epbl_tke_diags", ctypes.c_int), ("ks_massless_merge", ctypes.c_int)]
+        ("epbl_tke_diags", ctypes.c_int), ("ks_massless_merge", ctypes.c_int),
+        ("sw_source", ctypes.c_int), ("bound_salinity", ctypes.c_int), ("use_wet_dyn", ctypes.c_int),
+        ("min_salinity", ctypes.c_double), ("epbl_sw_ctke", ctypes.c_int)]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_ if n not in ()}

@@ -151,6 +151,11 @@ def default_config() -> VphysConfig:
     c.epbl_lt_lac5 = 0.95
     c.epbl_tke_diags = 0
     c.ks_massless_merge = 0
+    c.sw_source = 0
+    c.bound_salinity = 0
+    c.use_wet_dyn = 0
+    c.min_salinity = 0.0
+    c.epbl_sw_ctke = 1
     return c
 
 
@@ -272,6 +277,34 @@ class ConvectiveAdjustment:
         cfg.conv_kd = float(self.kd)
         cfg.conv_prandtl = float(self.prandtl)
         cfg.conv_n2_thresh = float(self.n2_threshold)
+        return cfg
+
+
+class ShortwavePenetration:
+    """Two-band shortwave penetration (python/rdb/forcing.py:93-115:
+    `ShortwavePenetration(fraction=0.0, band_ratio=0.58, zeta1=0.35,
+    zeta2=23.0, source="net_heat", epbl_tke_ledger=True)`).  `source="q_sw"`
+    reads the SW_NET field (q_sw + sw_ice) as the irradiance of the
+    penetration, KPP's B0 charge and EPBL's ledger; any other source is
+    refused, as sw_source_is_implemented does
+    (rdb_ocean_surface_flux.F90:814-822).  All inert at fraction=0."""
+
+    _SOURCE = {"net_heat": 0, "q_sw": 1}
+
+    def __init__(self, fraction=0.0, band_ratio=0.58, zeta1=0.35, zeta2=23.0, source="net_heat",
+                 epbl_tke_ledger=True):
+        if source not in self._SOURCE:
+            raise ValueError(f"ShortwavePenetration: source must be one of {sorted(self._SOURCE)}")
+        self.fraction, self.band_ratio, self.zeta1, self.zeta2 = fraction, band_ratio, zeta1, zeta2
+        self.source, self.epbl_tke_ledger = source, epbl_tke_ledger
+
+    def apply(self, cfg):
+        cfg.sw_pen_frac = float(self.fraction)
+        cfg.sw_band_ratio = float(self.band_ratio)
+        cfg.sw_zeta1 = float(self.zeta1)
+        cfg.sw_zeta2 = float(self.zeta2)
+        cfg.sw_source = self._SOURCE[self.source]
+        cfg.epbl_sw_ctke = 1 if self.epbl_tke_ledger else 0
         return cfg
 
 

@@ -50,7 +50,7 @@ int cuda_status(cudaError_t e, const char *where)
     return push_error(VPHYS_ERR_CUDA, "%s: CUDA error %d (%s)", where, (int)e, cudaGetErrorString(e));
 }
 
-constexpr int NFIXED = 41;
+constexpr int NFIXED = 43;
 constexpr unsigned MAGIC = 0x56504859u;   // "VPHY"
 
 struct Field {
@@ -139,6 +139,8 @@ size_t field_count(int nx, int ny, int nz, int field, bool *is_int)
     case VPHYS_FIELD_Q_SALT:
     case VPHYS_FIELD_WET:
     case VPHYS_FIELD_CORIOLIS:
+    case VPHYS_FIELD_SW_NET:
+    case VPHYS_FIELD_WET_DYN:
     case VPHYS_FIELD_MLD_EPBL:
     case VPHYS_FIELD_LA_EPBL:
     case VPHYS_FIELD_EPBL_TKE_WIND:
@@ -191,7 +193,8 @@ int init_field(vphys_handle h, int field, Field &fl)
     const size_t plane = (size_t)h->nx * h->ny;
     cudaStream_t s = h->stream;
     switch (field) {
-    case VPHYS_FIELD_WET: k_fill_double<<<fill_blocks(fl.n), 256, 0, s>>>((double *)fl.own, fl.n, 1.0); break;
+    case VPHYS_FIELD_WET:
+    case VPHYS_FIELD_WET_DYN: k_fill_double<<<fill_blocks(fl.n), 256, 0, s>>>((double *)fl.own, fl.n, 1.0); break;
     case VPHYS_FIELD_KV: k_fill_interfaces<<<fill_blocks(fl.n), 256, 0, s>>>((double *)fl.own, plane, h->nz, h->cfg.pp81_nu_bg); break;
     case VPHYS_FIELD_KT:
     case VPHYS_FIELD_KS: k_fill_interfaces<<<fill_blocks(fl.n), 256, 0, s>>>((double *)fl.own, plane, h->nz, h->cfg.pp81_kappa_bg); break;
@@ -224,6 +227,17 @@ int ensure(vphys_handle h, int field)
 }
 
 bool present(vphys_handle h, int field) { return h->f[slot_of(h, field)].ptr() != nullptr; }
+
+// The forcing fields a configuration reads: SW_NET under sw_source = 1,
+// WET_DYN under use_wet_dyn.  Held from create / set_config on (and
+// restored by an unbind), so every launch finds them.
+int prepare_sources(vphys_handle h)
+{
+    int st = VPHYS_OK;
+    if (h->cfg.sw_source && (st = ensure(h, VPHYS_FIELD_SW_NET))) return st;
+    if (h->cfg.use_wet_dyn && (st = ensure(h, VPHYS_FIELD_WET_DYN))) return st;
+    return st;
+}
 
 int validate(const vphys_config *c, int ntr)
 {
@@ -262,6 +276,12 @@ int validate(const vphys_config *c, int ntr)
     if (c->kappa_shear < 0 || c->kappa_shear > 1) return push_error(VPHYS_ERR_CONFIG, "kappa_shear must be 0 or 1");
     if (c->ks_massless_merge < 0 || c->ks_massless_merge > 1)
         return push_error(VPHYS_ERR_CONFIG, "ks_massless_merge must be 0 or 1");
+    if (c->sw_source < 0 || c->sw_source > 1)
+        return push_error(VPHYS_ERR_CONFIG, "sw_source must be 0 (net_heat) or 1 (q_sw)");
+    if (c->bound_salinity < 0 || c->bound_salinity > 1)
+        return push_error(VPHYS_ERR_CONFIG, "bound_salinity must be 0 or 1");
+    if (c->use_wet_dyn < 0 || c->use_wet_dyn > 1) return push_error(VPHYS_ERR_CONFIG, "use_wet_dyn must be 0 or 1");
+    if (c->epbl_sw_ctke < 0 || c->epbl_sw_ctke > 1) return push_error(VPHYS_ERR_CONFIG, "epbl_sw_ctke must be 0 or 1");
     // the inner solve must run at least once (the substep's adaptive-dt bands
     // read its decay lengths); both caps bound the per-column work
     if (c->ks_max_inner_it < 1 || c->ks_max_inner_it > 10000)
@@ -318,6 +338,8 @@ Params make_params(vphys_handle h)
     p.q_heat = D(VPHYS_FIELD_Q_HEAT);
     p.q_salt = D(VPHYS_FIELD_Q_SALT);
     p.wet = D(VPHYS_FIELD_WET);
+    p.sw_src = h->cfg.sw_source ? D(VPHYS_FIELD_SW_NET) : p.q_heat;
+    p.wet_dyn = h->cfg.use_wet_dyn ? D(VPHYS_FIELD_WET_DYN) : nullptr;
     p.tau_x = D(VPHYS_FIELD_TAU_X);
     p.tau_y = D(VPHYS_FIELD_TAU_Y);
     p.lambda_bot_u = D(VPHYS_FIELD_LAMBDA_BOT_U);
@@ -681,6 +703,7 @@ int vphys_config_default(vphys_config *c)
     if (!c) return push_error(VPHYS_ERR_CONFIG, "vphys_config_default: NULL");
     memset(c, 0, sizeof *c);
     c->use_closure = 1;
+    c->epbl_sw_ctke = 1;
     c->interior_closure = VPHYS_INTERIOR_PP81;
     c->pp81_nu0 = 1.0e-2;
     c->pp81_nu_bg = 1.0e-4;
@@ -820,6 +843,10 @@ int vphys_create(int nx, int ny, int nz, int ntracer, const vphys_config *cfg, v
             return st;
         }
     }
+    if ((st = prepare_sources(h))) {
+        vphys_destroy(&h);
+        return st;
+    }
     e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) {
         st = cuda_status(e, "vphys_create");
@@ -867,7 +894,7 @@ int vphys_set_config(vphys_handle h, const vphys_config *cfg)
     int st = validate(cfg, h->ntr);
     if (st) return st;
     h->cfg = *cfg;
-    return VPHYS_OK;
+    return prepare_sources(h);
 }
 
 int vphys_get_config(vphys_handle h, vphys_config *cfg)
@@ -901,6 +928,7 @@ int vphys_bind(vphys_handle h, int field, void *device_ptr)
     if (!device_ptr && !h->f[sl].own) {
         // restore a handle-owned buffer only for core fields / tracers
         if (sl < VPHYS_FIELD_LAMBDA_BOT_U || sl >= NFIXED) return ensure(h, field);
+        if (sl == VPHYS_FIELD_SW_NET || sl == VPHYS_FIELD_WET_DYN) return prepare_sources(h);
     }
     return VPHYS_OK;
 }

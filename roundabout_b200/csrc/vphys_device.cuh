@@ -552,18 +552,22 @@ __device__ __forceinline__ double sw_transmission(const vphys_config &c, double 
 // The kinematic heat flux KPP's B0 charges (rdb_ocean_vmix.F90:1321-1348 in
 // pass 1 with the lagged h_b, 1440-1466 in pass 2 with the new one): with
 // shortwave penetration on, Q_heat minus the penetrating part that passes the
-// boundary layer (MXL) or the surface layer h_sfc (LV1).
+// boundary layer (MXL) or the surface layer h_sfc (LV1), the part of
+// sw_pen_frac times the shortwave source *sw (Q_heat, or SW_NET under
+// sw_source = 1; read only with penetration on).
 // (the exponentials out of line, with scalar arguments, so the kernels that
 // call this keep their registers when shortwave penetration is off)
-static __device__ __noinline__ double sw_q_bl(double q_heat, double d, double pen, double R, double zeta1, double zeta2)
+static __device__ __noinline__ double sw_q_bl(double q_heat, const double *sw, double d, double pen, double R,
+                                               double zeta1, double zeta2)
 {
-    return q_heat - pen * q_heat * (R * sm_exp(xdiv(-d, zeta1)) + (1.0 - R) * sm_exp(xdiv(-d, zeta2)));
+    return q_heat - pen * *sw * (R * sm_exp(xdiv(-d, zeta1)) + (1.0 - R) * sm_exp(xdiv(-d, zeta2)));
 }
-__device__ __forceinline__ double kpp_q_t_kin(const vphys_config &c, double q_heat, double h_b, double h_sfc)
+__device__ __forceinline__ double kpp_q_t_kin(const vphys_config &c, double q_heat, const double *sw, double h_b,
+                                              double h_sfc)
 {
     if (c.sw_pen_frac != 0.0 && c.kpp_sw_method != VPHYS_KPP_SW_ALL) {
         const double d = (c.kpp_sw_method == VPHYS_KPP_SW_MXL) ? h_b : h_sfc;
-        return xdiv(sw_q_bl(q_heat, d, c.sw_pen_frac, c.sw_band_ratio, c.sw_zeta1, c.sw_zeta2), c.rho0 * c.cp);
+        return xdiv(sw_q_bl(q_heat, sw, d, c.sw_pen_frac, c.sw_band_ratio, c.sw_zeta1, c.sw_zeta2), c.rho0 * c.cp);
     }
     return xdiv(q_heat, c.rho0 * c.cp);
 }

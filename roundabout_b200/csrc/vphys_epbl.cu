@@ -221,8 +221,8 @@ __global__ void __launch_bounds__(128, 4) k_epbl(const Params p, double dt, doub
     const double *S = p.tr[c.idx_salinity] + col;
 
     double h[N], t0[N], s0[N], dpe_t[N], dpe_s[N], dch_t[N], dch_s[N], kd[N], ctke_sw[N];
-    const bool sw_on = c.sw_pen_frac != 0.0;
-    const double i0_col = sw_on ? c.sw_pen_frac * p.q_heat[col] * p.wet[col] : 0.0;
+    const bool sw_on = c.epbl_sw_ctke && c.sw_pen_frac != 0.0;
+    const double i0_col = sw_on ? c.sw_pen_frac * p.sw_src[col] * p.wet[col] : 0.0;
     double d_top_sw = 0.0, e1_top = 1.0, e2_top = 1.0;
     int k_sfc = nz;   // first live layer from the top (nz when none is live)
     for (int k = nz; k >= 1; --k) {

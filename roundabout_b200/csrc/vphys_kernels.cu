@@ -86,26 +86,33 @@ __global__ void k_surface_flux(const Params p, double inv_heat, double inv_salt)
     const double w = __ldg(p.wet + col);
     const int iT = p.cfg.idx_temperature, iS = p.cfg.idx_salinity, iPS = p.cfg.idx_pseudo_salt;
     const bool book = p.cfg.budgets && hk > H_VANISHED;
+    const double *wd = p.wet_dyn;   // the dynamic mask composes after the static one
     if (iT >= 0) {
-        const double cell = inv_heat * __ldg(p.q_heat + col) * w;
+        double cell = inv_heat * __ldg(p.q_heat + col) * w;
+        if (wd) cell = cell * __ldg(wd + col);
         p.tr[iT][idx] = conc_add_source(p.tr[iT][idx], hk, cell);
         if (p.cfg.budgets) p.heat_budget_surface[idx] += book ? cell : 0.0;
     }
     if (iS >= 0 || iPS >= 0) {
-        const double cell = inv_salt * __ldg(p.q_salt + col) * w;
+        double cell = inv_salt * __ldg(p.q_salt + col) * w;
+        if (wd) cell = cell * __ldg(wd + col);
         if (iS >= 0) {
             p.tr[iS][idx] = conc_add_source(p.tr[iS][idx], hk, cell);
             if (p.cfg.budgets) p.salt_budget_surface[idx] += book ? cell : 0.0;
         }
         if (iPS >= 0) p.tr[iPS][idx] = conc_add_source(p.tr[iPS][idx], hk, cell);
     }
+    // BOUND_SALINITY after the salt deposit (bound_salinity_top_impl,
+    // rdb_ocean_surface_flux.F90:1072-1091): static wet mask, not booked
+    if (p.cfg.bound_salinity && iS >= 0 && w > 0.5 && hk > H_DIV_EPS)
+        p.tr[iS][idx] = fmx(p.tr[iS][idx], p.cfg.min_salinity);
 }
 
 // ---------------------------------------------------------------------------
 // Shortwave penetration (ocean_surface_flux_apply_sw_penetration ->
 // apply_sw_penetration_impl, rdb_ocean_surface_flux.F90:1255-1370,
 // 1451-1530, with k_top = nz and k_bot = 1): the penetrating part
-// I0 = sw_pen_frac Q_heat wet of the surface lump leaves the first live layer
+// I0 = sw_pen_frac Q_heat wet (SW_NET for Q_heat under sw_source = 1) of the surface lump leaves the first live layer
 // and each live layer takes I0 (T(d_top) - T(d_bottom)), the deepest live
 // layer the rest (opaque bed); vanished layers pass the light on.  One thread
 // per column.
@@ -133,7 +140,7 @@ __global__ void k_sw_penetration(const Params p, double inv_scale)
             k_dep = k;
             break;
         }
-    const double i0col = c.sw_pen_frac * __ldg(p.q_heat + col) * __ldg(p.wet + col);
+    const double i0col = c.sw_pen_frac * __ldg(p.sw_src + col) * __ldg(p.wet + col);
     double d_top = 0.0;
     double trans_top = sw_transmission(c, d_top);
     for (int k = nz; k >= k_dep; --k) {
@@ -253,7 +260,7 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
         const double tau_mag = p.stress_mag[col];
         const double u_star = sqrt(xdiv(tau_mag, rho0));
         // pass 1 charges the shortwave that passes the lagged boundary layer
-        q_T_kin = kpp_q_t_kin(c, p.q_heat[col], h_b, HH(k_sfc));
+        q_T_kin = kpp_q_t_kin(c, p.q_heat[col], p.sw_src + col, h_b, HH(k_sfc));
         q_S_kin = xdiv(p.q_salt[col], rho0);
         double T_sfc = 0.0, S_sfc = 0.0;
         if (c.buoyancy_coeffs) {   // "eos": the surface layer's (T, S) (rdb_ocean_vmix.F90:1357-1376)
@@ -328,7 +335,7 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
         }
         // ---- KPP pass 2 scalars (rdb_ocean_vmix.F90:1429-1491) ----
         if (c.sw_pen_frac != 0.0) {   // pass 2 charges what passes the new boundary layer
-            q_T_kin = kpp_q_t_kin(c, p.q_heat[col], h_b, HH(k_sfc));
+            q_T_kin = kpp_q_t_kin(c, p.q_heat[col], p.sw_src + col, h_b, HH(k_sfc));
             B_0 = kpp_surface_b0(c, q_T_kin, q_S_kin, HH(k_sfc), T_sfc, S_sfc);
         }
         p.b0[col] = B_0;

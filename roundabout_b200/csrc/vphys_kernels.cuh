@@ -33,6 +33,9 @@ struct Params {
     double *rho, *u, *v, *kv, *kt, *ks;
     double *bl_depth, *b0;
     const double *stress_mag, *q_heat, *q_salt, *wet;
+    // the shortwave source the host selected (q_heat, or SW_NET under
+    // sw_source = 1) and the dynamic wet mask (NULL unless use_wet_dyn)
+    const double *sw_src, *wet_dyn;
     const double *tau_x, *tau_y, *lambda_bot_u, *lambda_bot_v;
     double *visc_rem_u, *visc_rem_v;
     double *gamma_t, *gamma_s;       // nullptr: not written

@@ -193,3 +193,74 @@ def test_mixed_step_with_shortwave(VP, oracle):
     vp.step(DT, 1)
     err = max(float(np.abs(np.asarray(vp.get_tracer(t)) - st.tracers[t]).max()) for t in range(ntr))
     assert err <= 1.0e-6, err
+
+
+def _sunlit_qsw(st):
+    """A net shortwave unlike Q_heat's own share, zero on every third row."""
+    st.q_heat[...] = np.abs(st.q_heat) + 60.0
+    st.sw_net[...] = 0.5 * st.q_heat + 150.0 * (np.arange(st.nx)[:, None] % 3 == 0)
+    st.sw_net[:, ::3] = 0.0
+
+
+def test_qsw_penetration_standalone(VP, oracle):
+    """sw_source = "q_sw": the penetration moves sw_pen_frac q_sw down the
+    column (apply_sw_penetration_impl with sw_net), bitwise."""
+    cols = columns(nx=40, ny=12, nz=20, seed=91, thin_frac=0.2)
+    cols.h[:10, :, -1] = 1.0e-4
+    cfg = hot_cfg(budgets=1, surface_flux=1, sw_source=1, **SW)
+    st = oracle_state(oracle, cols, cfg)
+    _sunlit_qsw(st)
+    vp = loaded(VP, cols, cfg)
+    vp.set("q_heat", st.q_heat)
+    vp.set("sw_net", st.sw_net)
+    for _ in range(2):
+        st.call("vpo_surface_flux", cfg, DT)
+        st.call("vpo_sw_penetration", cfg, DT)
+        vp.surface_flux(DT)
+        vp.sw_penetration(DT)
+    for t in range(st.ntr):
+        assert_bitwise(f"tracer{t}", vp.get_tracer(t), st.tracers[t])
+    assert_bitwise("heat_budget_surface", vp.get("heat_budget_surface"), st.heat_budget_surface)
+
+
+@pytest.mark.parametrize("method", [2, 3])
+def test_step_with_qsw(VP, oracle, method):
+    """Whole steps under sw_source = "q_sw": deposit, penetration, KPP's B0
+    charge and the non-local deposit all read q_sw; bitwise."""
+    cols = columns(nx=30, ny=18, nz=16, seed=92, thin_frac=0.1)
+    cfg = hot_cfg(budgets=1, surface_flux=1, sw_source=1, kpp_sw_method=method, **SW)
+    st = oracle_state(oracle, cols, cfg)
+    _sunlit_qsw(st)
+    vp = loaded(VP, cols, cfg)
+    vp.set("q_heat", st.q_heat)
+    vp.set("sw_net", st.sw_net)
+    assert st.call("vpo_step", cfg, DT, 3) == 0
+    vp.step(DT, 3)
+    for t in range(st.ntr):
+        assert_bitwise(f"tracer{t}", vp.get_tracer(t), st.tracers[t])
+    for n in ("kv", "kt", "bl_depth", "b0", "heat_budget", "heat_budget_surface"):
+        assert_bitwise(n, vp.get(n), getattr(st, n))
+
+
+@pytest.mark.parametrize("budgets", [0, 1])
+def test_bound_salinity_and_wet_dyn(VP, oracle, budgets):
+    """BOUND_SALINITY (the first live layer floored at min_salinity after the
+    deposit) and the dynamic wet/dry mask on the deposit, bitwise, standalone
+    and through whole steps."""
+    cols = columns(nx=33, ny=17, nz=12, seed=93, thin_frac=0.15)
+    cols.h[:8, :, -1] = 1.0e-4
+    cfg = hot_cfg(budgets=budgets, surface_flux=1, bound_salinity=1, min_salinity=34.9, use_wet_dyn=1)
+    st = oracle_state(oracle, cols, cfg)
+    st.wet_dyn[...] = ((np.arange(st.nx)[:, None] + 2 * np.arange(st.ny)[None, :]) % 5 != 0).astype(float)
+    vp = loaded(VP, cols, cfg)
+    vp.set("wet_dyn", st.wet_dyn)
+    st.call("vpo_surface_flux", cfg, DT)
+    vp.surface_flux(DT)
+    for t in range(st.ntr):
+        assert_bitwise(f"tracer{t}", vp.get_tracer(t), st.tracers[t])
+    assert st.call("vpo_step", cfg, DT, 2) == 0
+    vp.step(DT, 2)
+    for t in range(st.ntr):
+        assert_bitwise(f"tracer{t}", vp.get_tracer(t), st.tracers[t])
+    if budgets:
+        assert_bitwise("salt_budget_surface", vp.get("salt_budget_surface"), st.salt_budget_surface)
