@@ -105,7 +105,7 @@ def field_shape(field: int, nx: int, ny: int, nz: int):
                  FIELD_KD_EPBL):
         return (nx, ny, nz + 1)
     if field in (FIELD_BL_DEPTH, FIELD_B0, FIELD_STRESS_MAG, FIELD_Q_HEAT, FIELD_Q_SALT, FIELD_WET, FIELD_CORIOLIS,
-                 FIELD_MLD_EPBL, FIELD_LA_EPBL) or field in FIELD_EPBL_TKE.values():
+                 FIELD_MLD_EPBL, FIELD_LA_EPBL, FIELD_SW_NET, FIELD_WET_DYN) or field in FIELD_EPBL_TKE.values():
         return (nx, ny)
     if field in (FIELD_TAU_X, FIELD_LAMBDA_BOT_U, FIELD_K_TOP_U, FIELD_K_BOT_U):
         return (nx + 1, ny)

@@ -123,3 +123,12 @@ def test_epbl_knobs_are_validated(lib):
         EPBL(langmuir=object())
     lt = EPBL(langmuir=Langmuir(scheme="additive", coef=0.3)).apply(default_config())
     assert (lt.epbl_use_lt, lt.epbl_lt_scheme, lt.epbl_lt_enhance_coef) == (1, 2, 0.3)
+
+
+def test_every_named_field_has_a_shape():
+    """Each field the python mirror names maps to a Fortran-order shape."""
+    from roundabout_b200 import _ffi
+
+    for name, fid in _ffi.FIELD_NAMES.items():
+        shp = _ffi.field_shape(fid, 5, 4, 3)
+        assert len(shp) in (2, 3) and all(n > 0 for n in shp), name
