@@ -70,6 +70,9 @@ extern "C" {
 #define VPHYS_INTERIOR_PP81 1
 #define VPHYS_INTERIOR_NONE 4
 
+/* most bands of the chlorophyll shortwave scheme (MAX_SW_BANDS) */
+#define VPHYS_SW_NB_MAX 6
+
 /* ---- configuration ---------------------------------------------------
  * Every knob the path reads, with the reference default
  * (ocean_vmix_t rdb_ocean_vmix.F90:198-483; ocean_vdiff_t
@@ -289,6 +292,20 @@ typedef struct vphys_config {
      * (epbl_sw_ctke, rdb_ocean_epbl.F90:356-360, 905); 0 treats all of the
      * heat flux as a skin flux even with sw_pen_frac != 0 */
     int epbl_sw_ctke;         /* 1 */
+    /* Manizza (2005) chlorophyll N-band shortwave (sw_scheme = "manizza05";
+     * rdb_ocean_surface_flux.F90:742-812, 1606-1668, rdb_ocean_sw_chl.F90):
+     * the whole shortwave (sw_pen_frac must be 1) is absorbed in sw_nbands
+     * bands, T(d) = sum_n frac_n exp(-kappa_n d), with frac the visible 0.42
+     * split blue / red by sw_blue_frac and the rest shared evenly by bands
+     * 3..n, and kappa_n the per-column opacities of the SW_KAPPA field
+     * (vphys_sw_chl_apply fills them from the CHL field).  Read by the
+     * penetration, KPP's B0 charge and EPBL's shortwave ledger. */
+    int sw_chl;               /* 0 */
+    int sw_nbands;            /* 3, in [3, VPHYS_SW_NB_MAX] */
+    double sw_blue_frac;      /* 0.5 */
+    double sw_opacity_coef[2 * VPHYS_SW_NB_MAX]; /* (a_n, b_n) pairs, m-1: 0.0232 0.074, 0.225 0.037, 2.86 0 */
+    double sw_chl_power[VPHYS_SW_NB_MAX];        /* p_n: 0.674, 0.629, 0 */
+    double sw_opacity_land;   /* 10: kappa on land columns */
 } vphys_config;
 
 #define VPHYS_KPP_SW_ALL 1
@@ -345,6 +362,10 @@ enum vphys_field {
                                    when sw_source = 1 (allocated then) */
     VPHYS_FIELD_WET_DYN = 42,   /* in      (nx, ny) dynamic wet/dry cell mask, 1 wet, 0 dry (use_wet_dyn = 1;
                                    allocated then, filled with 1) */
+    VPHYS_FIELD_SW_CHL = 43,    /* in      (nx, ny) surface chlorophyll, mg m-3 (sw_chl = 1; filled with the
+                                   1e-4 floor) */
+    VPHYS_FIELD_SW_KAPPA = 44,  /* in/out  (nx, ny, VPHYS_SW_NB_MAX) band opacities, m-1, the first
+                                   sw_nbands planes read (sw_chl = 1; filled with 1) */
     VPHYS_FIELD_TRACER0 = 64    /* in/out  (nx, ny, nz); tracer t is
                                    VPHYS_FIELD_TRACER0 + t */
 };
@@ -440,6 +461,15 @@ int vphys_surface_flux(vphys_handle h, double dt);
  * at rdb_ocean_dyn.F90:1375 right after the surface deposit; vphys_step runs
  * it there when surface_flux is 1. */
 int vphys_sw_penetration(vphys_handle h, double dt);
+
+/* The band opacities of the chlorophyll shortwave scheme from the CHL field:
+ * SW_KAPPA(:,:,n) = a_n + b_n max(chl, 1e-4)^p_n on wet columns (the safe
+ * pow, rdb_sm_pow), sw_opacity_land on land, for n = 1..sw_nbands.
+ * Replaces sw_chl_fill_kappa / sw_kappa_band_impl / sw_opacity_manizza
+ * (rdb_ocean_sw_chl.F90:160-190, rdb_ocean_surface_flux.F90:784-793), run by
+ * sw_chl_apply after each chlorophyll read.  VPHYS_ERR_CONFIG unless
+ * sw_chl = 1. */
+int vphys_sw_chl_apply(vphys_handle h);
 
 /* Kappa-shear, column form: per wet column, the JHL08 steady (kappa, TKE)
  * pair solved surface-down on the interfaces with adaptive substepping over

@@ -28,7 +28,7 @@ class VpoState(ctypes.Structure):
                           "visc_rem_u", "visc_rem_v", "gamma_t", "gamma_s", "heat_budget", "salt_budget")
     ] + [(n, _ip) for n in ("k_top_u", "k_top_v", "k_bot_u", "k_bot_v")] + [("tr", ctypes.POINTER(_dp))] + [
         (n, _dp) for n in ("heat_budget_surface", "salt_budget_surface", "coriolis", "kd_shear", "tke_shear", "kd_epbl",
-                          "mld_epbl", "la_epbl")] + [("epbl_tke", _dp * 6)] + [(n, _dp) for n in ("sw_net", "wet_dyn")]
+                          "mld_epbl", "la_epbl")] + [("epbl_tke", _dp * 6)] + [(n, _dp) for n in ("sw_net", "wet_dyn", "sw_chl", "sw_kappa")]
 
 
 def build(force: bool = False) -> Path:
@@ -65,7 +65,8 @@ def lib():
         L.vpo_set_threads.argtypes = [ctypes.c_int]
         L.vpo_get_threads.restype = ctypes.c_int
         for name in ("vpo_eos_wright", "vpo_pp81", "vpo_seed_interior_none", "vpo_kpp_overlay",
-                     "vpo_kv_ml_invz2", "vpo_convection", "vpo_split", "vpo_kappa_shear_merge", "vpo_epbl_merge"):
+                     "vpo_kv_ml_invz2", "vpo_convection", "vpo_split", "vpo_kappa_shear_merge", "vpo_epbl_merge",
+                     "vpo_sw_chl_kappa"):
             getattr(L, name).argtypes = [ctypes.c_void_p, ctypes.POINTER(VpoState)]
             getattr(L, name).restype = None
         L.vpo_stress_mag.argtypes = [ctypes.POINTER(VpoState)]
@@ -136,6 +137,8 @@ class OracleState:
         self.epbl_tke = [f(nx, ny) for _ in range(6)]   # wind, conv, forcing, mixing, mech_decay, conv_decay
         self.sw_net = f(nx, ny)
         self.wet_dyn = np.ones((nx, ny), dtype=np.float64, order="F")
+        self.sw_chl = np.full((nx, ny), 1.0e-4, dtype=np.float64, order="F")
+        self.sw_kappa = np.ones((nx, ny, 6), dtype=np.float64, order="F")
         self.k_top_u = np.full((nx + 1, ny), nz, dtype=np.int32, order="F")
         self.k_top_v = np.full((nx, ny + 1), nz, dtype=np.int32, order="F")
         self.k_bot_u = np.ones((nx + 1, ny), dtype=np.int32, order="F")

@@ -608,6 +608,47 @@ static inline double sw_transmission(const vphys_config *c, double d)
     return c->sw_band_ratio * vpo_sm_exp(-d / c->sw_zeta1) + (1.0 - c->sw_band_ratio) * vpo_sm_exp(-d / c->sw_zeta2);
 }
 
+/* sw_band_fractions (rdb_ocean_surface_flux.F90:767-782): band n (1-based)
+ * of nb carries blue 0.42 / (1 - blue) 0.42 of the visible, or an even share
+ * of the near-infrared 0.58 for n >= 3. */
+double vpo_sw_band_frac(int n, int nb, double blue)
+{
+    const double vis = 0.42;
+    if (n == 1) return blue * vis;
+    if (n == 2) return (1.0 - blue) * vis;
+    return (1.0 - vis) / (double)(nb - 2);
+}
+
+/* sw_transmission_nb (:795-812): sum_n frac_n exp(-kappa_n(i,j) d). */
+double vpo_sw_transmission_nb(const vphys_config *c, const vpo_state *s, int i, int j, double d)
+{
+    const int nx = s->nx, ny = s->ny;
+    double trans = 0.0;
+    for (int n = 1; n <= c->sw_nbands; ++n)
+        trans = trans + vpo_sw_band_frac(n, c->sw_nbands, c->sw_blue_frac) *
+                            vpo_sm_exp(-(s->sw_kappa[(size_t)(i - 1) + (size_t)nx * (j - 1) + (size_t)nx * ny * (n - 1)] * d));
+    return trans;
+}
+
+/* sw_chl_fill_kappa -> sw_kappa_band_impl (rdb_ocean_sw_chl.F90:160-190) with
+ * sw_opacity_manizza (rdb_ocean_surface_flux.F90:784-793): kappa_n =
+ * a_n + b_n rdb_sm_pow(max(chl, 1e-4), p_n) on wet columns, the land value
+ * elsewhere. */
+void vpo_sw_chl_kappa(const vphys_config *c, vpo_state *s)
+{
+    const int nx = s->nx, ny = s->ny;
+    for (int n = 1; n <= c->sw_nbands; ++n)
+        for (int j = 1; j <= ny; ++j)
+            for (int i = 1; i <= nx; ++i) {
+                const size_t at = (size_t)(i - 1) + (size_t)nx * (j - 1) + (size_t)nx * ny * (n - 1);
+                s->sw_kappa[at] = C2(s->wet, i, j) > 0.5
+                                      ? c->sw_opacity_coef[2 * n - 2] +
+                                            c->sw_opacity_coef[2 * n - 1] *
+                                                vpo_sm_pow(fmx(C2(s->sw_chl, i, j), 1.0e-4), c->sw_chl_power[n - 1])
+                                      : c->sw_opacity_land;
+            }
+}
+
 /* The kinematic heat flux B0 charges (rdb_ocean_vmix.F90:1321-1348 in pass 1
  * with the lagged h_b, 1440-1466 in pass 2 with the new one): with
  * shortwave penetration on, Q_heat minus the penetrating part that passes
@@ -619,7 +660,12 @@ static inline double kpp_q_t_kin(const vphys_config *c, const vpo_state *s, int 
     if (c->sw_pen_frac != 0.0) {
         const double *sw = vpo_sw_source(c, s);
         double q_bl = C2(s->q_heat, i, j);
-        if (c->kpp_sw_method == VPHYS_KPP_SW_MXL)
+        if (c->sw_chl) {   /* the N-band twin, :1326-1336 */
+            if (c->kpp_sw_method == VPHYS_KPP_SW_MXL)
+                q_bl = q_bl - c->sw_pen_frac * C2(sw, i, j) * vpo_sw_transmission_nb(c, s, i, j, h_b);
+            else if (c->kpp_sw_method == VPHYS_KPP_SW_LV1)
+                q_bl = q_bl - c->sw_pen_frac * C2(sw, i, j) * vpo_sw_transmission_nb(c, s, i, j, C3(s->h, i, j, k_sfc));
+        } else if (c->kpp_sw_method == VPHYS_KPP_SW_MXL)
             q_bl = q_bl - c->sw_pen_frac * C2(sw, i, j) * sw_transmission(c, h_b);
         else if (c->kpp_sw_method == VPHYS_KPP_SW_LV1)
             q_bl = q_bl - c->sw_pen_frac * C2(sw, i, j) * sw_transmission(c, C3(s->h, i, j, k_sfc));
@@ -1369,7 +1415,10 @@ void vpo_sw_penetration(const vphys_config *c, vpo_state *s, double dt)
     for (int j = 1; j <= ny; ++j) {
         for (int i = 1; i <= nx; ++i) {
             const int kt = first_live(s->h, nx, ny, i, j, nz);
-            const double i0col = c->sw_pen_frac * C2(vpo_sw_source(c, s), i, j) * C2(s->wet, i, j);
+            /* the chlorophyll scheme absorbs all of the source (apply_sw_penetration_nb_impl, 1606-1668) */
+            const int nbs = c->sw_chl;
+            const double i0col = nbs ? C2(vpo_sw_source(c, s), i, j) * C2(s->wet, i, j)
+                                     : c->sw_pen_frac * C2(vpo_sw_source(c, s), i, j) * C2(s->wet, i, j);
             int k_dep = 1;
             for (int k = 1; k <= nz; ++k) {
                 if (C3(s->h, i, j, k) > H_VANISHED) {
@@ -1378,11 +1427,12 @@ void vpo_sw_penetration(const vphys_config *c, vpo_state *s, double dt)
                 }
             }
             double d_top = 0.0;
-            double trans_top = sw_transmission(c, d_top);
+            double trans_top = nbs ? vpo_sw_transmission_nb(c, s, i, j, d_top) : sw_transmission(c, d_top);
             for (int k = nz; k >= k_dep; --k) {
                 const double hk = C3(s->h, i, j, k);
                 const double d_bot = d_top + hk;
-                const double trans_bot = (k > k_dep) ? sw_transmission(c, d_bot) : 0.0;
+                const double trans_bot =
+                    (k > k_dep) ? (nbs ? vpo_sw_transmission_nb(c, s, i, j, d_bot) : sw_transmission(c, d_bot)) : 0.0;
                 if (hk > H_VANISHED) {
                     const double absorbed = i0col * (trans_top - trans_bot);
                     double add = inv_scale * absorbed;

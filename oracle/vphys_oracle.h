@@ -50,7 +50,13 @@ typedef struct vpo_state {
     double *epbl_tke[6];                    /* (nx,ny) EPBL TKE budget terms, written when epbl_tke_diags */
     double *sw_net;                         /* (nx,ny) the shortwave source under sw_source = 1 */
     double *wet_dyn;                        /* (nx,ny) dynamic wet mask, read under use_wet_dyn */
+    double *sw_chl;                         /* (nx,ny) surface chlorophyll, mg m-3 */
+    double *sw_kappa;                       /* (nx,ny,VPHYS_SW_NB_MAX) chlorophyll-scheme band opacities */
 } vpo_state;
+
+void vpo_sw_chl_kappa(const vphys_config *c, vpo_state *s);
+double vpo_sw_band_frac(int n, int nb, double blue);
+double vpo_sw_transmission_nb(const vphys_config *c, const vpo_state *s, int i, int j, double d);
 
 /* The shortwave source the configuration selects (ocean_surfflux_set_sw's
  * sw_from_qsw, rdb_ocean_surface_flux.F90:715-740): Q_heat, or the net

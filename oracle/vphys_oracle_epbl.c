@@ -303,6 +303,21 @@ void vpo_epbl(const vphys_config *c, vpo_state *s, double dt)
                 dch_s[k] = dmass * dsv_ds_k;
                 if (k > k_sfc) {
                     ctke_sw[k] = 0.0;   /* dead layers above the live surface take no light */
+                } else if (sw_on && c->sw_chl) {
+                    /* the chlorophyll N-band ledger (1143-1164): per band, the
+                     * difference form with the opaque bed at k = 1 */
+                    const double d_bot_sw = d_top_sw + hk;
+                    double phi_sum = 0.0;
+                    for (int n = 1; n <= c->sw_nbands; ++n) {
+                        const double kn = s->sw_kappa[(size_t)(i - 1) + (size_t)nx * (j - 1) + (size_t)nx * ny * (n - 1)];
+                        const double ea = vpo_sm_exp(-(kn * d_top_sw));
+                        const double eb = (k > 1) ? vpo_sm_exp(-(kn * d_bot_sw)) : 0.0;
+                        const double heat_nb =
+                            i0_col * vpo_sw_band_frac(n, c->sw_nbands, c->sw_blue_frac) * inv_rho0_cp * dt * (ea - eb);
+                        phi_sum = phi_sum + heat_nb * sw_pe_cost_shape(hk * kn);
+                    }
+                    ctke_sw[k] = -0.5 * GRAVITY * rho0 * dch_t[k] * phi_sum;
+                    d_top_sw = d_bot_sw;
                 } else if (sw_on) {
                     /* absorbed heat per band, difference form, opaque bed at k = 1 */
                     const double d_bot_sw = d_top_sw + hk;

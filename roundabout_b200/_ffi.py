@@ -73,6 +73,9 @@ FIELD_LA_EPBL = 34
 FIELD_EPBL_TKE = {"wind": 35, "conv": 36, "forcing": 37, "mixing": 38, "mech_decay": 39, "conv_decay": 40}
 FIELD_SW_NET = 41
 FIELD_WET_DYN = 42
+FIELD_SW_CHL = 43
+FIELD_SW_KAPPA = 44
+SW_NB_MAX = 6
 FIELD_TRACER0 = 64
 
 FIELD_NAMES = {
@@ -86,7 +89,8 @@ FIELD_NAMES = {
     "k_bot_v": FIELD_K_BOT_V, "coriolis": FIELD_CORIOLIS,
     "heat_budget_surface": FIELD_HEAT_BUDGET_SURFACE, "salt_budget_surface": FIELD_SALT_BUDGET_SURFACE,
     "kd_shear": FIELD_KD_SHEAR, "tke_shear": FIELD_TKE_SHEAR, "kd_epbl": FIELD_KD_EPBL, "mld_epbl": FIELD_MLD_EPBL,
-    "la_epbl": FIELD_LA_EPBL, "sw_net": FIELD_SW_NET, "wet_dyn": FIELD_WET_DYN,
+    "la_epbl": FIELD_LA_EPBL, "sw_net": FIELD_SW_NET, "wet_dyn": FIELD_WET_DYN, "sw_chl": FIELD_SW_CHL,
+    "sw_kappa": FIELD_SW_KAPPA,
     **{f"epbl_tke_{k}": v for k, v in FIELD_EPBL_TKE.items()},
 }
 INT_FIELDS = (FIELD_K_TOP_U, FIELD_K_TOP_V, FIELD_K_BOT_U, FIELD_K_BOT_V)
@@ -105,12 +109,14 @@ def field_shape(field: int, nx: int, ny: int, nz: int):
                  FIELD_KD_EPBL):
         return (nx, ny, nz + 1)
     if field in (FIELD_BL_DEPTH, FIELD_B0, FIELD_STRESS_MAG, FIELD_Q_HEAT, FIELD_Q_SALT, FIELD_WET, FIELD_CORIOLIS,
-                 FIELD_MLD_EPBL, FIELD_LA_EPBL, FIELD_SW_NET, FIELD_WET_DYN) or field in FIELD_EPBL_TKE.values():
+                 FIELD_MLD_EPBL, FIELD_LA_EPBL, FIELD_SW_NET, FIELD_WET_DYN, FIELD_SW_CHL) or field in FIELD_EPBL_TKE.values():
         return (nx, ny)
     if field in (FIELD_TAU_X, FIELD_LAMBDA_BOT_U, FIELD_K_TOP_U, FIELD_K_BOT_U):
         return (nx + 1, ny)
     if field in (FIELD_TAU_Y, FIELD_LAMBDA_BOT_V, FIELD_K_TOP_V, FIELD_K_BOT_V):
         return (nx, ny + 1)
+    if field == FIELD_SW_KAPPA:
+        return (nx, ny, SW_NB_MAX)
     raise KeyError(field)
 
 
@@ -163,10 +169,17 @@ class VphysConfig(ctypes.Structure):
             "epbl_lt_lac1", "epbl_lt_lac2", "epbl_lt_lac3", "epbl_lt_lac4", "epbl_lt_lac5")] + [
         ("epbl_tke_diags", ctypes.c_int), ("ks_massless_merge", ctypes.c_int),
         ("sw_source", ctypes.c_int), ("bound_salinity", ctypes.c_int), ("use_wet_dyn", ctypes.c_int),
-        ("min_salinity", ctypes.c_double), ("epbl_sw_ctke", ctypes.c_int)]
+        ("min_salinity", ctypes.c_double), ("epbl_sw_ctke", ctypes.c_int),
+        ("sw_chl", ctypes.c_int), ("sw_nbands", ctypes.c_int), ("sw_blue_frac", ctypes.c_double),
+        ("sw_opacity_coef", ctypes.c_double * (2 * SW_NB_MAX)), ("sw_chl_power", ctypes.c_double * SW_NB_MAX),
+        ("sw_opacity_land", ctypes.c_double)]
 
     def as_dict(self):
-        return {n: getattr(self, n) for n, _ in self._fields_ if n not in ()}
+        out = {}
+        for n, _ in self._fields_:
+            v = getattr(self, n)
+            out[n] = list(v) if isinstance(v, ctypes.Array) else v   # the band-coefficient arrays by value
+        return out
 
 
 class LibraryNotFoundError(FileNotFoundError):
@@ -229,6 +242,7 @@ _PROTOTYPES = {
     "vphys_stress_mag": (ctypes.c_int, [ctypes.c_void_p]),
     "vphys_surface_flux": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "vphys_sw_penetration": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    "vphys_sw_chl_apply": (ctypes.c_int, [ctypes.c_void_p]),
     "vphys_kappa_shear": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "vphys_epbl": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "vphys_mixed_redo_count": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint)]),

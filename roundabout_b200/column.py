@@ -152,6 +152,10 @@ class VerticalPhysics:
         """ocean_surface_flux_apply_tracers (rdb_ocean_surface_flux.F90:959-1070)."""
         _ffi.check(self.lib.vphys_surface_flux(self._h, float(dt)), "vphys_surface_flux")
 
+    def sw_chl_apply(self):
+        """sw_chl_fill_kappa (rdb_ocean_sw_chl.F90:160-190): the band opacities from the sw_chl field."""
+        _ffi.check(self.lib.vphys_sw_chl_apply(self._h), "vphys_sw_chl_apply")
+
     def sw_penetration(self, dt):
         """ocean_surface_flux_apply_sw_penetration (rdb_ocean_surface_flux.F90:1255-1370)."""
         _ffi.check(self.lib.vphys_sw_penetration(self._h, float(dt)), "vphys_sw_penetration")

@@ -156,6 +156,14 @@ def default_config() -> VphysConfig:
     c.use_wet_dyn = 0
     c.min_salinity = 0.0
     c.epbl_sw_ctke = 1
+    c.sw_chl = 0
+    c.sw_nbands = 3
+    c.sw_blue_frac = 0.5
+    for n, v in enumerate((0.0232, 0.074, 0.225, 0.037, 2.86, 0.0)):
+        c.sw_opacity_coef[n] = v
+    c.sw_chl_power[0] = 0.674
+    c.sw_chl_power[1] = 0.629
+    c.sw_opacity_land = 10.0
     return c
 
 

@@ -50,7 +50,7 @@ int cuda_status(cudaError_t e, const char *where)
     return push_error(VPHYS_ERR_CUDA, "%s: CUDA error %d (%s)", where, (int)e, cudaGetErrorString(e));
 }
 
-constexpr int NFIXED = 43;
+constexpr int NFIXED = 45;
 constexpr unsigned MAGIC = 0x56504859u;   // "VPHY"
 
 struct Field {
@@ -132,6 +132,7 @@ size_t field_count(int nx, int ny, int nz, int field, bool *is_int)
     case VPHYS_FIELD_KD_SHEAR:
     case VPHYS_FIELD_TKE_SHEAR:
     case VPHYS_FIELD_KD_EPBL: return X * Y * (Z + 1);
+    case VPHYS_FIELD_SW_KAPPA: return X * Y * VPHYS_SW_NB_MAX;
     case VPHYS_FIELD_BL_DEPTH:
     case VPHYS_FIELD_B0:
     case VPHYS_FIELD_STRESS_MAG:
@@ -141,6 +142,7 @@ size_t field_count(int nx, int ny, int nz, int field, bool *is_int)
     case VPHYS_FIELD_CORIOLIS:
     case VPHYS_FIELD_SW_NET:
     case VPHYS_FIELD_WET_DYN:
+    case VPHYS_FIELD_SW_CHL:
     case VPHYS_FIELD_MLD_EPBL:
     case VPHYS_FIELD_LA_EPBL:
     case VPHYS_FIELD_EPBL_TKE_WIND:
@@ -194,7 +196,9 @@ int init_field(vphys_handle h, int field, Field &fl)
     cudaStream_t s = h->stream;
     switch (field) {
     case VPHYS_FIELD_WET:
-    case VPHYS_FIELD_WET_DYN: k_fill_double<<<fill_blocks(fl.n), 256, 0, s>>>((double *)fl.own, fl.n, 1.0); break;
+    case VPHYS_FIELD_WET_DYN:
+    case VPHYS_FIELD_SW_KAPPA: k_fill_double<<<fill_blocks(fl.n), 256, 0, s>>>((double *)fl.own, fl.n, 1.0); break;
+    case VPHYS_FIELD_SW_CHL: k_fill_double<<<fill_blocks(fl.n), 256, 0, s>>>((double *)fl.own, fl.n, 1.0e-4); break;
     case VPHYS_FIELD_KV: k_fill_interfaces<<<fill_blocks(fl.n), 256, 0, s>>>((double *)fl.own, plane, h->nz, h->cfg.pp81_nu_bg); break;
     case VPHYS_FIELD_KT:
     case VPHYS_FIELD_KS: k_fill_interfaces<<<fill_blocks(fl.n), 256, 0, s>>>((double *)fl.own, plane, h->nz, h->cfg.pp81_kappa_bg); break;
@@ -236,6 +240,8 @@ int prepare_sources(vphys_handle h)
     int st = VPHYS_OK;
     if (h->cfg.sw_source && (st = ensure(h, VPHYS_FIELD_SW_NET))) return st;
     if (h->cfg.use_wet_dyn && (st = ensure(h, VPHYS_FIELD_WET_DYN))) return st;
+    if (h->cfg.sw_chl && (st = ensure(h, VPHYS_FIELD_SW_CHL))) return st;
+    if (h->cfg.sw_chl && (st = ensure(h, VPHYS_FIELD_SW_KAPPA))) return st;
     return st;
 }
 
@@ -282,6 +288,18 @@ int validate(const vphys_config *c, int ntr)
         return push_error(VPHYS_ERR_CONFIG, "bound_salinity must be 0 or 1");
     if (c->use_wet_dyn < 0 || c->use_wet_dyn > 1) return push_error(VPHYS_ERR_CONFIG, "use_wet_dyn must be 0 or 1");
     if (c->epbl_sw_ctke < 0 || c->epbl_sw_ctke > 1) return push_error(VPHYS_ERR_CONFIG, "epbl_sw_ctke must be 0 or 1");
+    if (c->sw_chl < 0 || c->sw_chl > 1) return push_error(VPHYS_ERR_CONFIG, "sw_chl must be 0 or 1");
+    if (c->sw_chl) {
+        // rdb_config_validate.F90:291-310, rdb_ocean_sw_chl.F90:87-103
+        if (c->sw_pen_frac != 1.0)
+            return push_error(VPHYS_ERR_CONFIG, "sw_chl band-absorbs the whole shortwave: sw_pen_frac must be 1");
+        if (c->sw_nbands < 3 || c->sw_nbands > VPHYS_SW_NB_MAX)
+            return push_error(VPHYS_ERR_CONFIG, "sw_nbands must be in [3, %d]", VPHYS_SW_NB_MAX);
+        for (int n = 0; n < c->sw_nbands; ++n)
+            if (!(c->sw_opacity_coef[2 * n] > 0.0))
+                return push_error(VPHYS_ERR_CONFIG, "sw_opacity_coef: band %d needs a positive clear-water opacity",
+                                  n + 1);
+    }
     // the inner solve must run at least once (the substep's adaptive-dt bands
     // read its decay lengths); both caps bound the per-column work
     if (c->ks_max_inner_it < 1 || c->ks_max_inner_it > 10000)
@@ -340,6 +358,7 @@ Params make_params(vphys_handle h)
     p.wet = D(VPHYS_FIELD_WET);
     p.sw_src = h->cfg.sw_source ? D(VPHYS_FIELD_SW_NET) : p.q_heat;
     p.wet_dyn = h->cfg.use_wet_dyn ? D(VPHYS_FIELD_WET_DYN) : nullptr;
+    p.sw_kappa = h->cfg.sw_chl ? D(VPHYS_FIELD_SW_KAPPA) : nullptr;
     p.tau_x = D(VPHYS_FIELD_TAU_X);
     p.tau_y = D(VPHYS_FIELD_TAU_Y);
     p.lambda_bot_u = D(VPHYS_FIELD_LAMBDA_BOT_U);
@@ -704,6 +723,14 @@ int vphys_config_default(vphys_config *c)
     memset(c, 0, sizeof *c);
     c->use_closure = 1;
     c->epbl_sw_ctke = 1;
+    // Manizza (2005) three-band defaults (rdb_config.F90:336-360)
+    c->sw_nbands = 3;
+    c->sw_blue_frac = 0.5;
+    const double coef[6] = {0.0232, 0.074, 0.225, 0.037, 2.86, 0.0};
+    for (int n = 0; n < 6; ++n) c->sw_opacity_coef[n] = coef[n];
+    c->sw_chl_power[0] = 0.674;
+    c->sw_chl_power[1] = 0.629;
+    c->sw_opacity_land = 10.0;
     c->interior_closure = VPHYS_INTERIOR_PP81;
     c->pp81_nu0 = 1.0e-2;
     c->pp81_nu_bg = 1.0e-4;
@@ -928,7 +955,9 @@ int vphys_bind(vphys_handle h, int field, void *device_ptr)
     if (!device_ptr && !h->f[sl].own) {
         // restore a handle-owned buffer only for core fields / tracers
         if (sl < VPHYS_FIELD_LAMBDA_BOT_U || sl >= NFIXED) return ensure(h, field);
-        if (sl == VPHYS_FIELD_SW_NET || sl == VPHYS_FIELD_WET_DYN) return prepare_sources(h);
+        if (sl == VPHYS_FIELD_SW_NET || sl == VPHYS_FIELD_WET_DYN || sl == VPHYS_FIELD_SW_CHL ||
+            sl == VPHYS_FIELD_SW_KAPPA)
+            return prepare_sources(h);
     }
     return VPHYS_OK;
 }
@@ -1063,6 +1092,17 @@ int vphys_sw_penetration(vphys_handle h, double dt)
     Params p = make_params(h);
     vphys::launch_sw_penetration(p, inv_heat, h->stream);
     return cuda_status(cudaGetLastError(), "vphys_sw_penetration launch");
+}
+
+int vphys_sw_chl_apply(vphys_handle h)
+{
+    if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_sw_chl_apply: bad handle");
+    if (!h->cfg.sw_chl) return push_error(VPHYS_ERR_CONFIG, "vphys_sw_chl_apply: sw_chl is 0");
+    int st = prepare_sources(h);
+    if (st) return st;
+    Params p = make_params(h);
+    vphys::launch_sw_chl_kappa(p, (const double *)h->f[VPHYS_FIELD_SW_CHL].ptr(), h->stream);
+    return cuda_status(cudaGetLastError(), "vphys_sw_chl_apply");
 }
 
 int vphys_kappa_shear(vphys_handle h, double dt)

@@ -562,11 +562,33 @@ static __device__ __noinline__ double sw_q_bl(double q_heat, const double *sw, d
 {
     return q_heat - pen * *sw * (R * sm_exp(xdiv(-d, zeta1)) + (1.0 - R) * sm_exp(xdiv(-d, zeta2)));
 }
-__device__ __forceinline__ double kpp_q_t_kin(const vphys_config &c, double q_heat, const double *sw, double h_b,
-                                              double h_sfc)
+// The chlorophyll scheme's share of the shortwave in band n (1-based) of nb
+// (sw_band_fractions, rdb_ocean_surface_flux.F90:767-782): the visible 0.42
+// split blue / red, the near infrared shared evenly by bands 3..nb.
+constexpr double SW_VIS_FRAC = 0.42;
+__device__ __forceinline__ double sw_band_frac(int n, int nb, double blue)
+{
+    if (n == 1) return blue * SW_VIS_FRAC;
+    if (n == 2) return (1.0 - blue) * SW_VIS_FRAC;
+    return xdiv(1.0 - SW_VIS_FRAC, (double)(nb - 2));
+}
+// sw_transmission_nb (:795-812): sum_n frac_n exp(-kappa_n d), kappa_n at
+// kap[(n-1) plane]
+static __device__ __noinline__ double sw_transmission_nb(double d, const double *kap, size_t plane, int nb,
+                                                         double blue)
+{
+    double trans = 0.0;
+    for (int n = 1; n <= nb; ++n) trans = trans + sw_band_frac(n, nb, blue) * sm_exp(-(kap[(size_t)(n - 1) * plane] * d));
+    return trans;
+}
+__device__ __forceinline__ double kpp_q_t_kin(const vphys_config &c, double q_heat, const double *sw, const double *kap,
+                                              size_t plane, double h_b, double h_sfc)
 {
     if (c.sw_pen_frac != 0.0 && c.kpp_sw_method != VPHYS_KPP_SW_ALL) {
         const double d = (c.kpp_sw_method == VPHYS_KPP_SW_MXL) ? h_b : h_sfc;
+        if (c.sw_chl)
+            return xdiv(q_heat - c.sw_pen_frac * *sw * sw_transmission_nb(d, kap, plane, c.sw_nbands, c.sw_blue_frac),
+                        c.rho0 * c.cp);
         return xdiv(sw_q_bl(q_heat, sw, d, c.sw_pen_frac, c.sw_band_ratio, c.sw_zeta1, c.sw_zeta2), c.rho0 * c.cp);
     }
     return xdiv(q_heat, c.rho0 * c.cp);

@@ -183,6 +183,24 @@ __device__ __forceinline__ double sw_pe_cost_shape(double tau)
     return xdiv(tau * (1.0 + sm_exp(-tau)) - 2.0 * em1, tau * em1);
 }
 
+// The chlorophyll N-band ledger of one live layer (rdb_ocean_epbl.F90:
+// 1143-1164): per band the heat absorbed between the layer's top and bottom
+// (the bed opaque), weighted by the PE-cost shape at the band's optical depth.
+static __device__ __noinline__ double sw_phi_nb(double i0, const double *kap, size_t plane, int nb, double blue,
+                                                double inv_rho0_cp, double dt, double d_top, double d_bot, double hk,
+                                                bool bed)
+{
+    double phi_sum = 0.0;
+    for (int n = 1; n <= nb; ++n) {
+        const double kn = kap[(size_t)(n - 1) * plane];
+        const double ea = sm_exp(-(kn * d_top));
+        const double eb = bed ? 0.0 : sm_exp(-(kn * d_bot));
+        const double heat_nb = i0 * sw_band_frac(n, nb, blue) * inv_rho0_cp * dt * (ea - eb);
+        phi_sum = phi_sum + heat_nb * sw_pe_cost_shape(hk * kn);
+    }
+    return phi_sum;
+}
+
 // the turbulent velocity scale (cube root of the TKE rate, or RH18)
 __device__ __forceinline__ double vstar_of(const vphys_config &c, double tke_here, double conv_perel, double ustar,
                                            double htot, double mld_guess, double dt)
@@ -255,6 +273,12 @@ __global__ void __launch_bounds__(128, 4) k_epbl(const Params p, double dt, doub
         dch_s[k] = dmass * dsv_ds_k;
         if (k > k_sfc || !sw_on) {
             ctke_sw[k] = 0.0;   // dead layers above the live surface take no light
+        } else if (c.sw_chl) {
+            const double d_bot_sw = d_top_sw + hk;
+            ctke_sw[k] = -0.5 * GRAVITY * rho0 * dch_t[k] *
+                         sw_phi_nb(i0_col, p.sw_kappa + col, P, c.sw_nbands, c.sw_blue_frac, inv_rho0_cp, dt,
+                                   d_top_sw, d_bot_sw, hk, k == 1);
+            d_top_sw = d_bot_sw;
         } else {
             const double d_bot_sw = d_top_sw + hk;
             double heat_sw1, heat_sw2;

@@ -140,14 +140,20 @@ __global__ void k_sw_penetration(const Params p, double inv_scale)
             k_dep = k;
             break;
         }
-    const double i0col = c.sw_pen_frac * __ldg(p.sw_src + col) * __ldg(p.wet + col);
+    // the chlorophyll scheme absorbs all of the source (apply_sw_penetration_nb_impl, :1606-1668)
+    const bool nbs = c.sw_chl != 0;
+    const double *kap = p.sw_kappa + col;
+    const double i0col = nbs ? __ldg(p.sw_src + col) * __ldg(p.wet + col)
+                             : c.sw_pen_frac * __ldg(p.sw_src + col) * __ldg(p.wet + col);
     double d_top = 0.0;
-    double trans_top = sw_transmission(c, d_top);
+    double trans_top = nbs ? sw_transmission_nb(d_top, kap, P, c.sw_nbands, c.sw_blue_frac) : sw_transmission(c, d_top);
     for (int k = nz; k >= k_dep; --k) {
         const size_t off = P * (size_t)(k - 1);
         const double hk = __ldg(hp + off);
         const double d_bot = d_top + hk;
-        const double trans_bot = (k > k_dep) ? sw_transmission(c, d_bot) : 0.0;
+        const double trans_bot = (k > k_dep) ? (nbs ? sw_transmission_nb(d_bot, kap, P, c.sw_nbands, c.sw_blue_frac)
+                                                    : sw_transmission(c, d_bot))
+                                             : 0.0;
         if (hk > H_VANISHED) {
             const double absorbed = i0col * (trans_top - trans_bot);
             double add = inv_scale * absorbed;
@@ -158,6 +164,30 @@ __global__ void k_sw_penetration(const Params p, double inv_scale)
         }
         d_top = d_bot;
     }
+}
+
+// The chlorophyll scheme's band opacities (sw_kappa_band_impl,
+// rdb_ocean_sw_chl.F90:176-190, with sw_opacity_manizza,
+// rdb_ocean_surface_flux.F90:784-793): a + b max(chl, 1e-4)^p on wet
+// columns through the safe pow, the land value elsewhere.  One thread per
+// column, every band.
+__global__ void k_sw_chl_kappa(const Params p, const double *__restrict__ chl, double *__restrict__ kappa)
+{
+    const size_t col = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (col >= p.plane) return;
+    const vphys_config &c = p.cfg;
+    const bool wet = __ldg(p.wet + col) > 0.5;
+    const double x = fmx(__ldg(chl + col), 1.0e-4);
+    for (int n = 0; n < c.sw_nbands; ++n)
+        kappa[col + (size_t)n * p.plane] =
+            wet ? c.sw_opacity_coef[2 * n] + c.sw_opacity_coef[2 * n + 1] * sm_pow(x, c.sw_chl_power[n])
+                : c.sw_opacity_land;
+}
+
+void launch_sw_chl_kappa(const Params &p, const double *chl, cudaStream_t stream)
+{
+    const unsigned blocks = (unsigned)((p.plane + 255) / 256);
+    k_sw_chl_kappa<<<blocks, 256, 0, stream>>>(p, chl, (double *)p.sw_kappa);
 }
 
 __global__ void k_stress_mag(const Params p, double *out)
@@ -260,7 +290,7 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
         const double tau_mag = p.stress_mag[col];
         const double u_star = sqrt(xdiv(tau_mag, rho0));
         // pass 1 charges the shortwave that passes the lagged boundary layer
-        q_T_kin = kpp_q_t_kin(c, p.q_heat[col], p.sw_src + col, h_b, HH(k_sfc));
+        q_T_kin = kpp_q_t_kin(c, p.q_heat[col], p.sw_src + col, p.sw_kappa + col, p.plane, h_b, HH(k_sfc));
         q_S_kin = xdiv(p.q_salt[col], rho0);
         double T_sfc = 0.0, S_sfc = 0.0;
         if (c.buoyancy_coeffs) {   // "eos": the surface layer's (T, S) (rdb_ocean_vmix.F90:1357-1376)
@@ -335,7 +365,7 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
         }
         // ---- KPP pass 2 scalars (rdb_ocean_vmix.F90:1429-1491) ----
         if (c.sw_pen_frac != 0.0) {   // pass 2 charges what passes the new boundary layer
-            q_T_kin = kpp_q_t_kin(c, p.q_heat[col], p.sw_src + col, h_b, HH(k_sfc));
+            q_T_kin = kpp_q_t_kin(c, p.q_heat[col], p.sw_src + col, p.sw_kappa + col, p.plane, h_b, HH(k_sfc));
             B_0 = kpp_surface_b0(c, q_T_kin, q_S_kin, HH(k_sfc), T_sfc, S_sfc);
         }
         p.b0[col] = B_0;

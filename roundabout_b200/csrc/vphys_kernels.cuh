@@ -36,6 +36,8 @@ struct Params {
     // the shortwave source the host selected (q_heat, or SW_NET under
     // sw_source = 1) and the dynamic wet mask (NULL unless use_wet_dyn)
     const double *sw_src, *wet_dyn;
+    // the chlorophyll scheme's band opacities, (nx, ny, VPHYS_SW_NB_MAX); NULL unless sw_chl
+    const double *sw_kappa;
     const double *tau_x, *tau_y, *lambda_bot_u, *lambda_bot_v;
     double *visc_rem_u, *visc_rem_v;
     double *gamma_t, *gamma_s;       // nullptr: not written
@@ -76,6 +78,7 @@ void launch_stress_mag(const Params &p, cudaStream_t stream);
 // work (per column, zeroed before the first call) carries each column's cost
 // from one call to the next; with `ordered`, the columns are solved heaviest
 // first through order (per column) bucketed in hist (1024 counts).
+void launch_sw_chl_kappa(const Params &p, const double *chl, cudaStream_t stream);
 void launch_kappa_shear(const Params &p, double dt, int *work, int *order, unsigned *hist, bool ordered,
                         cudaStream_t stream);
 // EPBL column solve into p.kd_epbl / p.mld_epbl (vphys_epbl.cu)

@@ -395,7 +395,7 @@ __global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, doubl
             const double u_star = sqrt(xdiv(p.stress_mag[col], rho0));
             // the heat flux pass 2 charged (shortwave: what passes h_b, or the
             // surface layer hi)
-            const double q_T_kin = kpp_q_t_kin(c, p.q_heat[col], p.sw_src + col, h_b, __ldg(hp + P * (size_t)(hi - 1)));
+            const double q_T_kin = kpp_q_t_kin(c, p.q_heat[col], p.sw_src + col, p.sw_kappa + col, p.plane, h_b, __ldg(hp + P * (size_t)(hi - 1)));
             const double q_S_kin = xdiv(p.q_salt[col], rho0);
             // with "eos" coefficients or shortwave B0 is the assembly's (pass 2
             // stored it before the solve changed the surface T and S); otherwise

@@ -89,7 +89,7 @@ def test_kappa_shear_knobs_are_validated(lib):
     h = ctypes.c_void_p()
     for name, value in (("ks_max_inner_it", 0), ("ks_max_substep_it", -1), ("eos_variant", 2), ("ks_lambda", 0.0),
                         ("kappa_shear", 2), ("ks_massless_merge", 2), ("sw_source", 2), ("bound_salinity", -1),
-                        ("use_wet_dyn", 3), ("epbl_sw_ctke", 2)):
+                        ("use_wet_dyn", 3), ("epbl_sw_ctke", 2), ("sw_chl", 2)):
         bad = default_config()
         setattr(bad, name, value)
         assert lib.vphys_create(4, 4, 4, 2, ctypes.byref(bad), ctypes.byref(h)) == _ffi.ERR_CONFIG, name
@@ -132,3 +132,20 @@ def test_every_named_field_has_a_shape():
     for name, fid in _ffi.FIELD_NAMES.items():
         shp = _ffi.field_shape(fid, 5, 4, 3)
         assert len(shp) in (2, 3) and all(n > 0 for n in shp), name
+
+
+def test_chlorophyll_knobs_are_validated(lib):
+    """The chlorophyll scheme needs sw_pen_frac = 1, 3..6 bands and a positive
+    clear-water opacity per band (rdb_config_validate.F90:291-310)."""
+    from roundabout_b200 import _ffi
+    from roundabout_b200.config import default_config
+
+    h = ctypes.c_void_p()
+    for over in (dict(sw_pen_frac=0.5), dict(sw_pen_frac=1.0, sw_nbands=2), dict(sw_pen_frac=1.0, sw_nbands=7),
+                 dict(sw_pen_frac=1.0, sw_nbands=4)):
+        bad = default_config()
+        bad.sw_chl = 1
+        for k, v in over.items():
+            setattr(bad, k, v)
+        assert lib.vphys_create(4, 4, 4, 2, ctypes.byref(bad), ctypes.byref(h)) == _ffi.ERR_CONFIG, over
+        assert h.value is None

@@ -7,7 +7,7 @@ OM4, RH18 and constant mstar, both velocity scales, mixing-length
 exponents 2 and 3, the LF17 Langmuir enhancement (rescale and additive), the TKE budget
 diagnostics, the MLD iteration with false
 position, bisection, the previous-MLD seed or none, both EOS variants, the
-penetrating-shortwave TKE ledger (from Q_heat or the q_sw source), nz from 1 to 100, vanished top layers and
+penetrating-shortwave TKE ledger (two-band from Q_heat or the q_sw source, or the chlorophyll N-band), nz from 1 to 100, vanished top layers and
 land; the merges (add, max,
 max_shear with kappa-shear) bitwise through the assembly and whole steps,
 with convection masked below EPBL's MLD; the mixed step within 1e-6.
@@ -50,6 +50,7 @@ KNOBS = {
     "langmuir_additive_sw": dict(epbl_use_lt=1, epbl_lt_scheme=2, sw_pen_frac=0.5, epbl_lt_lac2=0.1),
     "shortwave_qsw": dict(sw_pen_frac=0.7, sw_source=1, epbl_tke_diags=1),
     "shortwave_no_ledger": dict(sw_pen_frac=0.7, epbl_sw_ctke=0),
+    "chlorophyll": dict(sw_pen_frac=1.0, sw_chl=1, epbl_tke_diags=1),
     "shortwave_linear": dict(epbl_mstar_scheme=1, sw_pen_frac=1.0, eos_variant=1, eos_alpha_t=0.2, eos_beta_s=0.77,
                              sw_zeta1=1.5, sw_zeta2=9.0),
 }
@@ -67,6 +68,11 @@ def setup(VP, oracle, cols, cfg, prev_mld=None):
     if cfg.sw_source:
         st.sw_net[...] = np.abs(st.q_heat) * 0.8 + 40.0
         vp.set("sw_net", st.sw_net)
+    if cfg.sw_chl:
+        st.sw_chl[...] = np.abs(np.sin(np.arange(cols.nx * cols.ny))).reshape((cols.nx, cols.ny), order="F") * 3.0
+        st.call("vpo_sw_chl_kappa", cfg)
+        vp.set("sw_chl", st.sw_chl)
+        vp.sw_chl_apply()
     if prev_mld is not None:
         st.mld_epbl[...] = prev_mld
         vp.set("mld_epbl", prev_mld)

@@ -264,3 +264,57 @@ def test_bound_salinity_and_wet_dyn(VP, oracle, budgets):
         assert_bitwise(f"tracer{t}", vp.get_tracer(t), st.tracers[t])
     if budgets:
         assert_bitwise("salt_budget_surface", vp.get("salt_budget_surface"), st.salt_budget_surface)
+
+
+CHL = dict(sw_pen_frac=1.0, sw_chl=1)
+
+
+def _with_chl(VP, oracle, cols, cfg):
+    """Oracle and handle with the same chlorophyll; the band opacities from
+    vphys_sw_chl_apply must equal the oracle's bit for bit."""
+    st = oracle_state(oracle, cols, cfg)
+    st.q_heat[...] = np.abs(st.q_heat) + 60.0
+    st.sw_chl[...] = np.abs(np.cos(np.arange(st.nx * st.ny))).reshape((st.nx, st.ny), order="F") * 2.0
+    st.sw_chl[0, 0] = 0.0
+    st.call("vpo_sw_chl_kappa", cfg)
+    vp = loaded(VP, cols, cfg)
+    vp.set("q_heat", st.q_heat)
+    vp.set("sw_chl", st.sw_chl)
+    vp.sw_chl_apply()
+    assert_bitwise("sw_kappa", vp.get("sw_kappa")[:, :, :cfg.sw_nbands], st.sw_kappa[:, :, :cfg.sw_nbands])
+    return st, vp
+
+
+@pytest.mark.parametrize("nbands", [3, 5])
+def test_chl_penetration_standalone(VP, oracle, nbands):
+    """apply_sw_penetration_nb_impl: the whole source moved down the column
+    through the N-band transmission, bitwise."""
+    cols = columns(nx=40, ny=12, nz=20, seed=94, thin_frac=0.2)
+    cols.h[:10, :, -1] = 1.0e-4
+    cfg = hot_cfg(budgets=1, surface_flux=1, sw_nbands=nbands, **CHL)
+    for n in range(3, nbands):
+        cfg.sw_opacity_coef[2 * n], cfg.sw_opacity_coef[2 * n + 1], cfg.sw_chl_power[n] = 0.5 + n, 0.02, 0.4
+    st, vp = _with_chl(VP, oracle, cols, cfg)
+    for _ in range(2):
+        st.call("vpo_surface_flux", cfg, DT)
+        st.call("vpo_sw_penetration", cfg, DT)
+        vp.surface_flux(DT)
+        vp.sw_penetration(DT)
+    for t in range(st.ntr):
+        assert_bitwise(f"tracer{t}", vp.get_tracer(t), st.tracers[t])
+    assert_bitwise("heat_budget_surface", vp.get("heat_budget_surface"), st.heat_budget_surface)
+
+
+@pytest.mark.parametrize("method", [2, 3])
+def test_step_with_chl(VP, oracle, method):
+    """Whole steps under the chlorophyll scheme: penetration, KPP's N-band
+    charge (both passes and the non-local gamma), bitwise."""
+    cols = columns(nx=30, ny=18, nz=16, seed=95, thin_frac=0.1)
+    cfg = hot_cfg(budgets=1, surface_flux=1, kpp_sw_method=method, **CHL)
+    st, vp = _with_chl(VP, oracle, cols, cfg)
+    assert st.call("vpo_step", cfg, DT, 3) == 0
+    vp.step(DT, 3)
+    for t in range(st.ntr):
+        assert_bitwise(f"tracer{t}", vp.get_tracer(t), st.tracers[t])
+    for n in ("kv", "kt", "bl_depth", "b0", "heat_budget", "heat_budget_surface"):
+        assert_bitwise(n, vp.get(n), getattr(st, n))

@@ -91,6 +91,7 @@ EPBL_KNOBS = {
     "langmuir_additive": dict(epbl_use_lt=1, epbl_lt_scheme=2, sw_pen_frac=0.5),
     "shortwave_qsw": dict(sw_pen_frac=0.7, sw_source=1, epbl_tke_diags=1),
     "shortwave_no_ledger": dict(sw_pen_frac=0.7, epbl_sw_ctke=0),
+    "chlorophyll_4band": dict(sw_pen_frac=1.0, sw_chl=1, sw_nbands=4, epbl_tke_diags=1),
 }
 
 
@@ -105,12 +106,16 @@ def test_epbl_source_matches_oracle(oracle, host_libs, shape, knobs):
     _beta_plane(st)
     st.q_heat[...] *= 3.0
     st.sw_net[...] = np.abs(st.q_heat) * 0.8 + 40.0
+    if cfg.sw_chl:
+        cfg.sw_opacity_coef[6], cfg.sw_opacity_coef[7], cfg.sw_chl_power[3] = 0.8, 0.05, 0.5
+        st.sw_chl[...] = np.abs(np.sin(np.arange(nx * ny))).reshape((nx, ny), order="F") * 3.0
+        st.call("vpo_sw_chl_kappa", cfg)
     st.call("vpo_epbl", cfg, 3600.0)
     kd, mld, la = np.zeros_like(st.kd_epbl), np.zeros_like(st.mld_epbl), np.zeros_like(st.la_epbl)
     tke6 = np.zeros(6 * nx * ny)
     host_libs["epbl"].host_epbl(ctypes.byref(cfg), nx, ny, nz, _ptr(st.h), _ptr(st.tracers[cfg.idx_temperature]),
                                 _ptr(st.tracers[cfg.idx_salinity]), _ptr(st.wet), _ptr(st.coriolis),
-                                _ptr(st.stress_mag), _ptr(st.q_heat), _ptr(st.q_salt), _ptr(st.sw_net),
+                                _ptr(st.stress_mag), _ptr(st.q_heat), _ptr(st.q_salt), _ptr(st.sw_net), _ptr(st.sw_kappa),
                                 ctypes.c_double(3600.0),
                                 _ptr(kd), _ptr(mld), _ptr(la), _ptr(tke6))
     assert np.array_equal(kd, st.kd_epbl)

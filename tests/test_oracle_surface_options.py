@@ -190,3 +190,105 @@ def test_epbl_ledger_reads_qsw(oracle):
     c.call("vpo_epbl", c1, DT)
     assert np.array_equal(a.kd_epbl, b.kd_epbl) and np.array_equal(a.mld_epbl, b.mld_epbl)
     assert not np.array_equal(a.kd_epbl, c.kd_epbl)
+
+
+# ---- the chlorophyll N-band scheme (Manizza et al. 2005) -------------------
+CHL = dict(sw_pen_frac=1.0, sw_chl=1)
+
+
+def _chl_state(oracle, cfg, seed=86):
+    st = _state(oracle, cfg, seed=seed)
+    st.sw_chl[...] = np.abs(np.cos(np.arange(st.nx * st.ny))).reshape((st.nx, st.ny), order="F") * 2.0
+    st.sw_chl[0, 0] = 0.0                     # below the 1e-4 floor
+    st.call("vpo_sw_chl_kappa", cfg)
+    return st
+
+
+def test_chl_band_fractions_sum_to_one(oracle):
+    """sw_band_fractions: blue/red split of the visible 0.42, the rest shared
+    evenly; the bands sum to 1 for every band count."""
+    L = oracle.lib()
+    L.vpo_sw_band_frac.restype = __import__("ctypes").c_double
+    L.vpo_sw_band_frac.argtypes = [__import__("ctypes").c_int] * 2 + [__import__("ctypes").c_double]
+    for nb in range(3, 7):
+        fr = [L.vpo_sw_band_frac(n, nb, 0.3) for n in range(1, nb + 1)]
+        assert fr[0] == 0.3 * 0.42 and fr[1] == (1.0 - 0.3) * 0.42
+        assert abs(sum(fr) - 1.0) <= 4e-16
+
+
+def test_chl_kappa_in_closed_form(oracle):
+    """sw_opacity_manizza: kappa_n = a_n + b_n max(chl, 1e-4)^p_n on wet
+    columns (rdb_sm_pow: within 2 ulp of libm's pow), the land value on land."""
+    cfg = hot_cfg(**CHL)
+    st = _chl_state(oracle, cfg)
+    chl = np.maximum(st.sw_chl, 1.0e-4)
+    wet = st.wet > 0.5
+    for n in range(3):
+        a, b, p = cfg.sw_opacity_coef[2 * n], cfg.sw_opacity_coef[2 * n + 1], cfg.sw_chl_power[n]
+        want = a + b * chl ** p
+        got = st.sw_kappa[:, :, n]
+        assert np.allclose(got[wet], want[wet], rtol=4e-16, atol=0.0)
+        assert (got[~wet] == cfg.sw_opacity_land).all()
+    assert (st.sw_kappa[:, :, 3:] == 1.0).all()     # bands past sw_nbands untouched
+
+
+def test_chl_penetration_profile_and_conservation(oracle):
+    """apply_sw_penetration_nb_impl: all of the source leaves the first live
+    layer, each live layer takes I0 (T(d_top) - T(d_bot)) with the N-band T,
+    the deepest the rest; the column's heat content is kept to round-off."""
+    cfg = hot_cfg(surface_flux=1, **CHL)
+    st = _chl_state(oracle, cfg)
+    iT = cfg.idx_temperature
+    st.call("vpo_surface_flux", cfg, DT)
+    before, t0 = _heat_content(st, cfg), st.tracers[iT].copy()
+    st.call("vpo_sw_penetration", cfg, DT)
+    assert np.abs(_heat_content(st, cfg) - before).max() <= 1e-12 * np.abs(before).max()
+    # one wet column with every layer live, against the closed form
+    live = (st.h > 1.5e-4).all(axis=2) & (st.wet > 0.5)
+    i, j = np.argwhere(live)[0]
+    fr = np.array([0.5 * 0.42, 0.5 * 0.42, 0.58])
+    kap = st.sw_kappa[i, j, :3]
+    d = np.concatenate([[0.0], np.cumsum(st.h[i, j, ::-1])])          # interface depths from the surface
+    T = (fr[None, :] * np.exp(-kap[None, :] * d[:, None])).sum(axis=1)
+    T[-1] = 0.0                                                       # opaque bed
+    absorbed = st.q_heat[i, j] * (T[:-1] - T[1:])                     # surface-down
+    absorbed[0] -= st.q_heat[i, j]
+    dT = (st.tracers[iT][i, j, ::-1] - t0[i, j, ::-1]) * st.h[i, j, ::-1]
+    want = absorbed * DT / (cfg.rho0 * cfg.cp)
+    # T_new - T_old cancels: allow a few ulp of T times the layer thickness
+    tol = 1e-12 * np.abs(want) + 8 * np.finfo(float).eps * np.abs(t0[i, j, ::-1]) * st.h[i, j, ::-1]
+    assert (np.abs(dT - want) <= tol).all()
+    assert (want[1:] > 0).any()
+
+
+def test_chl_opaque_bands_leave_kpp_uncharged(oracle):
+    """With every band opaque (kappa 1e6 m-1) nothing passes the boundary
+    layer of a wet column: KPP's charge Q - q_sw T(h_b) is Q exactly, the
+    assembly of the shortwave-free path bit for bit."""
+    c0 = hot_cfg()
+    c1 = hot_cfg(kpp_sw_method=2, **CHL)
+    a, b = _state(oracle, c0, seed=87), _state(oracle, c1, seed=87)
+    b.sw_kappa[...] = 1.0e6
+    for s, c in ((a, c0), (b, c1)):
+        s.call("vpo_eos_wright", c)
+        assert s.call("vpo_build_coefficients", c) == 0
+    for n in ("kv", "kt", "bl_depth"):
+        assert np.array_equal(getattr(a, n), getattr(b, n)), n
+    # on land h_b = 0 and T(0) = 1: the whole source is charged there, as in the two-band form
+    wet = a.wet > 0.5
+    assert np.array_equal(a.b0[wet], b.b0[wet])
+
+
+def test_chl_epbl_ledger_with_grey_bands_is_single_band(oracle):
+    """The EPBL N-band ledger with every band at one opacity kappa equals a
+    two-band ledger of equal e-folding depths 1/kappa, to round-off."""
+    kap = 0.08
+    c_nb = hot_cfg(epbl=1, epbl_tke_diags=1, **CHL)
+    c_2b = hot_cfg(epbl=1, epbl_tke_diags=1, sw_pen_frac=1.0, sw_band_ratio=0.5, sw_zeta1=1.0 / kap,
+                   sw_zeta2=1.0 / kap)
+    a, b = _state(oracle, c_nb, seed=88), _state(oracle, c_2b, seed=88)
+    a.sw_kappa[...] = kap
+    a.call("vpo_epbl", c_nb, DT)
+    b.call("vpo_epbl", c_2b, DT)
+    assert np.allclose(a.mld_epbl, b.mld_epbl, rtol=1e-9, atol=1e-9)
+    assert np.allclose(a.kd_epbl, b.kd_epbl, rtol=1e-8, atol=1e-12)
