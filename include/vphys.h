@@ -306,6 +306,11 @@ typedef struct vphys_config {
     double sw_opacity_coef[2 * VPHYS_SW_NB_MAX]; /* (a_n, b_n) pairs, m-1: 0.0232 0.074, 0.225 0.037, 2.86 0 */
     double sw_chl_power[VPHYS_SW_NB_MAX];        /* p_n: 0.674, 0.629, 0 */
     double sw_opacity_land;   /* 10: kappa on land columns */
+    /* 1: the penetrating shortwave of a column is scaled by 1 - COVER_FRAC,
+     * the ice-shelf cover fraction, so no light reaches the water under a
+     * shelf (apply_sw_penetration_cover_impl / _nb_cover_impl,
+     * rdb_ocean_surface_flux.F90:1532-1604, 1670-1730) */
+    int use_cover_frac;       /* 0 */
 } vphys_config;
 
 #define VPHYS_KPP_SW_ALL 1
@@ -366,6 +371,8 @@ enum vphys_field {
                                    1e-4 floor) */
     VPHYS_FIELD_SW_KAPPA = 44,  /* in/out  (nx, ny, VPHYS_SW_NB_MAX) band opacities, m-1, the first
                                    sw_nbands planes read (sw_chl = 1; filled with 1) */
+    VPHYS_FIELD_COVER_FRAC = 45, /* in     (nx, ny) ice-shelf cover fraction in [0, 1] (use_cover_frac = 1;
+                                   filled with 0) */
     VPHYS_FIELD_TRACER0 = 64    /* in/out  (nx, ny, nz); tracer t is
                                    VPHYS_FIELD_TRACER0 + t */
 };

@@ -28,7 +28,7 @@ class VpoState(ctypes.Structure):
                           "visc_rem_u", "visc_rem_v", "gamma_t", "gamma_s", "heat_budget", "salt_budget")
     ] + [(n, _ip) for n in ("k_top_u", "k_top_v", "k_bot_u", "k_bot_v")] + [("tr", ctypes.POINTER(_dp))] + [
         (n, _dp) for n in ("heat_budget_surface", "salt_budget_surface", "coriolis", "kd_shear", "tke_shear", "kd_epbl",
-                          "mld_epbl", "la_epbl")] + [("epbl_tke", _dp * 6)] + [(n, _dp) for n in ("sw_net", "wet_dyn", "sw_chl", "sw_kappa")]
+                          "mld_epbl", "la_epbl")] + [("epbl_tke", _dp * 6)] + [(n, _dp) for n in ("sw_net", "wet_dyn", "sw_chl", "sw_kappa", "cover_frac")]
 
 
 def build(force: bool = False) -> Path:
@@ -139,6 +139,7 @@ class OracleState:
         self.wet_dyn = np.ones((nx, ny), dtype=np.float64, order="F")
         self.sw_chl = np.full((nx, ny), 1.0e-4, dtype=np.float64, order="F")
         self.sw_kappa = np.ones((nx, ny, 6), dtype=np.float64, order="F")
+        self.cover_frac = f(nx, ny)
         self.k_top_u = np.full((nx + 1, ny), nz, dtype=np.int32, order="F")
         self.k_top_v = np.full((nx, ny + 1), nz, dtype=np.int32, order="F")
         self.k_bot_u = np.ones((nx + 1, ny), dtype=np.int32, order="F")

@@ -1417,8 +1417,10 @@ void vpo_sw_penetration(const vphys_config *c, vpo_state *s, double dt)
             const int kt = first_live(s->h, nx, ny, i, j, nz);
             /* the chlorophyll scheme absorbs all of the source (apply_sw_penetration_nb_impl, 1606-1668) */
             const int nbs = c->sw_chl;
-            const double i0col = nbs ? C2(vpo_sw_source(c, s), i, j) * C2(s->wet, i, j)
-                                     : c->sw_pen_frac * C2(vpo_sw_source(c, s), i, j) * C2(s->wet, i, j);
+            double i0col = nbs ? C2(vpo_sw_source(c, s), i, j) * C2(s->wet, i, j)
+                               : c->sw_pen_frac * C2(vpo_sw_source(c, s), i, j) * C2(s->wet, i, j);
+            /* apply_sw_penetration_cover_impl / _nb_cover_impl (1532-1604, 1670-1730) */
+            if (c->use_cover_frac) i0col = i0col * (1.0 - C2(s->cover_frac, i, j));
             int k_dep = 1;
             for (int k = 1; k <= nz; ++k) {
                 if (C3(s->h, i, j, k) > H_VANISHED) {

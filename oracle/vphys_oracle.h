@@ -52,6 +52,7 @@ typedef struct vpo_state {
     double *wet_dyn;                        /* (nx,ny) dynamic wet mask, read under use_wet_dyn */
     double *sw_chl;                         /* (nx,ny) surface chlorophyll, mg m-3 */
     double *sw_kappa;                       /* (nx,ny,VPHYS_SW_NB_MAX) chlorophyll-scheme band opacities */
+    double *cover_frac;                     /* (nx,ny) ice-shelf cover fraction, read under use_cover_frac */
 } vpo_state;
 
 void vpo_sw_chl_kappa(const vphys_config *c, vpo_state *s);

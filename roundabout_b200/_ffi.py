@@ -75,6 +75,7 @@ FIELD_SW_NET = 41
 FIELD_WET_DYN = 42
 FIELD_SW_CHL = 43
 FIELD_SW_KAPPA = 44
+FIELD_COVER_FRAC = 45
 SW_NB_MAX = 6
 FIELD_TRACER0 = 64
 
@@ -90,7 +91,7 @@ FIELD_NAMES = {
     "heat_budget_surface": FIELD_HEAT_BUDGET_SURFACE, "salt_budget_surface": FIELD_SALT_BUDGET_SURFACE,
     "kd_shear": FIELD_KD_SHEAR, "tke_shear": FIELD_TKE_SHEAR, "kd_epbl": FIELD_KD_EPBL, "mld_epbl": FIELD_MLD_EPBL,
     "la_epbl": FIELD_LA_EPBL, "sw_net": FIELD_SW_NET, "wet_dyn": FIELD_WET_DYN, "sw_chl": FIELD_SW_CHL,
-    "sw_kappa": FIELD_SW_KAPPA,
+    "sw_kappa": FIELD_SW_KAPPA, "cover_frac": FIELD_COVER_FRAC,
     **{f"epbl_tke_{k}": v for k, v in FIELD_EPBL_TKE.items()},
 }
 INT_FIELDS = (FIELD_K_TOP_U, FIELD_K_TOP_V, FIELD_K_BOT_U, FIELD_K_BOT_V)
@@ -109,7 +110,8 @@ def field_shape(field: int, nx: int, ny: int, nz: int):
                  FIELD_KD_EPBL):
         return (nx, ny, nz + 1)
     if field in (FIELD_BL_DEPTH, FIELD_B0, FIELD_STRESS_MAG, FIELD_Q_HEAT, FIELD_Q_SALT, FIELD_WET, FIELD_CORIOLIS,
-                 FIELD_MLD_EPBL, FIELD_LA_EPBL, FIELD_SW_NET, FIELD_WET_DYN, FIELD_SW_CHL) or field in FIELD_EPBL_TKE.values():
+                 FIELD_MLD_EPBL, FIELD_LA_EPBL, FIELD_SW_NET, FIELD_WET_DYN, FIELD_SW_CHL,
+                 FIELD_COVER_FRAC) or field in FIELD_EPBL_TKE.values():
         return (nx, ny)
     if field in (FIELD_TAU_X, FIELD_LAMBDA_BOT_U, FIELD_K_TOP_U, FIELD_K_BOT_U):
         return (nx + 1, ny)
@@ -172,7 +174,7 @@ class VphysConfig(ctypes.Structure):
         ("min_salinity", ctypes.c_double), ("epbl_sw_ctke", ctypes.c_int),
         ("sw_chl", ctypes.c_int), ("sw_nbands", ctypes.c_int), ("sw_blue_frac", ctypes.c_double),
         ("sw_opacity_coef", ctypes.c_double * (2 * SW_NB_MAX)), ("sw_chl_power", ctypes.c_double * SW_NB_MAX),
-        ("sw_opacity_land", ctypes.c_double)]
+        ("sw_opacity_land", ctypes.c_double), ("use_cover_frac", ctypes.c_int)]
 
     def as_dict(self):
         out = {}

@@ -164,6 +164,7 @@ def default_config() -> VphysConfig:
     c.sw_chl_power[0] = 0.674
     c.sw_chl_power[1] = 0.629
     c.sw_opacity_land = 10.0
+    c.use_cover_frac = 0
     return c
 
 

@@ -50,7 +50,7 @@ int cuda_status(cudaError_t e, const char *where)
     return push_error(VPHYS_ERR_CUDA, "%s: CUDA error %d (%s)", where, (int)e, cudaGetErrorString(e));
 }
 
-constexpr int NFIXED = 45;
+constexpr int NFIXED = 46;
 constexpr unsigned MAGIC = 0x56504859u;   // "VPHY"
 
 struct Field {
@@ -143,6 +143,7 @@ size_t field_count(int nx, int ny, int nz, int field, bool *is_int)
     case VPHYS_FIELD_SW_NET:
     case VPHYS_FIELD_WET_DYN:
     case VPHYS_FIELD_SW_CHL:
+    case VPHYS_FIELD_COVER_FRAC:
     case VPHYS_FIELD_MLD_EPBL:
     case VPHYS_FIELD_LA_EPBL:
     case VPHYS_FIELD_EPBL_TKE_WIND:
@@ -242,6 +243,7 @@ int prepare_sources(vphys_handle h)
     if (h->cfg.use_wet_dyn && (st = ensure(h, VPHYS_FIELD_WET_DYN))) return st;
     if (h->cfg.sw_chl && (st = ensure(h, VPHYS_FIELD_SW_CHL))) return st;
     if (h->cfg.sw_chl && (st = ensure(h, VPHYS_FIELD_SW_KAPPA))) return st;
+    if (h->cfg.use_cover_frac && (st = ensure(h, VPHYS_FIELD_COVER_FRAC))) return st;
     return st;
 }
 
@@ -289,6 +291,8 @@ int validate(const vphys_config *c, int ntr)
     if (c->use_wet_dyn < 0 || c->use_wet_dyn > 1) return push_error(VPHYS_ERR_CONFIG, "use_wet_dyn must be 0 or 1");
     if (c->epbl_sw_ctke < 0 || c->epbl_sw_ctke > 1) return push_error(VPHYS_ERR_CONFIG, "epbl_sw_ctke must be 0 or 1");
     if (c->sw_chl < 0 || c->sw_chl > 1) return push_error(VPHYS_ERR_CONFIG, "sw_chl must be 0 or 1");
+    if (c->use_cover_frac < 0 || c->use_cover_frac > 1)
+        return push_error(VPHYS_ERR_CONFIG, "use_cover_frac must be 0 or 1");
     if (c->sw_chl) {
         // rdb_config_validate.F90:291-310, rdb_ocean_sw_chl.F90:87-103
         if (c->sw_pen_frac != 1.0)
@@ -359,6 +363,7 @@ Params make_params(vphys_handle h)
     p.sw_src = h->cfg.sw_source ? D(VPHYS_FIELD_SW_NET) : p.q_heat;
     p.wet_dyn = h->cfg.use_wet_dyn ? D(VPHYS_FIELD_WET_DYN) : nullptr;
     p.sw_kappa = h->cfg.sw_chl ? D(VPHYS_FIELD_SW_KAPPA) : nullptr;
+    p.cover_frac = h->cfg.use_cover_frac ? D(VPHYS_FIELD_COVER_FRAC) : nullptr;
     p.tau_x = D(VPHYS_FIELD_TAU_X);
     p.tau_y = D(VPHYS_FIELD_TAU_Y);
     p.lambda_bot_u = D(VPHYS_FIELD_LAMBDA_BOT_U);
@@ -956,7 +961,7 @@ int vphys_bind(vphys_handle h, int field, void *device_ptr)
         // restore a handle-owned buffer only for core fields / tracers
         if (sl < VPHYS_FIELD_LAMBDA_BOT_U || sl >= NFIXED) return ensure(h, field);
         if (sl == VPHYS_FIELD_SW_NET || sl == VPHYS_FIELD_WET_DYN || sl == VPHYS_FIELD_SW_CHL ||
-            sl == VPHYS_FIELD_SW_KAPPA)
+            sl == VPHYS_FIELD_SW_KAPPA || sl == VPHYS_FIELD_COVER_FRAC)
             return prepare_sources(h);
     }
     return VPHYS_OK;

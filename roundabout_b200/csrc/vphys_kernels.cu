@@ -143,8 +143,9 @@ __global__ void k_sw_penetration(const Params p, double inv_scale)
     // the chlorophyll scheme absorbs all of the source (apply_sw_penetration_nb_impl, :1606-1668)
     const bool nbs = c.sw_chl != 0;
     const double *kap = p.sw_kappa + col;
-    const double i0col = nbs ? __ldg(p.sw_src + col) * __ldg(p.wet + col)
-                             : c.sw_pen_frac * __ldg(p.sw_src + col) * __ldg(p.wet + col);
+    double i0col = nbs ? __ldg(p.sw_src + col) * __ldg(p.wet + col)
+                       : c.sw_pen_frac * __ldg(p.sw_src + col) * __ldg(p.wet + col);
+    if (p.cover_frac) i0col = i0col * (1.0 - __ldg(p.cover_frac + col));   // no light under an ice shelf
     double d_top = 0.0;
     double trans_top = nbs ? sw_transmission_nb(d_top, kap, P, c.sw_nbands, c.sw_blue_frac) : sw_transmission(c, d_top);
     for (int k = nz; k >= k_dep; --k) {

@@ -38,6 +38,7 @@ struct Params {
     const double *sw_src, *wet_dyn;
     // the chlorophyll scheme's band opacities, (nx, ny, VPHYS_SW_NB_MAX); NULL unless sw_chl
     const double *sw_kappa;
+    const double *cover_frac;   // ice-shelf cover fraction; NULL unless use_cover_frac
     const double *tau_x, *tau_y, *lambda_bot_u, *lambda_bot_v;
     double *visc_rem_u, *visc_rem_v;
     double *gamma_t, *gamma_s;       // nullptr: not written

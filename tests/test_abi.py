@@ -89,7 +89,8 @@ def test_kappa_shear_knobs_are_validated(lib):
     h = ctypes.c_void_p()
     for name, value in (("ks_max_inner_it", 0), ("ks_max_substep_it", -1), ("eos_variant", 2), ("ks_lambda", 0.0),
                         ("kappa_shear", 2), ("ks_massless_merge", 2), ("sw_source", 2), ("bound_salinity", -1),
-                        ("use_wet_dyn", 3), ("epbl_sw_ctke", 2), ("sw_chl", 2)):
+                        ("use_wet_dyn", 3), ("epbl_sw_ctke", 2), ("sw_chl", 2),
+                        ("use_cover_frac", 2)):
         bad = default_config()
         setattr(bad, name, value)
         assert lib.vphys_create(4, 4, 4, 2, ctypes.byref(bad), ctypes.byref(h)) == _ffi.ERR_CONFIG, name

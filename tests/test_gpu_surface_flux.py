@@ -318,3 +318,27 @@ def test_step_with_chl(VP, oracle, method):
         assert_bitwise(f"tracer{t}", vp.get_tracer(t), st.tracers[t])
     for n in ("kv", "kt", "bl_depth", "b0", "heat_budget", "heat_budget_surface"):
         assert_bitwise(n, vp.get(n), getattr(st, n))
+
+
+@pytest.mark.parametrize("chl", [0, 1])
+def test_cover_frac_penetration(VP, oracle, chl):
+    """The penetration under a partial ice-shelf cover, two-band and
+    chlorophyll forms, bitwise."""
+    cols = columns(nx=36, ny=10, nz=14, seed=96, thin_frac=0.1)
+    extra = CHL if chl else SW
+    cfg = hot_cfg(budgets=1, surface_flux=1, use_cover_frac=1, **extra)
+    if chl:
+        st, vp = _with_chl(VP, oracle, cols, cfg)
+    else:
+        st = oracle_state(oracle, cols, cfg)
+        vp = loaded(VP, cols, cfg)
+    st.cover_frac[...] = np.abs(np.sin(0.7 * np.arange(st.nx * st.ny))).reshape((st.nx, st.ny), order="F")
+    st.cover_frac[::4, :] = 1.0
+    vp.set("cover_frac", st.cover_frac)
+    st.call("vpo_surface_flux", cfg, DT)
+    st.call("vpo_sw_penetration", cfg, DT)
+    vp.surface_flux(DT)
+    vp.sw_penetration(DT)
+    for t in range(st.ntr):
+        assert_bitwise(f"tracer{t}", vp.get_tracer(t), st.tracers[t])
+    assert_bitwise("heat_budget_surface", vp.get("heat_budget_surface"), st.heat_budget_surface)

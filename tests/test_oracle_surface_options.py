@@ -292,3 +292,24 @@ def test_chl_epbl_ledger_with_grey_bands_is_single_band(oracle):
     b.call("vpo_epbl", c_2b, DT)
     assert np.allclose(a.mld_epbl, b.mld_epbl, rtol=1e-9, atol=1e-9)
     assert np.allclose(a.kd_epbl, b.kd_epbl, rtol=1e-8, atol=1e-12)
+
+
+def test_cover_frac_scales_the_penetration(oracle):
+    """apply_sw_penetration_cover_impl: I0 scaled by 1 - cover_frac.  No cover
+    is the uncovered path bit for bit; a fully covered column takes no light
+    (the deposit alone), in both the two-band and the chlorophyll forms."""
+    for extra in (SW, CHL):
+        c0 = hot_cfg(surface_flux=1, **extra)
+        c1 = hot_cfg(surface_flux=1, use_cover_frac=1, **extra)
+        a, b, d = (_state(oracle, c, seed=89) for c in (c0, c1, c1))
+        d.cover_frac[...] = np.where(np.arange(d.nx)[:, None] % 2 == 0, 1.0, 0.0)
+        for s, c in ((a, c0), (b, c1), (d, c1)):
+            s.call("vpo_surface_flux", c, DT)
+        dep = d.tracers[c1.idx_temperature].copy()
+        for s, c in ((a, c0), (b, c1), (d, c1)):
+            s.call("vpo_sw_penetration", c, DT)
+        iT = c1.idx_temperature
+        assert np.array_equal(a.tracers[iT], b.tracers[iT])
+        covered = np.arange(d.nx) % 2 == 0
+        assert np.array_equal(d.tracers[iT][covered], dep[covered])
+        assert np.array_equal(d.tracers[iT][~covered], a.tracers[iT][~covered])
