@@ -24,9 +24,18 @@ One JSON line from rank 0:
                uploads the state (h, u, v, tracers, forcing) from pinned host
                memory with vphys_set_field and downloads the results (u, v,
                tracers, kv, kt, ks, bl_depth) with vphys_get_field
-  roofline     dominant kernel: algorithmic bytes / its CUDA-event time vs the
-               measured HBM copy bandwidth (MEASURED_PEAKS.json)
+  roofline     dominant stage: algorithmic bytes / its CUDA-event time vs the
+               measured HBM copy bandwidth (MEASURED_PEAKS.json), every
+               stage's fraction, and the whole path's
   cpu_baseline the CPU restatement (oracle) on the host cores, bounded sample
+  gpu_launches the library's kernel launches in the timed region: the
+               launches of one untimed step, counted from the CUDA activity
+               trace, times the steps
+  forms        plain FP64 and mixed on this configuration; the learned-KPP
+               form (trained here) with its KPP stage time against the plain
+               KPP stage; the batched configuration (10 tracers, 15 % of the
+               wet columns with 1 mm layers, 24 graph-captured steps)
+  parity_slice the GPU step against the oracle on the CPU arm's slice
 
 Multi-GPU (torchrun): every rank owns an independent full-size domain
 (columns shard with no data-path exchange); value = all ranks' cells / the
@@ -69,8 +78,14 @@ def parse():
     ap.add_argument("--mixed-level", type=int, default=2, choices=[1, 2],
                     help="1: FP64 assembly, FP32 sweeps; 2: FP32 assembly too (the default)")
     ap.add_argument("--no-compare", action="store_true", help="skip the plain-FP64 timing and error check")
-    ap.add_argument("--learned-cols", type=int, default=1_048_576,
+    ap.add_argument("--learned-cols", type=int, default=4_000_000,
                     help="training columns of the learned-KPP surrogate timed beside the mixed form (0: skip)")
+    ap.add_argument("--learned-rounds", type=int, default=2,
+                    help="2: a second data round from the network's own trajectories, labelled by the plain KPP")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched configuration (10 tracers, 15%% thin-layer columns, 24-step graph)")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the GPU-vs-oracle comparison on the CPU arm's slice")
     return ap.parse_args()
 
 
@@ -222,7 +237,7 @@ def cpu_run(cfg_name: str, sample: str, steps: int, warmup: int, threads: int = 
     cells = cols.nx * cols.ny * cols.nz
     return {"value": cells * steps / el, "unit": "cells/s", "cores": threads, "kind": "port",
             "sample": f"{cols.nx}x{cols.ny}x{cols.nz} slice of the same generator, {ntr} tracers, {steps} steps "
-                      f"(C restatement of the reference, -O2 -ffp-contract=off, OpenMP)",
+                      f"(C restatement of the reference, gcc {o.CFLAGS_DESC}, OpenMP)",
             "ms_per_step": el / steps * 1e3}
 
 
@@ -344,35 +359,15 @@ def main():
 
     # ---- learned KPP + mixed solves: trained here on the plain KPP's columns ----
     if mixed and not args.no_compare and args.learned_cols > 0:
-        from roundabout_b200 import learned as L
+        forms["learned_kpp_mixed"] = learned_form(args, cols, ntr, nx, ny, nz, timed, cells, world)
 
-        sur, _ = L.train_surrogate(args.learned_cols, nz=nz, seed=100, epochs=4)
-        cfg_l = hot_path_config(ntracers=ntr)
-        cfg_l.mixed_precision = args.mixed_level
-        cfg_l.learned_kpp = 1
-        vl = VerticalPhysics(nx, ny, nz, ntr, cfg_l)
-        vl.load_columns(cols)
-        sur.attach(vl)
-        vpp = VerticalPhysics(nx, ny, nz, ntr, hot_path_config(ntracers=ntr))
-        vpp.load_columns(cols)
-        vl.step(dt, 1)
-        vpp.step(dt, 1)
-        torch.cuda.synchronize()
-        bl, blp = np.asarray(vl.get("bl_depth")), np.asarray(vpp.get("bl_depth"))
-        wetm = np.asarray(cols.wet) > 0
-        r = ((bl - blp) / np.maximum(blp, 1.0))[wetm]
-        vpp.close()
-        ms_l = timed(vl, args.steps, args.warmup)
-        forms["learned_kpp_mixed"] = {
-            "cells_per_s": cells * args.steps * world / (ms_l / 1e3), "ms_per_step": ms_l / args.steps,
-            "obl_rms_rel_vs_plain_1step": float(np.sqrt(np.mean(r * r))),
-            "train_columns": int(sur.ntrain), "collect_s": round(sur.collect_seconds, 2),
-            "train_s": round(sur.train_seconds, 2), "kpp": L.kpp_stats(vl)}
-        vl.close()
-        del sur
-
+    # ---- the timed region: K steps of the selected form; the clocks are
+    #      sampled from a second before it to half a second after it, with
+    #      untimed steps of the same form keeping the GPU loaded ----
     with ClockSampler(local) as clk:
+        keep_busy(vp, dt, 1.0)
         ms = timed(vp, args.steps, args.warmup)
+        keep_busy(vp, dt, 0.5)
     value = weak_scaling_value(cells, args.steps, world, ms)
     if mixed:
         forms["mixed"] = {"cells_per_s": value, "ms_per_step": ms / args.steps,
@@ -381,14 +376,19 @@ def main():
         if "plain_fp64" in forms:
             forms["mixed_over_plain"] = round(value / forms["plain_fp64"]["cells_per_s"], 3)
 
-    # ---- per-kernel device times (same stream, CUDA events) ----
+    # ---- kernel launches per step, counted by the CUDA activity trace ----
+    per_step, launch_names = count_launches(lambda: vp.step(dt, 1))
+
+    # ---- per-stage device times (same stream, CUDA events) of the launches
+    #      the step runs: the EOS, the assembly, the momentum solve (column
+    #      depths + face solve) and the fused tracer diffusion + non-local ----
     reps = 5
     stage_ms = {}
     stages = {
         "eos": lambda: vp.eos(),
         "assemble": lambda: vp.assemble(),
         "momentum": lambda: vp.vdiff_momentum(dt),
-        "tracers": lambda: vp.lib.vphys_step and _tracers_fused(vp, dt),
+        "tracers": lambda: vp.vdiff_tracers_nonlocal(dt),
     }
     for name, fn in stages.items():
         fn()
@@ -405,7 +405,7 @@ def main():
                  "assemble": "k_assemble<float>" if (mixed and args.mixed_level >= 2) else "k_assemble<double>",
                  # the stage's launches: the column-depth pass and the face solve
                  "momentum": "k_column_depth+k_momentum_mp" if mixed else "k_column_depth+k_momentum",
-                 "tracers": "k_spans+k_tracers_mp" if mixed else "k_tracers"}
+                 "tracers": "k_spans+k_tracers_mp+k_tracers_redo" if mixed else "k_tracers"}
     dom = max(("assemble", "momentum", "tracers", "eos"), key=lambda k: stage_ms[k])
     peak, peak_kind = peaks()
     achieved = bpc[dom] * cells / (stage_ms[dom] / 1e3) / 1e9
@@ -416,8 +416,10 @@ def main():
                 else "fallback 6.65 TB/s",
                 "algorithmic_bytes_per_cell": round(bpc[dom], 2),
                 "stage_ms": {k: round(v, 4) for k, v in stage_ms.items()},
+                "stage_frac": {k: round(bpc[k] * cells / (v / 1e3) / 1e9 / peak, 4) for k, v in stage_ms.items()},
                 "path_bytes_per_cell": round(bpc["path"], 2),
-                "path_achieved_gbs": round(bpc["path"] * cells / (ms / args.steps / 1e3) / 1e9, 1)}
+                "path_achieved_gbs": round(bpc["path"] * cells / (ms / args.steps / 1e3) / 1e9, 1),
+                "path_frac": round(bpc["path"] * cells / (ms / args.steps / 1e3) / 1e9 / peak, 4)}
 
     # ---- end to end through the C ABI with host buffers ----
     # Every step uploads its inputs from pinned host memory and downloads its
@@ -507,17 +509,30 @@ def main():
         one = cpu_run(args.config, args.cpu_sample, 1, 1, threads=1)
         cpu["single_thread"] = {"value": one["value"], "unit": "cells/s", "cores": 1}
         cpu["host"] = host_cpu()
+    vp.close()
+
+    # ---- the batched configuration (10 tracers, 15 % of the wet columns with
+    #      1 mm layers): 24 graph-captured steps of each form ----
+    if mixed and not args.no_compare and not args.no_batched:
+        forms["batched"] = batched_form(args, dt)
+
+    # ---- the GPU step against the oracle on the CPU arm's slice ----
+    parity = None
+    if rank == 0 and not args.no_parity:
+        parity = parity_slice(args, dt)
 
     clocks = clk.summary()
     line = {"metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if mixed else "f64", "data": "synthetic",
             "config": config_out, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": (6 if mixed else 4) * args.steps, "clocks": clocks, "forms": forms,
+            "gpu_launches": per_step * args.steps if per_step else None,
+            "gpu_launches_per_step": {"count": per_step, "kernels": launch_names,
+                                      "how": "CUDA activity trace (torch.profiler / CUPTI) of one untimed step"},
+            "clocks": clocks, "forms": forms, "parity_slice": parity,
             "mode": (f"FP64 state, FP32 assembly and Thomas sweeps with FP64 residual correction "
                      f"(mixed_precision={args.mixed_level})" if mixed
                      else "plain FP64, bit-identical to the CPU restatement")}
-    vp.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -525,12 +540,236 @@ def main():
         print(json.dumps(line), flush=True)
 
 
-def _tracers_fused(vp, dt):
-    """The step's tracer launch: diffusion of every tracer with the fused
-    non-local tendency (vphys_vdiff_tracers + vphys_nonlocal in one kernel is
-    what vphys_step runs; timed here through the diffusion entry point)."""
-    vp.vdiff_tracers(dt)
-    return True
+def keep_busy(vp, dt, seconds):
+    """Untimed steps for about `seconds` (keeps the GPU under load while the
+    clock sampler runs around the timed region)."""
+    import torch
+
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        vp.step(dt, 1)
+        torch.cuda.synchronize()
+
+
+def count_launches(fn):
+    """Kernel launches of `fn` (one untimed step), from the CUDA activity
+    trace: (count, {kernel name: launches}).  (None, reason) if the trace is
+    unavailable."""
+    import torch
+
+    try:
+        from torch.profiler import ProfilerActivity, profile
+
+        torch.cuda.synchronize()
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            fn()
+            torch.cuda.synchronize()
+        names = {}
+        for e in prof.events():
+            if e.device_type != torch.autograd.DeviceType.CUDA:
+                continue
+            n = e.name
+            if "vphys::" in n or n.startswith("k_") or "::k_" in n:
+                short = n.split("(")[0].replace("void ", "").replace("vphys::", "")
+                names[short] = names.get(short, 0) + 1
+        return sum(names.values()), names
+    except Exception as exc:  # noqa: BLE001 -- the count is a report, not the measurement
+        return None, f"unavailable: {type(exc).__name__}: {exc}"[:200]
+
+
+def learned_form(args, cols, ntr, nx, ny, nz, timed, cells, world):
+    """The learned-KPP form: the surrogate trained here on the plain KPP's
+    columns (training size and rounds as the arguments say), its one-step
+    OBL-depth error against the plain method over the wet columns, the step
+    time with the mixed solves, and the KPP stage's device time, plain
+    (bulk-Richardson search inside the assembly) vs learned (features, the
+    three tensor-core GEMMs, gate/check and the pass-1-free assembly), each
+    net of the assembly without KPP."""
+    import torch
+
+    from roundabout_b200 import learned as L
+    from roundabout_b200.column import VerticalPhysics
+    from roundabout_b200.config import hot_path_config
+
+    dt = 3600.0
+    sur, _ = L.train_surrogate(args.learned_cols, nz=nz, seed=100, epochs=4, rounds=args.learned_rounds)
+
+    def handle(learned_kpp, use_kpp=1, level=args.mixed_level):
+        cfg = hot_path_config(ntracers=ntr)
+        cfg.mixed_precision = level
+        cfg.learned_kpp = learned_kpp
+        cfg.use_kpp = use_kpp
+        vp = VerticalPhysics(nx, ny, nz, ntr, cfg)
+        vp.load_columns(cols)
+        if learned_kpp:
+            sur.attach(vp)
+        return vp
+
+    vl, vpp = handle(1), handle(0, level=0)
+    vl.step(dt, 1)
+    vpp.step(dt, 1)
+    torch.cuda.synchronize()
+    bl, blp = np.asarray(vl.get("bl_depth")), np.asarray(vpp.get("bl_depth"))
+    wetm = np.asarray(cols.wet) > 0
+    r = ((bl - blp) / np.maximum(blp, 1.0))[wetm]
+    vpp.close()
+    ms_l = timed(vl, args.steps, args.warmup)
+    out = {"cells_per_s": cells * args.steps * world / (ms_l / 1e3), "ms_per_step": ms_l / args.steps,
+           "obl_rms_rel_vs_plain_1step": float(np.sqrt(np.mean(r * r))),
+           "train_columns": int(sur.ntrain), "train_rounds": args.learned_rounds,
+           "collect_s": round(sur.collect_seconds, 2), "train_s": round(sur.train_seconds, 2),
+           "kpp": L.kpp_stats(vl)}
+    vl.close()
+
+    def time_assemble(vp, reps=10):
+        vp.eos()
+        for _ in range(3):
+            vp.assemble()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            vp.assemble()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    t = {}
+    for name, lk, uk in (("no_kpp", 0, 0), ("plain", 0, 1), ("learned", 1, 1)):
+        vp = handle(lk, uk)
+        t[name] = time_assemble(vp)
+        vp.close()
+    plain_stage = t["plain"] - t["no_kpp"]
+    learned_stage = t["learned"] - t["no_kpp"]
+    out["kpp_stage_ms"] = {"plain": round(plain_stage, 4), "learned": round(learned_stage, 4),
+                           "plain_over_learned": round(plain_stage / max(learned_stage, 1e-9), 3),
+                           "assemble_without_kpp": round(t["no_kpp"], 4),
+                           "how": "assembly with the KPP stage minus the assembly without it (CUDA events, 10 reps)"}
+    del sur
+    return out
+
+
+def batched_form(args, dt):
+    """The batched configuration: 1440x1080x75, T, S + 8 uniform passives,
+    15 % of the wet columns with 1-10 live 1 mm layers.  Each form runs 24
+    graph-captured steps (vphys_step_graph) from the same state; the first
+    24 give the mixed form's error against the plain FP64 path (which is the
+    oracle's arithmetic bit for bit) and, as its yardstick, the plain path's
+    own response to a +-1e-7 perturbation of its initial tracers; the second
+    24 (the graph replayed) are timed."""
+    import torch
+
+    from roundabout_b200.column import VerticalPhysics
+    from roundabout_b200.config import hot_path_config
+    from roundabout_b200.synthetic import CONFIGS, make_columns
+
+    spec = dict(CONFIGS["batched_1440x1080x75"])
+    ntr = spec.pop("ntracers")
+    cols = make_columns(ntracers=ntr, seed=4321, **spec)
+    nx, ny, nz = cols.nx, cols.ny, cols.nz
+    nsteps = 24
+    out = {"config": "batched_1440x1080x75", "tracers": ntr, "thin_frac": spec["thin_frac"],
+           "steps_per_graph": nsteps}
+    finals, times = {}, {}
+    for name, level in (("plain_fp64", 0), ("mixed", args.mixed_level)):
+        cfg = hot_path_config(ntracers=ntr)
+        cfg.mixed_precision = level
+        vp = VerticalPhysics(nx, ny, nz, ntr, cfg)
+        vp.load_columns(cols)
+        vp.step_graph(dt, nsteps)                 # capture + the first 24 steps
+        torch.cuda.synchronize()
+        finals[name] = [np.asarray(vp.get_tracer(t)) for t in range(ntr)]
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        vp.step_graph(dt, nsteps)                 # replay: timed
+        b.record()
+        torch.cuda.synchronize()
+        times[name] = a.elapsed_time(b) / nsteps
+        out[name] = {"ms_per_step": round(times[name], 4), "cells_per_s": nx * ny * nz / (times[name] / 1e3)}
+        if name == "mixed":
+            out[name]["fp64_resolved_groups_last_step"] = vp.mixed_redo_count()
+        vp.close()
+    # the plain path's own sensitivity: +-1e-7 on the initial tracers of live cells
+    rng = np.random.default_rng(0)
+    live = cols.h > 1.5e-4
+    cfg = hot_path_config(ntracers=ntr)
+    vp = VerticalPhysics(nx, ny, nz, ntr, cfg)
+    vp.load_columns(cols)
+    for t in range(ntr):
+        vp.set_tracer(t, cols.tracers[t] + rng.uniform(-1e-7, 1e-7, cols.h.shape) * live)
+    vp.step_graph(dt, nsteps)
+    torch.cuda.synchronize()
+    pert = [np.asarray(vp.get_tracer(t)) for t in range(ntr)]
+    vp.close()
+    iT, iS = 1, 0
+    err = [float(np.abs(finals["mixed"][t] - finals["plain_fp64"][t]).max()) for t in range(ntr)]
+    env = [float(np.abs(pert[t] - finals["plain_fp64"][t]).max()) for t in range(ntr)]
+    out["mixed_over_plain"] = round(times["plain_fp64"] / times["mixed"], 3)
+    out["max_abs_err_vs_fp64_24steps"] = {"T": err[iT], "S": err[iS],
+                                          "passive": max(e for t, e in enumerate(err) if t not in (iT, iS))}
+    out["fp64_response_to_1e-7_perturbation_24steps"] = {
+        "T": env[iT], "S": env[iS], "passive": max(e for t, e in enumerate(env) if t not in (iT, iS))}
+    return out
+
+
+def parity_slice(args, dt):
+    """The GPU step against the oracle on the CPU arm's 360x270x75 slice of
+    the benchmark's generator: plain FP64 after 3 steps (the max relative
+    difference over every output field, relative to the field's largest
+    magnitude; 0 means bit for bit) and the mixed form after one step (max
+    absolute tracer and velocity difference)."""
+    from oracle import oracle as o
+    from roundabout_b200.column import VerticalPhysics
+    from roundabout_b200.config import hot_path_config
+    from roundabout_b200.synthetic import CONFIGS, make_columns
+
+    o.build()
+    spec = dict(CONFIGS[args.config])
+    sx, sy = (int(x) for x in args.cpu_sample.lower().split("x"))
+    spec["nx"], spec["ny"] = min(sx, spec["nx"]), min(sy, spec["ny"])
+    ntr = spec.pop("ntracers")
+    cols = make_columns(ntracers=ntr, seed=1234, **spec)
+
+    def oracle_after(nsteps):
+        cfg = hot_path_config(ntracers=ntr)
+        st = o.OracleState(cols.nx, cols.ny, cols.nz, ntr)
+        st.seed_backgrounds(cfg)
+        for n in ("h", "u", "v", "tau_x", "tau_y", "q_heat", "q_salt", "wet"):
+            getattr(st, n)[...] = getattr(cols, n)
+        for t in range(ntr):
+            st.tracers[t][...] = cols.tracers[t]
+        st.stress_mag_from_tau()
+        st.call("vpo_step", cfg, dt, nsteps)
+        return st
+
+    def gpu_after(nsteps, level):
+        cfg = hot_path_config(ntracers=ntr)
+        cfg.mixed_precision = level
+        vp = VerticalPhysics(cols.nx, cols.ny, cols.nz, ntr, cfg)
+        vp.load_columns(cols)
+        vp.step(dt, nsteps)
+        return vp
+
+    o.set_threads(os.cpu_count() or 1)
+    st3 = oracle_after(3)
+    vp = gpu_after(3, 0)
+    rel = 0.0
+    for n in ("kv", "kt", "ks", "u", "v", "bl_depth", "rho"):
+        want = getattr(st3, n)
+        rel = max(rel, float(np.abs(np.asarray(vp.get(n)) - want).max()) / max(float(np.abs(want).max()), 1e-300))
+    for t in range(ntr):
+        want = st3.tracers[t]
+        rel = max(rel, float(np.abs(np.asarray(vp.get_tracer(t)) - want).max()) / float(np.abs(want).max() or 1.0))
+    vp.close()
+    st1 = oracle_after(1)
+    vm = gpu_after(1, args.mixed_level)
+    dtr = max(float(np.abs(np.asarray(vm.get_tracer(t)) - st1.tracers[t]).max()) for t in range(ntr))
+    duv = max(float(np.abs(np.asarray(vm.get(n)) - getattr(st1, n)).max()) for n in ("u", "v"))
+    vm.close()
+    return {"slice": f"{cols.nx}x{cols.ny}x{cols.nz}, {ntr} tracers, seed 1234 (the CPU arm's sample)",
+            "plain_fp64_3steps_max_rel_diff": rel,
+            "mixed_1step_max_abs_diff": {"tracers": dtr, "u_v": duv},
+            "bar": "plain <= 1e-12 relative (0: bit for bit); mixed <= 1e-6"}
 
 
 if __name__ == "__main__":

@@ -541,6 +541,14 @@ int vphys_vdiff_tracers(vphys_handle h, double dt);
  * vmix_apply_nonlocal_tendencies (rdb_ocean_vmix.F90:1605-1714). */
 int vphys_nonlocal(vphys_handle h, double dt);
 
+/* The tracer diffusion followed by the KPP non-local tendencies, as one fused
+ * launch: the launch vphys_step runs for this stage.  Replaces the pair of
+ * calls vdiff_apply_tracers then vmix_apply_nonlocal_tendencies that
+ * vmix_apply_in_stage makes back to back (rdb_ocean_dyn.F90:1856-1860;
+ * rdb_ocean_vdiff.F90:1107-1414, rdb_ocean_vmix.F90:1605-1714); the result
+ * equals vphys_vdiff_tracers then vphys_nonlocal.  Asynchronous. */
+int vphys_vdiff_tracers_nonlocal(vphys_handle h, double dt);
+
 /* n_steps of the whole chain (the body of vmix_apply_in_stage on a thermo
  * step, rdb_ocean_dyn.F90:1636-1900): [EOS] -> assemble -> momentum ->
  * tracers -> non-local, with the tracer solve and the non-local tendency
@@ -576,10 +584,9 @@ const char *vphys_version(void);
 int vphys_selftest_division(long long n_pairs, unsigned long long seed, int emin, int erange,
                             unsigned long long *mismatches);
 
-/* Allocation-free 1-2-1 smoothing.  No counterpart in the reference: it is
- * the masked 1-2-1 horizontal smoothing of the assembly gate
- * (vmix_smooth_121_impl, rdb_ocean_vmix.F90:2699-2748, which the reference
- * runs through its own smooth_scratch) offered to callers that cannot call
+/* Allocation-free 1-2-1 smoothing.  No counterpart in the reference.  It is
+ * the same wet-masked 1-2-1 horizontal smoothing that vphys_assemble applies
+ * when kd_smooth_iterations > 0, offered to callers that cannot call
  * cudaMalloc -- a host that owns all device memory through its own pool
  * (an OpenACC/Fortran model, a framework caching allocator) or code running
  * where allocating is not allowed.  `fld` is a device (nx, ny, nz+1)

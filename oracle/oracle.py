@@ -17,6 +17,17 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "_build" / "libvphys_oracle.so"
 
+def _cflags() -> str:
+    """The optimisation and floating-point flags the Makefile compiles with."""
+    for line in (HERE / "Makefile").read_text().splitlines():
+        if line.startswith("CFLAGS"):
+            flags = line.split("=", 1)[1].split()
+            return " ".join(f for f in flags if f.startswith(("-O", "-ffp", "-fno-fast", "-march")))
+    return "unknown"
+
+
+CFLAGS_DESC = _cflags()
+
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
 

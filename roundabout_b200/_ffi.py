@@ -252,6 +252,7 @@ _PROTOTYPES = {
     "vphys_vdiff_momentum": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "vphys_vdiff_tracers": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "vphys_nonlocal": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    "vphys_vdiff_tracers_nonlocal": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "vphys_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]),
     "vphys_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
     "vphys_last_error": (ctypes.c_int, [ctypes.c_int, ctypes.c_char_p, ctypes.c_int]),

@@ -19,10 +19,12 @@ from pathlib import Path
 CSRC = Path(__file__).resolve().parent / "csrc"
 OUT = CSRC / "_build"
 LIB = OUT / "libvphys.so"
-SOURCES = ["vphys_api.cu", "vphys_kernels.cu", "vphys_tracers.cu", "vphys_static.cu", "vphys_mixed.cu",
+SOURCES = ["vphys_api.cu", "vphys_kernels.cu", "vphys_momentum_tma.cu", "vphys_tracers.cu", "vphys_static.cu",
+           "vphys_mixed.cu",
            "vphys_gemm.cu", "vphys_learned.cu", "vphys_kshear.cu",
            "vphys_epbl.cu"]
-HEADERS = ["vphys_device.cuh", "vphys_faces.cuh", "vphys_kernels.cuh", "../../include/vphys.h"]
+HEADERS = ["vphys_device.cuh", "vphys_faces.cuh", "vphys_kernels.cuh", "vphys_tma.cuh", "vphys_tiles.cuh", "vphys_mom_ring.cuh",
+           "../../include/vphys.h"]
 # the mixed-precision solves carry no bitwise contract: FMA contraction allowed
 CONTRACT_OK = {"vphys_mixed.cu", "vphys_gemm.cu", "vphys_learned.cu"}
 

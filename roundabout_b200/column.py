@@ -186,6 +186,10 @@ class VerticalPhysics:
     def nonlocal_tendencies(self, dt):
         _ffi.check(self.lib.vphys_nonlocal(self._h, float(dt)), "vphys_nonlocal")
 
+    def vdiff_tracers_nonlocal(self, dt):
+        """The fused tracer diffusion + non-local launch that step() runs."""
+        _ffi.check(self.lib.vphys_vdiff_tracers_nonlocal(self._h, float(dt)), "vphys_vdiff_tracers_nonlocal")
+
     def step(self, dt, n_steps=1):
         _ffi.check(self.lib.vphys_step(self._h, float(dt), int(n_steps)), "vphys_step")
 

@@ -77,6 +77,8 @@ struct vphys_handle_s {
     int *span = nullptr;              // live spans of the columns (mixed-precision tracer solve)
     unsigned *mp_redo = nullptr;      // the mixed tracer solve's FP64 re-solve list (count + entries)
     double *zcol = nullptr;           // column depths for the momentum face thickness
+    unsigned char *mom_tiles = nullptr;   // skip flags of the TMA-staged momentum solve's face tiles
+    unsigned *dev_err = nullptr;      // bounded waits of the TMA-staged solves that ran out (0: none)
     // learned KPP surrogate (vphys_kpp_attach): the caller's weights and the scratch of one inference
     vphys_kpp_model kpp{};
     bool kpp_attached = false;
@@ -247,6 +249,14 @@ int prepare_sources(vphys_handle h)
     return st;
 }
 
+// What the handle stores after validation: the chlorophyll scheme absorbs the
+// whole shortwave, so an unset penetrating fraction (0) becomes 1
+// (set_sw_chl, rdb_ocean_sw_chl.F90:87-103).
+static void normalize_config(vphys_config &c)
+{
+    if (c.sw_chl && c.sw_pen_frac == 0.0) c.sw_pen_frac = 1.0;
+}
+
 int validate(const vphys_config *c, int ntr)
 {
     if (!c->use_closure)
@@ -295,8 +305,11 @@ int validate(const vphys_config *c, int ntr)
         return push_error(VPHYS_ERR_CONFIG, "use_cover_frac must be 0 or 1");
     if (c->sw_chl) {
         // rdb_config_validate.F90:291-310, rdb_ocean_sw_chl.F90:87-103
-        if (c->sw_pen_frac != 1.0)
-            return push_error(VPHYS_ERR_CONFIG, "sw_chl band-absorbs the whole shortwave: sw_pen_frac must be 1");
+        // 0 means "unset" there and is raised to 1 when the handle stores the
+        // configuration (normalize_config); any other value is refused
+        if (c->sw_pen_frac != 1.0 && c->sw_pen_frac != 0.0)
+            return push_error(VPHYS_ERR_CONFIG, "sw_chl band-absorbs the whole shortwave: sw_pen_frac must be 1 (or 0, "
+                                                "which selects 1)");
         if (c->sw_nbands < 3 || c->sw_nbands > VPHYS_SW_NB_MAX)
             return push_error(VPHYS_ERR_CONFIG, "sw_nbands must be in [3, %d]", VPHYS_SW_NB_MAX);
         for (int n = 0; n < c->sw_nbands; ++n)
@@ -386,6 +399,8 @@ Params make_params(vphys_handle h)
     p.span = h->span;
     p.mp_redo = h->mp_redo;
     p.zcol = h->zcol;
+    p.mom_tile_skip = h->mom_tiles;
+    p.dev_err = h->dev_err;
     p.coriolis = D(VPHYS_FIELD_CORIOLIS);
     p.kd_shear = D(VPHYS_FIELD_KD_SHEAR);
     p.tke_shear = D(VPHYS_FIELD_TKE_SHEAR);
@@ -408,6 +423,17 @@ int prepare_momentum(vphys_handle h)
             h->zcol = nullptr;
             cudaGetLastError();
             return push_error(VPHYS_ERR_ALLOC, "cudaMalloc of the column depths failed");
+        }
+    }
+    if (h->cfg.hvel_mom6 && !h->cfg.hvel_harmonic && !h->mom_tiles) {
+        Params q{};
+        q.nx = h->nx;
+        q.ny = h->ny;
+        cudaError_t e = cudaMalloc(&h->mom_tiles, (size_t)vphys::momentum_tma_tiles(q));
+        if (e != cudaSuccess) {
+            h->mom_tiles = nullptr;
+            cudaGetLastError();
+            return push_error(VPHYS_ERR_ALLOC, "cudaMalloc of the momentum tile flags failed");
         }
     }
     if (h->cfg.remnant) {
@@ -666,6 +692,20 @@ int run_assemble(vphys_handle h, const Params &p)
     return cuda_status(cudaGetLastError(), "vphys_assemble launch");
 }
 
+// A bounded wait of a TMA-staged solve that ran out leaves a nonzero code in
+// h->dev_err (its results are then not to be trusted); read after a
+// synchronisation, reported once and cleared.
+int check_dev_err(vphys_handle h)
+{
+    unsigned code = 0;
+    cudaError_t e = cudaMemcpy(&code, h->dev_err, sizeof code, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_status(e, "device error word");
+    if (code == 0) return VPHYS_OK;
+    cudaMemset(h->dev_err, 0, sizeof code);
+    return push_error(VPHYS_ERR_CUDA, "a bounded wait of a TMA-staged solve ran out (code %u); the last step's "
+                                      "results are incomplete", code);
+}
+
 int read_guard(vphys_handle h, int *status)
 {
     unsigned long long bad = 0;
@@ -843,6 +883,7 @@ int vphys_create(int nx, int ny, int nz, int ntracer, const vphys_config *cfg, v
         vphys_config_default(&c);
     int st = validate(&c, ntracer);
     if (st) return st;
+    normalize_config(c);
     vphys_handle h = new vphys_handle_s();
     h->nx = nx;
     h->ny = ny;
@@ -859,6 +900,14 @@ int vphys_create(int nx, int ny, int nz, int ntracer, const vphys_config *cfg, v
         return push_error(VPHYS_ERR_ALLOC, "vphys_create: cudaMalloc failed (%s)", cudaGetErrorString(e));
     }
     cudaMemset(h->guard_dev, 0, sizeof(unsigned long long));
+    e = cudaMalloc(&h->dev_err, sizeof(unsigned));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(h->guard_dev);
+        delete h;
+        return push_error(VPHYS_ERR_ALLOC, "vphys_create: cudaMalloc failed (%s)", cudaGetErrorString(e));
+    }
+    cudaMemset(h->dev_err, 0, sizeof(unsigned));
     const int core[] = {VPHYS_FIELD_H,        VPHYS_FIELD_RHO,        VPHYS_FIELD_U,      VPHYS_FIELD_V,
                         VPHYS_FIELD_KV,       VPHYS_FIELD_KT,         VPHYS_FIELD_KS,     VPHYS_FIELD_BL_DEPTH,
                         VPHYS_FIELD_B0,       VPHYS_FIELD_STRESS_MAG, VPHYS_FIELD_Q_HEAT, VPHYS_FIELD_Q_SALT,
@@ -905,6 +954,8 @@ int vphys_destroy(vphys_handle *hp)
     if (h->span) cudaFree(h->span);
     if (h->mp_redo) cudaFree(h->mp_redo);
     if (h->zcol) cudaFree(h->zcol);
+    if (h->mom_tiles) cudaFree(h->mom_tiles);
+    if (h->dev_err) cudaFree(h->dev_err);
     if (h->ks_work) cudaFree(h->ks_work);
     if (h->ks_order) cudaFree(h->ks_order);
     if (h->ks_hist) cudaFree(h->ks_hist);
@@ -926,6 +977,7 @@ int vphys_set_config(vphys_handle h, const vphys_config *cfg)
     int st = validate(cfg, h->ntr);
     if (st) return st;
     h->cfg = *cfg;
+    normalize_config(h->cfg);
     return prepare_sources(h);
 }
 
@@ -994,7 +1046,8 @@ int vphys_get_field(vphys_handle h, int field, void *host, size_t n)
     if (st) return st;
     cudaError_t e = cudaMemcpyAsync(host, h->f[sl].ptr(), h->f[sl].bytes(), cudaMemcpyDeviceToHost, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-    return cuda_status(e, "vphys_get_field");
+    if ((st = cuda_status(e, "vphys_get_field"))) return st;
+    return check_dev_err(h);
 }
 
 namespace {
@@ -1201,6 +1254,17 @@ int vphys_nonlocal(vphys_handle h, double dt)
     return cuda_status(cudaGetLastError(), "vphys_nonlocal launch");
 }
 
+int vphys_vdiff_tracers_nonlocal(vphys_handle h, double dt)
+{
+    if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_vdiff_tracers_nonlocal: bad handle");
+    int st = prepare_tracers(h);
+    if (st) return st;
+    if (h->ntr == 0) return VPHYS_OK;
+    Params p = make_params(h);
+    vphys::launch_tracers(p, dt, true, h->cfg.use_kpp && !h->cfg.epbl, h->stream);
+    return cuda_status(cudaGetLastError(), "vphys_vdiff_tracers_nonlocal launch");
+}
+
 int vphys_step(vphys_handle h, double dt, int n_steps)
 {
     if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_step: bad handle");
@@ -1296,7 +1360,10 @@ int vphys_step_graph(vphys_handle h, double dt, int n_steps)
 int vphys_synchronize(vphys_handle h)
 {
     if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_synchronize: bad handle");
-    return cuda_status(cudaStreamSynchronize(h->stream), "vphys_synchronize");
+    int st = cuda_status(cudaStreamSynchronize(h->stream), "vphys_synchronize");
+    if (st) return st;
+    if (h->aux_stream && (st = cuda_status(cudaStreamSynchronize(h->aux_stream), "vphys_synchronize"))) return st;
+    return check_dev_err(h);
 }
 
 int vphys_kpp_attach(vphys_handle h, const vphys_kpp_model *m)

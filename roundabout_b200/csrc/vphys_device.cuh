@@ -489,6 +489,12 @@ __device__ __forceinline__ unsigned long long l2_policy_evict_last()
     asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
     return p;
 }
+__device__ __forceinline__ unsigned long long l2_policy_evict_normal()
+{
+    unsigned long long p;
+    asm("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
 __device__ __forceinline__ unsigned long long l2_policy_evict_first()
 {
     unsigned long long p;
@@ -573,21 +579,22 @@ __device__ __forceinline__ double sw_band_frac(int n, int nb, double blue)
     return xdiv(1.0 - SW_VIS_FRAC, (double)(nb - 2));
 }
 // sw_transmission_nb (:795-812): sum_n frac_n exp(-kappa_n d), kappa_n at
-// kap[(n-1) plane]
-static __device__ __noinline__ double sw_transmission_nb(double d, const double *kap, size_t plane, int nb,
+// kap[col + (n-1) plane] (kap is the opacity field's base: the column offset is
+// applied here, so a null field is never offset)
+static __device__ __noinline__ double sw_transmission_nb(double d, const double *kap, size_t col, size_t plane, int nb,
                                                          double blue)
 {
     double trans = 0.0;
-    for (int n = 1; n <= nb; ++n) trans = trans + sw_band_frac(n, nb, blue) * sm_exp(-(kap[(size_t)(n - 1) * plane] * d));
+    for (int n = 1; n <= nb; ++n) trans = trans + sw_band_frac(n, nb, blue) * sm_exp(-(kap[col + (size_t)(n - 1) * plane] * d));
     return trans;
 }
 __device__ __forceinline__ double kpp_q_t_kin(const vphys_config &c, double q_heat, const double *sw, const double *kap,
-                                              size_t plane, double h_b, double h_sfc)
+                                              size_t col, size_t plane, double h_b, double h_sfc)
 {
     if (c.sw_pen_frac != 0.0 && c.kpp_sw_method != VPHYS_KPP_SW_ALL) {
         const double d = (c.kpp_sw_method == VPHYS_KPP_SW_MXL) ? h_b : h_sfc;
         if (c.sw_chl)
-            return xdiv(q_heat - c.sw_pen_frac * *sw * sw_transmission_nb(d, kap, plane, c.sw_nbands, c.sw_blue_frac),
+            return xdiv(q_heat - c.sw_pen_frac * *sw * sw_transmission_nb(d, kap, col, plane, c.sw_nbands, c.sw_blue_frac),
                         c.rho0 * c.cp);
         return xdiv(sw_q_bl(q_heat, sw, d, c.sw_pen_frac, c.sw_band_ratio, c.sw_zeta1, c.sw_zeta2), c.rho0 * c.cp);
     }

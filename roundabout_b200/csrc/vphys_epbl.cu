@@ -186,13 +186,13 @@ __device__ __forceinline__ double sw_pe_cost_shape(double tau)
 // The chlorophyll N-band ledger of one live layer (rdb_ocean_epbl.F90:
 // 1143-1164): per band the heat absorbed between the layer's top and bottom
 // (the bed opaque), weighted by the PE-cost shape at the band's optical depth.
-static __device__ __noinline__ double sw_phi_nb(double i0, const double *kap, size_t plane, int nb, double blue,
+static __device__ __noinline__ double sw_phi_nb(double i0, const double *kap, size_t col, size_t plane, int nb, double blue,
                                                 double inv_rho0_cp, double dt, double d_top, double d_bot, double hk,
                                                 bool bed)
 {
     double phi_sum = 0.0;
     for (int n = 1; n <= nb; ++n) {
-        const double kn = kap[(size_t)(n - 1) * plane];
+        const double kn = kap[col + (size_t)(n - 1) * plane];
         const double ea = sm_exp(-(kn * d_top));
         const double eb = bed ? 0.0 : sm_exp(-(kn * d_bot));
         const double heat_nb = i0 * sw_band_frac(n, nb, blue) * inv_rho0_cp * dt * (ea - eb);
@@ -276,7 +276,7 @@ __global__ void __launch_bounds__(128, 4) k_epbl(const Params p, double dt, doub
         } else if (c.sw_chl) {
             const double d_bot_sw = d_top_sw + hk;
             ctke_sw[k] = -0.5 * GRAVITY * rho0 * dch_t[k] *
-                         sw_phi_nb(i0_col, p.sw_kappa + col, P, c.sw_nbands, c.sw_blue_frac, inv_rho0_cp, dt,
+                         sw_phi_nb(i0_col, p.sw_kappa, col, P, c.sw_nbands, c.sw_blue_frac, inv_rho0_cp, dt,
                                    d_top_sw, d_bot_sw, hk, k == 1);
             d_top_sw = d_bot_sw;
         } else {

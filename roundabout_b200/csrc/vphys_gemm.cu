@@ -20,7 +20,11 @@
 //     32-lane quarter, alternate 16-column chunks), so the epilogue of tile i
 //     overlaps the loads and MMAs of tile i+1.
 // Every mbarrier wait is bounded: on expiry the CTA records an error code in
-// *err, skips the rest of its work and still frees its tensor memory.
+// *err and skips the rest of its work.  Before the teardown it drains what it
+// already issued -- the producer waits (bounded) for the bytes of every stage
+// it armed, the MMA issuer for its last commit, i.e. for every MMA issued --
+// so no TMA write or tensor-core access is in flight when the CTA frees its
+// tensor memory and exits.
 // No load is multicast; the kernel runs on the calling GPU's memory only.
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -253,10 +257,10 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
         if (lane == 0) {
             // ---- TMA producer ----
             const uint32_t bytes = (uint32_t)(GM + N) * GK * 2;
-            long long it = 0;
+            long long it = 0;   // stages armed so far
             for (int t = 0; t < my_tiles && !*abort_v; ++t) {
                 const int m0 = ((int)blockIdx.x + t * (int)gridDim.x) * GM;
-                for (int kt = 0; kt < nk; ++kt, ++it) {
+                for (int kt = 0; kt < nk; ++kt) {
                     const int s = (int)(it % GSTAGES);
                     const uint32_t round = (uint32_t)(it / GSTAGES);
                     if (!mbar_wait(&empty[s], (round & 1) ^ 1)) {
@@ -267,7 +271,18 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
                     mbar_expect_tx(&full[s], bytes);
                     tma_load_2d(sa + (size_t)s * GM * GK, &tmA, kt * GK, m0, &full[s]);
                     tma_load_2d(sb + (size_t)s * GN_MAX * GK, &tmB, kt * GK, 0, &full[s]);
+                    ++it;
                 }
+            }
+            if (*abort_v) {
+                // Drain: the loads of the last GSTAGES armed stages may still be
+                // writing shared memory.  Each stage's latest armed phase
+                // completes when its bytes have landed (whether or not the MMA
+                // warp consumed it), and no stage is re-armed after this point,
+                // so waiting on that phase's parity is unambiguous.
+                const long long first = it > GSTAGES ? it - GSTAGES : 0;
+                for (long long a = first; a < it; ++a)
+                    if (!mbar_wait(&full[(int)(a % GSTAGES)], (uint32_t)((a / GSTAGES) & 1))) atomicExch(g.err, 5);
             }
         }
     } else if (warp == 1) {
@@ -275,6 +290,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
             // ---- MMA issuer ----
             const uint32_t idesc = idesc_bf16(GM, N);
             long long it = 0;
+            int last_commit = -1;   // the tile of the last acc_full commit
             for (int t = 0; t < my_tiles && !*abort_v; ++t) {
                 const int a = t & 1;
                 if (!mbar_wait(&acc_empty[a], ((t >> 1) & 1) ^ 1)) {
@@ -316,7 +332,14 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
                 asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                                  smem_u32(&acc_full[a]))
                              : "memory");
+                last_commit = t;
                 if (!ok) break;
+            }
+            if (*abort_v && last_commit >= 0) {
+                // Drain: the commit arrives on acc_full once every MMA issued
+                // before it has retired (its shared-memory reads and its tensor-
+                // memory writes), so the teardown below frees nothing in use.
+                if (!mbar_wait(&acc_full[last_commit & 1], (uint32_t)((last_commit >> 1) & 1))) atomicExch(g.err, 6);
             }
         }
     } else {

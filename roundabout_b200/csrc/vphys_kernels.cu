@@ -22,6 +22,8 @@
 //   (the tracer kernel lives in vphys_tracers.cu)
 #include <cuda_runtime.h>
 
+#include <cstdlib>
+
 #include "vphys_device.cuh"
 #include "vphys_faces.cuh"
 #include "vphys_kernels.cuh"
@@ -142,17 +144,17 @@ __global__ void k_sw_penetration(const Params p, double inv_scale)
         }
     // the chlorophyll scheme absorbs all of the source (apply_sw_penetration_nb_impl, :1606-1668)
     const bool nbs = c.sw_chl != 0;
-    const double *kap = p.sw_kappa + col;
+    const double *kap = p.sw_kappa;   // base pointer: null unless sw_chl
     double i0col = nbs ? __ldg(p.sw_src + col) * __ldg(p.wet + col)
                        : c.sw_pen_frac * __ldg(p.sw_src + col) * __ldg(p.wet + col);
     if (p.cover_frac) i0col = i0col * (1.0 - __ldg(p.cover_frac + col));   // no light under an ice shelf
     double d_top = 0.0;
-    double trans_top = nbs ? sw_transmission_nb(d_top, kap, P, c.sw_nbands, c.sw_blue_frac) : sw_transmission(c, d_top);
+    double trans_top = nbs ? sw_transmission_nb(d_top, kap, col, P, c.sw_nbands, c.sw_blue_frac) : sw_transmission(c, d_top);
     for (int k = nz; k >= k_dep; --k) {
         const size_t off = P * (size_t)(k - 1);
         const double hk = __ldg(hp + off);
         const double d_bot = d_top + hk;
-        const double trans_bot = (k > k_dep) ? (nbs ? sw_transmission_nb(d_bot, kap, P, c.sw_nbands, c.sw_blue_frac)
+        const double trans_bot = (k > k_dep) ? (nbs ? sw_transmission_nb(d_bot, kap, col, P, c.sw_nbands, c.sw_blue_frac)
                                                     : sw_transmission(c, d_bot))
                                              : 0.0;
         if (hk > H_VANISHED) {
@@ -291,7 +293,7 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
         const double tau_mag = p.stress_mag[col];
         const double u_star = sqrt(xdiv(tau_mag, rho0));
         // pass 1 charges the shortwave that passes the lagged boundary layer
-        q_T_kin = kpp_q_t_kin(c, p.q_heat[col], p.sw_src + col, p.sw_kappa + col, p.plane, h_b, HH(k_sfc));
+        q_T_kin = kpp_q_t_kin(c, p.q_heat[col], p.sw_src + col, p.sw_kappa, col, p.plane, h_b, HH(k_sfc));
         q_S_kin = xdiv(p.q_salt[col], rho0);
         double T_sfc = 0.0, S_sfc = 0.0;
         if (c.buoyancy_coeffs) {   // "eos": the surface layer's (T, S) (rdb_ocean_vmix.F90:1357-1376)
@@ -366,7 +368,7 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
         }
         // ---- KPP pass 2 scalars (rdb_ocean_vmix.F90:1429-1491) ----
         if (c.sw_pen_frac != 0.0) {   // pass 2 charges what passes the new boundary layer
-            q_T_kin = kpp_q_t_kin(c, p.q_heat[col], p.sw_src + col, p.sw_kappa + col, p.plane, h_b, HH(k_sfc));
+            q_T_kin = kpp_q_t_kin(c, p.q_heat[col], p.sw_src + col, p.sw_kappa, col, p.plane, h_b, HH(k_sfc));
             B_0 = kpp_surface_b0(c, q_T_kin, q_S_kin, HH(k_sfc), T_sfc, S_sfc);
         }
         p.b0[col] = B_0;
@@ -1029,6 +1031,19 @@ void launch_column_depth(const Params &p, cudaStream_t stream)
     k_column_depth<<<dim3((p.nx + 127) / 128, p.ny), 128, 0, stream>>>(p);
 }
 
+// VPHYS_MOMENTUM_TMA=0 runs the register-prefetched solves where the
+// TMA-staged ones apply (for the exact solve the two give the same bits;
+// the switch is for comparing their speed).
+bool momentum_ring_enabled()
+{
+    static int on = -1;
+    if (on < 0) {
+        const char *e = getenv("VPHYS_MOMENTUM_TMA");
+        on = (e && atoi(e) == 0) ? 0 : 1;
+    }
+    return on == 1;
+}
+
 void launch_momentum(const Params &p, double dt, cudaStream_t stream)
 {
     if (p.cfg.hvel_mom6 && !p.cfg.hvel_harmonic) launch_column_depth(p, stream);
@@ -1036,6 +1051,7 @@ void launch_momentum(const Params &p, double dt, cudaStream_t stream)
         launch_momentum_mp(p, dt, stream);
         return;
     }
+    if (momentum_ring_enabled() && launch_momentum_tma(p, dt, stream)) return;
     static bool attr_set = false;
     if (!attr_set) {
         const int mx = (int)((size_t)VPHYS_NZ_MAX * MOM_THREADS * sizeof(double));

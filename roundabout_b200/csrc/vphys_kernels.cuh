@@ -51,6 +51,8 @@ struct Params {
     int *span;                        // per column: first | last live layer << 16 (0: none), scratch
     unsigned *mp_redo;                // mixed solves: count, then (group << 5 | tracer) re-solved in FP64
     double *zcol;                     // per column: -sum_k h, k = 1..nz in order (momentum z_clear), scratch
+    unsigned char *mom_tile_skip;     // per face tile of the TMA-staged momentum solve: 1 = nothing to solve
+    unsigned *dev_err;                // bounded waits that ran out (bit 0: consumer, 1: producer, 2: drain)
     const double *coriolis;           // (nx, ny) f, or nullptr (learned KPP features, kappa-shear f^2)
     double *kd_shear, *tke_shear;     // (nx, ny, nz+1) kappa-shear diffusivity and TKE, or nullptr
     double *kd_epbl, *mld_epbl;       // (nx, ny, nz+1) EPBL diffusivity, (nx, ny) its MLD, or nullptr
@@ -87,6 +89,15 @@ void launch_epbl(const Params &p, double dt, cudaStream_t stream);
 void launch_assemble(const Params &p, cudaStream_t stream);
 void launch_smooth(const Params &p, double *fld, double *scratch, cudaStream_t stream);
 void launch_momentum(const Params &p, double dt, cudaStream_t stream);
+// the TMA-staged exact momentum solve (vphys_momentum_tma.cu): false when the
+// configuration or the buffers do not qualify (the caller runs k_momentum)
+bool launch_momentum_tma(const Params &p, double dt, cudaStream_t stream);
+bool momentum_tma_eligible(const Params &p);
+int momentum_tma_tiles(const Params &p);
+// the same ring for the mixed-precision face solve (vphys_mixed.cu)
+bool launch_momentum_mp_tma(const Params &p, double dt, cudaStream_t stream);
+// false when VPHYS_MOMENTUM_TMA=0 asks for the register-prefetched solves
+bool momentum_ring_enabled();
 // -sum of h over each column, accumulated k = 1..nz as vdiff's z_clear does (into p.zcol)
 void launch_column_depth(const Params &p, cudaStream_t stream);
 void launch_tracers(const Params &p, double dt, bool diffuse, bool nonlocal, cudaStream_t stream);

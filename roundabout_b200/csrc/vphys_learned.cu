@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(FEAT_THREADS) k_kpp_features(const Params p, c
 
     const double u_star = sqrt(xdiv(p.stress_mag[col], rho0));
     // the B0 of KPP pass 1: with shortwave, the part passing the lagged h_b is not charged
-    const double q_T_kin = kpp_q_t_kin(c, p.q_heat[col], p.sw_src + col, p.sw_kappa + col, p.plane, p.bl_depth[col], HH(k_sfc));
+    const double q_T_kin = kpp_q_t_kin(c, p.q_heat[col], p.sw_src + col, p.sw_kappa, col, p.plane, p.bl_depth[col], HH(k_sfc));
     const double q_S_kin = xdiv(p.q_salt[col], rho0);
     double T_sfc = 0.0, S_sfc = 0.0;
     if (c.buoyancy_coeffs) {   // the same surface (T, S) the assembly's B0 will use

@@ -42,6 +42,7 @@
 #include "vphys_device.cuh"
 #include "vphys_faces.cuh"
 #include "vphys_kernels.cuh"
+#include "vphys_mom_ring.cuh"
 
 namespace vphys {
 
@@ -395,7 +396,7 @@ __global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, doubl
             const double u_star = sqrt(xdiv(p.stress_mag[col], rho0));
             // the heat flux pass 2 charged (shortwave: what passes h_b, or the
             // surface layer hi)
-            const double q_T_kin = kpp_q_t_kin(c, p.q_heat[col], p.sw_src + col, p.sw_kappa + col, p.plane, h_b, __ldg(hp + P * (size_t)(hi - 1)));
+            const double q_T_kin = kpp_q_t_kin(c, p.q_heat[col], p.sw_src + col, p.sw_kappa, col, p.plane, h_b, __ldg(hp + P * (size_t)(hi - 1)));
             const double q_S_kin = xdiv(p.q_salt[col], rho0);
             // with "eos" coefficients or shortwave B0 is the assembly's (pass 2
             // stored it before the solve changed the surface T and S); otherwise
@@ -610,6 +611,142 @@ __global__ void __launch_bounds__(MP_MOM_THREADS) k_momentum_mp(const Params p, 
     }
 }
 
+// One face of the mixed-precision solve at the default momentum knobs,
+// driven by the TMA-staged ring (momentum_ring_cta): the arithmetic of
+// solve_face_mp<., true> above, its t and v rows in the ring kernel's
+// shared-memory row area, the old velocity read again from L2 by the
+// back-substitution.
+struct MixedFace {
+    vphys_config c;
+    double *uf;
+    size_t PF;
+    float *st, *sv;
+    int tid, nz;
+    bool valid;
+    unsigned long long pol_keep;
+    float dtf, bbl_thick, i_hbbl, zacc, zcol_l, zcol_r, d_min;
+    float hv_p, zi_p, num_t, dz_t, q_prev, t_prev;
+    double w, u_c, u_m;
+
+    __device__ __forceinline__ void start(const Params &p, double dt, const FaceCells &fc, bool valid_, double *uf_,
+                                          size_t PF_, unsigned char *rows, int tid_)
+    {
+        c = p.cfg;
+        default_face_knobs(c);
+        uf = uf_;
+        PF = PF_;
+        nz = p.nz;
+        st = reinterpret_cast<float *>(rows);
+        sv = st + (size_t)nz * MT_TW;
+        tid = tid_;
+        valid = valid_;
+        pol_keep = l2_policy_evict_last();
+        dtf = (float)dt;
+        bbl_thick = (float)c.hbbl_visc;
+        i_hbbl = __frcp_rn(bbl_thick + (float)EPS_HVEL);
+        zacc = 0.0f;
+        zcol_l = (float)p.zcol[fc.cl];
+        zcol_r = (float)p.zcol[fc.cr];
+        d_min = fmn(-zcol_l, -zcol_r);
+        num_t = 0.0f;
+        dz_t = 1.0f;
+        q_prev = 1.0f;
+        t_prev = 0.0f;
+        w = 0.0;
+        u_m = 0.0;
+    }
+    __device__ __forceinline__ void first(double hl, double hr, double uw)
+    {
+        u_c = uw;
+        face_layer<float>(c, (float)hl, (float)hr, (float)u_c, 1, 1, d_min, i_hbbl, zacc, zcol_l, zcol_r, hv_p, zi_p);
+    }
+    template <bool NEXT>
+    __device__ __forceinline__ void step(int k, double hl, double hr, double kvl, double kvr, double u_next)
+    {
+        const float hv_0 = hv_p, zi_0 = zi_p;
+        const float num_b = num_t, dz_b = dz_t;
+        double u_p = 0.0;
+        if (NEXT) {
+            u_p = u_next;
+            face_layer<float>(c, (float)hl, (float)hr, (float)u_p, k + 1, 1, d_min, i_hbbl, zacc, zcol_l, zcol_r, hv_p,
+                              zi_p);
+            bool cut;
+            interface_coupling<float>(c, hv_0, hv_p, zi_0, dtf, 0.0f, bbl_thick, (float)kvl, (float)kvr, num_t, dz_t,
+                                      cut);
+        }
+        const float H = fmx(hv_0, (float)H_VANISHED);
+        float f_up = 0.0f, f_dn = 0.0f;
+        const float ex = 0.0f;
+        if (k == 1 && 1 < nz) f_up = __fdividef(num_t, dz_t);
+        if (k == nz && k > 1) f_dn = __fdividef(num_b, dz_b);
+        if (k > 1 && k < nz) {
+            f_dn = __fdividef(num_b, dz_b);
+            f_up = __fdividef(num_t, dz_t);
+        }
+        const double b = (double)f_dn * (u_m - u_c) + (double)f_up * (u_p - u_c) - (double)ex * u_c;
+        const float t_in = (f_dn != 0.0f) ? t_prev : 0.0f;
+        const float sx = H + ex + f_dn * q_prev;
+        float ip, t, qq;
+        pivot_row(sx, f_up, ip, t, qq);
+        w = b + mul_u(t_in, w);
+        const size_t s = (size_t)(k - 1) * MT_TW + tid;
+        sv[s] = (float)(w * (double)ip);
+        st[s] = t;
+        q_prev = qq;
+        t_prev = t;
+        u_m = u_c;
+        u_c = u_p;
+    }
+    __device__ __forceinline__ void row(int m, double hl, double hr, double kvl, double kvr, double uw)
+    {
+        step<true>(m, hl, hr, kvl, kvr, uw);
+    }
+    __device__ __forceinline__ void last() { step<false>(nz, 0.0, 0.0, 0.0, 0.0, 0.0); }
+    __device__ __forceinline__ void back()
+    {
+        float delta = 0.0f;
+        for (int k0 = nz; k0 >= 1; k0 -= MP_MOM_U) {
+            double uo[MP_MOM_U];
+#pragma unroll
+            for (int q = 0; q < MP_MOM_U; ++q) {
+                const int k = k0 - q;
+                uo[q] = (k >= 1 && valid) ? ld_hint(uf + PF * (size_t)(k - 1), pol_keep) : 0.0;
+            }
+#pragma unroll
+            for (int q = 0; q < MP_MOM_U; ++q) {
+                const int k = k0 - q;
+                if (k < 1) break;
+                const size_t s = (size_t)(k - 1) * MT_TW + tid;
+                delta = sv[s] + mul_u(st[s], delta);
+                if (valid) uf[PF * (size_t)(k - 1)] = uo[q] + (double)delta;
+            }
+        }
+    }
+};
+
+__global__ void __launch_bounds__(MT_THREADS, 2)
+    k_momentum_mp_tma(const __grid_constant__ MomMaps maps, const Params p, double dt, int ntiles)
+{
+    extern __shared__ __align__(128) unsigned char mt_smem[];
+    momentum_ring_cta<MixedFace>(maps, p, dt, ntiles, mt_smem);
+}
+
+bool launch_momentum_mp_tma(const Params &p, double dt, cudaStream_t stream)
+{
+    MomMaps maps;
+    int ntiles = 0;
+    if (!momentum_ring_prepare(p, &maps, &ntiles, stream)) return false;
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_momentum_mp_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        attr_set = true;
+    }
+    const size_t smem = mt_smem_bytes(p.nz);
+    const int grid = momentum_ring_grid((const void *)k_momentum_mp_tma, ntiles, smem);
+    k_momentum_mp_tma<<<grid, MT_THREADS, smem, stream>>>(maps, p, dt, ntiles);
+    return true;
+}
+
 template <bool TWO, int TPW>
 static void launch_tracers_mp_t(const Params &p, double dt, bool nonlocal, cudaStream_t stream)
 {
@@ -681,6 +818,7 @@ void launch_tracers_mp(const Params &p, double dt, bool nonlocal, cudaStream_t s
 
 void launch_momentum_mp(const Params &p, double dt, cudaStream_t stream)
 {
+    if (momentum_ring_enabled() && launch_momentum_mp_tma(p, dt, stream)) return;
     const int bs = MP_MOM_THREADS;
     static bool attr_set = false;
     if (!attr_set) {

@@ -230,7 +230,7 @@ __device__ __forceinline__ void tracer_columns(const Params &p, double dt, int d
         const double u_star = sqrt(xdiv(p.stress_mag[col], rho0));
         // the heat flux pass 2 charged (shortwave: what passes h_b, or the
         // surface layer k_hi)
-        q_T_kin = kpp_q_t_kin(c, p.q_heat[col], p.sw_src + col, p.sw_kappa + col, p.plane, h_b, h_hi);
+        q_T_kin = kpp_q_t_kin(c, p.q_heat[col], p.sw_src + col, p.sw_kappa, col, p.plane, h_b, h_hi);
         q_S_kin = xdiv(p.q_salt[col], rho0);
         // with "eos" coefficients or shortwave B0 is the assembly's (pass 2
         // stored it before the solve changed the surface T and S); otherwise

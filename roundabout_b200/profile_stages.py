@@ -4,7 +4,8 @@
     python -m roundabout_b200.profile_stages --config batched_1440x1080x75 --mixed 1
     python -m roundabout_b200.profile_stages --nx 512 --ny 384 --stages features,mlp
 
-Stages: eos, assemble, momentum, tracers, step (the path), kshear (the
+Stages: eos, assemble, momentum, tracers (the fused diffusion + non-local
+launch the step runs), step (the path), kshear (the
 kappa-shear column solve, vphys_kappa_shear, default knobs, Wright EOS), epbl
 (the EPBL column solve, vphys_epbl, default knobs: OM4 mstar), and
 features, mlp (the learned KPP's feature extraction and its three tensor-core
@@ -69,7 +70,7 @@ def main():
            "kshear": 8.0 * 7 + 16 * ifc,   # h, u and v (two faces each), T, S in; kd, tke out
            "epbl": 24.0 + 8 * ifc}         # h, T, S in; kd out (the 2-D forcing and MLD ~0.1 B/cell)
     fns = {"eos": vp.eos, "assemble": vp.assemble, "momentum": lambda: vp.vdiff_momentum(dt),
-           "tracers": lambda: vp.vdiff_tracers(dt), "step": lambda: vp.step(dt, 1),
+           "tracers": lambda: vp.vdiff_tracers_nonlocal(dt), "step": lambda: vp.step(dt, 1),
            "kshear": lambda: vp.kappa_shear(dt), "epbl": lambda: vp.epbl(dt)}
     ncols = args.nx * args.ny
     if "features" in args.stages or "mlp" in args.stages:

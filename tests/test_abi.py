@@ -136,8 +136,9 @@ def test_every_named_field_has_a_shape():
 
 
 def test_chlorophyll_knobs_are_validated(lib):
-    """The chlorophyll scheme needs sw_pen_frac = 1, 3..6 bands and a positive
-    clear-water opacity per band (rdb_config_validate.F90:291-310)."""
+    """The chlorophyll scheme needs sw_pen_frac = 1 (or 0, which selects 1),
+    3..6 bands and a positive clear-water opacity per band
+    (rdb_config_validate.F90:291-310)."""
     from roundabout_b200 import _ffi
     from roundabout_b200.config import default_config
 
@@ -150,3 +151,29 @@ def test_chlorophyll_knobs_are_validated(lib):
             setattr(bad, k, v)
         assert lib.vphys_create(4, 4, 4, 2, ctypes.byref(bad), ctypes.byref(h)) == _ffi.ERR_CONFIG, over
         assert h.value is None
+
+
+@pytest.mark.gpu
+def test_chlorophyll_unset_fraction_selects_one(lib):
+    """sw_chl = 1 with sw_pen_frac left at 0 ("unset") is accepted and stored
+    as 1, as the reference's set_sw_chl does (rdb_ocean_sw_chl.F90:87-103)."""
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from roundabout_b200 import _ffi
+    from roundabout_b200.config import default_config
+
+    cfg = default_config()
+    cfg.sw_chl = 1
+    cfg.sw_pen_frac = 0.0
+    h = ctypes.c_void_p()
+    assert lib.vphys_create(4, 4, 4, 2, ctypes.byref(cfg), ctypes.byref(h)) == _ffi.OK
+    got = _ffi.VphysConfig()
+    assert lib.vphys_get_config(h, ctypes.byref(got)) == _ffi.OK
+    assert got.sw_pen_frac == 1.0 and got.sw_chl == 1
+    cfg.sw_pen_frac = 0.0
+    assert lib.vphys_set_config(h, ctypes.byref(cfg)) == _ffi.OK
+    assert lib.vphys_get_config(h, ctypes.byref(got)) == _ffi.OK
+    assert got.sw_pen_frac == 1.0
+    assert lib.vphys_destroy(ctypes.byref(h)) == _ffi.OK
