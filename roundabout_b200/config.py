@@ -6,11 +6,15 @@ ocean_vdiff_t, rdb_ocean_vdiff.F90:78-260; namelist defaults
 src/core/rdb_config.F90:1872-1893, 1936-1945) -- the same values
 `vphys_config_default()` writes in C.
 
-The closure classes mirror python/rdb/closures.py (PacanowskiPhilander, KPP,
+The closure classes mirror the vertical closures of python/rdb/closures.py
+(PacanowskiPhilander, KPP, Langmuir, EPBL, KappaShear, ConvectiveAdjustment,
 BryanLewisBackground, ConstantBackground, NearSurfaceViscosity,
-ConvectiveAdjustment, HarmonicFaceThickness, ImplicitVerticalFriction,
-DiffusivityLimits): same names, same keyword meanings, each writing only its
-own knobs into the config through `apply(cfg)`.
+HarmonicFaceThickness, ThermoSubcycling, ImplicitVerticalFriction,
+DiffusivityLimits; TidalMixing, DoubleDiffusion and HenyeyBackground raise
+when applied): the same names, keywords, defaults and knob targets, each
+writing only its own knobs into the config through `apply(cfg)`.  Keywords
+that exist only here are listed in each class and default to the reference's
+behaviour.
 """
 from __future__ import annotations
 
@@ -198,17 +202,23 @@ def seed_backgrounds(cfg: VphysConfig):
 # Closure objects (python/rdb/closures.py:20-413)
 # ---------------------------------------------------------------------------
 class PacanowskiPhilander:
-    """PP81 interior closure; `enabled=False` selects interior_closure="none"."""
+    """PP81 interior closure (python/rdb/closures.py:20-47):
+    `PacanowskiPhilander(nu0=1e-2, nu_bg=1e-3, kappa_bg=1e-4, alpha=5.0,
+    shear2_floor=1e-9, enabled=True)`.  `enabled=False` turns the whole
+    closure off (`use_closure = .false.`), which selects the reference's
+    scalar-K vdiff path; this library refuses that configuration with
+    VPHYS_ERR_CONFIG when the handle is created or reconfigured."""
 
-    def __init__(self, nu0=1e-2, nu_bg=1e-4, kappa_bg=1e-5, alpha=5.0, shear2_floor=1e-10, enabled=True):
+    def __init__(self, nu0=1e-2, nu_bg=1e-3, kappa_bg=1e-4, alpha=5.0, shear2_floor=1e-9, enabled=True):
         self.nu0, self.nu_bg, self.kappa_bg = nu0, nu_bg, kappa_bg
         self.alpha, self.shear2_floor = alpha, shear2_floor
         self.enabled = bool(enabled)
 
     def apply(self, cfg):
-        cfg.interior_closure = INTERIOR_PP81 if self.enabled else INTERIOR_NONE
+        cfg.use_closure = int(self.enabled)
         if not self.enabled:
             return cfg
+        cfg.interior_closure = INTERIOR_PP81
         cfg.pp81_nu0 = float(self.nu0)
         cfg.pp81_nu_bg = float(self.nu_bg)
         cfg.pp81_kappa_bg = float(self.kappa_bg)
@@ -218,10 +228,22 @@ class PacanowskiPhilander:
 
 
 class KPP:
-    """KPP boundary-layer overlay (no shortwave penetration on this path)."""
+    """KPP boundary-layer overlay (python/rdb/closures.py:50-85):
+    `KPP(ri_crit=0.3, cs_nonlocal=6.3, c_vt2=1.8, shortwave_method="mxl_sw",
+    enabled=True)`; `shortwave_method` is the reference's kpp_sw_method
+    string ("all_sw", "mxl_sw", "lv1_sw": parse_kpp_sw_method,
+    rdb_ocean_vmix.F90:1561-1577).  Extra keywords of this library, left
+    unset by default: `alpha_T`, `beta_S` (the constant buoyancy
+    coefficients of KPP's B0)."""
 
-    def __init__(self, ri_crit=0.3, cs_nonlocal=6.3, c_vt2=1.8, alpha_T=None, beta_S=None, enabled=True):
+    _SW = {"all_sw": 1, "mxl_sw": 2, "lv1_sw": 3}
+
+    def __init__(self, ri_crit=0.3, cs_nonlocal=6.3, c_vt2=1.8, shortwave_method="mxl_sw", enabled=True,
+                 alpha_T=None, beta_S=None):
+        if shortwave_method not in self._SW:
+            raise ValueError(f"KPP: shortwave_method must be one of {sorted(self._SW)}")
         self.ri_crit, self.cs_nonlocal, self.c_vt2 = ri_crit, cs_nonlocal, c_vt2
+        self.shortwave_method = shortwave_method
         self.alpha_T, self.beta_S = alpha_T, beta_S
         self.enabled = bool(enabled)
 
@@ -232,6 +254,7 @@ class KPP:
         cfg.ri_crit = float(self.ri_crit)
         cfg.cs_nonlocal = float(self.cs_nonlocal)
         cfg.c_vt2 = float(self.c_vt2)
+        cfg.kpp_sw_method = self._SW[self.shortwave_method]
         if self.alpha_T is not None:
             cfg.alpha_T = float(self.alpha_T)
         if self.beta_S is not None:
@@ -240,7 +263,11 @@ class KPP:
 
 
 class BryanLewisBackground:
-    def __init__(self, kd_surface=1e-5, kd_deep=1.3e-4, z0=2500.0, delta=222.0, prandtl=-1.0):
+    """Depth-varying background Kd (python/rdb/closures.py:237-260):
+    `BryanLewisBackground(kd_surface=1e-5, kd_deep=1.3e-4, z0=2500.0,
+    delta=222.0, prandtl=1.0)`."""
+
+    def __init__(self, kd_surface=1e-5, kd_deep=1.3e-4, z0=2500.0, delta=222.0, prandtl=1.0):
         self.kd_surface, self.kd_deep, self.z0, self.delta, self.prandtl = kd_surface, kd_deep, z0, delta, prandtl
 
     def apply(self, cfg):
@@ -254,19 +281,23 @@ class BryanLewisBackground:
 
 
 class ConstantBackground:
-    def __init__(self, kv=1e-4, kt=1e-5):
+    """The scalar background floor (python/rdb/closures.py:284-295):
+    `ConstantBackground(kv=1e-3, kt=1e-4)` writes pp81_nu_bg /
+    pp81_kappa_bg, from which the vmix initialisation seeds the kv/kt/ks
+    floors (vmix_seed_backgrounds, rdb_ocean_vmix.F90:843-913)."""
+
+    def __init__(self, kv=1e-3, kt=1e-4):
         self.kv, self.kt = kv, kt
 
     def apply(self, cfg):
-        cfg.bkgnd_profile = 0
-        cfg.kv_bg = float(self.kv)
-        cfg.kt_bg = float(self.kt)
-        cfg.ks_bg = float(self.kt)
-        return cfg
+        cfg.pp81_nu_bg = float(self.kv)
+        cfg.pp81_kappa_bg = float(self.kt)
+        return seed_backgrounds(cfg)
 
 
 class NearSurfaceViscosity:
-    """KV_ML_INVZ2 surface band."""
+    """KV_ML_INVZ2 surface band (python/rdb/closures.py:298-319):
+    `NearSurfaceViscosity(kv=0.0, hmix=20.0)`."""
 
     def __init__(self, kv=0.0, hmix=20.0):
         self.kv, self.hmix = kv, hmix
@@ -278,6 +309,9 @@ class NearSurfaceViscosity:
 
 
 class ConvectiveAdjustment:
+    """(python/rdb/closures.py:200-213) `ConvectiveAdjustment(kd=1.0,
+    prandtl=1.0, n2_threshold=0.0)`."""
+
     def __init__(self, kd=1.0, prandtl=1.0, n2_threshold=0.0):
         self.kd, self.prandtl, self.n2_threshold = kd, prandtl, n2_threshold
 
@@ -397,41 +431,111 @@ class KappaShear:
 
 
 class HarmonicFaceThickness:
-    """`use_harmonic`: harmonic mean in the vdiff face-thickness denominators."""
+    """MOM6 HARMONIC_VISC (python/rdb/closures.py:322-336):
+    `HarmonicFaceThickness()` sets the namelist's harmonic_visc, which the
+    vdiff set-up copies into `use_harmonic`
+    (rdb_ocean_setup_vmix.F90:378-379): harmonic-mean face thickness in the
+    vertical-friction and diffusion matrices."""
 
     def apply(self, cfg):
         cfg.use_harmonic = 1
         return cfg
 
 
-class ImplicitVerticalFriction:
-    def __init__(self, stress=False, drag=False, harmonic_thickness=False, mom6_face_thickness=True,
-                 upwind=True, bbl_glue=False, hbbl=10.0):
-        self.stress, self.drag = stress, drag
-        self.harmonic_thickness, self.mom6_face_thickness = harmonic_thickness, mom6_face_thickness
-        self.upwind, self.bbl_glue, self.hbbl = upwind, bbl_glue, hbbl
+class ThermoSubcycling:
+    """(python/rdb/closures.py:339-352) `ThermoSubcycling(ratio=1)`: the
+    thermo step runs every `ratio` dynamics steps.  vphys_step IS the
+    thermo step of this path, so the caller calls it every `ratio` steps;
+    the object only checks the ratio."""
+
+    def __init__(self, ratio=1):
+        if int(ratio) < 1:
+            raise ValueError("ThermoSubcycling: ratio must be >= 1")
+        self.ratio = int(ratio)
 
     def apply(self, cfg):
-        cfg.implicit_stress = int(self.stress)
-        cfg.implicit_drag = int(self.drag)
-        cfg.hvel_mom6 = int(self.mom6_face_thickness)
-        cfg.hvel_harmonic = int(self.harmonic_thickness)
-        cfg.hvel_upwind = int(self.upwind)
-        cfg.bbl_glue = int(self.bbl_glue)
+        return cfg
+
+
+class ImplicitVerticalFriction:
+    """Implicit vertical friction (python/rdb/closures.py:355-392):
+    `ImplicitVerticalFriction(stress=False, drag=False,
+    harmonic_thickness=True, harmonic_visc=False, bbl_glue=True, hbbl=10.0,
+    bbl_piston=3e-4)`.  `harmonic_thickness` -> hvel_mom6 (MOM6's momentum
+    face thickness), `harmonic_visc` -> hvel_harmonic (which branch of it),
+    `bbl_glue` -> the BBL glue.  As in the reference's vdiff set-up, the
+    glue latches off unless a bottom drag is configured
+    (rdb_ocean_setup_vmix.F90:385-393, "No drag configured => the latch
+    leaves the glue OFF"); `bottom_drag=True` (an extra keyword of this
+    library, for a caller whose bottom-drag configuration is set) keeps it.
+    `upwind` (extra, default True as in the namelist) is hvel_upwind."""
+
+    def __init__(self, stress=False, drag=False, harmonic_thickness=True, harmonic_visc=False, bbl_glue=True,
+                 hbbl=10.0, bbl_piston=3e-4, bottom_drag=False, upwind=True):
+        self.stress, self.drag = stress, drag
+        self.harmonic_thickness, self.bbl_glue = harmonic_thickness, bbl_glue
+        self.harmonic_visc = harmonic_visc
+        self.hbbl, self.bbl_piston = hbbl, bbl_piston
+        self.bottom_drag, self.upwind = bottom_drag, upwind
+
+    def apply(self, cfg):
+        cfg.implicit_stress = int(bool(self.stress))
+        cfg.implicit_drag = int(bool(self.drag))
+        cfg.hvel_mom6 = int(bool(self.harmonic_thickness))
+        cfg.hvel_harmonic = int(bool(self.harmonic_visc))
+        cfg.bbl_glue = int(bool(self.bbl_glue) and bool(self.bottom_drag))
         cfg.hbbl_visc = float(self.hbbl)
+        cfg.bbl_piston = float(self.bbl_piston)
+        cfg.hvel_upwind = int(bool(self.upwind))
         return cfg
 
 
 class DiffusivityLimits:
-    def __init__(self, kv_max=HUGE, kd_max=HUGE, smoothing=0, guard=False):
+    """The floors/ceilings/smoothing gate (python/rdb/closures.py:395-405):
+    `DiffusivityLimits(kv_max=1e6, kd_max=1e6, smoothing=0)`; `guard` (an
+    extra keyword of this library, default off) is vmix_guard."""
+
+    def __init__(self, kv_max=1e6, kd_max=1e6, smoothing=0, guard=False):
         self.kv_max, self.kd_max, self.smoothing, self.guard = kv_max, kd_max, smoothing, guard
 
     def apply(self, cfg):
         cfg.kv_max = float(self.kv_max)
         cfg.kd_max = float(self.kd_max)
         cfg.kd_smooth_iterations = int(self.smoothing)
-        cfg.vmix_guard = int(self.guard)
+        cfg.vmix_guard = int(bool(self.guard))
         return cfg
+
+
+class _NotOnThisPath:
+    """A reference closure whose contribution this library does not build;
+    applying it raises, so a reference script fails loudly instead of
+    running without it."""
+
+    what = ""
+
+    def __init__(self, *args, **kwargs):
+        self.args, self.kwargs = args, kwargs
+
+    def apply(self, cfg):
+        raise NotImplementedError(f"{type(self).__name__}: {self.what} is not built in this library")
+
+
+class TidalMixing(_NotOnThisPath):
+    """(python/rdb/closures.py:183-197) St-Laurent/Simmons tidal mixing."""
+
+    what = "the tidal-mixing contributor"
+
+
+class DoubleDiffusion(_NotOnThisPath):
+    """(python/rdb/closures.py:216-234) salt fingering and diffusive convection."""
+
+    what = "the double-diffusion split of kt/ks"
+
+
+class HenyeyBackground(_NotOnThisPath):
+    """(python/rdb/closures.py:263-281) the latitude-scaled background."""
+
+    what = "the Henyey background"
 
 
 def compose(*closures, base: VphysConfig | None = None) -> VphysConfig:
