@@ -1031,9 +1031,8 @@ void launch_column_depth(const Params &p, cudaStream_t stream)
     k_column_depth<<<dim3((p.nx + 127) / 128, p.ny), 128, 0, stream>>>(p);
 }
 
-// VPHYS_MOMENTUM_TMA=0 runs the register-prefetched solves where the
-// TMA-staged ones apply (for the exact solve the two give the same bits;
-// the switch is for comparing their speed).
+// VPHYS_MOMENTUM_TMA=0 runs the register-prefetched mixed face solve where
+// the TMA-staged ring applies (the switch is for comparing their speed).
 bool momentum_ring_enabled()
 {
     static int on = -1;
@@ -1051,7 +1050,6 @@ void launch_momentum(const Params &p, double dt, cudaStream_t stream)
         launch_momentum_mp(p, dt, stream);
         return;
     }
-    if (momentum_ring_enabled() && launch_momentum_tma(p, dt, stream)) return;
     static bool attr_set = false;
     if (!attr_set) {
         const int mx = (int)((size_t)VPHYS_NZ_MAX * MOM_THREADS * sizeof(double));

@@ -89,13 +89,12 @@ void launch_epbl(const Params &p, double dt, cudaStream_t stream);
 void launch_assemble(const Params &p, cudaStream_t stream);
 void launch_smooth(const Params &p, double *fld, double *scratch, cudaStream_t stream);
 void launch_momentum(const Params &p, double dt, cudaStream_t stream);
-// the TMA-staged exact momentum solve (vphys_momentum_tma.cu): false when the
-// configuration or the buffers do not qualify (the caller runs k_momentum)
-bool launch_momentum_tma(const Params &p, double dt, cudaStream_t stream);
+// the TMA-staged ring of the mixed-precision face solve (vphys_mixed.cu,
+// host side in vphys_momentum_tma.cu): false when the configuration or the
+// buffers do not qualify (the caller runs k_momentum_mp)
+bool launch_momentum_mp_tma(const Params &p, double dt, cudaStream_t stream);
 bool momentum_tma_eligible(const Params &p);
 int momentum_tma_tiles(const Params &p);
-// the same ring for the mixed-precision face solve (vphys_mixed.cu)
-bool launch_momentum_mp_tma(const Params &p, double dt, cudaStream_t stream);
 // false when VPHYS_MOMENTUM_TMA=0 asks for the register-prefetched solves
 bool momentum_ring_enabled();
 // -sum of h over each column, accumulated k = 1..nz as vdiff's z_clear does (into p.zcol)

@@ -82,6 +82,8 @@ __host__ __device__ constexpr size_t mt_smem_bytes(int nz)
 // ring launch (false: the configuration or the buffers do not qualify), and
 // the persistent grid of a ring kernel.
 bool momentum_ring_prepare(const Params &p, MomMaps *maps, int *ntiles, cudaStream_t stream);
+// the tensor map of a level-major FP64 field [planes][n], boxes {box_x, box_y}
+bool tma_map_planes(CUtensorMap *m, const void *base, size_t n, int planes, int box_x, int box_y);
 int momentum_ring_grid(const void *kernel, int ntiles, size_t smem);
 
 template <class F>

@@ -355,6 +355,7 @@ __global__ void __launch_bounds__(32) k_tracers_redo(const Params p, double dt, 
         const int tix = (int)(ent & 31u);
         const unsigned g = ent >> 5;
         const int gi = (int)(g % (unsigned)ngx), j = (int)(g / (unsigned)ngx);
+        const int li = gi * 32 + (int)threadIdx.x;
         Params q = p;
         const vphys_config &c = p.cfg;
         q.ntr = 1;
@@ -363,12 +364,12 @@ __global__ void __launch_bounds__(32) k_tracers_redo(const Params p, double dt, 
         q.cfg.idx_salinity = (tix == c.idx_salinity) ? 0 : -1;
         q.cfg.idx_pseudo_salt = (tix == c.idx_pseudo_salt) ? 0 : -1;
         if (!p.ks_equals_kt && tix != c.idx_temperature) q.kt = p.ks;   // the second factorisation's tracers
-        tracer_columns<1, false, false>(q, dt, 1, nonlocal, gi * 32 + (int)threadIdx.x, j, smem, threadIdx.x, 32);
+        tracer_columns<1, false, false>(q, dt, 1, nonlocal, li, j, smem, threadIdx.x, 32);
         __syncwarp();
     }
 }
 
-void launch_tracers_redo(const Params &p, double dt, bool nonlocal, cudaStream_t stream)
+static void redo_attr()
 {
     static bool attr_set = false;
     if (!attr_set) {
@@ -376,10 +377,16 @@ void launch_tracers_redo(const Params &p, double dt, bool nonlocal, cudaStream_t
                              (int)((size_t)VPHYS_NZ_MAX * 32 * sizeof(double)));
         attr_set = true;
     }
+}
+
+void launch_tracers_redo(const Params &p, double dt, bool nonlocal, cudaStream_t stream)
+{
+    redo_attr();
     const int ngx = (p.nx + 31) / 32;
     const size_t smem = (size_t)p.nz * 32 * sizeof(double);
     k_tracers_redo<<<148 * 8, 32, smem, stream>>>(p, dt, nonlocal ? 1 : 0, ngx);
 }
+
 
 template <int NTR, bool TWO>
 static void launch_tracers_n(const Params &p, double dt, bool diffuse, bool nonlocal, cudaStream_t stream)

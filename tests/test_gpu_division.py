@@ -21,3 +21,4 @@ def test_division_helpers_match_ieee(emin, erange):
     _ffi.check(L.vphys_selftest_division(200_000_000, 20251203 + emin, emin, erange, ctypes.byref(bad)),
                "vphys_selftest_division")
     assert bad.value == 0
+

@@ -153,11 +153,13 @@ def test_large_increment_resolved_in_fp64(VP, oracle, case):
     errs = [maxabs(vp.get_tracer(t), st.tracers[t]) for t in range(ntr)]
     assert max(errs) <= TOL_TS, errs
     T = np.asarray(vp.get_tracer(1))
-    group_max = dT[:32].max(axis=(0, 2))          # columns 0..31 of each row j: one group
-    sure = np.flatnonzero(group_max > 2.2)
-    assert sure.size > 0
-    for j in sure:
-        assert_bitwise(f"T, re-solved group j={j}", T[:32, j], st.tracers[1][:32, j])
+    # a column whose own increment passes the bar lies in a re-solved group,
+    # whichever way the solve groups its columns
+    col_max = dT.max(axis=2)
+    sure = np.argwhere(col_max > 2.2)
+    assert sure.shape[0] > 0
+    for i, j in sure:
+        assert_bitwise(f"T, re-solved column ({i}, {j})", T[i, j], st.tracers[1][i, j])
     if cfg.budgets:
         want = st.heat_budget
         assert maxabs(vp.get("heat_budget"), want) <= 1e-6 * max(1.0, float(np.abs(want).max()))
