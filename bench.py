@@ -361,6 +361,10 @@ def main():
     if mixed and not args.no_compare and args.learned_cols > 0:
         forms["learned_kpp_mixed"] = learned_form(args, cols, ntr, nx, ny, nz, timed, cells, world)
 
+    # ---- the in-project autotuner picks the mixed solves' kernel variants on
+    #      this handle's state (the state is left as it was) ----
+    tune = vp.autotune(dt, reps=3) if mixed else None
+
     # ---- the timed region: K steps of the selected form; the clocks are
     #      sampled from a second before it to half a second after it, with
     #      untimed steps of the same form keeping the GPU loaded ----
@@ -372,7 +376,8 @@ def main():
     if mixed:
         forms["mixed"] = {"cells_per_s": value, "ms_per_step": ms / args.steps,
                           "fp64_resolved_groups_last_step": vp.mixed_redo_count(),
-                          "groups_per_step": ((nx + 31) // 32) * ny * ntr}
+                          "groups_per_step": ((nx + 31) // 32) * ny * ntr,
+                          "autotune_ms": tune}
         if "plain_fp64" in forms:
             forms["mixed_over_plain"] = round(value / forms["plain_fp64"]["cells_per_s"], 3)
 
@@ -676,6 +681,8 @@ def batched_form(args, dt):
         cfg.mixed_precision = level
         vp = VerticalPhysics(nx, ny, nz, ntr, cfg)
         vp.load_columns(cols)
+        if level:
+            out["mixed_autotune_ms"] = vp.autotune(dt, reps=2)
         vp.step_graph(dt, nsteps)                 # capture + the first 24 steps
         torch.cuda.synchronize()
         finals[name] = [np.asarray(vp.get_tracer(t)) for t in range(ntr)]

@@ -549,6 +549,28 @@ int vphys_nonlocal(vphys_handle h, double dt);
  * equals vphys_vdiff_tracers then vphys_nonlocal.  Asynchronous. */
 int vphys_vdiff_tracers_nonlocal(vphys_handle h, double dt);
 
+/* The in-project autotuner of the mixed-precision solves (no counterpart in
+ * the reference, whose solves have one form each).  Times every kernel
+ * variant of the mixed face solve and of the mixed tracer solve that the
+ * handle's configuration admits, on the handle's own state (after an EOS and
+ * an assembly, reps timed runs each after a warm-up, the state restored
+ * before every run), keeps the fastest of each for the handle's later steps,
+ * and restores the whole state (every field reads back as before the call).
+ * Variants: face solve 0 registers, 1 TMA-staged ring; tracer solve 0, 1, 2
+ * rows in shared memory with 1, 2 or 4 tracers per warp, 3 rows in tensor
+ * memory.  ms[0..1] receive the face-solve times and ms[2..5] the tracer
+ * times in milliseconds (-1: not admitted; ms may be NULL), chosen[0..1] the
+ * picks (may be NULL).  Needs device memory for a copy of the state while it
+ * runs.  Without mixed_precision it only reports the current picks.
+ * Synchronous. */
+int vphys_autotune(vphys_handle h, double dt, int reps, double *ms, int n_ms, int *chosen);
+
+/* Pins the kernel variants of the mixed solves (the numbering of
+ * vphys_autotune); a variant the configuration does not admit falls back to
+ * the register form (face solve) or one tracer per warp (tracer solve).  No
+ * counterpart in the reference. */
+int vphys_set_variants(vphys_handle h, int momentum, int tracers);
+
 /* n_steps of the whole chain (the body of vmix_apply_in_stage on a thermo
  * step, rdb_ocean_dyn.F90:1636-1900): [EOS] -> assemble -> momentum ->
  * tracers -> non-local, with the tracer solve and the non-local tendency

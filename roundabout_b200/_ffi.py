@@ -253,6 +253,9 @@ _PROTOTYPES = {
     "vphys_vdiff_tracers": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "vphys_nonlocal": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "vphys_vdiff_tracers_nonlocal": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    "vphys_set_variants": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "vphys_autotune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                      ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     "vphys_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]),
     "vphys_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
     "vphys_last_error": (ctypes.c_int, [ctypes.c_int, ctypes.c_char_p, ctypes.c_int]),

@@ -190,6 +190,31 @@ class VerticalPhysics:
         """The fused tracer diffusion + non-local launch that step() runs."""
         _ffi.check(self.lib.vphys_vdiff_tracers_nonlocal(self._h, float(dt)), "vphys_vdiff_tracers_nonlocal")
 
+    MOM_VARIANTS = ("registers", "tma_ring")
+    TRACER_VARIANTS = ("smem_1_per_warp", "smem_2_per_warp", "smem_4_per_warp", "tmem_rows")
+
+    def autotune(self, dt, reps=3):
+        """vphys_autotune: time the kernel variants of the mixed solves on
+        this handle's state, keep the fastest, leave the state unchanged.
+        Returns {"momentum": {variant: ms}, "tracers": {variant: ms},
+        "chosen": {"momentum": name, "tracers": name}} (ms only for the
+        variants the configuration admits)."""
+        import ctypes as C
+
+        ms = (C.c_double * 6)()
+        ch = (C.c_int * 2)()
+        _ffi.check(self.lib.vphys_autotune(self._h, float(dt), int(reps), ms, 6, ch), "vphys_autotune")
+        mom = {n: ms[i] for i, n in enumerate(self.MOM_VARIANTS) if ms[i] >= 0}
+        tr = {n: ms[2 + i] for i, n in enumerate(self.TRACER_VARIANTS) if ms[2 + i] >= 0}
+        return {"momentum": mom, "tracers": tr,
+                "chosen": {"momentum": self.MOM_VARIANTS[ch[0]], "tracers": self.TRACER_VARIANTS[ch[1]]}}
+
+    def set_variants(self, momentum, tracers):
+        """Pin the mixed solves' kernel variants (names of MOM_VARIANTS /
+        TRACER_VARIANTS)."""
+        _ffi.check(self.lib.vphys_set_variants(self._h, self.MOM_VARIANTS.index(momentum),
+                                               self.TRACER_VARIANTS.index(tracers)), "vphys_set_variants")
+
     def step(self, dt, n_steps=1):
         _ffi.check(self.lib.vphys_step(self._h, float(dt), int(n_steps)), "vphys_step")
 

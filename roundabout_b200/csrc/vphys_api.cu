@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/vphys.h"
+#include "vphys_device.cuh"
 #include "vphys_kernels.cuh"
 
 using vphys::Params;
@@ -76,6 +77,11 @@ struct vphys_handle_s {
     double *budget_scratch = nullptr;
     int *span = nullptr;              // live spans of the columns (mixed-precision tracer solve)
     unsigned *mp_redo = nullptr;      // the mixed tracer solve's FP64 re-solve list (count + entries)
+    unsigned *work_ctr = nullptr;     // the work counter of the dynamically scheduled mixed tracer solve
+    // kernel variants of the mixed solves (vphys_autotune); the defaults are
+    // the faster ones on 1440x1080x75 with 4 tracers
+    int var_mom = vphys::VAR_MOM_RING;
+    int var_tr = vphys::VAR_TR_SMEM1;
     double *zcol = nullptr;           // column depths for the momentum face thickness
     unsigned char *mom_tiles = nullptr;   // skip flags of the TMA-staged momentum solve's face tiles
     unsigned *dev_err = nullptr;      // bounded waits of the TMA-staged solves that ran out (0: none)
@@ -398,6 +404,9 @@ Params make_params(vphys_handle h)
     p.budget_scratch = h->budget_scratch;
     p.span = h->span;
     p.mp_redo = h->mp_redo;
+    p.work_ctr = h->work_ctr;
+    p.var_mom = h->var_mom;
+    p.var_tr = h->var_tr;
     p.zcol = h->zcol;
     p.mom_tile_skip = h->mom_tiles;
     p.dev_err = h->dev_err;
@@ -456,6 +465,16 @@ int prepare_tracers(vphys_handle h)
             h->span = nullptr;
             cudaGetLastError();
             return push_error(VPHYS_ERR_ALLOC, "cudaMalloc of the column spans failed");
+        }
+    }
+    if (h->cfg.mixed_precision && !h->work_ctr) {
+        cudaError_t e = cudaMalloc(&h->work_ctr, 4 * sizeof(unsigned));
+        if (e == cudaSuccess) e = cudaMemsetAsync(h->work_ctr, 0, 4 * sizeof(unsigned), h->stream);
+        if (e != cudaSuccess) {
+            if (h->work_ctr) cudaFree(h->work_ctr);
+            h->work_ctr = nullptr;
+            cudaGetLastError();
+            return push_error(VPHYS_ERR_ALLOC, "cudaMalloc of the work counter failed");
         }
     }
     if (h->cfg.mixed_precision && !h->mp_redo) {
@@ -953,6 +972,7 @@ int vphys_destroy(vphys_handle *hp)
     if (h->budget_scratch) cudaFree(h->budget_scratch);
     if (h->span) cudaFree(h->span);
     if (h->mp_redo) cudaFree(h->mp_redo);
+    if (h->work_ctr) cudaFree(h->work_ctr);
     if (h->zcol) cudaFree(h->zcol);
     if (h->mom_tiles) cudaFree(h->mom_tiles);
     if (h->dev_err) cudaFree(h->dev_err);
@@ -1263,6 +1283,114 @@ int vphys_vdiff_tracers_nonlocal(vphys_handle h, double dt)
     Params p = make_params(h);
     vphys::launch_tracers(p, dt, true, h->cfg.use_kpp && !h->cfg.epbl, h->stream);
     return cuda_status(cudaGetLastError(), "vphys_vdiff_tracers_nonlocal launch");
+}
+
+int vphys_set_variants(vphys_handle h, int momentum, int tracers)
+{
+    if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_set_variants: bad handle");
+    if (momentum < 0 || momentum >= vphys::N_VAR_MOM || tracers < 0 || tracers >= vphys::N_VAR_TR)
+        return push_error(VPHYS_ERR_CONFIG, "vphys_set_variants: momentum in [0, %d), tracers in [0, %d)",
+                          vphys::N_VAR_MOM, vphys::N_VAR_TR);
+    h->var_mom = momentum;
+    h->var_tr = tracers;
+    return VPHYS_OK;
+}
+
+int vphys_autotune(vphys_handle h, double dt, int reps, double *ms, int n_ms, int *chosen)
+{
+    if (!valid(h)) return push_error(VPHYS_ERR_BAD_HANDLE, "vphys_autotune: bad handle");
+    if (reps < 1 || reps > 100) return push_error(VPHYS_ERR_CONFIG, "vphys_autotune: reps must be in [1, 100]");
+    if (ms && n_ms > 0)
+        for (int i = 0; i < n_ms; ++i) ms[i] = -1.0;
+    if (!h->cfg.mixed_precision) {   // the exact solves have one form
+        if (chosen) chosen[0] = h->var_mom, chosen[1] = h->var_tr;
+        return VPHYS_OK;
+    }
+    int st;
+    if ((st = prepare_assemble(h)) || (st = prepare_momentum(h)) || (st = prepare_tracers(h))) return st;
+    // the handle's state, restored after the trials: every allocated real field
+    std::vector<std::pair<int, void *>> saved;
+    auto release = [&]() {
+        for (auto &s : saved) cudaFree(s.second);
+        saved.clear();
+    };
+    for (int id = 0; id < (int)h->f.size(); ++id) {
+        const Field &fl = h->f[id];
+        if (!fl.ptr() || fl.is_int) continue;
+        void *b = nullptr;
+        cudaError_t e = cudaMalloc(&b, fl.bytes());
+        if (e == cudaSuccess) e = cudaMemcpyAsync(b, fl.ptr(), fl.bytes(), cudaMemcpyDeviceToDevice, h->stream);
+        if (e != cudaSuccess) {
+            if (b) cudaFree(b);
+            cudaGetLastError();
+            release();
+            return push_error(VPHYS_ERR_ALLOC, "vphys_autotune: no room for a copy of the state (%s)",
+                              cudaGetErrorString(e));
+        }
+        saved.emplace_back(id, b);
+    }
+    auto restore = [&]() {
+        for (auto &s : saved)
+            cudaMemcpyAsync(h->f[s.first].ptr(), s.second, h->f[s.first].bytes(), cudaMemcpyDeviceToDevice, h->stream);
+    };
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    // the coefficients the solves read, as in a step
+    {
+        Params p = make_params(h);
+        if (h->cfg.eos_in_step) vphys::launch_eos_wright(p, h->stream);
+        if ((st = run_assemble(h, p))) {
+            release();
+            return st;
+        }
+    }
+    const bool kpp_nonlocal = h->cfg.use_kpp && !h->cfg.epbl;
+    auto trial = [&](auto launch) -> double {
+        float total = 0.0f;
+        for (int r = 0; r <= reps; ++r) {   // the first run is a warm-up
+            restore();
+            cudaEventRecord(e0, h->stream);
+            launch();
+            cudaEventRecord(e1, h->stream);
+            cudaEventSynchronize(e1);
+            float t = 0.0f;
+            cudaEventElapsedTime(&t, e0, e1);
+            if (r > 0) total += t;
+        }
+        return (double)total / reps;
+    };
+    double best_m = 1e30, best_t = 1e30;
+    int pick_m = h->var_mom, pick_t = h->var_tr;
+    for (int v = 0; v < vphys::N_VAR_MOM; ++v) {
+        Params p = make_params(h);
+        p.var_mom = v;
+        if (v == vphys::VAR_MOM_RING && !vphys::momentum_tma_eligible(p)) continue;
+        const double t = trial([&]() { vphys::launch_momentum(p, dt, h->stream); });
+        if (ms && v < n_ms) ms[v] = t;
+        if (t < best_m) best_m = t, pick_m = v;
+    }
+    for (int v = 0; v < vphys::N_VAR_TR && h->ntr > 0; ++v) {
+        Params p = make_params(h);
+        p.var_tr = v;
+        // variants other than one tracer per warp need one factorisation (ks = kt);
+        // the tensor-memory rows also need the default tracer knobs
+        if (v != vphys::VAR_TR_SMEM1 && !p.ks_equals_kt) continue;
+        if (v == vphys::VAR_TR_TMEM && !vphys::is_default_tracer_knobs(p.cfg)) continue;
+        const double t = trial([&]() { vphys::launch_tracers(p, dt, true, kpp_nonlocal, h->stream); });
+        if (ms && vphys::N_VAR_MOM + v < n_ms) ms[vphys::N_VAR_MOM + v] = t;
+        if (t < best_t) best_t = t, pick_t = v;
+    }
+    restore();
+    st = cuda_status(cudaStreamSynchronize(h->stream), "vphys_autotune");
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    release();
+    if (st) return st;
+    h->var_mom = pick_m;
+    h->var_tr = pick_t;
+    if (chosen) chosen[0] = pick_m, chosen[1] = pick_t;
+    return VPHYS_OK;
 }
 
 int vphys_step(vphys_handle h, double dt, int n_steps)

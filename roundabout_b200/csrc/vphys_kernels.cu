@@ -221,17 +221,26 @@ constexpr int ASM_THREADS = 128;
 // The assembly knobs of the default (benchmark) configuration: PP81, KPP
 // with constant buoyancy coefficients and no shortwave, Bryan-Lewis, no
 // KV_ML_INVZ2, convection or guard.
+// 1: the benchmark's knobs (PP81 + KPP + Bryan-Lewis, no other contributor,
+// guard or shortwave); 2: the same without KPP (the reference time of the
+// KPP stage); 0: anything else
+__host__ __device__ __forceinline__ int default_assembly_kind(const vphys_config &c)
+{
+    const bool rest = c.interior_closure == VPHYS_INTERIOR_PP81 && c.bkgnd_profile && !(c.kv_ml_invz2 > 0.0) &&
+                      !c.conv_enable && !c.vmix_guard && !c.buoyancy_coeffs && c.sw_pen_frac == 0.0 &&
+                      !c.kappa_shear && !c.epbl;
+    return rest ? (c.use_kpp ? 1 : 2) : 0;
+}
 __host__ __device__ __forceinline__ bool is_default_assembly_knobs(const vphys_config &c)
 {
-    return c.interior_closure == VPHYS_INTERIOR_PP81 && c.use_kpp && c.bkgnd_profile && !(c.kv_ml_invz2 > 0.0) &&
-           !c.conv_enable && !c.vmix_guard && !c.buoyancy_coeffs && c.sw_pen_frac == 0.0 && !c.kappa_shear && !c.epbl;
+    return default_assembly_kind(c) == 1;
 }
-__device__ __forceinline__ void default_assembly_knobs(vphys_config &c)
+__device__ __forceinline__ void default_assembly_knobs(vphys_config &c, int kind)
 {
     c.kappa_shear = 0;
     c.epbl = 0;
     c.interior_closure = VPHYS_INTERIOR_PP81;
-    c.use_kpp = 1;
+    c.use_kpp = (kind == 1) ? 1 : 0;
     c.bkgnd_profile = 1;
     c.kv_ml_invz2 = 0.0;
     c.conv_enable = 0;
@@ -240,7 +249,7 @@ __device__ __forceinline__ void default_assembly_knobs(vphys_config &c)
     c.sw_pen_frac = 0.0;
 }
 
-template <typename R, bool DEF>
+template <typename R, int DEF>
 __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -249,7 +258,7 @@ __global__ void __launch_bounds__(ASM_THREADS) k_assemble(const Params p)
     // DEF: the default assembly knobs (is_default_assembly_knobs) as
     // compile-time constants, so the other options' branches fold out
     vphys_config cd = p.cfg;
-    if (DEF) default_assembly_knobs(cd);
+    if (DEF) default_assembly_knobs(cd, DEF);
     const vphys_config &c = cd;
     const int nx = p.nx, nz = p.nz;
     const size_t P = p.plane, PU = p.plane_u, PV = p.plane_v;
@@ -978,17 +987,21 @@ void launch_stress_mag(const Params &p, cudaStream_t stream)
 void launch_assemble(const Params &p, cudaStream_t stream)
 {
     dim3 grid((p.nx + ASM_THREADS - 1) / ASM_THREADS, p.ny);
-    const bool def = is_default_assembly_knobs(p.cfg);
+    const int kind = default_assembly_kind(p.cfg);
     if (p.cfg.mixed_precision >= 2) {
-        if (def)
-            k_assemble<float, true><<<grid, ASM_THREADS, 0, stream>>>(p);
+        if (kind == 1)
+            k_assemble<float, 1><<<grid, ASM_THREADS, 0, stream>>>(p);
+        else if (kind == 2)
+            k_assemble<float, 2><<<grid, ASM_THREADS, 0, stream>>>(p);
         else
-            k_assemble<float, false><<<grid, ASM_THREADS, 0, stream>>>(p);
+            k_assemble<float, 0><<<grid, ASM_THREADS, 0, stream>>>(p);
     } else {
-        if (def)
-            k_assemble<double, true><<<grid, ASM_THREADS, 0, stream>>>(p);
+        if (kind == 1)
+            k_assemble<double, 1><<<grid, ASM_THREADS, 0, stream>>>(p);
+        else if (kind == 2)
+            k_assemble<double, 2><<<grid, ASM_THREADS, 0, stream>>>(p);
         else
-            k_assemble<double, false><<<grid, ASM_THREADS, 0, stream>>>(p);
+            k_assemble<double, 0><<<grid, ASM_THREADS, 0, stream>>>(p);
     }
 }
 
@@ -1029,18 +1042,6 @@ __global__ void k_column_depth(const Params p)
 void launch_column_depth(const Params &p, cudaStream_t stream)
 {
     k_column_depth<<<dim3((p.nx + 127) / 128, p.ny), 128, 0, stream>>>(p);
-}
-
-// VPHYS_MOMENTUM_TMA=0 runs the register-prefetched mixed face solve where
-// the TMA-staged ring applies (the switch is for comparing their speed).
-bool momentum_ring_enabled()
-{
-    static int on = -1;
-    if (on < 0) {
-        const char *e = getenv("VPHYS_MOMENTUM_TMA");
-        on = (e && atoi(e) == 0) ? 0 : 1;
-    }
-    return on == 1;
 }
 
 void launch_momentum(const Params &p, double dt, cudaStream_t stream)

@@ -10,6 +10,17 @@
 namespace vphys {
 
 constexpr int NZ_MAX = VPHYS_NZ_MAX + 1;   // per-column local arrays (>= nz + 1)
+
+// Kernel variants of the mixed-precision solves that vphys_autotune chooses
+// between (the same results up to FP32 rounding order; each applies where
+// its eligibility test passes, the register forms everywhere).
+constexpr int VAR_MOM_REGISTER = 0;   // k_momentum_mp: loads prefetched in registers
+constexpr int VAR_MOM_RING = 1;       // k_momentum_mp_tma: TMA-staged ring (vphys_mom_ring.cuh)
+constexpr int VAR_TR_SMEM1 = 0;       // k_tracers_mp, rows in shared memory, one tracer per warp
+constexpr int VAR_TR_SMEM2 = 1;       // the same, two tracers per warp (one factorisation)
+constexpr int VAR_TR_SMEM4 = 2;       // the same, four tracers per warp
+constexpr int VAR_TR_TMEM = 3;        // k_tracers_mp_tm, rows in tensor memory
+constexpr int N_VAR_MOM = 2, N_VAR_TR = 4;
 constexpr int NTR_MAX = 16;                // tracers a handle may carry
 
 // learned KPP surrogate: 75 feature levels below the surface layer,
@@ -50,6 +61,9 @@ struct Params {
     unsigned long long *guard_count;  // vmix_guard counter (device)
     int *span;                        // per column: first | last live layer << 16 (0: none), scratch
     unsigned *mp_redo;                // mixed solves: count, then (group << 5 | tracer) re-solved in FP64
+    unsigned *work_ctr;               // next work item of a dynamically scheduled solve (reset by k_spans)
+    int var_mom;                      // mixed face solve: VAR_MOM_REGISTER or VAR_MOM_RING (where eligible)
+    int var_tr;                       // mixed tracer solve: VAR_TR_* (where eligible)
     double *zcol;                     // per column: -sum_k h, k = 1..nz in order (momentum z_clear), scratch
     unsigned char *mom_tile_skip;     // per face tile of the TMA-staged momentum solve: 1 = nothing to solve
     unsigned *dev_err;                // bounded waits that ran out (bit 0: consumer, 1: producer, 2: drain)
@@ -95,8 +109,7 @@ void launch_momentum(const Params &p, double dt, cudaStream_t stream);
 bool launch_momentum_mp_tma(const Params &p, double dt, cudaStream_t stream);
 bool momentum_tma_eligible(const Params &p);
 int momentum_tma_tiles(const Params &p);
-// false when VPHYS_MOMENTUM_TMA=0 asks for the register-prefetched solves
-bool momentum_ring_enabled();
+
 // -sum of h over each column, accumulated k = 1..nz as vdiff's z_clear does (into p.zcol)
 void launch_column_depth(const Params &p, cudaStream_t stream);
 void launch_tracers(const Params &p, double dt, bool diffuse, bool nonlocal, cudaStream_t stream);

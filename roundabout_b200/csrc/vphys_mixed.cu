@@ -128,7 +128,10 @@ __global__ void k_spans(const Params p)
         }
     }
     p.span[col] = lo | (hi << 16);
-    if (p.mp_redo && col == 0) p.mp_redo[0] = 0;   // the re-solve list of the tracer kernel that follows
+    if (col == 0) {
+        if (p.mp_redo) p.mp_redo[0] = 0;     // the re-solve list of the tracer kernel that follows
+        if (p.work_ctr) p.work_ctr[0] = 0;   // and its work counter
+    }
 }
 
 // Back-substitution of one tracer column from the t and v rows; with FULL the
@@ -421,6 +424,349 @@ __global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, doubl
             tracer_back<false>(p, dt, t_ptr, hp, tu, vq, w_lo, w_hi, lo, hi, nullptr, false, false, 0.0, 0.0,
                                pol_once);
     }
+}
+
+// ---------------------------------------------------------------------------
+// Tracers with the solver rows in tensor memory.
+//
+// k_tracers_mp holds the t and v rows of a warp's 32 columns in shared
+// memory: 8 B per level and column, 19.2 KB per warp at nz = 75, which caps
+// it at ~11 warps per SM, and its per-level chains run at the pace of the
+// warps in flight (halving them doubled its time).  The 256 KB of tensor
+// memory of an SM are free on this path, so k_tracers_mp_tm keeps one
+// persistent CTA per SM whose first warps store their rows in tensor memory
+// (tcgen05.st of each level's (t, v) pair into the warp's 32 lanes, read
+// back eight levels at a time with tcgen05.ld; up to three warps per lane
+// quarter, 2 * nzp columns each) and whose other warps keep them in shared
+// memory: about twice the warps per SM.  The arithmetic is
+// k_tracers_mp<false, 1, true>'s, level for level (the default knobs, one
+// factorisation, one tracer per warp); work items are (32-column group,
+// tracer), tracer fastest, strided over all warps of the grid.
+// ---------------------------------------------------------------------------
+constexpr int TM_MAX_WARPS = 24;
+
+// rows of one warp in shared memory: level k at tu[(k-1)*32], vv[(k-1)*32]
+struct SRows {
+    float *tu, *vv;
+    int nz;   // rows above nz do not exist (the last block of a column may be partial)
+    __device__ __forceinline__ void put(int k, float t, float v)
+    {
+        tu[(size_t)(k - 1) * MP_TR_COLS] = t;
+        vv[(size_t)(k - 1) * MP_TR_COLS] = v;
+    }
+    __device__ __forceinline__ void done_writing() {}
+    // levels 8 kb + 1 .. 8 kb + 8
+    __device__ __forceinline__ void load8(int kb, float (&t)[8], float (&v)[8]) const
+    {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int k = 8 * kb + q + 1;
+            t[q] = (k <= nz) ? tu[(size_t)(k - 1) * MP_TR_COLS] : 0.0f;
+            v[q] = (k <= nz) ? vv[(size_t)(k - 1) * MP_TR_COLS] : 0.0f;
+        }
+    }
+};
+
+// rows of one warp in tensor memory: level k's (t, v) at columns
+// col0 + 2(k-1), 2(k-1)+1 of the warp's 32 lanes (taddr: lane << 16 | column)
+struct TRows {
+    uint32_t base;
+    __device__ __forceinline__ void put(int k, float t, float v)
+    {
+        __syncwarp();
+        asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1, %2};" ::"r"(base + 2u * (uint32_t)(k - 1)),
+                     "r"(__float_as_uint(t)), "r"(__float_as_uint(v))
+                     : "memory");
+    }
+    __device__ __forceinline__ void done_writing()
+    {
+        __syncwarp();
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+    }
+    __device__ __forceinline__ void load8(int kb, float (&t)[8], float (&v)[8]) const
+    {
+        uint32_t r[16];
+        __syncwarp();
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            : "r"(base + 16u * (uint32_t)kb));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            t[q] = __uint_as_float(r[2 * q]);
+            v[q] = __uint_as_float(r[2 * q + 1]);
+        }
+    }
+};
+
+// The back-substitution of one tracer column from the rows (tracer_back's
+// arithmetic, its levels taken in aligned blocks of eight so that a row
+// block is one tensor-memory load); FULL adds the KPP non-local deposit.
+template <bool FULL, class Rows>
+__device__ __forceinline__ void tracer_back_rows(const Params &p, double dt, double *__restrict__ trc,
+                                                 const double *__restrict__ hp, const Rows &rows, int w_lo, int w_hi,
+                                                 int lo, int hi, bool nl, double h_b, double q_kin,
+                                                 unsigned long long pol)
+{
+    const size_t P = p.plane;
+    const int nz = p.nz;
+    float delta = 0.0f;
+    double g_above = 0.0, d_run = 0.0, h_a = 0.0;
+    double h_c = (FULL && lo <= hi) ? __ldg(hp + P * (size_t)(hi - 1)) : 0.0;
+    for (int kb = (w_hi - 1) >> 3; kb >= ((w_lo - 1) >> 3); --kb) {
+        float t8[8], v8[8];
+        rows.load8(kb, t8, v8);
+        double dk[8];
+#pragma unroll
+        for (int q = 7; q >= 0; --q) {
+            const int k = 8 * kb + q + 1;
+            dk[q] = (k >= lo && k <= hi) ? ld_hint(trc + P * (size_t)(k - 1), pol) : 0.0;
+        }
+#pragma unroll
+        for (int q = 7; q >= 0; --q) {
+            const int k = 8 * kb + q + 1;
+            if (k > w_hi || k < w_lo) continue;
+            delta = v8[q] + mul_u(t8[q], delta);   // rows outside the span: v = t = 0
+            if (k < lo || k > hi) continue;
+            const size_t off = P * (size_t)(k - 1);
+            double x = dk[q] + (double)delta;
+            if (FULL) {
+                const double h_bl = (k > 1) ? __ldg(hp + off - P) : 0.0;
+                double gk = 0.0;
+                if (nl) {
+                    d_run = d_run + h_c;
+                    if (k > 1 && d_run < h_b) {
+                        const double sigma = xdiv(d_run, h_b);
+                        gk = p.cfg.cs_nonlocal * (sigma * (1.0 - sigma) * (1.0 - sigma)) * q_kin;
+                    }
+                }
+                double f_up = 0.0, f_dn = 0.0;
+                if (k < nz) f_up = nonlocal_face_flux(g_above, h_c, h_a);
+                if (k > 1) f_dn = nonlocal_face_flux(gk, h_bl, h_c);
+                x = conc_add_source(x, h_c, dt * (f_up - f_dn));
+                g_above = gk;
+                h_a = h_c;
+                h_c = h_bl;
+            }
+            trc[off] = x;
+        }
+    }
+}
+
+// One work item (32-column group g, tracer tr) of k_tracers_mp_tm.
+template <class Rows>
+__device__ __forceinline__ void tracer_item_tm(const Params &p, const vphys_config &c, double dt, int nonlocal,
+                                               int ngx, int item, Rows &rows, int lane)
+{
+    const int ntr = p.ntr, nx = p.nx, nz = p.nz;
+    const int tr = item % ntr;
+    const unsigned g = (unsigned)(item / ntr);
+    const int gi = (int)(g % (unsigned)ngx), j = (int)(g / (unsigned)ngx);
+    const int i = gi * MP_TR_COLS + lane;
+    const size_t P = p.plane;
+    const bool in_grid = i < nx;
+    const size_t col = (size_t)(in_grid ? i : 0) + (size_t)nx * j;
+    const double *__restrict__ hp = p.h + col;
+    const float HV = (float)H_VANISHED;
+    constexpr int U = MP_TR_U;
+
+    const int sp = in_grid ? p.span[col] : 0;
+    const bool live = (sp & 0xffff) > 0;
+    const int lo = live ? (sp & 0xffff) : nz + 1, hi = live ? (sp >> 16) : 0;
+    const int w_lo = __reduce_min_sync(0xffffffffu, live ? lo : 0x7fffffff);
+    const int w_hi = __reduce_max_sync(0xffffffffu, hi);
+    if (w_hi == 0) return;
+
+    const double *__restrict__ Kp = p.kt + col;
+    double *trc = p.tr[tr] + col;
+    const unsigned long long pol_keep = l2_policy_evict_last();
+    const float dtf = (float)dt;
+    float vsum = 0.0f;
+    {
+        const bool first = (w_lo == lo);
+        double h_c = first ? __ldg(hp + P * (size_t)(w_lo - 1)) : 0.0;
+        double d_c = first ? ld_hint(trc + P * (size_t)(w_lo - 1), pol_keep) : 0.0;
+        double d_m = 0.0, w = 0.0;
+        float f_dn = 0.0f, q_prev = 1.0f, t_prev = 0.0f;
+        for (int k0 = w_lo; k0 <= w_hi; k0 += U) {
+            double hn[U], kn[U], dn[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int k = k0 + u;
+                const bool need = k + 1 >= lo && k + 1 <= hi;
+                const size_t o = P * (size_t)k;
+                hn[u] = need ? __ldg(hp + o) : 0.0;
+                kn[u] = need ? __ldg(Kp + o) : 0.0;
+                dn[u] = need ? ld_hint(trc + o, pol_keep) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int k = k0 + u;
+                if (k > w_hi) break;
+                const float H = fmx((float)h_c, HV);
+                const float Hp = fmx((float)hn[u], HV);
+                const bool coupled = h_c > H_VANISHED && hn[u] > H_VANISHED;
+                const float f_up = coupled ? __fdividef(dtf * (float)kn[u], face_thick(H, Hp, c.use_harmonic)) : 0.0f;
+                float ip, t, qq;
+                pivot_row(H + f_dn * q_prev, f_up, ip, t, qq);
+                const double fd = (double)f_dn, fu = (double)f_up, ipd = (double)ip;
+                const double b = fd * (d_m - d_c) + fu * (dn[u] - d_c);
+                w = b + mul_u(t_prev, w);
+                const float vq = (float)(w * ipd);
+                rows.put(k, t, vq);
+                vsum += fabsf(vq);
+                d_m = d_c;
+                d_c = dn[u];
+                t_prev = t;
+                q_prev = qq;
+                f_dn = f_up;
+                h_c = hn[u];
+            }
+        }
+    }
+    rows.done_writing();
+
+    // a group whose increment reaches MP_DELTA_MAX goes to the FP64 re-solve
+    if (p.mp_redo && __any_sync(0xffffffffu, vsum > MP_DELTA_MAX)) {
+        float dmax = 0.0f, delta = 0.0f;
+        for (int kb = (w_hi - 1) >> 3; kb >= ((w_lo - 1) >> 3); --kb) {
+            float t8[8], v8[8];
+            rows.load8(kb, t8, v8);
+#pragma unroll
+            for (int q = 7; q >= 0; --q) {
+                const int k = 8 * kb + q + 1;
+                if (k > w_hi || k < w_lo) continue;
+                delta = v8[q] + mul_u(t8[q], delta);
+                dmax = fmaxf(dmax, fabsf(delta));
+            }
+        }
+        if (__any_sync(0xffffffffu, dmax > MP_DELTA_MAX)) {
+            if (lane == 0) {
+                const unsigned base = atomicAdd(p.mp_redo, 1u);
+                p.mp_redo[1 + base] = (g << 5) | (unsigned)tr;
+            }
+            return;
+        }
+    }
+
+    const unsigned long long pol_once = l2_policy_evict_first();
+    const int iT = c.idx_temperature, iS = c.idx_salinity, iPS = c.idx_pseudo_salt;
+    const bool full_t = nonlocal && c.use_kpp && (tr == iT || tr == iS || tr == iPS);
+    if (!full_t) {
+        tracer_back_rows<false>(p, dt, trc, hp, rows, w_lo, w_hi, lo, hi, false, 0.0, 0.0, pol_once);
+        return;
+    }
+    bool nl = live;
+    double h_b = 0.0, q_kin = 0.0;
+    if (nl) {
+        const double rho0 = c.rho0;
+        h_b = p.bl_depth[col];
+        const double u_star = sqrt(xdiv(p.stress_mag[col], rho0));
+        const double q_T_kin = kpp_q_t_kin(c, p.q_heat[col], p.sw_src + col, p.sw_kappa, col, p.plane, h_b,
+                                           __ldg(hp + P * (size_t)(hi - 1)));
+        const double q_S_kin = xdiv(p.q_salt[col], rho0);
+        const double B_0 = (GRAVITY / rho0) * (c.alpha_T * q_T_kin - c.beta_S * q_S_kin);
+        const double wstar3 = fmx(0.0, -B_0) * h_b;
+        const double w_star = sm_cbrt(wstar3);
+        const double w_s = sqrt(u_star * u_star + w_star * w_star);
+        nl = (h_b > 0.0 && w_s > 0.0 && B_0 < 0.0);
+        q_kin = (tr == iT) ? q_T_kin : q_S_kin;
+    }
+    tracer_back_rows<true>(p, dt, trc, hp, rows, w_lo, w_hi, lo, hi, nl, h_b, q_kin, pol_once);
+}
+
+// One CTA per SM: warps [0, nt_warps) keep their rows in tensor memory
+// (lane quarter warp % 4, columns (warp / 4) * 2 nzp), the others in
+// shared memory.  Warp 0 allocates all 512 columns before the work and frees
+// them after it.
+template <int MAXW>
+__global__ void __launch_bounds__(32 * MAXW, 1)
+    k_tracers_mp_tm(const Params p, double dt, int nonlocal, int ngx, int nitems, int nt_warps, int nzp)
+{
+    extern __shared__ __align__(16) float smf[];
+    __shared__ uint32_t tmem_slot;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nwarps = blockDim.x >> 5;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(
+                         (uint32_t)__cvta_generic_to_shared(&tmem_slot))
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tbase = tmem_slot;
+    vphys_config cd = p.cfg;
+    default_tracer_knobs(cd);
+    // items are handed out one at a time in order (a warp that drew land
+    // columns draws again at once), so neighbouring items -- the tracers of
+    // one column group -- run at about the same time and share h and K in L2
+    auto next = [&]() {
+        unsigned it = 0;
+        if (lane == 0) it = atomicAdd(p.work_ctr, 1u);
+        return (int)__shfl_sync(0xffffffffu, it, 0);
+    };
+    if (warp < nt_warps) {
+        TRows rows{tbase + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)((warp >> 2) * 2 * nzp)};
+        for (int item = next(); item < nitems; item = next()) tracer_item_tm(p, cd, dt, nonlocal, ngx, item, rows, lane);
+    } else {
+        const size_t NB = (size_t)p.nz * MP_TR_COLS;
+        float *tu = smf + (size_t)(warp - nt_warps) * 2 * NB + lane;
+        SRows rows{tu, tu + NB, p.nz};
+        for (int item = next(); item < nitems; item = next()) tracer_item_tm(p, cd, dt, nonlocal, ngx, item, rows, lane);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tbase) : "memory");
+    }
+}
+
+// The tensor-memory form applies to the default tracer knobs with ks = kt;
+// false: the caller runs k_tracers_mp.
+static bool launch_tracers_mp_tm(const Params &p, double dt, bool nonlocal, cudaStream_t stream)
+{
+    if (p.var_tr != VAR_TR_TMEM || !is_default_tracer_knobs(p.cfg) || !p.ks_equals_kt || p.ntr < 1 || !p.span ||
+        !p.work_ctr)
+        return false;
+    const int nzp = (p.nz + 7) & ~7;          // levels rounded to a row block
+    const int per_quarter = 512 / (2 * nzp);  // warps sharing one lane quarter
+    int nt = 4 * (per_quarter < 3 ? per_quarter : 3);
+    const size_t per_s = (size_t)p.nz * MP_TR_COLS * 2 * sizeof(float);
+    // Rows in tensor memory only: shared-memory rows squeeze the L1 that the
+    // tracers of a column group share for h and K (1440x1080x75, 4 tracers:
+    // 12 tensor-memory warps 3.9-4.2 ms; 12 of them + 11 shared-memory warps
+    // 6.05 ms; 11 shared-memory warps in the same kernel 4.65 ms).
+    const int ns = 0;
+    if (nt + ns < 1) return false;
+    static bool attr_set = false;
+    static int sms = 0;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_tracers_mp_tm<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+        cudaFuncSetAttribute(k_tracers_mp_tm<TM_MAX_WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+        attr_set = true;
+    }
+    const int ngx = (p.nx + MP_TR_COLS - 1) / MP_TR_COLS;
+    const long long nitems = (long long)ngx * p.ny * p.ntr;
+    if (nitems > 0x7fffffffLL) return false;
+    const int nwarps = nt + ns;
+    const int grid = (int)(nitems < (long long)sms * nwarps ? (nitems + nwarps - 1) / nwarps : sms);
+    if (nwarps <= 12)
+        k_tracers_mp_tm<12><<<grid, 32 * nwarps, (size_t)ns * per_s, stream>>>(p, dt, nonlocal ? 1 : 0, ngx,
+                                                                             (int)nitems, nt, nzp);
+    else
+        k_tracers_mp_tm<TM_MAX_WARPS><<<grid, 32 * nwarps, (size_t)ns * per_s, stream>>>(p, dt, nonlocal ? 1 : 0, ngx,
+                                                                                       (int)nitems, nt, nzp);
+    if (p.mp_redo) launch_tracers_redo(p, dt, nonlocal, stream);
+    return true;
 }
 
 // ---------------------------------------------------------------------------
@@ -786,39 +1132,27 @@ static void launch_tracers_mp_t(const Params &p, double dt, bool nonlocal, cudaS
     if (p.mp_redo) launch_tracers_redo(p, dt, nonlocal, stream);
 }
 
-// Tracers per warp: VPHYS_MP_TRACERS_PER_WARP (1, 2 or 4) when set, else 1
-// (measured on 1440x1080x75: sharing a warp saves the repeated factorisation
-// but the larger register and shared-memory footprint costs more warps per
-// SM than it gains).  A separate ks keeps one per warp.
-static int tracers_per_warp(int ntr)
-{
-    static int forced = -1;
-    if (forced < 0) {
-        const char *e = getenv("VPHYS_MP_TRACERS_PER_WARP");
-        forced = e ? atoi(e) : 0;
-        if (forced != 1 && forced != 2 && forced != 4) forced = 0;
-    }
-    (void)ntr;
-    return forced ? forced : 1;
-}
-
 void launch_tracers_mp(const Params &p, double dt, bool nonlocal, cudaStream_t stream)
 {
     k_spans<<<dim3((p.nx + 127) / 128, p.ny), 128, 0, stream>>>(p);
+    if (launch_tracers_mp_tm(p, dt, nonlocal, stream)) return;
     if (!p.ks_equals_kt) {
         launch_tracers_mp_t<true, 1>(p, dt, nonlocal, stream);
         return;
     }
-    switch (tracers_per_warp(p.ntr)) {
-    case 4: launch_tracers_mp_t<false, 4>(p, dt, nonlocal, stream); break;
-    case 2: launch_tracers_mp_t<false, 2>(p, dt, nonlocal, stream); break;
+    // tracers per warp (the variant vphys_autotune chose; a separate ks keeps
+    // one per warp): sharing a warp saves the repeated factorisation, at the
+    // price of a larger register and shared-memory footprint per warp
+    switch (p.var_tr) {
+    case VAR_TR_SMEM4: launch_tracers_mp_t<false, 4>(p, dt, nonlocal, stream); break;
+    case VAR_TR_SMEM2: launch_tracers_mp_t<false, 2>(p, dt, nonlocal, stream); break;
     default: launch_tracers_mp_t<false, 1>(p, dt, nonlocal, stream); break;
     }
 }
 
 void launch_momentum_mp(const Params &p, double dt, cudaStream_t stream)
 {
-    if (momentum_ring_enabled() && launch_momentum_mp_tma(p, dt, stream)) return;
+    if (p.var_mom == VAR_MOM_RING && launch_momentum_mp_tma(p, dt, stream)) return;
     const int bs = MP_MOM_THREADS;
     static bool attr_set = false;
     if (!attr_set) {
