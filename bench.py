@@ -507,6 +507,30 @@ def main():
                        "take alternate steps so one's download overlaps the other's upload (serial: one handle, "
                        "synchronous vphys_set_field / vphys_get_field)"}
 
+    # ---- conservation of the selected form, stated against the compensated
+    #      FP64 column contents (cfg.column_integrals) over one step from the
+    #      benchmark's state ----
+    if not args.no_compare:
+        ci_cfg = hot_path_config(ntracers=ntr)
+        ci_cfg.mixed_precision = args.mixed_level if mixed else 0
+        ci_cfg.column_integrals = 1
+        vp.set_config(ci_cfg)
+        vp.load_columns(cols)
+        vp.step(dt, 1)
+        old, new = np.asarray(vp.get("content_old")), np.asarray(vp.get("content_new"))
+        inc = np.zeros_like(old)
+        for t in range(ntr):
+            inc[:, :, t] = (np.abs(np.asarray(vp.get_tracer(t)) - cols.tracers[t]) * cols.h).sum(axis=2)
+        live = np.abs(old) > 0
+        forms["column_content_1step"] = {
+            "form": args.form, "max_rel_drift": float((np.abs(new - old)[live] / np.abs(old[live])).max()),
+            "max_drift_over_sum_h_abs_increment": float(
+                (np.abs(new - old)[live] / np.maximum(inc[live], 1e-300)).max()),
+            "how": "Neumaier-compensated FP64 sum_k h c over each column's live span before and after the "
+                   "tracer solve (with the fused non-local deposit), per column and tracer"}
+        cfg.column_integrals = 0
+        vp.set_config(cfg)
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_run(args.config, args.cpu_sample, 2, 1)

@@ -311,6 +311,13 @@ typedef struct vphys_config {
      * shelf (apply_sw_penetration_cover_impl / _nb_cover_impl,
      * rdb_ocean_surface_flux.F90:1532-1604, 1670-1730) */
     int use_cover_frac;       /* 0 */
+    /* 1: the tracer diffusion writes, per column and tracer, the content
+     * sum_k h_k c_k over the column's live span before the solve (terms
+     * added bottom-up) and after it (with the fused non-local deposit; terms
+     * added top-down), each an FP64 Neumaier-compensated sum, into the
+     * CONTENT_OLD / CONTENT_NEW fields.  No counterpart in the reference: a
+     * conservation diagnostic (the exact solve keeps it to FP64 round-off) */
+    int column_integrals;     /* 0 */
 } vphys_config;
 
 #define VPHYS_KPP_SW_ALL 1
@@ -373,6 +380,9 @@ enum vphys_field {
                                    sw_nbands planes read (sw_chl = 1; filled with 1) */
     VPHYS_FIELD_COVER_FRAC = 45, /* in     (nx, ny) ice-shelf cover fraction in [0, 1] (use_cover_frac = 1;
                                    filled with 0) */
+    VPHYS_FIELD_CONTENT_OLD = 46, /* out   (nx, ny, ntracer) compensated column content before the diffusion
+                                   (column_integrals = 1) */
+    VPHYS_FIELD_CONTENT_NEW = 47, /* out   (nx, ny, ntracer) the same after it */
     VPHYS_FIELD_TRACER0 = 64    /* in/out  (nx, ny, nz); tracer t is
                                    VPHYS_FIELD_TRACER0 + t */
 };

@@ -81,6 +81,7 @@ def lib():
             getattr(L, name).argtypes = [ctypes.c_void_p, ctypes.POINTER(VpoState)]
             getattr(L, name).restype = None
         L.vpo_stress_mag.argtypes = [ctypes.POINTER(VpoState)]
+        L.vpo_column_content.argtypes = [ctypes.POINTER(VpoState), ctypes.c_int, _dp]
         for name in ("vpo_assemble_gate", "vpo_build_coefficients"):
             getattr(L, name).argtypes = [ctypes.c_void_p, ctypes.POINTER(VpoState)]
             getattr(L, name).restype = ctypes.c_int
@@ -190,6 +191,15 @@ class OracleState:
     def stress_mag_from_tau(self):
         s = self._struct()
         lib().vpo_stress_mag(ctypes.byref(s))
+
+    def column_content(self, descending: bool) -> np.ndarray:
+        """Compensated sum_k h c over each column's live span, per tracer:
+        shape (nx, ny, ntr), Fortran order; the terms added top-down when
+        `descending`."""
+        out = np.zeros((self.nx, self.ny, max(1, self.ntr)), order="F")
+        s = self._struct()
+        lib().vpo_column_content(ctypes.byref(s), int(descending), out.ctypes.data_as(_dp))
+        return out[:, :, : self.ntr]
 
     def copy(self) -> "OracleState":
         o = OracleState.__new__(OracleState)

@@ -1467,3 +1467,52 @@ int vpo_step(const vphys_config *c, vpo_state *s, double dt, int n_steps)
     }
     return st;
 }
+
+/* =====================================================================
+ * Compensated column content (the diagnostic of cfg.column_integrals)
+ * ===================================================================== */
+/* Neumaier's improvement of Kahan summation (Z. Angew. Math. Mech. 54, 1974):
+ * the rounding error of every addition is carried in *cmp, whichever of the
+ * two operands is larger. */
+static inline void neumaier_add(double *sum, double *cmp, double x)
+{
+    const double t = *sum + x;
+    if (fabs(*sum) >= fabs(x))
+        *cmp += (*sum - t) + x;
+    else
+        *cmp += (x - t) + *sum;
+    *sum = t;
+}
+
+void vpo_column_content(const vpo_state *s, int descending, double *out)
+{
+    const int nx = s->nx, ny = s->ny, nz = s->nz;
+    const size_t plane = (size_t)nx * ny;
+#pragma omp parallel for
+    for (int j = 1; j <= ny; ++j)
+        for (int i = 1; i <= nx; ++i) {
+            int lo = 0, hi = 0;
+            for (int k = 1; k <= nz; ++k)
+                if (C3(s->h, i, j, k) > H_VANISHED) {
+                    lo = k;
+                    break;
+                }
+            if (lo > 0)
+                for (int k = nz; k >= lo; --k)
+                    if (C3(s->h, i, j, k) > H_VANISHED) {
+                        hi = k;
+                        break;
+                    }
+            const size_t col = (size_t)(i - 1) + (size_t)nx * (j - 1);
+            for (int t = 0; t < s->ntr; ++t) {
+                double sum = 0.0, cmp = 0.0;
+                if (lo > 0) {
+                    for (int n = 0; n <= hi - lo; ++n) {
+                        const int k = descending ? hi - n : lo + n;
+                        neumaier_add(&sum, &cmp, C3(s->h, i, j, k) * C3(s->tr[t], i, j, k));
+                    }
+                }
+                out[(size_t)t * plane + col] = sum + cmp;
+            }
+        }
+}

@@ -115,6 +115,12 @@ double vpo_epbl_lt_enhance(const vphys_config *c, double la, double b0, double u
 
 int vpo_step(const vphys_config *c, vpo_state *s, double dt, int n_steps);
 
+/* Compensated (Neumaier) FP64 content sum_k h_k c_k of every column and
+ * tracer over the column's live span (first live layer from the bed to the
+ * first from the surface; 0 without one), the terms added bottom-up
+ * (descending = 0) or top-down (descending = 1); out[t * nx * ny + col]. */
+void vpo_column_content(const vpo_state *s, int descending, double *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -76,6 +76,8 @@ FIELD_WET_DYN = 42
 FIELD_SW_CHL = 43
 FIELD_SW_KAPPA = 44
 FIELD_COVER_FRAC = 45
+FIELD_CONTENT_OLD = 46
+FIELD_CONTENT_NEW = 47
 SW_NB_MAX = 6
 FIELD_TRACER0 = 64
 
@@ -92,13 +94,16 @@ FIELD_NAMES = {
     "kd_shear": FIELD_KD_SHEAR, "tke_shear": FIELD_TKE_SHEAR, "kd_epbl": FIELD_KD_EPBL, "mld_epbl": FIELD_MLD_EPBL,
     "la_epbl": FIELD_LA_EPBL, "sw_net": FIELD_SW_NET, "wet_dyn": FIELD_WET_DYN, "sw_chl": FIELD_SW_CHL,
     "sw_kappa": FIELD_SW_KAPPA, "cover_frac": FIELD_COVER_FRAC,
+    "content_old": FIELD_CONTENT_OLD, "content_new": FIELD_CONTENT_NEW,
     **{f"epbl_tke_{k}": v for k, v in FIELD_EPBL_TKE.items()},
 }
 INT_FIELDS = (FIELD_K_TOP_U, FIELD_K_TOP_V, FIELD_K_BOT_U, FIELD_K_BOT_V)
 
 
-def field_shape(field: int, nx: int, ny: int, nz: int):
-    """Fortran-order shape of a field (matches vphys_field_shape in C)."""
+def field_shape(field: int, nx: int, ny: int, nz: int, ntr: int = 1):
+    """Fortran-order shape of a field (matches the counts of vphys_create)."""
+    if field in (FIELD_CONTENT_OLD, FIELD_CONTENT_NEW):
+        return (nx, ny, max(1, ntr))
     if field >= FIELD_TRACER0 or field in (FIELD_H, FIELD_RHO, FIELD_HEAT_BUDGET, FIELD_SALT_BUDGET,
                                            FIELD_HEAT_BUDGET_SURFACE, FIELD_SALT_BUDGET_SURFACE):
         return (nx, ny, nz)
@@ -174,7 +179,8 @@ class VphysConfig(ctypes.Structure):
         ("min_salinity", ctypes.c_double), ("epbl_sw_ctke", ctypes.c_int),
         ("sw_chl", ctypes.c_int), ("sw_nbands", ctypes.c_int), ("sw_blue_frac", ctypes.c_double),
         ("sw_opacity_coef", ctypes.c_double * (2 * SW_NB_MAX)), ("sw_chl_power", ctypes.c_double * SW_NB_MAX),
-        ("sw_opacity_land", ctypes.c_double), ("use_cover_frac", ctypes.c_int)]
+        ("sw_opacity_land", ctypes.c_double), ("use_cover_frac", ctypes.c_int),
+        ("column_integrals", ctypes.c_int)]
 
     def as_dict(self):
         out = {}

@@ -76,7 +76,7 @@ class VerticalPhysics:
         return _ffi.FIELD_NAMES[name]
 
     def shape(self, name):
-        return _ffi.field_shape(self._fid(name), self.nx, self.ny, self.nz)
+        return _ffi.field_shape(self._fid(name), self.nx, self.ny, self.nz, self.ntr)
 
     def set(self, name, array):
         fid = self._fid(name)

@@ -169,6 +169,7 @@ def default_config() -> VphysConfig:
     c.sw_chl_power[1] = 0.629
     c.sw_opacity_land = 10.0
     c.use_cover_frac = 0
+    c.column_integrals = 0
     return c
 
 

@@ -51,7 +51,7 @@ int cuda_status(cudaError_t e, const char *where)
     return push_error(VPHYS_ERR_CUDA, "%s: CUDA error %d (%s)", where, (int)e, cudaGetErrorString(e));
 }
 
-constexpr int NFIXED = 46;
+constexpr int NFIXED = 48;
 constexpr unsigned MAGIC = 0x56504859u;   // "VPHY"
 
 struct Field {
@@ -141,6 +141,8 @@ size_t field_count(int nx, int ny, int nz, int field, bool *is_int)
     case VPHYS_FIELD_TKE_SHEAR:
     case VPHYS_FIELD_KD_EPBL: return X * Y * (Z + 1);
     case VPHYS_FIELD_SW_KAPPA: return X * Y * VPHYS_SW_NB_MAX;
+    case VPHYS_FIELD_CONTENT_OLD:
+    case VPHYS_FIELD_CONTENT_NEW: return X * Y;   // times the tracer count: set by vphys_create
     case VPHYS_FIELD_BL_DEPTH:
     case VPHYS_FIELD_B0:
     case VPHYS_FIELD_STRESS_MAG:
@@ -309,6 +311,8 @@ int validate(const vphys_config *c, int ntr)
     if (c->sw_chl < 0 || c->sw_chl > 1) return push_error(VPHYS_ERR_CONFIG, "sw_chl must be 0 or 1");
     if (c->use_cover_frac < 0 || c->use_cover_frac > 1)
         return push_error(VPHYS_ERR_CONFIG, "use_cover_frac must be 0 or 1");
+    if (c->column_integrals < 0 || c->column_integrals > 1)
+        return push_error(VPHYS_ERR_CONFIG, "column_integrals must be 0 or 1");
     if (c->sw_chl) {
         // rdb_config_validate.F90:291-310, rdb_ocean_sw_chl.F90:87-103
         // 0 means "unset" there and is raised to 1 when the handle stores the
@@ -383,6 +387,8 @@ Params make_params(vphys_handle h)
     p.wet_dyn = h->cfg.use_wet_dyn ? D(VPHYS_FIELD_WET_DYN) : nullptr;
     p.sw_kappa = h->cfg.sw_chl ? D(VPHYS_FIELD_SW_KAPPA) : nullptr;
     p.cover_frac = h->cfg.use_cover_frac ? D(VPHYS_FIELD_COVER_FRAC) : nullptr;
+    p.content_old = h->cfg.column_integrals ? D(VPHYS_FIELD_CONTENT_OLD) : nullptr;
+    p.content_new = h->cfg.column_integrals ? D(VPHYS_FIELD_CONTENT_NEW) : nullptr;
     p.tau_x = D(VPHYS_FIELD_TAU_X);
     p.tau_y = D(VPHYS_FIELD_TAU_Y);
     p.lambda_bot_u = D(VPHYS_FIELD_LAMBDA_BOT_U);
@@ -459,6 +465,10 @@ int prepare_momentum(vphys_handle h)
 int prepare_tracers(vphys_handle h)
 {
     int st = VPHYS_OK;
+    if (h->cfg.column_integrals) {
+        if ((st = ensure(h, VPHYS_FIELD_CONTENT_OLD))) return st;
+        if ((st = ensure(h, VPHYS_FIELD_CONTENT_NEW))) return st;
+    }
     if (h->cfg.mixed_precision && !h->span) {
         cudaError_t e = cudaMalloc(&h->span, (size_t)h->nx * h->ny * sizeof(int));
         if (e != cudaSuccess) {
@@ -912,6 +922,7 @@ int vphys_create(int nx, int ny, int nz, int ntracer, const vphys_config *cfg, v
     h->f.resize(NFIXED + ntracer);
     for (int id = 0; id < NFIXED; ++id) h->f[id].n = field_count(nx, ny, nz, id, &h->f[id].is_int);
     for (int t = 0; t < ntracer; ++t) h->f[NFIXED + t].n = (size_t)nx * ny * nz;
+    h->f[VPHYS_FIELD_CONTENT_OLD].n = h->f[VPHYS_FIELD_CONTENT_NEW].n = (size_t)nx * ny * (ntracer > 0 ? ntracer : 1);
     cudaError_t e = cudaMalloc(&h->guard_dev, sizeof(unsigned long long));
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -1126,6 +1137,7 @@ int vphys_get_ptr(vphys_handle h, int field, void **ptr, int *nx, int *ny, int *
     bool is_int;
     size_t n = field_count(h->nx, h->ny, h->nz, field, &is_int);
     int X = h->nx, Y = h->ny, Z = 1;
+    if (field == VPHYS_FIELD_CONTENT_OLD || field == VPHYS_FIELD_CONTENT_NEW) n = 0, Z = h->ntr > 0 ? h->ntr : 1;
     if (n == (size_t)(h->nx + 1) * h->ny * h->nz || n == (size_t)(h->nx + 1) * h->ny) X = h->nx + 1;
     if (n == (size_t)h->nx * (h->ny + 1) * h->nz || n == (size_t)h->nx * (h->ny + 1)) Y = h->ny + 1;
     if (n == (size_t)X * Y * h->nz) Z = h->nz;

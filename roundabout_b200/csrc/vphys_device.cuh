@@ -606,7 +606,7 @@ __device__ __forceinline__ double kpp_q_t_kin(const vphys_config &c, double q_he
 // shortwave; a solve instantiated for them folds the other branches out.
 __host__ __device__ __forceinline__ bool is_default_tracer_knobs(const vphys_config &c)
 {
-    return !c.budgets && !c.use_harmonic && !c.buoyancy_coeffs && c.sw_pen_frac == 0.0;
+    return !c.budgets && !c.use_harmonic && !c.buoyancy_coeffs && c.sw_pen_frac == 0.0 && !c.column_integrals;
 }
 __device__ __forceinline__ void default_tracer_knobs(vphys_config &c)
 {
@@ -614,6 +614,21 @@ __device__ __forceinline__ void default_tracer_knobs(vphys_config &c)
     c.use_harmonic = 0;
     c.buoyancy_coeffs = 0;
     c.sw_pen_frac = 0.0;
+    c.column_integrals = 0;
+}
+
+// Neumaier's improvement of Kahan summation (Z. Angew. Math. Mech. 54, 1974):
+// the rounding error of every addition is carried in cmp, whichever of the
+// two operands is larger (the column-content diagnostic; the oracle's
+// neumaier_add, operation for operation).
+__device__ __forceinline__ void neumaier_add(double &sum, double &cmp, double x)
+{
+    const double t = sum + x;
+    if (fabs(sum) >= fabs(x))
+        cmp += (sum - t) + x;
+    else
+        cmp += (x - t) + sum;
+    sum = t;
 }
 
 }  // namespace vphys

@@ -50,6 +50,8 @@ struct Params {
     // the chlorophyll scheme's band opacities, (nx, ny, VPHYS_SW_NB_MAX); NULL unless sw_chl
     const double *sw_kappa;
     const double *cover_frac;   // ice-shelf cover fraction; NULL unless use_cover_frac
+    // compensated column content before / after the tracer diffusion, (nx, ny, ntr); NULL unless column_integrals
+    double *content_old, *content_new;
     const double *tau_x, *tau_y, *lambda_bot_u, *lambda_bot_v;
     double *visc_rem_u, *visc_rem_v;
     double *gamma_t, *gamma_s;       // nullptr: not written

@@ -137,11 +137,12 @@ __global__ void k_spans(const Params p)
 // Back-substitution of one tracer column from the t and v rows; with FULL the
 // heat/salt budgets and the KPP non-local deposit (nonlocal_face_flux,
 // rdb_ocean_vmix.F90:1605-1714) ride along.
-template <bool FULL>
+template <bool FULL, bool CI = false>
 __device__ __forceinline__ void tracer_back(const Params &p, double dt, double *__restrict__ trc,
                                             const double *__restrict__ hp, const float *tu, const float *vv, int w_lo,
                                             int w_hi, int lo, int hi, double *bud, bool nl_t, bool nl, double h_b,
-                                            double q_kin, unsigned long long pol)
+                                            double q_kin, unsigned long long pol, double *c_new = nullptr,
+                                            double *e_new = nullptr)
 {
     const size_t P = p.plane;
     const int nz = p.nz;
@@ -184,6 +185,7 @@ __device__ __forceinline__ void tracer_back(const Params &p, double dt, double *
                     x = conc_add_source(x, h_c, dt * (f_up - f_dn));
                     g_above = gk;
                 }
+                if (CI) neumaier_add(*c_new, *e_new, h_c * x);
                 h_a = h_c;
                 h_c = h_bl;
             }
@@ -202,7 +204,11 @@ struct TracerGroups {
 
 // TPW tracers per warp share one factorisation and one t array (TWO, a
 // separate ks, keeps one tracer per warp); their forward chains interleave.
-template <bool TWO, int TPW, bool DEF>
+// CI (one tracer per warp): the compensated column content before the solve
+// (terms bottom-up, from the FP64 old values of the upward pass) and after it
+// (top-down, the FP64 new values of the downward pass) into p.content_old /
+// p.content_new; a group re-solved in FP64 gets them from the re-solve.
+template <bool TWO, int TPW, bool DEF, bool CI = false>
 __global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, double dt, int nonlocal, int ngx,
                                                            const TracerGroups tg)
 {
@@ -252,7 +258,11 @@ __global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, doubl
     const int lo = live ? (sp & 0xffff) : nz + 1, hi = live ? (sp >> 16) : 0;
     const int w_lo = __reduce_min_sync(0xffffffffu, live ? lo : 0x7fffffff);
     const int w_hi = __reduce_max_sync(0xffffffffu, hi);
-    if (w_hi == 0) return;
+    if (w_hi == 0) {
+        if (CI && in_grid) p.content_old[col + P * (size_t)tix[0]] = p.content_new[col + P * (size_t)tix[0]] = 0.0;
+        return;
+    }
+    double c_old = 0.0, e_old = 0.0, c_new = 0.0, e_new = 0.0;   // CI: Neumaier sums and compensations
 
     const double *__restrict__ Kp = ((TWO && tix[0] != iT) ? p.ks : p.kt) + col;
     double *trc[TPW];
@@ -303,6 +313,7 @@ __global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, doubl
                 pivot_row(H + f_dn * q_prev, f_up, ip, t, qq);
                 const size_t s = (size_t)(k - 1) * MP_TR_COLS;
                 const double fd = (double)f_dn, fu = (double)f_up, ipd = (double)ip;
+                if (CI) neumaier_add(c_old, e_old, h_c * d_c[0]);   // rows off the span: 0 * 0
 #pragma unroll
                 for (int q = 0; q < TPW; ++q) {
                     const double b = fd * (d_m[q] - d_c[q]) + fu * (dn[u][q] - d_c[q]);
@@ -362,13 +373,14 @@ __global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, doubl
 #pragma unroll
         for (int q = 0; q < TPW; ++q) delta[q] = 0.0f;
         for (int k0 = w_hi; k0 >= w_lo; k0 -= U) {
-            double dk[U][TPW];
+            double dk[U][TPW], hk[U];
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const int k = k0 - u;
 #pragma unroll
                 for (int q = 0; q < TPW; ++q)
                     dk[u][q] = (k >= lo && k <= hi && q < nt) ? ld_hint(trc[q] + P * (size_t)(k - 1), pol_once) : 0.0;
+                if (CI) hk[u] = (k >= lo && k <= hi) ? __ldg(hp + P * (size_t)(k - 1)) : 0.0;
             }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
@@ -380,10 +392,15 @@ __global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, doubl
                 for (int q = 0; q < TPW; ++q) delta[q] = vv[(size_t)q * NB + s] + mul_u(tk, delta[q]);
                 if (k < lo || k > hi) continue;
                 const size_t off = P * (size_t)(k - 1);
+                if (CI) neumaier_add(c_new, e_new, hk[u] * (dk[u][0] + (double)delta[0]));
 #pragma unroll
                 for (int q = 0; q < TPW; ++q)
                     if (q < nt) trc[q][off] = dk[u][q] + (double)delta[q];
             }
+        }
+        if (CI && in_grid) {
+            p.content_old[col + P * (size_t)tix[0]] = c_old + e_old;
+            p.content_new[col + P * (size_t)tix[0]] = c_new + e_new;
         }
         return;
     }
@@ -418,7 +435,14 @@ __global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, doubl
         if (c.budgets && tr == iS) bud = p.salt_budget + col;
         double *t_ptr = p.tr[tr] + col;
         const float *vq = vv + (size_t)q * NB;
-        if (nl_t || bud)
+        if (CI) {
+            tracer_back<true, true>(p, dt, t_ptr, hp, tu, vq, w_lo, w_hi, lo, hi, bud, nl_t, nl, h_b, q_kin, pol_once,
+                                    &c_new, &e_new);
+            if (in_grid) {
+                p.content_old[col + P * (size_t)tr] = c_old + e_old;
+                p.content_new[col + P * (size_t)tr] = c_new + e_new;
+            }
+        } else if (nl_t || bud)
             tracer_back<true>(p, dt, t_ptr, hp, tu, vq, w_lo, w_hi, lo, hi, bud, nl_t, nl, h_b, q_kin, pol_once);
         else
             tracer_back<false>(p, dt, t_ptr, hp, tu, vq, w_lo, w_hi, lo, hi, nullptr, false, false, 0.0, 0.0,
@@ -1102,6 +1126,8 @@ static void launch_tracers_mp_t(const Params &p, double dt, bool nonlocal, cudaS
         const int mx = (int)((size_t)VPHYS_NZ_MAX * MP_TR_COLS * (1 + TPW) * sizeof(float));
         cudaFuncSetAttribute(k_tracers_mp<TWO, TPW, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
         cudaFuncSetAttribute(k_tracers_mp<TWO, TPW, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+        if (TPW == 1)
+            cudaFuncSetAttribute(k_tracers_mp<TWO, 1, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
         attr_set = true;
     }
     // tracers with a non-local deposit or a budget first, one per group; the
@@ -1127,6 +1153,8 @@ static void launch_tracers_mp_t(const Params &p, double dt, bool nonlocal, cudaS
     const unsigned blocks = (unsigned)ngx * (unsigned)p.ny * (unsigned)tg.ngroups;
     if (is_default_tracer_knobs(p.cfg))
         k_tracers_mp<TWO, TPW, true><<<blocks, MP_TR_COLS, smem, stream>>>(p, dt, nonlocal ? 1 : 0, ngx, tg);
+    else if (TPW == 1 && p.content_old)
+        k_tracers_mp<TWO, 1, false, true><<<blocks, MP_TR_COLS, smem, stream>>>(p, dt, nonlocal ? 1 : 0, ngx, tg);
     else
         k_tracers_mp<TWO, TPW, false><<<blocks, MP_TR_COLS, smem, stream>>>(p, dt, nonlocal ? 1 : 0, ngx, tg);
     if (p.mp_redo) launch_tracers_redo(p, dt, nonlocal, stream);
@@ -1140,10 +1168,11 @@ void launch_tracers_mp(const Params &p, double dt, bool nonlocal, cudaStream_t s
         launch_tracers_mp_t<true, 1>(p, dt, nonlocal, stream);
         return;
     }
-    // tracers per warp (the variant vphys_autotune chose; a separate ks keeps
-    // one per warp): sharing a warp saves the repeated factorisation, at the
-    // price of a larger register and shared-memory footprint per warp
-    switch (p.var_tr) {
+    // tracers per warp (the variant vphys_autotune chose; a separate ks or
+    // the column-content diagnostic keeps one per warp): sharing a warp saves
+    // the repeated factorisation, at the price of a larger register and
+    // shared-memory footprint per warp
+    switch (p.content_old ? VAR_TR_SMEM1 : p.var_tr) {
     case VAR_TR_SMEM4: launch_tracers_mp_t<false, 4>(p, dt, nonlocal, stream); break;
     case VAR_TR_SMEM2: launch_tracers_mp_t<false, 2>(p, dt, nonlocal, stream); break;
     default: launch_tracers_mp_t<false, 1>(p, dt, nonlocal, stream); break;

@@ -75,8 +75,10 @@ __device__ __forceinline__ void tracer_row(int k, int nz, bool use_harmonic, dou
 }
 
 // The columns of one warp: column (i, j) on this lane, `tid` its slot in the
-// block's shared memory of `bs` columns.
-template <int NTR, bool TWO, bool DEF>
+// block's shared memory of `bs` columns.  CI: with the diffusion, the
+// compensated column content before it (terms bottom-up, in the upward pass)
+// and after it (top-down, in the downward pass) into p.content_old / _new.
+template <int NTR, bool TWO, bool DEF, bool CI = false>
 __device__ __forceinline__ void tracer_columns(const Params &p, double dt, int diffuse, int nonlocal, int i, int j,
                                                double *smem, int tid, int bs)
 {
@@ -137,7 +139,14 @@ __device__ __forceinline__ void tracer_columns(const Params &p, double dt, int d
     const unsigned full = 0xffffffffu;
     const int w_lo = __reduce_min_sync(full, live ? k_lo : 0x7fffffff);
     const int w_hi = __reduce_max_sync(full, live ? k_hi : 0);
-    if (w_hi == 0) return;   // no live layer anywhere in this warp
+    if (w_hi == 0) {   // no live layer anywhere in this warp
+        if (CI && diffuse && in_grid)
+            for (int t = 0; t < ntr; ++t) p.content_old[col + P * (size_t)t] = p.content_new[col + P * (size_t)t] = 0.0;
+        return;
+    }
+    double c_old[NTR], e_old[NTR], c_new[NTR], e_new[NTR];   // CI: Neumaier sums and their compensations
+#pragma unroll
+    for (int t = 0; t < NTR; ++t) c_old[t] = e_old[t] = c_new[t] = e_new[t] = 0.0;
 
     double *trc[NTR];
 #pragma unroll
@@ -211,6 +220,11 @@ __device__ __forceinline__ void tracer_columns(const Params &p, double dt, int d
                             r_prev[t] = r;
                             st_hint(rbuf[t] + off, r, pol_keep);
                         }
+                    }
+                    if (CI) {
+#pragma unroll
+                        for (int t = 0; t < NTR; ++t)
+                            if (t < ntr) neumaier_add(c_old[t], e_old[t], h_c * xs[u][t]);
                     }
                     KA_k = kap[u];
                     h_m = h_c;
@@ -319,6 +333,7 @@ __device__ __forceinline__ void tracer_columns(const Params &p, double dt, int d
                             if (t == iT) x = conc_add_source(x, h_c, fT);
                             else if (t == iS || t == iPS) x = conc_add_source(x, h_c, fS);
                         }
+                        if (CI && diffuse) neumaier_add(c_new[t], e_new[t], h_c * x);
                         trc[t][off] = x;
                     }
                 }
@@ -329,15 +344,23 @@ __device__ __forceinline__ void tracer_columns(const Params &p, double dt, int d
             }
         }
     }
+    if (CI && diffuse && in_grid) {
+#pragma unroll
+        for (int t = 0; t < NTR; ++t)
+            if (t < ntr) {
+                p.content_old[col + P * (size_t)t] = c_old[t] + e_old[t];
+                p.content_new[col + P * (size_t)t] = c_new[t] + e_new[t];
+            }
+    }
 #undef HH
 }
 
-template <int NTR, bool TWO, bool DEF>
+template <int NTR, bool TWO, bool DEF, bool CI>
 __global__ void __launch_bounds__(128) k_tracers(const Params p, double dt, int diffuse, int nonlocal)
 {
     extern __shared__ double smem[];
-    tracer_columns<NTR, TWO, DEF>(p, dt, diffuse, nonlocal, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y, smem,
-                             threadIdx.x, blockDim.x);
+    tracer_columns<NTR, TWO, DEF, CI>(p, dt, diffuse, nonlocal, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y,
+                                      smem, threadIdx.x, blockDim.x);
 }
 
 // The FP64 re-solve of the (32-column group, tracer) pairs that the
@@ -364,7 +387,13 @@ __global__ void __launch_bounds__(32) k_tracers_redo(const Params p, double dt, 
         q.cfg.idx_salinity = (tix == c.idx_salinity) ? 0 : -1;
         q.cfg.idx_pseudo_salt = (tix == c.idx_pseudo_salt) ? 0 : -1;
         if (!p.ks_equals_kt && tix != c.idx_temperature) q.kt = p.ks;   // the second factorisation's tracers
-        tracer_columns<1, false, false>(q, dt, 1, nonlocal, li, j, smem, threadIdx.x, 32);
+        if (p.content_old) {
+            q.content_old = p.content_old + p.plane * (size_t)tix;   // the tracer's plane of the content fields
+            q.content_new = p.content_new + p.plane * (size_t)tix;
+            tracer_columns<1, false, false, true>(q, dt, 1, nonlocal, li, j, smem, threadIdx.x, 32);
+        } else {
+            tracer_columns<1, false, false>(q, dt, 1, nonlocal, li, j, smem, threadIdx.x, 32);
+        }
         __syncwarp();
     }
 }
@@ -398,15 +427,18 @@ static void launch_tracers_n(const Params &p, double dt, bool diffuse, bool nonl
     static bool attr_set = false;
     if (!attr_set) {
         const int mx = (int)((size_t)VPHYS_NZ_MAX * bs * sizeof(double) * (TWO ? 2 : 1));
-        cudaFuncSetAttribute(k_tracers<NTR, TWO, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-        cudaFuncSetAttribute(k_tracers<NTR, TWO, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+        cudaFuncSetAttribute(k_tracers<NTR, TWO, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+        cudaFuncSetAttribute(k_tracers<NTR, TWO, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+        cudaFuncSetAttribute(k_tracers<NTR, TWO, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
         attr_set = true;
     }
     dim3 grid((p.nx + bs - 1) / bs, p.ny);
     if (is_default_tracer_knobs(p.cfg))
-        k_tracers<NTR, TWO, true><<<grid, bs, smem, stream>>>(p, dt, diffuse ? 1 : 0, nonlocal ? 1 : 0);
+        k_tracers<NTR, TWO, true, false><<<grid, bs, smem, stream>>>(p, dt, diffuse ? 1 : 0, nonlocal ? 1 : 0);
+    else if (p.content_old && diffuse)
+        k_tracers<NTR, TWO, false, true><<<grid, bs, smem, stream>>>(p, dt, 1, nonlocal ? 1 : 0);
     else
-        k_tracers<NTR, TWO, false><<<grid, bs, smem, stream>>>(p, dt, diffuse ? 1 : 0, nonlocal ? 1 : 0);
+        k_tracers<NTR, TWO, false, false><<<grid, bs, smem, stream>>>(p, dt, diffuse ? 1 : 0, nonlocal ? 1 : 0);
 }
 
 void launch_tracers(const Params &p, double dt, bool diffuse, bool nonlocal, cudaStream_t stream)
