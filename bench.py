@@ -86,6 +86,10 @@ def parse():
                     help="skip the batched configuration (10 tracers, 15%% thin-layer columns, 24-step graph)")
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the GPU-vs-oracle comparison on the CPU arm's slice")
+    ap.add_argument("--variants", default=None,
+                    help="momentum,tracers kernel variants of the mixed solves to pin instead of autotuning "
+                         "(e.g. tma_ring,smem_1_per_warp: a profiling run under ncu, whose serialised launches "
+                         "would skew the autotuner's timings)")
     return ap.parse_args()
 
 
@@ -363,7 +367,12 @@ def main():
 
     # ---- the in-project autotuner picks the mixed solves' kernel variants on
     #      this handle's state (the state is left as it was) ----
-    tune = vp.autotune(dt, reps=3) if mixed else None
+    if mixed and args.variants:
+        mv, tv = args.variants.split(",")
+        vp.set_variants(mv, tv)
+        tune = {"pinned": {"momentum": mv, "tracers": tv}}
+    else:
+        tune = vp.autotune(dt, reps=3) if mixed else None
 
     # ---- the timed region: K steps of the selected form; the clocks are
     #      sampled from a second before it to half a second after it, with
@@ -409,7 +418,9 @@ def main():
     kernel_of = {"eos": "k_eos_wright",
                  "assemble": "k_assemble<float>" if (mixed and args.mixed_level >= 2) else "k_assemble<double>",
                  # the stage's launches: the column-depth pass and the face solve
-                 "momentum": "k_column_depth+k_momentum_mp" if mixed else "k_column_depth+k_momentum",
+                 "momentum": ("k_column_depth+k_mom_tile_flags+k_momentum_mp_tma"
+                              if mixed and (tune or {}).get("chosen", {}).get("momentum") == "tma_ring"
+                              else ("k_column_depth+k_momentum_mp" if mixed else "k_column_depth+k_momentum")),
                  "tracers": "k_spans+k_tracers_mp+k_tracers_redo" if mixed else "k_tracers"}
     dom = max(("assemble", "momentum", "tracers", "eos"), key=lambda k: stage_ms[k])
     peak, peak_kind = peaks()

@@ -35,6 +35,9 @@ def main():
     ap.add_argument("--mixed", type=int, default=0, choices=[0, 1, 2],
                     help="1: FP32 sweeps + FP64 residual; 2: also the FP32 assembly")
     ap.add_argument("--stages", default="eos,assemble,momentum,tracers,step")
+    ap.add_argument("--variants", default=None,
+                    help="momentum,tracers kernel variants of the mixed solves (VerticalPhysics.MOM_VARIANTS / "
+                         "TRACER_VARIANTS names), e.g. tma_ring,tmem_rows; default: the handle's")
     args = ap.parse_args()
 
     import torch
@@ -54,6 +57,9 @@ def main():
     cfg.mixed_precision = int(args.mixed)
     vp = VerticalPhysics(args.nx, args.ny, args.nz, args.ntr, cfg)
     vp.load_columns(cols)
+    if args.variants:
+        mom, trv = args.variants.split(",")
+        vp.set_variants(mom, trv)
     dt = 3600.0
     vp.step(dt, args.warmup)
     if "kshear" in args.stages:
