@@ -23,7 +23,7 @@ SOURCES = ["vphys_api.cu", "vphys_kernels.cu", "vphys_momentum_tma.cu", "vphys_t
            "vphys_mixed.cu",
            "vphys_gemm.cu", "vphys_learned.cu", "vphys_kshear.cu",
            "vphys_epbl.cu"]
-HEADERS = ["vphys_device.cuh", "vphys_faces.cuh", "vphys_kernels.cuh", "vphys_tma.cuh", "vphys_tiles.cuh", "vphys_mom_ring.cuh",
+HEADERS = ["vphys_device.cuh", "vphys_faces.cuh", "vphys_kernels.cuh", "vphys_tma.cuh", "vphys_tiles.cuh", "vphys_mom_ring.cuh", "vphys_tmem.cuh",
            "../../include/vphys.h"]
 # the mixed-precision solves carry no bitwise contract: FMA contraction allowed
 CONTRACT_OK = {"vphys_mixed.cu", "vphys_gemm.cu", "vphys_learned.cu"}

@@ -43,6 +43,7 @@
 #include "vphys_faces.cuh"
 #include "vphys_kernels.cuh"
 #include "vphys_mom_ring.cuh"
+#include "vphys_tmem.cuh"
 
 namespace vphys {
 
@@ -151,11 +152,14 @@ __device__ __forceinline__ void tracer_back(const Params &p, double dt, double *
     double h_c = (FULL && lo <= hi) ? __ldg(hp + P * (size_t)(hi - 1)) : 0.0;
     constexpr int BU = FULL ? MP_TR_UF : MP_TR_U;   // the deposit's registers leave room for fewer loads
     for (int k0 = w_hi; k0 >= w_lo; k0 -= BU) {
-        double dk[BU];
+        // the block's old values and, with the deposit, the thicknesses one
+        // level down: loaded ahead, so no level waits on its own load
+        double dk[BU], hb[BU];
 #pragma unroll
         for (int u = 0; u < BU; ++u) {
             const int k = k0 - u;
             dk[u] = (k >= lo && k <= hi) ? ld_hint(trc + P * (size_t)(k - 1), pol) : 0.0;
+            if (FULL) hb[u] = (k > 1 && k >= lo && k <= hi) ? __ldg(hp + P * (size_t)(k - 2)) : 0.0;
         }
 #pragma unroll
         for (int u = 0; u < BU; ++u) {
@@ -169,7 +173,7 @@ __device__ __forceinline__ void tracer_back(const Params &p, double dt, double *
             double x = d_k + (double)delta;
             if (FULL) {
                 if (bud) bud[off] = bud[off] + (h_c * x - h_c * d_k);
-                const double h_bl = (k > 1) ? __ldg(hp + off - P) : 0.0;
+                const double h_bl = hb[u];
                 if (nl_t) {
                     double gk = 0.0;
                     if (nl) {
@@ -194,9 +198,111 @@ __device__ __forceinline__ void tracer_back(const Params &p, double dt, double *
     }
 }
 
+// The non-local column scalars of a live column (FP64, as KPP pass 2): the
+// boundary-layer depth h_b and the kinematic heat and salt fluxes; true when
+// the column takes the deposit (h_b > 0, w_s > 0, B_0 < 0).
+__device__ __forceinline__ bool nonlocal_column(const Params &p, const vphys_config &c, size_t col,
+                                                const double *__restrict__ hp, int hi, double &h_b, double &q_T_kin,
+                                                double &q_S_kin)
+{
+    const double rho0 = c.rho0;
+    h_b = p.bl_depth[col];
+    const double u_star = sqrt(xdiv(p.stress_mag[col], rho0));
+    // the heat flux pass 2 charged (shortwave: what passes h_b, or the
+    // surface layer hi)
+    q_T_kin = kpp_q_t_kin(c, p.q_heat[col], p.sw_src + col, p.sw_kappa, col, p.plane, h_b,
+                          __ldg(hp + p.plane * (size_t)(hi - 1)));
+    q_S_kin = xdiv(p.q_salt[col], rho0);
+    // with "eos" coefficients or shortwave B0 is the assembly's (pass 2
+    // stored it before the solve changed the surface T and S); otherwise
+    // the same number recomputed
+    const double B_0 = (c.buoyancy_coeffs || c.sw_pen_frac != 0.0)
+                           ? p.b0[col]
+                           : (GRAVITY / rho0) * (c.alpha_T * q_T_kin - c.beta_S * q_S_kin);
+    const double wstar3 = fmx(0.0, -B_0) * h_b;
+    const double w_star = sm_cbrt(wstar3);
+    const double w_s = sqrt(u_star * u_star + w_star * w_star);
+    return h_b > 0.0 && w_s > 0.0 && B_0 < 0.0;
+}
+
+// tracer_back<true> for the TPW tracers of a group in one downward pass: the
+// thicknesses, the running depth and the shape of the non-local profile are
+// loaded and computed once for the group, each tracer keeping its own
+// increment, budget and deposit (dep[q]: the tracer takes the KPP deposit
+// with kinematic flux q_kin[q]; nl: the column is convective).  Per tracer
+// the arithmetic is tracer_back<true>'s.
+template <int TPW>
+__device__ __forceinline__ void tracer_back_group(const Params &p, double dt, double *const (&trc)[TPW], int nt,
+                                                  const double *__restrict__ hp, const float *tu, const float *vv,
+                                                  size_t NB, int w_lo, int w_hi, int lo, int hi,
+                                                  double *const (&bud)[TPW], const bool (&dep)[TPW], bool nl,
+                                                  double h_b, const double (&q_kin)[TPW], unsigned long long pol)
+{
+    const size_t P = p.plane;
+    const int nz = p.nz;
+    float delta[TPW];
+    double g_above[TPW];
+#pragma unroll
+    for (int q = 0; q < TPW; ++q) delta[q] = 0.0f, g_above[q] = 0.0;
+    double d_run = 0.0, h_a = 0.0;
+    double h_c = (lo <= hi) ? __ldg(hp + P * (size_t)(hi - 1)) : 0.0;
+    constexpr int BU = MP_TR_U;
+    for (int k0 = w_hi; k0 >= w_lo; k0 -= BU) {
+        double dk[BU][TPW], hb[BU];
+#pragma unroll
+        for (int u = 0; u < BU; ++u) {
+            const int k = k0 - u;
+            const bool in = k >= lo && k <= hi;
+#pragma unroll
+            for (int q = 0; q < TPW; ++q) dk[u][q] = (in && q < nt) ? ld_hint(trc[q] + P * (size_t)(k - 1), pol) : 0.0;
+            hb[u] = (in && k > 1) ? __ldg(hp + P * (size_t)(k - 2)) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < BU; ++u) {
+            const int k = k0 - u;
+            if (k < w_lo) break;
+            const size_t s = (size_t)(k - 1) * MP_TR_COLS;
+            const float tk = tu[s];
+#pragma unroll
+            for (int q = 0; q < TPW; ++q) delta[q] = vv[(size_t)q * NB + s] + mul_u(tk, delta[q]);
+            if (k < lo || k > hi) continue;
+            const size_t off = P * (size_t)(k - 1);
+            const double h_bl = hb[u];
+            double shape = 0.0;   // cs_nonlocal * sigma (1 - sigma)^2 inside the boundary layer
+            bool in_bl = false;
+            if (nl) {
+                d_run = d_run + h_c;
+                if (k > 1 && d_run < h_b) {
+                    const double sigma = xdiv(d_run, h_b);
+                    shape = p.cfg.cs_nonlocal * (sigma * (1.0 - sigma) * (1.0 - sigma));
+                    in_bl = true;
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < TPW; ++q) {
+                if (q >= nt) break;
+                const double d_k = dk[u][q];
+                double x = d_k + (double)delta[q];
+                if (bud[q]) bud[q][off] = bud[q][off] + (h_c * x - h_c * d_k);
+                if (dep[q]) {
+                    const double gk = in_bl ? shape * q_kin[q] : 0.0;
+                    double f_up = 0.0, f_dn = 0.0;
+                    if (k < nz) f_up = nonlocal_face_flux(g_above[q], h_c, h_a);
+                    if (k > 1) f_dn = nonlocal_face_flux(gk, h_bl, h_c);
+                    x = conc_add_source(x, h_c, dt * (f_up - f_dn));
+                    g_above[q] = gk;
+                }
+                trc[q][off] = x;
+            }
+            h_a = h_c;
+            h_c = h_bl;
+        }
+    }
+}
+
 // Tracer groups of a launch: the first `single` groups hold one tracer each
-// (those with a non-local deposit or a budget, whose back-substitution is
-// their own), the rest up to TPW tracers in the order of `perm`.
+// (one tracer per warp: every tracer; otherwise none), the rest up to TPW
+// tracers in the order of `perm`.
 struct TracerGroups {
     int single, ngroups;
     signed char perm[NTR_MAX];
@@ -404,49 +510,57 @@ __global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, doubl
         }
         return;
     }
-    for (int q = 0; q < nt; ++q) {
-        const int tr = tix[q];
-        // ---- non-local column scalars (FP64, as KPP pass 2) ----
-        const bool nl_t = nonlocal && c.use_kpp && (tr == iT || tr == iS || tr == iPS);
-        bool nl = nl_t && live;
-        double h_b = 0.0, q_kin = 0.0;
-        if (nl) {
-            const double rho0 = c.rho0;
-            h_b = p.bl_depth[col];
-            const double u_star = sqrt(xdiv(p.stress_mag[col], rho0));
-            // the heat flux pass 2 charged (shortwave: what passes h_b, or the
-            // surface layer hi)
-            const double q_T_kin = kpp_q_t_kin(c, p.q_heat[col], p.sw_src + col, p.sw_kappa, col, p.plane, h_b, __ldg(hp + P * (size_t)(hi - 1)));
-            const double q_S_kin = xdiv(p.q_salt[col], rho0);
-            // with "eos" coefficients or shortwave B0 is the assembly's (pass 2
-            // stored it before the solve changed the surface T and S); otherwise
-            // the same number recomputed
-            const double B_0 = (c.buoyancy_coeffs || c.sw_pen_frac != 0.0)
-                                   ? p.b0[col]
-                                   : (GRAVITY / rho0) * (c.alpha_T * q_T_kin - c.beta_S * q_S_kin);
-            const double wstar3 = fmx(0.0, -B_0) * h_b;
-            const double w_star = sm_cbrt(wstar3);
-            const double w_s = sqrt(u_star * u_star + w_star * w_star);
-            nl = (h_b > 0.0 && w_s > 0.0 && B_0 < 0.0);
-            q_kin = (tr == iT) ? q_T_kin : q_S_kin;
+    if constexpr (TPW > 1) {
+        // a group with a deposit or a budget: one fused downward pass
+        double *bud[TPW], q_kin[TPW];
+        bool dep[TPW], any_dep = false;
+#pragma unroll
+        for (int q = 0; q < TPW; ++q) {
+            const int tr = tix[q];
+            dep[q] = q < nt && nonlocal && c.use_kpp && (tr == iT || tr == iS || tr == iPS);
+            any_dep = any_dep || dep[q];
+            bud[q] = nullptr;
+            if (q < nt && c.budgets && tr == iT) bud[q] = p.heat_budget + col;
+            if (q < nt && c.budgets && tr == iS) bud[q] = p.salt_budget + col;
         }
-        double *bud = nullptr;
-        if (c.budgets && tr == iT) bud = p.heat_budget + col;
-        if (c.budgets && tr == iS) bud = p.salt_budget + col;
-        double *t_ptr = p.tr[tr] + col;
-        const float *vq = vv + (size_t)q * NB;
-        if (CI) {
-            tracer_back<true, true>(p, dt, t_ptr, hp, tu, vq, w_lo, w_hi, lo, hi, bud, nl_t, nl, h_b, q_kin, pol_once,
-                                    &c_new, &e_new);
-            if (in_grid) {
-                p.content_old[col + P * (size_t)tr] = c_old + e_old;
-                p.content_new[col + P * (size_t)tr] = c_new + e_new;
-            }
-        } else if (nl_t || bud)
-            tracer_back<true>(p, dt, t_ptr, hp, tu, vq, w_lo, w_hi, lo, hi, bud, nl_t, nl, h_b, q_kin, pol_once);
-        else
-            tracer_back<false>(p, dt, t_ptr, hp, tu, vq, w_lo, w_hi, lo, hi, nullptr, false, false, 0.0, 0.0,
+        bool nl = false;
+        double h_b = 0.0, q_T_kin = 0.0, q_S_kin = 0.0;
+        if (any_dep && live) nl = nonlocal_column(p, c, col, hp, hi, h_b, q_T_kin, q_S_kin);
+#pragma unroll
+        for (int q = 0; q < TPW; ++q) q_kin[q] = (tix[q] == iT) ? q_T_kin : q_S_kin;
+        tracer_back_group<TPW>(p, dt, trc, nt, hp, tu, vv, NB, w_lo, w_hi, lo, hi, bud, dep, nl, h_b, q_kin,
                                pol_once);
+        return;
+    } else {
+        for (int q = 0; q < nt; ++q) {
+            const int tr = tix[q];
+            // ---- non-local column scalars (FP64, as KPP pass 2) ----
+            const bool nl_t = nonlocal && c.use_kpp && (tr == iT || tr == iS || tr == iPS);
+            bool nl = nl_t && live;
+            double h_b = 0.0, q_kin = 0.0;
+            if (nl) {
+                double q_T_kin, q_S_kin;
+                nl = nonlocal_column(p, c, col, hp, hi, h_b, q_T_kin, q_S_kin);
+                q_kin = (tr == iT) ? q_T_kin : q_S_kin;
+            }
+            double *bud = nullptr;
+            if (c.budgets && tr == iT) bud = p.heat_budget + col;
+            if (c.budgets && tr == iS) bud = p.salt_budget + col;
+            double *t_ptr = p.tr[tr] + col;
+            const float *vq = vv + (size_t)q * NB;
+            if (CI) {
+                tracer_back<true, true>(p, dt, t_ptr, hp, tu, vq, w_lo, w_hi, lo, hi, bud, nl_t, nl, h_b, q_kin,
+                                        pol_once, &c_new, &e_new);
+                if (in_grid) {
+                    p.content_old[col + P * (size_t)tr] = c_old + e_old;
+                    p.content_new[col + P * (size_t)tr] = c_new + e_new;
+                }
+            } else if (nl_t || bud)
+                tracer_back<true>(p, dt, t_ptr, hp, tu, vq, w_lo, w_hi, lo, hi, bud, nl_t, nl, h_b, q_kin, pol_once);
+            else
+                tracer_back<false>(p, dt, t_ptr, hp, tu, vq, w_lo, w_hi, lo, hi, nullptr, false, false, 0.0, 0.0,
+                                   pol_once);
+        }
     }
 }
 
@@ -495,28 +609,12 @@ struct SRows {
 // col0 + 2(k-1), 2(k-1)+1 of the warp's 32 lanes (taddr: lane << 16 | column)
 struct TRows {
     uint32_t base;
-    __device__ __forceinline__ void put(int k, float t, float v)
-    {
-        __syncwarp();
-        asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1, %2};" ::"r"(base + 2u * (uint32_t)(k - 1)),
-                     "r"(__float_as_uint(t)), "r"(__float_as_uint(v))
-                     : "memory");
-    }
-    __device__ __forceinline__ void done_writing()
-    {
-        __syncwarp();
-        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-    }
+    __device__ __forceinline__ void put(int k, float t, float v) { tmem_put2(base, k, __float_as_uint(t), __float_as_uint(v)); }
+    __device__ __forceinline__ void done_writing() { tmem_store_done(); }
     __device__ __forceinline__ void load8(int kb, float (&t)[8], float (&v)[8]) const
     {
         uint32_t r[16];
-        __syncwarp();
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-            : "r"(base + 16u * (uint32_t)kb));
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        tmem_get16(base, kb, r);
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
             t[q] = __uint_as_float(r[2 * q]);
@@ -542,11 +640,12 @@ __device__ __forceinline__ void tracer_back_rows(const Params &p, double dt, dou
     for (int kb = (w_hi - 1) >> 3; kb >= ((w_lo - 1) >> 3); --kb) {
         float t8[8], v8[8];
         rows.load8(kb, t8, v8);
-        double dk[8];
+        double dk[8], hb[8];   // old values and (deposit) the thicknesses one level down, loaded ahead
 #pragma unroll
         for (int q = 7; q >= 0; --q) {
             const int k = 8 * kb + q + 1;
             dk[q] = (k >= lo && k <= hi) ? ld_hint(trc + P * (size_t)(k - 1), pol) : 0.0;
+            if (FULL) hb[q] = (k > 1 && k >= lo && k <= hi) ? __ldg(hp + P * (size_t)(k - 2)) : 0.0;
         }
 #pragma unroll
         for (int q = 7; q >= 0; --q) {
@@ -557,7 +656,7 @@ __device__ __forceinline__ void tracer_back_rows(const Params &p, double dt, dou
             const size_t off = P * (size_t)(k - 1);
             double x = dk[q] + (double)delta;
             if (FULL) {
-                const double h_bl = (k > 1) ? __ldg(hp + off - P) : 0.0;
+                const double h_bl = hb[q];
                 double gk = 0.0;
                 if (nl) {
                     d_run = d_run + h_c;
@@ -712,16 +811,10 @@ __global__ void __launch_bounds__(32 * MAXW, 1)
     extern __shared__ __align__(16) float smf[];
     __shared__ uint32_t tmem_slot;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nwarps = blockDim.x >> 5;
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(
-                         (uint32_t)__cvta_generic_to_shared(&tmem_slot))
-                     : "memory");
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-    }
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    if (warp == 0) tmem_alloc_all(&tmem_slot);
+    tmem_fence_before();
     __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    tmem_fence_after();
     const uint32_t tbase = tmem_slot;
     vphys_config cd = p.cfg;
     default_tracer_knobs(cd);
@@ -734,7 +827,7 @@ __global__ void __launch_bounds__(32 * MAXW, 1)
         return (int)__shfl_sync(0xffffffffu, it, 0);
     };
     if (warp < nt_warps) {
-        TRows rows{tbase + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)((warp >> 2) * 2 * nzp)};
+        TRows rows{tmem_warp_slot(tbase, warp, nzp)};
         for (int item = next(); item < nitems; item = next()) tracer_item_tm(p, cd, dt, nonlocal, ngx, item, rows, lane);
     } else {
         const size_t NB = (size_t)p.nz * MP_TR_COLS;
@@ -742,11 +835,11 @@ __global__ void __launch_bounds__(32 * MAXW, 1)
         SRows rows{tu, tu + NB, p.nz};
         for (int item = next(); item < nitems; item = next()) tracer_item_tm(p, cd, dt, nonlocal, ngx, item, rows, lane);
     }
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    tmem_fence_before();
     __syncthreads();
     if (warp == 0) {
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tbase) : "memory");
+        tmem_fence_after();
+        tmem_free_all(tbase);
     }
 }
 
@@ -1130,25 +1223,29 @@ static void launch_tracers_mp_t(const Params &p, double dt, bool nonlocal, cudaS
             cudaFuncSetAttribute(k_tracers_mp<TWO, 1, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
         attr_set = true;
     }
-    // tracers with a non-local deposit or a budget first, one per group; the
-    // plain diffusions after them, TPW per group
+    // one tracer per warp: every tracer its own group.  TPW per warp: the
+    // tracers with the salt deposit (salinity, pseudo-salt: the same flux)
+    // first, then the heat deposit, then the rest, TPW per group, so that a
+    // group's deposits share their column scalars and profile
     const vphys_config &c = p.cfg;
     TracerGroups tg{};
     int n = 0;
-    for (int t = 0; t < p.ntr; ++t) {
-        const bool full = (nonlocal && c.use_kpp &&
-                           (t == c.idx_temperature || t == c.idx_salinity || t == c.idx_pseudo_salt)) ||
-                          (c.budgets && (t == c.idx_temperature || t == c.idx_salinity));
-        if (full || TPW == 1) tg.perm[n++] = (signed char)t;
+    if (TPW == 1) {
+        for (int t = 0; t < p.ntr; ++t) tg.perm[n++] = (signed char)t;
+        tg.single = n;
+        tg.ngroups = n;
+    } else {
+        const bool dep = nonlocal && c.use_kpp;
+        for (int cls = 0; cls < 3; ++cls)
+            for (int t = 0; t < p.ntr; ++t) {
+                const int k = (dep && (t == c.idx_salinity || t == c.idx_pseudo_salt)) ? 0
+                              : (dep && t == c.idx_temperature)                         ? 1
+                                                                                        : 2;
+                if (k == cls) tg.perm[n++] = (signed char)t;
+            }
+        tg.single = 0;
+        tg.ngroups = (p.ntr + TPW - 1) / TPW;
     }
-    tg.single = n;
-    for (int t = 0; t < p.ntr && TPW > 1; ++t) {
-        const bool full = (nonlocal && c.use_kpp &&
-                           (t == c.idx_temperature || t == c.idx_salinity || t == c.idx_pseudo_salt)) ||
-                          (c.budgets && (t == c.idx_temperature || t == c.idx_salinity));
-        if (!full) tg.perm[n++] = (signed char)t;
-    }
-    tg.ngroups = tg.single + (p.ntr - tg.single + TPW - 1) / TPW;
     const int ngx = (p.nx + MP_TR_COLS - 1) / MP_TR_COLS;
     const unsigned blocks = (unsigned)ngx * (unsigned)p.ny * (unsigned)tg.ngroups;
     if (is_default_tracer_knobs(p.cfg))
