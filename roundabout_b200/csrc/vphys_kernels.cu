@@ -776,20 +776,31 @@ __device__ __forceinline__ void solve_face(const Params &p, double dt, int i, in
     double cp_prev = 0.0, dp_prev = 0.0, gp_prev = 0.0;
     const double lam = (c.implicit_drag && !c.bbl_glue) ? (XF ? p.lambda_bot_u : p.lambda_bot_v)[f] : 0.0;
     const double inv_rho0 = 1.0 / c.rho0;
-    for (int k0 = 1; k0 <= nz; k0 += MOM_U) {
-        double hln[MOM_U], hrn[MOM_U], un[MOM_U], kvln[MOM_U], kvrn[MOM_U];
+    // level k + 1's data for row k; the loads of block k0 + MOM_U are issued
+    // before block k0 is computed (two register buffers; a block's d' stores
+    // go to its own levels, below the next block's loads)
+    auto load_up = [&](int k0, double (&hl_)[MOM_U], double (&hr_)[MOM_U], double (&u_)[MOM_U],
+                       double (&kl_)[MOM_U], double (&kr_)[MOM_U]) {
 #pragma unroll
         for (int q = 0; q < MOM_U; ++q) {
             const int k = k0 + q;
             if (k < nz) {
                 const size_t o = P * (size_t)k;
-                hln[q] = __ldg(hl + o);
-                hrn[q] = __ldg(hr + o);
-                kvln[q] = __ldg(kvl + o);
-                kvrn[q] = __ldg(kvr + o);
-                un[q] = uf[PF * (size_t)k];
+                hl_[q] = __ldg(hl + o);
+                hr_[q] = __ldg(hr + o);
+                kl_[q] = __ldg(kvl + o);
+                kr_[q] = __ldg(kvr + o);
+                u_[q] = uf[PF * (size_t)k];
+            } else {
+                hl_[q] = hr_[q] = kl_[q] = kr_[q] = u_[q] = 0.0;
             }
         }
+    };
+    double hln[MOM_U], hrn[MOM_U], un[MOM_U], kvln[MOM_U], kvrn[MOM_U];
+    load_up(1, hln, hrn, un, kvln, kvrn);
+    for (int k0 = 1; k0 <= nz; k0 += MOM_U) {
+        double hlx[MOM_U], hrx[MOM_U], ux[MOM_U], kvlx[MOM_U], kvrx[MOM_U];
+        load_up(k0 + MOM_U, hlx, hrx, ux, kvlx, kvrx);
 #pragma unroll
         for (int q = 0; q < MOM_U; ++q) {
             const int k = k0 + q;
@@ -855,22 +866,37 @@ __device__ __forceinline__ void solve_face(const Params &p, double dt, int i, in
                 u_k = u_kp1;
             }
         }
+#pragma unroll
+        for (int q = 0; q < MOM_U; ++q) {
+            hln[q] = hlx[q];
+            hrn[q] = hrx[q];
+            un[q] = ux[q];
+            kvln[q] = kvlx[q];
+            kvrn[q] = kvrx[q];
+        }
     }
-    // back-substitution (momentum into u, remnant into visc_rem)
+    // back-substitution (momentum into u, remnant into visc_rem); the d' of
+    // block k0 - MOM_U are loaded while block k0 is computed
     double u_next = dp_prev;
     double g_next = fmn(gp_prev, 1.0);
     uf[PF * (size_t)(nz - 1)] = u_next;
     if (vrem) vrem[PF * (size_t)(nz - 1)] = g_next;
-    for (int k0 = nz - 1; k0 >= 1; k0 -= MOM_U) {
-        double dps[MOM_U], gps[MOM_U];
+    auto load_down = [&](int k0, double (&d_)[MOM_U], double (&g_)[MOM_U]) {
 #pragma unroll
         for (int q = 0; q < MOM_U; ++q) {
             const int k = k0 - q;
+            d_[q] = g_[q] = 0.0;
             if (k >= 1) {
-                dps[q] = ld_hint(uf + PF * (size_t)(k - 1), pol_keep);
-                if (vrem) gps[q] = ld_hint(vrem + PF * (size_t)(k - 1), pol_keep);
+                d_[q] = ld_hint(uf + PF * (size_t)(k - 1), pol_keep);
+                if (vrem) g_[q] = ld_hint(vrem + PF * (size_t)(k - 1), pol_keep);
             }
         }
+    };
+    double dps[MOM_U], gps[MOM_U];
+    load_down(nz - 1, dps, gps);
+    for (int k0 = nz - 1; k0 >= 1; k0 -= MOM_U) {
+        double dpx[MOM_U], gpx[MOM_U];
+        load_down(k0 - MOM_U, dpx, gpx);
 #pragma unroll
         for (int q = 0; q < MOM_U; ++q) {
             const int k = k0 - q;
@@ -883,6 +909,11 @@ __device__ __forceinline__ void solve_face(const Params &p, double dt, int i, in
                     vrem[PF * (size_t)(k - 1)] = g_next;
                 }
             }
+        }
+#pragma unroll
+        for (int q = 0; q < MOM_U; ++q) {
+            dps[q] = dpx[q];
+            gps[q] = gpx[q];
         }
     }
 }

@@ -151,16 +151,21 @@ __device__ __forceinline__ void tracer_back(const Params &p, double dt, double *
     double g_above = 0.0, d_run = 0.0, h_a = 0.0;
     double h_c = (FULL && lo <= hi) ? __ldg(hp + P * (size_t)(hi - 1)) : 0.0;
     constexpr int BU = FULL ? MP_TR_UF : MP_TR_U;   // the deposit's registers leave room for fewer loads
-    for (int k0 = w_hi; k0 >= w_lo; k0 -= BU) {
-        // the block's old values and, with the deposit, the thicknesses one
-        // level down: loaded ahead, so no level waits on its own load
-        double dk[BU], hb[BU];
+    // a block's old values and, with the deposit, the thicknesses one level
+    // down, loaded while the block above is computed
+    auto load_down = [&](int k0, double (&db_)[BU], double (&hb_)[BU]) {
 #pragma unroll
         for (int u = 0; u < BU; ++u) {
             const int k = k0 - u;
-            dk[u] = (k >= lo && k <= hi) ? ld_hint(trc + P * (size_t)(k - 1), pol) : 0.0;
-            if (FULL) hb[u] = (k > 1 && k >= lo && k <= hi) ? __ldg(hp + P * (size_t)(k - 2)) : 0.0;
+            db_[u] = (k >= lo && k <= hi) ? ld_hint(trc + P * (size_t)(k - 1), pol) : 0.0;
+            if (FULL) hb_[u] = (k > 1 && k >= lo && k <= hi) ? __ldg(hp + P * (size_t)(k - 2)) : 0.0;
         }
+    };
+    double dk[BU], hb[BU];
+    load_down(w_hi, dk, hb);
+    for (int k0 = w_hi; k0 >= w_lo; k0 -= BU) {
+        double dx[BU], hx[BU];
+        load_down(k0 - BU, dx, hx);
 #pragma unroll
         for (int u = 0; u < BU; ++u) {
             const int k = k0 - u;
@@ -194,6 +199,11 @@ __device__ __forceinline__ void tracer_back(const Params &p, double dt, double *
                 h_c = h_bl;
             }
             trc[off] = x;
+        }
+#pragma unroll
+        for (int u = 0; u < BU; ++u) {
+            dk[u] = dx[u];
+            if (FULL) hb[u] = hx[u];
         }
     }
 }
@@ -247,16 +257,21 @@ __device__ __forceinline__ void tracer_back_group(const Params &p, double dt, do
     double d_run = 0.0, h_a = 0.0;
     double h_c = (lo <= hi) ? __ldg(hp + P * (size_t)(hi - 1)) : 0.0;
     constexpr int BU = MP_TR_U;
-    for (int k0 = w_hi; k0 >= w_lo; k0 -= BU) {
-        double dk[BU][TPW], hb[BU];
+    auto load_down = [&](int k0, double (&db_)[BU][TPW], double (&hb_)[BU]) {
 #pragma unroll
         for (int u = 0; u < BU; ++u) {
             const int k = k0 - u;
             const bool in = k >= lo && k <= hi;
 #pragma unroll
-            for (int q = 0; q < TPW; ++q) dk[u][q] = (in && q < nt) ? ld_hint(trc[q] + P * (size_t)(k - 1), pol) : 0.0;
-            hb[u] = (in && k > 1) ? __ldg(hp + P * (size_t)(k - 2)) : 0.0;
+            for (int q = 0; q < TPW; ++q) db_[u][q] = (in && q < nt) ? ld_hint(trc[q] + P * (size_t)(k - 1), pol) : 0.0;
+            hb_[u] = (in && k > 1) ? __ldg(hp + P * (size_t)(k - 2)) : 0.0;
         }
+    };
+    double dk[BU][TPW], hb[BU];
+    load_down(w_hi, dk, hb);
+    for (int k0 = w_hi; k0 >= w_lo; k0 -= BU) {
+        double dx[BU][TPW], hx[BU];
+        load_down(k0 - BU, dx, hx);
 #pragma unroll
         for (int u = 0; u < BU; ++u) {
             const int k = k0 - u;
@@ -296,6 +311,12 @@ __device__ __forceinline__ void tracer_back_group(const Params &p, double dt, do
             }
             h_a = h_c;
             h_c = h_bl;
+        }
+#pragma unroll
+        for (int u = 0; u < BU; ++u) {
+            hb[u] = hx[u];
+#pragma unroll
+            for (int q = 0; q < TPW; ++q) dk[u][q] = dx[u][q];
         }
     }
 }
@@ -393,18 +414,26 @@ __global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, doubl
             w[q] = 0.0;
         }
         float f_dn = 0.0f, q_prev = 1.0f, t_prev = 0.0f;
-        for (int k0 = w_lo; k0 <= w_hi; k0 += U) {
-            double hn[U], kn[U], dn[U][TPW];
+        // row k reads h, K and d one level up; the loads of block k0 + U are
+        // issued before block k0 is computed (two register buffers), so the
+        // first row of a block does not wait on its own loads
+        auto load_block = [&](int k0, double (&hb_)[U], double (&kb_)[U], double (&db_)[U][TPW]) {
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                const int k = k0 + u;   // row k reads h, K and d one level up
+                const int k = k0 + u;
                 const bool need = k + 1 >= lo && k + 1 <= hi;
                 const size_t o = P * (size_t)k;
-                hn[u] = need ? __ldg(hp + o) : 0.0;
-                kn[u] = need ? __ldg(Kp + o) : 0.0;
+                hb_[u] = need ? __ldg(hp + o) : 0.0;
+                kb_[u] = need ? __ldg(Kp + o) : 0.0;
 #pragma unroll
-                for (int q = 0; q < TPW; ++q) dn[u][q] = (need && q < nt) ? ld_hint(trc[q] + o, pol_keep) : 0.0;
+                for (int q = 0; q < TPW; ++q) db_[u][q] = (need && q < nt) ? ld_hint(trc[q] + o, pol_keep) : 0.0;
             }
+        };
+        double hn[U], kn[U], dn[U][TPW];
+        load_block(w_lo, hn, kn, dn);
+        for (int k0 = w_lo; k0 <= w_hi; k0 += U) {
+            double hx[U], kx[U], dx[U][TPW];
+            load_block(k0 + U, hx, kx, dx);
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const int k = k0 + u;
@@ -435,6 +464,13 @@ __global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, doubl
                 q_prev = qq;
                 f_dn = f_up;
                 h_c = hn[u];
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                hn[u] = hx[u];
+                kn[u] = kx[u];
+#pragma unroll
+                for (int q = 0; q < TPW; ++q) dn[u][q] = dx[u][q];
             }
         }
     }
@@ -478,16 +514,22 @@ __global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, doubl
         float delta[TPW];
 #pragma unroll
         for (int q = 0; q < TPW; ++q) delta[q] = 0.0f;
-        for (int k0 = w_hi; k0 >= w_lo; k0 -= U) {
-            double dk[U][TPW], hk[U];
+        // old values (and CI: thicknesses) of block k0 - U loaded while block k0 is computed
+        auto load_down = [&](int k0, double (&db_)[U][TPW], double (&hb_)[U]) {
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const int k = k0 - u;
 #pragma unroll
                 for (int q = 0; q < TPW; ++q)
-                    dk[u][q] = (k >= lo && k <= hi && q < nt) ? ld_hint(trc[q] + P * (size_t)(k - 1), pol_once) : 0.0;
-                if (CI) hk[u] = (k >= lo && k <= hi) ? __ldg(hp + P * (size_t)(k - 1)) : 0.0;
+                    db_[u][q] = (k >= lo && k <= hi && q < nt) ? ld_hint(trc[q] + P * (size_t)(k - 1), pol_once) : 0.0;
+                if (CI) hb_[u] = (k >= lo && k <= hi) ? __ldg(hp + P * (size_t)(k - 1)) : 0.0;
             }
+        };
+        double dk[U][TPW], hk[U];
+        load_down(w_hi, dk, hk);
+        for (int k0 = w_hi; k0 >= w_lo; k0 -= U) {
+            double dx[U][TPW], hx[U];
+            load_down(k0 - U, dx, hx);
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const int k = k0 - u;
@@ -502,6 +544,12 @@ __global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, doubl
 #pragma unroll
                 for (int q = 0; q < TPW; ++q)
                     if (q < nt) trc[q][off] = dk[u][q] + (double)delta[q];
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                hk[u] = hx[u];
+#pragma unroll
+                for (int q = 0; q < TPW; ++q) dk[u][q] = dx[u][q];
             }
         }
         if (CI && in_grid) {
@@ -637,16 +685,23 @@ __device__ __forceinline__ void tracer_back_rows(const Params &p, double dt, dou
     float delta = 0.0f;
     double g_above = 0.0, d_run = 0.0, h_a = 0.0;
     double h_c = (FULL && lo <= hi) ? __ldg(hp + P * (size_t)(hi - 1)) : 0.0;
-    for (int kb = (w_hi - 1) >> 3; kb >= ((w_lo - 1) >> 3); --kb) {
-        float t8[8], v8[8];
-        rows.load8(kb, t8, v8);
-        double dk[8], hb[8];   // old values and (deposit) the thicknesses one level down, loaded ahead
+    // old values and (deposit) the thicknesses one level down of row block
+    // kb - 1, loaded while block kb is computed
+    auto load_down = [&](int kb, double (&db_)[8], double (&hb_)[8]) {
 #pragma unroll
         for (int q = 7; q >= 0; --q) {
             const int k = 8 * kb + q + 1;
-            dk[q] = (k >= lo && k <= hi) ? ld_hint(trc + P * (size_t)(k - 1), pol) : 0.0;
-            if (FULL) hb[q] = (k > 1 && k >= lo && k <= hi) ? __ldg(hp + P * (size_t)(k - 2)) : 0.0;
+            db_[q] = (k >= lo && k <= hi) ? ld_hint(trc + P * (size_t)(k - 1), pol) : 0.0;
+            if (FULL) hb_[q] = (k > 1 && k >= lo && k <= hi) ? __ldg(hp + P * (size_t)(k - 2)) : 0.0;
         }
+    };
+    double dk[8], hb[8];
+    load_down((w_hi - 1) >> 3, dk, hb);
+    for (int kb = (w_hi - 1) >> 3; kb >= ((w_lo - 1) >> 3); --kb) {
+        float t8[8], v8[8];
+        rows.load8(kb, t8, v8);
+        double dx[8], hx[8];
+        load_down(kb - 1, dx, hx);
 #pragma unroll
         for (int q = 7; q >= 0; --q) {
             const int k = 8 * kb + q + 1;
@@ -674,6 +729,11 @@ __device__ __forceinline__ void tracer_back_rows(const Params &p, double dt, dou
                 h_c = h_bl;
             }
             trc[off] = x;
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            dk[q] = dx[q];
+            if (FULL) hb[q] = hx[q];
         }
     }
 }
@@ -713,17 +773,23 @@ __device__ __forceinline__ void tracer_item_tm(const Params &p, const vphys_conf
         double d_c = first ? ld_hint(trc + P * (size_t)(w_lo - 1), pol_keep) : 0.0;
         double d_m = 0.0, w = 0.0;
         float f_dn = 0.0f, q_prev = 1.0f, t_prev = 0.0f;
-        for (int k0 = w_lo; k0 <= w_hi; k0 += U) {
-            double hn[U], kn[U], dn[U];
+        // the loads of block k0 + U are issued before block k0 is computed
+        auto load_block = [&](int k0, double (&hb_)[U], double (&kb_)[U], double (&db_)[U]) {
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const int k = k0 + u;
                 const bool need = k + 1 >= lo && k + 1 <= hi;
                 const size_t o = P * (size_t)k;
-                hn[u] = need ? __ldg(hp + o) : 0.0;
-                kn[u] = need ? __ldg(Kp + o) : 0.0;
-                dn[u] = need ? ld_hint(trc + o, pol_keep) : 0.0;
+                hb_[u] = need ? __ldg(hp + o) : 0.0;
+                kb_[u] = need ? __ldg(Kp + o) : 0.0;
+                db_[u] = need ? ld_hint(trc + o, pol_keep) : 0.0;
             }
+        };
+        double hn[U], kn[U], dn[U];
+        load_block(w_lo, hn, kn, dn);
+        for (int k0 = w_lo; k0 <= w_hi; k0 += U) {
+            double hx[U], kx[U], dx[U];
+            load_block(k0 + U, hx, kx, dx);
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const int k = k0 + u;
@@ -746,6 +812,12 @@ __device__ __forceinline__ void tracer_item_tm(const Params &p, const vphys_conf
                 q_prev = qq;
                 f_dn = f_up;
                 h_c = hn[u];
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                hn[u] = hx[u];
+                kn[u] = kx[u];
+                dn[u] = dx[u];
             }
         }
     }
@@ -784,17 +856,8 @@ __device__ __forceinline__ void tracer_item_tm(const Params &p, const vphys_conf
     bool nl = live;
     double h_b = 0.0, q_kin = 0.0;
     if (nl) {
-        const double rho0 = c.rho0;
-        h_b = p.bl_depth[col];
-        const double u_star = sqrt(xdiv(p.stress_mag[col], rho0));
-        const double q_T_kin = kpp_q_t_kin(c, p.q_heat[col], p.sw_src + col, p.sw_kappa, col, p.plane, h_b,
-                                           __ldg(hp + P * (size_t)(hi - 1)));
-        const double q_S_kin = xdiv(p.q_salt[col], rho0);
-        const double B_0 = (GRAVITY / rho0) * (c.alpha_T * q_T_kin - c.beta_S * q_S_kin);
-        const double wstar3 = fmx(0.0, -B_0) * h_b;
-        const double w_star = sm_cbrt(wstar3);
-        const double w_s = sqrt(u_star * u_star + w_star * w_star);
-        nl = (h_b > 0.0 && w_s > 0.0 && B_0 < 0.0);
+        double q_T_kin, q_S_kin;
+        nl = nonlocal_column(p, c, col, hp, hi, h_b, q_T_kin, q_S_kin);
         q_kin = (tr == iT) ? q_T_kin : q_S_kin;
     }
     tracer_back_rows<true>(p, dt, trc, hp, rows, w_lo, w_hi, lo, hi, nl, h_b, q_kin, pol_once);

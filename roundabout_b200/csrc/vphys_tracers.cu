@@ -174,19 +174,27 @@ __device__ __forceinline__ void tracer_columns(const Params &p, double dt, int d
         double r_prev[NTR];
 #pragma unroll
         for (int t = 0; t < NTR; ++t) r_prev[t] = 0.0;
-        for (int k0 = w_lo; k0 <= w_hi; k0 += TR_U) {
-            double xs[TR_U][NTR], hps[TR_U], kap[TR_U], kbp[TR_U];
+        // the loads of block k0 + TR_U are issued before block k0 is computed
+        // (two register buffers; the block's stores go to its own levels)
+        auto load_up = [&](int k0, double (&xs_)[TR_U][NTR], double (&hps_)[TR_U], double (&kap_)[TR_U],
+                           double (&kbp_)[TR_U]) {
 #pragma unroll
             for (int u = 0; u < TR_U; ++u) {
                 const int k = k0 + u;
                 const bool act = live && k >= k_lo && k <= k_hi;
                 const size_t off = P * (size_t)(k - 1);
-                hps[u] = (act && k < nz) ? __ldg(hp + off + P) : 0.0;
-                kap[u] = (act && k < nz) ? ld_hint(KA + off + P, pol_once) : 0.0;
-                if (TWO) kbp[u] = (act && k < nz) ? ld_hint(KB + off + P, pol_once) : 0.0;
+                hps_[u] = (act && k < nz) ? __ldg(hp + off + P) : 0.0;
+                kap_[u] = (act && k < nz) ? ld_hint(KA + off + P, pol_once) : 0.0;
+                kbp_[u] = (TWO && act && k < nz) ? ld_hint(KB + off + P, pol_once) : 0.0;
 #pragma unroll
-                for (int t = 0; t < NTR; ++t) xs[u][t] = (act && t < ntr) ? trc[t][off] : 0.0;
+                for (int t = 0; t < NTR; ++t) xs_[u][t] = (act && t < ntr) ? trc[t][off] : 0.0;
             }
+        };
+        double xs[TR_U][NTR], hps[TR_U], kap[TR_U], kbp[TR_U];
+        load_up(w_lo, xs, hps, kap, kbp);
+        for (int k0 = w_lo; k0 <= w_hi; k0 += TR_U) {
+            double xs_n[TR_U][NTR], hps_n[TR_U], kap_n[TR_U], kbp_n[TR_U];
+            load_up(k0 + TR_U, xs_n, hps_n, kap_n, kbp_n);
 #pragma unroll
             for (int u = 0; u < TR_U; ++u) {
                 const int k = k0 + u;
@@ -231,6 +239,14 @@ __device__ __forceinline__ void tracer_columns(const Params &p, double dt, int d
                     h_c = h_p;
                 }
             }
+#pragma unroll
+            for (int u = 0; u < TR_U; ++u) {
+                hps[u] = hps_n[u];
+                kap[u] = kap_n[u];
+                kbp[u] = kbp_n[u];
+#pragma unroll
+                for (int t = 0; t < NTR; ++t) xs[u][t] = xs_n[u][t];
+            }
         }
     }
 
@@ -266,20 +282,26 @@ __device__ __forceinline__ void tracer_columns(const Params &p, double dt, int d
     double gT_above = 0.0, gS_above = 0.0;
     double d_run = 0.0;
     double h_c = h_hi, h_a = 0.0;   // layer above k_hi is vanished: its flux is closed
-    for (int k0 = w_hi; k0 >= w_lo; k0 -= TR_U) {
-        double rs[TR_U][NTR], hbs[TR_U];
+    // the loads of block k0 - TR_U are issued before block k0 is computed
+    auto load_down = [&](int k0, double (&rs_)[TR_U][NTR], double (&hbs_)[TR_U]) {
 #pragma unroll
         for (int u = 0; u < TR_U; ++u) {
             const int k = k0 - u;
             const bool act = live && k >= k_lo && k <= k_hi;
             const size_t off = P * (size_t)(k - 1);
-            hbs[u] = (act && k > 1) ? __ldg(hp + off - P) : 0.0;
+            hbs_[u] = (act && k > 1) ? __ldg(hp + off - P) : 0.0;
 #pragma unroll
             for (int t = 0; t < NTR; ++t)
-                rs[u][t] = (act && t < ntr && (diffuse || t == iT || t == iS || t == iPS))
-                               ? ld_hint((diffuse ? rbuf[t] : trc[t]) + off, pol_keep)
-                               : 0.0;
+                rs_[u][t] = (act && t < ntr && (diffuse || t == iT || t == iS || t == iPS))
+                                ? ld_hint((diffuse ? rbuf[t] : trc[t]) + off, pol_keep)
+                                : 0.0;
         }
+    };
+    double rs[TR_U][NTR], hbs[TR_U];
+    load_down(w_hi, rs, hbs);
+    for (int k0 = w_hi; k0 >= w_lo; k0 -= TR_U) {
+        double rs_n[TR_U][NTR], hbs_n[TR_U];
+        load_down(k0 - TR_U, rs_n, hbs_n);
 #pragma unroll
         for (int u = 0; u < TR_U; ++u) {
             const int k = k0 - u;
@@ -342,6 +364,12 @@ __device__ __forceinline__ void tracer_columns(const Params &p, double dt, int d
                 h_a = h_c;
                 h_c = h_bl;
             }
+        }
+#pragma unroll
+        for (int u = 0; u < TR_U; ++u) {
+            hbs[u] = hbs_n[u];
+#pragma unroll
+            for (int t = 0; t < NTR; ++t) rs[u][t] = rs_n[u][t];
         }
     }
     if (CI && diffuse && in_grid) {
