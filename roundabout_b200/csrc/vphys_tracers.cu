@@ -91,6 +91,15 @@ __device__ __forceinline__ void tracer_columns(const Params &p, double dt, int d
 #else
     constexpr int TR_U = NTR <= 8 ? 2 : 1;
 #endif
+    // PIPE: the loads of the next level block are issued before the current
+    // block is computed (two register buffers).  Up to VPHYS_TR_PIPE_MAX
+    // tracers per thread; above it the doubled load code of the unrolled
+    // tracer loop costs more than the overlap gains, and each block loads
+    // just before its arithmetic.
+#ifndef VPHYS_TR_PIPE_MAX
+#define VPHYS_TR_PIPE_MAX 4
+#endif
+    constexpr bool PIPE = NTR <= VPHYS_TR_PIPE_MAX;
     vphys_config cd = p.cfg;   // DEF: the default knobs folded in (is_default_tracer_knobs)
     if (DEF) default_tracer_knobs(cd);
     const vphys_config &c = cd;
@@ -191,10 +200,13 @@ __device__ __forceinline__ void tracer_columns(const Params &p, double dt, int d
             }
         };
         double xs[TR_U][NTR], hps[TR_U], kap[TR_U], kbp[TR_U];
-        load_up(w_lo, xs, hps, kap, kbp);
+        if constexpr (PIPE) load_up(w_lo, xs, hps, kap, kbp);
         for (int k0 = w_lo; k0 <= w_hi; k0 += TR_U) {
             double xs_n[TR_U][NTR], hps_n[TR_U], kap_n[TR_U], kbp_n[TR_U];
-            load_up(k0 + TR_U, xs_n, hps_n, kap_n, kbp_n);
+            if constexpr (PIPE)
+                load_up(k0 + TR_U, xs_n, hps_n, kap_n, kbp_n);
+            else
+                load_up(k0, xs, hps, kap, kbp);
 #pragma unroll
             for (int u = 0; u < TR_U; ++u) {
                 const int k = k0 + u;
@@ -239,13 +251,15 @@ __device__ __forceinline__ void tracer_columns(const Params &p, double dt, int d
                     h_c = h_p;
                 }
             }
+            if constexpr (PIPE) {
 #pragma unroll
-            for (int u = 0; u < TR_U; ++u) {
-                hps[u] = hps_n[u];
-                kap[u] = kap_n[u];
-                kbp[u] = kbp_n[u];
+                for (int u = 0; u < TR_U; ++u) {
+                    hps[u] = hps_n[u];
+                    kap[u] = kap_n[u];
+                    kbp[u] = kbp_n[u];
 #pragma unroll
-                for (int t = 0; t < NTR; ++t) xs[u][t] = xs_n[u][t];
+                    for (int t = 0; t < NTR; ++t) xs[u][t] = xs_n[u][t];
+                }
             }
         }
     }
@@ -298,10 +312,13 @@ __device__ __forceinline__ void tracer_columns(const Params &p, double dt, int d
         }
     };
     double rs[TR_U][NTR], hbs[TR_U];
-    load_down(w_hi, rs, hbs);
+    if constexpr (PIPE) load_down(w_hi, rs, hbs);
     for (int k0 = w_hi; k0 >= w_lo; k0 -= TR_U) {
         double rs_n[TR_U][NTR], hbs_n[TR_U];
-        load_down(k0 - TR_U, rs_n, hbs_n);
+        if constexpr (PIPE)
+            load_down(k0 - TR_U, rs_n, hbs_n);
+        else
+            load_down(k0, rs, hbs);
 #pragma unroll
         for (int u = 0; u < TR_U; ++u) {
             const int k = k0 - u;
@@ -365,11 +382,13 @@ __device__ __forceinline__ void tracer_columns(const Params &p, double dt, int d
                 h_c = h_bl;
             }
         }
+        if constexpr (PIPE) {
 #pragma unroll
-        for (int u = 0; u < TR_U; ++u) {
-            hbs[u] = hbs_n[u];
+            for (int u = 0; u < TR_U; ++u) {
+                hbs[u] = hbs_n[u];
 #pragma unroll
-            for (int t = 0; t < NTR; ++t) rs[u][t] = rs_n[u][t];
+                for (int t = 0; t < NTR; ++t) rs[u][t] = rs_n[u][t];
+            }
         }
     }
     if (CI && diffuse && in_grid) {
