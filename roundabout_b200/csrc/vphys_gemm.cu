@@ -133,32 +133,74 @@ __device__ __forceinline__ float tanh_hw(float x)
     asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
 }
+// GELU, tanh form (Hendrycks & Gimpel 2016): 0.5 x (1 + tanh(c (x + 0.044715 x^3))),
+// c = sqrt(2/pi), with the argument as x (c + c 0.044715 x^2) and the result as
+// hx + hx t (hx = x / 2): three multiply-adds around the hardware tanh
+constexpr float GELU_C0 = 0.7978845608028654f;
+constexpr float GELU_C1 = 0.7978845608028654f * 0.044715f;
+__device__ __forceinline__ float gelu_arg(float x) { return x * fmaf(GELU_C1, x * x, GELU_C0); }
 __device__ __forceinline__ float gelu_tanh(float x)
 {
-    // GELU, tanh form (Hendrycks & Gimpel 2016)
-    const float c = 0.7978845608028654f;   // sqrt(2/pi)
-    const float t = tanh_hw(c * (x + 0.044715f * x * x * x));
-    return 0.5f * x * (1.0f + t);
+    const float t = tanh_hw(gelu_arg(x));
+    const float hx = 0.5f * x;
+    return fmaf(hx, t, hx);
 }
 __device__ __forceinline__ float gelu_tanh_grad(float x)
 {
-    const float c = 0.7978845608028654f;
-    const float t = tanh_hw(c * (x + 0.044715f * x * x * x));
-    return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * c * (1.0f + 3.0f * 0.044715f * x * x);
+    const float t = tanh_hw(gelu_arg(x));
+    return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * GELU_C0 * (1.0f + 3.0f * 0.044715f * x * x);
 }
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar)
 {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16])
+__device__ __forceinline__ void tmem_ld16_async(uint32_t taddr, uint32_t (&r)[16])
 {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
           "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
         : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16])
+{
+    tmem_ld16_async(taddr, r);
+    tmem_ld_wait();
+}
+
+// The inference epilogues (vphys_kpp's in-step forward: alpha = 1, a bias,
+// no gradient input, row-major 16-byte-aligned outputs only), without the
+// general epilogue's per-element option tests.  EP 1: a hidden layer, BF16 of
+// GELU(v + bias); EP 2: the output layer, FP32 v + bias.
+template <int EP>
+__device__ __forceinline__ void epilogue16_inf(const GemmEpi &g, int row, int c0, const uint32_t (&r)[16])
+{
+    float b[16];
+    const float4 *b4 = reinterpret_cast<const float4 *>(g.bias + c0);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const float4 v = __ldg(b4 + q);
+        b[4 * q] = v.x, b[4 * q + 1] = v.y, b[4 * q + 2] = v.z, b[4 * q + 3] = v.w;
+    }
+    if (EP == 1) {
+        __nv_bfloat162 pk[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+            pk[q] = __floats2bfloat162_rn(gelu_tanh(__uint_as_float(r[2 * q]) + b[2 * q]),
+                                          gelu_tanh(__uint_as_float(r[2 * q + 1]) + b[2 * q + 1]));
+        uint4 *o4 = reinterpret_cast<uint4 *>(g.out_bf16 + (size_t)row * g.ld_bf16 + c0);
+        o4[0] = *reinterpret_cast<uint4 *>(&pk[0]);
+        o4[1] = *reinterpret_cast<uint4 *>(&pk[4]);
+    } else {
+        float4 *o4 = reinterpret_cast<float4 *>(g.out_f32 + (size_t)row * g.ld_f32 + c0);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            o4[q] = make_float4(__uint_as_float(r[4 * q]) + b[4 * q], __uint_as_float(r[4 * q + 1]) + b[4 * q + 1],
+                                __uint_as_float(r[4 * q + 2]) + b[4 * q + 2],
+                                __uint_as_float(r[4 * q + 3]) + b[4 * q + 3]);
+    }
 }
 
 // epilogue of one 16-column chunk of one row (v[] = accumulator values)
@@ -209,6 +251,8 @@ __device__ __forceinline__ void epilogue16(const GemmEpi &g, int row, int c0, co
     }
 }
 
+// EP: 0 the general epilogue (training), 1 / 2 the inference epilogues
+template <int EP>
 __global__ void __launch_bounds__(GEMM_THREADS, 1)
     k_gemm_tn(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const GemmEpi g)
 {
@@ -356,10 +400,26 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             if (!ok || *abort_v) break;
             const int row = ((int)blockIdx.x + t * (int)gridDim.x) * GM + quarter * 32 + lane;
-            for (int c0 = half * 16; c0 < N; c0 += 32) {
-                uint32_t r[16];
-                tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(a * GN_MAX + c0), r);
-                if (row < g.M) epilogue16(g, row, c0, r);
+            const uint32_t tl = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(a * GN_MAX);
+            if (EP == 0) {
+                for (int c0 = half * 16; c0 < N; c0 += 32) {
+                    uint32_t r[16];
+                    tmem_ld16(tl + (uint32_t)c0, r);
+                    if (row < g.M) epilogue16(g, row, c0, r);
+                }
+            } else {
+                // two chunks per wait: the second load overlaps the first's latency
+                for (int c0 = half * 16; c0 < N; c0 += 64) {
+                    uint32_t r0[16], r1[16];
+                    const bool two = c0 + 32 < N;
+                    tmem_ld16_async(tl + (uint32_t)c0, r0);
+                    if (two) tmem_ld16_async(tl + (uint32_t)(c0 + 32), r1);
+                    tmem_ld_wait();
+                    if (row < g.M) {
+                        epilogue16_inf<EP>(g, row, c0, r0);
+                        if (two) epilogue16_inf<EP>(g, row, c0 + 32, r1);
+                    }
+                }
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
@@ -420,7 +480,9 @@ int gemm_tn_bf16(const void *A, long long lda, const void *B, long long ldb, int
         return report_error(VPHYS_ERR_CUDA, "vphys_gemm_tn_bf16: cuTensorMapEncodeTiled failed");
     static bool attr_set = false;
     if (!attr_set) {
-        cudaFuncSetAttribute(k_gemm_tn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM);
+        cudaFuncSetAttribute(k_gemm_tn<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM);
+        cudaFuncSetAttribute(k_gemm_tn<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM);
+        cudaFuncSetAttribute(k_gemm_tn<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GEMM_SMEM);
         attr_set = true;
     }
     GemmEpi g{};
@@ -450,7 +512,16 @@ int gemm_tn_bf16(const void *A, long long lda, const void *B, long long ldb, int
         if (sms <= 0) sms = 148;
     }
     const int tiles = (M + GM - 1) / GM;
-    k_gemm_tn<<<tiles < sms ? tiles : sms, GEMM_THREADS, GEMM_SMEM, stream>>>(ma, mb, g);
+    const int grid = tiles < sms ? tiles : sms;
+    // the inference forms: alpha 1, a 16-byte-aligned bias, no gradient
+    // input, one row-major vector output
+    const bool inf = alpha == 1.0f && bias && ((((uintptr_t)bias) & 15) == 0) && !zin && !out_bf16_t && g.vec;
+    if (inf && act && out_bf16 && !out_f32)
+        k_gemm_tn<1><<<grid, GEMM_THREADS, GEMM_SMEM, stream>>>(ma, mb, g);
+    else if (inf && !act && out_f32 && !out_bf16)
+        k_gemm_tn<2><<<grid, GEMM_THREADS, GEMM_SMEM, stream>>>(ma, mb, g);
+    else
+        k_gemm_tn<0><<<grid, GEMM_THREADS, GEMM_SMEM, stream>>>(ma, mb, g);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return report_error(VPHYS_ERR_CUDA, cudaGetErrorString(e));
     return VPHYS_OK;
