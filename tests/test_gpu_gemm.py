@@ -83,6 +83,37 @@ def test_gemm_epilogue_gelu_bias_transposed(env):
     assert torch.equal(o16t, o16.T.contiguous())
 
 
+@pytest.mark.parametrize("M,N,K", [(1000, 256, 160), (777, 256, 256)])
+def test_gemm_inference_hidden_layer(env, M, N, K):
+    """The hidden-layer inference form (alpha 1, bias, GELU, BF16 output only)
+    against the general form of the same product and torch."""
+    torch = env[0]
+    g = torch.Generator(device="cuda").manual_seed(M + N + K)
+    A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
+    B = (0.1 * torch.randn(N, K, device="cuda", generator=g)).to(torch.bfloat16)
+    bias = torch.randn(N, device="cuda", generator=g)
+    _, o16, _ = run(env, A, B, bias=bias, act=1, f32=False, bf16=True)
+    _, o16g, _ = run(env, A, B, bias=bias, act=1, f32=True, bf16=True)   # the general epilogue
+    assert torch.equal(o16, o16g)
+    a = gelu(A.float() @ B.float().T + bias)
+    tol = 2e-3 * float(a.abs().max()) + 1e-2 * float(a.abs().max()) / 128
+    assert float((o16.float() - a).abs().max()) <= tol
+
+
+@pytest.mark.parametrize("M,N,K", [(1000, 80, 256), (4099, 80, 256)])
+def test_gemm_inference_output_layer(env, M, N, K):
+    """The output-layer inference form (alpha 1, bias, FP32 output only)."""
+    torch = env[0]
+    g = torch.Generator(device="cuda").manual_seed(M + 3 * N + K)
+    A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
+    B = torch.randn(N, K, device="cuda", generator=g).to(torch.bfloat16)
+    bias = torch.randn(N, device="cuda", generator=g)
+    o32, _, _ = run(env, A, B, bias=bias)
+    ref = A.float() @ B.float().T + bias
+    assert float((o32 - ref).abs().max()) <= 2e-3 * float(ref.abs().max())
+    assert not torch.isnan(o32).any()
+
+
 def test_gemm_epilogue_gelu_backward(env):
     torch = env[0]
     M, N, K = 333, 256, 80
