@@ -472,6 +472,34 @@ __device__ __forceinline__ double conc_add_source(double c, double h, double src
 {
     return (h > H_VANISHED) ? c + xdiv(src, h + H_DIV_EPS) : c;
 }
+// the same with the quotient from r = rcp_of(h + H_DIV_EPS), made once for
+// the tracers a layer deposits into (qdiv(src, r) is src / (h + H_DIV_EPS)
+// bit for bit)
+__device__ __forceinline__ double conc_add_source_r(double c, double h, double src, const Rcp &r)
+{
+    return (h > H_VANISHED) ? c + qdiv(src, r) : c;
+}
+
+// 1 / b for the mixed-precision solves, which carry no bitwise contract:
+// the hardware's approximate FP64 reciprocal refined by two Newton-Raphson
+// steps y <- y + y (1 - b y), each of which squares the relative error, so
+// the result is within an ulp or two of 1/b (b positive and normal here: a
+// layer thickness plus H_DIV_EPS, a boundary-layer depth)
+__device__ __forceinline__ double rcp_nr(double b)
+{
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
+    double e = fma(-b, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-b, y, 1.0);
+    return fma(y, e, y);
+}
+// conc_add_source of the mixed-precision solves: the quotient as a product
+// with r = rcp_nr(h + H_DIV_EPS)
+__device__ __forceinline__ double conc_add_source_mp(double c, double h, double src, double r)
+{
+    return (h > H_VANISHED) ? c + src * r : c;
+}
 
 // nonlocal_face_flux (rdb_ocean_vmix.F90:1694-1714)
 __device__ __forceinline__ double nonlocal_face_flux(double gamma, double h_below, double h_above)

@@ -150,6 +150,7 @@ __device__ __forceinline__ void tracer_back(const Params &p, double dt, double *
     float delta = 0.0f;
     double g_above = 0.0, d_run = 0.0, h_a = 0.0;
     double h_c = (FULL && lo <= hi) ? __ldg(hp + P * (size_t)(hi - 1)) : 0.0;
+    const double r_hb = (FULL && nl) ? rcp_nr(h_b) : 0.0;   // sigma = d_run / h_b as a product
     constexpr int BU = FULL ? MP_TR_UF : MP_TR_U;   // the deposit's registers leave room for fewer loads
     // a block's old values and, with the deposit, the thicknesses one level
     // down, loaded while the block above is computed
@@ -184,14 +185,15 @@ __device__ __forceinline__ void tracer_back(const Params &p, double dt, double *
                     if (nl) {
                         d_run = d_run + h_c;
                         if (k > 1 && d_run < h_b) {
-                            const double sigma = xdiv(d_run, h_b);
+                            const double sigma = d_run * r_hb;
                             gk = p.cfg.cs_nonlocal * (sigma * (1.0 - sigma) * (1.0 - sigma)) * q_kin;
                         }
                     }
                     double f_up = 0.0, f_dn = 0.0;
                     if (k < nz) f_up = nonlocal_face_flux(g_above, h_c, h_a);
                     if (k > 1) f_dn = nonlocal_face_flux(gk, h_bl, h_c);
-                    x = conc_add_source(x, h_c, dt * (f_up - f_dn));
+                    const double src = dt * (f_up - f_dn);
+                    if (src != 0.0) x = conc_add_source_mp(x, h_c, src, rcp_nr(h_c + H_DIV_EPS));
                     g_above = gk;
                 }
                 if (CI) neumaier_add(*c_new, *e_new, h_c * x);
@@ -256,6 +258,10 @@ __device__ __forceinline__ void tracer_back_group(const Params &p, double dt, do
     for (int q = 0; q < TPW; ++q) delta[q] = 0.0f, g_above[q] = 0.0;
     double d_run = 0.0, h_a = 0.0;
     double h_c = (lo <= hi) ? __ldg(hp + P * (size_t)(hi - 1)) : 0.0;
+    const double r_hb = nl ? rcp_nr(h_b) : 0.0;   // sigma = d_run / h_b as a product
+    bool any_dep = false;
+#pragma unroll
+    for (int q = 0; q < TPW; ++q) any_dep = any_dep || dep[q];
     constexpr int BU = MP_TR_U;
     auto load_down = [&](int k0, double (&db_)[BU][TPW], double (&hb_)[BU]) {
 #pragma unroll
@@ -288,11 +294,13 @@ __device__ __forceinline__ void tracer_back_group(const Params &p, double dt, do
             if (nl) {
                 d_run = d_run + h_c;
                 if (k > 1 && d_run < h_b) {
-                    const double sigma = xdiv(d_run, h_b);
+                    const double sigma = d_run * r_hb;
                     shape = p.cfg.cs_nonlocal * (sigma * (1.0 - sigma) * (1.0 - sigma));
                     in_bl = true;
                 }
             }
+            // one reciprocal of the layer for every tracer's deposit
+            const double r_h = any_dep ? rcp_nr(h_c + H_DIV_EPS) : 0.0;
 #pragma unroll
             for (int q = 0; q < TPW; ++q) {
                 if (q >= nt) break;
@@ -304,7 +312,7 @@ __device__ __forceinline__ void tracer_back_group(const Params &p, double dt, do
                     double f_up = 0.0, f_dn = 0.0;
                     if (k < nz) f_up = nonlocal_face_flux(g_above[q], h_c, h_a);
                     if (k > 1) f_dn = nonlocal_face_flux(gk, h_bl, h_c);
-                    x = conc_add_source(x, h_c, dt * (f_up - f_dn));
+                    x = conc_add_source_mp(x, h_c, dt * (f_up - f_dn), r_h);
                     g_above[q] = gk;
                 }
                 trc[q][off] = x;
@@ -685,6 +693,7 @@ __device__ __forceinline__ void tracer_back_rows(const Params &p, double dt, dou
     float delta = 0.0f;
     double g_above = 0.0, d_run = 0.0, h_a = 0.0;
     double h_c = (FULL && lo <= hi) ? __ldg(hp + P * (size_t)(hi - 1)) : 0.0;
+    const double r_hb = (FULL && nl) ? rcp_nr(h_b) : 0.0;   // sigma = d_run / h_b as a product
     // old values and (deposit) the thicknesses one level down of row block
     // kb - 1, loaded while block kb is computed
     auto load_down = [&](int kb, double (&db_)[8], double (&hb_)[8]) {
@@ -716,14 +725,15 @@ __device__ __forceinline__ void tracer_back_rows(const Params &p, double dt, dou
                 if (nl) {
                     d_run = d_run + h_c;
                     if (k > 1 && d_run < h_b) {
-                        const double sigma = xdiv(d_run, h_b);
+                        const double sigma = d_run * r_hb;
                         gk = p.cfg.cs_nonlocal * (sigma * (1.0 - sigma) * (1.0 - sigma)) * q_kin;
                     }
                 }
                 double f_up = 0.0, f_dn = 0.0;
                 if (k < nz) f_up = nonlocal_face_flux(g_above, h_c, h_a);
                 if (k > 1) f_dn = nonlocal_face_flux(gk, h_bl, h_c);
-                x = conc_add_source(x, h_c, dt * (f_up - f_dn));
+                const double src = dt * (f_up - f_dn);
+                if (src != 0.0) x = conc_add_source_mp(x, h_c, src, rcp_nr(h_c + H_DIV_EPS));
                 g_above = gk;
                 h_a = h_c;
                 h_c = h_bl;

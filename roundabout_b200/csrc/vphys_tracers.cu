@@ -296,6 +296,8 @@ __device__ __forceinline__ void tracer_columns(const Params &p, double dt, int d
     double gT_above = 0.0, gS_above = 0.0;
     double d_run = 0.0;
     double h_c = h_hi, h_a = 0.0;   // layer above k_hi is vanished: its flux is closed
+    // sigma = d_run / h_b with one reciprocal per column (qdiv: the quotient bit for bit)
+    const Rcp r_hb = rcp_of(nl ? h_b : 1.0);
     // the loads of block k0 - TR_U are issued before block k0 is computed
     auto load_down = [&](int k0, double (&rs_)[TR_U][NTR], double (&hbs_)[TR_U]) {
 #pragma unroll
@@ -331,7 +333,7 @@ __device__ __forceinline__ void tracer_columns(const Params &p, double dt, int d
                 if (nl) {
                     d_run = d_run + h_c;
                     if (k > 1 && d_run < h_b) {
-                        const double sigma = xdiv(d_run, h_b);
+                        const double sigma = qdiv(d_run, r_hb);
                         const double g_shape = sigma * (1.0 - sigma) * (1.0 - sigma);
                         const double gamma_factor = c.cs_nonlocal * g_shape;
                         gT = gamma_factor * q_T_kin;
@@ -352,6 +354,15 @@ __device__ __forceinline__ void tracer_columns(const Params &p, double dt, int d
                     fT = dt * (fT_up - fT_dn);
                     fS = dt * (fS_up - fS_dn);
                 }
+                // conc_add_source's quotients src / (h + H_DIV_EPS), one reciprocal for
+                // the layer (salinity and pseudo-salt share fS); a zero source adds
+                // itself, as xdiv(+-0, b > 0) = +-0
+                double incT = fT, incS = fS;
+                if (do_nl && (fT != 0.0 || fS != 0.0)) {
+                    const Rcp r_h = rcp_of(h_c + H_DIV_EPS);
+                    if (fT != 0.0) incT = qdiv(fT, r_h);
+                    if (fS != 0.0) incS = qdiv(fS, r_h);
+                }
 #pragma unroll
                 for (int t = 0; t < NTR; ++t) {
                     if (t < ntr && (diffuse || t == iT || t == iS || t == iPS)) {
@@ -368,9 +379,9 @@ __device__ __forceinline__ void tracer_columns(const Params &p, double dt, int d
                                 bud[off] = bud[off] + (p_new - p_old);
                             }
                         }
-                        if (do_nl) {
-                            if (t == iT) x = conc_add_source(x, h_c, fT);
-                            else if (t == iS || t == iPS) x = conc_add_source(x, h_c, fS);
+                        if (do_nl && h_c > H_VANISHED) {
+                            if (t == iT) x = x + incT;
+                            else if (t == iS || t == iPS) x = x + incS;
                         }
                         if (CI && diffuse) neumaier_add(c_new[t], e_new[t], h_c * x);
                         trc[t][off] = x;

@@ -96,8 +96,9 @@ def test_gemm_inference_hidden_layer(env, M, N, K):
     _, o16g, _ = run(env, A, B, bias=bias, act=1, f32=True, bf16=True)   # the general epilogue
     assert torch.equal(o16, o16g)
     a = gelu(A.float() @ B.float().T + bias)
-    tol = 2e-3 * float(a.abs().max()) + 1e-2 * float(a.abs().max()) / 128
-    assert float((o16.float() - a).abs().max()) <= tol
+    # the accumulation order (2e-3 of the scale) plus half a BF16 ulp of each value
+    tol = 2e-3 * float(a.abs().max()) + a.abs() / 256
+    assert bool(((o16.float() - a).abs() <= tol).all())
 
 
 @pytest.mark.parametrize("M,N,K", [(1000, 80, 256), (4099, 80, 256)])
