@@ -421,7 +421,9 @@ def main():
                  "momentum": ("k_column_depth+k_mom_tile_flags+k_momentum_mp_tma"
                               if mixed and (tune or {}).get("chosen", {}).get("momentum") == "tma_ring"
                               else ("k_column_depth+k_momentum_mp" if mixed else "k_column_depth+k_momentum")),
-                 "tracers": "k_spans+k_tracers_mp+k_tracers_redo" if mixed else "k_tracers"}
+                 "tracers": (("k_spans+k_tracers_mp_tm+k_tracers_redo"
+                              if (tune or {}).get("chosen", {}).get("tracers") == "tmem_rows"
+                              else "k_spans+k_tracers_mp+k_tracers_redo") if mixed else "k_tracers")}
     dom = max(("assemble", "momentum", "tracers", "eos"), key=lambda k: stage_ms[k])
     peak, peak_kind = peaks()
     achieved = bpc[dom] * cells / (stage_ms[dom] / 1e3) / 1e9

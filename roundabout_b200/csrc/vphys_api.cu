@@ -80,7 +80,7 @@ struct vphys_handle_s {
     unsigned *work_ctr = nullptr;     // the work counter of the dynamically scheduled mixed tracer solve
     // kernel variants of the mixed solves (vphys_autotune); the defaults are
     // the faster ones on 1440x1080x75 with 4 tracers
-    int var_mom = vphys::VAR_MOM_RING;
+    int var_mom = vphys::VAR_MOM_REGISTER;
     int var_tr = vphys::VAR_TR_SMEM1;
     double *zcol = nullptr;           // column depths for the momentum face thickness
     unsigned char *mom_tiles = nullptr;   // skip flags of the TMA-staged momentum solve's face tiles

@@ -55,7 +55,15 @@ constexpr int MP_TR_COLS = 32;      // columns (lanes) per tracer block
 #define VPHYS_MP_MOM_THREADS 32
 #endif
 #ifndef VPHYS_MP_MOM_U
-#define VPHYS_MP_MOM_U 6   // 1440x1080x75 default-knob solve: 3.10 ms with 4, 2.87 with 6 or 8 (still 11 warps/SM)
+// levels per load block of the register face solve, whose loads of the next
+// block are in flight during the current one (1440x1080x75: 2.57 ms with 4,
+// 2.65 with 6, 3.31 with 8 -- registers; before the pipelining 2.87 with 6)
+#define VPHYS_MP_MOM_U 4
+#endif
+#ifndef VPHYS_MP_MOM_UB
+// levels per load block of the ring face solve's back-substitution
+// (1440x1080x75: 2.84 ms with 4, 2.75 with 6, 2.69 with 8)
+#define VPHYS_MP_MOM_UB 8
 #endif
 constexpr int MP_TR_U = VPHYS_MP_TR_U;                // levels per tracer load block
 #ifndef VPHYS_MP_TR_UF
@@ -64,6 +72,7 @@ constexpr int MP_TR_U = VPHYS_MP_TR_U;                // levels per tracer load 
 constexpr int MP_TR_UF = VPHYS_MP_TR_UF;   // levels per load block of the back-substitution with the non-local deposit
 constexpr int MP_MOM_THREADS = VPHYS_MP_MOM_THREADS;  // face columns per momentum block
 constexpr int MP_MOM_U = VPHYS_MP_MOM_U;              // levels per momentum load block
+constexpr int MP_MOM_UB = VPHYS_MP_MOM_UB;            // levels per load block of the ring solve's back-substitution
 // Largest tracer increment (in the tracer's units) a mixed solve keeps.  The
 // FP32 couplings and the FP32 back-substitution leave an error of about
 // 3 eps_32 |delta| (eps_32 = 6e-8): 2 units keep it under 4e-7.  A column
@@ -1039,20 +1048,29 @@ __device__ __forceinline__ void solve_face_mp(const Params &p, double dt, int i,
     // and the FP64 forward accumulations of the increment and of the remnant
     float f_prev = 0.0f, q_prev = 1.0f, t_prev = 0.0f;
     double w = 0.0, wr = 0.0;
-    for (int k0 = 1; k0 <= nz; k0 += MP_MOM_U) {
-        double hln[MP_MOM_U], hrn[MP_MOM_U], un[MP_MOM_U], kvln[MP_MOM_U], kvrn[MP_MOM_U];
+    // level k + 1's data for row k; the loads of block k0 + MP_MOM_U are
+    // issued before block k0 is computed (two register buffers)
+    auto load_up = [&](int k0, double (&hl_)[MP_MOM_U], double (&hr_)[MP_MOM_U], double (&u_)[MP_MOM_U],
+                       double (&kl_)[MP_MOM_U], double (&kr_)[MP_MOM_U]) {
 #pragma unroll
         for (int q = 0; q < MP_MOM_U; ++q) {
             const int k = k0 + q;
+            hl_[q] = hr_[q] = kl_[q] = kr_[q] = u_[q] = 0.0;
             if (k < nz) {
                 const size_t o = P * (size_t)k;
-                hln[q] = __ldg(hl + o);
-                hrn[q] = __ldg(hr + o);
-                kvln[q] = __ldg(kvl + o);
-                kvrn[q] = __ldg(kvr + o);
-                un[q] = ld_hint(uf + PF * (size_t)k, pol_keep);
+                hl_[q] = __ldg(hl + o);
+                hr_[q] = __ldg(hr + o);
+                kl_[q] = __ldg(kvl + o);
+                kr_[q] = __ldg(kvr + o);
+                u_[q] = ld_hint(uf + PF * (size_t)k, pol_keep);
             }
         }
+    };
+    double hln[MP_MOM_U], hrn[MP_MOM_U], un[MP_MOM_U], kvln[MP_MOM_U], kvrn[MP_MOM_U];
+    load_up(1, hln, hrn, un, kvln, kvrn);
+    for (int k0 = 1; k0 <= nz; k0 += MP_MOM_U) {
+        double hlx[MP_MOM_U], hrx[MP_MOM_U], ux[MP_MOM_U], kvlx[MP_MOM_U], kvrx[MP_MOM_U];
+        load_up(k0 + MP_MOM_U, hlx, hrx, ux, kvlx, kvrx);
 #pragma unroll
         for (int q = 0; q < MP_MOM_U; ++q) {
             const int k = k0 + q;
@@ -1104,17 +1122,30 @@ __device__ __forceinline__ void solve_face_mp(const Params &p, double dt, int i,
             u_m = u_c;
             u_c = u_p;
         }
+#pragma unroll
+        for (int q = 0; q < MP_MOM_U; ++q) {
+            hln[q] = hlx[q];
+            hrn[q] = hrx[q];
+            un[q] = ux[q];
+            kvln[q] = kvlx[q];
+            kvrn[q] = kvrx[q];
+        }
     }
     (void)f_prev;
     // back-substitution: increment (+ the remnant, RHS 1, clipped at 1 as it goes)
     float delta = 0.0f, gam = 0.0f;
-    for (int k0 = nz; k0 >= 1; k0 -= MP_MOM_U) {
-        double uo[MP_MOM_U];
+    auto load_down = [&](int k0, double (&u_)[MP_MOM_U]) {
 #pragma unroll
         for (int q = 0; q < MP_MOM_U; ++q) {
             const int k = k0 - q;
-            if (k >= 1) uo[q] = ld_hint(uf + PF * (size_t)(k - 1), pol_keep);
+            u_[q] = (k >= 1) ? ld_hint(uf + PF * (size_t)(k - 1), pol_keep) : 0.0;
         }
+    };
+    double uo[MP_MOM_U];
+    load_down(nz, uo);
+    for (int k0 = nz; k0 >= 1; k0 -= MP_MOM_U) {
+        double uox[MP_MOM_U];
+        load_down(k0 - MP_MOM_U, uox);
 #pragma unroll
         for (int q = 0; q < MP_MOM_U; ++q) {
             const int k = k0 - q;
@@ -1129,6 +1160,8 @@ __device__ __forceinline__ void solve_face_mp(const Params &p, double dt, int i,
                 vrem[o] = (double)gam;
             }
         }
+#pragma unroll
+        for (int q = 0; q < MP_MOM_U; ++q) uo[q] = uox[q];
     }
 }
 
@@ -1241,15 +1274,15 @@ struct MixedFace {
     __device__ __forceinline__ void back()
     {
         float delta = 0.0f;
-        for (int k0 = nz; k0 >= 1; k0 -= MP_MOM_U) {
-            double uo[MP_MOM_U];
+        for (int k0 = nz; k0 >= 1; k0 -= MP_MOM_UB) {
+            double uo[MP_MOM_UB];
 #pragma unroll
-            for (int q = 0; q < MP_MOM_U; ++q) {
+            for (int q = 0; q < MP_MOM_UB; ++q) {
                 const int k = k0 - q;
                 uo[q] = (k >= 1 && valid) ? ld_hint(uf + PF * (size_t)(k - 1), pol_keep) : 0.0;
             }
 #pragma unroll
-            for (int q = 0; q < MP_MOM_U; ++q) {
+            for (int q = 0; q < MP_MOM_UB; ++q) {
                 const int k = k0 - q;
                 if (k < 1) break;
                 const size_t s = (size_t)(k - 1) * MT_TW + tid;
