@@ -69,7 +69,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="eddy_1440x1080x75")
-    ap.add_argument("--e2e-steps", type=int, default=4)
+    ap.add_argument("--e2e-steps", type=int, default=-1,
+                    help="steps of the end-to-end timing (0: none; default: the timed steps, 4 to 12)")
     ap.add_argument("--cpu-sample", default="360x270", help="nx x ny of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--form", default="mixed", choices=["mixed", "plain"],
@@ -447,6 +448,9 @@ def main():
     # overlaps the other's upload on the full-duplex host link; each handle
     # has its own pinned result buffers.
     e2e = None
+    if args.e2e_steps < 0:
+        # the timed steps, bounded: each end-to-end step moves ~15 GB over the host link
+        args.e2e_steps = min(max(args.steps, 4), 12)
     if args.e2e_steps > 0:
         import ctypes
 
@@ -514,7 +518,7 @@ def main():
         e2e = {"value": cells * args.e2e_steps * world / el, "unit": "cells/s", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "ms_per_step": el / args.e2e_steps * 1e3,
                "serial_ms_per_step": el_serial / args.e2e_steps * 1e3,
-               "serial_cells_per_s": cells * args.e2e_steps * world / el_serial,
+               "serial_cells_per_s": cells * args.e2e_steps * world / el_serial, "steps": args.e2e_steps,
                "what": "C ABI: vphys_set_field_async (pinned host -> HBM) of h, u, v, tracers, forcing; vphys_step; "
                        "vphys_get_field_async of u, v, tracers, kv, kt, ks, bl_depth; two handles on two streams "
                        "take alternate steps so one's download overlaps the other's upload (serial: one handle, "
