@@ -706,6 +706,16 @@ int vphys_gemm_tn_bf16(const void *A, long long lda, const void *B, long long ld
                        float alpha, const float *bias, const float *zin, int ld_z, int act, float *out_f32,
                        int ld_f32, void *out_bf16, int ld_bf16, void *out_bf16_t, int ld_t, int *err, void *stream);
 
+/* The surrogate's forward pass in one launch (the three layers of
+ * vphys_kpp's in-step inference): Y[M,80] = (GELU(GELU(X W1^T + b1) W2^T + b2))
+ * W3^T + b3 with X [M,160] BF16, W1 [256,160], W2 [256,256], W3 [80,256] BF16
+ * (K contiguous), b1/b2 [256], b3 [80] and Y FP32.  The hidden activations
+ * stay in shared memory (BF16, as the three separate GEMMs round them), so Y
+ * equals three vphys_gemm_tn_bf16 calls bit for bit.  Every pointer 16-byte
+ * aligned; M <= 0 is a no-op.  *err as for vphys_gemm_tn_bf16. */
+int vphys_mlp3_bf16(const void *X, int M, const void *W1, const float *b1, const void *W2, const float *b2,
+                    const void *W3, const float *b3, float *Y, int *err, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -88,7 +88,7 @@ struct vphys_handle_s {
     // learned KPP surrogate (vphys_kpp_attach): the caller's weights and the scratch of one inference
     vphys_kpp_model kpp{};
     bool kpp_attached = false;
-    void *kX = nullptr, *kH1 = nullptr, *kH2 = nullptr;
+    void *kX = nullptr;
     float *kY = nullptr, *kcolH = nullptr, *kpred = nullptr, *kcheck = nullptr;
     unsigned char *kgate = nullptr;
     unsigned long long *kstats = nullptr;
@@ -609,15 +609,8 @@ int run_learned_kpp(vphys_handle h, Params &p)
     vphys::launch_kpp_features(p, nullptr, h->kX, nullptr, 0, m.feat_mean, m.feat_istd, m.gate_limit, h->kgate,
                                h->kcolH, s);
     int st;
-    if ((st = vphys::gemm_tn_bf16(h->kX, vphys::LK_INP, m.w1, vphys::LK_INP, ncols, vphys::LK_HID, vphys::LK_INP,
-                                  1.0f, m.b1, nullptr, 0, 1, nullptr, 0, h->kH1, vphys::LK_HID, nullptr, 0, h->kerr, s)))
-        return st;
-    if ((st = vphys::gemm_tn_bf16(h->kH1, vphys::LK_HID, m.w2, vphys::LK_HID, ncols, vphys::LK_HID, vphys::LK_HID,
-                                  1.0f, m.b2, nullptr, 0, 1, nullptr, 0, h->kH2, vphys::LK_HID, nullptr, 0, h->kerr, s)))
-        return st;
-    if ((st = vphys::gemm_tn_bf16(h->kH2, vphys::LK_HID, m.w3, vphys::LK_HID, ncols, vphys::LK_OUTP, vphys::LK_HID,
-                                  1.0f, m.b3, nullptr, 0, 0, h->kY, vphys::LK_OUTP, nullptr, 0, nullptr, 0, h->kerr, s)))
-        return st;
+    // the three layers in one launch, the hidden activations on chip
+    if ((st = vphys::mlp3_bf16(h->kX, ncols, m.w1, m.b1, m.w2, m.b2, m.w3, m.b3, h->kY, h->kerr, s))) return st;
     vphys::launch_kpp_apply((size_t)ncols, h->kY, m.target_mean0, m.target_std0, h->kgate, h->kcolH, h->kpred,
                             h->kcheck, h->kstats, h->kgen++, m.check_fraction, s);
     p.kpp_pred = h->kpred;
@@ -629,10 +622,10 @@ int run_learned_kpp(vphys_handle h, Params &p)
 
 void free_kpp(vphys_handle h)
 {
-    void *bufs[] = {h->kX, h->kH1, h->kH2, h->kY, h->kcolH, h->kpred, h->kcheck, h->kgate, h->kstats, h->kerr};
+    void *bufs[] = {h->kX, h->kY, h->kcolH, h->kpred, h->kcheck, h->kgate, h->kstats, h->kerr};
     for (void *b : bufs)
         if (b) cudaFree(b);
-    h->kX = h->kH1 = h->kH2 = nullptr;
+    h->kX = nullptr;
     h->kY = h->kcolH = h->kpred = h->kcheck = nullptr;
     h->kgate = nullptr;
     h->kstats = nullptr;
@@ -1526,8 +1519,6 @@ int vphys_kpp_attach(vphys_handle h, const vphys_kpp_model *m)
         void **p;
         size_t bytes;
     } want[] = {{&h->kX, nc * vphys::LK_INP * 2},
-                {&h->kH1, nc * vphys::LK_HID * 2},
-                {&h->kH2, nc * vphys::LK_HID * 2},
                 {(void **)&h->kY, nc * vphys::LK_OUTP * sizeof(float)},
                 {(void **)&h->kcolH, nc * sizeof(float)},
                 {(void **)&h->kpred, nc * sizeof(float)},

@@ -434,6 +434,287 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1)
     }
 }
 
+// ---- the three layers of the KPP surrogate in one kernel -----------------------
+// Y = (GELU(GELU(X W1^T + b1) W2^T + b2)) W3^T + b3 for 128-row tiles, the
+// hidden activations never leaving the SM: the epilogue warps write GELU(H)
+// as BF16 straight into shared memory in the layout a TMA load with 128-byte
+// swizzle produces (the A operand of the next layer's MMAs), so the layers
+// make no HBM round trip.  Per tile the products and their order are those
+// of three k_gemm_tn<1/1/2> launches (K slices in order, K = 16 per MMA), so
+// Y is theirs bit for bit.  Roles as in k_gemm_tn: warp 0 lane 0 streams the
+// X tile and the weights' 64-wide K slices (W1: 3, W2: 4, W3: 4 per tile)
+// through an ML_STAGES ring, warp 1 lane 0 issues the MMAs, warps 2-9 drain
+// the accumulator.  Barriers: x_full / x_empty (the X tile), w_full / w_empty
+// (the weight ring), acc_full (a layer's accumulator is complete: three
+// phases per tile), h_full (the hidden tile in shared memory is written and
+// the accumulator read: two phases per tile).  Every wait is bounded.
+constexpr int ML_STAGES = 3;
+constexpr int ML_XCH = 3;                        // 64-wide K slices of X (160 -> 192, zero-filled)
+constexpr int ML_HCH = 4;                        // 64-wide K slices of a hidden tile (256)
+constexpr int ML_CHUNK_X = GM * GK * 2;          // bytes of one [128 x 64] BF16 slice
+constexpr int ML_WSTAGE = GN_MAX * GK * 2;       // bytes of one [256 x 64] weight slice
+constexpr size_t ML_SMEM = (size_t)ML_XCH * ML_CHUNK_X + (size_t)ML_HCH * ML_CHUNK_X + (size_t)ML_STAGES * ML_WSTAGE +
+                           1024 /* barriers */ + 1024 /* align */;
+constexpr int ML_ACC3 = 256;                     // tensor-memory column of the output layer's accumulator
+// 16 epilogue warps (four per lane quarter, each a quarter of the columns):
+// the epilogue is the kernel's bound, and it cannot overlap the next tile's
+// MMAs here as it does in k_gemm_tn
+constexpr int ML_EPI = 16;
+constexpr int ML_THREADS = 64 + 32 * ML_EPI;
+
+struct MlpArgs {
+    int M;
+    const float *b1, *b2, *b3;
+    float *Y;   // [M, LK_OUTP]
+    int *err;
+};
+
+// GELU(v + bias) of 16 accumulator columns of row r into the hidden tile
+// (row r, columns c0..c0+15: two 16-byte units of the 128-byte-swizzled slice)
+__device__ __forceinline__ void mlp_hidden16(uint8_t *hs, int r, int c0, const float *__restrict__ bias,
+                                             const uint32_t (&v)[16])
+{
+    float b[16];
+    const float4 *b4 = reinterpret_cast<const float4 *>(bias + c0);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const float4 t = __ldg(b4 + q);
+        b[4 * q] = t.x, b[4 * q + 1] = t.y, b[4 * q + 2] = t.z, b[4 * q + 3] = t.w;
+    }
+    __nv_bfloat162 pk[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+        pk[q] = __floats2bfloat162_rn(gelu_tanh(__uint_as_float(v[2 * q]) + b[2 * q]),
+                                      gelu_tanh(__uint_as_float(v[2 * q + 1]) + b[2 * q + 1]));
+    const int kt = c0 >> 6, ch = (c0 & 63) >> 3;   // slice, first 16-byte unit of the 128-byte row
+    uint8_t *row = hs + (size_t)kt * ML_CHUNK_X + (size_t)r * 128;
+    *reinterpret_cast<uint4 *>(row + (((ch) ^ (r & 7)) << 4)) = *reinterpret_cast<uint4 *>(&pk[0]);
+    *reinterpret_cast<uint4 *>(row + (((ch + 1) ^ (r & 7)) << 4)) = *reinterpret_cast<uint4 *>(&pk[4]);
+}
+
+__global__ void __launch_bounds__(ML_THREADS, 1)
+    k_mlp3(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmW1,
+           const __grid_constant__ CUtensorMap tmW2, const __grid_constant__ CUtensorMap tmW3, const MlpArgs g)
+{
+    extern __shared__ uint8_t smraw[];
+    uint8_t *sm = reinterpret_cast<uint8_t *>(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
+    uint8_t *sx = sm;                                           // X tile: ML_XCH slices
+    uint8_t *sh = sx + (size_t)ML_XCH * ML_CHUNK_X;             // hidden tile: ML_HCH slices
+    uint8_t *sw = sh + (size_t)ML_HCH * ML_CHUNK_X;             // weight ring
+    uint64_t *x_full = reinterpret_cast<uint64_t *>(sw + (size_t)ML_STAGES * ML_WSTAGE);
+    uint64_t *x_empty = x_full + 1;
+    uint64_t *w_full = x_empty + 1;                             // [ML_STAGES]
+    uint64_t *w_empty = w_full + ML_STAGES;                     // [ML_STAGES]
+    uint64_t *acc_full = w_empty + ML_STAGES;
+    uint64_t *h_full = acc_full + 1;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(h_full + 1);
+    int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tiles = (g.M + GM - 1) / GM;
+    const int my_tiles = (tiles > (int)blockIdx.x) ? (tiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+
+    if (threadIdx.x == 0) {
+        mbar_init(x_full, 1);
+        mbar_init(x_empty, 1);
+        for (int s = 0; s < ML_STAGES; ++s) {
+            mbar_init(&w_full[s], 1);
+            mbar_init(&w_empty[s], 1);
+        }
+        mbar_init(acc_full, 1);
+        mbar_init(h_full, ML_EPI);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    volatile int *abort_v = abort_flag;
+    // the weight slices of one tile, in the order the MMA warp takes them
+    constexpr int NW = ML_XCH + 2 * ML_HCH;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---- TMA producer ----
+            long long it = 0;   // weight slices armed so far
+            int xt = 0;         // X tiles armed so far
+            bool lost = false;
+            for (int t = 0; t < my_tiles && !lost; ++t) {
+                const int m0 = ((int)blockIdx.x + t * (int)gridDim.x) * GM;
+                if (!mbar_wait(x_empty, (uint32_t)((t & 1) ^ 1)) || *abort_v) {
+                    atomicExch(g.err, 1);
+                    *abort_v = 1;
+                    break;
+                }
+                mbar_expect_tx(x_full, (uint32_t)(ML_XCH * ML_CHUNK_X));
+                for (int c = 0; c < ML_XCH; ++c) tma_load_2d(sx + (size_t)c * ML_CHUNK_X, &tmX, c * GK, m0, x_full);
+                ++xt;
+                for (int w = 0; w < NW; ++w, ++it) {
+                    const int s = (int)(it % ML_STAGES);
+                    if (!mbar_wait(&w_empty[s], (uint32_t)(((it / ML_STAGES) & 1) ^ 1)) || *abort_v) {
+                        atomicExch(g.err, 1);
+                        *abort_v = 1;
+                        lost = true;
+                        break;
+                    }
+                    uint8_t *dst = sw + (size_t)s * ML_WSTAGE;
+                    if (w < ML_XCH) {
+                        mbar_expect_tx(&w_full[s], (uint32_t)(GN_MAX * GK * 2));
+                        tma_load_2d(dst, &tmW1, w * GK, 0, &w_full[s]);
+                    } else if (w < ML_XCH + ML_HCH) {
+                        mbar_expect_tx(&w_full[s], (uint32_t)(GN_MAX * GK * 2));
+                        tma_load_2d(dst, &tmW2, (w - ML_XCH) * GK, 0, &w_full[s]);
+                    } else {
+                        mbar_expect_tx(&w_full[s], (uint32_t)(LK_OUTP * GK * 2));
+                        tma_load_2d(dst, &tmW3, (w - ML_XCH - ML_HCH) * GK, 0, &w_full[s]);
+                    }
+                }
+            }
+            if (*abort_v) {
+                // drain: the bytes of every armed slice and X tile land before the CTA exits
+                const long long first = it > ML_STAGES ? it - ML_STAGES : 0;
+                for (long long a = first; a < it; ++a)
+                    if (!mbar_wait(&w_full[(int)(a % ML_STAGES)], (uint32_t)((a / ML_STAGES) & 1))) atomicExch(g.err, 5);
+                if (xt > 0 && !mbar_wait(x_full, (uint32_t)((xt - 1) & 1))) atomicExch(g.err, 5);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---- MMA issuer ----
+            long long it = 0;
+            long long commits = 0;   // acc_full commits so far
+            bool ok = true;
+            for (int t = 0; t < my_tiles && ok && !*abort_v; ++t) {
+                if (!mbar_wait(x_full, (uint32_t)(t & 1))) {
+                    atomicExch(g.err, 2);
+                    *abort_v = 1;
+                    break;
+                }
+                for (int layer = 0; layer < 3 && ok; ++layer) {
+                    if (layer > 0 && !mbar_wait(h_full, (uint32_t)((2 * t + layer - 1) & 1))) {
+                        atomicExch(g.err, 4);
+                        *abort_v = 1;
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const int nch = layer == 0 ? ML_XCH : ML_HCH;
+                    const int N = layer == 2 ? LK_OUTP : GN_MAX;
+                    const uint32_t idesc = idesc_bf16(GM, N);
+                    const uint32_t d = tmem + (uint32_t)(layer == 2 ? ML_ACC3 : 0);
+                    const uint8_t *abase = layer == 0 ? sx : sh;
+                    for (int c = 0; c < nch; ++c, ++it) {
+                        const int s = (int)(it % ML_STAGES);
+                        if (!mbar_wait(&w_full[s], (uint32_t)((it / ML_STAGES) & 1))) {
+                            atomicExch(g.err, 2);
+                            *abort_v = 1;
+                            ok = false;
+                            break;
+                        }
+                        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                        const uint8_t *as = abase + (size_t)c * ML_CHUNK_X;
+                        const uint8_t *bs = sw + (size_t)s * ML_WSTAGE;
+#pragma unroll
+                        for (int kk = 0; kk < GK / 16; ++kk) {
+                            const uint64_t ad = smem_desc_sw128(as + kk * 32);
+                            const uint64_t bd = smem_desc_sw128(bs + kk * 32);
+                            const uint32_t acc = (c > 0 || kk > 0) ? 1u : 0u;
+                            asm volatile(
+                                "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                                " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
+                                "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+                                : "memory");
+                        }
+                        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                         smem_u32(&w_empty[s]))
+                                     : "memory");
+                    }
+                    if (layer == 0)   // the X tile is read once the first layer's MMAs retire
+                        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                         smem_u32(x_empty))
+                                     : "memory");
+                    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                     smem_u32(acc_full))
+                                 : "memory");
+                    ++commits;
+                }
+            }
+            if (*abort_v && commits > 0) {
+                // drain: the last commit arrives once every MMA issued before it has retired
+                if (!mbar_wait(acc_full, (uint32_t)((commits - 1) & 1))) atomicExch(g.err, 6);
+            }
+        }
+    } else {
+        // ---- epilogue warps 2..17: lanes of quarter warp % 4; group (warp - 2) / 4 takes
+        //      the 16-column chunks group, group + 4, ... ----
+        const int quarter = warp & 3;
+        const int grp = (warp - 2) >> 2;
+        const int r = quarter * 32 + lane;   // row of the tile
+        const uint32_t tl = tmem + ((uint32_t)(quarter * 32) << 16);
+        bool ok = true;
+        for (int t = 0; t < my_tiles && ok; ++t) {
+            const int row = ((int)blockIdx.x + t * (int)gridDim.x) * GM + r;
+            for (int layer = 0; layer < 3; ++layer) {
+                if (!mbar_wait(acc_full, (uint32_t)((3 * t + layer) & 1))) {
+                    if (lane == 0) atomicExch(g.err, 3);
+                    *abort_v = 1;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                if (*abort_v) {
+                    ok = false;
+                    break;
+                }
+                if (layer < 2) {
+                    const float *bias = layer == 0 ? g.b1 : g.b2;
+                    for (int c0 = grp * 16; c0 < GN_MAX; c0 += 128) {
+                        uint32_t v0[16], v1[16];
+                        tmem_ld16_async(tl + (uint32_t)c0, v0);
+                        tmem_ld16_async(tl + (uint32_t)(c0 + 64), v1);
+                        tmem_ld_wait();
+                        mlp_hidden16(sh, r, c0, bias, v0);
+                        mlp_hidden16(sh, r, c0 + 64, bias, v1);
+                    }
+                    // the hidden tile is visible to the tensor cores' reads, the accumulator read
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(h_full);
+                } else {
+                    for (int c0 = grp * 16; c0 < LK_OUTP; c0 += 64) {
+                        uint32_t v[16];
+                        tmem_ld16(tl + (uint32_t)(ML_ACC3 + c0), v);
+                        if (row < g.M) {
+                            float4 *o4 = reinterpret_cast<float4 *>(g.Y + (size_t)row * LK_OUTP + c0);
+                            const float4 *b4 = reinterpret_cast<const float4 *>(g.b3 + c0);
+#pragma unroll
+                            for (int q = 0; q < 4; ++q) {
+                                const float4 b = __ldg(b4 + q);
+                                o4[q] = make_float4(__uint_as_float(v[4 * q]) + b.x, __uint_as_float(v[4 * q + 1]) + b.y,
+                                                    __uint_as_float(v[4 * q + 2]) + b.z,
+                                                    __uint_as_float(v[4 * q + 3]) + b.w);
+                            }
+                        }
+                    }
+                    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+    }
+}
+
 // ---- host side ---------------------------------------------------------------
 static PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 {
@@ -527,7 +808,49 @@ int gemm_tn_bf16(const void *A, long long lda, const void *B, long long ldb, int
     return VPHYS_OK;
 }
 
+// The surrogate's forward pass in one launch: X [M, LK_INP] BF16 (the padded
+// inputs zero), W1 [LK_HID, LK_INP], W2 [LK_HID, LK_HID], W3 [LK_OUTP, LK_HID]
+// BF16 K-contiguous, biases FP32, Y [M, LK_OUTP] FP32; every pointer 16-byte
+// aligned.
+int mlp3_bf16(const void *X, int M, const void *W1, const float *b1, const void *W2, const float *b2, const void *W3,
+              const float *b3, float *Y, int *err, cudaStream_t stream)
+{
+    if (M <= 0) return VPHYS_OK;
+    if ((((uintptr_t)X) | ((uintptr_t)W1) | ((uintptr_t)W2) | ((uintptr_t)W3) | ((uintptr_t)b1) | ((uintptr_t)b2) |
+         ((uintptr_t)b3) | ((uintptr_t)Y)) &
+        15)
+        return report_error(VPHYS_ERR_BAD_SHAPE, "vphys_mlp3_bf16: every operand must be 16-byte aligned");
+    CUtensorMap mx, m1, m2, m3;
+    if (!make_map(&mx, X, M, LK_INP, LK_INP, GM) || !make_map(&m1, W1, LK_HID, LK_INP, LK_INP, LK_HID) ||
+        !make_map(&m2, W2, LK_HID, LK_HID, LK_HID, LK_HID) || !make_map(&m3, W3, LK_OUTP, LK_HID, LK_HID, LK_OUTP))
+        return report_error(VPHYS_ERR_CUDA, "vphys_mlp3_bf16: cuTensorMapEncodeTiled failed");
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_mlp3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ML_SMEM);
+        attr_set = true;
+    }
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    MlpArgs a{M, b1, b2, b3, Y, err};
+    const int tiles = (M + GM - 1) / GM;
+    k_mlp3<<<tiles < sms ? tiles : sms, ML_THREADS, ML_SMEM, stream>>>(mx, m1, m2, m3, a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return report_error(VPHYS_ERR_CUDA, cudaGetErrorString(e));
+    return VPHYS_OK;
+}
+
 }  // namespace vphys
+
+extern "C" int vphys_mlp3_bf16(const void *X, int M, const void *W1, const float *b1, const void *W2, const float *b2,
+                               const void *W3, const float *b3, float *Y, int *err, void *stream)
+{
+    return vphys::mlp3_bf16(X, M, W1, b1, W2, b2, W3, b3, Y, err, reinterpret_cast<cudaStream_t>(stream));
+}
 
 extern "C" int vphys_gemm_tn_bf16(const void *A, long long lda, const void *B, long long ldb, int M, int N, int K,
                                   float alpha, const float *bias, const float *zin, int ld_z, int act, float *out_f32,

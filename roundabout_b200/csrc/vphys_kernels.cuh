@@ -132,6 +132,8 @@ void launch_kpp_apply(size_t ncols, const float *Y, float tmean0, float tstd0, c
 int gemm_tn_bf16(const void *A, long long lda, const void *B, long long ldb, int M, int N, int K, float alpha,
                  const float *bias, const float *zin, int ld_z, int act, float *out_f32, int ld_f32, void *out_bf16,
                  int ld_bf16, void *out_bf16_t, int ld_t, int *err, cudaStream_t stream);
+int mlp3_bf16(const void *X, int M, const void *W1, const float *b1, const void *W2, const float *b2, const void *W3,
+              const float *b3, float *Y, int *err, cudaStream_t stream);
 void launch_selftest_division(unsigned long long seed, long long per_thread, int emin, int erange,
                               unsigned long long *bad, cudaStream_t stream);
 

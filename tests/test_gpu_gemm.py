@@ -146,3 +146,33 @@ def test_gemm_rejects_bad_shapes(env):
     st = lib.vphys_gemm_tn_bf16(P(A), 64, P(B), 64, 128, 24, 64, 1.0, None, None, 0, 0, None, 0, None, 0, None, 0,
                                 None, None)
     assert st == _ffi.ERR_BAD_SHAPE
+
+
+@pytest.mark.parametrize("M", [1000, 5003, 128])
+def test_mlp3_equals_three_gemms(env, M):
+    """vphys_mlp3_bf16 (the surrogate's three layers in one launch, hidden
+    activations on chip) against the three inference GEMMs it replaces: the
+    same products in the same order, so bit for bit."""
+    torch, lib, _ffi = env
+    g = torch.Generator(device="cuda").manual_seed(M)
+    X = torch.zeros(M, 160, device="cuda", dtype=torch.bfloat16)
+    X[:, :154] = torch.randn(M, 154, device="cuda", generator=g).to(torch.bfloat16)
+    W1 = (0.1 * torch.randn(256, 160, device="cuda", generator=g)).to(torch.bfloat16)
+    W2 = (0.06 * torch.randn(256, 256, device="cuda", generator=g)).to(torch.bfloat16)
+    W3 = (0.06 * torch.randn(80, 256, device="cuda", generator=g)).to(torch.bfloat16)
+    b1 = 0.1 * torch.randn(256, device="cuda", generator=g)
+    b2 = 0.1 * torch.randn(256, device="cuda", generator=g)
+    b3 = 0.1 * torch.randn(80, device="cuda", generator=g)
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    Y = torch.full((M, 80), float("nan"), device="cuda")
+    st = lib.vphys_mlp3_bf16(P(X), M, P(W1), P(b1), P(W2), P(b2), P(W3), P(b3), P(Y), P(err), None)
+    assert st == 0, _ffi.last_error()
+    _, H1, _ = run(env, X, W1, bias=b1, act=1, f32=False, bf16=True)
+    _, H2, _ = run(env, H1, W2, bias=b2, act=1, f32=False, bf16=True)
+    Y3, _, _ = run(env, H2, W3, bias=b3)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    assert torch.equal(Y, Y3)
+    ref = gelu(gelu(X.float() @ W1.float().T + b1).to(torch.bfloat16).float() @ W2.float().T + b2)
+    ref = ref.to(torch.bfloat16).float() @ W3.float().T + b3
+    assert float((Y - ref).abs().max()) <= 2e-2 * float(ref.abs().max())
