@@ -3,7 +3,8 @@ cells), FP32 solves with the FP64 residual correction and the learned KPP,
 4 passive tracers, 30 % land, every field resident in HBM, graph-captured
 steps.
 
-    python -m roundabout_b200.combined_eval [--steps 48] [--train-cols 2000000]
+    python -m roundabout_b200.combined_eval [--steps 48] [--train-cols 2000000] [--mixed-level 2]
+                                            [--variants registers,tmem_rows]
 
 The domain is generated on the device (synthetic.make_columns_device) and
 bound zero-copy.  The same initial state (regenerated from the seed) is then
@@ -27,6 +28,11 @@ def main():
     ap.add_argument("--train-cols", type=int, default=2_000_000)
     ap.add_argument("--config", default="combined_3600x2700x75")
     ap.add_argument("--seed", type=int, default=4321)
+    ap.add_argument("--mixed-level", type=int, default=2, choices=[1, 2],
+                    help="1: FP64 assembly, FP32 solves; 2: FP32 assembly too (the bench's mixed form)")
+    ap.add_argument("--variants", default="registers,tmem_rows",
+                    help="kernel forms of the mixed solves (the autotuner's copy of the state does not fit "
+                         "beside this domain; the default is its pick on 1440x1080x75)")
     args = ap.parse_args()
 
     import numpy as np
@@ -53,9 +59,11 @@ def main():
                                    passive_init=spec.get("passive_init", "uniform"))
 
     cfg = hot_path_config(ntracers=ntr)
-    cfg.mixed_precision = 1
+    cfg.mixed_precision = args.mixed_level
     cfg.learned_kpp = 1
     vp = VerticalPhysics(nx, ny, nz, ntr, cfg)
+    vp.set_variants(*args.variants.split(","))
+    out["mixed_level"], out["variants"] = args.mixed_level, args.variants
     d = generate()
     bind_device_columns(vp, d)
     init = {"u": d["u"].clone(), "v": d["v"].clone(), "tracers": [t.clone() for t in d["tracers"]]}

@@ -79,7 +79,7 @@ def main():
            "tracers": lambda: vp.vdiff_tracers_nonlocal(dt), "step": lambda: vp.step(dt, 1),
            "kshear": lambda: vp.kappa_shear(dt), "epbl": lambda: vp.epbl(dt)}
     ncols = args.nx * args.ny
-    if "features" in args.stages or "mlp" in args.stages:
+    if "features" in args.stages or "mlp" in args.stages:   # mlp: three GEMMs; mlp3: the fused network
         import ctypes
 
         from . import _ffi
@@ -97,8 +97,18 @@ def main():
 
         fns["features"] = features
         fns["mlp"] = lambda: sur.forward(X)
+        Y3 = torch.empty(ncols, L.NOUTP, device="cuda")
+        kerr = torch.zeros(1, dtype=torch.int32, device="cuda")
+
+        def mlp3():
+            _ffi.check(vp.lib.vphys_mlp3_bf16(L._p(X), ncols, L._p(sur.Wb[0]), L._p(sur.b[0]), L._p(sur.Wb[1]),
+                                               L._p(sur.b[1]), L._p(sur.Wb[2]), L._p(sur.b[2]), L._p(Y3), L._p(kerr),
+                                               None), "vphys_mlp3_bf16")
+
+        fns["mlp3"] = mlp3
         bpc["features"] = 40.0 + L.NINP * 2.0 / args.nz   # h, rho, u, v (two faces each) -> X
         bpc["mlp"] = (L.NINP * 2 + 4 * L.NHID * 2 + L.NOUTP * 4) / args.nz   # X in, H1/H2 out+in, Y out
+        bpc["mlp3"] = (L.NINP * 2 + L.NOUTP * 4) / args.nz                    # X in, Y out
     out = {}
     for name in args.stages.split(","):
         fn = fns[name]
