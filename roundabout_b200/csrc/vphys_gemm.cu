@@ -453,8 +453,9 @@ constexpr int ML_XCH = 3;                        // 64-wide K slices of X (160 -
 constexpr int ML_HCH = 4;                        // 64-wide K slices of a hidden tile (256)
 constexpr int ML_CHUNK_X = GM * GK * 2;          // bytes of one [128 x 64] BF16 slice
 constexpr int ML_WSTAGE = GN_MAX * GK * 2;       // bytes of one [256 x 64] weight slice
+constexpr int ML_NBIAS = 2 * GN_MAX + LK_OUTP;   // b1, b2, b3, staged in shared memory
 constexpr size_t ML_SMEM = (size_t)ML_XCH * ML_CHUNK_X + (size_t)ML_HCH * ML_CHUNK_X + (size_t)ML_STAGES * ML_WSTAGE +
-                           1024 /* barriers */ + 1024 /* align */;
+                           (size_t)ML_NBIAS * 4 + 1024 /* barriers */ + 1024 /* align */;
 constexpr int ML_ACC3 = 256;                     // tensor-memory column of the output layer's accumulator
 // 16 epilogue warps (four per lane quarter, each a quarter of the columns):
 // the epilogue is the kernel's bound, and it cannot overlap the next tile's
@@ -471,14 +472,13 @@ struct MlpArgs {
 
 // GELU(v + bias) of 16 accumulator columns of row r into the hidden tile
 // (row r, columns c0..c0+15: two 16-byte units of the 128-byte-swizzled slice)
-__device__ __forceinline__ void mlp_hidden16(uint8_t *hs, int r, int c0, const float *__restrict__ bias,
-                                             const uint32_t (&v)[16])
+__device__ __forceinline__ void mlp_hidden16(uint8_t *hs, int r, int c0, const float *bias, const uint32_t (&v)[16])
 {
-    float b[16];
+    float b[16];   // the layer's bias, staged in shared memory
     const float4 *b4 = reinterpret_cast<const float4 *>(bias + c0);
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-        const float4 t = __ldg(b4 + q);
+        const float4 t = b4[q];
         b[4 * q] = t.x, b[4 * q + 1] = t.y, b[4 * q + 2] = t.z, b[4 * q + 3] = t.w;
     }
     __nv_bfloat162 pk[8];
@@ -501,7 +501,8 @@ __global__ void __launch_bounds__(ML_THREADS, 1)
     uint8_t *sx = sm;                                           // X tile: ML_XCH slices
     uint8_t *sh = sx + (size_t)ML_XCH * ML_CHUNK_X;             // hidden tile: ML_HCH slices
     uint8_t *sw = sh + (size_t)ML_HCH * ML_CHUNK_X;             // weight ring
-    uint64_t *x_full = reinterpret_cast<uint64_t *>(sw + (size_t)ML_STAGES * ML_WSTAGE);
+    float *sb = reinterpret_cast<float *>(sw + (size_t)ML_STAGES * ML_WSTAGE);   // b1 | b2 | b3
+    uint64_t *x_full = reinterpret_cast<uint64_t *>(sb + ML_NBIAS);
     uint64_t *x_empty = x_full + 1;
     uint64_t *w_full = x_empty + 1;                             // [ML_STAGES]
     uint64_t *w_empty = w_full + ML_STAGES;                     // [ML_STAGES]
@@ -526,6 +527,8 @@ __global__ void __launch_bounds__(ML_THREADS, 1)
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    for (int i = threadIdx.x; i < ML_NBIAS; i += blockDim.x)
+        sb[i] = i < GN_MAX ? g.b1[i] : (i < 2 * GN_MAX ? g.b2[i - GN_MAX] : g.b3[i - 2 * GN_MAX]);
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                      "r"(TMEM_COLS)
@@ -672,7 +675,7 @@ __global__ void __launch_bounds__(ML_THREADS, 1)
                     break;
                 }
                 if (layer < 2) {
-                    const float *bias = layer == 0 ? g.b1 : g.b2;
+                    const float *bias = sb + (layer == 0 ? 0 : GN_MAX);
                     for (int c0 = grp * 16; c0 < GN_MAX; c0 += 128) {
                         uint32_t v0[16], v1[16];
                         tmem_ld16_async(tl + (uint32_t)c0, v0);
@@ -692,10 +695,10 @@ __global__ void __launch_bounds__(ML_THREADS, 1)
                         tmem_ld16(tl + (uint32_t)(ML_ACC3 + c0), v);
                         if (row < g.M) {
                             float4 *o4 = reinterpret_cast<float4 *>(g.Y + (size_t)row * LK_OUTP + c0);
-                            const float4 *b4 = reinterpret_cast<const float4 *>(g.b3 + c0);
+                            const float4 *b4 = reinterpret_cast<const float4 *>(sb + 2 * GN_MAX + c0);
 #pragma unroll
                             for (int q = 0; q < 4; ++q) {
-                                const float4 b = __ldg(b4 + q);
+                                const float4 b = b4[q];
                                 o4[q] = make_float4(__uint_as_float(v[4 * q]) + b.x, __uint_as_float(v[4 * q + 1]) + b.y,
                                                     __uint_as_float(v[4 * q + 2]) + b.z,
                                                     __uint_as_float(v[4 * q + 3]) + b.w);

@@ -130,7 +130,10 @@ __global__ void __launch_bounds__(FEAT_THREADS) k_kpp_features(const Params p, c
     // block during the current one measured slower here: 156 registers
     // against 100 leave 12 warps per SM instead of 20.)
     double H = all_zero ? 0.0 : h_above;
-    constexpr int FEAT_U = 4;
+#ifndef VPHYS_FEAT_U
+#define VPHYS_FEAT_U 4
+#endif
+    constexpr int FEAT_U = VPHYS_FEAT_U;
     for (int m0 = 0; m0 < LK_LEV; m0 += FEAT_U) {
         double hk[FEAT_U], rk[FEAT_U], ua[FEAT_U], ub[FEAT_U], va[FEAT_U], vb[FEAT_U];
 #pragma unroll
