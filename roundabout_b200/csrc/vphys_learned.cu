@@ -12,10 +12,11 @@
 // (signed log1p(|x|/1e-6) of those two), each standardised with the training
 // set's mean and standard deviation.  Outputs: log(h_b / 10 m), log(h_b w_s)
 // and the shape G(sigma) * 27/4 at the 75 interfaces below the surface, each
-// standardised the same way.  The GEMMs are vphys_gemm_tn_bf16 (tcgen05).
+// standardised the same way.  Training's GEMMs are vphys_gemm_tn_bf16 (tcgen05).
 //
-// In a step with cfg.learned_kpp: k_kpp_roll -> k_kpp_features -> 3 GEMMs ->
-// k_kpp_apply, then the assembly takes h_b from the network for every column
+// In a step with cfg.learned_kpp: k_kpp_roll -> k_kpp_features -> k_mlp3 (the
+// three layers in one launch, vphys_gemm.cu) -> k_kpp_apply, then the
+// assembly takes h_b from the network for every column
 // except (a) those whose standardised features leave [-gate, gate] (range
 // gate), (b) a hashed `check_fraction` of the columns, which run the plain
 // pass 1 and count a failure when the network's h_b differs from it by more
