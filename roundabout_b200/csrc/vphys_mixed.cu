@@ -640,14 +640,13 @@ __global__ void __launch_bounds__(MP_TR_COLS) k_tracers_mp(const Params p, doubl
 // persistent CTA per SM whose first warps store their rows in tensor memory
 // (tcgen05.st of each level's (t, v) pair into the warp's 32 lanes, read
 // back eight levels at a time with tcgen05.ld; up to three warps per lane
-// quarter, 2 * nzp columns each) and whose other warps keep them in shared
-// memory: about twice the warps per SM.  The arithmetic is
+// quarter, 2 * nzp columns each); the kernel can give further warps rows in
+// shared memory, which the launcher does not use (they squeeze the L1 the
+// tracers of a column group share).  The arithmetic is
 // k_tracers_mp<false, 1, true>'s, level for level (the default knobs, one
 // factorisation, one tracer per warp); work items are (32-column group,
 // tracer), tracer fastest, strided over all warps of the grid.
 // ---------------------------------------------------------------------------
-constexpr int TM_MAX_WARPS = 24;
-
 // rows of one warp in shared memory: level k at tu[(k-1)*32], vv[(k-1)*32]
 struct SRows {
     float *tu, *vv;
@@ -946,7 +945,6 @@ static bool launch_tracers_mp_tm(const Params &p, double dt, bool nonlocal, cuda
     static int sms = 0;
     if (!attr_set) {
         cudaFuncSetAttribute(k_tracers_mp_tm<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
-        cudaFuncSetAttribute(k_tracers_mp_tm<TM_MAX_WARPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -958,12 +956,9 @@ static bool launch_tracers_mp_tm(const Params &p, double dt, bool nonlocal, cuda
     if (nitems > 0x7fffffffLL) return false;
     const int nwarps = nt + ns;
     const int grid = (int)(nitems < (long long)sms * nwarps ? (nitems + nwarps - 1) / nwarps : sms);
-    if (nwarps <= 12)
-        k_tracers_mp_tm<12><<<grid, 32 * nwarps, (size_t)ns * per_s, stream>>>(p, dt, nonlocal ? 1 : 0, ngx,
-                                                                             (int)nitems, nt, nzp);
-    else
-        k_tracers_mp_tm<TM_MAX_WARPS><<<grid, 32 * nwarps, (size_t)ns * per_s, stream>>>(p, dt, nonlocal ? 1 : 0, ngx,
-                                                                                       (int)nitems, nt, nzp);
+    // nwarps <= 12: at most three warps per lane quarter, no shared-memory rows
+    k_tracers_mp_tm<12><<<grid, 32 * nwarps, (size_t)ns * per_s, stream>>>(p, dt, nonlocal ? 1 : 0, ngx,
+                                                                         (int)nitems, nt, nzp);
     if (p.mp_redo) launch_tracers_redo(p, dt, nonlocal, stream);
     return true;
 }
