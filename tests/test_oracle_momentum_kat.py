@@ -21,7 +21,19 @@ tests' own:
       untouched without viscosity, and diffuses down with it
       (test_stress_placement_and_sign, :310-389);
   (e) a face touching land takes no stress, an all-wet face the full
-      increment (test_stress_land_masked, :391-454).
+      increment (test_stress_land_masked, :391-454);
+and from tests/test_ocean_vdiff_bbl.F90 (the harmonic face thickness and the
+bottom-boundary-layer glue, with the viscous remnant gamma):
+  (f) thickening layers, strong drag, hvel_mom6: gamma finite, in (0, 1],
+      non-decreasing from the bed up and strictly smaller at the bed
+      (test_hvel_mom6_bounded, :119-185);
+  (g) the glue on a thin bed sliver: gamma finite and in (0, 1]
+      (test_bbl_glue_finite, :187-252);
+  (h) the glue's piston damps the bed velocity harder than the plain drag
+      (test_bbl_glue_damps, :254-331);
+  (i) an exactly collapsed interior layer with viscosity across it (the
+      arithmetic face thickness is 0 there): gamma finite and in (0, 1]
+      (test_collapsed_layer_finite, :458-522).
 """
 import numpy as np
 
@@ -135,3 +147,64 @@ def test_implicit_stress_skips_faces_touching_land(oracle):
     st.call("vpo_vdiff_momentum", c, DT)
     assert abs(st.u[2, 1, NZ - 1]) < 1.0e-14
     assert abs(st.u[1, 1, NZ - 1] - DT * TAUX / (RHO0 * H0)) < 1.0e-12
+
+
+def remnant_ok(g):
+    return bool(np.isfinite(g).all() and (g > 0.0).all() and (g <= 1.0 + 1e-12).all())
+
+
+def test_remnant_with_harmonic_faces_bounded_and_monotone(oracle):
+    nz, DT, LAM = 6, 450.0, 0.08
+    c = cfg(implicit_drag=1, hvel_mom6=1, remnant=1)
+    st = oracle.OracleState(4, 4, nz, 1)
+    for k in range(nz):
+        st.h[:, :, k] = 12.0 * (k + 1)
+    interior_kv(st, 0.2)
+    st.lambda_bot_u[...] = LAM
+    st.lambda_bot_v[...] = LAM
+    st.call("vpo_vdiff_momentum", c, DT)
+    g = st.visc_rem_u[1, 1, :]
+    assert remnant_ok(g)
+    assert all(g[k] >= g[k - 1] - 1e-13 for k in range(1, nz))
+    assert g[0] < g[-1] - 1e-10
+
+
+def test_glue_remnant_finite_on_a_thin_bed_sliver(oracle):
+    c = cfg(implicit_drag=1, hvel_mom6=1, bbl_glue=1, remnant=1)
+    st = oracle.OracleState(4, 4, 4, 1)
+    for k, hk in enumerate((0.05, 1.0, 10.0, 25.0)):
+        st.h[:, :, k] = hk
+    interior_kv(st, 0.1)
+    st.lambda_bot_u[...] = 0.02
+    st.lambda_bot_v[...] = 0.02
+    st.call("vpo_vdiff_momentum", c, 600.0)
+    assert np.isfinite(st.visc_rem_u[1, 1, :]).all() and np.isfinite(st.visc_rem_v[1, 1, :]).all()
+    assert remnant_ok(st.visc_rem_u[1, 1, :])
+
+
+def test_glue_damps_the_bed_harder_than_the_plain_drag(oracle):
+    DT, LAM, U0 = 300.0, 0.01, 0.5
+    bed = []
+    for glue in (0, 1):
+        c = cfg(implicit_drag=1, hvel_mom6=1, bbl_glue=glue)
+        st = oracle.OracleState(4, 4, 4, 1)
+        for k, hk in enumerate((0.2, 5.0, 15.0, 25.0)):
+            st.h[:, :, k] = hk
+        interior_kv(st, 1.0e-4)   # below the glue's kv_bbl = bbl_piston * hbbl_visc = 3e-3
+        st.u[...] = U0
+        st.lambda_bot_u[...] = LAM
+        st.lambda_bot_v[...] = LAM
+        st.call("vpo_vdiff_momentum", c, DT)
+        bed.append(st.u[1, 1, 0])
+    assert 0.0 < bed[0] < U0
+    assert bed[1] < bed[0] - 1e-6
+
+
+def test_collapsed_interior_layer_keeps_the_remnant_finite(oracle):
+    c = cfg(hvel_mom6=0, remnant=1)
+    st = oracle.OracleState(4, 4, 4, 1)
+    for k, hk in enumerate((10.0, 0.0, 12.0, 20.0)):
+        st.h[:, :, k] = hk
+    interior_kv(st, 0.2)
+    st.call("vpo_vdiff_momentum", c, 450.0)
+    assert remnant_ok(st.visc_rem_u[1, 1, :]) and remnant_ok(st.visc_rem_v[1, 1, :])
