@@ -11,7 +11,9 @@ implicit tracer diffusion with EPBL's kd as the diffusivity.
 * collapsed top layers (:720-790): kd and MLD equal those of the column
   without them, no mixing on the interfaces above the first live layer;
 * the OM4 mstar (:243-281) in closed form on a neutral two-layer column,
-  including its zero-Ekman-term limit.
+  including its zero-Ekman-term limit;
+* the convective seed of the first cooled step, nstar (-0.5 rho0 h B0)
+  (:281-341).
 """
 import math
 
@@ -298,3 +300,20 @@ def test_tke_budget_closes(oracle, q_heat, sw):
         assert (conv > 0.0).all()
     else:
         assert (forcing < 0.0).all() or (mixing > 0.0).all()
+
+
+def test_convective_seed(oracle):
+    """The convective ledger term of the first step of pure cooling on a
+    stable column is nstar (-0.5 rho0 h_sfc B0), B0 = g alpha q_T / rho0 under
+    the linear EOS, to 1e-10 relative; the bed and surface interfaces carry
+    no diffusivity (test_ocean_epbl.F90:281-341)."""
+    nz, dz, dt, q_heat = 8, 5.0, 1800.0, -200.0
+    cfg = epbl_config(epbl_tke_diags=1)
+    st = stratified(oracle, nz, dz, 15.0, 0.05, nx=6, ny=4)
+    run_steps(st, cfg, dt, 1, 1, stress=0.0, q_heat=q_heat)
+    b0 = G * ALPHA_LIN * (q_heat / (RHO0 * CP)) / RHO0
+    ctke = -0.5 * RHO0 * dz * b0 * dt
+    assert ctke > 0.0
+    conv_expected = cfg.epbl_nstar * ctke / dt
+    assert abs(st.epbl_tke[1][3, 2] - conv_expected) < 1.0e-10 * conv_expected
+    assert abs(st.kd_epbl[3, 2, 0]) < 1.0e-30 and abs(st.kd_epbl[3, 2, nz]) < 1.0e-30
