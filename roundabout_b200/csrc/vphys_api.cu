@@ -85,6 +85,12 @@ struct vphys_handle_s {
     double *zcol = nullptr;           // column depths for the momentum face thickness
     unsigned char *mom_tiles = nullptr;   // skip flags of the TMA-staged momentum solve's face tiles
     unsigned *dev_err = nullptr;      // bounded waits of the TMA-staged solves that ran out (0: none)
+    // ks is bitwise kt: the assembly gate last wrote both under floors that
+    // agree, and the caller has written neither since, so a tracer solve may
+    // factorise once.  While a pointer to either has been handed out or a
+    // buffer is bound to either, a standalone tracer solve never assumes it.
+    bool ks_is_kt = false;
+    bool k_ptr_given = false;
     // learned KPP surrogate (vphys_kpp_attach): the caller's weights and the scratch of one inference
     vphys_kpp_model kpp{};
     bool kpp_attached = false;
@@ -108,6 +114,20 @@ struct vphys_handle_s {
 namespace {
 
 bool valid(vphys_handle h) { return h != nullptr && h->magic == MAGIC; }
+
+bool is_k_field(int field) { return field == VPHYS_FIELD_KT || field == VPHYS_FIELD_KS; }
+
+// A tracer solve run on its own factorises once only when ks is the gate's
+// copy of kt; coefficients a caller wrote or can write get two
+// factorisations (kt for temperature, ks for the rest).
+void standalone_k(vphys_handle h, Params &p)
+{
+    if (!h->ks_is_kt || h->k_ptr_given || h->f[VPHYS_FIELD_KT].bound || h->f[VPHYS_FIELD_KS].bound)
+        p.ks_equals_kt = 0;
+}
+
+// After the gate has written kt and ks: ks is bitwise kt where the floors agree.
+void gate_wrote_k(vphys_handle h) { h->ks_is_kt = h->cfg.bkgnd_profile || h->cfg.kt_bg == h->cfg.ks_bg; }
 
 int slot_of(const vphys_handle_s *h, int field)
 {
@@ -1053,6 +1073,7 @@ int vphys_set_field(vphys_handle h, int field, const void *host, size_t n)
     if (!host) return push_error(VPHYS_ERR_BAD_SHAPE, "vphys_set_field: NULL host buffer");
     int st = ensure(h, field);
     if (st) return st;
+    if (is_k_field(field)) h->ks_is_kt = false;
     cudaError_t e = cudaMemcpyAsync(h->f[sl].ptr(), host, h->f[sl].bytes(), cudaMemcpyHostToDevice, h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     return cuda_status(e, "vphys_set_field");
@@ -1106,6 +1127,7 @@ int vphys_set_field_async(vphys_handle h, int field, const void *host, size_t n)
     int st;
     const int sl = copy_slot(h, field, host, n, "vphys_set_field_async", &st);
     if (sl < 0) return st;
+    if (is_k_field(field)) h->ks_is_kt = false;
     return cuda_status(cudaMemcpyAsync(h->f[sl].ptr(), host, h->f[sl].bytes(), cudaMemcpyHostToDevice, h->stream),
                        "vphys_set_field_async");
 }
@@ -1126,6 +1148,7 @@ int vphys_get_ptr(vphys_handle h, int field, void **ptr, int *nx, int *ny, int *
     if (sl < 0) return push_error(VPHYS_ERR_NOT_FOUND, "vphys_get_ptr: unknown field id %d", field);
     int st = ensure(h, field);
     if (st) return st;
+    if (is_k_field(field)) h->k_ptr_given = true;
     if (ptr) *ptr = h->f[sl].ptr();
     bool is_int;
     size_t n = field_count(h->nx, h->ny, h->nz, field, &is_int);
@@ -1241,6 +1264,7 @@ int vphys_assemble(vphys_handle h)
     Params p = make_params(h);
     if ((st = run_learned_kpp(h, p))) return st;
     if ((st = run_assemble(h, p))) return st;
+    gate_wrote_k(h);
     if (h->cfg.vmix_guard) {
         int gs = VPHYS_OK;
         if ((st = read_guard(h, &gs))) return st;
@@ -1266,6 +1290,7 @@ int vphys_vdiff_tracers(vphys_handle h, double dt)
     if (st) return st;
     if (h->ntr == 0) return VPHYS_OK;
     Params p = make_params(h);
+    standalone_k(h, p);
     vphys::launch_tracers(p, dt, true, false, h->stream);
     return cuda_status(cudaGetLastError(), "vphys_vdiff_tracers launch");
 }
@@ -1286,6 +1311,7 @@ int vphys_vdiff_tracers_nonlocal(vphys_handle h, double dt)
     if (st) return st;
     if (h->ntr == 0) return VPHYS_OK;
     Params p = make_params(h);
+    standalone_k(h, p);
     vphys::launch_tracers(p, dt, true, h->cfg.use_kpp && !h->cfg.epbl, h->stream);
     return cuda_status(cudaGetLastError(), "vphys_vdiff_tracers_nonlocal launch");
 }
@@ -1415,6 +1441,7 @@ int vphys_step(vphys_handle h, double dt, int n_steps)
     Params p = make_params(h);
     if ((st = launch_steps(h, p, dt, n_steps))) return st;
     if ((st = cuda_status(cudaGetLastError(), "vphys_step launch"))) return st;
+    gate_wrote_k(h);
     if (h->cfg.vmix_guard) {
         int gs = VPHYS_OK;
         if ((st = read_guard(h, &gs))) return st;
@@ -1482,6 +1509,7 @@ int vphys_step_graph(vphys_handle h, double dt, int n_steps)
     cudaError_t e = cudaGraphLaunch(h->gexec, h->stream);
     if (e != cudaSuccess) return cuda_status(e, "vphys_step_graph launch");
     h->gen += n_steps;
+    gate_wrote_k(h);
     if (h->cfg.vmix_guard) {
         int gs = VPHYS_OK;
         if ((st = read_guard(h, &gs))) return st;

@@ -185,6 +185,49 @@ def test_tracers_and_nonlocal(VP, oracle, case, ntr):
             assert_bitwise(f"tracer{t} (non-local)", vp.get_tracer(t), st.tracers[t])
 
 
+def test_tracers_follow_a_caller_written_ks(VP, oracle):
+    """kt diffuses temperature and ks salinity and the passive tracers, also
+    when the caller writes ks after an assembly, through vphys_set_field or in
+    a bound buffer: the one-factorisation shortcut is only for the gate's
+    own ks, which is bitwise kt under the default floors."""
+    import torch
+
+    cols = columns(seed=23)
+    cfg = hot_cfg()
+    st = oracle_state(oracle, cols, cfg)
+    vp = gpu_state(VP, cols, cfg)
+    st.call("vpo_eos_wright", cfg)
+    vp.eos()
+    assert st.call("vpo_build_coefficients", cfg) == 0
+    vp.assemble()
+    st.ks[...] = 3.0 * st.ks
+    vp.set("ks", st.ks)
+    st.call("vpo_vdiff_tracers", cfg, DT)
+    vp.vdiff_tracers(DT)
+    for t in range(st.ntr):
+        assert_bitwise(f"tracer{t} (ks written)", vp.get_tracer(t), st.tracers[t])
+    # the gate's coefficients again: one factorisation, the same answer as the oracle
+    assert st.call("vpo_build_coefficients", cfg) == 0
+    vp.assemble()
+    st.call("vpo_vdiff_tracers", cfg, DT)
+    vp.vdiff_tracers(DT)
+    for t in range(st.ntr):
+        assert_bitwise(f"tracer{t} (gate's ks)", vp.get_tracer(t), st.tracers[t])
+    # a bound ks, scaled in place after the assembly wrote it
+    ks_t = torch.zeros(st.ks.size, dtype=torch.float64, device="cuda")
+    vp.bind("ks", ks_t)
+    assert st.call("vpo_build_coefficients", cfg) == 0
+    vp.assemble()
+    torch.cuda.synchronize()
+    ks_t.mul_(0.5)
+    torch.cuda.synchronize()
+    st.ks[...] = 0.5 * st.ks
+    st.call("vpo_vdiff_tracers", cfg, DT)
+    vp.vdiff_tracers(DT)
+    for t in range(st.ntr):
+        assert_bitwise(f"tracer{t} (bound ks)", vp.get_tracer(t), st.tracers[t])
+
+
 @pytest.mark.parametrize("shape", [(24, 20, 12), (7, 5, 1), (9, 4, 2), (33, 17, 3), (130, 9, 20)])
 def test_full_step(VP, oracle, shape):
     nx, ny, nz = shape
