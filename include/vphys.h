@@ -543,7 +543,11 @@ int vphys_vdiff_momentum(vphys_handle h, double dt);
 
 /* Backward-Euler vertical diffusion: kt on temperature, ks on salinity and
  * every other tracer.  Replaces vdiff_apply_tracers
- * (rdb_ocean_vdiff.F90:1107-1414). */
+ * (rdb_ocean_vdiff.F90:1107-1414).  One factorisation serves every tracer
+ * only while ks is the assembly gate's bitwise copy of kt (written by
+ * vphys_assemble or vphys_step under floors that agree, and neither field
+ * written by the caller since, bound to a caller's buffer or handed out by
+ * vphys_get_ptr); otherwise kt and ks are factorised separately. */
 int vphys_vdiff_tracers(vphys_handle h, double dt);
 
 /* KPP non-local tendencies on T (gamma_t), S and pseudo-salt (gamma_s),
