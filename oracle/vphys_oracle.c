@@ -3,7 +3,8 @@
  * the reference lines it restates; loop variables are 1-based like the
  * Fortran so the index arithmetic can be read against it line by line.
  *
- * Build: gcc -O2 -ffp-contract=off -fopenmp -fPIC -shared (oracle/Makefile).
+ * Build: gcc -O3 -ffp-contract=off -fno-fast-math -fopenmp -fPIC -shared
+ * (oracle/Makefile).
  */
 #include "vphys_oracle.h"
 

@@ -7,9 +7,15 @@
  * against the reference's own golden vectors (tests/test_safe_math_golden.inc,
  * transcribed by tests/golden/make_safe_math_golden.py); the physics is
  * checked against the reference's analytic known-answer tests
- * (tests/test_ocean_pp81.F90, test_ocean_kpp.F90, test_ocean_vdiff.F90,
+ * (tests/test_ocean_pp81.F90, test_ocean_kpp.F90, test_ocean_kpp_nonlocal.F90,
+ * test_ocean_kpp_convective.F90, test_ocean_buoyancy_flux.F90,
+ * test_ocean_vdiff.F90, test_ocean_vdiff_implicit_stress_drag.F90,
+ * test_ocean_vdiff_bbl.F90, test_ocean_visc_rem.F90,
  * test_ocean_vmix_assembly.F90, test_ocean_bkgnd_mixing.F90,
- * test_ocean_kpp_nonlocal.F90) re-expressed in tests/test_oracle_*.py;
+ * test_ocean_vmix_no_pp81.F90, test_ocean_convection.F90,
+ * test_ocean_kv_ml_invz2.F90, test_ocean_wright_eos.F90,
+ * test_ocean_sw_chl.F90, test_ocean_epbl_max_shear.F90) re-expressed in
+ * tests/test_oracle_*.py;
  * kappa-shear (vphys_oracle_kshear.c) against the reference's golden kd
  * profile (tests/test_ocean_kappa_shear.F90:286-393, 1e-6 relative); EPBL
  * (vphys_oracle_epbl.c) against the physical tests of test_ocean_epbl.F90.
