@@ -552,7 +552,12 @@ int vphys_vdiff_tracers(vphys_handle h, double dt);
 
 /* KPP non-local tendencies on T (gamma_t), S and pseudo-salt (gamma_s),
  * using the gamma of the last vphys_assemble.  Replaces
- * vmix_apply_nonlocal_tendencies (rdb_ocean_vmix.F90:1605-1714). */
+ * vmix_apply_nonlocal_tendencies (rdb_ocean_vmix.F90:1605-1714).  The
+ * kernel re-derives gamma per column from h, BL_DEPTH, B0, STRESS_MAG,
+ * Q_HEAT, Q_SALT and the shortwave fields rather than storing it, so those
+ * must hold what vphys_assemble read (as in the reference's stage order,
+ * where nothing writes them in between); the same holds for
+ * vphys_vdiff_tracers_nonlocal. */
 int vphys_nonlocal(vphys_handle h, double dt);
 
 /* The tracer diffusion followed by the KPP non-local tendencies, as one fused
