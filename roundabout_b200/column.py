@@ -181,9 +181,15 @@ class VerticalPhysics:
         _ffi.check(self.lib.vphys_vdiff_momentum(self._h, float(dt)), "vphys_vdiff_momentum")
 
     def vdiff_tracers(self, dt):
+        """vdiff_apply_tracers (rdb_ocean_vdiff.F90:1107-1414): kt on
+        temperature, ks on salinity and the other tracers, as the fields hold
+        them (a ks set or bound by the caller is used as written)."""
         _ffi.check(self.lib.vphys_vdiff_tracers(self._h, float(dt)), "vphys_vdiff_tracers")
 
     def nonlocal_tendencies(self, dt):
+        """vmix_apply_nonlocal_tendencies (rdb_ocean_vmix.F90:1605-1714) with the
+        gamma of the last assemble(); h, bl_depth, b0 and the forcing must
+        still hold what assemble() read."""
         _ffi.check(self.lib.vphys_nonlocal(self._h, float(dt)), "vphys_nonlocal")
 
     def vdiff_tracers_nonlocal(self, dt):
