@@ -81,6 +81,22 @@ def test_create_without_a_device_fails_cleanly(lib):
     assert _ffi.last_error(0)
 
 
+def test_python_driver_raises_without_a_device(lib):
+    """The Python driver has no CPU fallback: without a device it raises a
+    typed error carrying the library's message."""
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    from roundabout_b200 import _ffi
+    from roundabout_b200.column import VerticalPhysics
+
+    with pytest.raises(_ffi.VphysError) as err:
+        VerticalPhysics(8, 8, 4, 2)
+    assert err.value.status in (_ffi.ERR_ALLOC, _ffi.ERR_CUDA)
+    assert "vphys_create" in str(err.value)
+
+
 def test_kappa_shear_knobs_are_validated(lib):
     """The kappa-shear knobs are checked at create, before any device work."""
     from roundabout_b200 import _ffi
