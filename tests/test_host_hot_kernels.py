@@ -1,6 +1,8 @@
 """The CUDA source of the step's plain FP64 kernels -- the Wright EOS, the
-assembly (k_assemble and the 1-2-1 smoothing), the momentum face solves and
-the tracer solve with its fused non-local deposit -- compiled as host C++ and
+stress magnitude, the surface deposit, the shortwave penetration and the
+chlorophyll opacities, the assembly (k_assemble and the 1-2-1 smoothing), the
+momentum face solves and the tracer solve with its fused non-local deposit,
+and whole steps in the library's launch order -- compiled as host C++ and
 run thread by thread on the CPU, against the oracle, bit for bit.
 
 The kernels' arithmetic is plain IEEE FP64 in a fixed order without FMA
@@ -71,6 +73,12 @@ def hot(tmp_path_factory, oracle):
     L.host_assemble.restype = ctypes.c_ulonglong
     L.host_momentum.argtypes = [ctypes.c_void_p, S, ctypes.c_double, ctypes.c_int]
     L.host_tracers.argtypes = [ctypes.c_void_p, S, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    for fn in ("host_stress_mag", "host_sw_chl_kappa"):
+        getattr(L, fn).argtypes = [ctypes.c_void_p, S]
+    for fn in ("host_surface_flux", "host_sw_penetration"):
+        getattr(L, fn).argtypes = [ctypes.c_void_p, S, ctypes.c_double]
+    L.host_step.argtypes = [ctypes.c_void_p, S, ctypes.c_double, ctypes.c_int]
+    L.host_step.restype = ctypes.c_ulonglong
     return L
 
 
@@ -200,3 +208,74 @@ def test_fused_tracer_launch_and_a_caller_written_ks(oracle, hot):
     run(hot, "host_tracers", cfg, host, DT, 1, 1, 0)
     for t in range(4):
         assert_bitwise(f"tracer{t}", host.tracers[t], ref.tracers[t])
+
+
+SW = dict(sw_pen_frac=0.6, sw_band_ratio=0.58, sw_zeta1=0.35, sw_zeta2=23.0)
+CHL = dict(sw_pen_frac=1.0, sw_chl=1)
+FORCING = {
+    "deposit_budgets": dict(budgets=1),
+    "two_band": dict(SW),
+    "two_band_qsw_wetdyn": dict(SW, sw_source=1, use_wet_dyn=1, budgets=1),
+    "chlorophyll": dict(CHL),
+    "cover_bound_salinity": dict(SW, use_cover_frac=1, bound_salinity=1, min_salinity=34.5),
+}
+
+
+@pytest.mark.parametrize("shape", [(24, 20, 12), (9, 4, 2), (20, 9, 75)])
+@pytest.mark.parametrize("case", sorted(FORCING))
+def test_forcing_kernels_source_matches_oracle(oracle, hot, shape, case):
+    nx, ny, nz = shape
+    cfg = hot_cfg(surface_flux=1, **FORCING[case])
+    host, ref = state_pair(oracle, shape, cfg, seed=3 * sum(shape) + len(case), thin=0.15)
+    rng = np.random.default_rng(sum(shape))
+    extra = {"sw_net": rng.uniform(0.0, 300.0, (nx, ny)), "wet_dyn": (rng.random((nx, ny)) > 0.2) * 1.0,
+             "sw_chl": rng.uniform(-1.0, 3.0, (nx, ny)), "cover_frac": rng.uniform(0.0, 1.0, (nx, ny))}
+    for s in (host, ref):
+        s.q_heat[...] = np.abs(s.q_heat) + 50.0
+        for n, a in extra.items():
+            getattr(s, n)[...] = a
+    ref.stress_mag[...] = 0.0
+    ref.stress_mag_from_tau()
+    run(hot, "host_stress_mag", cfg, host)
+    assert_bitwise("stress_mag", host.stress_mag, ref.stress_mag)
+    if cfg.sw_chl:
+        ref.call("vpo_sw_chl_kappa", cfg)
+        run(hot, "host_sw_chl_kappa", cfg, host)
+        assert_bitwise("sw_kappa", host.sw_kappa, ref.sw_kappa)
+    ref.call("vpo_surface_flux", cfg, DT)
+    run(hot, "host_surface_flux", cfg, host, DT)
+    ref.call("vpo_sw_penetration", cfg, DT)
+    run(hot, "host_sw_penetration", cfg, host, DT)
+    for t in range(ref.ntr):
+        assert_bitwise(f"tracer{t}", host.tracers[t], ref.tracers[t])
+    if cfg.budgets:
+        assert_bitwise("heat_budget_surface", host.heat_budget_surface, ref.heat_budget_surface)
+        assert_bitwise("salt_budget_surface", host.salt_budget_surface, ref.salt_budget_surface)
+
+
+STEP = {
+    "hot_path_budgets": dict(budgets=1),
+    "surface_two_band": dict(SW, surface_flux=1, budgets=1),
+    "none_closure_smoothing": dict(interior_closure=4, kd_smooth_iterations=1),
+    "remnant_glue_drag": dict(remnant=1, bbl_glue=1, implicit_drag=1, implicit_stress=1),
+}
+
+
+@pytest.mark.parametrize("shape", [(24, 20, 12), (7, 5, 1), (9, 4, 2), (20, 9, 75)])
+@pytest.mark.parametrize("case", sorted(STEP))
+def test_three_steps_match_the_oracle_step(oracle, hot, shape, case):
+    cfg = hot_cfg(**STEP[case])
+    host, ref = state_pair(oracle, shape, cfg, seed=5 * sum(shape) + len(case), thin=0.1)
+    rng = np.random.default_rng(len(case))
+    for n in ("lambda_bot_u", "lambda_bot_v"):
+        a = rng.uniform(0.0, 1.0e-4, getattr(ref, n).shape)
+        getattr(ref, n)[...] = a
+        getattr(host, n)[...] = a
+    assert ref.call("vpo_step", cfg, DT, 3) == 0
+    assert run(hot, "host_step", cfg, host, DT, 3) == 0
+    for n in ("kv", "kt", "ks", "u", "v", "bl_depth", "b0", "rho"):
+        assert_bitwise(n, getattr(host, n), getattr(ref, n))
+    for t in range(ref.ntr):
+        assert_bitwise(f"tracer{t}", host.tracers[t], ref.tracers[t])
+    if cfg.budgets:
+        assert_bitwise("heat_budget", host.heat_budget, ref.heat_budget)
