@@ -279,3 +279,28 @@ def test_three_steps_match_the_oracle_step(oracle, hot, shape, case):
         assert_bitwise(f"tracer{t}", host.tracers[t], ref.tracers[t])
     if cfg.budgets:
         assert_bitwise("heat_budget", host.heat_budget, ref.heat_budget)
+
+
+@pytest.mark.parametrize("shape", [(24, 20, 12), (9, 4, 3), (20, 9, 75)])
+def test_zlevel_faces_source_matches_oracle(oracle, hot, shape):
+    """The momentum solve with caller-set first-live indices on the faces
+    (the z-level faces: ocean_vcoord_k_bot_from_target's rule, the larger of
+    the two cells' first live layers)."""
+    cfg = hot_cfg(zlevel_faces=1)
+    host, ref = state_pair(oracle, shape, cfg, seed=7 * sum(shape), thin=0.2)
+    nx, ny, _ = shape
+    live = ref.h > 1.5e-4
+    kb = np.where(live.any(2), live.argmax(2) + 1, 1)
+    ia, ib = np.clip(np.arange(nx + 1) - 1, 0, nx - 1), np.clip(np.arange(nx + 1), 0, nx - 1)
+    ja, jb = np.clip(np.arange(ny + 1) - 1, 0, ny - 1), np.clip(np.arange(ny + 1), 0, ny - 1)
+    for s in (host, ref):
+        s.k_bot_u[...] = np.maximum(kb[ia, :], kb[ib, :])
+        s.k_bot_v[...] = np.maximum(kb[:, ja], kb[:, jb])
+    ref.call("vpo_eos_wright", cfg)
+    assert ref.call("vpo_build_coefficients", cfg) == 0
+    for n in ("rho", "kv", "kt", "ks", "bl_depth", "b0"):
+        getattr(host, n)[...] = getattr(ref, n)
+    ref.call("vpo_vdiff_momentum", cfg, DT)
+    run(hot, "host_momentum", cfg, host, DT, 1)
+    for n in ("u", "v"):
+        assert_bitwise(n, getattr(host, n), getattr(ref, n))
