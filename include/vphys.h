@@ -391,7 +391,8 @@ typedef struct vphys_handle_s *vphys_handle;
 
 /* ---- lifecycle ------------------------------------------------------- */
 
-/* Fill *cfg with the reference defaults listed above. */
+/* Fill *cfg with the reference defaults listed above (each field cites its
+ * namelist key and type default). */
 int vphys_config_default(vphys_config *cfg);
 
 /* Allocate a handle for an (nx, ny, nz) grid with ntracer tracers and
@@ -403,27 +404,35 @@ int vphys_config_default(vphys_config *cfg);
 int vphys_create(int nx, int ny, int nz, int ntracer, const vphys_config *cfg,
                  vphys_handle *out);
 
-/* Idempotent on NULL; frees every handle-owned buffer; *h = NULL. */
+/* Idempotent on NULL; frees every handle-owned buffer; *h = NULL.  Replaces
+ * rdb_ocean_destroy (include/rdb_ocean.h:119). */
 int vphys_destroy(vphys_handle *h);
 
-/* Replace the configuration (validated; VPHYS_ERR_CONFIG on a bad one). */
+/* Replace the configuration (validated; VPHYS_ERR_CONFIG on a bad one).  No
+ * counterpart in the reference's C ABI, whose configuration is the namelist
+ * text of rdb_ocean_create_from_string (include/rdb_ocean.h:108). */
 int vphys_set_config(vphys_handle h, const vphys_config *cfg);
 int vphys_get_config(vphys_handle h, vphys_config *cfg);
 
 /* Run the handle's work on this CUDA stream (cudaStream_t as void*;
- * NULL = the legacy default stream). */
+ * NULL = the legacy default stream).  No counterpart in the reference. */
 int vphys_set_stream(vphys_handle h, void *stream);
 
 /* Zero-copy: use the caller's device array for `field` from now on.
  * The pointer must stay valid while the handle uses it.  The handle's own
  * buffer for the field is freed (a bound state is never held twice); NULL
  * unbinds and gives the field a fresh handle-owned buffer with its default
- * contents.  Synchronises the device when a buffer is freed. */
+ * contents.  Synchronises the device when a buffer is freed.  The other
+ * direction of the reference's zero-copy getters rdb_ocean_get_*_ptr
+ * (include/rdb_ocean.h:338-387), which vphys_get_ptr replaces. */
 int vphys_bind(vphys_handle h, int field, void *device_ptr);
 
 /* Synchronous host<->device copies of a whole field (n = element count,
  * checked against the field's shape: VPHYS_ERR_BAD_SHAPE).  Double fields
- * take double*, the K_TOP/K_BOT fields int32*. */
+ * take double*, the K_TOP/K_BOT fields int32*.  Replace the setters
+ * rdb_ocean_set_h / _u / _v / _wind / _heat_flux / _salt_flux / _tracer
+ * (include/rdb_ocean.h:419-447) and, for reading, rdb_ocean_refresh_host
+ * (:327) with the host arrays. */
 int vphys_set_field(vphys_handle h, int field, const void *host, size_t n);
 int vphys_get_field(vphys_handle h, int field, void *host, size_t n);
 
@@ -518,7 +527,8 @@ int vphys_epbl(vphys_handle h, double dt);
 /* Mixed-precision tracer solves (mixed_precision >= 1): the number of
  * (32-column group, tracer) pairs whose one-step increment reached 2 units
  * in the last solve and were re-solved on the FP64 path (bitwise the exact
- * results).  Synchronises the handle's stream; 0 when nothing is mixed. */
+ * results).  Synchronises the handle's stream; 0 when nothing is mixed.  No
+ * counterpart in the reference. */
 int vphys_mixed_redo_count(vphys_handle h, unsigned *groups);
 
 /* The whole coefficient build: interior closure (PP81 or background seed),
@@ -602,10 +612,12 @@ int vphys_step(vphys_handle h, double dt, int n_steps);
  * handle's stream; a change of any bound pointer, of the configuration, of
  * dt, n_steps or of the attached surrogate recaptures.  Results are those of
  * vphys_step(h, dt, n_steps).  (The learned KPP's sampled-check columns are
- * fixed per capture.)  Asynchronous. */
+ * fixed per capture.)  Asynchronous.  No counterpart in the reference: the
+ * CUDA-graph form of vphys_step. */
 int vphys_step_graph(vphys_handle h, double dt, int n_steps);
 
-/* Block until the handle's stream is idle; VPHYS_ERR_CUDA on a CUDA error. */
+/* Block until the handle's stream is idle; VPHYS_ERR_CUDA on a CUDA error.
+ * No counterpart in the reference (whose calls return synchronised). */
 int vphys_synchronize(vphys_handle h);
 
 /* ---- errors ------------------------------------------------------------
@@ -614,14 +626,16 @@ int vphys_synchronize(vphys_handle h);
  * out of range or cap <= 0 (rdb_ocean_last_error, include/rdb_ocean.h:314). */
 int vphys_last_error(int idx, char *buf, int cap);
 
-/* Library version string (static storage). */
+/* Library version string (static storage).  No counterpart in the
+ * reference's C ABI. */
 const char *vphys_version(void);
 
 /* Device self-test of the exact division used by the kernels (a zero-guarded
  * quotient and a shared-reciprocal quotient with Markstein's correction):
  * compares both with the IEEE quotient a/b on n_pairs seeded operand pairs,
  * exponents in [emin, emin+erange), and writes the number of differing bits
- * patterns to *mismatches (0 expected).  Synchronous. */
+ * patterns to *mismatches (0 expected).  Synchronous.  No counterpart in the
+ * reference. */
 int vphys_selftest_division(long long n_pairs, unsigned long long seed, int emin, int erange,
                             unsigned long long *mismatches);
 
@@ -644,7 +658,8 @@ int vphys_smooth_121_static(double *fld, const double *wet, int nx, int ny, int 
                             void *stream);
 
 /* sizeof(vphys_config) as compiled into the library, so a binding in another
- * language can verify its mirror of the struct before passing one. */
+ * language can verify its mirror of the struct before passing one.  No
+ * counterpart in the reference (its configuration is namelist text). */
 size_t vphys_config_sizeof(void);
 
 /* ---- learned KPP surrogate: building blocks ---------------------------------
