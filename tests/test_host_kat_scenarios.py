@@ -3,11 +3,14 @@ tests/test_gpu_kat_scenarios.py: thin bed slivers under strong drag,
 collapsed and pinched layers, the glue, the no-slip remnant, KPP mixed and
 neutral columns, the closure "none", convection, the surface viscosity band,
 Bryan-Lewis floors, smoothing around a dry column, tracers with their own
-diffusivities, Manizza opacities, Wright states) run through the CUDA source
-of the plain kernels compiled for the host (tests/test_host_hot_kernels.py)
-and compared with the oracle bit for bit, in every CPU run of the suite.
-The kappa-shear and EPBL scenarios need those kernels' own sources, which
-tests/test_host_kernels.py checks."""
+diffusivities, Manizza opacities, Wright states, kappa-shear over the closure
+"none" and under the EPBL combines) run through the CUDA source of the
+kernels compiled for the host (the plain step's kernels of
+tests/test_host_hot_kernels.py, the kappa-shear kernel of
+tests/test_host_kernels.py) and compared with the oracle bit for bit, in
+every CPU run of the suite."""
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -15,6 +18,7 @@ from roundabout_b200.config import INTERIOR_NONE, INTERIOR_PP81
 from tests import test_gpu_kat_scenarios as K
 from tests._cases import assert_bitwise
 from tests.test_host_hot_kernels import hot, run  # noqa: F401  (the compiled host kernels)
+from tests.test_host_kernels import _ptr, host_libs  # noqa: F401  (the kappa-shear host kernel)
 
 COEFFS = K.COEFFS
 
@@ -302,3 +306,40 @@ def test_wright_at_the_reference_states(oracle, hot):
     st.call("vpo_eos_wright", c)
     run(hot, "host_eos", c, host)
     same(host, st, ("rho",))
+
+
+# ---------------------------------------- kappa-shear and the EPBL merges ----
+
+def host_kappa_shear(host_libs, c, st, dt):
+    host_libs["kshear"].host_kappa_shear(ctypes.byref(c), st.nx, st.ny, st.nz, _ptr(st.h), _ptr(st.u), _ptr(st.v),
+                                         _ptr(st.tracers[c.idx_temperature]), _ptr(st.tracers[c.idx_salinity]),
+                                         _ptr(st.wet), _ptr(st.coriolis), ctypes.c_double(dt), _ptr(st.kd_shear),
+                                         _ptr(st.tke_shear))
+
+
+@pytest.mark.parametrize("du", [0.0, 0.2])
+def test_interior_none_with_kappa_shear(oracle, hot, host_libs, du):
+    c = K.shear_cfg()
+    st = K.shear_jump(oracle, c, du)
+    host = clone(oracle, st)
+    st.call("vpo_kappa_shear", c, 1800.0)
+    host_kappa_shear(host_libs, c, host, 1800.0)
+    same(host, st, ("kd_shear", "tke_shear"))
+    assert st.call("vpo_build_coefficients", c) == 0
+    assert run(hot, "host_assemble", c, host) == 0
+    same(host, st, ("kv", "kt", "ks"))
+
+
+@pytest.mark.parametrize("combine", [1, 2, 3])
+def test_epbl_combines_over_kappa_shear(oracle, hot, host_libs, combine):
+    c = K.shear_cfg(epbl=1, epbl_prandtl=1.5, epbl_combine=combine)
+    st = K.shear_jump(oracle, c, 0.2)
+    st.kd_epbl[...] = 0.0
+    st.kd_epbl[:, :, 2] = 0.05
+    st.kd_epbl[:, :, 6] = 1.0e-4
+    host = clone(oracle, st)
+    st.call("vpo_kappa_shear", c, 1800.0)
+    host_kappa_shear(host_libs, c, host, 1800.0)
+    assert st.call("vpo_build_coefficients", c) == 0
+    assert run(hot, "host_assemble", c, host) == 0
+    same(host, st, ("kv", "kt", "ks"))
