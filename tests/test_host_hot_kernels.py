@@ -304,3 +304,32 @@ def test_zlevel_faces_source_matches_oracle(oracle, hot, shape):
     run(hot, "host_momentum", cfg, host, DT, 1)
     for n in ("u", "v"):
         assert_bitwise(n, getattr(host, n), getattr(ref, n))
+
+
+@pytest.mark.parametrize("shape", [(24, 20, 12), (9, 4, 2), (20, 9, 75)])
+@pytest.mark.parametrize("case", sorted(ASSEMBLE))
+def test_fp32_assembly_source_within_fp32_of_the_oracle(oracle, hot, shape, case):
+    """k_assemble<float> (mixed_precision = 2: the boundary-layer walk in FP64,
+    the interface sweep in FP32) against the FP64 oracle: bl_depth and b0 bit
+    for bit; kv, kt, ks within 5e-5 relative; gamma within 1e-5 of its
+    field's largest value (its shape function cancels to ~0 at the base of
+    the layer).  The host stands an exact quotient in for the GPU's fast
+    FP32 one, so the GPU tests bound the kernel's own FP32 results."""
+    cfg = hot_cfg(**ASSEMBLE[case])
+    cfg32 = hot_cfg(mixed_precision=2, **ASSEMBLE[case])
+    host, ref = state_pair(oracle, shape, cfg, seed=sum(shape) + 11 * len(case))
+    ref.call("vpo_eos_wright", cfg)
+    host.rho[...] = ref.rho
+    lagged = np.abs(np.sin(np.arange(ref.bl_depth.size))).reshape(ref.bl_depth.shape, order="F") * 80.0
+    for s in (host, ref):
+        s.bl_depth[...] = lagged
+    assert ref.call("vpo_build_coefficients", cfg) == 0
+    assert run(hot, "host_assemble", cfg32, host) == 0
+    for n in ("bl_depth", "b0"):
+        assert_bitwise(n, getattr(host, n), getattr(ref, n))
+    for n in ("kv", "kt", "ks"):
+        a, b = getattr(host, n), getattr(ref, n)
+        assert (np.abs(a - b) <= 5.0e-5 * np.abs(b)).all(), (n, np.abs(a - b).max())
+    for n in ("gamma_t", "gamma_s"):
+        a, b = getattr(host, n), getattr(ref, n)
+        assert np.abs(a - b).max() <= 1.0e-5 * max(np.abs(b).max(), 1e-300), n
